@@ -1,0 +1,190 @@
+/*
+ * softflow_gpu.h -- C ABI of the B200 implementation of the SoftFlow
+ * per-timestep hot path (libsoftflow_b200.so).
+ *
+ * The library replaces the bodies of the reference engine's step
+ * (ramc77/SoftFlow src/engine/simulation.cpp:470-801): lattice moments,
+ * BGK / MRT / regularized collision with Guo forcing, streaming with
+ * halfway bounce-back, body force and force cap, Peskin 4-point IBM spread /
+ * interpolation / multi-direct forcing, membrane forces, soft contact,
+ * marker motion, and the advection-diffusion scalar step.
+ *
+ * Conventions
+ *   - Every entry point returns an int status: SFG_OK (0) or an SFG_ERR_*
+ *     code; sfg_last_error() gives the message.  No exception crosses the
+ *     ABI.  A caller maps a nonzero status to its own error type (the
+ *     reference engine throws std::runtime_error, which pybind11 turns into
+ *     a Python exception).
+ *   - Host arrays are FP64 in the reference's canonical layouts:
+ *     populations [9][ny][nx] (LatticeField::f_, lattice_field.h:53-56),
+ *     scalar fields [ny][nx], marker vectors [markers][2] in capsule-major,
+ *     node-minor order (CapsuleSystem iteration order).
+ *   - A context holds one or more independent channels ("ensemble"); every
+ *     step advances all of them with one launch per kernel phase.
+ *   - A context is driven by one host thread.
+ */
+#ifndef SOFTFLOW_GPU_H
+#define SOFTFLOW_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SFG_ABI_VERSION 1
+
+enum sfg_status {
+    SFG_OK = 0,
+    SFG_ERR_ARG = 1,       /* invalid argument (caller error)                 */
+    SFG_ERR_STATE = 2,     /* call not valid in the context's current state   */
+    SFG_ERR_CUDA = 3,      /* CUDA runtime error (message has the CUDA text)  */
+    SFG_ERR_CAPACITY = 4,  /* a fixed capacity was exceeded                   */
+    SFG_ERR_NUMERIC = 5    /* non-finite marker state was detected            */
+};
+
+/* Storage precision of the lattice populations. */
+enum sfg_precision {
+    SFG_FP64 = 0,   /* FP64 storage and arithmetic                              */
+    SFG_FP32 = 1,   /* FP32 storage and arithmetic                              */
+    SFG_FP16S = 2   /* FP16 storage of f - w (rounded to nearest even), FP32 math */
+};
+
+enum sfg_collision { SFG_BGK = 0, SFG_MRT = 1, SFG_REGULARIZED = 2 };
+enum sfg_membrane_model { SFG_HOOKEAN = 0, SFG_NEO_HOOKEAN = 1, SFG_SKALAK = 2, SFG_WLC = 3 };
+
+/* Channel parameters: the fields of the reference SimulationParams that the
+ * path reads (src/core/parameters.h:41-342), for a channel periodic in x
+ * with SOLID rows 0 and ny-1 (or periodic in y). */
+typedef struct sfg_channel_params {
+    int nx, ny;
+    int collision;              /* sfg_collision                               */
+    double tau, rho0;
+    double mrt_se, mrt_s_eps, mrt_sq;
+    double body_fx, body_fy;
+    int periodic_y;
+    double max_lattice_force;
+    int ibm_iterations;
+    double dt;
+    double rep_epsilon, rep_sigma, rep_r_cut;
+    int rep_power;
+    double rep_damping_normal, rep_friction;
+    int scalar_enabled;
+    double scalar_D;
+    int scalar_periodic_y;
+    double scalar_inlet;
+} sfg_channel_params;
+
+/* Membrane parameters (reference MembraneParams, parameters.h:82-136). */
+typedef struct sfg_membrane_params {
+    int model;                  /* sfg_membrane_model */
+    double k_stretch, G_s, C_skalak;
+    double wlc_L_max_ratio, wlc_kBT_p, wlc_k_pow;
+    double k_bend;
+    int use_helfrich;
+    double kappa_0;
+    double k_area, k_perimeter, gamma_visc, eta_membrane;
+} sfg_membrane_params;
+
+/* Rest state of one capsule (reference Capsule constructor,
+ * src/membrane/capsule.cpp:7-141). */
+typedef struct sfg_capsule_rest {
+    int num_nodes;
+    double rest_area, rest_perimeter;
+    double wlc_kBT_p, wlc_k_pow;    /* resolved WLC constants (capsule.cpp:92-123) */
+} sfg_capsule_rest;
+
+typedef struct sfg_context sfg_context;
+
+/* ---- library ------------------------------------------------------------ */
+int sfg_abi_version(void);
+/* Message of the last failed call on this thread (empty if none). */
+const char* sfg_last_error(void);
+
+/* ---- host-side setup helpers (no device work) ---------------------------
+ * Rest geometry of a circular capsule: replaces Capsule::Capsule
+ * (capsule.cpp:7-141) for CapsuleShape::CIRCLE.  num_nodes <= 0 selects
+ * Capsule::computeOptimalNodes (capsule.h:14-17); *rest_out->num_nodes
+ * reports the count used.  Output arrays hold at least that many nodes
+ * (pos: 2 per node).  rest_ang / rest_ds are zero unless use_helfrich. */
+int sfg_build_circle_capsule(double cx, double cy, double radius, int num_nodes,
+                             const sfg_membrane_params* mp, sfg_capsule_rest* rest_out,
+                             double* pos_out, double* rest_len_out, double* rest_ang_out,
+                             double* rest_ds_out, int capacity);
+
+/* Seeded rejection placement: replaces Simulation::addCapsuleRandom
+ * (simulation.cpp:220-274), same std::mt19937 draws.  existing_centroid
+ * [n_existing][2] and existing_radius [n_existing] describe capsules already
+ * in the channel.  Placed centres/radii go to out_center [cap][2] and
+ * out_radius [cap]; *n_placed and *n_attempts are set. */
+int sfg_place_random(int count, double x0, double y0, double x1, double y1, double rmin,
+                     double rmax, int num_nodes, int seed, double min_gap, int max_attempts,
+                     int check_walls, int nx, int ny, int n_existing,
+                     const double* existing_centroid, const double* existing_radius,
+                     int capacity, double* out_center, double* out_radius, int* n_placed,
+                     int* n_attempts);
+
+/* ---- context ------------------------------------------------------------ */
+int sfg_create(int device, int precision, sfg_context** out);
+int sfg_destroy(sfg_context* ctx);
+
+/* Adds a channel (before sfg_initialize).  Replaces LBMSolver construction
+ * (lbm_solver.cpp:12-67) and the parameter plumbing of Simulation. */
+int sfg_add_channel(sfg_context* ctx, const sfg_channel_params* p, int* channel_out);
+
+/* Adds one capsule to a channel (before sfg_initialize): node positions
+ * pos [n][2], rest edge lengths, Helfrich rest angles and arc lengths (may be
+ * NULL when use_helfrich == 0).  Replaces CapsuleSystem::addCapsule
+ * (capsule_system.cpp:5-9). */
+int sfg_add_capsule(sfg_context* ctx, int channel, const sfg_membrane_params* mp,
+                    const sfg_capsule_rest* rest, const double* pos, const double* rest_len,
+                    const double* rest_ang, const double* rest_ds, int* capsule_out);
+
+/* Allocates device state and sets every channel to equilibrium at rho0 with
+ * u = 0 (LBMSolver::initialize, lbm_solver.cpp:130-170; scalar initialised to
+ * zero, advection_diffusion.cpp:46-57). */
+int sfg_initialize(sfg_context* ctx);
+
+/* Advances every channel by nsteps steps of Simulation::step
+ * (simulation.cpp:470-700).  Asynchronous: returns after enqueueing. */
+int sfg_step(sfg_context* ctx, int nsteps);
+
+/* Waits for queued work; reports kernel status bits (see softflow docs) and
+ * returns SFG_ERR_NUMERIC if a non-finite marker was seen. */
+int sfg_synchronize(sfg_context* ctx, unsigned* status_out);
+
+/* ---- state transfer (synchronous) ---------------------------------------- */
+int sfg_get_populations(sfg_context* ctx, int channel, double* f);
+int sfg_set_populations(sfg_context* ctx, int channel, const double* f);
+/* rho, u and the lattice force of the last step (any pointer may be NULL),
+ * as LatticeField::computeMacroscopic leaves them (lattice_field.cpp:28-73). */
+int sfg_get_macroscopic(sfg_context* ctx, int channel, double* rho, double* ux, double* uy,
+                        double* Fx, double* Fy);
+int sfg_get_markers(sfg_context* ctx, int channel, double* pos, double* vel, double* force);
+int sfg_set_markers(sfg_context* ctx, int channel, const double* pos, const double* vel);
+/* Concentration field and equilibrium populations g = w C
+ * (AdvectionDiffusion::setRegion semantics, advection_diffusion.cpp:59-71). */
+int sfg_set_concentration(sfg_context* ctx, int channel, const double* C);
+/* Concentration (and, if g != NULL, the scalar populations [9][ny][nx]). */
+int sfg_get_concentration(sfg_context* ctx, int channel, double* C, double* g);
+/* Cells whose force was capped in the last step (Simulation::
+ * last_capped_nodes_, simulation.cpp:588-609). */
+int sfg_get_capped_count(sfg_context* ctx, int channel, int* count);
+/* Contact pairs visited per marker in the last step (cell-list bookkeeping). */
+int sfg_get_contact_counts(sfg_context* ctx, int channel, int* counts);
+
+/* ---- diagnostics ---------------------------------------------------------- */
+int sfg_num_channels(const sfg_context* ctx, int* n);
+int sfg_channel_counts(const sfg_context* ctx, int channel, int* num_capsules, int* num_markers);
+int sfg_step_count(const sfg_context* ctx, long long* steps);
+/* Kernel launches issued per step (for launch accounting). */
+int sfg_launches_per_step(const sfg_context* ctx, int* launches);
+/* Host-visible timing of the last sfg_step call in milliseconds, measured
+ * with CUDA events on the context stream (valid after sfg_synchronize). */
+int sfg_last_step_ms(sfg_context* ctx, float* ms);
+/* CUDA stream of the context (cudaStream_t), for callers that interleave
+ * their own work. */
+int sfg_get_stream(const sfg_context* ctx, void** stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SOFTFLOW_GPU_H */

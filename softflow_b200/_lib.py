@@ -1,0 +1,137 @@
+"""ctypes binding of libsoftflow_b200.so (include/softflow_gpu.h).
+
+The library is built in-tree (``python -m softflow_b200.build``).  There is no
+CPU fallback: if the library is missing or cannot be loaded, importing the
+engine raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsoftflow_b200.so")
+
+SFG_FP64, SFG_FP32, SFG_FP16S = 0, 1, 2
+PRECISIONS = {"fp64": SFG_FP64, "fp32": SFG_FP32, "fp16s": SFG_FP16S}
+
+STATUS_NAN_MARKER = 1
+STATUS_LIST_OVERFLOW = 2
+STATUS_CAPSULE_TOO_BIG = 4
+
+
+class ChannelParamsC(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("collision", C.c_int),
+        ("tau", C.c_double), ("rho0", C.c_double),
+        ("mrt_se", C.c_double), ("mrt_s_eps", C.c_double), ("mrt_sq", C.c_double),
+        ("body_fx", C.c_double), ("body_fy", C.c_double),
+        ("periodic_y", C.c_int), ("max_lattice_force", C.c_double),
+        ("ibm_iterations", C.c_int), ("dt", C.c_double),
+        ("rep_epsilon", C.c_double), ("rep_sigma", C.c_double), ("rep_r_cut", C.c_double),
+        ("rep_power", C.c_int), ("rep_damping_normal", C.c_double), ("rep_friction", C.c_double),
+        ("scalar_enabled", C.c_int), ("scalar_D", C.c_double),
+        ("scalar_periodic_y", C.c_int), ("scalar_inlet", C.c_double),
+    ]
+
+
+class MembraneParamsC(C.Structure):
+    _fields_ = [
+        ("model", C.c_int), ("k_stretch", C.c_double), ("G_s", C.c_double),
+        ("C_skalak", C.c_double), ("wlc_L_max_ratio", C.c_double),
+        ("wlc_kBT_p", C.c_double), ("wlc_k_pow", C.c_double), ("k_bend", C.c_double),
+        ("use_helfrich", C.c_int), ("kappa_0", C.c_double), ("k_area", C.c_double),
+        ("k_perimeter", C.c_double), ("gamma_visc", C.c_double), ("eta_membrane", C.c_double),
+    ]
+
+
+class CapsuleRestC(C.Structure):
+    _fields_ = [
+        ("num_nodes", C.c_int), ("rest_area", C.c_double), ("rest_perimeter", C.c_double),
+        ("wlc_kBT_p", C.c_double), ("wlc_k_pow", C.c_double),
+    ]
+
+
+class SoftFlowGpuError(RuntimeError):
+    """Raised when a C-ABI call returns a nonzero status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[sfg status {code}] {message}")
+        self.code = code
+
+
+_lib = None
+
+_P = C.POINTER
+_D = _P(C.c_double)
+_I = _P(C.c_int)
+SIGNATURES = {
+    "sfg_abi_version": (C.c_int, []),
+    "sfg_last_error": (C.c_char_p, []),
+    "sfg_build_circle_capsule": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int,
+                                           _P(MembraneParamsC), _P(CapsuleRestC), _D, _D, _D, _D,
+                                           C.c_int]),
+    "sfg_place_random": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                   C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int,
+                                   C.c_int, C.c_int, C.c_int, C.c_int, _D, _D, C.c_int, _D, _D,
+                                   _I, _I]),
+    "sfg_create": (C.c_int, [C.c_int, C.c_int, _P(C.c_void_p)]),
+    "sfg_destroy": (C.c_int, [C.c_void_p]),
+    "sfg_add_channel": (C.c_int, [C.c_void_p, _P(ChannelParamsC), _I]),
+    "sfg_add_capsule": (C.c_int, [C.c_void_p, C.c_int, _P(MembraneParamsC), _P(CapsuleRestC),
+                                  _D, _D, _D, _D, _I]),
+    "sfg_initialize": (C.c_int, [C.c_void_p]),
+    "sfg_step": (C.c_int, [C.c_void_p, C.c_int]),
+    "sfg_synchronize": (C.c_int, [C.c_void_p, _P(C.c_uint)]),
+    "sfg_get_populations": (C.c_int, [C.c_void_p, C.c_int, _D]),
+    "sfg_set_populations": (C.c_int, [C.c_void_p, C.c_int, _D]),
+    "sfg_get_macroscopic": (C.c_int, [C.c_void_p, C.c_int, _D, _D, _D, _D, _D]),
+    "sfg_get_markers": (C.c_int, [C.c_void_p, C.c_int, _D, _D, _D]),
+    "sfg_set_markers": (C.c_int, [C.c_void_p, C.c_int, _D, _D]),
+    "sfg_set_concentration": (C.c_int, [C.c_void_p, C.c_int, _D]),
+    "sfg_get_concentration": (C.c_int, [C.c_void_p, C.c_int, _D, _D]),
+    "sfg_get_capped_count": (C.c_int, [C.c_void_p, C.c_int, _I]),
+    "sfg_get_contact_counts": (C.c_int, [C.c_void_p, C.c_int, _I]),
+    "sfg_num_channels": (C.c_int, [C.c_void_p, _I]),
+    "sfg_channel_counts": (C.c_int, [C.c_void_p, C.c_int, _I, _I]),
+    "sfg_step_count": (C.c_int, [C.c_void_p, _P(C.c_longlong)]),
+    "sfg_launches_per_step": (C.c_int, [C.c_void_p, _I]),
+    "sfg_last_step_ms": (C.c_int, [C.c_void_p, _P(C.c_float)]),
+    "sfg_get_stream": (C.c_int, [C.c_void_p, _P(C.c_void_p)]),
+}
+
+
+def lib():
+    """Load the library (once).  Raises if it is missing: no fallback."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing; build it with `python -m softflow_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def check(code: int) -> None:
+    if code != 0:
+        msg = lib().sfg_last_error().decode(errors="replace")
+        raise SoftFlowGpuError(code, msg)
+
+
+def dptr(a):
+    """numpy float64 array -> double* (None passes through)."""
+    if a is None:
+        return None
+    return a.ctypes.data_as(_D)
+
+
+def iptr(a):
+    if a is None:
+        return None
+    return a.ctypes.data_as(_I)

@@ -1,0 +1,159 @@
+// collide.cuh -- D2Q9 collision operators with Guo forcing, one cell in registers.
+//
+// The arithmetic keeps the reference's evaluation order (bgk_collision.cpp:42-85,
+// regularized_bgk.cpp:123-180, mrt_collision.cpp:239-322) so that the FP64
+// instantiation, compiled without FMA contraction, reproduces the reference
+// bit for bit; the FP32 instantiation uses the same formulas in float.
+#pragma once
+#include "common.cuh"
+
+namespace sfg {
+
+// Moments of one cell in the reference's summation order
+// (lattice_field.cpp:220-227): rho = sum f_q, j = sum f_q e_q, q = 0..8.
+template <typename R>
+__device__ __forceinline__ void cell_moments(const R f[9], R& rho, R& jx, R& jy) {
+    rho = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
+    jx = f[1] - f[3] + f[5] - f[6] - f[7] + f[8];
+    jy = f[2] - f[4] + f[5] + f[6] - f[7] - f[8];
+}
+
+// u = (j + F/2) / rho, zero for rho <= 1e-15 (lattice_field.cpp:229-237).
+template <typename R>
+__device__ __forceinline__ void cell_velocity(R rho, R jx, R jy, R Gx, R Gy, R& ux, R& uy) {
+    if (rho > R(1e-15)) {
+        ux = (jx + R(0.5) * Gx) / rho;
+        uy = (jy + R(0.5) * Gy) / rho;
+    } else {
+        ux = R(0);
+        uy = R(0);
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void collide_bgk(R f[9], R r, R vx, R vy, R fx, R fy, R om) {
+    const R om1 = R(1) - om;
+    const R guo = R(1) - R(0.5) * om;
+    const R inv_cs2 = R(3), inv_cs4 = R(9);
+    const R uu = vx * vx + vy * vy;
+    const R uu_term = R(-0.5) * inv_cs2 * uu;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        const R ex = R(cx_of(q)), ey = R(cy_of(q));
+        const R eu = ex * vx + ey * vy;
+        const R w = R(w_of(q));
+        R feq = w * r * (R(1) + eu * inv_cs2 + R(0.5) * eu * eu * inv_cs4 + uu_term);
+        R tx = (ex - vx) * inv_cs2 + (eu * inv_cs4) * ex;
+        R ty = (ey - vy) * inv_cs2 + (eu * inv_cs4) * ey;
+        R Fi = guo * w * (tx * fx + ty * fy);
+        f[q] = om1 * f[q] + om * feq + Fi;
+    }
+}
+
+// Equilibrium in the form of reference lattice.h:35-39.
+template <typename R>
+__device__ __forceinline__ R feq_ref(int q, R rho, R ux, R uy) {
+    const R cs2 = R(1.0 / 3.0);
+    const R cs4 = cs2 * cs2;
+    R eu = R(cx_of(q)) * ux + R(cy_of(q)) * uy;
+    R uu = ux * ux + uy * uy;
+    return R(w_of(q)) * rho * (R(1) + eu / cs2 + (eu * eu) / (R(2) * cs4) - uu / (R(2) * cs2));
+}
+
+// Regularized BGK keeping the first-order non-equilibrium moment.
+template <typename R>
+__device__ __forceinline__ void collide_regularized(R f[9], R rho, R ux, R uy, R Fx, R Fy, R omega) {
+    const R cs2 = R(1.0 / 3.0);
+    const R cs4_2 = R(2) * cs2 * cs2;
+    R fe[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) fe[q] = feq_ref(q, rho, ux, uy);
+    R jx = R(0), jy = R(0), pxx = R(0), pxy = R(0), pyy = R(0);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        const R cx = R(cx_of(q)), cy = R(cy_of(q));
+        R fneq = f[q] - fe[q];
+        jx += fneq * cx;
+        jy += fneq * cy;
+        pxx += fneq * cx * cx;
+        pxy += fneq * cx * cy;
+        pyy += fneq * cy * cy;
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        const int icx = cx_of(q), icy = cy_of(q);
+        const R cx = R(icx), cy = R(icy);
+        R Qxx = R(icx * icx) - cs2;
+        R Qxy = R(icx * icy);
+        R Qyy = R(icy * icy) - cs2;
+        R fneq_reg = R(w_of(q)) * ((cx * jx + cy * jy) / cs2 +
+                                   (Qxx * pxx + R(2) * Qxy * pxy + Qyy * pyy) / cs4_2);
+        R eu = cx * ux + cy * uy;
+        R Fi = (R(1) - R(0.5) * omega) * R(w_of(q)) *
+               ((cx - ux + eu * cx / cs2) * Fx / cs2 + (cy - uy + eu * cy / cs2) * Fy / cs2);
+        f[q] = fe[q] + (R(1) - omega) * fneq_reg + Fi;
+    }
+}
+
+// D2Q9 MRT (Lallemand-Luo basis) with the Guo source in moment space.
+template <typename R>
+__device__ __forceinline__ void collide_mrt(R f[9], R r, R vx, R vy, R fx, R fy, R sn, R s1, R s2,
+                                            R s4) {
+    const R s6 = s4;
+    R m0 = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
+    R m1 = R(-4) * f[0] - f[1] - f[2] - f[3] - f[4] + R(2) * f[5] + R(2) * f[6] + R(2) * f[7] +
+           R(2) * f[8];
+    R m2 = R(4) * f[0] - R(2) * f[1] - R(2) * f[2] - R(2) * f[3] - R(2) * f[4] + f[5] + f[6] +
+           f[7] + f[8];
+    R m3 = f[1] - f[3] + f[5] - f[6] - f[7] + f[8];
+    R m4 = R(-2) * f[1] + R(2) * f[3] + f[5] - f[6] - f[7] + f[8];
+    R m5 = f[2] - f[4] + f[5] + f[6] - f[7] - f[8];
+    R m6 = R(-2) * f[2] + R(2) * f[4] + f[5] + f[6] - f[7] - f[8];
+    R m7 = f[1] - f[2] + f[3] - f[4];
+    R m8 = f[5] - f[6] + f[7] - f[8];
+    R uu = vx * vx + vy * vy;
+    R meq1 = R(-2) * r + R(3) * r * uu;
+    R meq2 = r - R(3) * r * uu;
+    R meq4 = -r * vx;
+    R meq6 = -r * vy;
+    R meq7 = r * (vx * vx - vy * vy);
+    R meq8 = r * vx * vy;
+    R uF = vx * fx + vy * fy;
+    R Sb1 = R(6) * uF, Sb2 = R(-6) * uF;
+    R Sb3 = fx, Sb4 = -fx, Sb5 = fy, Sb6 = -fy;
+    R Sb7 = R(2) * (vx * fx - vy * fy);
+    R Sb8 = vx * fy + vy * fx;
+    m1 = m1 - s1 * (m1 - meq1) + (R(1) - s1 * R(0.5)) * Sb1;
+    m2 = m2 - s2 * (m2 - meq2) + (R(1) - s2 * R(0.5)) * Sb2;
+    m3 = m3 + Sb3;
+    m4 = m4 - s4 * (m4 - meq4) + (R(1) - s4 * R(0.5)) * Sb4;
+    m5 = m5 + Sb5;
+    m6 = m6 - s6 * (m6 - meq6) + (R(1) - s6 * R(0.5)) * Sb6;
+    m7 = m7 - sn * (m7 - meq7) + (R(1) - sn * R(0.5)) * Sb7;
+    m8 = m8 - sn * (m8 - meq8) + (R(1) - sn * R(0.5)) * Sb8;
+    const R k9 = R(9), k36 = R(36), k18 = R(18), k6 = R(6), k4 = R(4), k12 = R(12);
+    f[0] = m0 / k9 - m1 / k9 + m2 / k9;
+    f[1] = m0 / k9 - m1 / k36 - m2 / k18 + m3 / k6 - m4 / k6 + m7 / k4;
+    f[2] = m0 / k9 - m1 / k36 - m2 / k18 + m5 / k6 - m6 / k6 - m7 / k4;
+    f[3] = m0 / k9 - m1 / k36 - m2 / k18 - m3 / k6 + m4 / k6 + m7 / k4;
+    f[4] = m0 / k9 - m1 / k36 - m2 / k18 - m5 / k6 + m6 / k6 - m7 / k4;
+    f[5] = m0 / k9 + m1 / k18 + m2 / k36 + m3 / k6 + m4 / k12 + m5 / k6 + m6 / k12 + m8 / k4;
+    f[6] = m0 / k9 + m1 / k18 + m2 / k36 - m3 / k6 - m4 / k12 + m5 / k6 + m6 / k12 - m8 / k4;
+    f[7] = m0 / k9 + m1 / k18 + m2 / k36 - m3 / k6 - m4 / k12 - m5 / k6 - m6 / k12 + m8 / k4;
+    f[8] = m0 / k9 + m1 / k18 + m2 / k36 + m3 / k6 + m4 / k12 - m5 / k6 - m6 / k12 - m8 / k4;
+}
+
+// Passive-scalar BGK collision with the first-order equilibrium
+// (advection_diffusion.cpp:137-151): g* = g - w_s (g - w C (1 + 3 e.u)).
+template <typename R>
+__device__ __forceinline__ void collide_scalar(R g[9], R C, R ux, R uy, R omega_s) {
+    const R inv_cs2 = R(3);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        const R eu = R(cx_of(q)) * ux + R(cy_of(q)) * uy;
+        const R geq = R(w_of(q)) * C * (R(1) + eu * inv_cs2);
+        g[q] = g[q] - omega_s * (g[q] - geq);
+    }
+}
+
+}  // namespace sfg

@@ -1,0 +1,94 @@
+// common.cuh -- shared device types and constants for the SoftFlow B200 path.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sfg {
+
+// D2Q9 velocity set in the reference's numbering (src/lbm/lattice.h:12-27):
+//   6 2 5
+//   3 0 1
+//   7 4 8
+__host__ __device__ constexpr int cx_of(int q) {
+    return q == 1 || q == 5 || q == 8 ? 1 : (q == 3 || q == 6 || q == 7 ? -1 : 0);
+}
+__host__ __device__ constexpr int cy_of(int q) {
+    return q == 2 || q == 5 || q == 6 ? 1 : (q == 4 || q == 7 || q == 8 ? -1 : 0);
+}
+__host__ __device__ constexpr int opp_of(int q) {
+    return q == 0 ? 0 : (q <= 4 ? ((q + 1) % 4) + 1 : ((q - 5 + 2) % 4) + 5);
+}
+__host__ __device__ constexpr double w_of(int q) {
+    return q == 0 ? 4.0 / 9.0 : (q <= 4 ? 1.0 / 9.0 : 1.0 / 36.0);
+}
+static_assert(opp_of(1) == 3 && opp_of(2) == 4 && opp_of(3) == 1 && opp_of(4) == 2, "opp");
+static_assert(opp_of(5) == 7 && opp_of(6) == 8 && opp_of(7) == 5 && opp_of(8) == 6, "opp");
+
+// Force-tile geometry: lattice forces from the immersed boundary live in
+// 32 x 8 tiles that are only materialised where markers touch the lattice.
+constexpr int TILE_W = 32;
+constexpr int TILE_H = 8;
+constexpr int TILE_CELLS = TILE_W * TILE_H;
+
+// Storage precision of the populations.
+enum Precision : int { PREC_FP64 = 0, PREC_FP32 = 1, PREC_FP16S = 2 };
+
+// Per-channel constants, read by every kernel (device copy in global memory).
+struct ChannelDev {
+    int nx, ny, pitch;          // pitch: row stride in elements
+    int periodic_y;             // 0: rows 0 and ny-1 are SOLID walls
+    long long plane;            // elements per population plane (ny * pitch)
+    long long cell_off;         // offset of this channel in one-plane arrays
+    long long f_off;            // = 9 * cell_off: plane 0 in the population buffers
+    long long g_off;            // = 9 * cell_off: plane 0 in the scalar buffers
+    int collision;              // 0 BGK, 1 MRT, 2 regularized
+    int ibm_iterations;
+    double omega, tau;
+    double mrt_se, mrt_s_eps, mrt_sq;
+    double body_fx, body_fy;
+    double max_force;
+    double F_uni_x, F_uni_y;    // capped body force (FLUID cells, untouched tiles)
+    double dt;
+    // scalar transport
+    int adr, adr_periodic_y;
+    double omega_s;
+    // force tiles
+    int tiles_x, tiles_y;
+    int tile_base;              // first global tile index of this channel
+    // markers / capsules
+    int cap_begin, cap_end;
+    int mk_begin, mk_end;
+    // contact grid (reference cell_list.h:36-87)
+    int ncx, ncy, cell_base;
+    double cdx, cdy, y_bot, y_top;
+    double rep_epsilon, rep_sigma, rep_r_cut, rep_damping, rep_friction;
+    int rep_power;
+    int brute_contact;          // <= 100 markers: all pairs, one-sided
+};
+
+// Per-capsule constants (reference Capsule members, capsule.h:77-142).
+struct CapsuleDev {
+    int off, n, chan, model;
+    int use_helfrich;
+    double k_stretch, G_s, C_skalak;
+    double wlc_L_max_ratio, wlc_kBT_p, wlc_k_pow;
+    double k_bend, k_area, k_perimeter, gamma_visc, eta_membrane;
+    double rest_area, rest_perimeter;
+    int periodic_nx;
+};
+
+// Work item of the lattice kernels: one row segment of one channel.
+struct RowItem {
+    int chan, y, x0, len;
+};
+
+// Status word bits written by kernels (host reads them after a sync).
+enum StatusBits : unsigned {
+    ST_NAN_MARKER = 1u,         // non-finite marker position seen
+    ST_LIST_OVERFLOW = 2u,      // a per-tile marker list exceeded its capacity
+    ST_CAPSULE_TOO_BIG = 4u,    // a capsule exceeded the per-warp node capacity
+};
+
+}  // namespace sfg

@@ -1,0 +1,926 @@
+// context.cu -- the C ABI (include/softflow_gpu.h): device context, channel
+// and capsule registration, per-step kernel sequence (captured in CUDA
+// graphs), and state transfer.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/softflow_gpu.h"
+#include "lattice.cuh"
+#include "sfg_internal.h"
+
+using namespace sfg;
+
+namespace sfg_host {
+static thread_local std::string g_err;
+void set_error(const std::string& msg) { g_err = msg; }
+}  // namespace sfg_host
+
+static int fail(int code, const std::string& msg) {
+    sfg_host::set_error(msg);
+    return code;
+}
+
+#define CU(x)                                                                           \
+    do {                                                                                \
+        cudaError_t e_ = (x);                                                           \
+        if (e_ != cudaSuccess)                                                          \
+            return fail(SFG_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+namespace {
+
+struct CapsuleHost {
+    sfg_membrane_params mp;
+    sfg_capsule_rest rest;
+    std::vector<double> pos, rest_len, rest_ang, rest_ds;
+};
+
+struct ChanHost {
+    sfg_channel_params p;
+    ChannelDev d;
+    std::vector<CapsuleHost> caps;
+    long long fluid_cells = 0;
+};
+
+__global__ void k_step_flags(const ChannelDev* __restrict__ chans, int nch, int* stepped,
+                             int* adr_pending, int* c_fresh) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nch) return;
+    if (chans[c].adr) {
+        if (adr_pending[c]) c_fresh[c] = 0;
+        adr_pending[c] = 1;
+    }
+    stepped[c] = 1;
+}
+
+__global__ void k_flush_flags(int nch, int* adr_pending, int* c_fresh) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nch) return;
+    if (adr_pending[c]) c_fresh[c] = 0;
+    adr_pending[c] = 0;
+}
+
+struct Feq9 {
+    double v[9];
+};
+
+template <typename S, typename R>
+__global__ void k_pop_fill(S* __restrict__ f, ChannelDev ch, Feq9 v) {
+    const long long N = (long long)ch.plane;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 9 * N;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int q = (int)(i / N);
+        PopIO<S, R>::store(f + ch.f_off + i, q, (R)v.v[q]);
+    }
+}
+
+template <typename R>
+__global__ void k_scalar_set(const double* __restrict__ C, R* __restrict__ g0, R* __restrict__ g1,
+                             R* __restrict__ cf, ChannelDev ch) {
+    const long long N = (long long)ch.nx * ch.ny;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(i / ch.nx), x = (int)(i % ch.nx);
+        const long long n = (long long)y * ch.pitch + x;
+        const double c = C[i];
+        cf[ch.cell_off + n] = (R)c;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            const R v = (R)(w_of(q) * c);
+            g0[ch.g_off + q * ch.plane + n] = v;
+            g1[ch.g_off + q * ch.plane + n] = v;
+        }
+    }
+}
+
+template <typename R>
+__global__ void k_scalar_export(const R* __restrict__ g, ChannelDev ch, double* __restrict__ C,
+                                double* __restrict__ gout) {
+    const long long N = (long long)ch.nx * ch.ny;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(i / ch.nx), x = (int)(i % ch.nx);
+        const long long n = (long long)y * ch.pitch + x;
+        R v[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) v[q] = g[ch.g_off + q * ch.plane + n];
+        const R s = v[0] + v[1] + v[2] + v[3] + v[4] + v[5] + v[6] + v[7] + v[8];
+        C[i] = (double)s;
+        if (gout)
+            for (int q = 0; q < 9; ++q) gout[q * N + i] = (double)v[q];
+    }
+}
+
+int io_blocks(long long n) {
+    long long g = (n + 255) / 256;
+    return (int)std::min<long long>(std::max<long long>(g, 1), 4096);
+}
+
+double phi_exact(double r) {
+    // Peskin 4-point kernel (delta_function.h:18-26)
+    const double ar = std::abs(r);
+    if (ar <= 1.0) return 0.125 * (3.0 - 2.0 * ar + std::sqrt(1.0 + 4.0 * ar - 4.0 * ar * ar));
+    if (ar <= 2.0) return 0.125 * (5.0 - 2.0 * ar - std::sqrt(-7.0 + 12.0 * ar - 4.0 * ar * ar));
+    return 0.0;
+}
+
+}  // namespace
+
+struct sfg_context {
+    int device = 0;
+    int precision = SFG_FP32;
+    cudaStream_t stream = nullptr;
+    std::vector<ChanHost> ch;
+    bool initialized = false;
+
+    // device state
+    ChannelDev* d_chans = nullptr;
+    RowItem* d_items = nullptr;
+    int n_items = 0;
+    void* f[2] = {nullptr, nullptr};
+    void* g[2] = {nullptr, nullptr};
+    void* cfield = nullptr;
+    bool any_adr = false;
+    CapsuleDev* d_caps = nullptr;
+    int* d_has_prev = nullptr;
+    MarkerBufs mb{};
+    int M = 0, NC = 0, maxn = 0, Kmax = 1;
+    TileBufs tb;
+    ContactBufs cb;
+    int ncells = 0;
+    double* d_phi = nullptr;
+    int* d_stepped = nullptr;
+    int* d_adr_pending = nullptr;
+    int* d_c_fresh = nullptr;
+    unsigned* d_status = nullptr;
+    double* d_io = nullptr;
+    size_t io_doubles = 0;
+    int spread_grid = 0;
+
+    long long steps = 0;
+    bool adr_pending_h = false;
+    int g_cur = 0;
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    bool use_graphs = true;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int launches = 0;
+
+    size_t elem_size() const { return precision == SFG_FP64 ? 8 : (precision == SFG_FP32 ? 4 : 2); }
+    size_t real_size() const { return precision == SFG_FP64 ? 8 : 4; }
+};
+
+// ------------------------------------------------------------------------
+// library
+// ------------------------------------------------------------------------
+extern "C" int sfg_abi_version(void) { return SFG_ABI_VERSION; }
+extern "C" const char* sfg_last_error(void) { return sfg_host::g_err.c_str(); }
+
+extern "C" int sfg_create(int device, int precision, sfg_context** out) {
+    if (!out) return fail(SFG_ERR_ARG, "sfg_create: null output");
+    if (precision < SFG_FP64 || precision > SFG_FP16S)
+        return fail(SFG_ERR_ARG, "sfg_create: unknown precision");
+    int ndev = 0;
+    CU(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(SFG_ERR_ARG, "sfg_create: bad device ordinal");
+    CU(cudaSetDevice(device));
+    auto* c = new sfg_context();
+    c->device = device;
+    c->precision = precision;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+    if (e != cudaSuccess) {
+        delete c;
+        return fail(SFG_ERR_CUDA, std::string("sfg_create: ") + cudaGetErrorString(e));
+    }
+    *out = c;
+    return SFG_OK;
+}
+
+static void free_all(sfg_context* c) {
+    auto F = [](void* p) {
+        if (p) cudaFree(p);
+    };
+    for (int i = 0; i < 2; ++i) {
+        if (c->gexec[i]) cudaGraphExecDestroy(c->gexec[i]);
+        c->gexec[i] = nullptr;
+        F(c->f[i]);
+        F(c->g[i]);
+        F(c->tb.tile_slot[i]);
+        F(c->tb.fin[i]);
+    }
+    F(c->cfield);
+    F(c->d_chans);
+    F(c->d_items);
+    F(c->d_caps);
+    F(c->d_has_prev);
+    F(c->mb.pos); F(c->mb.vel); F(c->mb.frc); F(c->mb.dF); F(c->mb.ds);
+    F(c->mb.rest_len); F(c->mb.rest_ang); F(c->mb.rest_ds); F(c->mb.prev_len);
+    F(c->mb.mk_cap); F(c->mb.mk_chan); F(c->mb.ix0); F(c->mb.iy0); F(c->mb.valid);
+    F(c->mb.pair_count);
+    F(c->tb.tile_chan); F(c->tb.tile_flag); F(c->tb.tile_cnt); F(c->tb.cursor);
+    F(c->tb.slot_scan); F(c->tb.list_off); F(c->tb.slot_tile); F(c->tb.n_slots);
+    F(c->tb.list); F(c->tb.scan_tmp); F(c->tb.acc); F(c->tb.gsnap); F(c->tb.capped);
+    F(c->tb.fluid_touched);
+    F(c->cb.cell_of); F(c->cb.cell_cnt); F(c->cb.cell_start); F(c->cb.cursor); F(c->cb.list);
+    F(c->cb.scan_tmp);
+    F(c->d_phi); F(c->d_stepped); F(c->d_adr_pending); F(c->d_c_fresh); F(c->d_status);
+    F(c->d_io);
+}
+
+extern "C" int sfg_destroy(sfg_context* c) {
+    if (!c) return SFG_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    free_all(c);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return SFG_OK;
+}
+
+extern "C" int sfg_add_channel(sfg_context* c, const sfg_channel_params* p, int* out) {
+    if (!c || !p) return fail(SFG_ERR_ARG, "sfg_add_channel: null argument");
+    if (c->initialized) return fail(SFG_ERR_STATE, "sfg_add_channel: context already initialized");
+    if (p->nx < 4 || p->ny < 3) return fail(SFG_ERR_ARG, "sfg_add_channel: need nx >= 4, ny >= 3");
+    if (!(p->tau > 0.5)) return fail(SFG_ERR_ARG, "sfg_add_channel: tau must exceed 0.5");
+    if (p->collision < 0 || p->collision > 2)
+        return fail(SFG_ERR_ARG, "sfg_add_channel: unknown collision model");
+    if (p->scalar_enabled && !(p->scalar_D > 0.0))
+        return fail(SFG_ERR_ARG, "sfg_add_channel: scalar diffusivity must be positive");
+    if (p->rep_r_cut <= 0.0) return fail(SFG_ERR_ARG, "sfg_add_channel: r_cut must be positive");
+    ChanHost h;
+    h.p = *p;
+    c->ch.push_back(h);
+    if (out) *out = (int)c->ch.size() - 1;
+    return SFG_OK;
+}
+
+extern "C" int sfg_add_capsule(sfg_context* c, int channel, const sfg_membrane_params* mp,
+                               const sfg_capsule_rest* rest, const double* pos,
+                               const double* rest_len, const double* rest_ang,
+                               const double* rest_ds, int* out) {
+    if (!c || !mp || !rest || !pos || !rest_len)
+        return fail(SFG_ERR_ARG, "sfg_add_capsule: null argument");
+    if (c->initialized) return fail(SFG_ERR_STATE, "sfg_add_capsule: context already initialized");
+    if (channel < 0 || channel >= (int)c->ch.size())
+        return fail(SFG_ERR_ARG, "sfg_add_capsule: bad channel");
+    if (rest->num_nodes < 3) return fail(SFG_ERR_ARG, "sfg_add_capsule: need >= 3 nodes");
+    if (mp->use_helfrich && (!rest_ang || !rest_ds))
+        return fail(SFG_ERR_ARG, "sfg_add_capsule: Helfrich bending needs rest angles");
+    CapsuleHost ch;
+    ch.mp = *mp;
+    ch.rest = *rest;
+    const int n = rest->num_nodes;
+    ch.pos.assign(pos, pos + 2 * n);
+    ch.rest_len.assign(rest_len, rest_len + n);
+    if (rest_ang) ch.rest_ang.assign(rest_ang, rest_ang + n);
+    else ch.rest_ang.assign(n, 0.0);
+    if (rest_ds) ch.rest_ds.assign(rest_ds, rest_ds + n);
+    else ch.rest_ds.assign(n, 0.0);
+    c->ch[channel].caps.push_back(std::move(ch));
+    if (out) *out = (int)c->ch[channel].caps.size() - 1;
+    return SFG_OK;
+}
+
+template <typename T>
+static cudaError_t dalloc(T** p, size_t n) {
+    return cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T));
+}
+
+// ------------------------------------------------------------------------
+// initialize
+// ------------------------------------------------------------------------
+extern "C" int sfg_initialize(sfg_context* c) {
+    if (!c) return fail(SFG_ERR_ARG, "sfg_initialize: null context");
+    if (c->initialized) return fail(SFG_ERR_STATE, "sfg_initialize: already initialized");
+    if (c->ch.empty()) return fail(SFG_ERR_STATE, "sfg_initialize: no channel");
+    CU(cudaSetDevice(c->device));
+    const int nch = (int)c->ch.size();
+    long long cell_off = 0;
+    int tile_base = 0, cell_base = 0, cap_base = 0, mk_base = 0;
+    std::vector<RowItem> items;
+    std::vector<CapsuleDev> caps;
+    std::vector<double> pos, rest_len, rest_ang, rest_ds;
+    std::vector<int> mk_cap, mk_chan, tile_chan;
+    c->any_adr = false;
+    c->maxn = 0;
+    c->Kmax = 1;
+    for (int ci = 0; ci < nch; ++ci) {
+        ChanHost& h = c->ch[ci];
+        const sfg_channel_params& p = h.p;
+        ChannelDev d{};
+        d.nx = p.nx;
+        d.ny = p.ny;
+        d.pitch = (p.nx + 31) / 32 * 32;
+        d.periodic_y = p.periodic_y ? 1 : 0;
+        d.plane = (long long)d.ny * d.pitch;
+        d.cell_off = cell_off;
+        d.f_off = 9 * cell_off;
+        d.g_off = 9 * cell_off;
+        cell_off += d.plane;
+        d.collision = p.collision;
+        d.ibm_iterations = p.ibm_iterations > 1 ? p.ibm_iterations : 1;
+        d.tau = p.tau;
+        d.omega = 1.0 / p.tau;
+        d.mrt_se = p.mrt_se;
+        d.mrt_s_eps = p.mrt_s_eps;
+        d.mrt_sq = p.mrt_sq;
+        d.body_fx = p.body_fx;
+        d.body_fy = p.body_fy;
+        d.max_force = p.max_lattice_force;
+        {   // capped body force on FLUID cells away from the markers
+            double fx = 0.0 + p.body_fx, fy = 0.0 + p.body_fy;
+            const double Fm = p.max_lattice_force, f2 = fx * fx + fy * fy;
+            if (f2 > Fm * Fm) {
+                const double sc = Fm / std::sqrt(f2);
+                fx *= sc;
+                fy *= sc;
+            }
+            d.F_uni_x = fx;
+            d.F_uni_y = fy;
+        }
+        d.dt = p.dt;
+        d.adr = p.scalar_enabled ? 1 : 0;
+        d.adr_periodic_y = p.scalar_periodic_y ? 1 : 0;
+        d.omega_s = 1.0 / (3.0 * p.scalar_D + 0.5);
+        c->any_adr |= d.adr != 0;
+        d.tiles_x = (p.nx + TILE_W - 1) / TILE_W;
+        d.tiles_y = (p.ny + TILE_H - 1) / TILE_H;
+        d.tile_base = tile_base;
+        tile_base += d.tiles_x * d.tiles_y;
+        for (int t = 0; t < d.tiles_x * d.tiles_y; ++t) tile_chan.push_back(ci);
+        // capsules of this channel, channel-major
+        d.cap_begin = cap_base;
+        d.mk_begin = mk_base;
+        for (const CapsuleHost& cp : h.caps) {
+            CapsuleDev cd{};
+            cd.off = mk_base;
+            cd.n = cp.rest.num_nodes;
+            cd.chan = ci;
+            cd.model = cp.mp.model;
+            cd.use_helfrich = cp.mp.use_helfrich;
+            cd.k_stretch = cp.mp.k_stretch;
+            cd.G_s = cp.mp.G_s;
+            cd.C_skalak = cp.mp.C_skalak;
+            cd.wlc_L_max_ratio = cp.mp.wlc_L_max_ratio;
+            cd.wlc_kBT_p = cp.rest.wlc_kBT_p;
+            cd.wlc_k_pow = cp.rest.wlc_k_pow;
+            cd.k_bend = cp.mp.k_bend;
+            cd.k_area = cp.mp.k_area;
+            cd.k_perimeter = cp.mp.k_perimeter;
+            cd.gamma_visc = cp.mp.gamma_visc;
+            cd.eta_membrane = cp.mp.eta_membrane;
+            cd.rest_area = cp.rest.rest_area;
+            cd.rest_perimeter = cp.rest.rest_perimeter;
+            cd.periodic_nx = p.nx;
+            caps.push_back(cd);
+            c->maxn = std::max(c->maxn, cd.n);
+            for (int k = 0; k < cd.n; ++k) {
+                pos.push_back(cp.pos[2 * k]);
+                pos.push_back(cp.pos[2 * k + 1]);
+                rest_len.push_back(cp.rest_len[k]);
+                rest_ang.push_back(cp.rest_ang[k]);
+                rest_ds.push_back(cp.rest_ds[k]);
+                mk_cap.push_back(cap_base);
+                mk_chan.push_back(ci);
+            }
+            mk_base += cd.n;
+            ++cap_base;
+        }
+        d.cap_end = cap_base;
+        d.mk_end = mk_base;
+        if (d.cap_end > d.cap_begin) c->Kmax = std::max(c->Kmax, d.ibm_iterations);
+        // contact cell list geometry (cell_list.h:36-87, periodic in x)
+        d.y_bot = 0.5;
+        d.y_top = (double)p.ny - 1.5;
+        {
+            const double x_extent = (double)p.nx;
+            d.ncx = std::max(1, (int)std::floor(x_extent / p.rep_r_cut));
+            d.ncy = std::max(1, (int)std::floor((d.y_top - d.y_bot) / p.rep_r_cut));
+            d.cdx = x_extent / (double)d.ncx;
+            d.cdy = (d.y_top - d.y_bot) / (double)d.ncy;
+        }
+        d.brute_contact = (d.mk_end - d.mk_begin) <= 100 ? 1 : 0;
+        d.cell_base = cell_base;
+        if (!d.brute_contact) cell_base += d.ncx * d.ncy;
+        d.rep_epsilon = p.rep_epsilon;
+        d.rep_sigma = p.rep_sigma;
+        d.rep_r_cut = p.rep_r_cut;
+        d.rep_damping = p.rep_damping_normal;
+        d.rep_friction = p.rep_friction;
+        d.rep_power = p.rep_power;
+        // lattice row segments: at most 256 cells, rounded to warps
+        const int nseg = (p.nx + 255) / 256;
+        int seg = (p.nx + nseg - 1) / nseg;
+        seg = (seg + 31) / 32 * 32;
+        const int y0 = p.periodic_y ? 0 : 1, y1 = p.periodic_y ? p.ny : p.ny - 1;
+        for (int y = y0; y < y1; ++y)
+            for (int x0 = 0; x0 < p.nx; x0 += seg) items.push_back({ci, y, x0, std::min(seg, p.nx - x0)});
+        h.fluid_cells = (long long)p.nx * (y1 - y0);
+        h.d = d;
+    }
+    c->M = mk_base;
+    c->NC = cap_base;
+    c->ncells = cell_base;
+    c->n_items = (int)items.size();
+    c->maxn = (c->maxn + 31) / 32 * 32;
+    if (membrane_smem_bytes(c->maxn) > 227 * 1024)
+        return fail(SFG_ERR_CAPACITY, "sfg_initialize: capsules with more than 640 nodes");
+    if (c->maxn > 0) CU(prepare_membrane(c->maxn));
+
+    std::vector<ChannelDev> dch(nch);
+    for (int i = 0; i < nch; ++i) dch[i] = c->ch[i].d;
+    CU(dalloc(&c->d_chans, nch));
+    CU(cudaMemcpy(c->d_chans, dch.data(), sizeof(ChannelDev) * nch, cudaMemcpyHostToDevice));
+    CU(dalloc(&c->d_items, items.size()));
+    CU(cudaMemcpy(c->d_items, items.data(), sizeof(RowItem) * items.size(), cudaMemcpyHostToDevice));
+
+    // populations
+    const size_t nelem = 9 * (size_t)cell_off;
+    for (int i = 0; i < 2; ++i) CU(cudaMalloc(&c->f[i], nelem * c->elem_size()));
+    if (c->any_adr) {
+        for (int i = 0; i < 2; ++i) {
+            CU(cudaMalloc(&c->g[i], nelem * c->real_size()));
+            CU(cudaMemset(c->g[i], 0, nelem * c->real_size()));
+        }
+        CU(cudaMalloc(&c->cfield, (size_t)cell_off * c->real_size()));
+        CU(cudaMemset(c->cfield, 0, (size_t)cell_off * c->real_size()));
+    }
+    for (int ci = 0; ci < nch; ++ci) {
+        const ChannelDev& d = c->ch[ci].d;
+        Feq9 v;
+        // feq(rho0, 0, 0) in the form of lattice.h:35-39
+        const double cs2 = 1.0 / 3.0, cs4 = cs2 * cs2;
+        for (int q = 0; q < 9; ++q) {
+            const double eu = 0.0, uu = 0.0;
+            v.v[q] = w_of(q) * c->ch[ci].p.rho0 *
+                     (1.0 + eu / cs2 + (eu * eu) / (2.0 * cs4) - uu / (2.0 * cs2));
+        }
+        for (int i = 0; i < 2; ++i) {
+            if (c->precision == SFG_FP64)
+                k_pop_fill<double, double><<<io_blocks(9 * d.plane), 256, 0, c->stream>>>(
+                    (double*)c->f[i], d, v);
+            else if (c->precision == SFG_FP32)
+                k_pop_fill<float, float><<<io_blocks(9 * d.plane), 256, 0, c->stream>>>(
+                    (float*)c->f[i], d, v);
+            else
+                k_pop_fill<__half, float><<<io_blocks(9 * d.plane), 256, 0, c->stream>>>(
+                    (__half*)c->f[i], d, v);
+        }
+    }
+    CU(cudaGetLastError());
+
+    // markers
+    const int M = c->M;
+    CU(dalloc(&c->mb.pos, M));
+    CU(dalloc(&c->mb.vel, M));
+    CU(dalloc(&c->mb.frc, M));
+    CU(dalloc(&c->mb.dF, M));
+    CU(dalloc(&c->mb.ds, M));
+    CU(dalloc(&c->mb.rest_len, M));
+    CU(dalloc(&c->mb.rest_ang, M));
+    CU(dalloc(&c->mb.rest_ds, M));
+    CU(dalloc(&c->mb.prev_len, M));
+    CU(dalloc(&c->mb.mk_cap, M));
+    CU(dalloc(&c->mb.mk_chan, M));
+    CU(dalloc(&c->mb.ix0, M));
+    CU(dalloc(&c->mb.iy0, M));
+    CU(dalloc(&c->mb.valid, M));
+    CU(dalloc(&c->mb.pair_count, M));
+    CU(dalloc(&c->d_caps, c->NC));
+    CU(dalloc(&c->d_has_prev, c->NC));
+    if (M > 0) {
+        CU(cudaMemcpy(c->mb.pos, pos.data(), sizeof(double) * 2 * M, cudaMemcpyHostToDevice));
+        CU(cudaMemset(c->mb.vel, 0, sizeof(double2) * M));
+        CU(cudaMemset(c->mb.frc, 0, sizeof(double2) * M));
+        CU(cudaMemset(c->mb.dF, 0, sizeof(double2) * M));
+        CU(cudaMemset(c->mb.pair_count, 0, sizeof(int) * M));
+        CU(cudaMemcpy(c->mb.rest_len, rest_len.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
+        // Kelvin-Voigt previous lengths start at the rest lengths (capsule.cpp:85-86)
+        CU(cudaMemcpy(c->mb.prev_len, rest_len.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(c->mb.rest_ang, rest_ang.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(c->mb.rest_ds, rest_ds.data(), sizeof(double) * M, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(c->mb.mk_cap, mk_cap.data(), sizeof(int) * M, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(c->mb.mk_chan, mk_chan.data(), sizeof(int) * M, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(c->d_caps, caps.data(), sizeof(CapsuleDev) * c->NC, cudaMemcpyHostToDevice));
+        CU(cudaMemset(c->d_has_prev, 0, sizeof(int) * c->NC));
+    }
+
+    // force tiles
+    TileBufs& tb = c->tb;
+    tb.T = tile_base;
+    tb.max_slots = M > 0 ? (int)std::min<long long>(tile_base, 8LL * M) : 1;
+    const int T = tb.T;
+    CU(dalloc(&tb.tile_chan, T));
+    CU(cudaMemcpy(tb.tile_chan, tile_chan.data(), sizeof(int) * T, cudaMemcpyHostToDevice));
+    CU(dalloc(&tb.tile_flag, T));
+    CU(dalloc(&tb.tile_cnt, T));
+    CU(dalloc(&tb.cursor, T));
+    CU(dalloc(&tb.slot_scan, T));
+    CU(dalloc(&tb.list_off, T));
+    for (int i = 0; i < 2; ++i) {
+        CU(dalloc(&tb.tile_slot[i], T));
+        CU(cudaMemset(tb.tile_slot[i], 0xff, sizeof(int) * std::max(T, 1)));
+        CU(cudaMalloc(&tb.fin[i], (size_t)tb.max_slots * 2 * TILE_CELLS * c->real_size()));
+    }
+    CU(dalloc(&tb.slot_tile, tb.max_slots));
+    CU(dalloc(&tb.n_slots, 1));
+    CU(cudaMemset(tb.n_slots, 0, sizeof(int)));
+    CU(dalloc(&tb.list, 8LL * M));
+    CU(dalloc(&tb.scan_tmp, scan_tmp_ints(T)));
+    CU(dalloc(&tb.acc, (size_t)tb.max_slots * 2 * TILE_CELLS));
+    CU(cudaMalloc(&tb.gsnap, (size_t)tb.max_slots * 2 * TILE_CELLS * c->real_size()));
+    CU(dalloc(&tb.capped, nch));
+    CU(dalloc(&tb.fluid_touched, nch));
+    CU(cudaMemset(tb.capped, 0, sizeof(int) * nch));
+    CU(cudaMemset(tb.fluid_touched, 0, sizeof(int) * nch));
+
+    // contact cells
+    CU(dalloc(&c->cb.cell_of, M));
+    CU(dalloc(&c->cb.cell_cnt, c->ncells));
+    CU(dalloc(&c->cb.cell_start, c->ncells));
+    CU(dalloc(&c->cb.cursor, c->ncells));
+    CU(dalloc(&c->cb.list, M));
+    CU(dalloc(&c->cb.scan_tmp, scan_tmp_ints(c->ncells)));
+    CU(cudaMemset(c->cb.cell_cnt, 0, sizeof(int) * std::max(c->ncells, 1)));
+    CU(cudaMemset(c->cb.cell_start, 0, sizeof(int) * std::max(c->ncells, 1)));
+
+    // Peskin table (delta_function.h:29-37)
+    {
+        std::vector<double> tbl(1025);
+        for (int i = 0; i <= 1024; ++i) tbl[i] = phi_exact(2.0 * static_cast<double>(i) / 1024);
+        CU(dalloc(&c->d_phi, 1025));
+        CU(cudaMemcpy(c->d_phi, tbl.data(), sizeof(double) * 1025, cudaMemcpyHostToDevice));
+    }
+    CU(dalloc(&c->d_stepped, nch));
+    CU(dalloc(&c->d_adr_pending, nch));
+    CU(dalloc(&c->d_c_fresh, nch));
+    CU(dalloc(&c->d_status, 1));
+    CU(cudaMemset(c->d_stepped, 0, sizeof(int) * nch));
+    CU(cudaMemset(c->d_adr_pending, 0, sizeof(int) * nch));
+    CU(cudaMemset(c->d_c_fresh, 0, sizeof(int) * nch));
+    CU(cudaMemset(c->d_status, 0, sizeof(unsigned)));
+
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+    c->spread_grid = std::max(1, std::min(tb.max_slots, nsm * 4));
+    CU(cudaStreamSynchronize(c->stream));
+    c->initialized = true;
+    c->steps = 0;
+    return SFG_OK;
+}
+
+// ------------------------------------------------------------------------
+// one step
+// ------------------------------------------------------------------------
+template <typename S, typename R>
+static int enqueue_step_t(sfg_context* c, int p) {
+    cudaStream_t st = c->stream;
+    const int nch = (int)c->ch.size();
+    int launches = 0;
+    if (c->M > 0) {
+        cudaMemsetAsync(c->tb.capped, 0, sizeof(int) * nch, st);
+        cudaMemsetAsync(c->tb.fluid_touched, 0, sizeof(int) * nch, st);
+        launch_membrane(c->d_caps, c->NC, c->mb, c->d_has_prev, c->maxn, c->d_status, st);
+        launch_contact(c->d_chans, c->M, c->mb, c->cb, c->ncells, st);
+        launch_tiles(c->d_chans, c->d_caps, c->M, c->mb, c->tb, c->tb.T, p, c->d_status, st);
+        launch_spread<R>(c->d_chans, c->mb, c->tb, p, c->d_phi, 0, c->spread_grid, c->d_status, st);
+        launches += 1 + (c->ncells > 0 ? 7 : 1) + 9 + 1;
+        for (int k = 1; k < c->Kmax; ++k) {
+            launch_mdf_interp<S, R>(c->d_chans, c->M, c->mb, static_cast<const S*>(c->f[p]), c->tb,
+                                    p, c->d_phi, k, st);
+            launch_spread<R>(c->d_chans, c->mb, c->tb, p, c->d_phi, k, c->spread_grid, c->d_status,
+                             st);
+            launches += 2;
+        }
+    }
+    LatticeLaunch L{c->d_items, c->n_items, c->d_chans, c->f[p], c->f[1 - p], c->g[p],
+                    c->g[1 - p], c->cfield, c->d_stepped, c->d_adr_pending, c->d_c_fresh,
+                    c->any_adr};
+    TileViewArgs tv{c->M > 0 ? c->tb.tile_slot[p] : nullptr,
+                    c->M > 0 ? c->tb.tile_slot[1 - p] : nullptr, c->tb.fin[p], c->tb.gsnap,
+                    c->tb.fin[1 - p]};
+    launch_lattice_step<S, R>(L, tv, st);
+    k_step_flags<<<(nch + 127) / 128, 128, 0, st>>>(c->d_chans, nch, c->d_stepped,
+                                                    c->d_adr_pending, c->d_c_fresh);
+    launches += 2;
+    if (c->M > 0) {
+        launch_interp_move<S, R>(c->d_chans, c->M, c->mb, static_cast<const S*>(c->f[1 - p]),
+                                 c->tb, p, c->d_phi, st);
+        launches += 1;
+    }
+    c->launches = launches;
+    return SFG_OK;
+}
+
+static int enqueue_step(sfg_context* c, int p) {
+    if (c->precision == SFG_FP64) return enqueue_step_t<double, double>(c, p);
+    if (c->precision == SFG_FP32) return enqueue_step_t<float, float>(c, p);
+    return enqueue_step_t<__half, float>(c, p);
+}
+
+static int build_graphs(sfg_context* c) {
+    for (int p = 0; p < 2; ++p) {
+        cudaGraph_t g = nullptr;
+        CU(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_step(c, p);
+        CU(cudaStreamEndCapture(c->stream, &g));
+        cudaError_t e = cudaGraphInstantiate(&c->gexec[p], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess)
+            return fail(SFG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    }
+    return SFG_OK;
+}
+
+extern "C" int sfg_step(sfg_context* c, int nsteps) {
+    if (!c) return fail(SFG_ERR_ARG, "sfg_step: null context");
+    if (!c->initialized) return fail(SFG_ERR_STATE, "sfg_step: context not initialized");
+    if (nsteps < 0) return fail(SFG_ERR_ARG, "sfg_step: negative step count");
+    CU(cudaSetDevice(c->device));
+    if (c->use_graphs && !c->gexec[0]) {
+        int rc = build_graphs(c);
+        if (rc != SFG_OK) return rc;
+    }
+    CU(cudaEventRecord(c->ev0, c->stream));
+    for (int i = 0; i < nsteps; ++i) {
+        const int p = (int)(c->steps & 1);
+        if (c->use_graphs) CU(cudaGraphLaunch(c->gexec[p], c->stream));
+        else enqueue_step(c, p);
+        if (c->any_adr) {
+            if (c->adr_pending_h) c->g_cur = 1 - p;
+            c->adr_pending_h = true;
+        }
+        ++c->steps;
+    }
+    CU(cudaEventRecord(c->ev1, c->stream));
+    CU(cudaGetLastError());
+    return SFG_OK;
+}
+
+extern "C" int sfg_synchronize(sfg_context* c, unsigned* status_out) {
+    if (!c) return fail(SFG_ERR_ARG, "sfg_synchronize: null context");
+    CU(cudaSetDevice(c->device));
+    CU(cudaStreamSynchronize(c->stream));
+    unsigned st = 0;
+    if (c->d_status) CU(cudaMemcpy(&st, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (status_out) *status_out = st;
+    if (st & (ST_LIST_OVERFLOW | ST_CAPSULE_TOO_BIG))
+        return fail(SFG_ERR_CAPACITY,
+                    st & ST_LIST_OVERFLOW ? "a force-tile marker list exceeded 4096 entries"
+                                          : "a capsule exceeded the per-warp node capacity");
+    return SFG_OK;
+}
+
+extern "C" int sfg_last_step_ms(sfg_context* c, float* ms) {
+    if (!c || !ms) return fail(SFG_ERR_ARG, "sfg_last_step_ms: null argument");
+    CU(cudaEventElapsedTime(ms, c->ev0, c->ev1));
+    return SFG_OK;
+}
+
+// ------------------------------------------------------------------------
+// state transfer
+// ------------------------------------------------------------------------
+static int check_chan(sfg_context* c, int ch, const char* who) {
+    if (!c) return fail(SFG_ERR_ARG, std::string(who) + ": null context");
+    if (!c->initialized) return fail(SFG_ERR_STATE, std::string(who) + ": context not initialized");
+    if (ch < 0 || ch >= (int)c->ch.size()) return fail(SFG_ERR_ARG, std::string(who) + ": bad channel");
+    return SFG_OK;
+}
+
+static int ensure_io(sfg_context* c, size_t ndoubles) {
+    if (c->io_doubles >= ndoubles) return SFG_OK;
+    if (c->d_io) cudaFree(c->d_io);
+    c->d_io = nullptr;
+    c->io_doubles = 0;
+    CU(cudaMalloc(&c->d_io, ndoubles * sizeof(double)));
+    c->io_doubles = ndoubles;
+    return SFG_OK;
+}
+
+static TileViewArgs last_view(sfg_context* c) {
+    // the tile set of the last completed step (parity (steps - 1) & 1)
+    const int lp = (int)((c->steps + 1) & 1);
+    TileViewArgs tv{c->M > 0 ? c->tb.tile_slot[lp] : nullptr, c->M > 0 ? c->tb.tile_slot[1 - lp] : nullptr,
+                    c->tb.fin[lp], c->tb.gsnap, c->tb.fin[1 - lp]};
+    return tv;
+}
+
+extern "C" int sfg_get_populations(sfg_context* c, int chi, double* f) {
+    int rc = check_chan(c, chi, "sfg_get_populations");
+    if (rc) return rc;
+    if (!f) return fail(SFG_ERR_ARG, "sfg_get_populations: null output");
+    const ChannelDev& d = c->ch[chi].d;
+    const size_t n = 9ULL * d.nx * d.ny;
+    if ((rc = ensure_io(c, n))) return rc;
+    const int p = (int)(c->steps & 1);
+    if (c->precision == SFG_FP64) launch_pop_export<double, double>(c->f[p], c->d_io, d, c->stream);
+    else if (c->precision == SFG_FP32) launch_pop_export<float, float>(c->f[p], c->d_io, d, c->stream);
+    else launch_pop_export<__half, float>(c->f[p], c->d_io, d, c->stream);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(f, c->d_io, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return SFG_OK;
+}
+
+extern "C" int sfg_set_populations(sfg_context* c, int chi, const double* f) {
+    int rc = check_chan(c, chi, "sfg_set_populations");
+    if (rc) return rc;
+    if (!f) return fail(SFG_ERR_ARG, "sfg_set_populations: null input");
+    const ChannelDev& d = c->ch[chi].d;
+    const size_t n = 9ULL * d.nx * d.ny;
+    if ((rc = ensure_io(c, n))) return rc;
+    CU(cudaMemcpyAsync(c->d_io, f, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    for (int i = 0; i < 2; ++i) {
+        if (c->precision == SFG_FP64) launch_pop_import<double, double>(c->d_io, c->f[i], d, c->stream);
+        else if (c->precision == SFG_FP32) launch_pop_import<float, float>(c->d_io, c->f[i], d, c->stream);
+        else launch_pop_import<__half, float>(c->d_io, c->f[i], d, c->stream);
+    }
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(c->stream));
+    return SFG_OK;
+}
+
+extern "C" int sfg_get_macroscopic(sfg_context* c, int chi, double* rho, double* ux, double* uy,
+                                   double* Fx, double* Fy) {
+    int rc = check_chan(c, chi, "sfg_get_macroscopic");
+    if (rc) return rc;
+    const ChannelDev& d = c->ch[chi].d;
+    const size_t N = (size_t)d.nx * d.ny;
+    if ((rc = ensure_io(c, 5 * N))) return rc;
+    const int p = (int)(c->steps & 1);
+    const TileViewArgs tv = last_view(c);
+    const int stepped = c->steps > 0;
+    double* o = c->d_io;
+    if (c->precision == SFG_FP64)
+        launch_macro_export<double, double>(c->f[p], d, tv, stepped, o, o + N, o + 2 * N, o + 3 * N, o + 4 * N, c->stream);
+    else if (c->precision == SFG_FP32)
+        launch_macro_export<float, float>(c->f[p], d, tv, stepped, o, o + N, o + 2 * N, o + 3 * N, o + 4 * N, c->stream);
+    else
+        launch_macro_export<__half, float>(c->f[p], d, tv, stepped, o, o + N, o + 2 * N, o + 3 * N, o + 4 * N, c->stream);
+    CU(cudaGetLastError());
+    double* outs[5] = {rho, ux, uy, Fx, Fy};
+    for (int k = 0; k < 5; ++k)
+        if (outs[k])
+            CU(cudaMemcpyAsync(outs[k], o + k * N, N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return SFG_OK;
+}
+
+extern "C" int sfg_get_markers(sfg_context* c, int chi, double* pos, double* vel, double* force) {
+    int rc = check_chan(c, chi, "sfg_get_markers");
+    if (rc) return rc;
+    const ChannelDev& d = c->ch[chi].d;
+    const int n = d.mk_end - d.mk_begin;
+    if (n > 0) {
+        if (pos) CU(cudaMemcpyAsync(pos, c->mb.pos + d.mk_begin, sizeof(double2) * n, cudaMemcpyDeviceToHost, c->stream));
+        if (vel) CU(cudaMemcpyAsync(vel, c->mb.vel + d.mk_begin, sizeof(double2) * n, cudaMemcpyDeviceToHost, c->stream));
+        if (force) CU(cudaMemcpyAsync(force, c->mb.frc + d.mk_begin, sizeof(double2) * n, cudaMemcpyDeviceToHost, c->stream));
+    }
+    CU(cudaStreamSynchronize(c->stream));
+    return SFG_OK;
+}
+
+extern "C" int sfg_set_markers(sfg_context* c, int chi, const double* pos, const double* vel) {
+    int rc = check_chan(c, chi, "sfg_set_markers");
+    if (rc) return rc;
+    const ChannelDev& d = c->ch[chi].d;
+    const int n = d.mk_end - d.mk_begin;
+    if (n > 0) {
+        if (pos) CU(cudaMemcpyAsync(c->mb.pos + d.mk_begin, pos, sizeof(double2) * n, cudaMemcpyHostToDevice, c->stream));
+        if (vel) CU(cudaMemcpyAsync(c->mb.vel + d.mk_begin, vel, sizeof(double2) * n, cudaMemcpyHostToDevice, c->stream));
+    }
+    CU(cudaStreamSynchronize(c->stream));
+    return SFG_OK;
+}
+
+// Runs the pending scalar step of the last lattice step, if any.
+template <typename S, typename R>
+static int flush_scalar_t(sfg_context* c) {
+    const int P = (int)(c->steps & 1);
+    LatticeLaunch L{c->d_items, c->n_items, c->d_chans, c->f[P], nullptr, c->g[P], c->g[1 - P],
+                    c->cfield, c->d_stepped, c->d_adr_pending, c->d_c_fresh, c->any_adr};
+    launch_scalar_flush<S, R>(L, last_view(c), c->stream);
+    const int nch = (int)c->ch.size();
+    k_flush_flags<<<(nch + 127) / 128, 128, 0, c->stream>>>(nch, c->d_adr_pending, c->d_c_fresh);
+    CU(cudaGetLastError());
+    c->g_cur = 1 - P;
+    c->adr_pending_h = false;
+    return SFG_OK;
+}
+
+static int flush_scalar(sfg_context* c) {
+    if (!c->any_adr || !c->adr_pending_h) return SFG_OK;
+    if (c->precision == SFG_FP64) return flush_scalar_t<double, double>(c);
+    if (c->precision == SFG_FP32) return flush_scalar_t<float, float>(c);
+    return flush_scalar_t<__half, float>(c);
+}
+
+extern "C" int sfg_set_concentration(sfg_context* c, int chi, const double* C) {
+    int rc = check_chan(c, chi, "sfg_set_concentration");
+    if (rc) return rc;
+    if (!C) return fail(SFG_ERR_ARG, "sfg_set_concentration: null input");
+    const ChannelDev& d = c->ch[chi].d;
+    if (!d.adr) return fail(SFG_ERR_STATE, "sfg_set_concentration: scalar transport is off");
+    if ((rc = flush_scalar(c))) return rc;
+    const size_t N = (size_t)d.nx * d.ny;
+    if ((rc = ensure_io(c, N))) return rc;
+    CU(cudaMemcpyAsync(c->d_io, C, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (c->precision == SFG_FP64)
+        k_scalar_set<double><<<io_blocks(N), 256, 0, c->stream>>>(c->d_io, (double*)c->g[0], (double*)c->g[1], (double*)c->cfield, d);
+    else
+        k_scalar_set<float><<<io_blocks(N), 256, 0, c->stream>>>(c->d_io, (float*)c->g[0], (float*)c->g[1], (float*)c->cfield, d);
+    const int one = 1;
+    CU(cudaMemcpyAsync(c->d_c_fresh + chi, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(c->stream));
+    return SFG_OK;
+}
+
+extern "C" int sfg_get_concentration(sfg_context* c, int chi, double* C, double* g) {
+    int rc = check_chan(c, chi, "sfg_get_concentration");
+    if (rc) return rc;
+    const ChannelDev& d = c->ch[chi].d;
+    if (!d.adr) return fail(SFG_ERR_STATE, "sfg_get_concentration: scalar transport is off");
+    if ((rc = flush_scalar(c))) return rc;
+    const size_t N = (size_t)d.nx * d.ny;
+    if ((rc = ensure_io(c, 10 * N))) return rc;
+    double* o = c->d_io;
+    if (c->precision == SFG_FP64)
+        k_scalar_export<double><<<io_blocks(N), 256, 0, c->stream>>>((const double*)c->g[c->g_cur], d, o, g ? o + N : nullptr);
+    else
+        k_scalar_export<float><<<io_blocks(N), 256, 0, c->stream>>>((const float*)c->g[c->g_cur], d, o, g ? o + N : nullptr);
+    CU(cudaGetLastError());
+    if (C) CU(cudaMemcpyAsync(C, o, N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (g) CU(cudaMemcpyAsync(g, o + N, 9 * N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return SFG_OK;
+}
+
+extern "C" int sfg_get_capped_count(sfg_context* c, int chi, int* count) {
+    int rc = check_chan(c, chi, "sfg_get_capped_count");
+    if (rc) return rc;
+    if (!count) return fail(SFG_ERR_ARG, "sfg_get_capped_count: null output");
+    CU(cudaStreamSynchronize(c->stream));
+    if (c->steps == 0) { *count = 0; return SFG_OK; }
+    const ChanHost& h = c->ch[chi];
+    int capped = 0, touched = 0;
+    CU(cudaMemcpy(&capped, c->tb.capped + chi, sizeof(int), cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(&touched, c->tb.fluid_touched + chi, sizeof(int), cudaMemcpyDeviceToHost));
+    const double bx = 0.0 + h.p.body_fx, by = 0.0 + h.p.body_fy;
+    const double Fm = h.p.max_lattice_force;
+    const bool body_capped = bx * bx + by * by > Fm * Fm;
+    long long total = capped;
+    if (body_capped) total += h.fluid_cells - touched;
+    *count = (int)total;
+    return SFG_OK;
+}
+
+extern "C" int sfg_get_contact_counts(sfg_context* c, int chi, int* counts) {
+    int rc = check_chan(c, chi, "sfg_get_contact_counts");
+    if (rc) return rc;
+    const ChannelDev& d = c->ch[chi].d;
+    const int n = d.mk_end - d.mk_begin;
+    if (n > 0 && counts)
+        CU(cudaMemcpyAsync(counts, c->mb.pair_count + d.mk_begin, sizeof(int) * n, cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return SFG_OK;
+}
+
+extern "C" int sfg_num_channels(const sfg_context* c, int* n) {
+    if (!c || !n) return fail(SFG_ERR_ARG, "sfg_num_channels: null argument");
+    *n = (int)c->ch.size();
+    return SFG_OK;
+}
+
+extern "C" int sfg_channel_counts(const sfg_context* c, int chi, int* ncaps, int* nmk) {
+    if (!c || chi < 0 || chi >= (int)c->ch.size()) return fail(SFG_ERR_ARG, "sfg_channel_counts: bad argument");
+    int m = 0;
+    for (const auto& cp : c->ch[chi].caps) m += cp.rest.num_nodes;
+    if (ncaps) *ncaps = (int)c->ch[chi].caps.size();
+    if (nmk) *nmk = m;
+    return SFG_OK;
+}
+
+extern "C" int sfg_step_count(const sfg_context* c, long long* s) {
+    if (!c || !s) return fail(SFG_ERR_ARG, "sfg_step_count: null argument");
+    *s = c->steps;
+    return SFG_OK;
+}
+
+extern "C" int sfg_launches_per_step(const sfg_context* c, int* l) {
+    if (!c || !l) return fail(SFG_ERR_ARG, "sfg_launches_per_step: null argument");
+    *l = c->launches;
+    return SFG_OK;
+}
+
+extern "C" int sfg_get_stream(const sfg_context* c, void** s) {
+    if (!c || !s) return fail(SFG_ERR_ARG, "sfg_get_stream: null argument");
+    *s = (void*)c->stream;
+    return SFG_OK;
+}

@@ -1,0 +1,339 @@
+// lattice.cuh -- fused lattice step (collide + push-stream + halfway bounce-back),
+// the lagged fused scalar step, and the population/macroscopic I/O kernels.
+//
+// State between steps is the post-stream population field (the reference's
+// LatticeField::f_ after LBMSolver::step, lbm_solver.cpp:172-207).  One
+// kernel launch reads every population once (own cell, aligned) and writes
+// it once (to the downstream neighbour, or reflected into the own cell when
+// that neighbour is a wall: the halfway bounce-back of bounce_back.cpp:12-41
+// folded into the store).
+//
+// Storage types: double (FP64), float (FP32), or __half holding f - w
+// (FP16-shifted), with FP32 arithmetic for the last two.
+#pragma once
+#include "collide.cuh"
+
+namespace sfg {
+
+template <typename S, typename R>
+struct PopIO;
+template <>
+struct PopIO<double, double> {
+    static __device__ __forceinline__ double load(const double* p, int) { return __ldg(p); }
+    static __device__ __forceinline__ void store(double* p, int, double v) { *p = v; }
+    static __host__ __device__ double to_host(double s, int) { return s; }
+};
+template <>
+struct PopIO<float, float> {
+    static __device__ __forceinline__ float load(const float* p, int) { return __ldg(p); }
+    static __device__ __forceinline__ void store(float* p, int, float v) { *p = v; }
+};
+template <>
+struct PopIO<__half, float> {
+    // populations stored as deviations from the rest-state weight w_q
+    static __device__ __forceinline__ float load(const __half* p, int q) {
+        return float(w_of(q)) + __half2float(__ldg(p));
+    }
+    static __device__ __forceinline__ void store(__half* p, int q, float v) {
+        *p = __float2half_rn(v - float(w_of(q)));
+    }
+};
+
+// Per-cell forces of one step: Guo force F, the force G that entered the
+// macroscopic velocity the reference's collide reads, and the previous
+// step's force P (for the scalar step's velocity).
+template <typename R>
+struct CellForces {
+    R Fx, Fy, Gx, Gy, Px, Py;
+};
+
+struct TileView {
+    const int* cur_slot;   // global tile -> slot of this step (-1: untouched)
+    const int* prev_slot;  // same for the previous step
+    const void* cur_fin;   // [slot][2][TILE_CELLS] capped total force, R
+    const void* cur_G;     // [slot][2][TILE_CELLS] force before the last MDF sweep, R
+    const void* prev_fin;
+};
+
+template <typename R>
+__device__ __forceinline__ CellForces<R> cell_forces(const ChannelDev& ch, int x, int y,
+                                                     const TileView& tv, int stepped) {
+    CellForces<R> cf;
+    const R Fux = R(ch.F_uni_x), Fuy = R(ch.F_uni_y);
+    const R Pux = stepped ? Fux : R(0), Puy = stepped ? Fuy : R(0);
+    const bool mdf = ch.ibm_iterations > 1;
+    if (ch.cap_end > ch.cap_begin && tv.cur_slot != nullptr) {
+        const int t = ch.tile_base + (y / TILE_H) * ch.tiles_x + (x / TILE_W);
+        const int cell = (y % TILE_H) * TILE_W + (x % TILE_W);
+        const int s = tv.cur_slot[t];
+        const int ps = tv.prev_slot[t];
+        const R* fin = static_cast<const R*>(tv.cur_fin);
+        const R* gs = static_cast<const R*>(tv.cur_G);
+        const R* pfin = static_cast<const R*>(tv.prev_fin);
+        if (s >= 0) {
+            cf.Fx = fin[(size_t)s * 2 * TILE_CELLS + cell];
+            cf.Fy = fin[(size_t)s * 2 * TILE_CELLS + TILE_CELLS + cell];
+        } else {
+            cf.Fx = Fux;
+            cf.Fy = Fuy;
+        }
+        if (ps >= 0) {
+            cf.Px = pfin[(size_t)ps * 2 * TILE_CELLS + cell];
+            cf.Py = pfin[(size_t)ps * 2 * TILE_CELLS + TILE_CELLS + cell];
+        } else {
+            cf.Px = Pux;
+            cf.Py = Puy;
+        }
+        if (mdf) {
+            if (s >= 0) {
+                cf.Gx = gs[(size_t)s * 2 * TILE_CELLS + cell];
+                cf.Gy = gs[(size_t)s * 2 * TILE_CELLS + TILE_CELLS + cell];
+            } else {
+                cf.Gx = R(0);
+                cf.Gy = R(0);
+            }
+        } else {
+            cf.Gx = cf.Px;
+            cf.Gy = cf.Py;
+        }
+    } else {
+        cf.Fx = Fux;
+        cf.Fy = Fuy;
+        cf.Px = Pux;
+        cf.Py = Puy;
+        // with MDF the reference recomputes the moments with the (empty)
+        // immersed-boundary force before colliding
+        cf.Gx = mdf ? R(0) : Pux;
+        cf.Gy = mdf ? R(0) : Puy;
+    }
+    return cf;
+}
+
+// Downstream target of population q leaving (x, y): returns false when the
+// neighbour is a wall (the population is then reflected into the own cell).
+__device__ __forceinline__ bool downstream(const ChannelDev& ch, int x, int y, int q, int wall_mode,
+                                           int& xd, int& yd) {
+    xd = x + cx_of(q);
+    yd = y + cy_of(q);
+    if (xd < 0) xd += ch.nx;
+    if (xd >= ch.nx) xd -= ch.nx;
+    if (wall_mode == 0) {            // SOLID rows 0 and ny-1
+        return !(yd == 0 || yd == ch.ny - 1);
+    } else if (wall_mode == 1) {     // periodic in y
+        if (yd < 0) yd += ch.ny;
+        if (yd >= ch.ny) yd -= ch.ny;
+        return true;
+    }
+    return yd >= 0 && yd < ch.ny;    // open y with reflection at the domain edge
+}
+
+template <typename S, typename R, bool ADR>
+__global__ void __launch_bounds__(256)
+k_lattice_step(const RowItem* __restrict__ items, const ChannelDev* __restrict__ chans,
+               const S* __restrict__ src, S* __restrict__ dst, const R* __restrict__ gsrc,
+               R* __restrict__ gdst, const R* __restrict__ cfield, TileView tv,
+               const int* __restrict__ stepped, const int* __restrict__ adr_pending,
+               const int* __restrict__ c_fresh) {
+    const RowItem it = items[blockIdx.x];
+    if ((int)threadIdx.x >= it.len) return;
+    const ChannelDev& ch = chans[it.chan];
+    const int x = it.x0 + threadIdx.x, y = it.y;
+    const long long n = (long long)y * ch.pitch + x;
+    const S* fs = src + ch.f_off + n;
+    R f[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) f[q] = PopIO<S, R>::load(fs + q * ch.plane, q);
+    R rho, jx, jy;
+    cell_moments(f, rho, jx, jy);
+    const int st = stepped[it.chan];
+    const CellForces<R> cf = cell_forces<R>(ch, x, y, tv, st);
+    R ux, uy;
+    cell_velocity(rho, jx, jy, cf.Gx, cf.Gy, ux, uy);
+    if (ch.collision == 2) {
+        collide_regularized(f, rho, ux, uy, cf.Fx, cf.Fy, R(ch.omega));
+    } else if (ch.collision == 1) {
+        collide_mrt(f, rho, ux, uy, cf.Fx, cf.Fy, R(ch.omega), R(ch.mrt_se), R(ch.mrt_s_eps),
+                    R(ch.mrt_sq));
+    } else {
+        collide_bgk(f, rho, ux, uy, cf.Fx, cf.Fy, R(ch.omega));
+    }
+    const int wall_mode = ch.periodic_y ? 1 : 0;
+    S* fd = dst + ch.f_off;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        int xd, yd;
+        if (downstream(ch, x, y, q, wall_mode, xd, yd))
+            PopIO<S, R>::store(fd + q * ch.plane + (long long)yd * ch.pitch + xd, q, f[q]);
+        else
+            PopIO<S, R>::store(fd + opp_of(q) * ch.plane + n, opp_of(q), f[q]);
+    }
+    if (ADR) {
+        // Scalar step of the previous lattice step (it needs that step's
+        // final velocity, which is only known once its populations have been
+        // streamed): advection_diffusion.cpp:84-223.
+        if (ch.adr && adr_pending[it.chan]) {
+            R g[9];
+            const R* gp = gsrc + ch.g_off + n;
+#pragma unroll
+            for (int q = 0; q < 9; ++q) g[q] = gp[q * ch.plane];
+            R C;
+            if (c_fresh[it.chan]) C = cfield[ch.cell_off + n];
+            else C = g[0] + g[1] + g[2] + g[3] + g[4] + g[5] + g[6] + g[7] + g[8];
+            R vx, vy;
+            cell_velocity(rho, jx, jy, cf.Px, cf.Py, vx, vy);
+            collide_scalar(g, C, vx, vy, R(ch.omega_s));
+            const int gwall = ch.periodic_y ? (ch.adr_periodic_y ? 1 : 2) : 0;
+            R* gd = gdst + ch.g_off;
+#pragma unroll
+            for (int q = 0; q < 9; ++q) {
+                int xd, yd;
+                if (downstream(ch, x, y, q, gwall, xd, yd))
+                    gd[q * ch.plane + (long long)yd * ch.pitch + xd] = g[q];
+                else
+                    gd[opp_of(q) * ch.plane + n] = g[q];
+            }
+        }
+    }
+}
+
+// Scalar step alone (used to bring the scalar up to date before a host read).
+template <typename S, typename R>
+__global__ void __launch_bounds__(256)
+k_scalar_flush(const RowItem* __restrict__ items, const ChannelDev* __restrict__ chans,
+               const S* __restrict__ src, const R* __restrict__ gsrc, R* __restrict__ gdst,
+               const R* __restrict__ cfield, TileView tv_last, const int* __restrict__ stepped_prev,
+               const int* __restrict__ adr_pending, const int* __restrict__ c_fresh) {
+    const RowItem it = items[blockIdx.x];
+    if ((int)threadIdx.x >= it.len) return;
+    const ChannelDev& ch = chans[it.chan];
+    if (!ch.adr || !adr_pending[it.chan]) return;
+    const int x = it.x0 + threadIdx.x, y = it.y;
+    const long long n = (long long)y * ch.pitch + x;
+    const S* fs = src + ch.f_off + n;
+    R f[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) f[q] = PopIO<S, R>::load(fs + q * ch.plane, q);
+    R rho, jx, jy;
+    cell_moments(f, rho, jx, jy);
+    // the force of the last completed step plays the role of P here; it is
+    // that step's "cur" tile set, passed as cur_* in tv_last
+    const CellForces<R> cf = cell_forces<R>(ch, x, y, tv_last, 1);
+    R g[9];
+    const R* gp = gsrc + ch.g_off + n;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) g[q] = gp[q * ch.plane];
+    R C;
+    if (c_fresh[it.chan]) C = cfield[ch.cell_off + n];
+    else C = g[0] + g[1] + g[2] + g[3] + g[4] + g[5] + g[6] + g[7] + g[8];
+    R vx, vy;
+    cell_velocity(rho, jx, jy, cf.Fx, cf.Fy, vx, vy);
+    collide_scalar(g, C, vx, vy, R(ch.omega_s));
+    const int gwall = ch.periodic_y ? (ch.adr_periodic_y ? 1 : 2) : 0;
+    R* gd = gdst + ch.g_off;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        int xd, yd;
+        if (downstream(ch, x, y, q, gwall, xd, yd))
+            gd[q * ch.plane + (long long)yd * ch.pitch + xd] = g[q];
+        else
+            gd[opp_of(q) * ch.plane + n] = g[q];
+    }
+    (void)stepped_prev;
+}
+
+// ---- host <-> device population transfer (canonical FP64 [9][ny][nx]) ----
+
+template <typename S, typename R>
+__global__ void k_pop_import(const double* __restrict__ in, S* __restrict__ out, ChannelDev ch) {
+    const long long N = (long long)ch.nx * ch.ny;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 9 * N;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int q = (int)(i / N);
+        const long long r = i % N;
+        const int y = (int)(r / ch.nx), x = (int)(r % ch.nx);
+        PopIO<S, R>::store(out + ch.f_off + q * ch.plane + (long long)y * ch.pitch + x, q,
+                           (R)in[i]);
+    }
+}
+
+template <typename S>
+__device__ __forceinline__ double pop_export_one(const S* p, int q);
+template <>
+__device__ __forceinline__ double pop_export_one<double>(const double* p, int) { return *p; }
+template <>
+__device__ __forceinline__ double pop_export_one<float>(const float* p, int) { return (double)*p; }
+template <>
+__device__ __forceinline__ double pop_export_one<__half>(const __half* p, int q) {
+    return w_of(q) + (double)__half2float(*p);
+}
+
+template <typename S>
+__global__ void k_pop_export(const S* __restrict__ in, double* __restrict__ out, ChannelDev ch) {
+    const long long N = (long long)ch.nx * ch.ny;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 9 * N;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int q = (int)(i / N);
+        const long long r = i % N;
+        const int y = (int)(r / ch.nx), x = (int)(r % ch.nx);
+        out[i] = pop_export_one<S>(in + ch.f_off + q * ch.plane + (long long)y * ch.pitch + x, q);
+    }
+}
+
+// Macroscopic fields of the current state with the force of the last step
+// (reference LatticeField::computeMacroscopic, lattice_field.cpp:28-73).
+// Also exports that force field.
+template <typename S, typename R>
+__global__ void k_macro_export(const S* __restrict__ in, ChannelDev ch, TileView tv_last,
+                               int stepped, double* __restrict__ rho_o, double* __restrict__ ux_o,
+                               double* __restrict__ uy_o, double* __restrict__ Fx_o,
+                               double* __restrict__ Fy_o) {
+    const long long N = (long long)ch.nx * ch.ny;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(i / ch.nx), x = (int)(i % ch.nx);
+        const bool solid = !ch.periodic_y && (y == 0 || y == ch.ny - 1);
+        // last step's force (the "cur" tile set of that step)
+        R Fx, Fy;
+        if (!stepped) {
+            Fx = R(0);
+            Fy = R(0);
+        } else {
+            CellForces<R> cf = cell_forces<R>(ch, x, y, tv_last, 1);
+            Fx = cf.Fx;
+            Fy = cf.Fy;
+            if (solid) {
+                bool touched = false;
+                if (ch.cap_end > ch.cap_begin && tv_last.cur_slot != nullptr) {
+                    const int t = ch.tile_base + (y / TILE_H) * ch.tiles_x + (x / TILE_W);
+                    touched = tv_last.cur_slot[t] >= 0;
+                }
+                if (!touched) {
+                    Fx = R(0);
+                    Fy = R(0);
+                }
+            }
+        }
+        if (Fx_o) {
+            Fx_o[i] = (double)Fx;
+            Fy_o[i] = (double)Fy;
+        }
+        if (solid) {
+            rho_o[i] = 0.0;
+            ux_o[i] = 0.0;
+            uy_o[i] = 0.0;
+            continue;
+        }
+        R f[9];
+        const long long n = (long long)y * ch.pitch + x;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) f[q] = PopIO<S, R>::load(in + ch.f_off + q * ch.plane + n, q);
+        R rho, jx, jy, ux, uy;
+        cell_moments(f, rho, jx, jy);
+        cell_velocity(rho, jx, jy, Fx, Fy, ux, uy);
+        rho_o[i] = (double)rho;
+        ux_o[i] = (double)ux;
+        uy_o[i] = (double)uy;
+    }
+}
+
+}  // namespace sfg

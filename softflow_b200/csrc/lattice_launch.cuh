@@ -1,0 +1,78 @@
+// lattice_launch.cuh -- host launch wrappers of the lattice kernels; included
+// by lattice_f64.cu (FP64, no FMA contraction) and lattice_f32.cu (FP32 and
+// FP16-shifted storage).
+#pragma once
+#include "lattice.cuh"
+#include "sfg_internal.h"
+
+namespace sfg {
+
+inline TileView to_view(const TileViewArgs& a) {
+    TileView v;
+    v.cur_slot = a.cur_slot;
+    v.prev_slot = a.prev_slot;
+    v.cur_fin = a.cur_fin;
+    v.cur_G = a.cur_G;
+    v.prev_fin = a.prev_fin;
+    return v;
+}
+
+template <typename S, typename R>
+void launch_lattice_step(const LatticeLaunch& L, const TileViewArgs& tv, cudaStream_t st) {
+    if (L.n_items == 0) return;
+    if (L.any_adr)
+        k_lattice_step<S, R, true><<<L.n_items, 256, 0, st>>>(
+            L.items, L.chans, static_cast<const S*>(L.src), static_cast<S*>(L.dst),
+            static_cast<const R*>(L.gsrc), static_cast<R*>(L.gdst),
+            static_cast<const R*>(L.cfield), to_view(tv), L.stepped, L.adr_pending, L.c_fresh);
+    else
+        k_lattice_step<S, R, false><<<L.n_items, 256, 0, st>>>(
+            L.items, L.chans, static_cast<const S*>(L.src), static_cast<S*>(L.dst), nullptr,
+            nullptr, nullptr, to_view(tv), L.stepped, L.adr_pending, L.c_fresh);
+}
+
+template <typename S, typename R>
+void launch_scalar_flush(const LatticeLaunch& L, const TileViewArgs& tv_last, cudaStream_t st) {
+    if (L.n_items == 0 || !L.any_adr) return;
+    k_scalar_flush<S, R><<<L.n_items, 256, 0, st>>>(
+        L.items, L.chans, static_cast<const S*>(L.src), static_cast<const R*>(L.gsrc),
+        static_cast<R*>(L.gdst), static_cast<const R*>(L.cfield), to_view(tv_last), L.stepped,
+        L.adr_pending, L.c_fresh);
+}
+
+inline int io_grid(long long n) {
+    long long g = (n + 255) / 256;
+    return (int)(g > 4096 ? 4096 : (g < 1 ? 1 : g));
+}
+
+template <typename S, typename R>
+void launch_pop_import(const double* in, void* out, const ChannelDev& ch, cudaStream_t st) {
+    k_pop_import<S, R><<<io_grid(9LL * ch.nx * ch.ny), 256, 0, st>>>(in, static_cast<S*>(out), ch);
+}
+
+template <typename S, typename R>
+void launch_pop_export(const void* in, double* out, const ChannelDev& ch, cudaStream_t st) {
+    k_pop_export<S><<<io_grid(9LL * ch.nx * ch.ny), 256, 0, st>>>(static_cast<const S*>(in), out,
+                                                                  ch);
+}
+
+template <typename S, typename R>
+void launch_macro_export(const void* in, const ChannelDev& ch, const TileViewArgs& tv_last,
+                         int stepped, double* rho, double* ux, double* uy, double* Fx, double* Fy,
+                         cudaStream_t st) {
+    k_macro_export<S, R><<<io_grid((long long)ch.nx * ch.ny), 256, 0, st>>>(
+        static_cast<const S*>(in), ch, to_view(tv_last), stepped, rho, ux, uy, Fx, Fy);
+}
+
+#define SFG_LATTICE_INST(S, R)                                                                   \
+    template void launch_lattice_step<S, R>(const LatticeLaunch&, const TileViewArgs&,           \
+                                            cudaStream_t);                                        \
+    template void launch_scalar_flush<S, R>(const LatticeLaunch&, const TileViewArgs&,           \
+                                            cudaStream_t);                                        \
+    template void launch_pop_import<S, R>(const double*, void*, const ChannelDev&, cudaStream_t); \
+    template void launch_pop_export<S, R>(const void*, double*, const ChannelDev&, cudaStream_t); \
+    template void launch_macro_export<S, R>(const void*, const ChannelDev&, const TileViewArgs&,  \
+                                            int, double*, double*, double*, double*, double*,     \
+                                            cudaStream_t);
+
+}  // namespace sfg

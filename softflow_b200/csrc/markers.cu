@@ -1,0 +1,876 @@
+// markers.cu -- marker-side kernels (FP64, compiled with --fmad=false).
+//
+// Membrane mechanics follow reference src/membrane/capsule.cpp:149-671,
+// contact follows src/membrane/repulsion.cpp:6-284 with the cell list of
+// src/membrane/cell_list.h:36-146, and the immersed-boundary coupling
+// follows src/coupling/immersed_boundary.cpp:25-286.
+//
+// Spreading is a deterministic gather: every lattice cell of a touched
+// 32 x 8 force tile sums the contributions of the markers whose 4 x 4
+// stencil covers it, in ascending marker order (the reference's serial
+// order), with no floating-point atomics.
+#include <climits>
+
+#include "markers.cuh"
+#include "lattice.cuh"
+#include "sfg_internal.h"
+
+namespace sfg {
+
+// ============================ membrane forces ==============================
+// One warp per capsule.  Nodes are staged in shared memory; lanes work on
+// nodes/edges in parallel; the ring reductions (area, perimeter) run
+// sequentially in lane 0 in the reference's order.  Each node applies the
+// contributions of its two edges (or three bending stencils) in the order
+// in which the reference's edge loop reaches them.
+
+constexpr int MEM_WARPS = 4;
+constexpr int MEM_DOUBLES_PER_NODE = 11;  // P, F, E, GN, GP (2 each) + OK
+
+__device__ __forceinline__ void apply_edges(double2* F, const double2* E, const double* OK, int n,
+                                            int k, double s_first, double s_second) {
+    // node k is the first node of edge k and the second node of edge k-1
+    double2 a = F[k];
+    if (k == 0) {
+        if (OK[0] != 0.0) { a.x = a.x + s_first * E[0].x; a.y = a.y + s_first * E[0].y; }
+        if (n > 1 && OK[n - 1] != 0.0) {
+            a.x = a.x + s_second * E[n - 1].x;
+            a.y = a.y + s_second * E[n - 1].y;
+        }
+    } else {
+        if (OK[k - 1] != 0.0) {
+            a.x = a.x + s_second * E[k - 1].x;
+            a.y = a.y + s_second * E[k - 1].y;
+        }
+        if (OK[k] != 0.0) { a.x = a.x + s_first * E[k].x; a.y = a.y + s_first * E[k].y; }
+    }
+    F[k] = a;
+}
+// s_first / s_second are +1 or -1: multiplying by them is exact, so
+// a + (-1) * e == a - e bit for bit.
+
+__global__ void k_membrane(const CapsuleDev* __restrict__ caps, int ncaps, MarkerBufs mb,
+                           int* __restrict__ has_prev, int maxn, unsigned* status) {
+    extern __shared__ double smem[];
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int c = blockIdx.x * MEM_WARPS + warp;
+    if (c >= ncaps) return;
+    double* base = smem + (size_t)warp * MEM_DOUBLES_PER_NODE * maxn;
+    double2* P = reinterpret_cast<double2*>(base);
+    double2* F = P + maxn;
+    double2* E = F + maxn;
+    double2* GN = E + maxn;
+    double2* GP = GN + maxn;
+    double* OK = reinterpret_cast<double*>(GP + maxn);
+    const CapsuleDev cp = caps[c];
+    const int n = cp.n, off = cp.off;
+    if (n > maxn) {
+        if (lane == 0) atomicOr(status, (unsigned)ST_CAPSULE_TOO_BIG);
+        return;
+    }
+    const double Lx = (double)cp.periodic_nx;
+    for (int k = lane; k < n; k += 32) {
+        P[k] = mb.pos[off + k];
+        F[k] = make_double2(0.0, 0.0);
+    }
+    __syncwarp();
+
+    // ---- stretching (capsule.cpp:338-470) ----
+    for (int i = lane; i < n; i += 32) {
+        const int j = (i + 1) % n;
+        const double2 diff = min_image_d(P[j], P[i], Lx);
+        const double L = norm_d(diff);
+        if (L < 1e-15) { OK[i] = 0.0; continue; }
+        const double L0 = mb.rest_len[off + i];
+        double F_mag;
+        if (cp.model == 1) {            // Neo-Hookean
+            double lambda = L / L0;
+            double inv3 = 1.0 / (lambda * lambda * lambda);
+            F_mag = cp.G_s * (lambda - inv3);
+        } else if (cp.model == 2) {     // Skalak
+            double lambda = L / L0;
+            double l2 = lambda * lambda;
+            F_mag = cp.G_s * lambda * (l2 - 1.0) * (1.0 + cp.C_skalak);
+        } else if (cp.model == 3) {     // WLC + power-law repulsion
+            double L_max = cp.wlc_L_max_ratio * L0;
+            double x = L / L_max;
+            if (x > 0.99) x = 0.99;
+            double F_wlc = cp.wlc_kBT_p * (1.0 / (4.0 * (1.0 - x) * (1.0 - x)) - 0.25 + x);
+            double F_pow = -cp.wlc_k_pow / L;
+            F_mag = F_wlc + F_pow;
+        } else {                        // Hookean
+            F_mag = cp.k_stretch * (L / L0 - 1.0);
+        }
+        const double2 dir = make_double2(diff.x / L, diff.y / L);
+        E[i] = make_double2(dir.x * F_mag, dir.y * F_mag);
+        OK[i] = 1.0;
+    }
+    __syncwarp();
+    for (int k = lane; k < n; k += 32) apply_edges(F, E, OK, n, k, 1.0, -1.0);
+    __syncwarp();
+
+    // ---- bending (capsule.cpp:476-541) ----
+    if (cp.use_helfrich) {
+        for (int i = lane; i < n; i += 32) {
+            const int ip = (i - 1 + n) % n, in = (i + 1) % n;
+            const double2 ep = min_image_d(P[i], P[ip], Lx);
+            const double2 en = min_image_d(P[in], P[i], Lx);
+            const double lp2 = ep.x * ep.x + ep.y * ep.y, ln2 = en.x * en.x + en.y * en.y;
+            if (lp2 < 1e-30 || ln2 < 1e-30) { OK[i] = 0.0; continue; }
+            const double dth = atan2(ep.x * en.y - ep.y * en.x, ep.x * en.x + ep.y * en.y) -
+                               mb.rest_ang[off + i];
+            const double cc = -cp.k_bend * dth / mb.rest_ds[off + i];
+            const double2 gn = make_double2(-en.y / ln2, en.x / ln2);
+            const double2 gp = make_double2(-ep.y / lp2, ep.x / lp2);
+            GN[i] = make_double2(gn.x * cc, gn.y * cc);
+            GP[i] = make_double2(gp.x * cc, gp.y * cc);
+            E[i] = make_double2((gn.x + gp.x) * cc, (gn.y + gp.y) * cc);
+            OK[i] = 1.0;
+        }
+        __syncwarp();
+        for (int k = lane; k < n; k += 32) {
+            // stencils i in {k-1, k, k+1} touch node k; apply in loop order
+            int ids[3] = {(k - 1 + n) % n, k, (k + 1) % n};
+            for (int a = 0; a < 3; ++a)
+                for (int b = a + 1; b < 3; ++b)
+                    if (ids[b] < ids[a]) { int t = ids[a]; ids[a] = ids[b]; ids[b] = t; }
+            double2 acc = F[k];
+            for (int a = 0; a < 3; ++a) {
+                const int i = ids[a];
+                if (a > 0 && i == ids[a - 1]) continue;
+                if (OK[i] == 0.0) continue;
+                if ((i + 1) % n == k) { acc.x = acc.x + GN[i].x; acc.y = acc.y + GN[i].y; }
+                if ((i - 1 + n) % n == k) { acc.x = acc.x + GP[i].x; acc.y = acc.y + GP[i].y; }
+                if (i == k) { acc.x = acc.x - E[i].x; acc.y = acc.y - E[i].y; }
+            }
+            F[k] = acc;
+        }
+    } else {
+        for (int i = lane; i < n; i += 32) {
+            const double2 dp = min_image_d(P[(i - 1 + n) % n], P[i], Lx);
+            const double2 dn = min_image_d(P[(i + 1) % n], P[i], Lx);
+            const double2 lap = make_double2(dp.x + dn.x, dp.y + dn.y);
+            F[i] = make_double2(F[i].x + lap.x * cp.k_bend, F[i].y + lap.y * cp.k_bend);
+        }
+    }
+    __syncwarp();
+
+    // ---- ring reductions in the reference's order (capsule.cpp:175-204) ----
+    double sarea = 0.0, perim = 0.0;
+    if (lane == 0) {
+        if (Lx > 0.0) {
+            double2 cur = P[0];
+            for (int i = 0; i < n; ++i) {
+                double2 nxt;
+                if (i + 1 < n) {
+                    double2 d = min_image_d(P[i + 1], P[i], Lx);
+                    nxt = make_double2(cur.x + d.x, cur.y + d.y);
+                } else {
+                    nxt = P[0];
+                }
+                sarea += cur.x * nxt.y - cur.y * nxt.x;
+                cur = nxt;
+            }
+        } else {
+            for (int i = 0; i < n; ++i) {
+                const double2 a = P[i], b = P[(i + 1) % n];
+                sarea += a.x * b.y - a.y * b.x;
+            }
+        }
+        for (int i = 0; i < n; ++i) perim += norm_d(min_image_d(P[(i + 1) % n], P[i], Lx));
+    }
+    sarea = __shfl_sync(0xffffffffu, sarea, 0);
+    perim = __shfl_sync(0xffffffffu, perim, 0);
+
+    // ---- area penalty (capsule.cpp:547-586) ----
+    {
+        const double A = 0.5 * fabs(sarea), A0 = cp.rest_area;
+        if (!(A0 < 1e-15)) {
+            const double coeff = -cp.k_area * (A - A0) / A0;
+            const double sign = (sarea >= 0.0) ? 1.0 : -1.0;
+            for (int i = lane; i < n; i += 32) {
+                const double2 ep = min_image_d(P[i], P[(i - 1 + n) % n], Lx);
+                const double2 en = min_image_d(P[(i + 1) % n], P[i], Lx);
+                double2 o = make_double2((ep.y + en.y) * 0.5, (-ep.x + -en.x) * 0.5);
+                const double len = norm_d(o);
+                if (len < 1e-15) continue;
+                o = make_double2(o.x / len * sign, o.y / len * sign);
+                F[i] = make_double2(F[i].x + o.x * coeff, F[i].y + o.y * coeff);
+            }
+        }
+    }
+    __syncwarp();
+
+    // ---- perimeter penalty (capsule.cpp:588-604) ----
+    {
+        const double P0 = cp.rest_perimeter;
+        if (!(P0 < 1e-15)) {
+            const double coeff = -cp.k_perimeter * (perim - P0) / P0;
+            for (int i = lane; i < n; i += 32) {
+                const double2 diff = min_image_d(P[(i + 1) % n], P[i], Lx);
+                const double L = norm_d(diff);
+                if (L < 1e-15) { OK[i] = 0.0; continue; }
+                E[i] = make_double2(diff.x / L * coeff, diff.y / L * coeff);
+                OK[i] = 1.0;
+            }
+            __syncwarp();
+            for (int k = lane; k < n; k += 32) apply_edges(F, E, OK, n, k, -1.0, 1.0);
+            __syncwarp();
+        }
+    }
+
+    // ---- lab-frame damping (capsule.cpp:606-610) ----
+    for (int k = lane; k < n; k += 32) {
+        const double2 v = mb.vel[off + k];
+        F[k] = make_double2(F[k].x - v.x * cp.gamma_visc, F[k].y - v.y * cp.gamma_visc);
+    }
+    __syncwarp();
+
+    // ---- Kelvin-Voigt membrane viscosity (capsule.cpp:612-671) ----
+    if (cp.eta_membrane > 0.0) {
+        if (!has_prev[c]) {
+            for (int i = lane; i < n; i += 32)
+                mb.prev_len[off + i] = norm_d(min_image_d(P[(i + 1) % n], P[i], Lx));
+            __syncwarp();
+            if (lane == 0) has_prev[c] = 1;
+        } else {
+            for (int i = lane; i < n; i += 32) {
+                const double2 diff = min_image_d(P[(i + 1) % n], P[i], Lx);
+                const double L = norm_d(diff);
+                if (L < 1e-15) { OK[i] = 0.0; continue; }
+                const double strain = (L - mb.prev_len[off + i]) / mb.rest_len[off + i];
+                const double Fv = cp.eta_membrane * strain;
+                E[i] = make_double2(diff.x / L * Fv, diff.y / L * Fv);
+                OK[i] = 1.0;
+                mb.prev_len[off + i] = L;
+            }
+            __syncwarp();
+            for (int k = lane; k < n; k += 32) apply_edges(F, E, OK, n, k, 1.0, -1.0);
+            __syncwarp();
+        }
+    }
+    for (int k = lane; k < n; k += 32) mb.frc[off + k] = F[k];
+}
+
+// ================================ contact ==================================
+
+__device__ __forceinline__ int contact_cell(const ChannelDev& ch, double2 p) {
+    if (!finite2(p)) return 0;
+    const double Lx = (double)ch.nx;
+    double px = p.x - 0.0;
+    px = fmod(px, Lx);
+    if (px < 0.0) px += Lx;
+    int cx = (int)floor(px / ch.cdx);
+    int cy = (int)floor((p.y - ch.y_bot) / ch.cdy);
+    if (cx < 0) cx = 0;
+    if (cx >= ch.ncx) cx = ch.ncx - 1;
+    if (cy < 0) cy = 0;
+    if (cy >= ch.ncy) cy = ch.ncy - 1;
+    return cy * ch.ncx + cx;
+}
+
+__device__ __forceinline__ double2 pair_force(const ChannelDev& ch, double2 pa, double2 va,
+                                              double2 pb, double2 vb) {
+    const double Lx = (double)ch.nx;
+    double2 diff = make_double2(pa.x - pb.x, pa.y - pb.y);
+    if (Lx > 0.0) {
+        if (diff.x > 0.5 * Lx) diff.x -= Lx;
+        if (diff.x < -0.5 * Lx) diff.x += Lx;
+    }
+    const double r = norm_d(diff);
+    if (r < 1e-15 || r >= ch.rep_r_cut) return make_double2(0.0, 0.0);
+    const double2 nrm = make_double2(diff.x / r, diff.y / r);
+    const double F_rep = ch.rep_epsilon * pow(ch.rep_sigma / r, (double)ch.rep_power);
+    double F_n = F_rep;
+    double2 F_t = make_double2(0.0, 0.0);
+    if (ch.rep_damping > 0.0 || ch.rep_friction > 0.0) {
+        const double2 vr = make_double2(va.x - vb.x, va.y - vb.y);
+        const double v_n = vr.x * nrm.x + vr.y * nrm.y;
+        F_n = F_rep - ch.rep_damping * v_n;
+        if (F_n < 0.0) F_n = 0.0;
+        if (ch.rep_friction > 0.0) {
+            const double2 vt = make_double2(vr.x - nrm.x * v_n, vr.y - nrm.y * v_n);
+            const double vtm = norm_d(vt);
+            if (vtm > 1e-12) {
+                const double s = -ch.rep_friction * F_n;
+                F_t = make_double2(vt.x / vtm * s, vt.y / vtm * s);
+            }
+        }
+    }
+    return make_double2(nrm.x * F_n + F_t.x, nrm.y * F_n + F_t.y);
+}
+
+__global__ void k_contact_bin(const ChannelDev* __restrict__ chans, int M, MarkerBufs mb,
+                              int* __restrict__ cell_of, int* __restrict__ cell_cnt) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    const ChannelDev& ch = chans[mb.mk_chan[m]];
+    if (ch.brute_contact) return;
+    const int c = ch.cell_base + contact_cell(ch, mb.pos[m]);
+    cell_of[m] = c;
+    atomicAdd(&cell_cnt[c], 1);
+}
+
+__global__ void k_contact_fill(const ChannelDev* __restrict__ chans, int M, MarkerBufs mb,
+                               const int* __restrict__ cell_of, const int* __restrict__ cell_start,
+                               int* __restrict__ cursor, int* __restrict__ list) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    const ChannelDev& ch = chans[mb.mk_chan[m]];
+    if (ch.brute_contact) return;
+    const int c = cell_of[m];
+    list[cell_start[c] + atomicAdd(&cursor[c], 1)] = m;
+}
+
+// Cells hold a handful of markers: insertion sort restores the reference's
+// insertion order (capsule-major, node-minor = ascending marker index).
+__global__ void k_contact_sort(int ncells, const int* __restrict__ cell_start,
+                               const int* __restrict__ cell_cnt, int* __restrict__ list) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    int* a = list + cell_start[c];
+    const int n = cell_cnt[c];
+    for (int i = 1; i < n; ++i) {
+        const int v = a[i];
+        int j = i - 1;
+        while (j >= 0 && a[j] > v) { a[j + 1] = a[j]; --j; }
+        a[j + 1] = v;
+    }
+}
+
+__global__ void k_contact_force(const ChannelDev* __restrict__ chans, int M, MarkerBufs mb,
+                                const int* __restrict__ cell_of, const int* __restrict__ cell_start,
+                                const int* __restrict__ cell_cnt, const int* __restrict__ list) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    const ChannelDev& ch = chans[mb.mk_chan[m]];
+    const int cap = mb.mk_cap[m];
+    const double2 pa = mb.pos[m], va = mb.vel[m];
+    double2 F = mb.frc[m];
+    int count = 0;
+    if (ch.brute_contact) {
+        for (int b = ch.mk_begin; b < ch.mk_end; ++b) {
+            if (mb.mk_cap[b] == cap) continue;
+            const double2 f = pair_force(ch, pa, va, mb.pos[b], mb.vel[b]);
+            F.x = F.x + f.x;
+            F.y = F.y + f.y;
+            ++count;
+        }
+    } else {
+        const int ci = cell_of[m] - ch.cell_base;
+        const int cx = ci % ch.ncx, cy = ci / ch.ncx;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int yy = cy + dy;
+            if (yy < 0 || yy >= ch.ncy) continue;
+            for (int dx = -1; dx <= 1; ++dx) {
+                int xx = cx + dx;
+                if (xx < 0) xx += ch.ncx;
+                if (xx >= ch.ncx) xx -= ch.ncx;
+                const int cell = ch.cell_base + yy * ch.ncx + xx;
+                const int s = cell_start[cell], e = s + cell_cnt[cell];
+                for (int k = s; k < e; ++k) {
+                    const int b = list[k];
+                    if (mb.mk_cap[b] == cap) continue;
+                    const double2 f = pair_force(ch, pa, va, mb.pos[b], mb.vel[b]);
+                    F.x = F.x + f.x;
+                    F.y = F.y + f.y;
+                    ++count;
+                }
+            }
+        }
+    }
+    const double2 z = make_double2(0.0, 0.0);
+    double2 f = pair_force(ch, pa, va, make_double2(pa.x, ch.y_bot), z);
+    F.x = F.x + f.x;
+    F.y = F.y + f.y;
+    f = pair_force(ch, pa, va, make_double2(pa.x, ch.y_top), z);
+    F.x = F.x + f.x;
+    F.y = F.y + f.y;
+    mb.frc[m] = F;
+    mb.pair_count[m] = count;
+}
+
+// ====================== immersed-boundary force tiles ======================
+
+// Tiles covered by the stencil of a marker (at most 4 columns x 2 rows).
+__device__ __forceinline__ int stencil_tiles(const ChannelDev& ch, int ix0, int iy0, int out[8]) {
+    int tys[2], nty = 0;
+    for (int iy = iy0 - 1; iy <= iy0 + 2; ++iy) {
+        if (iy < 0 || iy >= ch.ny) continue;
+        const int ty = iy / TILE_H;
+        if (nty == 0 || tys[nty - 1] != ty) tys[nty++] = ty;
+    }
+    int txs[4], ntx = 0;
+    for (int ix = ix0 - 1; ix <= ix0 + 2; ++ix) {
+        int jx = ix;
+        if (jx < 0) jx += ch.nx;
+        if (jx >= ch.nx) jx -= ch.nx;
+        if (jx < 0 || jx >= ch.nx) continue;
+        const int tx = jx / TILE_W;
+        bool dup = false;
+        for (int a = 0; a < ntx; ++a) dup |= (txs[a] == tx);
+        if (!dup) txs[ntx++] = tx;
+    }
+    int n = 0;
+    for (int a = 0; a < nty; ++a)
+        for (int b = 0; b < ntx; ++b) out[n++] = ch.tile_base + tys[a] * ch.tiles_x + txs[b];
+    return n;
+}
+
+// Per-marker preparation: arc length ds (min-image, immersed_boundary.cpp:
+// 164-173), stencil origin, validity, and the tile occupancy counts.
+__global__ void k_ibm_prep(const ChannelDev* __restrict__ chans,
+                           const CapsuleDev* __restrict__ caps, int M, MarkerBufs mb,
+                           int* __restrict__ tile_flag, int* __restrict__ tile_cnt,
+                           unsigned* status) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    const ChannelDev& ch = chans[mb.mk_chan[m]];
+    const CapsuleDev& cp = caps[mb.mk_cap[m]];
+    const int k = m - cp.off, n = cp.n;
+    const int kp = cp.off + (k - 1 + n) % n, kn = cp.off + (k + 1) % n;
+    const double Lx = (double)ch.nx;
+    const double2 p = mb.pos[m];
+    const double dp = norm_d(min_image_d(p, mb.pos[kp], Lx));
+    const double dn = norm_d(min_image_d(mb.pos[kn], p, Lx));
+    mb.ds[m] = 0.5 * (dp + dn);
+    int ok = finite2(p);
+    int ix0 = 0, iy0 = 0;
+    if (ok) {
+        // markers more than one period outside the lattice are skipped (the
+        // reference indexes out of range there); wrapped x stays in [0, nx)
+        if (p.x < -(double)ch.nx + 2.0 || p.x >= 2.0 * (double)ch.nx - 3.0) ok = 0;
+        if (fabs(p.y) > 1e9) ok = 0;
+    }
+    if (ok) {
+        ix0 = (int)floor(p.x);
+        iy0 = (int)floor(p.y);
+        if (iy0 < -2 || iy0 >= ch.ny + 2) ok = 0;
+    } else if (!finite2(p)) {
+        atomicOr(status, (unsigned)ST_NAN_MARKER);
+    }
+    mb.ix0[m] = ix0;
+    mb.iy0[m] = iy0;
+    mb.valid[m] = ok;
+    if (!ok) return;
+    int t[8];
+    const int nt = stencil_tiles(ch, ix0, iy0, t);
+    for (int a = 0; a < nt; ++a) {
+        tile_flag[t[a]] = 1;
+        atomicAdd(&tile_cnt[t[a]], 1);
+    }
+}
+
+__global__ void k_tile_slots(int T, const int* __restrict__ tile_flag,
+                             const int* __restrict__ slot_scan, int* __restrict__ tile_slot,
+                             int* __restrict__ slot_tile) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    if (tile_flag[t]) {
+        tile_slot[t] = slot_scan[t];
+        slot_tile[slot_scan[t]] = t;
+    } else {
+        tile_slot[t] = -1;
+    }
+}
+
+__global__ void k_tile_fill(const ChannelDev* __restrict__ chans, int M, MarkerBufs mb,
+                            const int* __restrict__ list_off, int* __restrict__ cursor,
+                            int* __restrict__ list) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M || !mb.valid[m]) return;
+    const ChannelDev& ch = chans[mb.mk_chan[m]];
+    int t[8];
+    const int nt = stencil_tiles(ch, mb.ix0[m], mb.iy0[m], t);
+    for (int a = 0; a < nt; ++a) list[list_off[t[a]] + atomicAdd(&cursor[t[a]], 1)] = m;
+}
+
+// Stencil column of lattice column jx for a marker with origin ix0 (the
+// unwrapped index the reference uses in rx = x - ix); false if uncovered.
+__device__ __forceinline__ bool stencil_ix(int jx, int ix0, int nx, int& ix) {
+    int d = jx - ix0;
+    if (d >= -1 && d <= 2) { ix = jx; return true; }
+    d = jx - nx - ix0;
+    if (d >= -1 && d <= 2) { ix = jx - nx; return true; }
+    d = jx + nx - ix0;
+    if (d >= -1 && d <= 2) { ix = jx + nx; return true; }
+    return false;
+}
+
+constexpr int SPREAD_THREADS = TILE_CELLS;  // one thread per tile cell
+constexpr int SPREAD_LIST_CAP = 4096;       // markers per tile list
+constexpr int SPREAD_CHUNK = 256;
+
+// Deterministic spread into force tiles for MDF sweep `sweep`.  Sweep 0
+// spreads the membrane + contact forces (immersed_boundary.cpp:25-100);
+// sweep k >= 1 adds the corrections dF (:231-286).  On a channel's last
+// sweep the kernel also adds the body force on FLUID cells, applies the force
+// cap and counts capped cells (simulation.cpp:540-609), writing the final
+// tile force `fin` (real type R).
+template <typename R>
+__global__ void __launch_bounds__(SPREAD_THREADS)
+k_spread(const ChannelDev* __restrict__ chans, const int* __restrict__ tile_chan,
+         const int* __restrict__ n_slots_p, const int* __restrict__ slot_tile,
+         const int* __restrict__ tile_cnt, const int* __restrict__ list_off,
+         const int* __restrict__ list, MarkerBufs mb, const double* __restrict__ phi_tbl,
+         double* __restrict__ acc, R* __restrict__ gsnap, R* __restrict__ fin, int sweep,
+         int* __restrict__ capped, int* __restrict__ fluid_touched, unsigned* status) {
+    __shared__ int s_list[SPREAD_LIST_CAP];
+    __shared__ double s_x[SPREAD_CHUNK], s_y[SPREAD_CHUNK], s_fx[SPREAD_CHUNK], s_fy[SPREAD_CHUNK],
+        s_ds[SPREAD_CHUNK];
+    __shared__ int s_ix0[SPREAD_CHUNK], s_iy0[SPREAD_CHUNK], s_ok[SPREAD_CHUNK];
+    __shared__ double s_tbl[1025];
+    __shared__ int s_red[2];
+    for (int i = threadIdx.x; i < 1025; i += blockDim.x) s_tbl[i] = phi_tbl[i];
+    const int n_slots = *n_slots_p;
+    const int tid = threadIdx.x;
+    const int lx = tid % TILE_W, ly = tid / TILE_W;
+    for (int slot = blockIdx.x; slot < n_slots; slot += gridDim.x) {
+        const int t = slot_tile[slot];
+        const ChannelDev& ch = chans[tile_chan[t]];
+        const int K = ch.ibm_iterations > 1 ? ch.ibm_iterations : 1;
+        if (sweep >= K) continue;  // CTA-uniform
+        const int local = t - ch.tile_base;
+        const int ty = local / ch.tiles_x, tx = local % ch.tiles_x;
+        const int jx = tx * TILE_W + lx, jy = ty * TILE_H + ly;
+        const bool active = jx < ch.nx && jy < ch.ny;
+        int cnt = tile_cnt[t];
+        if (cnt > SPREAD_LIST_CAP) {
+            if (tid == 0) atomicOr(status, (unsigned)ST_LIST_OVERFLOW);
+            cnt = SPREAD_LIST_CAP;
+        }
+        int pow2 = 1;
+        while (pow2 < cnt) pow2 <<= 1;
+        __syncthreads();
+        for (int i = tid; i < pow2; i += blockDim.x)
+            s_list[i] = (i < cnt) ? list[list_off[t] + i] : INT_MAX;
+        __syncthreads();
+        // bitonic sort: ascending marker index = the reference's loop order
+        for (int k = 2; k <= pow2; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = tid; i < pow2; i += blockDim.x) {
+                    const int l = i ^ j;
+                    if (l > i) {
+                        const int a = s_list[i], b = s_list[l];
+                        const bool up = (i & k) == 0;
+                        if ((a > b) == up) { s_list[i] = b; s_list[l] = a; }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        const size_t cell = (size_t)slot * 2 * TILE_CELLS + tid;
+        double ax = 0.0, ay = 0.0;
+        if (sweep > 0) {
+            ax = acc[cell];
+            ay = acc[cell + TILE_CELLS];
+        }
+        const bool last = (sweep == K - 1);
+        if (last && K > 1) {
+            gsnap[cell] = (R)ax;
+            gsnap[cell + TILE_CELLS] = (R)ay;
+        }
+        for (int c0 = 0; c0 < cnt; c0 += SPREAD_CHUNK) {
+            const int nc = min(SPREAD_CHUNK, cnt - c0);
+            __syncthreads();
+            if (tid < nc) {
+                const int m = s_list[c0 + tid];
+                const double2 p = mb.pos[m];
+                const double2 f = sweep == 0 ? mb.frc[m] : mb.dF[m];
+                s_x[tid] = p.x;
+                s_y[tid] = p.y;
+                s_fx[tid] = f.x;
+                s_fy[tid] = f.y;
+                s_ds[tid] = mb.ds[m];
+                s_ix0[tid] = mb.ix0[m];
+                s_iy0[tid] = mb.iy0[m];
+                s_ok[tid] = !(isnan(f.x) || isnan(f.y));
+            }
+            __syncthreads();
+            if (active) {
+                for (int i = 0; i < nc; ++i) {
+                    if (!s_ok[i]) continue;
+                    const int dyc = jy - s_iy0[i];
+                    if (dyc < -1 || dyc > 2) continue;
+                    int ix;
+                    if (!stencil_ix(jx, s_ix0[i], ch.nx, ix)) continue;
+                    const double rx = s_x[i] - (double)ix, ry = s_y[i] - (double)jy;
+                    const double w = phi_lut(s_tbl, rx) * phi_lut(s_tbl, ry);
+                    if (w > 1e-15) {
+                        ax += s_fx[i] * w * s_ds[i];
+                        ay += s_fy[i] * w * s_ds[i];
+                    }
+                }
+            }
+        }
+        if (!last) {
+            acc[cell] = ax;
+            acc[cell + TILE_CELLS] = ay;
+            continue;
+        }
+        // finalize: body force on FLUID cells, then the force cap
+        if (tid == 0) { s_red[0] = 0; s_red[1] = 0; }
+        __syncthreads();
+        if (active) {
+            const bool fluid = ch.periodic_y || (jy != 0 && jy != ch.ny - 1);
+            if (fluid && (ch.body_fx != 0.0 || ch.body_fy != 0.0)) {
+                ax += ch.body_fx;
+                ay += ch.body_fy;
+            }
+            const double Fm = ch.max_force, Fm2 = Fm * Fm;
+            const double f2 = ax * ax + ay * ay;
+            int cap_here = 0;
+            if (f2 > Fm2) {
+                const double sc = Fm / sqrt(f2);
+                ax *= sc;
+                ay *= sc;
+                cap_here = 1;
+            }
+            if (cap_here) atomicAdd(&s_red[0], 1);
+            if (fluid) atomicAdd(&s_red[1], 1);
+        }
+        acc[cell] = ax;
+        acc[cell + TILE_CELLS] = ay;
+        fin[cell] = (R)ax;
+        fin[cell + TILE_CELLS] = (R)ay;
+        __syncthreads();
+        if (tid == 0) {
+            if (s_red[0]) atomicAdd(&capped[tile_chan[t]], s_red[0]);
+            if (s_red[1]) atomicAdd(&fluid_touched[tile_chan[t]], s_red[1]);
+        }
+    }
+}
+
+// Lattice velocity at a cell for interpolation: moments of the populations
+// plus half the given force, zero on SOLID wall rows (lattice_field.cpp:28-73).
+template <typename S, typename R>
+__device__ __forceinline__ void cell_rho_j(const ChannelDev& ch, const S* __restrict__ f, int jx,
+                                           int jy, double& rho, double& jxo, double& jyo,
+                                           bool& solid) {
+    solid = !ch.periodic_y && (jy == 0 || jy == ch.ny - 1);
+    if (solid) { rho = 0.0; jxo = 0.0; jyo = 0.0; return; }
+    const long long n = (long long)jy * ch.pitch + jx;
+    R v[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) v[q] = PopIO<S, R>::load(f + ch.f_off + q * ch.plane + n, q);
+    R r, a, b;
+    cell_moments(v, r, a, b);
+    rho = (double)r;
+    jxo = (double)a;
+    jyo = (double)b;
+}
+
+__device__ __forceinline__ size_t tile_cell_index(const ChannelDev& ch, const int* tile_slot,
+                                                  int jx, int jy) {
+    const int t = ch.tile_base + (jy / TILE_H) * ch.tiles_x + (jx / TILE_W);
+    const int s = tile_slot[t];
+    return (size_t)s * 2 * TILE_CELLS + (jy % TILE_H) * TILE_W + (jx % TILE_W);
+}
+
+// MDF correction of one sweep (immersed_boundary.cpp:355-394): interpolate
+// u = (j + F/2)/rho with the force spread so far, then
+// dF = 2 rho(nearest node) (U_prev - U_interp).
+template <typename S, typename R>
+__global__ void k_mdf_interp(const ChannelDev* __restrict__ chans, int M, MarkerBufs mb,
+                             const S* __restrict__ f, const int* __restrict__ tile_slot,
+                             const double* __restrict__ acc, const double* __restrict__ phi_tbl,
+                             int sweep) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    const ChannelDev& ch = chans[mb.mk_chan[m]];
+    if (sweep >= ch.ibm_iterations || !mb.valid[m]) return;
+    const double2 p = mb.pos[m];
+    const int ix0 = mb.ix0[m], iy0 = mb.iy0[m];
+    double ux = 0.0, uy = 0.0;
+    for (int iy = iy0 - 1; iy <= iy0 + 2; ++iy) {
+        for (int ix = ix0 - 1; ix <= ix0 + 2; ++ix) {
+            int jx = ix;
+            if (jx < 0) jx += ch.nx;
+            if (jx >= ch.nx) jx -= ch.nx;
+            const int jy = iy;
+            if (jy < 0 || jy >= ch.ny || jx < 0 || jx >= ch.nx) continue;
+            const double w = phi_lut(phi_tbl, p.x - (double)ix) * phi_lut(phi_tbl, p.y - (double)iy);
+            if (w > 1e-15) {
+                double rho, jxm, jym;
+                bool solid;
+                cell_rho_j<S, R>(ch, f, jx, jy, rho, jxm, jym, solid);
+                double cu = 0.0, cv = 0.0;
+                if (!solid && rho > 1e-15) {
+                    const size_t ci = tile_cell_index(ch, tile_slot, jx, jy);
+                    cu = (jxm + 0.5 * acc[ci]) / rho;
+                    cv = (jym + 0.5 * acc[ci + TILE_CELLS]) / rho;
+                }
+                ux += cu * w;
+                uy += cv * w;
+            }
+        }
+    }
+    double rho_local = 1.0;
+    int ixr = (int)(p.x + 0.5), iyr = (int)(p.y + 0.5);
+    if (ixr < 0) ixr += ch.nx;
+    if (ixr >= ch.nx) ixr -= ch.nx;
+    if (iyr >= 0 && iyr < ch.ny && ixr >= 0 && ixr < ch.nx) {
+        double jxm, jym;
+        bool solid;
+        cell_rho_j<S, R>(ch, f, ixr, iyr, rho_local, jxm, jym, solid);
+    }
+    const double2 v = mb.vel[m];
+    const double dux = v.x - ux, duy = v.y - uy;
+    mb.dF[m] = make_double2(dux * (2.0 * rho_local), duy * (2.0 * rho_local));
+}
+
+// Interpolate the new velocity and move the markers (simulation.cpp:656-675,
+// capsule.cpp:267-297).
+template <typename S, typename R>
+__global__ void k_interp_move(const ChannelDev* __restrict__ chans, int M, MarkerBufs mb,
+                              const S* __restrict__ f, const int* __restrict__ tile_slot,
+                              const R* __restrict__ fin, const double* __restrict__ phi_tbl) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    const ChannelDev& ch = chans[mb.mk_chan[m]];
+    double2 p = mb.pos[m];
+    double ux = 0.0, uy = 0.0;
+    if (mb.valid[m]) {
+        const int ix0 = mb.ix0[m], iy0 = mb.iy0[m];
+        for (int iy = iy0 - 1; iy <= iy0 + 2; ++iy) {
+            for (int ix = ix0 - 1; ix <= ix0 + 2; ++ix) {
+                int jx = ix;
+                if (jx < 0) jx += ch.nx;
+                if (jx >= ch.nx) jx -= ch.nx;
+                const int jy = iy;
+                if (jy < 0 || jy >= ch.ny || jx < 0 || jx >= ch.nx) continue;
+                const double w =
+                    phi_lut(phi_tbl, p.x - (double)ix) * phi_lut(phi_tbl, p.y - (double)iy);
+                if (w > 1e-15) {
+                    double rho, jxm, jym;
+                    bool solid;
+                    cell_rho_j<S, R>(ch, f, jx, jy, rho, jxm, jym, solid);
+                    double cu = 0.0, cv = 0.0;
+                    if (!solid && rho > 1e-15) {
+                        const size_t ci = tile_cell_index(ch, tile_slot, jx, jy);
+                        cu = (jxm + 0.5 * (double)fin[ci]) / rho;
+                        cv = (jym + 0.5 * (double)fin[ci + TILE_CELLS]) / rho;
+                    }
+                    ux += cu * w;
+                    uy += cv * w;
+                }
+            }
+        }
+    }
+    mb.vel[m] = make_double2(ux, uy);
+    p.x = p.x + ux * ch.dt;
+    p.y = p.y + uy * ch.dt;
+    const double Lx = (double)ch.nx;
+    if (isfinite(p.x)) {
+        // the reference wraps with while-loops (capsule.cpp:287-296); moves
+        // are far below one period, so a bounded loop gives the same result
+        int it = 0;
+        while (p.x < 0.0 && it < 8) { p.x += Lx; ++it; }
+        while (p.x >= Lx && it < 16) { p.x -= Lx; ++it; }
+        if (p.x < 0.0 || p.x >= Lx) {
+            p.x = fmod(p.x, Lx);
+            if (p.x < 0.0) p.x += Lx;
+        }
+    }
+    if (!ch.periodic_y) {
+        const double ymin = 1.5, ymax = (double)ch.ny - 1.5;
+        if (p.y < ymin) p.y = ymin;
+        if (p.y > ymax) p.y = ymax;
+    }
+    mb.pos[m] = p;
+}
+
+// ============================ launch wrappers ==============================
+
+size_t membrane_smem_bytes(int maxn) {
+    return (size_t)MEM_WARPS * MEM_DOUBLES_PER_NODE * maxn * sizeof(double);
+}
+
+cudaError_t prepare_membrane(int maxn) {
+    const size_t smem = membrane_smem_bytes(maxn);
+    if (smem <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(k_membrane, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem);
+}
+
+void launch_membrane(const CapsuleDev* caps, int ncaps, const MarkerBufs& mb, int* has_prev,
+                     int maxn, unsigned* status, cudaStream_t st) {
+    if (ncaps == 0) return;
+    const size_t smem = membrane_smem_bytes(maxn);
+    const int blocks = (ncaps + MEM_WARPS - 1) / MEM_WARPS;
+    k_membrane<<<blocks, MEM_WARPS * 32, smem, st>>>(caps, ncaps, mb, has_prev, maxn, status);
+}
+
+void launch_contact(const ChannelDev* chans, int M, const MarkerBufs& mb, ContactBufs& cb,
+                    int ncells, cudaStream_t st) {
+    if (M == 0) return;
+    const int B = 256, G = (M + B - 1) / B;
+    if (ncells > 0) {
+        cudaMemsetAsync(cb.cell_cnt, 0, sizeof(int) * ncells, st);
+        cudaMemsetAsync(cb.cursor, 0, sizeof(int) * ncells, st);
+        k_contact_bin<<<G, B, 0, st>>>(chans, M, mb, cb.cell_of, cb.cell_cnt);
+        scan_exclusive(cb.cell_cnt, cb.cell_start, ncells, cb.scan_tmp, nullptr, st);
+        k_contact_fill<<<G, B, 0, st>>>(chans, M, mb, cb.cell_of, cb.cell_start, cb.cursor,
+                                        cb.list);
+        k_contact_sort<<<(ncells + B - 1) / B, B, 0, st>>>(ncells, cb.cell_start, cb.cell_cnt,
+                                                           cb.list);
+    }
+    k_contact_force<<<G, B, 0, st>>>(chans, M, mb, cb.cell_of, cb.cell_start, cb.cell_cnt,
+                                     cb.list);
+}
+
+void launch_tiles(const ChannelDev* chans, const CapsuleDev* caps, int M, const MarkerBufs& mb,
+                  TileBufs& tb, int T, int parity, unsigned* status, cudaStream_t st) {
+    const int B = 256, G = (M + B - 1) / B;
+    cudaMemsetAsync(tb.tile_flag, 0, sizeof(int) * T, st);
+    cudaMemsetAsync(tb.tile_cnt, 0, sizeof(int) * T, st);
+    cudaMemsetAsync(tb.cursor, 0, sizeof(int) * T, st);
+    k_ibm_prep<<<G, B, 0, st>>>(chans, caps, M, mb, tb.tile_flag, tb.tile_cnt, status);
+    scan_exclusive(tb.tile_flag, tb.slot_scan, T, tb.scan_tmp, tb.n_slots, st);
+    scan_exclusive(tb.tile_cnt, tb.list_off, T, tb.scan_tmp, nullptr, st);
+    k_tile_slots<<<(T + B - 1) / B, B, 0, st>>>(T, tb.tile_flag, tb.slot_scan,
+                                                tb.tile_slot[parity], tb.slot_tile);
+    k_tile_fill<<<G, B, 0, st>>>(chans, M, mb, tb.list_off, tb.cursor, tb.list);
+}
+
+template <typename R>
+void launch_spread(const ChannelDev* chans, const MarkerBufs& mb, TileBufs& tb, int parity,
+                   const double* phi_tbl, int sweep, int grid, unsigned* status, cudaStream_t st) {
+    k_spread<R><<<grid, SPREAD_THREADS, 0, st>>>(
+        chans, tb.tile_chan, tb.n_slots, tb.slot_tile, tb.tile_cnt, tb.list_off, tb.list, mb,
+        phi_tbl, tb.acc, static_cast<R*>(tb.gsnap), static_cast<R*>(tb.fin[parity]), sweep,
+        tb.capped, tb.fluid_touched, status);
+}
+template void launch_spread<double>(const ChannelDev*, const MarkerBufs&, TileBufs&, int,
+                                    const double*, int, int, unsigned*, cudaStream_t);
+template void launch_spread<float>(const ChannelDev*, const MarkerBufs&, TileBufs&, int,
+                                   const double*, int, int, unsigned*, cudaStream_t);
+
+template <typename S, typename R>
+void launch_mdf_interp(const ChannelDev* chans, int M, const MarkerBufs& mb, const S* f,
+                       TileBufs& tb, int parity, const double* phi_tbl, int sweep,
+                       cudaStream_t st) {
+    const int B = 128, G = (M + B - 1) / B;
+    k_mdf_interp<S, R><<<G, B, 0, st>>>(chans, M, mb, f, tb.tile_slot[parity], tb.acc, phi_tbl,
+                                        sweep);
+}
+
+template <typename S, typename R>
+void launch_interp_move(const ChannelDev* chans, int M, const MarkerBufs& mb, const S* f,
+                        TileBufs& tb, int parity, const double* phi_tbl, cudaStream_t st) {
+    const int B = 128, G = (M + B - 1) / B;
+    k_interp_move<S, R><<<G, B, 0, st>>>(chans, M, mb, f, tb.tile_slot[parity],
+                                         static_cast<const R*>(tb.fin[parity]), phi_tbl);
+}
+
+#define SFG_INST(S, R)                                                                          \
+    template void launch_mdf_interp<S, R>(const ChannelDev*, int, const MarkerBufs&, const S*,  \
+                                          TileBufs&, int, const double*, int, cudaStream_t);    \
+    template void launch_interp_move<S, R>(const ChannelDev*, int, const MarkerBufs&, const S*, \
+                                           TileBufs&, int, const double*, cudaStream_t);
+SFG_INST(double, double)
+SFG_INST(float, float)
+SFG_INST(__half, float)
+#undef SFG_INST
+
+}  // namespace sfg

@@ -1,0 +1,98 @@
+// sfg_internal.h -- device buffer bundles and launch wrappers shared by the
+// translation units of libsoftflow_b200.so (not part of the C ABI).
+#pragma once
+#include "common.cuh"
+#include "markers.cuh"
+
+namespace sfg {
+
+struct ContactBufs {
+    int* cell_of = nullptr;     // [M] global contact cell of each marker
+    int* cell_cnt = nullptr;    // [ncells]
+    int* cell_start = nullptr;  // [ncells]
+    int* cursor = nullptr;      // [ncells]
+    int* list = nullptr;        // [M]
+    int* scan_tmp = nullptr;
+};
+
+struct TileBufs {
+    int T = 0;                  // force tiles over all channels
+    int max_slots = 0;
+    int* tile_chan = nullptr;   // [T]
+    int* tile_flag = nullptr;   // [T]
+    int* tile_cnt = nullptr;    // [T] markers whose stencil covers the tile
+    int* cursor = nullptr;      // [T]
+    int* slot_scan = nullptr;   // [T]
+    int* list_off = nullptr;    // [T]
+    int* tile_slot[2] = {nullptr, nullptr};  // [T] per step parity
+    int* slot_tile = nullptr;   // [max_slots]
+    int* n_slots = nullptr;     // [1]
+    int* list = nullptr;        // [8 M]
+    int* scan_tmp = nullptr;
+    double* acc = nullptr;      // [max_slots][2][TILE_CELLS]
+    void* gsnap = nullptr;      // [max_slots][2][TILE_CELLS] (R)
+    void* fin[2] = {nullptr, nullptr};
+    int* capped = nullptr;      // [nchan]
+    int* fluid_touched = nullptr;
+};
+
+// Exclusive prefix sum of n ints (three kernels, graph-capturable);
+// `total` (device int, may be null) receives the sum.
+void scan_exclusive(const int* in, int* out, int n, int* tmp, int* total, cudaStream_t st);
+size_t scan_tmp_ints(int n);
+
+// Capsules of up to maxn nodes; > 48 KB of shared memory needs opting in.
+size_t membrane_smem_bytes(int maxn);
+cudaError_t prepare_membrane(int maxn);
+void launch_membrane(const CapsuleDev* caps, int ncaps, const MarkerBufs& mb, int* has_prev,
+                     int maxn, unsigned* status, cudaStream_t st);
+void launch_contact(const ChannelDev* chans, int M, const MarkerBufs& mb, ContactBufs& cb,
+                    int ncells, cudaStream_t st);
+void launch_tiles(const ChannelDev* chans, const CapsuleDev* caps, int M, const MarkerBufs& mb,
+                  TileBufs& tb, int T, int parity, unsigned* status, cudaStream_t st);
+template <typename R>
+void launch_spread(const ChannelDev* chans, const MarkerBufs& mb, TileBufs& tb, int parity,
+                   const double* phi_tbl, int sweep, int grid, unsigned* status, cudaStream_t st);
+template <typename S, typename R>
+void launch_mdf_interp(const ChannelDev* chans, int M, const MarkerBufs& mb, const S* f,
+                       TileBufs& tb, int parity, const double* phi_tbl, int sweep, cudaStream_t st);
+template <typename S, typename R>
+void launch_interp_move(const ChannelDev* chans, int M, const MarkerBufs& mb, const S* f,
+                        TileBufs& tb, int parity, const double* phi_tbl, cudaStream_t st);
+
+// Lattice kernels (lattice_f64.cu / lattice_f32.cu).
+struct LatticeLaunch {
+    const RowItem* items;
+    int n_items;
+    const ChannelDev* chans;
+    const void* src;
+    void* dst;
+    const void* gsrc;
+    void* gdst;
+    const void* cfield;
+    const int* stepped;
+    const int* adr_pending;
+    const int* c_fresh;
+    bool any_adr;
+};
+struct TileViewArgs {
+    const int* cur_slot;
+    const int* prev_slot;
+    const void* cur_fin;
+    const void* cur_G;
+    const void* prev_fin;
+};
+template <typename S, typename R>
+void launch_lattice_step(const LatticeLaunch& L, const TileViewArgs& tv, cudaStream_t st);
+template <typename S, typename R>
+void launch_scalar_flush(const LatticeLaunch& L, const TileViewArgs& tv_last, cudaStream_t st);
+template <typename S, typename R>
+void launch_pop_import(const double* in, void* out, const ChannelDev& ch, cudaStream_t st);
+template <typename S, typename R>
+void launch_pop_export(const void* in, double* out, const ChannelDev& ch, cudaStream_t st);
+template <typename S, typename R>
+void launch_macro_export(const void* in, const ChannelDev& ch, const TileViewArgs& tv_last,
+                         int stepped, double* rho, double* ux, double* uy, double* Fx, double* Fy,
+                         cudaStream_t st);
+
+}  // namespace sfg

@@ -1,0 +1,681 @@
+"""Host mirror of the reference engine API on top of the C ABI.
+
+Names, argument meanings and defaults follow the reference's pybind11
+module ``softflow_core`` (python/bindings.cpp:128-307 for the parameter
+structs, :846-981 for ``Simulation``), so a script written against the
+reference's core API runs here unchanged for the hot-path features:
+
+    p = SimulationParams(); p.nx, p.ny = 400, 80
+    p.fluid.boundary_type = BoundaryType.PERIODIC
+    p.fluid.collision_model = CollisionModel.REGULARIZED
+    sim = Simulation(p)
+    sim.addCapsuleRandom(30, 20, 10, 380, 70, 3, 3, 24, mp, seed=42)
+    sim.initialize(); sim.run(1000)
+    ux = sim.field().velocity_x()
+
+``Ensemble`` runs many independent channels in one device context: every
+step is one launch per kernel phase over all channels.
+
+All numerical work of a step runs in libsoftflow_b200.so on the GPU.  The
+host side only builds rest geometry at setup and moves data on request.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib as L
+
+PI = 3.14159265358979323846
+
+
+class CollisionModel(enum.IntEnum):
+    BGK = 0
+    MRT = 1
+    REGULARIZED = 2
+
+
+class MembraneModel(enum.IntEnum):
+    HOOKEAN = 0
+    NEO_HOOKEAN = 1
+    SKALAK = 2
+    WLC = 3
+
+
+class BoundaryType(enum.IntEnum):
+    INLET_OUTLET = 0
+    PERIODIC = 1
+    CLOSED = 2
+
+
+class CapsuleShape(enum.IntEnum):
+    CIRCLE = 0
+    ELLIPSE = 1
+    BICONCAVE = 2
+    FIBER = 3
+
+
+@dataclass
+class FluidParams:
+    """Reference FluidParams (parameters.h:41-79), hot-path fields."""
+    tau: float = 0.8
+    rho0: float = 1.0
+    boundary_type: BoundaryType = BoundaryType.INLET_OUTLET
+    body_force_x: float = 0.0
+    body_force_y: float = 0.0
+    collision_model: CollisionModel = CollisionModel.BGK
+    use_mrt: bool = False
+    mrt_se: float = 1.4
+    mrt_s_eps: float = 1.4
+    mrt_sq: float = 1.4
+    periodic_y: bool = False
+
+
+@dataclass
+class MembraneParams:
+    """Reference MembraneParams (parameters.h:82-136)."""
+    model: MembraneModel = MembraneModel.HOOKEAN
+    k_stretch: float = 0.1
+    G_s: float = 0.1
+    C_skalak: float = 1.0
+    wlc_L_max_ratio: float = 2.2
+    wlc_kBT_p: float = 0.0
+    wlc_k_pow: float = 0.0
+    k_bend: float = 0.005
+    use_helfrich_bending: bool = False
+    kappa_0: float = 0.0
+    k_area: float = 0.5
+    k_perimeter: float = 0.1
+    gamma_visc: float = 0.01
+    eta_membrane: float = 0.05
+    shape: CapsuleShape = CapsuleShape.CIRCLE
+    is_rigid: bool = False
+    density: float = 1.0
+
+    def to_c(self) -> L.MembraneParamsC:
+        if self.shape != CapsuleShape.CIRCLE:
+            raise NotImplementedError("only circular rest shapes are on this path")
+        if self.is_rigid:
+            raise NotImplementedError("rigid capsules are not on this path")
+        return L.MembraneParamsC(
+            model=int(self.model), k_stretch=self.k_stretch, G_s=self.G_s,
+            C_skalak=self.C_skalak, wlc_L_max_ratio=self.wlc_L_max_ratio,
+            wlc_kBT_p=self.wlc_kBT_p, wlc_k_pow=self.wlc_k_pow, k_bend=self.k_bend,
+            use_helfrich=int(bool(self.use_helfrich_bending)), kappa_0=self.kappa_0,
+            k_area=self.k_area, k_perimeter=self.k_perimeter, gamma_visc=self.gamma_visc,
+            eta_membrane=self.eta_membrane)
+
+
+@dataclass
+class RepulsionParams:
+    """Reference RepulsionParams (parameters.h:138-161)."""
+    epsilon: float = 0.05
+    sigma: float = 1.0
+    r_cut: float = 3.5
+    power: int = 4
+    damping_normal: float = 0.0
+    friction_coeff: float = 0.0
+
+
+@dataclass
+class ScalarParams:
+    """Reference ScalarParams (parameters.h:177-205), one species."""
+    enabled: bool = False
+    n_species: int = 1
+    diffusivity: List[float] = field(default_factory=lambda: [0.01])
+    inlet_concentration: List[float] = field(default_factory=lambda: [0.0])
+    periodic_y: bool = False
+
+
+@dataclass
+class SimulationParams:
+    """Reference SimulationParams (parameters.h:279-342), hot-path fields,
+    plus the device options ``precision`` ("fp64" | "fp32" | "fp16s") and
+    ``device``."""
+    nx: int = 200
+    ny: int = 50
+    dt: float = 1.0
+    ibm_iterations: int = 1
+    max_lattice_force: float = 0.01
+    fluid: FluidParams = field(default_factory=FluidParams)
+    membrane: MembraneParams = field(default_factory=MembraneParams)
+    repulsion: RepulsionParams = field(default_factory=RepulsionParams)
+    scalar: ScalarParams = field(default_factory=ScalarParams)
+    precision: str = "fp32"
+    device: int = 0
+
+    def kinematicViscosity(self) -> float:
+        return (self.fluid.tau - 0.5) / 3.0
+
+    def to_c(self) -> L.ChannelParamsC:
+        f = self.fluid
+        if f.boundary_type != BoundaryType.PERIODIC:
+            raise NotImplementedError(
+                "only BoundaryType.PERIODIC channels are on this path (Zou-He inlet/outlet "
+                "and closed boxes are not implemented)")
+        coll = CollisionModel.MRT if f.use_mrt else CollisionModel(f.collision_model)
+        if self.scalar.enabled and self.scalar.n_species != 1:
+            raise NotImplementedError("one scalar species is supported")
+        return L.ChannelParamsC(
+            nx=self.nx, ny=self.ny, collision=int(coll), tau=f.tau, rho0=f.rho0,
+            mrt_se=f.mrt_se, mrt_s_eps=f.mrt_s_eps, mrt_sq=f.mrt_sq,
+            body_fx=f.body_force_x, body_fy=f.body_force_y, periodic_y=int(bool(f.periodic_y)),
+            max_lattice_force=self.max_lattice_force, ibm_iterations=self.ibm_iterations,
+            dt=self.dt, rep_epsilon=self.repulsion.epsilon, rep_sigma=self.repulsion.sigma,
+            rep_r_cut=self.repulsion.r_cut, rep_power=self.repulsion.power,
+            rep_damping_normal=self.repulsion.damping_normal,
+            rep_friction=self.repulsion.friction_coeff,
+            scalar_enabled=int(bool(self.scalar.enabled)),
+            scalar_D=(self.scalar.diffusivity[0] if self.scalar.diffusivity else 0.01),
+            scalar_periodic_y=int(bool(self.scalar.periodic_y)),
+            scalar_inlet=(self.scalar.inlet_concentration[0]
+                          if self.scalar.inlet_concentration else 0.0))
+
+
+@dataclass
+class _CapsuleRec:
+    mp: MembraneParams
+    rest: L.CapsuleRestC
+    pos: np.ndarray
+    rest_len: np.ndarray
+    rest_ang: np.ndarray
+    rest_ds: np.ndarray
+    type_id: int
+
+
+def build_circle_capsule(center, radius: float, num_nodes: int, mp: MembraneParams):
+    """Rest geometry of a circular capsule (reference capsule.cpp:7-141)."""
+    lib = L.lib()
+    mpc = mp.to_c()
+    rest = L.CapsuleRestC()
+    L.check(lib.sfg_build_circle_capsule(float(center[0]), float(center[1]), float(radius),
+                                         int(num_nodes), C.byref(mpc), C.byref(rest),
+                                         None, None, None, None, 0))
+    n = rest.num_nodes
+    pos = np.zeros(2 * n)
+    rl, ra, rd = np.zeros(n), np.zeros(n), np.zeros(n)
+    L.check(lib.sfg_build_circle_capsule(float(center[0]), float(center[1]), float(radius),
+                                         int(num_nodes), C.byref(mpc), C.byref(rest),
+                                         L.dptr(pos), L.dptr(rl), L.dptr(ra), L.dptr(rd), n))
+    return rest, pos, rl, ra, rd
+
+
+def _centroid_periodic(pos: np.ndarray, nx: int):
+    """Capsule::centroid with minimum image (capsule.cpp:159-173), evaluated
+    sequentially in IEEE double like the reference."""
+    p = pos.reshape(-1, 2)
+    Lx = float(nx)
+    rx, ry = float(p[0, 0]), float(p[0, 1])
+    sx, sy = rx, ry
+    for i in range(1, len(p)):
+        dx = float(p[i, 0]) - rx
+        dy = float(p[i, 1]) - ry
+        if dx > 0.5 * Lx:
+            dx -= Lx
+        if dx < -0.5 * Lx:
+            dx += Lx
+        sx = sx + (rx + dx)
+        sy = sy + (ry + dy)
+    n = float(len(p))
+    return sx / n, sy / n
+
+
+class _Channel:
+    def __init__(self, params: SimulationParams):
+        self.params = params
+        self.cparams = params.to_c()
+        self.caps: List[_CapsuleRec] = []
+        self.walls_in_placement = False
+
+    def add_capsule(self, center, radius, num_nodes=0, mparams=None, type_id=0):
+        mp = mparams if mparams is not None else self.params.membrane
+        rest, pos, rl, ra, rd = build_circle_capsule(center, radius, num_nodes, mp)
+        self.caps.append(_CapsuleRec(mp, rest, pos, rl, ra, rd, type_id))
+        return len(self.caps) - 1
+
+    def add_random(self, count, x0, y0, x1, y1, rmin, rmax, num_nodes, mparams, type_id, seed,
+                   min_gap, max_attempts, check_walls):
+        n_ex = len(self.caps)
+        cen = np.zeros(2 * max(n_ex, 1))
+        rad = np.zeros(max(n_ex, 1))
+        for i, c in enumerate(self.caps):
+            cx, cy = _centroid_periodic(c.pos, self.params.nx)
+            cen[2 * i], cen[2 * i + 1] = cx, cy
+            rad[i] = math.sqrt(c.rest.rest_area / PI)
+        out_c = np.zeros(2 * max(count, 1))
+        out_r = np.zeros(max(count, 1))
+        placed, attempts = C.c_int(0), C.c_int(0)
+        L.check(L.lib().sfg_place_random(
+            int(count), float(x0), float(y0), float(x1), float(y1), float(rmin), float(rmax),
+            int(num_nodes), int(seed), float(min_gap), int(max_attempts), int(bool(check_walls)),
+            int(self.params.nx), int(self.params.ny), n_ex, L.dptr(cen), L.dptr(rad),
+            int(count), L.dptr(out_c), L.dptr(out_r), C.byref(placed), C.byref(attempts)))
+        for i in range(placed.value):
+            self.add_capsule((out_c[2 * i], out_c[2 * i + 1]), out_r[i], num_nodes, mparams,
+                             type_id)
+        print(f"Placed {placed.value}/{count} capsules ({attempts.value} attempts)")
+        return placed.value
+
+
+class _Context:
+    """One device context holding one or more channels."""
+
+    def __init__(self, channels: Sequence[_Channel], precision: str, device: int):
+        if precision not in L.PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(L.PRECISIONS)}")
+        lib = L.lib()
+        self._lib = lib
+        self.precision = precision
+        h = C.c_void_p()
+        L.check(lib.sfg_create(int(device), L.PRECISIONS[precision], C.byref(h)))
+        self._h = h
+        try:
+            for ch in channels:
+                idx = C.c_int()
+                L.check(lib.sfg_add_channel(h, C.byref(ch.cparams), C.byref(idx)))
+                for rec in ch.caps:
+                    mpc = rec.mp.to_c()
+                    L.check(lib.sfg_add_capsule(h, idx.value, C.byref(mpc), C.byref(rec.rest),
+                                                L.dptr(rec.pos), L.dptr(rec.rest_len),
+                                                L.dptr(rec.rest_ang), L.dptr(rec.rest_ds), None))
+            L.check(lib.sfg_initialize(h))
+        except Exception:
+            lib.sfg_destroy(h)
+            self._h = None
+            raise
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.sfg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n: int):
+        L.check(self._lib.sfg_step(self._h, int(n)))
+
+    def synchronize(self) -> int:
+        st = C.c_uint(0)
+        L.check(self._lib.sfg_synchronize(self._h, C.byref(st)))
+        return st.value
+
+    def last_step_ms(self) -> float:
+        ms = C.c_float()
+        L.check(self._lib.sfg_last_step_ms(self._h, C.byref(ms)))
+        return ms.value
+
+    def launches_per_step(self) -> int:
+        v = C.c_int()
+        L.check(self._lib.sfg_launches_per_step(self._h, C.byref(v)))
+        return v.value
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        L.check(self._lib.sfg_get_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+
+class FieldView:
+    """Lattice field of one channel (reference LatticeField views,
+    bindings.cpp:313-383).  Arrays are copies taken at the call."""
+
+    def __init__(self, ctx: _Context, chan: int, nx: int, ny: int):
+        self._ctx, self._ch, self.nx, self.ny = ctx, chan, nx, ny
+
+    def getNx(self):
+        return self.nx
+
+    def getNy(self):
+        return self.ny
+
+    def size(self):
+        return self.nx * self.ny
+
+    def _macro(self):
+        N = self.nx * self.ny
+        out = [np.zeros(N) for _ in range(5)]
+        L.check(self._ctx._lib.sfg_get_macroscopic(self._ctx._h, self._ch,
+                                                   *[L.dptr(a) for a in out]))
+        return [a.reshape(self.ny, self.nx) for a in out]
+
+    def macroscopic(self):
+        """(rho, ux, uy, Fx, Fy), each [ny][nx]."""
+        return tuple(self._macro())
+
+    def density(self):
+        return self._macro()[0]
+
+    def velocity_x(self):
+        return self._macro()[1]
+
+    def velocity_y(self):
+        return self._macro()[2]
+
+    def force_x(self):
+        return self._macro()[3]
+
+    def force_y(self):
+        return self._macro()[4]
+
+    def distributions(self):
+        """Populations [9][ny][nx] (reference layout f[q*N + y*nx + x])."""
+        f = np.zeros(9 * self.nx * self.ny)
+        L.check(self._ctx._lib.sfg_get_populations(self._ctx._h, self._ch, L.dptr(f)))
+        return f.reshape(9, self.ny, self.nx)
+
+    def set_distributions(self, f: np.ndarray):
+        a = np.ascontiguousarray(f, dtype=np.float64).ravel()
+        if a.size != 9 * self.nx * self.ny:
+            raise ValueError("populations must have 9*ny*nx entries")
+        L.check(self._ctx._lib.sfg_set_populations(self._ctx._h, self._ch, L.dptr(a)))
+
+    def getRho(self, x, y):
+        return float(self.density()[y, x])
+
+    def getUx(self, x, y):
+        return float(self.velocity_x()[y, x])
+
+    def getUy(self, x, y):
+        return float(self.velocity_y()[y, x])
+
+
+class CapsuleView:
+    def __init__(self, system: "CapsuleSystemView", idx: int):
+        self._s, self._i = system, idx
+
+    def numNodes(self):
+        return self._s._counts[self._i]
+
+    def getTypeId(self):
+        return self._s._types[self._i]
+
+    getType = getTypeId
+
+    def _slice(self, arr):
+        o = self._s._offsets[self._i]
+        return arr[o:o + self.numNodes()]
+
+    def node_positions_array(self):
+        return self._slice(self._s.positions()).copy()
+
+    def nodePosition(self, k):
+        return tuple(self._slice(self._s.positions())[k])
+
+    def nodeVelocity(self, k):
+        return tuple(self._slice(self._s.velocities())[k])
+
+    def nodeForce(self, k):
+        return tuple(self._slice(self._s.forces())[k])
+
+    def centroid(self):
+        return _centroid_periodic(self.node_positions_array(), self._s._nx)
+
+    def area(self):
+        """|shoelace area| on min-image-unwrapped nodes (capsule.cpp:175-195)."""
+        p = self.node_positions_array()
+        Lx = float(self._s._nx)
+        uw = [(float(p[0, 0]), float(p[0, 1]))]
+        for i in range(1, len(p)):
+            dx = float(p[i, 0]) - float(p[i - 1, 0])
+            dy = float(p[i, 1]) - float(p[i - 1, 1])
+            if dx > 0.5 * Lx:
+                dx -= Lx
+            if dx < -0.5 * Lx:
+                dx += Lx
+            uw.append((uw[-1][0] + dx, uw[-1][1] + dy))
+        A = 0.0
+        for i in range(len(uw)):
+            a, b = uw[i], uw[(i + 1) % len(uw)]
+            A += a[0] * b[1] - a[1] * b[0]
+        return 0.5 * abs(A)
+
+    def perimeter(self):
+        p = self.node_positions_array()
+        Lx = float(self._s._nx)
+        P = 0.0
+        for i in range(len(p)):
+            j = (i + 1) % len(p)
+            dx = float(p[j, 0]) - float(p[i, 0])
+            dy = float(p[j, 1]) - float(p[i, 1])
+            if dx > 0.5 * Lx:
+                dx -= Lx
+            if dx < -0.5 * Lx:
+                dx += Lx
+            P += math.sqrt(dx * dx + dy * dy)
+        return P
+
+
+class CapsuleSystemView:
+    """Marker state of one channel (reference CapsuleSystem, capsule-major)."""
+
+    def __init__(self, ctx: _Context, chan: int, recs: List[_CapsuleRec], nx: int):
+        self._ctx, self._ch, self._nx = ctx, chan, nx
+        self._counts = [r.rest.num_nodes for r in recs]
+        self._types = [r.type_id for r in recs]
+        self._offsets = np.concatenate([[0], np.cumsum(self._counts)]).astype(int)
+        self.M = int(self._offsets[-1])
+
+    def numCapsules(self):
+        return len(self._counts)
+
+    def totalNodes(self):
+        return self.M
+
+    def __len__(self):
+        return self.numCapsules()
+
+    def __getitem__(self, i):
+        if i < 0 or i >= self.numCapsules():
+            raise IndexError("Capsule index out of range")
+        return CapsuleView(self, i)
+
+    def _get(self):
+        pos, vel, frc = np.zeros(2 * self.M), np.zeros(2 * self.M), np.zeros(2 * self.M)
+        if self.M:
+            L.check(self._ctx._lib.sfg_get_markers(self._ctx._h, self._ch, L.dptr(pos),
+                                                   L.dptr(vel), L.dptr(frc)))
+        return pos.reshape(-1, 2), vel.reshape(-1, 2), frc.reshape(-1, 2)
+
+    def positions(self):
+        return self._get()[0]
+
+    def velocities(self):
+        return self._get()[1]
+
+    def forces(self):
+        return self._get()[2]
+
+    def set_state(self, pos: Optional[np.ndarray] = None, vel: Optional[np.ndarray] = None):
+        p = None if pos is None else np.ascontiguousarray(pos, dtype=np.float64).ravel()
+        v = None if vel is None else np.ascontiguousarray(vel, dtype=np.float64).ravel()
+        L.check(self._ctx._lib.sfg_set_markers(self._ctx._h, self._ch, L.dptr(p), L.dptr(v)))
+
+    def contact_counts(self):
+        c = np.zeros(max(self.M, 1), dtype=np.int32)
+        L.check(self._ctx._lib.sfg_get_contact_counts(self._ctx._h, self._ch, L.iptr(c)))
+        return c[:self.M]
+
+
+class ScalarView:
+    """Advection-diffusion scalar of one channel (reference AdvectionDiffusion,
+    bindings.cpp:422-455)."""
+
+    def __init__(self, ctx: _Context, chan: int, nx: int, ny: int):
+        self._ctx, self._ch, self.nx, self.ny = ctx, chan, nx, ny
+
+    def concentration(self, species: int = 0):
+        Cf = np.zeros(self.nx * self.ny)
+        L.check(self._ctx._lib.sfg_get_concentration(self._ctx._h, self._ch, L.dptr(Cf), None))
+        return Cf.reshape(self.ny, self.nx)
+
+    def populations(self):
+        """Scalar populations [9][ny][nx]."""
+        Cf = np.zeros(self.nx * self.ny)
+        g = np.zeros(9 * self.nx * self.ny)
+        L.check(self._ctx._lib.sfg_get_concentration(self._ctx._h, self._ch, L.dptr(Cf),
+                                                     L.dptr(g)))
+        return g.reshape(9, self.ny, self.nx)
+
+    def setConcentration(self, Cfield: np.ndarray):
+        """Sets C and the equilibrium populations g = w C."""
+        a = np.ascontiguousarray(Cfield, dtype=np.float64).ravel()
+        if a.size != self.nx * self.ny:
+            raise ValueError("concentration must have ny*nx entries")
+        L.check(self._ctx._lib.sfg_set_concentration(self._ctx._h, self._ch, L.dptr(a)))
+
+    def setRegion(self, x0, y0, x1, y1, concentration, species=0):
+        Cf = self.concentration()
+        Cf[max(0, y0):min(self.ny, y1), max(0, x0):min(self.nx, x1)] = concentration
+        self.setConcentration(Cf)
+
+    def setPoint(self, x, y, concentration, species=0):
+        if 0 <= x < self.nx and 0 <= y < self.ny:
+            Cf = self.concentration()
+            Cf[y, x] = concentration
+            self.setConcentration(Cf)
+
+
+class Ensemble:
+    """Many independent channels advanced together on one GPU.
+
+    Build channels with ``add_channel(params)`` -> index, add capsules through
+    ``addCapsule`` / ``addCapsuleRandom`` with that index, then
+    ``initialize()`` and ``run(n)``.  Each channel's results equal the same
+    channel run alone.
+    """
+
+    def __init__(self, precision: str = "fp32", device: int = 0):
+        self.precision = precision
+        self.device = device
+        self._chans: List[_Channel] = []
+        self._ctx: Optional[_Context] = None
+        self._steps = 0
+
+    def add_channel(self, params: SimulationParams) -> int:
+        if self._ctx is not None:
+            raise RuntimeError("channels must be added before initialize()")
+        self._chans.append(_Channel(params))
+        return len(self._chans) - 1
+
+    def addCapsule(self, chan, center, radius, num_nodes=0, mparams=None, type=0):
+        self._pre_init()
+        return self._chans[chan].add_capsule(center, radius, num_nodes, mparams, type)
+
+    def addCapsuleRandom(self, chan, count, x0, y0, x1, y1, radius_min, radius_max,
+                         num_nodes=0, mparams=None, type=0, seed=12345, min_gap=1.0,
+                         max_attempts=0, check_walls=None):
+        self._pre_init()
+        ch = self._chans[chan]
+        cw = ch.walls_in_placement if check_walls is None else check_walls
+        return ch.add_random(count, x0, y0, x1, y1, radius_min, radius_max, num_nodes, mparams,
+                             type, seed, min_gap, max_attempts, cw)
+
+    def setChannelWalls(self, chan: int, enabled: bool = True):
+        """Apply the channel-builder wall test in random placement
+        (simulation.cpp:250-256), as the declarative Python API does."""
+        self._chans[chan].walls_in_placement = bool(enabled)
+
+    def _pre_init(self):
+        if self._ctx is not None:
+            raise RuntimeError("capsules must be added before initialize()")
+
+    def initialize(self):
+        if self._ctx is not None:
+            raise RuntimeError("already initialized")
+        self._ctx = _Context(self._chans, self.precision, self.device)
+        self._steps = 0
+
+    def _need(self):
+        if self._ctx is None:
+            raise RuntimeError("call initialize() first")
+        return self._ctx
+
+    def step(self):
+        self._need().step(1)
+        self._steps += 1
+
+    def run(self, num_steps: int):
+        ctx = self._need()
+        ctx.step(num_steps)
+        self._steps += int(num_steps)
+        ctx.synchronize()
+
+    def synchronize(self) -> int:
+        return self._need().synchronize()
+
+    def currentStep(self) -> int:
+        return self._steps
+
+    def num_channels(self) -> int:
+        return len(self._chans)
+
+    def field(self, chan: int = 0) -> FieldView:
+        p = self._chans[chan].params
+        return FieldView(self._need(), chan, p.nx, p.ny)
+
+    def capsules(self, chan: int = 0) -> CapsuleSystemView:
+        return CapsuleSystemView(self._need(), chan, self._chans[chan].caps,
+                                 self._chans[chan].params.nx)
+
+    def advectionDiffusion(self, chan: int = 0) -> Optional[ScalarView]:
+        p = self._chans[chan].params
+        if not p.scalar.enabled:
+            return None
+        return ScalarView(self._need(), chan, p.nx, p.ny)
+
+    def lastCappedNodes(self, chan: int = 0) -> int:
+        v = C.c_int()
+        L.check(self._need()._lib.sfg_get_capped_count(self._ctx._h, chan, C.byref(v)))
+        return v.value
+
+    def getMaxSpeed(self, chan: int = 0) -> float:
+        """max |u| over non-SOLID cells (simulation.cpp:892-907)."""
+        rho, ux, uy, _, _ = self.field(chan).macroscopic()
+        p = self._chans[chan].params
+        sp = ux * ux + uy * uy
+        if not p.fluid.periodic_y:
+            sp = sp[1:-1]
+        return float(math.sqrt(float(sp.max()))) if sp.size else 0.0
+
+    def context(self) -> _Context:
+        return self._need()
+
+    def close(self):
+        if self._ctx is not None:
+            self._ctx.close()
+            self._ctx = None
+
+
+class Simulation(Ensemble):
+    """Single-channel engine with the reference ``Simulation`` API
+    (bindings.cpp:846-981)."""
+
+    def __init__(self, params: SimulationParams):
+        super().__init__(params.precision, params.device)
+        self.add_channel(params)
+        self._params = params
+
+    def params(self) -> SimulationParams:
+        return self._params
+
+    def addCapsule(self, center, radius, num_nodes=0, mparams=None, type=0):
+        return super().addCapsule(0, center, radius, num_nodes, mparams, type)
+
+    def addCapsuleRandom(self, count, x0, y0, x1, y1, radius_min, radius_max, num_nodes=0,
+                         mparams=None, type=0, seed=12345, min_gap=1.0, max_attempts=0,
+                         check_walls=None):
+        return super().addCapsuleRandom(0, count, x0, y0, x1, y1, radius_min, radius_max,
+                                        num_nodes, mparams, type, seed, min_gap, max_attempts,
+                                        check_walls)
+
+    def setChannelWalls(self, enabled: bool = True):
+        super().setChannelWalls(0, enabled)

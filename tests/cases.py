@@ -1,0 +1,157 @@
+"""Shared test cases: the same channel set up on the CPU oracle and on the
+GPU library.  A case is a dict:
+
+    spec:     oracle.ChannelSpec keyword arguments
+    capsules: list of ("add", cx, cy, r, nn, membrane_kwargs)
+              or ("random", count, x0, y0, x1, y1, rmin, rmax, nn,
+                  membrane_kwargs, seed, min_gap, check_walls)
+    conc:     None or a function (nx, ny) -> initial concentration [ny][nx]
+"""
+from __future__ import annotations
+
+import numpy as np
+
+import oracle as O
+
+
+def gaussian_conc(cx, cy, sigma):
+    def f(nx, ny):
+        y, x = np.mgrid[0:ny, 0:nx]
+        return np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2.0 * sigma * sigma))
+    return f
+
+
+SKALAK_C1 = dict(model=O.SKALAK, G_s=0.06, C_skalak=10.0, k_bend=0.0)
+WLC_HELF = dict(model=O.WLC, G_s=0.06, use_helfrich=1, k_bend=0.01)
+
+CASES = {
+    # config 0 geometry (400 x 80 regularized channel, fx = 3e-5)
+    "c0": dict(spec=dict(nx=400, ny=80, collision=O.REGULARIZED, tau=0.8, body_fx=3e-5),
+               capsules=[], conc=None),
+    "bgk_small": dict(spec=dict(nx=64, ny=20, collision=O.BGK, tau=0.8, body_fx=3e-5),
+                      capsules=[], conc=None),
+    "mrt_small": dict(spec=dict(nx=64, ny=20, collision=O.MRT, tau=0.8, body_fx=3e-5),
+                      capsules=[], conc=None),
+    "reg_small": dict(spec=dict(nx=64, ny=20, collision=O.REGULARIZED, tau=1.2, body_fx=3e-5),
+                      capsules=[], conc=None),
+    # config 1: 30 Skalak capsules placed from seed 42, 5 MDF sweeps
+    "c1": dict(spec=dict(nx=400, ny=80, collision=O.REGULARIZED, tau=0.8, body_fx=3e-5,
+                         ibm_iterations=5),
+               capsules=[("random", 30, 20, 10, 380, 70, 3.0, 3.0, 24, SKALAK_C1, 42, 1.0, True)],
+               conc=None),
+    "c1_plain": dict(spec=dict(nx=400, ny=80, collision=O.REGULARIZED, tau=0.8, body_fx=3e-5,
+                               ibm_iterations=1),
+                     capsules=[("random", 30, 20, 10, 380, 70, 3.0, 3.0, 24, SKALAK_C1, 42,
+                                1.0, True)],
+                     conc=None),
+    # one capsule, no contact, across the periodic seam
+    "seam_single": dict(spec=dict(nx=64, ny=32, collision=O.BGK, tau=0.8, body_fx=2e-5,
+                                  ibm_iterations=3),
+                        capsules=[("add", 1.5, 15.3, 5.0, 32,
+                                   dict(model=O.NEO_HOOKEAN, G_s=0.05))],
+                        conc=None),
+    # config 2 in miniature: MRT, WLC + Helfrich and Skalak, scalar transport
+    "mini_c2": dict(spec=dict(nx=128, ny=64, collision=O.MRT, tau=0.8, body_fx=1e-5,
+                              scalar_enabled=1, scalar_D=0.05),
+                    capsules=[("random", 6, 0, 8, 128, 56, 6.0, 6.0, 48, WLC_HELF, 11, 1.0, True),
+                              ("random", 6, 0, 8, 128, 56, 3.0, 3.0, 24, SKALAK_C1, 12, 1.0, True)],
+                    conc=gaussian_conc(64.0, 31.5, 20.0)),
+    # two capsules in contact, fewer than 100 markers (all-pairs contact),
+    # with normal damping and Coulomb friction
+    "contact_brute": dict(spec=dict(nx=40, ny=40, collision=O.BGK, tau=0.8, body_fx=1e-5,
+                                    rep_damping_normal=0.1, rep_friction=0.2),
+                          capsules=[("add", 10.0, 20.0, 4.0, 0, dict(model=O.HOOKEAN)),
+                                    ("add", 19.5, 21.0, 4.0, 0, dict(model=O.NEO_HOOKEAN))],
+                          conc=None),
+    # pure diffusion (reference tests/verification/test_pure_diffusion.cpp)
+    "diffusion": dict(spec=dict(nx=256, ny=8, collision=O.BGK, tau=0.6, periodic_y=1,
+                                scalar_enabled=1, scalar_D=0.05, scalar_periodic_y=1),
+                      capsules=[], conc=None),
+}
+
+
+def build_oracle(case, impl="sfo"):
+    s = O.OracleSim(O.ChannelSpec(**case["spec"]), impl)
+    for c in case["capsules"]:
+        if c[0] == "add":
+            _, cx, cy, r, nn, mk = c
+            s.add_capsule(cx, cy, r, nn, O.Membrane(**mk))
+        else:
+            _, count, x0, y0, x1, y1, rmin, rmax, nn, mk, seed, gap, walls = c
+            s.add_capsule_random(count, x0, y0, x1, y1, rmin, rmax, nn, O.Membrane(**mk),
+                                 seed=seed, min_gap=gap, check_walls=walls)
+    s.initialize()
+    if case["conc"] is not None:
+        sp = case["spec"]
+        s.set_concentration(case["conc"](sp["nx"], sp["ny"]))
+    return s
+
+
+def gpu_params(case, precision):
+    import softflow_b200 as S
+    sp = dict(O.ChannelSpec(**case["spec"]).__dict__)
+    p = S.SimulationParams()
+    p.nx, p.ny = sp["nx"], sp["ny"]
+    p.dt = sp["dt"]
+    p.ibm_iterations = sp["ibm_iterations"]
+    p.max_lattice_force = sp["max_lattice_force"]
+    p.fluid.boundary_type = S.BoundaryType.PERIODIC
+    p.fluid.tau, p.fluid.rho0 = sp["tau"], sp["rho0"]
+    p.fluid.collision_model = S.CollisionModel(sp["collision"])
+    p.fluid.mrt_se, p.fluid.mrt_s_eps, p.fluid.mrt_sq = sp["mrt_se"], sp["mrt_s_eps"], sp["mrt_sq"]
+    p.fluid.body_force_x, p.fluid.body_force_y = sp["body_fx"], sp["body_fy"]
+    p.fluid.periodic_y = bool(sp["periodic_y"])
+    p.repulsion.epsilon, p.repulsion.sigma = sp["rep_epsilon"], sp["rep_sigma"]
+    p.repulsion.r_cut, p.repulsion.power = sp["rep_r_cut"], sp["rep_power"]
+    p.repulsion.damping_normal = sp["rep_damping_normal"]
+    p.repulsion.friction_coeff = sp["rep_friction"]
+    p.scalar.enabled = bool(sp["scalar_enabled"])
+    p.scalar.diffusivity = [sp["scalar_D"]]
+    p.scalar.periodic_y = bool(sp["scalar_periodic_y"])
+    p.scalar.inlet_concentration = [sp["scalar_inlet"]]
+    p.precision = precision
+    return p
+
+
+def gpu_membrane(mk):
+    import softflow_b200 as S
+    m = O.Membrane(**mk)
+    return S.MembraneParams(
+        model=S.MembraneModel(m.model), k_stretch=m.k_stretch, G_s=m.G_s, C_skalak=m.C_skalak,
+        wlc_L_max_ratio=m.wlc_L_max_ratio, wlc_kBT_p=m.wlc_kBT_p, wlc_k_pow=m.wlc_k_pow,
+        k_bend=m.k_bend, use_helfrich_bending=bool(m.use_helfrich), kappa_0=m.kappa_0,
+        k_area=m.k_area, k_perimeter=m.k_perimeter, gamma_visc=m.gamma_visc,
+        eta_membrane=m.eta_membrane)
+
+
+def add_case_capsules(ens, chan, case):
+    for c in case["capsules"]:
+        if c[0] == "add":
+            _, cx, cy, r, nn, mk = c
+            ens.addCapsule(chan, (cx, cy), r, nn, gpu_membrane(mk))
+        else:
+            _, count, x0, y0, x1, y1, rmin, rmax, nn, mk, seed, gap, walls = c
+            ens.addCapsuleRandom(chan, count, x0, y0, x1, y1, rmin, rmax, nn, gpu_membrane(mk),
+                                 seed=seed, min_gap=gap, check_walls=walls)
+
+
+def build_gpu(case, precision="fp32"):
+    import softflow_b200 as S
+    sim = S.Simulation(gpu_params(case, precision))
+    add_case_capsules(sim, 0, case)
+    sim.initialize()
+    if case["conc"] is not None:
+        sp = case["spec"]
+        sim.advectionDiffusion().setConcentration(case["conc"](sp["nx"], sp["ny"]))
+    return sim
+
+
+def fluid_rows(case):
+    sp = case["spec"]
+    return slice(0, sp["ny"]) if sp.get("periodic_y") else slice(1, sp["ny"] - 1)
+
+
+def rel_l2(a, b):
+    d = np.linalg.norm((a - b).ravel())
+    n = np.linalg.norm(b.ravel())
+    return d / n if n > 0 else d

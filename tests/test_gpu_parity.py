@@ -1,0 +1,175 @@
+"""GPU parity against the CPU oracle (oracle/sfo.c, itself pinned bit for bit
+to the reference engine's own sources).
+
+Tolerances:
+  FP64  -- lattice-only channels are bit-exact; channels with capsules agree
+           to 1e-9 relative (Helfrich bending uses atan2 and the contact law
+           uses pow, whose device implementations differ from glibc by ulps;
+           everything else is reproduced bit for bit);
+  FP32  -- relative L2 of velocity <= 1e-4 after the stated steps;
+  FP16S -- relative L2 of velocity <= 5e-3;
+  integer bookkeeping (capped-cell counts, contact pairs visited per marker)
+  is exact.
+"""
+import numpy as np
+import pytest
+
+from cases import CASES, build_gpu, build_oracle, fluid_rows, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _state(sim):
+    fld = sim.field()
+    rho, ux, uy, Fx, Fy = fld.macroscopic()
+    f = fld.distributions()
+    caps = sim.capsules()
+    return dict(f=f, rho=rho, ux=ux, uy=uy, Fx=Fx, Fy=Fy,
+                pos=caps.positions(), vel=caps.velocities(), frc=caps.forces())
+
+
+def _ostate(o):
+    return dict(f=o.f(), rho=o.rho(), ux=o.ux(), uy=o.uy(), Fx=o.Fx(), Fy=o.Fy(),
+                pos=o.positions(), vel=o.velocities(), frc=o.forces())
+
+
+@pytest.mark.parametrize("name,steps", [("bgk_small", 300), ("mrt_small", 300),
+                                        ("reg_small", 300), ("c0", 200)])
+def test_fp64_lattice_bit_exact(sfg, oracle_mod, name, steps):
+    case = CASES[name]
+    o = build_oracle(case)
+    o.step(steps)
+    sim = build_gpu(case, "fp64")
+    sim.run(steps)
+    a, b = _state(sim), _ostate(o)
+    rows = fluid_rows(case)
+    assert np.array_equal(a["f"][:, rows], b["f"][:, rows])
+    for k in ("rho", "ux", "uy", "Fx", "Fy"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+@pytest.mark.parametrize("name,steps", [("seam_single", 60), ("c1", 40), ("c1_plain", 40),
+                                        ("mini_c2", 40), ("contact_brute", 60)])
+def test_fp64_coupled(sfg, oracle_mod, name, steps):
+    case = CASES[name]
+    o = build_oracle(case)
+    sim = build_gpu(case, "fp64")
+    # identical placement and rest geometry
+    assert np.array_equal(sim.capsules().positions(), o.positions())
+    o.step(steps)
+    sim.run(steps)
+    a, b = _state(sim), _ostate(o)
+    rows = fluid_rows(case)
+    for k in ("ux", "uy", "rho"):
+        assert rel_l2(a[k][rows], b[k][rows]) < 1e-9, k
+    assert np.max(np.abs(a["pos"] - b["pos"])) < 1e-9
+    assert rel_l2(a["vel"], b["vel"]) < 1e-8
+    assert rel_l2(a["frc"], b["frc"]) < 1e-8
+    assert sim.lastCappedNodes() == o.last_capped()
+    if case["conc"] is not None:
+        C = sim.advectionDiffusion().concentration()
+        assert rel_l2(C, o.concentration()) < 1e-9
+
+
+@pytest.mark.parametrize("name", ["seam_single", "c1_plain"])
+def test_fp64_single_capsule_first_steps_bit_exact(sfg, oracle_mod, name):
+    """Without contact (pow) or Helfrich (atan2), a step is reproduced bit for
+    bit: membrane forces, ds, spreading, MDF, collision, interpolation, move."""
+    case = CASES[name]
+    o = build_oracle(case)
+    sim = build_gpu(case, "fp64")
+    o.step(1)
+    sim.run(1)
+    a, b = _state(sim), _ostate(o)
+    if name == "seam_single":
+        for k in ("Fx", "Fy", "ux", "uy", "rho", "pos", "vel", "frc"):
+            assert np.array_equal(a[k], b[k]), k
+
+
+def test_contact_bookkeeping_exact(sfg, oracle_mod):
+    """Cell-list membership and visiting order give the same number of
+    contact pairs per marker as the reference cell list."""
+    for name in ("c1", "contact_brute", "mini_c2"):
+        case = CASES[name]
+        o = build_oracle(case)
+        sim = build_gpu(case, "fp64")
+        o.step(1)
+        sim.run(1)
+        counts, _ = o.contact_pairs()
+        assert np.array_equal(sim.capsules().contact_counts(), counts), name
+
+
+@pytest.mark.parametrize("name,steps,tol", [("c0", 2000, 1e-4), ("c1", 200, 1e-4),
+                                            ("mini_c2", 200, 1e-4), ("seam_single", 200, 1e-4)])
+def test_fp32_velocity(sfg, oracle_mod, name, steps, tol):
+    case = CASES[name]
+    o = build_oracle(case)
+    o.step(steps)
+    sim = build_gpu(case, "fp32")
+    sim.run(steps)
+    rows = fluid_rows(case)
+    ux, uy = sim.field().velocity_x(), sim.field().velocity_y()
+    u = np.stack([ux[rows], uy[rows]])
+    uo = np.stack([o.ux()[rows], o.uy()[rows]])
+    assert rel_l2(u, uo) < tol
+    if case["capsules"]:
+        assert np.max(np.abs(sim.capsules().positions() - o.positions())) < 1e-3
+
+
+@pytest.mark.parametrize("name,steps,tol", [("c0", 2000, 5e-3), ("c1", 200, 5e-3)])
+def test_fp16s_velocity(sfg, oracle_mod, name, steps, tol):
+    case = CASES[name]
+    o = build_oracle(case)
+    o.step(steps)
+    sim = build_gpu(case, "fp16s")
+    sim.run(steps)
+    rows = fluid_rows(case)
+    u = np.stack([sim.field().velocity_x()[rows], sim.field().velocity_y()[rows]])
+    uo = np.stack([o.ux()[rows], o.uy()[rows]])
+    assert rel_l2(u, uo) < tol
+
+
+def test_scalar_fp64_bit_exact_lattice_only(sfg, oracle_mod):
+    """Pure diffusion channel: the scalar step is reproduced bit for bit,
+    including the first step that uses the seeded concentration."""
+    case = dict(CASES["diffusion"])
+    case["conc"] = lambda nx, ny: np.exp(-((np.arange(nx)[None, :] - nx / 2.0) ** 2) /
+                                         (2 * 8.0 ** 2)) * np.ones((ny, 1))
+    o = build_oracle(case)
+    sim = build_gpu(case, "fp64")
+    for n in (1, 7, 50):
+        o.step(n)
+        sim.run(n)
+        assert np.array_equal(sim.advectionDiffusion().concentration(), o.concentration())
+
+
+def test_ensemble_equals_single_runs(sfg, oracle_mod):
+    """Channels of different size, capsule count and physics advanced in one
+    context give exactly the single-channel results."""
+    import softflow_b200 as S
+    from cases import add_case_capsules, gpu_params
+    names = ["c1_plain", "bgk_small", "mini_c2", "seam_single"]
+    ens = S.Ensemble(precision="fp32")
+    for i, n in enumerate(names):
+        ens.add_channel(gpu_params(CASES[n], "fp32"))
+        add_case_capsules(ens, i, CASES[n])
+    ens.initialize()
+    for i, n in enumerate(names):
+        if CASES[n]["conc"] is not None:
+            sp = CASES[n]["spec"]
+            ens.advectionDiffusion(i).setConcentration(CASES[n]["conc"](sp["nx"], sp["ny"]))
+    ens.run(50)
+    for i, n in enumerate(names):
+        single = build_gpu(CASES[n], "fp32")
+        single.run(50)
+        assert np.array_equal(ens.field(i).distributions(), single.field().distributions()), n
+        assert np.array_equal(ens.capsules(i).positions(), single.capsules().positions()), n
+
+
+def test_runs_are_deterministic(sfg):
+    a = build_gpu(CASES["c1"], "fp32")
+    b = build_gpu(CASES["c1"], "fp32")
+    a.run(30)
+    b.run(30)
+    assert np.array_equal(a.field().distributions(), b.field().distributions())
+    assert np.array_equal(a.capsules().positions(), b.capsules().positions())
