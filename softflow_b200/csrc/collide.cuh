@@ -143,6 +143,88 @@ __device__ __forceinline__ void collide_mrt(R f[9], R r, R vx, R vy, R fx, R fy,
     f[8] = m0 / k9 + m1 / k18 + m2 / k36 + m3 / k6 + m4 / k12 - m5 / k6 - m6 / k12 - m8 / k4;
 }
 
+// ---------------------------------------------------------------------------
+// FP32 forms.  The FP32 path is checked against the FP64 oracle with a
+// tolerance, so it uses algebraically equal, division-free expressions
+// (1/cs^2 = 3, 1/(2 cs^4) = 4.5, reciprocals of the inverse-transform
+// denominators) instead of the reference's evaluation order.
+// ---------------------------------------------------------------------------
+template <>
+__device__ __forceinline__ void collide_mrt<float>(float f[9], float r, float vx, float vy,
+                                                   float fx, float fy, float sn, float s1,
+                                                   float s2, float s4) {
+    const float m0 = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
+    const float a = f[1] + f[2] + f[3] + f[4];
+    const float d = f[5] + f[6] + f[7] + f[8];
+    float m1 = -4.f * f[0] - a + 2.f * d;
+    float m2 = 4.f * f[0] - 2.f * a + d;
+    const float m3 = f[1] - f[3] + f[5] - f[6] - f[7] + f[8] + fx;   // + Sb3
+    float m4 = -2.f * (f[1] - f[3]) + f[5] - f[6] - f[7] + f[8];
+    const float m5 = f[2] - f[4] + f[5] + f[6] - f[7] - f[8] + fy;   // + Sb5
+    float m6 = -2.f * (f[2] - f[4]) + f[5] + f[6] - f[7] - f[8];
+    float m7 = f[1] - f[2] + f[3] - f[4];
+    float m8 = f[5] - f[6] + f[7] - f[8];
+    const float uu = vx * vx + vy * vy;
+    const float uF = vx * fx + vy * fy;
+    m1 = m1 - s1 * (m1 - (-2.f * r + 3.f * r * uu)) + (1.f - 0.5f * s1) * (6.f * uF);
+    m2 = m2 - s2 * (m2 - (r - 3.f * r * uu)) - (1.f - 0.5f * s2) * (6.f * uF);
+    m4 = m4 - s4 * (m4 + r * vx) - (1.f - 0.5f * s4) * fx;
+    m6 = m6 - s4 * (m6 + r * vy) - (1.f - 0.5f * s4) * fy;
+    m7 = m7 - sn * (m7 - r * (vx * vx - vy * vy)) + (1.f - 0.5f * sn) * (2.f * (vx * fx - vy * fy));
+    m8 = m8 - sn * (m8 - r * vx * vy) + (1.f - 0.5f * sn) * (vx * fy + vy * fx);
+    const float c9 = 1.f / 9.f, c18 = 1.f / 18.f, c36 = 1.f / 36.f, c6 = 1.f / 6.f,
+                c12 = 1.f / 12.f;
+    const float b0 = c9 * m0;
+    const float bA = b0 - c36 * m1 - c18 * m2;   // axis directions
+    const float bD = b0 + c18 * m1 + c36 * m2;   // diagonals
+    f[0] = c9 * (m0 - m1 + m2);
+    f[1] = bA + c6 * (m3 - m4) + 0.25f * m7;
+    f[2] = bA + c6 * (m5 - m6) - 0.25f * m7;
+    f[3] = bA - c6 * (m3 - m4) + 0.25f * m7;
+    f[4] = bA - c6 * (m5 - m6) - 0.25f * m7;
+    const float px = c6 * m3 + c12 * m4, py = c6 * m5 + c12 * m6;
+    f[5] = bD + px + py + 0.25f * m8;
+    f[6] = bD - px + py - 0.25f * m8;
+    f[7] = bD - px - py + 0.25f * m8;
+    f[8] = bD + px - py - 0.25f * m8;
+}
+
+template <>
+__device__ __forceinline__ void collide_regularized<float>(float f[9], float rho, float ux,
+                                                           float uy, float Fx, float Fy,
+                                                           float omega) {
+    const float uu15 = 1.5f * (ux * ux + uy * uy);
+    float fe[9];
+    float jx = 0.f, jy = 0.f, pxx = 0.f, pxy = 0.f, pyy = 0.f;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        const float cx = float(cx_of(q)), cy = float(cy_of(q));
+        const float eu = cx * ux + cy * uy;
+        fe[q] = float(w_of(q)) * rho * (1.f + 3.f * eu + 4.5f * eu * eu - uu15);
+        const float fneq = f[q] - fe[q];
+        if (cx_of(q) != 0) { jx += cx * fneq; pxx += fneq; }
+        if (cy_of(q) != 0) { jy += cy * fneq; pyy += fneq; }
+        if (cx_of(q) * cy_of(q) != 0) pxy += cx * cy * fneq;
+    }
+    const float om1 = 1.f - omega, guo = 1.f - 0.5f * omega;
+    // Q:Pi/(2 cs^4) with Q = e e - cs^2 I
+    const float trP = (pxx + pyy) * (1.f / 3.f);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        const int icx = cx_of(q), icy = cy_of(q);
+        const float cx = float(icx), cy = float(icy), w = float(w_of(q));
+        float qp = -trP;
+        if (icx) qp += pxx;
+        if (icy) qp += pyy;
+        if (icx * icy) qp += 2.f * cx * cy * pxy;
+        const float fneq_reg = w * (3.f * (cx * jx + cy * jy) + 4.5f * qp);
+        const float eu = cx * ux + cy * uy;
+        const float Fi = guo * w * ((3.f * (cx - ux) + 9.f * eu * cx) * Fx +
+                                    (3.f * (cy - uy) + 9.f * eu * cy) * Fy);
+        f[q] = fe[q] + om1 * fneq_reg + Fi;
+    }
+}
+
 // Passive-scalar BGK collision with the first-order equilibrium
 // (advection_diffusion.cpp:137-151): g* = g - w_s (g - w C (1 + 3 e.u)).
 template <typename R>

@@ -109,22 +109,52 @@ __device__ __forceinline__ CellForces<R> cell_forces(const ChannelDev& ch, int x
     return cf;
 }
 
-// Downstream target of population q leaving (x, y): returns false when the
-// neighbour is a wall (the population is then reflected into the own cell).
-__device__ __forceinline__ bool downstream(const ChannelDev& ch, int x, int y, int q, int wall_mode,
-                                           int& xd, int& yd) {
-    xd = x + cx_of(q);
-    yd = y + cy_of(q);
-    if (xd < 0) xd += ch.nx;
-    if (xd >= ch.nx) xd -= ch.nx;
-    if (wall_mode == 0) {            // SOLID rows 0 and ny-1
-        return !(yd == 0 || yd == ch.ny - 1);
-    } else if (wall_mode == 1) {     // periodic in y
-        if (yd < 0) yd += ch.ny;
-        if (yd >= ch.ny) yd -= ch.ny;
-        return true;
+// Neighbour columns/rows of a cell and the wall flags of its two
+// neighbouring rows.  y-wall modes: 0 = SOLID rows 0 and ny-1, 1 = periodic,
+// 2 = reflection at the domain edge (scalar with open y).
+struct Nbr {
+    int xm, xp, ym, yp;
+    bool wall_m, wall_p;
+};
+
+__device__ __forceinline__ Nbr neighbours(int x, int y, int nx, int ny, int mode) {
+    Nbr b;
+    b.xm = (x == 0) ? nx - 1 : x - 1;
+    b.xp = (x == nx - 1) ? 0 : x + 1;
+    if (mode == 1) {
+        b.ym = (y == 0) ? ny - 1 : y - 1;
+        b.yp = (y == ny - 1) ? 0 : y + 1;
+        b.wall_m = b.wall_p = false;
+    } else if (mode == 0) {
+        b.ym = y - 1;
+        b.yp = y + 1;
+        b.wall_m = (b.ym == 0);
+        b.wall_p = (b.yp == ny - 1);
+    } else {
+        b.ym = y - 1;
+        b.yp = y + 1;
+        b.wall_m = (b.ym < 0);
+        b.wall_p = (b.yp >= ny);
     }
-    return yd >= 0 && yd < ch.ny;    // open y with reflection at the domain edge
+    return b;
+}
+
+// Push the nine post-collision values of cell (x, y): to the downstream
+// neighbour, or reflected into the own cell when that neighbour is a wall.
+template <typename S, typename R>
+__device__ __forceinline__ void push_cell(S* __restrict__ fd, const R f[9], int x, int y, int n,
+                                          int pitch, int plane, const Nbr& b) {
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        const int cx = cx_of(q), cy = cy_of(q);
+        const bool wall = (cy > 0 && b.wall_p) || (cy < 0 && b.wall_m);
+        const int xd = cx == 0 ? x : (cx > 0 ? b.xp : b.xm);
+        const int yd = cy == 0 ? y : (cy > 0 ? b.yp : b.ym);
+        if (!wall)
+            PopIO<S, R>::store(fd + q * plane + yd * pitch + xd, q, f[q]);
+        else
+            PopIO<S, R>::store(fd + opp_of(q) * plane + n, opp_of(q), f[q]);
+    }
 }
 
 template <typename S, typename R, bool ADR>
@@ -137,36 +167,30 @@ k_lattice_step(const RowItem* __restrict__ items, const ChannelDev* __restrict__
     const RowItem it = items[blockIdx.x];
     if ((int)threadIdx.x >= it.len) return;
     const ChannelDev& ch = chans[it.chan];
+    const int nx = ch.nx, ny = ch.ny, pitch = ch.pitch, plane = (int)ch.plane;
     const int x = it.x0 + threadIdx.x, y = it.y;
-    const long long n = (long long)y * ch.pitch + x;
-    const S* fs = src + ch.f_off + n;
+    const int n = y * pitch + x;
+    const S* __restrict__ fs = src + ch.f_off + n;
     R f[9];
 #pragma unroll
-    for (int q = 0; q < 9; ++q) f[q] = PopIO<S, R>::load(fs + q * ch.plane, q);
+    for (int q = 0; q < 9; ++q) f[q] = PopIO<S, R>::load(fs + q * plane, q);
     R rho, jx, jy;
     cell_moments(f, rho, jx, jy);
     const int st = stepped[it.chan];
     const CellForces<R> cf = cell_forces<R>(ch, x, y, tv, st);
     R ux, uy;
     cell_velocity(rho, jx, jy, cf.Gx, cf.Gy, ux, uy);
-    if (ch.collision == 2) {
+    const int coll = ch.collision;
+    if (coll == 2) {
         collide_regularized(f, rho, ux, uy, cf.Fx, cf.Fy, R(ch.omega));
-    } else if (ch.collision == 1) {
+    } else if (coll == 1) {
         collide_mrt(f, rho, ux, uy, cf.Fx, cf.Fy, R(ch.omega), R(ch.mrt_se), R(ch.mrt_s_eps),
                     R(ch.mrt_sq));
     } else {
         collide_bgk(f, rho, ux, uy, cf.Fx, cf.Fy, R(ch.omega));
     }
-    const int wall_mode = ch.periodic_y ? 1 : 0;
-    S* fd = dst + ch.f_off;
-#pragma unroll
-    for (int q = 0; q < 9; ++q) {
-        int xd, yd;
-        if (downstream(ch, x, y, q, wall_mode, xd, yd))
-            PopIO<S, R>::store(fd + q * ch.plane + (long long)yd * ch.pitch + xd, q, f[q]);
-        else
-            PopIO<S, R>::store(fd + opp_of(q) * ch.plane + n, opp_of(q), f[q]);
-    }
+    const Nbr b = neighbours(x, y, nx, ny, ch.periodic_y ? 1 : 0);
+    push_cell<S, R>(dst + ch.f_off, f, x, y, n, pitch, plane, b);
     if (ADR) {
         // Scalar step of the previous lattice step (it needs that step's
         // final velocity, which is only known once its populations have been
@@ -175,70 +199,54 @@ k_lattice_step(const RowItem* __restrict__ items, const ChannelDev* __restrict__
             R g[9];
             const R* gp = gsrc + ch.g_off + n;
 #pragma unroll
-            for (int q = 0; q < 9; ++q) g[q] = gp[q * ch.plane];
+            for (int q = 0; q < 9; ++q) g[q] = gp[q * plane];
             R C;
             if (c_fresh[it.chan]) C = cfield[ch.cell_off + n];
             else C = g[0] + g[1] + g[2] + g[3] + g[4] + g[5] + g[6] + g[7] + g[8];
             R vx, vy;
             cell_velocity(rho, jx, jy, cf.Px, cf.Py, vx, vy);
             collide_scalar(g, C, vx, vy, R(ch.omega_s));
-            const int gwall = ch.periodic_y ? (ch.adr_periodic_y ? 1 : 2) : 0;
-            R* gd = gdst + ch.g_off;
-#pragma unroll
-            for (int q = 0; q < 9; ++q) {
-                int xd, yd;
-                if (downstream(ch, x, y, q, gwall, xd, yd))
-                    gd[q * ch.plane + (long long)yd * ch.pitch + xd] = g[q];
-                else
-                    gd[opp_of(q) * ch.plane + n] = g[q];
-            }
+            const int gmode = ch.periodic_y ? (ch.adr_periodic_y ? 1 : 2) : 0;
+            const Nbr gb = gmode == (ch.periodic_y ? 1 : 0) ? b : neighbours(x, y, nx, ny, gmode);
+            push_cell<R, R>(gdst + ch.g_off, g, x, y, n, pitch, plane, gb);
         }
     }
 }
 
-// Scalar step alone (used to bring the scalar up to date before a host read).
+// Scalar step alone (brings the scalar up to date before a host read).
 template <typename S, typename R>
 __global__ void __launch_bounds__(256)
 k_scalar_flush(const RowItem* __restrict__ items, const ChannelDev* __restrict__ chans,
                const S* __restrict__ src, const R* __restrict__ gsrc, R* __restrict__ gdst,
-               const R* __restrict__ cfield, TileView tv_last, const int* __restrict__ stepped_prev,
-               const int* __restrict__ adr_pending, const int* __restrict__ c_fresh) {
+               const R* __restrict__ cfield, TileView tv_last, const int* __restrict__ adr_pending,
+               const int* __restrict__ c_fresh) {
     const RowItem it = items[blockIdx.x];
     if ((int)threadIdx.x >= it.len) return;
     const ChannelDev& ch = chans[it.chan];
     if (!ch.adr || !adr_pending[it.chan]) return;
+    const int nx = ch.nx, ny = ch.ny, pitch = ch.pitch, plane = (int)ch.plane;
     const int x = it.x0 + threadIdx.x, y = it.y;
-    const long long n = (long long)y * ch.pitch + x;
+    const int n = y * pitch + x;
     const S* fs = src + ch.f_off + n;
     R f[9];
 #pragma unroll
-    for (int q = 0; q < 9; ++q) f[q] = PopIO<S, R>::load(fs + q * ch.plane, q);
+    for (int q = 0; q < 9; ++q) f[q] = PopIO<S, R>::load(fs + q * plane, q);
     R rho, jx, jy;
     cell_moments(f, rho, jx, jy);
-    // the force of the last completed step plays the role of P here; it is
-    // that step's "cur" tile set, passed as cur_* in tv_last
+    // the force of the last completed step (its "cur" tile set)
     const CellForces<R> cf = cell_forces<R>(ch, x, y, tv_last, 1);
     R g[9];
     const R* gp = gsrc + ch.g_off + n;
 #pragma unroll
-    for (int q = 0; q < 9; ++q) g[q] = gp[q * ch.plane];
+    for (int q = 0; q < 9; ++q) g[q] = gp[q * plane];
     R C;
     if (c_fresh[it.chan]) C = cfield[ch.cell_off + n];
     else C = g[0] + g[1] + g[2] + g[3] + g[4] + g[5] + g[6] + g[7] + g[8];
     R vx, vy;
     cell_velocity(rho, jx, jy, cf.Fx, cf.Fy, vx, vy);
     collide_scalar(g, C, vx, vy, R(ch.omega_s));
-    const int gwall = ch.periodic_y ? (ch.adr_periodic_y ? 1 : 2) : 0;
-    R* gd = gdst + ch.g_off;
-#pragma unroll
-    for (int q = 0; q < 9; ++q) {
-        int xd, yd;
-        if (downstream(ch, x, y, q, gwall, xd, yd))
-            gd[q * ch.plane + (long long)yd * ch.pitch + xd] = g[q];
-        else
-            gd[opp_of(q) * ch.plane + n] = g[q];
-    }
-    (void)stepped_prev;
+    const int gmode = ch.periodic_y ? (ch.adr_periodic_y ? 1 : 2) : 0;
+    push_cell<R, R>(gdst + ch.g_off, g, x, y, n, pitch, plane, neighbours(x, y, nx, ny, gmode));
 }
 
 // ---- host <-> device population transfer (canonical FP64 [9][ny][nx]) ----

@@ -36,7 +36,7 @@ void launch_scalar_flush(const LatticeLaunch& L, const TileViewArgs& tv_last, cu
     if (L.n_items == 0 || !L.any_adr) return;
     k_scalar_flush<S, R><<<L.n_items, 256, 0, st>>>(
         L.items, L.chans, static_cast<const S*>(L.src), static_cast<const R*>(L.gsrc),
-        static_cast<R*>(L.gdst), static_cast<const R*>(L.cfield), to_view(tv_last), L.stepped,
+        static_cast<R*>(L.gdst), static_cast<const R*>(L.cfield), to_view(tv_last),
         L.adr_pending, L.c_fresh);
 }
 

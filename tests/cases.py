@@ -125,14 +125,16 @@ def gpu_membrane(mk):
 
 
 def add_case_capsules(ens, chan, case):
+    import softflow_b200 as S
     for c in case["capsules"]:
         if c[0] == "add":
             _, cx, cy, r, nn, mk = c
-            ens.addCapsule(chan, (cx, cy), r, nn, gpu_membrane(mk))
+            S.Ensemble.addCapsule(ens, chan, (cx, cy), r, nn, gpu_membrane(mk))
         else:
             _, count, x0, y0, x1, y1, rmin, rmax, nn, mk, seed, gap, walls = c
-            ens.addCapsuleRandom(chan, count, x0, y0, x1, y1, rmin, rmax, nn, gpu_membrane(mk),
-                                 seed=seed, min_gap=gap, check_walls=walls)
+            S.Ensemble.addCapsuleRandom(ens, chan, count, x0, y0, x1, y1, rmin, rmax, nn,
+                                        gpu_membrane(mk), seed=seed, min_gap=gap,
+                                        check_walls=walls)
 
 
 def build_gpu(case, precision="fp32"):
