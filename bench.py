@@ -1,0 +1,452 @@
+#!/usr/bin/env python
+"""Headline benchmark of the SoftFlow hot path on B200.
+
+Default workload (c3): the 256-channel capsule ensemble (seed 7) advanced in
+one context, FP16-shifted population storage with FP32 arithmetic, 5 MDF
+sweeps.  The metric is capsule-steps/s (sum over channels of capsules x
+steps per second); MLUPS and marker-updates/s are reported beside it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c3|c2|c1|c0]
+                  [--precision fp16s|fp32|fp64] [--impl product|reference]
+
+value     device time (CUDA events on the context stream) of K steps with the
+          state resident in HBM; max over ranks; whole-job aggregate.
+e2e       the same K steps through the public API from host buffers: the
+          initial populations and markers are uploaded from pinned host memory
+          inside the timed region, and every step reads all marker positions
+          back to the host.
+roofline  the lattice kernel (fused collide + stream + bounce-back + lagged
+          scalar step), timed live with CUDA events in a profiling pass;
+          algorithmic bytes = one read + one write of 9 populations per fluid
+          cell (+ the same for the scalar where enabled).
+cpu_baseline  the reference engine's own sources (oracle/_ref, Release flags,
+          OpenMP over all host cores) on a bounded sample of the workload.
+
+Multi-GPU: the channels are independent, so each rank runs the full
+workload on its own GPU with no collective on the data path (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--workload", default="c3", choices=["c3", "c2", "c1", "c0"])
+    ap.add_argument("--precision", default="fp16s", choices=["fp16s", "fp32", "fp64"])
+    ap.add_argument("--impl", default="product", choices=["product", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the per-channel plain form")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- ranks ----
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg, local):
+    if pg is not None:
+        import torch
+        pg.barrier(device_ids=[local])
+        torch.cuda.synchronize()
+
+
+def allmax(pg, v: float) -> float:
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+# --------------------------------------------------------------- clocks ----
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = max(float(r[2]) for r in rows)
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def peaks():
+    try:
+        with open(PEAKS_FILE) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+# ------------------------------------------------------------ workloads ----
+def bytes_per_cell(precision: str) -> int:
+    return {"fp64": 144, "fp32": 72, "fp16s": 36}[precision]
+
+
+def scalar_bytes_per_cell(precision: str) -> int:
+    return 144 if precision == "fp64" else 72
+
+
+def run_product(args, world, rank, local, pg):
+    import numpy as np
+    import softflow_b200 as S
+    from softflow_b200 import workloads as W
+    plans = W.PLANS[args.workload](args.precision)
+    ens = W.build(plans, precision=args.precision, device=local)
+    ctx = ens.context()
+    cells, caps, markers, scal = W.totals(plans, ens)
+    nch = len(plans)
+
+    # warm-up (graphs are built on the first call)
+    ctx.step(args.warmup)
+    ctx.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(pg, local)
+    ctx.step(args.steps)
+    ctx.synchronize()
+    ms = ctx.last_step_ms()
+    barrier(pg, local)
+    clk = clocks.stop()
+    ms_max = allmax(pg, ms)
+    launches = ctx.launches_per_step()
+
+    sec = ms_max / 1e3
+    cap_steps = caps * args.steps * world / sec
+    mlups = cells * args.steps * world / sec / 1e6
+    mk_upd = markers * args.steps * world / sec
+
+    # profiling pass: per-phase CUDA-event times (eager launches)
+    prof_steps = max(5, min(args.steps, 50))
+    ctx.set_profiling(True)
+    ctx.reset_phase_times()
+    ctx.step(prof_steps)
+    ctx.synchronize()
+    phases = ctx.phase_times()
+    ctx.set_profiling(False)
+    lat_ms = phases["lattice"] / prof_steps
+    alg_bytes = cells * bytes_per_cell(args.precision) + scal * scalar_bytes_per_cell(
+        args.precision)
+    achieved = alg_bytes / (lat_ms / 1e3) / 1e9 if lat_ms > 0 else 0.0
+    peak, peak_kind = peaks()
+    total_phase = sum(phases.values()) or 1.0
+
+    # e2e: host-resident initial state, per-step marker readback
+    e2e = run_e2e(args, plans, ens, pg, local)
+
+    # plain per-channel form (each channel its own context, run one after the other)
+    plain = None
+    if args.workload == "c3" and not args.no_plain:
+        plain = run_plain(args, plans, local)
+
+    out = {
+        "metric": "capsule-steps/s",
+        "value": cap_steps,
+        "unit": "capsule-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": {"fp16s": "fp16-storage/fp32", "fp32": "fp32", "fp64": "fp64"}[args.precision],
+        "data": "synthetic (seeded placement; no datasets)",
+        "config": {"workload": args.workload, "channels": nch, "fluid_cells": cells,
+                   "capsules": caps, "markers": markers, "precision": args.precision,
+                   "mdf_sweeps": max(p.params.ibm_iterations for p in plans),
+                   "l2": "state larger than L2 (no flush needed)" if alg_bytes > 126e6
+                         else "state fits L2 (L2-resident workload)",
+                   "parallelism": f"replicas x{world} (independent channels)"},
+        "mlups": mlups,
+        "marker_updates_per_s": mk_upd,
+        "gpu_launches": launches * args.steps,
+        "phase_ms_per_step": {k: v / prof_steps for k, v in phases.items()},
+        "roofline": {"kernel": "k_lattice_step", "bound": "hbm", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind,
+                     "share_of_step": phases["lattice"] / total_phase,
+                     "algorithmic_bytes_per_launch": alg_bytes, "traffic": None},
+        "e2e": e2e,
+        "clocks": clk,
+    }
+    if plain is not None:
+        out["plain"] = plain
+        out["batched_vs_plain"] = cap_steps / world / plain["value"] if plain["value"] else None
+    ens.close()
+    return out
+
+
+def run_e2e(args, plans, ens, pg, local):
+    """K steps from host-resident state through the public API."""
+    import numpy as np
+    import torch
+    from softflow_b200 import _lib as L
+    import ctypes as C
+    ctx = ens.context()
+    lib = ctx._lib
+    # pinned host copies of the current state
+    pops, mk = [], []
+    for i, pl in enumerate(plans):
+        f = ens.field(i).distributions()
+        t = torch.empty(f.size, dtype=torch.float64, pin_memory=True)
+        t.numpy()[:] = f.ravel()
+        pops.append(t)
+    M = sum(r.rest.num_nodes for c in ens._chans for r in c.caps)
+    pos_h = torch.empty(2 * max(M, 1), dtype=torch.float64, pin_memory=True)
+    vel_h = torch.empty(2 * max(M, 1), dtype=torch.float64, pin_memory=True)
+    lib.sfg_get_all_markers(ctx._h, L.dptr(pos_h.numpy()), L.dptr(vel_h.numpy()))
+    h2d = sum(p.numel() * 8 for p in pops)
+    d2h_step = 2 * 8 * 2 * M
+    barrier(pg, local)
+    t0 = time.perf_counter()
+    for i in range(len(plans)):
+        L.check(lib.sfg_set_populations(ctx._h, i, L.dptr(pops[i].numpy())))
+    for s in range(args.steps):
+        L.check(lib.sfg_step(ctx._h, 1))
+        L.check(lib.sfg_get_all_markers(ctx._h, L.dptr(pos_h.numpy()), L.dptr(vel_h.numpy())))
+    ctx.synchronize()
+    t1 = time.perf_counter()
+    sec = allmax(pg, t1 - t0)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    caps = sum(len(c.caps) for c in ens._chans)
+    return {"value": caps * args.steps * world / sec, "unit": "capsule-steps/s",
+            "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h_step,
+            "note": "initial state uploaded from pinned host memory inside the timed region; "
+                    "every step reads all marker positions and velocities back"}
+
+
+def run_plain(args, plans, local, max_channels=256, steps=None):
+    """The plain GPU form: every channel in its own context, stepped one after
+    the other (no batching), FP32 storage."""
+    from softflow_b200 import workloads as W
+    steps = steps or max(10, min(args.steps, 40))
+    total_caps_steps = 0
+    total_ms = 0.0
+    for pl in plans[:max_channels]:
+        pl.params.precision = "fp32"
+        ens = W.build([pl], precision="fp32", device=local)
+        ctx = ens.context()
+        ctx.step(3)
+        ctx.synchronize()
+        ctx.step(steps)
+        ctx.synchronize()
+        total_ms += ctx.last_step_ms()
+        total_caps_steps += len(ens._chans[0].caps) * steps
+        ens.close()
+    return {"value": total_caps_steps / (total_ms / 1e3), "unit": "capsule-steps/s",
+            "form": "one context per channel, FP32, stepped sequentially",
+            "steps_per_channel": steps}
+
+
+# ------------------------------------------------------------ CPU side ----
+def oracle_spec(params):
+    import oracle as O
+    f = params.fluid
+    return O.ChannelSpec(
+        nx=params.nx, ny=params.ny, collision=int(f.collision_model), tau=f.tau, rho0=f.rho0,
+        mrt_se=f.mrt_se, mrt_s_eps=f.mrt_s_eps, mrt_sq=f.mrt_sq, body_fx=f.body_force_x,
+        body_fy=f.body_force_y, periodic_y=int(f.periodic_y),
+        max_lattice_force=params.max_lattice_force, ibm_iterations=params.ibm_iterations,
+        dt=params.dt, scalar_enabled=int(params.scalar.enabled),
+        scalar_D=params.scalar.diffusivity[0] if params.scalar.diffusivity else 0.01)
+
+
+def oracle_membrane(mp):
+    import oracle as O
+    return O.Membrane(model=int(mp.model), k_stretch=mp.k_stretch, G_s=mp.G_s,
+                      C_skalak=mp.C_skalak, wlc_L_max_ratio=mp.wlc_L_max_ratio,
+                      wlc_kBT_p=mp.wlc_kBT_p, wlc_k_pow=mp.wlc_k_pow, k_bend=mp.k_bend,
+                      use_helfrich=int(mp.use_helfrich_bending), kappa_0=mp.kappa_0,
+                      k_area=mp.k_area, k_perimeter=mp.k_perimeter,
+                      gamma_visc=mp.gamma_visc, eta_membrane=mp.eta_membrane)
+
+
+def cpu_sims(plans, impl, threads):
+    import io
+    import contextlib
+    import numpy as np
+    import oracle as O
+    sims = []
+    for pl in plans:
+        s = O.OracleSim(oracle_spec(pl.params), impl, fast=(impl == "ref"), threads=threads)
+        with contextlib.redirect_stdout(io.StringIO()):
+            for (count, x0, y0, x1, y1, r, nodes, mp, seed) in pl.placements:
+                s.add_capsule_random(count, x0, y0, x1, y1, r, r, nodes, oracle_membrane(mp),
+                                     seed=seed, min_gap=1.0, check_walls=True)
+        s.initialize()
+        if pl.gaussian is not None:
+            cx, cy, sg = pl.gaussian
+            p = pl.params
+            y, x = np.mgrid[0:p.ny, 0:p.nx]
+            s.set_concentration(np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2.0 * sg * sg)))
+        sims.append(s)
+    return sims
+
+
+def cpu_kind():
+    import oracle as O
+    return ("reference", "ref") if os.path.exists(O.REF_FAST_LIB) else ("port", "sfo")
+
+
+def sample_plans(workload, precision):
+    """Bounded CPU sample of the workload."""
+    from softflow_b200 import workloads as W
+    plans = W.PLANS[workload](precision)
+    if workload == "c3":
+        return plans[:32], "first 32 of 256 channels"
+    return plans, "full workload"
+
+
+def run_cpu_baseline(workload, precision, steps=None, budget_s=20.0):
+    kind, impl = cpu_kind()
+    threads = (os.cpu_count() or 1) if impl == "ref" else 1
+    plans, what = sample_plans(workload, precision)
+    sims = cpu_sims(plans, impl, threads)
+    caps = sum(s.num_capsules for s in sims)
+    # one step to estimate the cost, then a window of ~budget_s
+    t0 = time.perf_counter()
+    for s in sims:
+        s.step(1)
+    dt1 = max(time.perf_counter() - t0, 1e-6)
+    n = steps or max(1, min(200, int(budget_s / dt1)))
+    t0 = time.perf_counter()
+    for s in sims:
+        s.step(n)
+    sec = time.perf_counter() - t0
+    return {"value": caps * n / sec, "unit": "capsule-steps/s", "cores": threads,
+            "kind": kind, "sample": f"{what}, {n} steps each after 1 warm-up step"}
+
+
+def run_reference_arm(args):
+    """The reference's own CPU implementation (oracle/_ref, Release flags,
+    all host threads) on the same workload and metric, one bounded sample
+    (a fixed channel subset) per step."""
+    kind, impl = cpu_kind()
+    threads = (os.cpu_count() or 1) if impl == "ref" else 1
+    plans, what = sample_plans(args.workload, args.precision)
+    if args.workload == "c3":
+        plans, what = plans[:8], "first 8 of 256 channels per step"
+    sims = cpu_sims(plans, impl, threads)
+    caps = sum(s.num_capsules for s in sims)
+    for _ in range(args.warmup):
+        for s in sims:
+            s.step(1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for s in sims:
+            s.step(1)
+    sec = time.perf_counter() - t0
+    v = caps * args.steps / sec
+    return {
+        "impl": "reference", "metric": "capsule-steps/s", "value": v, "unit": "capsule-steps/s",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
+        "data": "synthetic (seeded placement; no datasets)",
+        "config": {"workload": args.workload, "sample": what},
+        "cpu_baseline": {"value": v, "unit": "capsule-steps/s", "cores": threads, "kind": kind,
+                         "sample": what},
+        "e2e": {"value": v, "unit": "capsule-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return 0
+        print(json.dumps(run_reference_arm(args)), flush=True)
+        return 0
+    world, rank, local, pg = dist_setup(args)
+    out = run_product(args, world, rank, local, pg)
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            out["cpu_baseline"] = run_cpu_baseline(args.workload, args.precision)
+        except Exception as e:  # the baseline is reported, never required
+            out["cpu_baseline"] = {"value": None, "error": str(e)}
+    if pg is not None:
+        pg.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -45,7 +45,8 @@ enum sfg_status {
 enum sfg_precision {
     SFG_FP64 = 0,   /* FP64 storage and arithmetic                              */
     SFG_FP32 = 1,   /* FP32 storage and arithmetic                              */
-    SFG_FP16S = 2   /* FP16 storage of f - w (rounded to nearest even), FP32 math */
+    SFG_FP16S = 2   /* binary16 storage of (f - w) * 2^12 with stochastic rounding
+                       inside the time loop, FP32 arithmetic                    */
 };
 
 enum sfg_collision { SFG_BGK = 0, SFG_MRT = 1, SFG_REGULARIZED = 2 };
@@ -160,6 +161,8 @@ int sfg_get_macroscopic(sfg_context* ctx, int channel, double* rho, double* ux, 
                         double* Fx, double* Fy);
 int sfg_get_markers(sfg_context* ctx, int channel, double* pos, double* vel, double* force);
 int sfg_set_markers(sfg_context* ctx, int channel, const double* pos, const double* vel);
+/* Marker positions / velocities of every channel at once (channel-major). */
+int sfg_get_all_markers(sfg_context* ctx, double* pos, double* vel);
 /* Concentration field and equilibrium populations g = w C
  * (AdvectionDiffusion::setRegion semantics, advection_diffusion.cpp:59-71). */
 int sfg_set_concentration(sfg_context* ctx, int channel, const double* C);
@@ -180,6 +183,24 @@ int sfg_launches_per_step(const sfg_context* ctx, int* launches);
 /* Host-visible timing of the last sfg_step call in milliseconds, measured
  * with CUDA events on the context stream (valid after sfg_synchronize). */
 int sfg_last_step_ms(sfg_context* ctx, float* ms);
+/* Per-phase timing, the counterpart of the reference's per-module Profiler
+ * timers (simulation.cpp:194-208, io/profiler.h:12-90).  With profiling on,
+ * sfg_step runs each step eagerly and accumulates CUDA-event times per
+ * phase (milliseconds, indexed by sfg_phase). */
+enum sfg_phase {
+    SFG_PHASE_MEMBRANE = 0,     /* "Membrane forces"                          */
+    SFG_PHASE_CONTACT = 1,      /* "Repulsion forces" (cell list + contact)   */
+    SFG_PHASE_IBM_TILES = 2,    /* force-tile occupancy and marker lists      */
+    SFG_PHASE_IBM_SPREAD = 3,   /* "IBM spread" (all MDF sweeps)              */
+    SFG_PHASE_MDF_INTERP = 4,   /* MDF interpolation sweeps                   */
+    SFG_PHASE_LATTICE = 5,      /* "LBM step" (+ fused scalar step)           */
+    SFG_PHASE_BOOKKEEPING = 6,  /* per-step flags                             */
+    SFG_PHASE_INTERP_MOVE = 7,  /* "IBM interpolate" + marker move            */
+    SFG_NUM_PHASES = 8
+};
+int sfg_set_profiling(sfg_context* ctx, int on);
+int sfg_get_phase_times(sfg_context* ctx, float* ms, int n);
+int sfg_reset_phase_times(sfg_context* ctx);
 /* CUDA stream of the context (cudaStream_t), for callers that interleave
  * their own work. */
 int sfg_get_stream(const sfg_context* ctx, void** stream);

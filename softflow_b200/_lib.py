@@ -88,6 +88,7 @@ SIGNATURES = {
     "sfg_get_macroscopic": (C.c_int, [C.c_void_p, C.c_int, _D, _D, _D, _D, _D]),
     "sfg_get_markers": (C.c_int, [C.c_void_p, C.c_int, _D, _D, _D]),
     "sfg_set_markers": (C.c_int, [C.c_void_p, C.c_int, _D, _D]),
+    "sfg_get_all_markers": (C.c_int, [C.c_void_p, _D, _D]),
     "sfg_set_concentration": (C.c_int, [C.c_void_p, C.c_int, _D]),
     "sfg_get_concentration": (C.c_int, [C.c_void_p, C.c_int, _D, _D]),
     "sfg_get_capped_count": (C.c_int, [C.c_void_p, C.c_int, _I]),
@@ -98,7 +99,13 @@ SIGNATURES = {
     "sfg_launches_per_step": (C.c_int, [C.c_void_p, _I]),
     "sfg_last_step_ms": (C.c_int, [C.c_void_p, _P(C.c_float)]),
     "sfg_get_stream": (C.c_int, [C.c_void_p, _P(C.c_void_p)]),
+    "sfg_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+    "sfg_get_phase_times": (C.c_int, [C.c_void_p, _P(C.c_float), C.c_int]),
+    "sfg_reset_phase_times": (C.c_int, [C.c_void_p]),
 }
+
+PHASES = ["membrane", "contact", "ibm_tiles", "ibm_spread", "mdf_interp", "lattice",
+          "bookkeeping", "interp_move"]
 
 
 def lib():

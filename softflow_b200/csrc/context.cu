@@ -46,8 +46,9 @@ struct ChanHost {
 };
 
 __global__ void k_step_flags(const ChannelDev* __restrict__ chans, int nch, int* stepped,
-                             int* adr_pending, int* c_fresh) {
+                             int* adr_pending, int* c_fresh, unsigned* step_ctr) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c == 0) *step_ctr += 1u;
     if (c >= nch) return;
     if (chans[c].adr) {
         if (adr_pending[c]) c_fresh[c] = 0;
@@ -156,6 +157,7 @@ struct sfg_context {
     int* d_adr_pending = nullptr;
     int* d_c_fresh = nullptr;
     unsigned* d_status = nullptr;
+    unsigned* d_step_ctr = nullptr;
     double* d_io = nullptr;
     size_t io_doubles = 0;
     int spread_grid = 0;
@@ -167,6 +169,11 @@ struct sfg_context {
     bool use_graphs = true;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int launches = 0;
+    // per-phase timing (profiling mode runs the step eagerly)
+    bool profiling = false;
+    std::vector<cudaEvent_t> pev;
+    std::vector<int> pev_phase;
+    float phase_ms[SFG_NUM_PHASES] = {0};
 
     size_t elem_size() const { return precision == SFG_FP64 ? 8 : (precision == SFG_FP32 ? 4 : 2); }
     size_t real_size() const { return precision == SFG_FP64 ? 8 : 4; }
@@ -228,6 +235,7 @@ static void free_all(sfg_context* c) {
     F(c->cb.cell_of); F(c->cb.cell_cnt); F(c->cb.cell_start); F(c->cb.cursor); F(c->cb.list);
     F(c->cb.scan_tmp);
     F(c->d_phi); F(c->d_stepped); F(c->d_adr_pending); F(c->d_c_fresh); F(c->d_status);
+    F(c->d_step_ctr);
     F(c->d_io);
 }
 
@@ -238,6 +246,7 @@ extern "C" int sfg_destroy(sfg_context* c) {
     free_all(c);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    for (cudaEvent_t e : c->pev) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return SFG_OK;
@@ -561,6 +570,8 @@ extern "C" int sfg_initialize(sfg_context* c) {
     CU(dalloc(&c->d_adr_pending, nch));
     CU(dalloc(&c->d_c_fresh, nch));
     CU(dalloc(&c->d_status, 1));
+    CU(dalloc(&c->d_step_ctr, 1));
+    CU(cudaMemset(c->d_step_ctr, 0, sizeof(unsigned)));
     CU(cudaMemset(c->d_stepped, 0, sizeof(int) * nch));
     CU(cudaMemset(c->d_adr_pending, 0, sizeof(int) * nch));
     CU(cudaMemset(c->d_c_fresh, 0, sizeof(int) * nch));
@@ -578,40 +589,63 @@ extern "C" int sfg_initialize(sfg_context* c) {
 // ------------------------------------------------------------------------
 // one step
 // ------------------------------------------------------------------------
+static void mark(sfg_context* c, int phase) {
+    if (!c->profiling) return;
+    const size_t i = c->pev_phase.size();
+    if (i >= c->pev.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        c->pev.push_back(e);
+    }
+    cudaEventRecord(c->pev[i], c->stream);
+    c->pev_phase.push_back(phase);
+}
+
 template <typename S, typename R>
 static int enqueue_step_t(sfg_context* c, int p) {
     cudaStream_t st = c->stream;
     const int nch = (int)c->ch.size();
     int launches = 0;
+    mark(c, -1);
     if (c->M > 0) {
         cudaMemsetAsync(c->tb.capped, 0, sizeof(int) * nch, st);
         cudaMemsetAsync(c->tb.fluid_touched, 0, sizeof(int) * nch, st);
         launch_membrane(c->d_caps, c->NC, c->mb, c->d_has_prev, c->maxn, c->d_status, st);
+        mark(c, SFG_PHASE_MEMBRANE);
         launch_contact(c->d_chans, c->M, c->mb, c->cb, c->ncells, st);
+        mark(c, SFG_PHASE_CONTACT);
         launch_tiles(c->d_chans, c->d_caps, c->M, c->mb, c->tb, c->tb.T, p, c->d_status, st);
+        mark(c, SFG_PHASE_IBM_TILES);
         launch_spread<R>(c->d_chans, c->mb, c->tb, p, c->d_phi, 0, c->spread_grid, c->d_status, st);
+        mark(c, SFG_PHASE_IBM_SPREAD);
         launches += 1 + (c->ncells > 0 ? 7 : 1) + 9 + 1;
         for (int k = 1; k < c->Kmax; ++k) {
             launch_mdf_interp<S, R>(c->d_chans, c->M, c->mb, static_cast<const S*>(c->f[p]), c->tb,
                                     p, c->d_phi, k, st);
+            mark(c, SFG_PHASE_MDF_INTERP);
             launch_spread<R>(c->d_chans, c->mb, c->tb, p, c->d_phi, k, c->spread_grid, c->d_status,
                              st);
+            mark(c, SFG_PHASE_IBM_SPREAD);
             launches += 2;
         }
     }
     LatticeLaunch L{c->d_items, c->n_items, c->d_chans, c->f[p], c->f[1 - p], c->g[p],
                     c->g[1 - p], c->cfield, c->d_stepped, c->d_adr_pending, c->d_c_fresh,
-                    c->any_adr};
+                    c->d_step_ctr, c->any_adr};
     TileViewArgs tv{c->M > 0 ? c->tb.tile_slot[p] : nullptr,
                     c->M > 0 ? c->tb.tile_slot[1 - p] : nullptr, c->tb.fin[p], c->tb.gsnap,
                     c->tb.fin[1 - p]};
     launch_lattice_step<S, R>(L, tv, st);
+    mark(c, SFG_PHASE_LATTICE);
     k_step_flags<<<(nch + 127) / 128, 128, 0, st>>>(c->d_chans, nch, c->d_stepped,
-                                                    c->d_adr_pending, c->d_c_fresh);
+                                                    c->d_adr_pending, c->d_c_fresh,
+                                                    c->d_step_ctr);
+    mark(c, SFG_PHASE_BOOKKEEPING);
     launches += 2;
     if (c->M > 0) {
         launch_interp_move<S, R>(c->d_chans, c->M, c->mb, static_cast<const S*>(c->f[1 - p]),
                                  c->tb, p, c->d_phi, st);
+        mark(c, SFG_PHASE_INTERP_MOVE);
         launches += 1;
     }
     c->launches = launches;
@@ -650,8 +684,21 @@ extern "C" int sfg_step(sfg_context* c, int nsteps) {
     CU(cudaEventRecord(c->ev0, c->stream));
     for (int i = 0; i < nsteps; ++i) {
         const int p = (int)(c->steps & 1);
-        if (c->use_graphs) CU(cudaGraphLaunch(c->gexec[p], c->stream));
-        else enqueue_step(c, p);
+        if (c->profiling) {
+            c->pev_phase.clear();
+            enqueue_step(c, p);
+            CU(cudaStreamSynchronize(c->stream));
+            for (size_t k = 1; k < c->pev_phase.size(); ++k) {
+                float ms = 0.f;
+                CU(cudaEventElapsedTime(&ms, c->pev[k - 1], c->pev[k]));
+                const int ph = c->pev_phase[k];
+                if (ph >= 0 && ph < SFG_NUM_PHASES) c->phase_ms[ph] += ms;
+            }
+        } else if (c->use_graphs) {
+            CU(cudaGraphLaunch(c->gexec[p], c->stream));
+        } else {
+            enqueue_step(c, p);
+        }
         if (c->any_adr) {
             if (c->adr_pending_h) c->g_cur = 1 - p;
             c->adr_pending_h = true;
@@ -786,6 +833,17 @@ extern "C" int sfg_get_markers(sfg_context* c, int chi, double* pos, double* vel
     return SFG_OK;
 }
 
+extern "C" int sfg_get_all_markers(sfg_context* c, double* pos, double* vel) {
+    if (!c) return fail(SFG_ERR_ARG, "sfg_get_all_markers: null context");
+    if (!c->initialized) return fail(SFG_ERR_STATE, "sfg_get_all_markers: context not initialized");
+    if (c->M > 0) {
+        if (pos) CU(cudaMemcpyAsync(pos, c->mb.pos, sizeof(double2) * c->M, cudaMemcpyDeviceToHost, c->stream));
+        if (vel) CU(cudaMemcpyAsync(vel, c->mb.vel, sizeof(double2) * c->M, cudaMemcpyDeviceToHost, c->stream));
+    }
+    CU(cudaStreamSynchronize(c->stream));
+    return SFG_OK;
+}
+
 extern "C" int sfg_set_markers(sfg_context* c, int chi, const double* pos, const double* vel) {
     int rc = check_chan(c, chi, "sfg_set_markers");
     if (rc) return rc;
@@ -804,7 +862,8 @@ template <typename S, typename R>
 static int flush_scalar_t(sfg_context* c) {
     const int P = (int)(c->steps & 1);
     LatticeLaunch L{c->d_items, c->n_items, c->d_chans, c->f[P], nullptr, c->g[P], c->g[1 - P],
-                    c->cfield, c->d_stepped, c->d_adr_pending, c->d_c_fresh, c->any_adr};
+                    c->cfield, c->d_stepped, c->d_adr_pending, c->d_c_fresh, c->d_step_ctr,
+                    c->any_adr};
     launch_scalar_flush<S, R>(L, last_view(c), c->stream);
     const int nch = (int)c->ch.size();
     k_flush_flags<<<(nch + 127) / 128, 128, 0, c->stream>>>(nch, c->d_adr_pending, c->d_c_fresh);
@@ -916,6 +975,24 @@ extern "C" int sfg_step_count(const sfg_context* c, long long* s) {
 extern "C" int sfg_launches_per_step(const sfg_context* c, int* l) {
     if (!c || !l) return fail(SFG_ERR_ARG, "sfg_launches_per_step: null argument");
     *l = c->launches;
+    return SFG_OK;
+}
+
+extern "C" int sfg_set_profiling(sfg_context* c, int on) {
+    if (!c) return fail(SFG_ERR_ARG, "sfg_set_profiling: null context");
+    c->profiling = on != 0;
+    return SFG_OK;
+}
+
+extern "C" int sfg_get_phase_times(sfg_context* c, float* ms, int n) {
+    if (!c || !ms) return fail(SFG_ERR_ARG, "sfg_get_phase_times: null argument");
+    for (int i = 0; i < n && i < SFG_NUM_PHASES; ++i) ms[i] = c->phase_ms[i];
+    return SFG_OK;
+}
+
+extern "C" int sfg_reset_phase_times(sfg_context* c) {
+    if (!c) return fail(SFG_ERR_ARG, "sfg_reset_phase_times: null context");
+    for (int i = 0; i < SFG_NUM_PHASES; ++i) c->phase_ms[i] = 0.f;
     return SFG_OK;
 }
 

@@ -15,27 +15,60 @@
 
 namespace sfg {
 
+// FP16-shifted storage: h = (f - w_q) * 2^12 in binary16.  The power-of-two
+// scale moves the deviations (|f - w| <= ~0.6) away from the subnormal range
+// without changing their relative precision.  Stores inside the time loop
+// round stochastically: the 13 float mantissa bits below the binary16 LSB
+// are dithered with hashed bits before truncation, so rounding errors are
+// unbiased and uncorrelated between cells (round-to-nearest gives every cell
+// of a uniform row the same error, which acts as a spurious body force).
+// Values below the binary16 normal range round to nearest.
+constexpr float FP16S_SCALE = 4096.0f;
+constexpr float FP16S_UNSCALE = 1.0f / 4096.0f;
+
+__device__ __forceinline__ uint32_t mix32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+
+__device__ __forceinline__ __half f2h_stochastic(float v, uint32_t r) {
+    if (fabsf(v) < 6.103515625e-05f) return __float2half_rn(v);
+    uint32_t u = __float_as_uint(v);
+    u += r & 0x1FFFu;
+    u &= ~0x1FFFu;
+    return __float2half_rz(__uint_as_float(u));
+}
+
 template <typename S, typename R>
 struct PopIO;
 template <>
 struct PopIO<double, double> {
     static __device__ __forceinline__ double load(const double* p, int) { return __ldg(p); }
     static __device__ __forceinline__ void store(double* p, int, double v) { *p = v; }
-    static __host__ __device__ double to_host(double s, int) { return s; }
+    static __device__ __forceinline__ void store_sr(double* p, int, double v, uint32_t) { *p = v; }
 };
 template <>
 struct PopIO<float, float> {
     static __device__ __forceinline__ float load(const float* p, int) { return __ldg(p); }
     static __device__ __forceinline__ void store(float* p, int, float v) { *p = v; }
+    static __device__ __forceinline__ void store_sr(float* p, int, float v, uint32_t) { *p = v; }
 };
 template <>
 struct PopIO<__half, float> {
-    // populations stored as deviations from the rest-state weight w_q
     static __device__ __forceinline__ float load(const __half* p, int q) {
-        return float(w_of(q)) + __half2float(__ldg(p));
+        return float(w_of(q)) + __half2float(__ldg(p)) * FP16S_UNSCALE;
     }
     static __device__ __forceinline__ void store(__half* p, int q, float v) {
-        *p = __float2half_rn(v - float(w_of(q)));
+        *p = __float2half_rn((v - float(w_of(q))) * FP16S_SCALE);
+    }
+    // r: per-cell seed; each direction draws its own 13 dither bits
+    static __device__ __forceinline__ void store_sr(__half* p, int q, float v, uint32_t r) {
+        const uint32_t d = (r + (uint32_t)q * 0x9E3779B9u) * 1664525u + 1013904223u;
+        *p = f2h_stochastic((v - float(w_of(q))) * FP16S_SCALE, d >> 19);
     }
 };
 
@@ -143,7 +176,7 @@ __device__ __forceinline__ Nbr neighbours(int x, int y, int nx, int ny, int mode
 // neighbour, or reflected into the own cell when that neighbour is a wall.
 template <typename S, typename R>
 __device__ __forceinline__ void push_cell(S* __restrict__ fd, const R f[9], int x, int y, int n,
-                                          int pitch, int plane, const Nbr& b) {
+                                          int pitch, int plane, const Nbr& b, uint32_t seed) {
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
         const int cx = cx_of(q), cy = cy_of(q);
@@ -151,9 +184,9 @@ __device__ __forceinline__ void push_cell(S* __restrict__ fd, const R f[9], int 
         const int xd = cx == 0 ? x : (cx > 0 ? b.xp : b.xm);
         const int yd = cy == 0 ? y : (cy > 0 ? b.yp : b.ym);
         if (!wall)
-            PopIO<S, R>::store(fd + q * plane + yd * pitch + xd, q, f[q]);
+            PopIO<S, R>::store_sr(fd + q * plane + yd * pitch + xd, q, f[q], seed);
         else
-            PopIO<S, R>::store(fd + opp_of(q) * plane + n, opp_of(q), f[q]);
+            PopIO<S, R>::store_sr(fd + opp_of(q) * plane + n, opp_of(q), f[q], seed);
     }
 }
 
@@ -163,7 +196,7 @@ k_lattice_step(const RowItem* __restrict__ items, const ChannelDev* __restrict__
                const S* __restrict__ src, S* __restrict__ dst, const R* __restrict__ gsrc,
                R* __restrict__ gdst, const R* __restrict__ cfield, TileView tv,
                const int* __restrict__ stepped, const int* __restrict__ adr_pending,
-               const int* __restrict__ c_fresh) {
+               const int* __restrict__ c_fresh, const unsigned* __restrict__ step_ctr) {
     const RowItem it = items[blockIdx.x];
     if ((int)threadIdx.x >= it.len) return;
     const ChannelDev& ch = chans[it.chan];
@@ -190,7 +223,8 @@ k_lattice_step(const RowItem* __restrict__ items, const ChannelDev* __restrict__
         collide_bgk(f, rho, ux, uy, cf.Fx, cf.Fy, R(ch.omega));
     }
     const Nbr b = neighbours(x, y, nx, ny, ch.periodic_y ? 1 : 0);
-    push_cell<S, R>(dst + ch.f_off, f, x, y, n, pitch, plane, b);
+    const uint32_t seed = mix32((uint32_t)(ch.cell_off + n) ^ mix32(*step_ctr + 0x51ED270Bu));
+    push_cell<S, R>(dst + ch.f_off, f, x, y, n, pitch, plane, b, seed);
     if (ADR) {
         // Scalar step of the previous lattice step (it needs that step's
         // final velocity, which is only known once its populations have been
@@ -208,7 +242,7 @@ k_lattice_step(const RowItem* __restrict__ items, const ChannelDev* __restrict__
             collide_scalar(g, C, vx, vy, R(ch.omega_s));
             const int gmode = ch.periodic_y ? (ch.adr_periodic_y ? 1 : 2) : 0;
             const Nbr gb = gmode == (ch.periodic_y ? 1 : 0) ? b : neighbours(x, y, nx, ny, gmode);
-            push_cell<R, R>(gdst + ch.g_off, g, x, y, n, pitch, plane, gb);
+            push_cell<R, R>(gdst + ch.g_off, g, x, y, n, pitch, plane, gb, 0u);
         }
     }
 }
@@ -246,7 +280,8 @@ k_scalar_flush(const RowItem* __restrict__ items, const ChannelDev* __restrict__
     cell_velocity(rho, jx, jy, cf.Fx, cf.Fy, vx, vy);
     collide_scalar(g, C, vx, vy, R(ch.omega_s));
     const int gmode = ch.periodic_y ? (ch.adr_periodic_y ? 1 : 2) : 0;
-    push_cell<R, R>(gdst + ch.g_off, g, x, y, n, pitch, plane, neighbours(x, y, nx, ny, gmode));
+    push_cell<R, R>(gdst + ch.g_off, g, x, y, n, pitch, plane, neighbours(x, y, nx, ny, gmode),
+                    0u);
 }
 
 // ---- host <-> device population transfer (canonical FP64 [9][ny][nx]) ----
@@ -272,7 +307,7 @@ template <>
 __device__ __forceinline__ double pop_export_one<float>(const float* p, int) { return (double)*p; }
 template <>
 __device__ __forceinline__ double pop_export_one<__half>(const __half* p, int q) {
-    return w_of(q) + (double)__half2float(*p);
+    return w_of(q) + (double)__half2float(*p) * (double)FP16S_UNSCALE;
 }
 
 template <typename S>

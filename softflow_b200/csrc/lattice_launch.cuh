@@ -24,11 +24,12 @@ void launch_lattice_step(const LatticeLaunch& L, const TileViewArgs& tv, cudaStr
         k_lattice_step<S, R, true><<<L.n_items, 256, 0, st>>>(
             L.items, L.chans, static_cast<const S*>(L.src), static_cast<S*>(L.dst),
             static_cast<const R*>(L.gsrc), static_cast<R*>(L.gdst),
-            static_cast<const R*>(L.cfield), to_view(tv), L.stepped, L.adr_pending, L.c_fresh);
+            static_cast<const R*>(L.cfield), to_view(tv), L.stepped, L.adr_pending, L.c_fresh,
+            L.step_ctr);
     else
         k_lattice_step<S, R, false><<<L.n_items, 256, 0, st>>>(
             L.items, L.chans, static_cast<const S*>(L.src), static_cast<S*>(L.dst), nullptr,
-            nullptr, nullptr, to_view(tv), L.stepped, L.adr_pending, L.c_fresh);
+            nullptr, nullptr, to_view(tv), L.stepped, L.adr_pending, L.c_fresh, L.step_ctr);
 }
 
 template <typename S, typename R>

@@ -73,6 +73,7 @@ struct LatticeLaunch {
     const int* stepped;
     const int* adr_pending;
     const int* c_fresh;
+    const unsigned* step_ctr;   // device step counter (stochastic-rounding seed)
     bool any_adr;
 };
 struct TileViewArgs {

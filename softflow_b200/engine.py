@@ -318,6 +318,18 @@ class _Context:
         L.check(self._lib.sfg_launches_per_step(self._h, C.byref(v)))
         return v.value
 
+    def set_profiling(self, on: bool):
+        L.check(self._lib.sfg_set_profiling(self._h, int(bool(on))))
+
+    def phase_times(self) -> dict:
+        """Accumulated milliseconds per phase since the last reset."""
+        arr = (C.c_float * len(L.PHASES))()
+        L.check(self._lib.sfg_get_phase_times(self._h, arr, len(L.PHASES)))
+        return {k: float(v) for k, v in zip(L.PHASES, arr)}
+
+    def reset_phase_times(self):
+        L.check(self._lib.sfg_reset_phase_times(self._h))
+
     def stream(self) -> int:
         s = C.c_void_p()
         L.check(self._lib.sfg_get_stream(self._h, C.byref(s)))
