@@ -174,6 +174,24 @@ int sfg_get_capped_count(sfg_context* ctx, int channel, int* count);
 /* Contact pairs visited per marker in the last step (cell-list bookkeeping). */
 int sfg_get_contact_counts(sfg_context* ctx, int channel, int* counts);
 
+/* ---- standalone operators on caller buffers ------------------------------ */
+/* Spreads marker forces onto a lattice force field: the operation of
+ * ImmersedBoundary::spreadForces (reference immersed_boundary.cpp:25-100)
+ * on caller-provided DEVICE buffers, enqueued on `stream` (a cudaStream_t,
+ * NULL for the default stream).
+ *   nx, ny       lattice size; x is periodic (arc lengths use the minimum image)
+ *   ncaps        number of closed marker rings
+ *   d_offsets    [ncaps + 1] first marker of each ring, d_offsets[ncaps] = M
+ *   d_pos        [M][2] marker positions      d_force  [M][2] marker forces
+ *   d_Fx, d_Fy   [ny][nx] lattice force; the spread sum is added (F += sum)
+ *   num_markers  M
+ * Deterministic: each cell sums its contributions in ascending marker order
+ * (the reference's serial order) without floating-point atomics.  Scratch
+ * memory is taken with cudaMallocAsync on the stream and released on it. */
+int sfg_spread_forces(int nx, int ny, int ncaps, const int* d_offsets, const double* d_pos,
+                      const double* d_force, double* d_Fx, double* d_Fy, int num_markers,
+                      void* stream);
+
 /* ---- diagnostics ---------------------------------------------------------- */
 int sfg_num_channels(const sfg_context* ctx, int* n);
 int sfg_channel_counts(const sfg_context* ctx, int channel, int* num_capsules, int* num_markers);

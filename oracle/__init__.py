@@ -153,6 +153,8 @@ def _load(path: str, prefix: str):
         "capsule_centroid": (None, [C.c_void_p, C.c_int, d, d]),
         "set_concentration": (None, [C.c_void_p, d]),
         "phi": (C.c_double, [C.c_double]),
+        "spread_forces": (None, [C.c_void_p]),
+        "compute_membrane_forces": (None, [C.c_void_p]),
     }
     fns = {}
     for name, (res, args) in sig.items():
@@ -300,6 +302,27 @@ class OracleSim:
         x, y = C.c_double(), C.c_double()
         self._fn["capsule_centroid"](self._h, c, C.byref(x), C.byref(y))
         return x.value, y.value
+
+    def _view(self, name, n):
+        ptr = self._fn[name](self._h)
+        return np.ctypeslib.as_array(ptr, shape=(n,))
+
+    def set_markers(self, pos=None, vel=None, force=None):
+        """Overwrite marker state in place ([M][2] arrays)."""
+        M = self.num_markers
+        for name, arr in (("pos", pos), ("vel", vel), ("force", force)):
+            if arr is not None:
+                self._view(name, 2 * M)[:] = np.asarray(arr, dtype=np.float64).ravel()
+
+    def spread(self, clear=True):
+        """ImmersedBoundary::spreadForces on the current marker forces; returns
+        (Fx, Fy).  Only the C restatement exposes this."""
+        N = self.spec.nx * self.spec.ny
+        if clear:
+            self._view("Fx", N)[:] = 0.0
+            self._view("Fy", N)[:] = 0.0
+        self._fn["spread_forces"](self._h)
+        return self.Fx(), self.Fy()
 
     def contact_pairs(self):
         """(counts per marker, flat neighbour list) of the last contact pass."""

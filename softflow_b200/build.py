@@ -25,6 +25,7 @@ UNITS = [
     ("lattice_f64.cu", ["--fmad=false"]),
     ("lattice_f32.cu", []),
     ("markers.cu", ["--fmad=false"]),
+    ("spread_standalone.cu", ["--fmad=false"]),
     ("scan.cu", []),
     ("context.cu", []),
 ]

@@ -227,7 +227,7 @@ static void free_all(sfg_context* c) {
     F(c->mb.pos); F(c->mb.vel); F(c->mb.frc); F(c->mb.dF); F(c->mb.ds);
     F(c->mb.rest_len); F(c->mb.rest_ang); F(c->mb.rest_ds); F(c->mb.prev_len);
     F(c->mb.mk_cap); F(c->mb.mk_chan); F(c->mb.ix0); F(c->mb.iy0); F(c->mb.valid);
-    F(c->mb.pair_count);
+    F(c->mb.pair_count); F(c->mb.wx); F(c->mb.wy);
     F(c->tb.tile_chan); F(c->tb.tile_flag); F(c->tb.tile_cnt); F(c->tb.cursor);
     F(c->tb.slot_scan); F(c->tb.list_off); F(c->tb.slot_tile); F(c->tb.n_slots);
     F(c->tb.list); F(c->tb.scan_tmp); F(c->tb.acc); F(c->tb.gsnap); F(c->tb.capped);
@@ -423,13 +423,11 @@ extern "C" int sfg_initialize(sfg_context* c) {
         d.rep_damping = p.rep_damping_normal;
         d.rep_friction = p.rep_friction;
         d.rep_power = p.rep_power;
-        // lattice row segments: at most 256 cells, rounded to warps
-        const int nseg = (p.nx + 255) / 256;
-        int seg = (p.nx + nseg - 1) / nseg;
-        seg = (seg + 31) / 32 * 32;
+        // lattice work items: 32-cell row runs (one warp each)
         const int y0 = p.periodic_y ? 0 : 1, y1 = p.periodic_y ? p.ny : p.ny - 1;
         for (int y = y0; y < y1; ++y)
-            for (int x0 = 0; x0 < p.nx; x0 += seg) items.push_back({ci, y, x0, std::min(seg, p.nx - x0)});
+            for (int x0 = 0; x0 < p.nx; x0 += ITEM_CELLS)
+                items.push_back({ci, y, x0, std::min(ITEM_CELLS, p.nx - x0)});
         h.fluid_cells = (long long)p.nx * (y1 - y0);
         h.d = d;
     }
@@ -501,6 +499,8 @@ extern "C" int sfg_initialize(sfg_context* c) {
     CU(dalloc(&c->mb.iy0, M));
     CU(dalloc(&c->mb.valid, M));
     CU(dalloc(&c->mb.pair_count, M));
+    CU(dalloc(&c->mb.wx, 4LL * M));
+    CU(dalloc(&c->mb.wy, 4LL * M));
     CU(dalloc(&c->d_caps, c->NC));
     CU(dalloc(&c->d_has_prev, c->NC));
     if (M > 0) {
@@ -579,7 +579,7 @@ extern "C" int sfg_initialize(sfg_context* c) {
 
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-    c->spread_grid = std::max(1, std::min(tb.max_slots, nsm * 4));
+    c->spread_grid = std::max(1, std::min((tb.max_slots + 7) / 8, nsm * 4));
     CU(cudaStreamSynchronize(c->stream));
     c->initialized = true;
     c->steps = 0;
@@ -614,7 +614,8 @@ static int enqueue_step_t(sfg_context* c, int p) {
         mark(c, SFG_PHASE_MEMBRANE);
         launch_contact(c->d_chans, c->M, c->mb, c->cb, c->ncells, st);
         mark(c, SFG_PHASE_CONTACT);
-        launch_tiles(c->d_chans, c->d_caps, c->M, c->mb, c->tb, c->tb.T, p, c->d_status, st);
+        launch_tiles(c->d_chans, c->d_caps, c->M, c->mb, c->tb, c->tb.T, p, c->d_phi, c->d_status,
+                     st);
         mark(c, SFG_PHASE_IBM_TILES);
         launch_spread<R>(c->d_chans, c->mb, c->tb, p, c->d_phi, 0, c->spread_grid, c->d_status, st);
         mark(c, SFG_PHASE_IBM_SPREAD);

@@ -99,7 +99,9 @@ __device__ __forceinline__ CellForces<R> cell_forces(const ChannelDev& ch, int x
         const int t = ch.tile_base + (y / TILE_H) * ch.tiles_x + (x / TILE_W);
         const int cell = (y % TILE_H) * TILE_W + (x % TILE_W);
         const int s = tv.cur_slot[t];
-        const int ps = tv.prev_slot[t];
+        // the previous step's force is only read where it is used: as G
+        // without MDF, and by the scalar step
+        const int ps = (!mdf || ch.adr) ? tv.prev_slot[t] : -1;
         const R* fin = static_cast<const R*>(tv.cur_fin);
         const R* gs = static_cast<const R*>(tv.cur_G);
         const R* pfin = static_cast<const R*>(tv.prev_fin);
@@ -141,6 +143,10 @@ __device__ __forceinline__ CellForces<R> cell_forces(const ChannelDev& ch, int x
     }
     return cf;
 }
+
+// Lattice work items are 32-cell row runs, one per warp.
+constexpr int ITEM_CELLS = 32;
+constexpr int ITEMS_PER_CTA = 8;
 
 // Neighbour columns/rows of a cell and the wall flags of its two
 // neighbouring rows.  y-wall modes: 0 = SOLID rows 0 and ny-1, 1 = periodic,
@@ -192,16 +198,19 @@ __device__ __forceinline__ void push_cell(S* __restrict__ fd, const R f[9], int 
 
 template <typename S, typename R, bool ADR>
 __global__ void __launch_bounds__(256)
-k_lattice_step(const RowItem* __restrict__ items, const ChannelDev* __restrict__ chans,
+k_lattice_step(const RowItem* __restrict__ items, int n_items, const ChannelDev* __restrict__ chans,
                const S* __restrict__ src, S* __restrict__ dst, const R* __restrict__ gsrc,
                R* __restrict__ gdst, const R* __restrict__ cfield, TileView tv,
                const int* __restrict__ stepped, const int* __restrict__ adr_pending,
                const int* __restrict__ c_fresh, const unsigned* __restrict__ step_ctr) {
-    const RowItem it = items[blockIdx.x];
-    if ((int)threadIdx.x >= it.len) return;
+    const int item = blockIdx.x * ITEMS_PER_CTA + (threadIdx.x >> 5);
+    if (item >= n_items) return;
+    const RowItem it = items[item];
+    const int lane = threadIdx.x & 31;
+    if (lane >= it.len) return;
     const ChannelDev& ch = chans[it.chan];
     const int nx = ch.nx, ny = ch.ny, pitch = ch.pitch, plane = (int)ch.plane;
-    const int x = it.x0 + threadIdx.x, y = it.y;
+    const int x = it.x0 + lane, y = it.y;
     const int n = y * pitch + x;
     const S* __restrict__ fs = src + ch.f_off + n;
     R f[9];
@@ -250,16 +259,19 @@ k_lattice_step(const RowItem* __restrict__ items, const ChannelDev* __restrict__
 // Scalar step alone (brings the scalar up to date before a host read).
 template <typename S, typename R>
 __global__ void __launch_bounds__(256)
-k_scalar_flush(const RowItem* __restrict__ items, const ChannelDev* __restrict__ chans,
+k_scalar_flush(const RowItem* __restrict__ items, int n_items, const ChannelDev* __restrict__ chans,
                const S* __restrict__ src, const R* __restrict__ gsrc, R* __restrict__ gdst,
                const R* __restrict__ cfield, TileView tv_last, const int* __restrict__ adr_pending,
                const int* __restrict__ c_fresh) {
-    const RowItem it = items[blockIdx.x];
-    if ((int)threadIdx.x >= it.len) return;
+    const int item = blockIdx.x * ITEMS_PER_CTA + (threadIdx.x >> 5);
+    if (item >= n_items) return;
+    const RowItem it = items[item];
+    const int lane = threadIdx.x & 31;
+    if (lane >= it.len) return;
     const ChannelDev& ch = chans[it.chan];
     if (!ch.adr || !adr_pending[it.chan]) return;
     const int nx = ch.nx, ny = ch.ny, pitch = ch.pitch, plane = (int)ch.plane;
-    const int x = it.x0 + threadIdx.x, y = it.y;
+    const int x = it.x0 + lane, y = it.y;
     const int n = y * pitch + x;
     const S* fs = src + ch.f_off + n;
     R f[9];

@@ -20,23 +20,25 @@ inline TileView to_view(const TileViewArgs& a) {
 template <typename S, typename R>
 void launch_lattice_step(const LatticeLaunch& L, const TileViewArgs& tv, cudaStream_t st) {
     if (L.n_items == 0) return;
+    const int grid = (L.n_items + ITEMS_PER_CTA - 1) / ITEMS_PER_CTA;
     if (L.any_adr)
-        k_lattice_step<S, R, true><<<L.n_items, 256, 0, st>>>(
-            L.items, L.chans, static_cast<const S*>(L.src), static_cast<S*>(L.dst),
+        k_lattice_step<S, R, true><<<grid, 32 * ITEMS_PER_CTA, 0, st>>>(
+            L.items, L.n_items, L.chans, static_cast<const S*>(L.src), static_cast<S*>(L.dst),
             static_cast<const R*>(L.gsrc), static_cast<R*>(L.gdst),
             static_cast<const R*>(L.cfield), to_view(tv), L.stepped, L.adr_pending, L.c_fresh,
             L.step_ctr);
     else
-        k_lattice_step<S, R, false><<<L.n_items, 256, 0, st>>>(
-            L.items, L.chans, static_cast<const S*>(L.src), static_cast<S*>(L.dst), nullptr,
+        k_lattice_step<S, R, false><<<grid, 32 * ITEMS_PER_CTA, 0, st>>>(
+            L.items, L.n_items, L.chans, static_cast<const S*>(L.src), static_cast<S*>(L.dst), nullptr,
             nullptr, nullptr, to_view(tv), L.stepped, L.adr_pending, L.c_fresh, L.step_ctr);
 }
 
 template <typename S, typename R>
 void launch_scalar_flush(const LatticeLaunch& L, const TileViewArgs& tv_last, cudaStream_t st) {
     if (L.n_items == 0 || !L.any_adr) return;
-    k_scalar_flush<S, R><<<L.n_items, 256, 0, st>>>(
-        L.items, L.chans, static_cast<const S*>(L.src), static_cast<const R*>(L.gsrc),
+    k_scalar_flush<S, R><<<(L.n_items + ITEMS_PER_CTA - 1) / ITEMS_PER_CTA,
+                           32 * ITEMS_PER_CTA, 0, st>>>(
+        L.items, L.n_items, L.chans, static_cast<const S*>(L.src), static_cast<const R*>(L.gsrc),
         static_cast<R*>(L.gdst), static_cast<const R*>(L.cfield), to_view(tv_last),
         L.adr_pending, L.c_fresh);
 }

@@ -421,8 +421,8 @@ __device__ __forceinline__ int stencil_tiles(const ChannelDev& ch, int ix0, int 
 // 164-173), stencil origin, validity, and the tile occupancy counts.
 __global__ void k_ibm_prep(const ChannelDev* __restrict__ chans,
                            const CapsuleDev* __restrict__ caps, int M, MarkerBufs mb,
-                           int* __restrict__ tile_flag, int* __restrict__ tile_cnt,
-                           unsigned* status) {
+                           const double* __restrict__ phi_tbl, int* __restrict__ tile_flag,
+                           int* __restrict__ tile_cnt, unsigned* status) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
     const ChannelDev& ch = chans[mb.mk_chan[m]];
@@ -453,6 +453,12 @@ __global__ void k_ibm_prep(const ChannelDev* __restrict__ chans,
     mb.iy0[m] = iy0;
     mb.valid[m] = ok;
     if (!ok) return;
+    // Peskin weights of the stencil, evaluated once per step (delta_function.h:44-59)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        mb.wx[4 * m + k] = phi_lut(phi_tbl, p.x - (double)(ix0 - 1 + k));
+        mb.wy[4 * m + k] = phi_lut(phi_tbl, p.y - (double)(iy0 - 1 + k));
+    }
     int t[8];
     const int nt = stencil_tiles(ch, ix0, iy0, t);
     for (int a = 0; a < nt; ++a) {
@@ -497,147 +503,163 @@ __device__ __forceinline__ bool stencil_ix(int jx, int ix0, int nx, int& ix) {
     return false;
 }
 
-constexpr int SPREAD_THREADS = TILE_CELLS;  // one thread per tile cell
-constexpr int SPREAD_LIST_CAP = 4096;       // markers per tile list
-constexpr int SPREAD_CHUNK = 256;
+constexpr int SPREAD_WARPS = 8;       // force tiles processed per CTA (one per warp)
+constexpr int SPREAD_LCAP = 384;      // list entries sorted in shared memory per warp
+constexpr int SPREAD_LIST_MAX = 4096; // longer lists are clamped and flagged
 
 // Deterministic spread into force tiles for MDF sweep `sweep`.  Sweep 0
 // spreads the membrane + contact forces (immersed_boundary.cpp:25-100);
-// sweep k >= 1 adds the corrections dF (:231-286).  On a channel's last
-// sweep the kernel also adds the body force on FLUID cells, applies the force
-// cap and counts capped cells (simulation.cpp:540-609), writing the final
-// tile force `fin` (real type R).
+// sweep k >= 1 adds the corrections dF (:231-286).  One warp owns one tile:
+// it sorts the tile's marker list (ascending marker index = the reference's
+// loop order), then applies the markers one after the other, 16 lanes
+// covering the 4 x 4 stencil, so every cell receives its contributions in
+// the reference's order.  On a channel's last sweep the warp also adds the
+// body force on FLUID cells, applies the force cap and counts capped cells
+// (simulation.cpp:540-609), writing the final tile force `fin` (type R).
 template <typename R>
-__global__ void __launch_bounds__(SPREAD_THREADS)
+__global__ void __launch_bounds__(SPREAD_WARPS * 32)
 k_spread(const ChannelDev* __restrict__ chans, const int* __restrict__ tile_chan,
          const int* __restrict__ n_slots_p, const int* __restrict__ slot_tile,
          const int* __restrict__ tile_cnt, const int* __restrict__ list_off,
-         const int* __restrict__ list, MarkerBufs mb, const double* __restrict__ phi_tbl,
-         double* __restrict__ acc, R* __restrict__ gsnap, R* __restrict__ fin, int sweep,
-         int* __restrict__ capped, int* __restrict__ fluid_touched, unsigned* status) {
-    __shared__ int s_list[SPREAD_LIST_CAP];
-    __shared__ double s_x[SPREAD_CHUNK], s_y[SPREAD_CHUNK], s_fx[SPREAD_CHUNK], s_fy[SPREAD_CHUNK],
-        s_ds[SPREAD_CHUNK];
-    __shared__ int s_ix0[SPREAD_CHUNK], s_iy0[SPREAD_CHUNK], s_ok[SPREAD_CHUNK];
-    __shared__ double s_tbl[1025];
-    __shared__ int s_red[2];
-    for (int i = threadIdx.x; i < 1025; i += blockDim.x) s_tbl[i] = phi_tbl[i];
+         int* __restrict__ list, MarkerBufs mb, double* __restrict__ acc, R* __restrict__ gsnap,
+         R* __restrict__ fin, int sweep, int* __restrict__ capped,
+         int* __restrict__ fluid_touched, unsigned* status) {
+    __shared__ double s_acc[SPREAD_WARPS][2][TILE_CELLS];
+    __shared__ int s_list[SPREAD_WARPS][SPREAD_LCAP];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double* ax = s_acc[warp][0];
+    double* ay = s_acc[warp][1];
+    int* sl = s_list[warp];
     const int n_slots = *n_slots_p;
-    const int tid = threadIdx.x;
-    const int lx = tid % TILE_W, ly = tid / TILE_W;
-    for (int slot = blockIdx.x; slot < n_slots; slot += gridDim.x) {
+    const int sx = lane & 3, sy = (lane >> 2) & 3;
+    for (int slot = blockIdx.x * SPREAD_WARPS + warp; slot < n_slots;
+         slot += gridDim.x * SPREAD_WARPS) {
         const int t = slot_tile[slot];
-        const ChannelDev& ch = chans[tile_chan[t]];
+        const int chan = tile_chan[t];
+        const ChannelDev& ch = chans[chan];
         const int K = ch.ibm_iterations > 1 ? ch.ibm_iterations : 1;
-        if (sweep >= K) continue;  // CTA-uniform
+        if (sweep >= K) continue;  // warp-uniform
+        const int nx = ch.nx, ny = ch.ny;
         const int local = t - ch.tile_base;
-        const int ty = local / ch.tiles_x, tx = local % ch.tiles_x;
-        const int jx = tx * TILE_W + lx, jy = ty * TILE_H + ly;
-        const bool active = jx < ch.nx && jy < ch.ny;
+        const int x0 = (local % ch.tiles_x) * TILE_W, y0 = (local / ch.tiles_x) * TILE_H;
         int cnt = tile_cnt[t];
-        if (cnt > SPREAD_LIST_CAP) {
-            if (tid == 0) atomicOr(status, (unsigned)ST_LIST_OVERFLOW);
-            cnt = SPREAD_LIST_CAP;
-        }
-        int pow2 = 1;
-        while (pow2 < cnt) pow2 <<= 1;
-        __syncthreads();
-        for (int i = tid; i < pow2; i += blockDim.x)
-            s_list[i] = (i < cnt) ? list[list_off[t] + i] : INT_MAX;
-        __syncthreads();
-        // bitonic sort: ascending marker index = the reference's loop order
-        for (int k = 2; k <= pow2; k <<= 1) {
-            for (int j = k >> 1; j > 0; j >>= 1) {
-                for (int i = tid; i < pow2; i += blockDim.x) {
-                    const int l = i ^ j;
-                    if (l > i) {
-                        const int a = s_list[i], b = s_list[l];
-                        const bool up = (i & k) == 0;
-                        if ((a > b) == up) { s_list[i] = b; s_list[l] = a; }
+        const int off = list_off[t];
+        const int* lst;
+        if (cnt <= SPREAD_LCAP) {
+            int pow2 = 1;
+            while (pow2 < cnt) pow2 <<= 1;
+            for (int i = lane; i < pow2; i += 32) sl[i] = i < cnt ? list[off + i] : INT_MAX;
+            __syncwarp();
+            for (int k = 2; k <= pow2; k <<= 1)
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    for (int i = lane; i < pow2; i += 32) {
+                        const int l = i ^ j;
+                        if (l > i) {
+                            const int a = sl[i], b = sl[l];
+                            if ((a > b) == ((i & k) == 0)) { sl[i] = b; sl[l] = a; }
+                        }
                     }
+                    __syncwarp();
                 }
-                __syncthreads();
+            lst = sl;
+        } else {
+            if (cnt > SPREAD_LIST_MAX) {
+                if (lane == 0) atomicOr(status, (unsigned)ST_LIST_OVERFLOW);
+                cnt = SPREAD_LIST_MAX;
             }
+            if (lane == 0) {  // long lists are rare: sort in place
+                int* a = list + off;
+                for (int i = 1; i < cnt; ++i) {
+                    const int v = a[i];
+                    int j = i - 1;
+                    while (j >= 0 && a[j] > v) { a[j + 1] = a[j]; --j; }
+                    a[j + 1] = v;
+                }
+            }
+            __syncwarp();
+            lst = list + off;
         }
-        const size_t cell = (size_t)slot * 2 * TILE_CELLS + tid;
-        double ax = 0.0, ay = 0.0;
-        if (sweep > 0) {
-            ax = acc[cell];
-            ay = acc[cell + TILE_CELLS];
-        }
+        const size_t base = (size_t)slot * 2 * TILE_CELLS;
         const bool last = (sweep == K - 1);
-        if (last && K > 1) {
-            gsnap[cell] = (R)ax;
-            gsnap[cell + TILE_CELLS] = (R)ay;
-        }
-        for (int c0 = 0; c0 < cnt; c0 += SPREAD_CHUNK) {
-            const int nc = min(SPREAD_CHUNK, cnt - c0);
-            __syncthreads();
-            if (tid < nc) {
-                const int m = s_list[c0 + tid];
-                const double2 p = mb.pos[m];
-                const double2 f = sweep == 0 ? mb.frc[m] : mb.dF[m];
-                s_x[tid] = p.x;
-                s_y[tid] = p.y;
-                s_fx[tid] = f.x;
-                s_fy[tid] = f.y;
-                s_ds[tid] = mb.ds[m];
-                s_ix0[tid] = mb.ix0[m];
-                s_iy0[tid] = mb.iy0[m];
-                s_ok[tid] = !(isnan(f.x) || isnan(f.y));
+        for (int c = lane; c < TILE_CELLS; c += 32) {
+            const double vx = sweep > 0 ? acc[base + c] : 0.0;
+            const double vy = sweep > 0 ? acc[base + TILE_CELLS + c] : 0.0;
+            ax[c] = vx;
+            ay[c] = vy;
+            if (last && K > 1) {
+                gsnap[base + c] = (R)vx;
+                gsnap[base + TILE_CELLS + c] = (R)vy;
             }
-            __syncthreads();
-            if (active) {
-                for (int i = 0; i < nc; ++i) {
-                    if (!s_ok[i]) continue;
-                    const int dyc = jy - s_iy0[i];
-                    if (dyc < -1 || dyc > 2) continue;
-                    int ix;
-                    if (!stencil_ix(jx, s_ix0[i], ch.nx, ix)) continue;
-                    const double rx = s_x[i] - (double)ix, ry = s_y[i] - (double)jy;
-                    const double w = phi_lut(s_tbl, rx) * phi_lut(s_tbl, ry);
-                    if (w > 1e-15) {
-                        ax += s_fx[i] * w * s_ds[i];
-                        ay += s_fy[i] * w * s_ds[i];
+        }
+        __syncwarp();
+        for (int i = 0; i < cnt; ++i) {
+            const int m = lst[i];
+            if (lane < 16) {
+                const double2 fo = sweep == 0 ? mb.frc[m] : mb.dF[m];
+                if (!(isnan(fo.x) || isnan(fo.y))) {
+                    const int iy = mb.iy0[m] - 1 + sy;
+                    int jx = mb.ix0[m] - 1 + sx;
+                    if (jx < 0) jx += nx;
+                    if (jx >= nx) jx -= nx;
+                    const int cxl = jx - x0, cyl = iy - y0;
+                    if (iy >= 0 && iy < ny && cxl >= 0 && cxl < TILE_W && cyl >= 0 &&
+                        cyl < TILE_H) {
+                        const double w = mb.wx[4 * m + sx] * mb.wy[4 * m + sy];
+                        if (w > 1e-15) {
+                            const double ds = mb.ds[m];
+                            const int c = cyl * TILE_W + cxl;
+                            ax[c] += fo.x * w * ds;
+                            ay[c] += fo.y * w * ds;
+                        }
                     }
                 }
             }
+            __syncwarp();
         }
         if (!last) {
-            acc[cell] = ax;
-            acc[cell + TILE_CELLS] = ay;
+            for (int c = lane; c < TILE_CELLS; c += 32) {
+                acc[base + c] = ax[c];
+                acc[base + TILE_CELLS + c] = ay[c];
+            }
+            __syncwarp();
             continue;
         }
         // finalize: body force on FLUID cells, then the force cap
-        if (tid == 0) { s_red[0] = 0; s_red[1] = 0; }
-        __syncthreads();
-        if (active) {
-            const bool fluid = ch.periodic_y || (jy != 0 && jy != ch.ny - 1);
-            if (fluid && (ch.body_fx != 0.0 || ch.body_fy != 0.0)) {
-                ax += ch.body_fx;
-                ay += ch.body_fy;
+        int n_cap = 0, n_fluid = 0;
+        const double Fm = ch.max_force, Fm2 = Fm * Fm;
+        const bool body = (ch.body_fx != 0.0 || ch.body_fy != 0.0);
+        for (int c = lane; c < TILE_CELLS; c += 32) {
+            const int jx = x0 + (c % TILE_W), jy = y0 + (c / TILE_W);
+            double vx = ax[c], vy = ay[c];
+            if (jx < nx && jy < ny) {
+                const bool fluid = ch.periodic_y || (jy != 0 && jy != ny - 1);
+                if (fluid && body) {
+                    vx += ch.body_fx;
+                    vy += ch.body_fy;
+                }
+                const double f2 = vx * vx + vy * vy;
+                if (f2 > Fm2) {
+                    const double sc = Fm / sqrt(f2);
+                    vx *= sc;
+                    vy *= sc;
+                    ++n_cap;
+                }
+                n_fluid += fluid ? 1 : 0;
             }
-            const double Fm = ch.max_force, Fm2 = Fm * Fm;
-            const double f2 = ax * ax + ay * ay;
-            int cap_here = 0;
-            if (f2 > Fm2) {
-                const double sc = Fm / sqrt(f2);
-                ax *= sc;
-                ay *= sc;
-                cap_here = 1;
-            }
-            if (cap_here) atomicAdd(&s_red[0], 1);
-            if (fluid) atomicAdd(&s_red[1], 1);
+            acc[base + c] = vx;
+            acc[base + TILE_CELLS + c] = vy;
+            fin[base + c] = (R)vx;
+            fin[base + TILE_CELLS + c] = (R)vy;
         }
-        acc[cell] = ax;
-        acc[cell + TILE_CELLS] = ay;
-        fin[cell] = (R)ax;
-        fin[cell + TILE_CELLS] = (R)ay;
-        __syncthreads();
-        if (tid == 0) {
-            if (s_red[0]) atomicAdd(&capped[tile_chan[t]], s_red[0]);
-            if (s_red[1]) atomicAdd(&fluid_touched[tile_chan[t]], s_red[1]);
+        for (int o = 16; o > 0; o >>= 1) {
+            n_cap += __shfl_down_sync(0xffffffffu, n_cap, o);
+            n_fluid += __shfl_down_sync(0xffffffffu, n_fluid, o);
         }
+        if (lane == 0) {
+            if (n_cap) atomicAdd(&capped[chan], n_cap);
+            if (n_fluid) atomicAdd(&fluid_touched[chan], n_fluid);
+        }
+        __syncwarp();
     }
 }
 
@@ -689,7 +711,7 @@ __global__ void k_mdf_interp(const ChannelDev* __restrict__ chans, int M, Marker
             if (jx >= ch.nx) jx -= ch.nx;
             const int jy = iy;
             if (jy < 0 || jy >= ch.ny || jx < 0 || jx >= ch.nx) continue;
-            const double w = phi_lut(phi_tbl, p.x - (double)ix) * phi_lut(phi_tbl, p.y - (double)iy);
+            const double w = mb.wx[4 * m + (ix - ix0 + 1)] * mb.wy[4 * m + (iy - iy0 + 1)];
             if (w > 1e-15) {
                 double rho, jxm, jym;
                 bool solid;
@@ -739,8 +761,7 @@ __global__ void k_interp_move(const ChannelDev* __restrict__ chans, int M, Marke
                 if (jx >= ch.nx) jx -= ch.nx;
                 const int jy = iy;
                 if (jy < 0 || jy >= ch.ny || jx < 0 || jx >= ch.nx) continue;
-                const double w =
-                    phi_lut(phi_tbl, p.x - (double)ix) * phi_lut(phi_tbl, p.y - (double)iy);
+                const double w = mb.wx[4 * m + (ix - ix0 + 1)] * mb.wy[4 * m + (iy - iy0 + 1)];
                 if (w > 1e-15) {
                     double rho, jxm, jym;
                     bool solid;
@@ -820,12 +841,13 @@ void launch_contact(const ChannelDev* chans, int M, const MarkerBufs& mb, Contac
 }
 
 void launch_tiles(const ChannelDev* chans, const CapsuleDev* caps, int M, const MarkerBufs& mb,
-                  TileBufs& tb, int T, int parity, unsigned* status, cudaStream_t st) {
+                  TileBufs& tb, int T, int parity, const double* phi_tbl, unsigned* status,
+                  cudaStream_t st) {
     const int B = 256, G = (M + B - 1) / B;
     cudaMemsetAsync(tb.tile_flag, 0, sizeof(int) * T, st);
     cudaMemsetAsync(tb.tile_cnt, 0, sizeof(int) * T, st);
     cudaMemsetAsync(tb.cursor, 0, sizeof(int) * T, st);
-    k_ibm_prep<<<G, B, 0, st>>>(chans, caps, M, mb, tb.tile_flag, tb.tile_cnt, status);
+    k_ibm_prep<<<G, B, 0, st>>>(chans, caps, M, mb, phi_tbl, tb.tile_flag, tb.tile_cnt, status);
     scan_exclusive(tb.tile_flag, tb.slot_scan, T, tb.scan_tmp, tb.n_slots, st);
     scan_exclusive(tb.tile_cnt, tb.list_off, T, tb.scan_tmp, nullptr, st);
     k_tile_slots<<<(T + B - 1) / B, B, 0, st>>>(T, tb.tile_flag, tb.slot_scan,
@@ -836,10 +858,11 @@ void launch_tiles(const ChannelDev* chans, const CapsuleDev* caps, int M, const 
 template <typename R>
 void launch_spread(const ChannelDev* chans, const MarkerBufs& mb, TileBufs& tb, int parity,
                    const double* phi_tbl, int sweep, int grid, unsigned* status, cudaStream_t st) {
-    k_spread<R><<<grid, SPREAD_THREADS, 0, st>>>(
+    (void)phi_tbl;
+    k_spread<R><<<grid, SPREAD_WARPS * 32, 0, st>>>(
         chans, tb.tile_chan, tb.n_slots, tb.slot_tile, tb.tile_cnt, tb.list_off, tb.list, mb,
-        phi_tbl, tb.acc, static_cast<R*>(tb.gsnap), static_cast<R*>(tb.fin[parity]), sweep,
-        tb.capped, tb.fluid_touched, status);
+        tb.acc, static_cast<R*>(tb.gsnap), static_cast<R*>(tb.fin[parity]), sweep, tb.capped,
+        tb.fluid_touched, status);
 }
 template void launch_spread<double>(const ChannelDev*, const MarkerBufs&, TileBufs&, int,
                                     const double*, int, int, unsigned*, cudaStream_t);

@@ -28,6 +28,8 @@ struct MarkerBufs {
     int* iy0;
     int* valid;         // finite position with its stencil rows near the lattice
     int* pair_count;    // contact pairs visited per marker (bookkeeping)
+    double* wx;         // [M][4] phi(x - ix) for ix = ix0-1 .. ix0+2 (this step)
+    double* wy;         // [M][4] phi(y - iy) for iy = iy0-1 .. iy0+2
 };
 
 // ---------------- Peskin 4-point delta via the 1024-bin table --------------

@@ -49,7 +49,8 @@ void launch_membrane(const CapsuleDev* caps, int ncaps, const MarkerBufs& mb, in
 void launch_contact(const ChannelDev* chans, int M, const MarkerBufs& mb, ContactBufs& cb,
                     int ncells, cudaStream_t st);
 void launch_tiles(const ChannelDev* chans, const CapsuleDev* caps, int M, const MarkerBufs& mb,
-                  TileBufs& tb, int T, int parity, unsigned* status, cudaStream_t st);
+                  TileBufs& tb, int T, int parity, const double* phi_tbl, unsigned* status,
+                  cudaStream_t st);
 template <typename R>
 void launch_spread(const ChannelDev* chans, const MarkerBufs& mb, TileBufs& tb, int parity,
                    const double* phi_tbl, int sweep, int grid, unsigned* status, cudaStream_t st);

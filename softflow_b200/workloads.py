@@ -12,12 +12,15 @@ c3  256 independent channels drawn from seed 7: nx in {200, 208, ..., 800},
     G_s log-uniform in [0.01, 0.1], tau uniform in [0.6, 1.0], fx uniform in
     [1e-5, 5e-5]; regularized collision, 5 MDF sweeps.  Channel i places its
     capsules from seed fnv1a64(str(i)) & 0x7fffffff with centres in
-    x [0, nx), y [8, ny - 8].
+    x [8, nx - 8], y [8, ny - 8].
 
-Centres are kept WALL_MARGIN = 8 lu from the walls (configuration 1 keeps
-them 10 lu away).  Capsules seeded against a wall have nodes inside the
-y-clamp band, and with multi-direct forcing the reference algorithm itself
-diverges on such channels within a few hundred steps.
+Centres are kept MARGIN = 8 lu from the walls and from the periodic seam
+(configuration 1 keeps them 10 lu from the walls and 20 lu from the seam).
+The reference placement tests overlap with the plain distance between
+centres, without the periodic image, so capsules seeded at both ends of a
+channel can overlap across the seam; capsules seeded against a wall have
+nodes inside the y-clamp band.  With multi-direct forcing the reference
+algorithm diverges within a few steps on channels seeded either way.
 
 Membrane constants not fixed by the configuration use the reference Python
 API defaults (C_skalak 10, k_area 0.5, k_perimeter 0.1, gamma 0.01,
@@ -83,14 +86,14 @@ def plan_c1(precision="fp32") -> List[ChannelPlan]:
     return [ChannelPlan(p, [(30, 20, 10, 380, 70, 3.0, 24, skalak(), 42)])]
 
 
-WALL_MARGIN = 8
+MARGIN = 8
 
 
 def plan_c2(precision="fp32") -> List[ChannelPlan]:
     p = channel_params(4096, 1024, CollisionModel.MRT, 0.8, 1e-5, 1, precision, scalar_D=0.05)
-    m = WALL_MARGIN
-    return [ChannelPlan(p, [(1000, 0, m, 4096, 1024 - m, 6.0, 48, wlc_helfrich(), 11),
-                            (1000, 0, m, 4096, 1024 - m, 3.0, 24, skalak(), 12)],
+    m = MARGIN
+    return [ChannelPlan(p, [(1000, m, m, 4096 - m, 1024 - m, 6.0, 48, wlc_helfrich(), 11),
+                            (1000, m, m, 4096 - m, 1024 - m, 3.0, 24, skalak(), 12)],
                         gaussian=(2048.0, 511.5, 20.0))]
 
 
@@ -106,8 +109,8 @@ def plan_c3(precision="fp32", n_channels=256, ibm_iterations=5) -> List[ChannelP
         fx = float(rng.uniform(1e-5, 5e-5))
         p = channel_params(nx, ny, CollisionModel.REGULARIZED, tau, fx, ibm_iterations, precision)
         seed = fnv1a64(str(i)) & 0x7FFFFFFF
-        m = WALL_MARGIN
-        plans.append(ChannelPlan(p, [(ncap, 0, m, nx, ny - m, 3.0, 24, skalak(G_s), seed)]))
+        m = MARGIN
+        plans.append(ChannelPlan(p, [(ncap, m, m, nx - m, ny - m, 3.0, 24, skalak(G_s), seed)]))
     return plans
 
 
