@@ -192,6 +192,23 @@ int sfg_spread_forces(int nx, int ny, int ncaps, const int* d_offsets, const dou
                       const double* d_force, double* d_Fx, double* d_Fy, int num_markers,
                       void* stream);
 
+/* The spread of sfg_spread_forces for callers that cannot allocate device
+ * memory inside a call (a host engine or framework that owns the device
+ * memory budget through its own pool, or a loop that must not stall on
+ * cudaMalloc / cudaFree).  No counterpart in the reference, which runs on the
+ * CPU.  It allocates nothing: its scratch is a fixed 2 MiB device array held
+ * by every GPU that loads the library until the process exits.
+ * Limits: num_markers <= 32768 and ceil(nx/32) * ceil(ny/8) <= 32768 force
+ * tiles; larger calls return SFG_ERR_CAPACITY.  All calls share the array:
+ * calls whose GPU work overlaps (other streams or host threads on the same
+ * device) race and must be serialized by the caller.  The first call on each
+ * device looks up the array's device address with that device current; make
+ * it before any stream capture on that device.  Results equal
+ * sfg_spread_forces bit for bit. */
+int sfg_spread_forces_noalloc(int nx, int ny, int ncaps, const int* d_offsets,
+                              const double* d_pos, const double* d_force, double* d_Fx,
+                              double* d_Fy, int num_markers, void* stream);
+
 /* ---- diagnostics ---------------------------------------------------------- */
 int sfg_num_channels(const sfg_context* ctx, int* n);
 int sfg_channel_counts(const sfg_context* ctx, int channel, int* num_capsules, int* num_markers);

@@ -101,6 +101,9 @@ SIGNATURES = {
     "sfg_get_stream": (C.c_int, [C.c_void_p, _P(C.c_void_p)]),
     "sfg_spread_forces": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "sfg_spread_forces_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                            C.c_void_p]),
     "sfg_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "sfg_get_phase_times": (C.c_int, [C.c_void_p, _P(C.c_float), C.c_int]),
     "sfg_reset_phase_times": (C.c_int, [C.c_void_p]),

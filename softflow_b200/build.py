@@ -26,6 +26,7 @@ UNITS = [
     ("lattice_f32.cu", []),
     ("markers.cu", ["--fmad=false"]),
     ("spread_standalone.cu", ["--fmad=false"]),
+    ("spread_noalloc.cu", []),
     ("scan.cu", []),
     ("context.cu", []),
 ]
