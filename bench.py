@@ -58,7 +58,7 @@ def parse():
 
 
 # ---------------------------------------------------------------- ranks ----
-def dist_setup(args):
+def dist_setup(args, backend="nccl"):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -67,26 +67,45 @@ def dist_setup(args):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
         pg = dist
     return world, rank, local, pg
 
 
 def barrier(pg, local):
-    if pg is not None:
-        import torch
+    if pg is None:
+        return
+    import torch
+    if pg.get_backend() == "nccl":
         pg.barrier(device_ids=[local])
         torch.cuda.synchronize()
+    else:
+        pg.barrier()
 
 
 def allmax(pg, v: float) -> float:
+    """Max over ranks (timings are taken as the slowest rank's)."""
     if pg is None:
         return v
     import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
+
+
+def make_plans(workload, precision, world=1, rank=0):
+    """Work of one rank.  The ensemble is sharded: rank r runs channels
+    [256 r, 256 (r + 1)) of one seeded sequence, so every rank has a distinct
+    256-channel ensemble (weak scaling, no data-path collective).  The
+    single-channel workloads run one replica per rank."""
+    from softflow_b200 import workloads as W
+    if workload == "c3":
+        per = 256
+        return W.plan_c3(precision, n_channels=per * world)[per * rank: per * (rank + 1)]
+    return W.PLANS[workload](precision)
 
 
 # --------------------------------------------------------------- clocks ----
@@ -164,7 +183,7 @@ def run_product(args, world, rank, local, pg):
     import numpy as np
     import softflow_b200 as S
     from softflow_b200 import workloads as W
-    plans = W.PLANS[args.workload](args.precision)
+    plans = make_plans(args.workload, args.precision, world, rank)
     ens = W.build(plans, precision=args.precision, device=local)
     ctx = ens.context()
     cells, caps, markers, scal = W.totals(plans, ens)
@@ -231,7 +250,8 @@ def run_product(args, world, rank, local, pg):
                    "mdf_sweeps": max(p.params.ibm_iterations for p in plans),
                    "l2": "state larger than L2 (no flush needed)" if alg_bytes > 126e6
                          else "state fits L2 (L2-resident workload)",
-                   "parallelism": f"replicas x{world} (independent channels)"},
+                   "parallelism": (f"channel shards x{world} (256 distinct channels per rank)"
+                                   if args.workload == "c3" else f"replicas x{world}")},
         "mlups": mlups,
         "marker_updates_per_s": mk_upd,
         "gpu_launches": launches * args.steps,

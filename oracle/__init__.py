@@ -324,6 +324,13 @@ class OracleSim:
         self._fn["spread_forces"](self._h)
         return self.Fx(), self.Fy()
 
+    def compute_membrane(self):
+        """Capsule::computeMembraneForces on the current state (forces cleared
+        first); the result is in forces()."""
+        M = self.num_markers
+        self._view("force", 2 * M)[:] = 0.0
+        self._fn["compute_membrane_forces"](self._h)
+
     def contact_pairs(self):
         """(counts per marker, flat neighbour list) of the last contact pass."""
         M = self.num_markers

@@ -173,3 +173,28 @@ def test_runs_are_deterministic(sfg):
     b.run(30)
     assert np.array_equal(a.field().distributions(), b.field().distributions())
     assert np.array_equal(a.capsules().positions(), b.capsules().positions())
+
+
+@pytest.mark.parametrize("name", ["bgk_small", "mrt_small", "reg_small", "seam_single",
+                                  "contact_brute", "mini_c2", "c1"])
+def test_fp64_matches_reference_golden(sfg, name):
+    """Against outputs of the reference's own sources (tests/golden)."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                             f"{name}.npz"))
+    case = CASES[name]
+    sim = build_gpu(case, "fp64")
+    sim.run(int(g["steps"]))
+    a = _state(sim)
+    rows = fluid_rows(case)
+    if "f" in g:      # lattice only: bit for bit
+        assert np.array_equal(a["f"][:, rows], g["f"])
+        assert np.array_equal(a["ux"], g["ux"]) and np.array_equal(a["uy"], g["uy"])
+    else:
+        for k in ("ux", "uy", "rho"):
+            assert rel_l2(a[k][rows], g[k][rows]) < 1e-9, k
+        assert np.max(np.abs(a["pos"] - g["pos"])) < 1e-9
+        assert rel_l2(a["frc"], g["force"]) < 1e-8
+    assert sim.lastCappedNodes() == int(g["capped"])
+    if "C" in g:
+        assert rel_l2(sim.advectionDiffusion().concentration(), g["C"]) < 1e-9
