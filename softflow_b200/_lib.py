@@ -105,6 +105,7 @@ SIGNATURES = {
                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                             C.c_void_p]),
     "sfg_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+    "sfg_set_lattice_variant": (C.c_int, [C.c_void_p, C.c_int]),
     "sfg_get_phase_times": (C.c_int, [C.c_void_p, _P(C.c_float), C.c_int]),
     "sfg_reset_phase_times": (C.c_int, [C.c_void_p]),
 }

@@ -29,6 +29,14 @@ __device__ __forceinline__ void cell_velocity(R rho, R jx, R jy, R Gx, R Gy, R& 
         uy = R(0);
     }
 }
+// FP32 form: one correctly rounded reciprocal and two products.
+template <>
+__device__ __forceinline__ void cell_velocity<float>(float rho, float jx, float jy, float Gx,
+                                                     float Gy, float& ux, float& uy) {
+    const float inv = rho > 1e-15f ? __frcp_rn(rho) : 0.0f;
+    ux = (jx + 0.5f * Gx) * inv;
+    uy = (jy + 0.5f * Gy) * inv;
+}
 
 template <typename R>
 __device__ __forceinline__ void collide_bgk(R f[9], R r, R vx, R vy, R fx, R fy, R om) {

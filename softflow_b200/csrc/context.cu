@@ -141,6 +141,9 @@ struct sfg_context {
     ChannelDev* d_chans = nullptr;
     RowItem* d_items = nullptr;
     int n_items = 0;
+    RowItem* d_items4 = nullptr;
+    int n_items4 = 0;
+    bool use_vec4 = false;
     void* f[2] = {nullptr, nullptr};
     void* g[2] = {nullptr, nullptr};
     void* cfield = nullptr;
@@ -161,12 +164,15 @@ struct sfg_context {
     double* d_io = nullptr;
     size_t io_doubles = 0;
     int spread_grid = 0;
+    int persistent_ctas = 296;
+    int shared_collision = -1;
 
     long long steps = 0;
     bool adr_pending_h = false;
     int g_cur = 0;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     bool use_graphs = true;
+    bool force_scalar_lattice = false;  // diagnostics: use the one-cell-per-thread kernel
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int launches = 0;
     // per-phase timing (profiling mode runs the step eagerly)
@@ -178,6 +184,14 @@ struct sfg_context {
     size_t elem_size() const { return precision == SFG_FP64 ? 8 : (precision == SFG_FP32 ? 4 : 2); }
     size_t real_size() const { return precision == SFG_FP64 ? 8 : 4; }
 };
+
+namespace sfg {
+int lattice_ctas_per_sm(int precision, bool adr) {
+    if (precision == SFG_FP64) return lattice_ctas_per_sm_t<double, double>(adr);
+    if (precision == SFG_FP32) return lattice_ctas_per_sm_t<float, float>(adr);
+    return lattice_ctas_per_sm_t<__half, float>(adr);
+}
+}  // namespace sfg
 
 // ------------------------------------------------------------------------
 // library
@@ -222,6 +236,7 @@ static void free_all(sfg_context* c) {
     F(c->cfield);
     F(c->d_chans);
     F(c->d_items);
+    F(c->d_items4);
     F(c->d_caps);
     F(c->d_has_prev);
     F(c->mb.pos); F(c->mb.vel); F(c->mb.frc); F(c->mb.dF); F(c->mb.ds);
@@ -312,8 +327,9 @@ extern "C" int sfg_initialize(sfg_context* c) {
     const int nch = (int)c->ch.size();
     long long cell_off = 0;
     int tile_base = 0, cell_base = 0, cap_base = 0, mk_base = 0;
-    std::vector<RowItem> items;
+    std::vector<RowItem> items, items4;
     std::vector<CapsuleDev> caps;
+    bool all_vec4 = true;
     std::vector<double> pos, rest_len, rest_ang, rest_ds;
     std::vector<int> mk_cap, mk_chan, tile_chan;
     c->any_adr = false;
@@ -428,6 +444,10 @@ extern "C" int sfg_initialize(sfg_context* c) {
         for (int y = y0; y < y1; ++y)
             for (int x0 = 0; x0 < p.nx; x0 += ITEM_CELLS)
                 items.push_back({ci, y, x0, std::min(ITEM_CELLS, p.nx - x0)});
+        if (p.nx % 4 != 0) all_vec4 = false;
+        for (int y = y0; y < y1; ++y)
+            for (int x0 = 0; x0 < p.nx; x0 += VEC_RUN)
+                items4.push_back({ci, y, x0, std::min(VEC_RUN, p.nx - x0)});
         h.fluid_cells = (long long)p.nx * (y1 - y0);
         h.d = d;
     }
@@ -446,6 +466,14 @@ extern "C" int sfg_initialize(sfg_context* c) {
     CU(cudaMemcpy(c->d_chans, dch.data(), sizeof(ChannelDev) * nch, cudaMemcpyHostToDevice));
     CU(dalloc(&c->d_items, items.size()));
     CU(cudaMemcpy(c->d_items, items.data(), sizeof(RowItem) * items.size(), cudaMemcpyHostToDevice));
+    c->use_vec4 = all_vec4 && !c->force_scalar_lattice;
+    c->shared_collision = c->ch[0].p.collision;
+    for (const ChanHost& h : c->ch)
+        if (h.p.collision != c->shared_collision) c->shared_collision = -1;
+    c->n_items4 = (int)items4.size();
+    CU(dalloc(&c->d_items4, items4.size()));
+    CU(cudaMemcpy(c->d_items4, items4.data(), sizeof(RowItem) * items4.size(),
+                  cudaMemcpyHostToDevice));
 
     // populations
     const size_t nelem = 9 * (size_t)cell_off;
@@ -580,6 +608,7 @@ extern "C" int sfg_initialize(sfg_context* c) {
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
     c->spread_grid = std::max(1, std::min((tb.max_slots + 7) / 8, nsm * 4));
+    c->persistent_ctas = nsm * lattice_ctas_per_sm(c->precision, c->any_adr);
     CU(cudaStreamSynchronize(c->stream));
     c->initialized = true;
     c->steps = 0;
@@ -632,7 +661,8 @@ static int enqueue_step_t(sfg_context* c, int p) {
     }
     LatticeLaunch L{c->d_items, c->n_items, c->d_chans, c->f[p], c->f[1 - p], c->g[p],
                     c->g[1 - p], c->cfield, c->d_stepped, c->d_adr_pending, c->d_c_fresh,
-                    c->d_step_ctr, c->any_adr};
+                    c->d_step_ctr, c->any_adr, c->d_items4, c->n_items4, c->use_vec4,
+                    c->persistent_ctas, c->shared_collision};
     TileViewArgs tv{c->M > 0 ? c->tb.tile_slot[p] : nullptr,
                     c->M > 0 ? c->tb.tile_slot[1 - p] : nullptr, c->tb.fin[p], c->tb.gsnap,
                     c->tb.fin[1 - p]};
@@ -864,7 +894,7 @@ static int flush_scalar_t(sfg_context* c) {
     const int P = (int)(c->steps & 1);
     LatticeLaunch L{c->d_items, c->n_items, c->d_chans, c->f[P], nullptr, c->g[P], c->g[1 - P],
                     c->cfield, c->d_stepped, c->d_adr_pending, c->d_c_fresh, c->d_step_ctr,
-                    c->any_adr};
+                    c->any_adr, c->d_items4, c->n_items4, false, 0, -1};
     launch_scalar_flush<S, R>(L, last_view(c), c->stream);
     const int nch = (int)c->ch.size();
     k_flush_flags<<<(nch + 127) / 128, 128, 0, c->stream>>>(nch, c->d_adr_pending, c->d_c_fresh);
@@ -994,6 +1024,14 @@ extern "C" int sfg_get_phase_times(sfg_context* c, float* ms, int n) {
 extern "C" int sfg_reset_phase_times(sfg_context* c) {
     if (!c) return fail(SFG_ERR_ARG, "sfg_reset_phase_times: null context");
     for (int i = 0; i < SFG_NUM_PHASES; ++i) c->phase_ms[i] = 0.f;
+    return SFG_OK;
+}
+
+extern "C" int sfg_set_lattice_variant(sfg_context* c, int variant) {
+    if (!c) return fail(SFG_ERR_ARG, "sfg_set_lattice_variant: null context");
+    if (c->initialized) return fail(SFG_ERR_STATE, "sfg_set_lattice_variant: before sfg_initialize");
+    if (variant < 0 || variant > 1) return fail(SFG_ERR_ARG, "sfg_set_lattice_variant: 0 or 1");
+    c->force_scalar_lattice = variant == 1;
     return SFG_OK;
 }
 

@@ -36,11 +36,11 @@ __device__ __forceinline__ uint32_t mix32(uint32_t x) {
 }
 
 __device__ __forceinline__ __half f2h_stochastic(float v, uint32_t r) {
-    if (fabsf(v) < 6.103515625e-05f) return __float2half_rn(v);
-    uint32_t u = __float_as_uint(v);
-    u += r & 0x1FFFu;
-    u &= ~0x1FFFu;
-    return __float2half_rz(__uint_as_float(u));
+    // branch-free: both roundings, then a select
+    const uint32_t u = (__float_as_uint(v) + (r & 0x1FFFu)) & ~0x1FFFu;
+    const __half hs = __float2half_rz(__uint_as_float(u));
+    const __half hn = __float2half_rn(v);
+    return fabsf(v) < 6.103515625e-05f ? hn : hs;
 }
 
 template <typename S, typename R>
@@ -253,6 +253,388 @@ k_lattice_step(const RowItem* __restrict__ items, int n_items, const ChannelDev*
             const Nbr gb = gmode == (ch.periodic_y ? 1 : 0) ? b : neighbours(x, y, nx, ny, gmode);
             push_cell<R, R>(gdst + ch.g_off, g, x, y, n, pitch, plane, gb, 0u);
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Vectorised lattice step: each lane owns 4 consecutive cells of a row, loads
+// every population plane with one aligned vector load (16 B for FP32, 8 B for
+// FP16-shifted, 2 x 16 B for FP64), collides the 4 cells, and stores.  Planes
+// without an x shift (q = 0, 2, 4, and every reflected population) are stored
+// as aligned vectors in place.  For the x-shifted planes the lane takes the
+// one value that crosses its 4-cell boundary from its neighbour with a warp
+// shuffle, so these stores are aligned vectors too; only the ends of each
+// 128-cell run use narrow stores.  Needs nx % 4 == 0.
+// ---------------------------------------------------------------------------
+constexpr int VEC_RUN = 128;   // cells per warp work item
+
+template <typename S>
+struct Vec;
+template <>
+struct Vec<float> {
+    static __device__ __forceinline__ void load4(const float* p, float v[4]) {
+        const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    }
+    static __device__ __forceinline__ void store4(float* p, float a, float b, float c, float d) {
+        *reinterpret_cast<float4*>(p) = make_float4(a, b, c, d);
+    }
+    static __device__ __forceinline__ void store2(float* p, float a, float b) {
+        *reinterpret_cast<float2*>(p) = make_float2(a, b);
+    }
+};
+template <>
+struct Vec<double> {
+    static __device__ __forceinline__ void load4(const double* p, double v[4]) {
+        const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+        const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    }
+    static __device__ __forceinline__ void store4(double* p, double a, double b, double c,
+                                                  double d) {
+        reinterpret_cast<double2*>(p)[0] = make_double2(a, b);
+        reinterpret_cast<double2*>(p)[1] = make_double2(c, d);
+    }
+    static __device__ __forceinline__ void store2(double* p, double a, double b) {
+        *reinterpret_cast<double2*>(p) = make_double2(a, b);
+    }
+};
+template <>
+struct Vec<__half> {
+    static __device__ __forceinline__ void load4(const __half* p, __half v[4]) {
+        const uint2 a = __ldg(reinterpret_cast<const uint2*>(p));
+        const __half2 lo = *reinterpret_cast<const __half2*>(&a.x);
+        const __half2 hi = *reinterpret_cast<const __half2*>(&a.y);
+        v[0] = __low2half(lo); v[1] = __high2half(lo);
+        v[2] = __low2half(hi); v[3] = __high2half(hi);
+    }
+    static __device__ __forceinline__ void store4(__half* p, __half a, __half b, __half c,
+                                                  __half d) {
+        const __half2 lo = __halves2half2(a, b), hi = __halves2half2(c, d);
+        uint2 u;
+        u.x = *reinterpret_cast<const unsigned*>(&lo);
+        u.y = *reinterpret_cast<const unsigned*>(&hi);
+        *reinterpret_cast<uint2*>(p) = u;
+    }
+    static __device__ __forceinline__ void store2(__half* p, __half a, __half b) {
+        *reinterpret_cast<__half2*>(p) = __halves2half2(a, b);
+    }
+};
+
+// Storage encoding of one value (identity for FP32/FP64; for FP16-shifted the
+// scaled deviation with stochastic rounding, see PopIO<__half, float>).
+template <typename S, typename R>
+struct Enc {
+    static __device__ __forceinline__ R dec(S s, int) { return (R)s; }
+    static __device__ __forceinline__ S enc(R v, int, uint32_t) { return (S)v; }
+};
+template <>
+struct Enc<__half, float> {
+    static __device__ __forceinline__ float dec(__half s, int q) {
+        return float(w_of(q)) + __half2float(s) * FP16S_UNSCALE;
+    }
+    static __device__ __forceinline__ __half enc(float v, int q, uint32_t r) {
+        const uint32_t d = (r + (uint32_t)q * 0x9E3779B9u) * 1664525u + 1013904223u;
+        return f2h_stochastic((v - float(w_of(q))) * FP16S_SCALE, d >> 19);
+    }
+};
+
+template <typename S>
+__device__ __forceinline__ S shfl_up1(S v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+template <typename S>
+__device__ __forceinline__ S shfl_down1(S v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+template <>
+__device__ __forceinline__ __half shfl_up1<__half>(__half v) {
+    unsigned short u = __half_as_ushort(v);
+    return __ushort_as_half((unsigned short)__shfl_up_sync(0xffffffffu, (unsigned)u, 1));
+}
+template <>
+__device__ __forceinline__ __half shfl_down1<__half>(__half v) {
+    unsigned short u = __half_as_ushort(v);
+    return __ushort_as_half((unsigned short)__shfl_down_sync(0xffffffffu, (unsigned)u, 1));
+}
+
+// Stores 4 encoded values of one plane.  `row` points at the target row of
+// the plane, `x` is the lane's first cell, dx the x shift (-1, 0, +1); run
+// covers cells [x0, x0 + len) of an nx-periodic row.  All lanes of the warp
+// must call this (shuffles).
+template <typename S>
+__device__ __forceinline__ void store_plane4(S* __restrict__ row, const S v[4], int dx, int x,
+                                             int x0, int len, int nx, bool active, int lane,
+                                             int last_lane) {
+    if (dx == 0) {
+        if (active) Vec<S>::store4(row + x, v[0], v[1], v[2], v[3]);
+        return;
+    }
+    if (dx > 0) {
+        const S prev = shfl_up1(v[3]);
+        if (!active) return;
+        if (lane > 0) {
+            Vec<S>::store4(row + x, prev, v[0], v[1], v[2]);
+        } else {
+            row[x + 1] = v[0];
+            Vec<S>::store2(row + x + 2, v[1], v[2]);
+        }
+        if (lane == last_lane) {
+            int xe = x0 + len;
+            if (xe >= nx) xe -= nx;
+            row[xe] = v[3];
+        }
+    } else {
+        const S next = shfl_down1(v[0]);
+        if (!active) return;
+        if (lane < last_lane) {
+            Vec<S>::store4(row + x, v[1], v[2], v[3], next);
+        } else {
+            Vec<S>::store2(row + x, v[1], v[2]);
+            row[x + 2] = v[3];
+        }
+        if (lane == 0) {
+            int xb = x0 - 1;
+            if (xb < 0) xb += nx;
+            row[xb] = v[0];
+        }
+    }
+}
+
+template <typename S, typename R>
+__device__ __forceinline__ void push_vec4(S* __restrict__ fd, R f[9][4], int x, int x0, int len,
+                                          int nx, int y, int ym, int yp, bool wall_m, bool wall_p,
+                                          int pitch, int plane, bool active, int lane,
+                                          int last_lane, uint32_t seed) {
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        const int cx = cx_of(q), cy = cy_of(q);
+        const bool wall = (cy > 0 && wall_p) || (cy < 0 && wall_m);
+        const int qq = wall ? opp_of(q) : q;
+        S e[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) e[i] = Enc<S, R>::enc(f[q][i], qq, seed + 0x632BE5ABu * i);
+        if (wall) {
+            store_plane4<S>(fd + qq * plane + y * pitch, e, 0, x, x0, len, nx, active, lane,
+                            last_lane);
+        } else {
+            const int yd = cy == 0 ? y : (cy > 0 ? yp : ym);
+            store_plane4<S>(fd + q * plane + yd * pitch, e, cx, x, x0, len, nx, active, lane,
+                            last_lane);
+        }
+    }
+}
+
+// Force-tile slots of a 4-cell run (the 4 cells share a tile: x % 4 == 0).
+struct RunTiles {
+    int s, ps;      // current / previous slot, -1 when untouched (or no tiles)
+    int cell;       // index of the run's first cell inside the tile
+};
+
+__device__ __forceinline__ RunTiles run_tiles(const ChannelDev& ch, int x, int y,
+                                              const TileView& tv) {
+    RunTiles r{-1, -1, 0};
+    if (ch.cap_end > ch.cap_begin && tv.cur_slot != nullptr) {
+        const int t = ch.tile_base + (y / TILE_H) * ch.tiles_x + (x / TILE_W);
+        r.cell = (y % TILE_H) * TILE_W + (x % TILE_W);
+        r.s = tv.cur_slot[t];
+        const bool mdf = ch.ibm_iterations > 1;
+        r.ps = (!mdf || ch.adr) ? tv.prev_slot[t] : -1;
+    }
+    return r;
+}
+
+// Forces of cell i of a run (same rules as cell_forces).
+template <typename R>
+__device__ __forceinline__ CellForces<R> run_forces(const ChannelDev& ch, const RunTiles& rt,
+                                                    int i, const TileView& tv, int stepped) {
+    CellForces<R> cf;
+    const R Fux = R(ch.F_uni_x), Fuy = R(ch.F_uni_y);
+    const R Pux = stepped ? Fux : R(0), Puy = stepped ? Fuy : R(0);
+    const bool mdf = ch.ibm_iterations > 1;
+    const int c = rt.cell + i;
+    if (rt.s >= 0) {
+        const R* fin = static_cast<const R*>(tv.cur_fin) + (size_t)rt.s * 2 * TILE_CELLS;
+        cf.Fx = fin[c];
+        cf.Fy = fin[TILE_CELLS + c];
+    } else {
+        cf.Fx = Fux;
+        cf.Fy = Fuy;
+    }
+    if (rt.ps >= 0) {
+        const R* pf = static_cast<const R*>(tv.prev_fin) + (size_t)rt.ps * 2 * TILE_CELLS;
+        cf.Px = pf[c];
+        cf.Py = pf[TILE_CELLS + c];
+    } else {
+        cf.Px = Pux;
+        cf.Py = Puy;
+    }
+    if (mdf) {
+        if (rt.s >= 0) {
+            const R* gs = static_cast<const R*>(tv.cur_G) + (size_t)rt.s * 2 * TILE_CELLS;
+            cf.Gx = gs[c];
+            cf.Gy = gs[TILE_CELLS + c];
+        } else {
+            cf.Gx = R(0);
+            cf.Gy = R(0);
+        }
+    } else {
+        cf.Gx = cf.Px;
+        cf.Gy = cf.Py;
+    }
+    return cf;
+}
+
+// Forces of 4 consecutive cells (same force tile: x is a multiple of 4).
+template <typename R>
+__device__ __forceinline__ void cell_forces4(const ChannelDev& ch, int x, int y,
+                                             const TileView& tv, int stepped,
+                                             CellForces<R> cf[4]) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) cf[i] = cell_forces<R>(ch, x + i, y, tv, stepped);
+}
+
+// Collision of one cell: COLL >= 0 fixes the operator at compile time (one
+// operator per kernel keeps the code small); COLL < 0 selects per channel.
+template <typename R, int COLL>
+__device__ __forceinline__ void collide_cell(R c[9], R rho, R ux, R uy, R Fx, R Fy,
+                                             const ChannelDev& ch) {
+    const int coll = COLL >= 0 ? COLL : ch.collision;
+    if (coll == 2)
+        collide_regularized(c, rho, ux, uy, Fx, Fy, R(ch.omega));
+    else if (coll == 1)
+        collide_mrt(c, rho, ux, uy, Fx, Fy, R(ch.omega), R(ch.mrt_se), R(ch.mrt_s_eps),
+                    R(ch.mrt_sq));
+    else
+        collide_bgk(c, rho, ux, uy, Fx, Fy, R(ch.omega));
+}
+
+template <typename S, typename R, bool ADR, int COLL>
+__device__ __forceinline__ void lattice_run4(const RowItem& it, const ChannelDev& ch, int st,
+                                             const S* __restrict__ src, S* __restrict__ dst,
+                                             const R* __restrict__ gsrc, R* __restrict__ gdst,
+                                             const R* __restrict__ cfield, const TileView& tv,
+                                             bool adr_on, bool fresh, uint32_t step_mix,
+                                             int lane) {
+    const bool active = 4 * lane < it.len;
+    const int last_lane = (it.len >> 2) - 1;
+    const int nx = ch.nx, ny = ch.ny, pitch = ch.pitch, plane = (int)ch.plane;
+    const int x0 = it.x0, y = it.y;
+    const int x = x0 + 4 * lane;
+    const int n = y * pitch + (active ? x : x0);
+    R f[9][4];
+    {
+        const S* fs = src + ch.f_off + n;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            S v[4];
+            if (active) {
+                Vec<S>::load4(fs + q * plane, v);
+            } else {
+                v[0] = v[1] = v[2] = v[3] = S(0);
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) f[q][i] = Enc<S, R>::dec(v[i], q);
+        }
+    }
+    // per cell: forces, moments and collision; the scalar step keeps only
+    // the moments and the previous force it needs
+    R rho[ADR ? 4 : 1], jx[ADR ? 4 : 1], jy[ADR ? 4 : 1], Px[ADR ? 4 : 1], Py[ADR ? 4 : 1];
+    const RunTiles rt = active ? run_tiles(ch, x, y, tv) : RunTiles{-1, -1, 0};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        R c[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) c[q] = f[q][i];
+        R r, a, bj;
+        cell_moments(c, r, a, bj);
+        if (active) {
+            const CellForces<R> cf = run_forces<R>(ch, rt, i, tv, st);
+            R ux, uy;
+            cell_velocity(r, a, bj, cf.Gx, cf.Gy, ux, uy);
+            collide_cell<R, COLL>(c, r, ux, uy, cf.Fx, cf.Fy, ch);
+            if (ADR) {
+                Px[i] = cf.Px;
+                Py[i] = cf.Py;
+            }
+        }
+        if (ADR) {
+            rho[i] = r;
+            jx[i] = a;
+            jy[i] = bj;
+        }
+#pragma unroll
+        for (int q = 0; q < 9; ++q) f[q][i] = c[q];
+    }
+    const Nbr b = neighbours(0, y, nx, ny, ch.periodic_y ? 1 : 0);
+    const uint32_t seed = mix32((uint32_t)(ch.cell_off + n) ^ step_mix);
+    push_vec4<S, R>(dst + ch.f_off, f, x, x0, it.len, nx, y, b.ym, b.yp, b.wall_m, b.wall_p,
+                    pitch, plane, active, lane, last_lane, seed);
+    if (ADR) {
+        if (adr_on) {   // warp-uniform
+            R g[9][4];
+            const R* gp = gsrc + ch.g_off + n;
+#pragma unroll
+            for (int q = 0; q < 9; ++q) {
+                if (active) Vec<R>::load4(gp + q * plane, g[q]);
+                else g[q][0] = g[q][1] = g[q][2] = g[q][3] = R(0);
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                R c[9];
+#pragma unroll
+                for (int q = 0; q < 9; ++q) c[q] = g[q][i];
+                if (active) {
+                    R C = fresh ? cfield[ch.cell_off + n + i]
+                                : c[0] + c[1] + c[2] + c[3] + c[4] + c[5] + c[6] + c[7] + c[8];
+                    R vx, vy;
+                    cell_velocity(rho[i], jx[i], jy[i], Px[i], Py[i], vx, vy);
+                    collide_scalar(c, C, vx, vy, R(ch.omega_s));
+                }
+#pragma unroll
+                for (int q = 0; q < 9; ++q) g[q][i] = c[q];
+            }
+            const int gmode = ch.periodic_y ? (ch.adr_periodic_y ? 1 : 2) : 0;
+            const Nbr gb = neighbours(0, y, nx, ny, gmode);
+            push_vec4<R, R>(gdst + ch.g_off, g, x, x0, it.len, nx, y, gb.ym, gb.yp, gb.wall_m,
+                            gb.wall_p, pitch, plane, active, lane, last_lane, 0u);
+        }
+    }
+}
+
+// Persistent form: every warp walks a contiguous chunk of 128-cell runs,
+// prefetching the next run descriptor, so the dependent loads of a run's
+// metadata overlap the previous run's work.
+// Resident CTAs per SM requested from the compiler: 3 (80 registers) for the
+// FP32-arithmetic fluid step, 2 with the fused scalar step, 1 for FP64.
+template <typename R, bool ADR>
+constexpr int lattice_min_ctas() { return sizeof(R) == 8 ? 1 : (ADR ? 2 : 3); }
+
+template <typename S, typename R, bool ADR, int COLL>
+__global__ void __launch_bounds__(256, lattice_min_ctas<R, ADR>())
+k_lattice_step4(const RowItem* __restrict__ items, int n_items,
+                const ChannelDev* __restrict__ chans, const S* __restrict__ src,
+                S* __restrict__ dst, const R* __restrict__ gsrc, R* __restrict__ gdst,
+                const R* __restrict__ cfield, TileView tv, const int* __restrict__ stepped,
+                const int* __restrict__ adr_pending, const int* __restrict__ c_fresh,
+                const unsigned* __restrict__ step_ctr) {
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int chunk = (n_items + nwarps - 1) / nwarps;
+    const int i0 = gwarp * chunk;
+    const int i1 = min(n_items, i0 + chunk);
+    if (i0 >= i1) return;                      // warp-uniform
+    const uint32_t step_mix = mix32(*step_ctr + 0x51ED270Bu);
+    RowItem next = items[i0];
+    for (int item = i0; item < i1; ++item) {
+        const RowItem it = next;
+        if (item + 1 < i1) next = items[item + 1];
+        const ChannelDev& ch = chans[it.chan];
+        const int st = stepped[it.chan];
+        bool adr_on = false, fresh = false;
+        if (ADR) {
+            adr_on = ch.adr && adr_pending[it.chan];
+            fresh = adr_on && c_fresh[it.chan] != 0;
+        }
+        lattice_run4<S, R, ADR, COLL>(it, ch, st, src, dst, gsrc, gdst, cfield, tv, adr_on,
+                                      fresh, step_mix, lane);
     }
 }
 

@@ -2,6 +2,8 @@
 // by lattice_f64.cu (FP64, no FMA contraction) and lattice_f32.cu (FP32 and
 // FP16-shifted storage).
 #pragma once
+#include <algorithm>
+
 #include "lattice.cuh"
 #include "sfg_internal.h"
 
@@ -17,8 +19,36 @@ inline TileView to_view(const TileViewArgs& a) {
     return v;
 }
 
+template <typename S, typename R, bool ADR, int COLL>
+static void launch_step4(const LatticeLaunch& L, const TileViewArgs& tv, int grid,
+                         cudaStream_t st) {
+    k_lattice_step4<S, R, ADR, COLL><<<grid, 32 * ITEMS_PER_CTA, 0, st>>>(
+        L.items4, L.n_items4, L.chans, static_cast<const S*>(L.src), static_cast<S*>(L.dst),
+        static_cast<const R*>(L.gsrc), static_cast<R*>(L.gdst), static_cast<const R*>(L.cfield),
+        to_view(tv), L.stepped, L.adr_pending, L.c_fresh, L.step_ctr);
+}
+
+template <typename S, typename R, bool ADR>
+static void launch_step4_coll(const LatticeLaunch& L, const TileViewArgs& tv, int grid,
+                              cudaStream_t st) {
+    switch (L.collision) {
+        case 0: launch_step4<S, R, ADR, 0>(L, tv, grid, st); break;
+        case 1: launch_step4<S, R, ADR, 1>(L, tv, grid, st); break;
+        case 2: launch_step4<S, R, ADR, 2>(L, tv, grid, st); break;
+        default: launch_step4<S, R, ADR, -1>(L, tv, grid, st); break;
+    }
+}
+
 template <typename S, typename R>
 void launch_lattice_step(const LatticeLaunch& L, const TileViewArgs& tv, cudaStream_t st) {
+    if (L.use_vec4) {
+        if (L.n_items4 == 0) return;
+        const int grid = std::max(1, std::min(L.persistent_ctas,
+                                              (L.n_items4 + ITEMS_PER_CTA - 1) / ITEMS_PER_CTA));
+        if (L.any_adr) launch_step4_coll<S, R, true>(L, tv, grid, st);
+        else launch_step4_coll<S, R, false>(L, tv, grid, st);
+        return;
+    }
     if (L.n_items == 0) return;
     const int grid = (L.n_items + ITEMS_PER_CTA - 1) / ITEMS_PER_CTA;
     if (L.any_adr)
@@ -29,8 +59,9 @@ void launch_lattice_step(const LatticeLaunch& L, const TileViewArgs& tv, cudaStr
             L.step_ctr);
     else
         k_lattice_step<S, R, false><<<grid, 32 * ITEMS_PER_CTA, 0, st>>>(
-            L.items, L.n_items, L.chans, static_cast<const S*>(L.src), static_cast<S*>(L.dst), nullptr,
-            nullptr, nullptr, to_view(tv), L.stepped, L.adr_pending, L.c_fresh, L.step_ctr);
+            L.items, L.n_items, L.chans, static_cast<const S*>(L.src), static_cast<S*>(L.dst),
+            nullptr, nullptr, nullptr, to_view(tv), L.stepped, L.adr_pending, L.c_fresh,
+            L.step_ctr);
 }
 
 template <typename S, typename R>
@@ -67,7 +98,21 @@ void launch_macro_export(const void* in, const ChannelDev& ch, const TileViewArg
         static_cast<const S*>(in), ch, to_view(tv_last), stepped, rho, ux, uy, Fx, Fy);
 }
 
+template <typename S, typename R>
+int lattice_ctas_per_sm_t(bool adr) {
+    // the generic-collision instance has the largest footprint
+    int n = 0;
+    if (adr)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_lattice_step4<S, R, true, -1>,
+                                                      32 * ITEMS_PER_CTA, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_lattice_step4<S, R, false, -1>,
+                                                      32 * ITEMS_PER_CTA, 0);
+    return n > 0 ? n : 1;
+}
+
 #define SFG_LATTICE_INST(S, R)                                                                   \
+    template int lattice_ctas_per_sm_t<S, R>(bool);                                              \
     template void launch_lattice_step<S, R>(const LatticeLaunch&, const TileViewArgs&,           \
                                             cudaStream_t);                                        \
     template void launch_scalar_flush<S, R>(const LatticeLaunch&, const TileViewArgs&,           \

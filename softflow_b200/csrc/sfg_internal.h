@@ -76,6 +76,11 @@ struct LatticeLaunch {
     const int* c_fresh;
     const unsigned* step_ctr;   // device step counter (stochastic-rounding seed)
     bool any_adr;
+    const RowItem* items4;      // 128-cell runs for the vectorised kernel
+    int n_items4;
+    bool use_vec4;              // every channel has nx % 4 == 0
+    int persistent_ctas;        // grid of the persistent vectorised kernel
+    int collision;              // shared collision model of all channels, -1 if mixed
 };
 struct TileViewArgs {
     const int* cur_slot;
@@ -84,6 +89,10 @@ struct TileViewArgs {
     const void* cur_G;
     const void* prev_fin;
 };
+// Resident CTAs per SM of the persistent lattice kernel (occupancy query).
+int lattice_ctas_per_sm(int precision, bool adr);
+template <typename S, typename R>
+int lattice_ctas_per_sm_t(bool adr);
 template <typename S, typename R>
 void launch_lattice_step(const LatticeLaunch& L, const TileViewArgs& tv, cudaStream_t st);
 template <typename S, typename R>

@@ -265,7 +265,8 @@ class _Channel:
 class _Context:
     """One device context holding one or more channels."""
 
-    def __init__(self, channels: Sequence[_Channel], precision: str, device: int):
+    def __init__(self, channels: Sequence[_Channel], precision: str, device: int,
+                 lattice_variant: int = 0):
         if precision not in L.PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(L.PRECISIONS)}")
         lib = L.lib()
@@ -275,6 +276,7 @@ class _Context:
         L.check(lib.sfg_create(int(device), L.PRECISIONS[precision], C.byref(h)))
         self._h = h
         try:
+            L.check(lib.sfg_set_lattice_variant(h, int(lattice_variant)))
             for ch in channels:
                 idx = C.c_int()
                 L.check(lib.sfg_add_channel(h, C.byref(ch.cparams), C.byref(idx)))
@@ -565,9 +567,10 @@ class Ensemble:
     channel run alone.
     """
 
-    def __init__(self, precision: str = "fp32", device: int = 0):
+    def __init__(self, precision: str = "fp32", device: int = 0, lattice_variant: int = 0):
         self.precision = precision
         self.device = device
+        self.lattice_variant = lattice_variant
         self._chans: List[_Channel] = []
         self._ctx: Optional[_Context] = None
         self._steps = 0
@@ -603,7 +606,7 @@ class Ensemble:
     def initialize(self):
         if self._ctx is not None:
             raise RuntimeError("already initialized")
-        self._ctx = _Context(self._chans, self.precision, self.device)
+        self._ctx = _Context(self._chans, self.precision, self.device, self.lattice_variant)
         self._steps = 0
 
     def _need(self):
