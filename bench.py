@@ -367,7 +367,7 @@ def cpu_sims(plans, impl, threads):
         with contextlib.redirect_stdout(io.StringIO()):
             for (count, x0, y0, x1, y1, r, nodes, mp, seed) in pl.placements:
                 s.add_capsule_random(count, x0, y0, x1, y1, r, r, nodes, oracle_membrane(mp),
-                                     seed=seed, min_gap=1.0, check_walls=True)
+                                     seed=seed, min_gap=pl.min_gap, check_walls=True)
         s.initialize()
         if pl.gaussian is not None:
             cx, cy, sg = pl.gaussian

@@ -209,6 +209,39 @@ int sfg_spread_forces_noalloc(int nx, int ny, int ncaps, const int* d_offsets,
                               const double* d_pos, const double* d_force, double* d_Fx,
                               double* d_Fy, int num_markers, void* stream);
 
+/* ---- learned multi-direct forcing: the per-marker network ------------------
+ * An 8 -> 64 -> 64 -> 2 ReLU network (4866 FP32 parameters: W1 [64x8], b1,
+ * W2 [64x64], b2, W3 [2x64], b3) trained and evaluated on the tensor cores
+ * with BF16 operands and FP32 accumulation.  The reference's counterpart is
+ * the FP64 surrogate SimpleNN (src/ml/simple_nn.cpp:10-262: same layer
+ * shapes with 9 inputs, He initialisation, mean/std normalisation, MSE
+ * gradient), trained there with SGD on the CPU and not used by its step.
+ * Device pointers are given as `d_`; calls are ordered on `stream` and return
+ * after it has finished.  Features are raw (the network normalises them);
+ * targets are raw (normalised inside). */
+typedef struct sfg_mlp sfg_mlp;
+#define SFG_MLP_NUM_PARAMS 4866
+int sfg_mlp_create(int device, sfg_mlp** out);
+int sfg_mlp_destroy(sfg_mlp* m);
+/* Sets the FP32 parameters (host array) and resets the Adam state. */
+int sfg_mlp_set_params(sfg_mlp* m, const float* params);
+int sfg_mlp_get_params(sfg_mlp* m, float* params);
+/* Input mean/std [8] and output mean/std [2]; every std must be > 0. */
+int sfg_mlp_set_normalization(sfg_mlp* m, const float* in_mean, const float* in_std,
+                              const float* out_mean, const float* out_std);
+/* d_y [n x 2] = network(d_x [n x 8]), de-normalised. */
+int sfg_mlp_forward(sfg_mlp* m, const float* d_x, int n, float* d_y, void* stream);
+/* Gradient of the loss mean((y - t)^2) over the n samples and both outputs
+ * (normalised targets) into the host array grad [4866]; loss optional. */
+int sfg_mlp_gradients(sfg_mlp* m, const float* d_x, const float* d_t, int n, float* grad,
+                      float* loss, void* stream);
+/* floor(n / batch) Adam steps (beta 0.9 / 0.999, eps 1e-8) over consecutive
+ * batches of the given data; losses (host, optional) receives each step's
+ * batch loss. */
+int sfg_mlp_train(sfg_mlp* m, const float* d_x, const float* d_t, int n, int batch, float lr,
+                  float* losses, void* stream);
+int sfg_mlp_step_count(sfg_mlp* m, int* steps);
+
 /* ---- diagnostics ---------------------------------------------------------- */
 int sfg_num_channels(const sfg_context* ctx, int* n);
 int sfg_channel_counts(const sfg_context* ctx, int channel, int* num_capsules, int* num_markers);

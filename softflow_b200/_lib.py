@@ -108,6 +108,18 @@ SIGNATURES = {
     "sfg_set_lattice_variant": (C.c_int, [C.c_void_p, C.c_int]),
     "sfg_get_phase_times": (C.c_int, [C.c_void_p, _P(C.c_float), C.c_int]),
     "sfg_reset_phase_times": (C.c_int, [C.c_void_p]),
+    "sfg_mlp_create": (C.c_int, [C.c_int, _P(C.c_void_p)]),
+    "sfg_mlp_destroy": (C.c_int, [C.c_void_p]),
+    "sfg_mlp_set_params": (C.c_int, [C.c_void_p, _P(C.c_float)]),
+    "sfg_mlp_get_params": (C.c_int, [C.c_void_p, _P(C.c_float)]),
+    "sfg_mlp_set_normalization": (C.c_int, [C.c_void_p, _P(C.c_float), _P(C.c_float),
+                                            _P(C.c_float), _P(C.c_float)]),
+    "sfg_mlp_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "sfg_mlp_gradients": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                    _P(C.c_float), _P(C.c_float), C.c_void_p]),
+    "sfg_mlp_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float,
+                                _P(C.c_float), C.c_void_p]),
+    "sfg_mlp_step_count": (C.c_int, [C.c_void_p, _P(C.c_int)]),
 }
 
 PHASES = ["membrane", "contact", "ibm_tiles", "ibm_spread", "mdf_interp", "lattice",

@@ -28,6 +28,7 @@ UNITS = [
     ("spread_standalone.cu", ["--fmad=false"]),
     ("spread_noalloc.cu", []),
     ("scan.cu", []),
+    ("mlp.cu", []),
     ("context.cu", []),
 ]
 HOST_UNITS = [("host_setup.cpp", ["-ffp-contract=off"])]

@@ -12,7 +12,8 @@ c3  256 independent channels drawn from seed 7: nx in {200, 208, ..., 800},
     G_s log-uniform in [0.01, 0.1], tau uniform in [0.6, 1.0], fx uniform in
     [1e-5, 5e-5]; regularized collision, 5 MDF sweeps.  Channel i places its
     capsules from seed fnv1a64(str(i)) & 0x7fffffff with centres in
-    x [8, nx - 8], y [8, ny - 8].
+    x [8, nx - 8], y [8, ny - 8] and surfaces at least 3.5 lu apart (the
+    contact cut-off).
 
 Centres are kept MARGIN = 8 lu from the walls and from the periodic seam
 (configuration 1 keeps them 10 lu from the walls and 20 lu from the seam).
@@ -73,6 +74,7 @@ class ChannelPlan:
     params: SimulationParams
     # (count, x0, y0, x1, y1, r, nodes, membrane, seed)
     placements: List[Tuple] = field(default_factory=list)
+    min_gap: float = 1.0       # surface gap of the rejection test (lu)
     gaussian: Tuple = None     # (cx, cy, sigma) for the scalar
 
 
@@ -87,6 +89,11 @@ def plan_c1(precision="fp32") -> List[ChannelPlan]:
 
 
 MARGIN = 8
+# c3 rejects placements whose surfaces come closer than the contact cut-off
+# (3.5 lu): capsules seeded 1 lu apart start inside each other's repulsion
+# range, the spread contact forces exceed the 0.01 lattice-force cap, and
+# with 5 MDF sweeps the flow diverges within a few hundred steps.
+C3_MIN_GAP = 3.5
 
 
 def plan_c2(precision="fp32") -> List[ChannelPlan]:
@@ -110,7 +117,8 @@ def plan_c3(precision="fp32", n_channels=256, ibm_iterations=5) -> List[ChannelP
         p = channel_params(nx, ny, CollisionModel.REGULARIZED, tau, fx, ibm_iterations, precision)
         seed = fnv1a64(str(i)) & 0x7FFFFFFF
         m = MARGIN
-        plans.append(ChannelPlan(p, [(ncap, m, m, nx - m, ny - m, 3.0, 24, skalak(G_s), seed)]))
+        plans.append(ChannelPlan(p, [(ncap, m, m, nx - m, ny - m, 3.0, 24, skalak(G_s), seed)],
+                                 min_gap=C3_MIN_GAP))
     return plans
 
 
@@ -131,7 +139,7 @@ def build(plans: List[ChannelPlan], precision: str = None, device: int = 0,
             sink = contextlib.nullcontext() if verbose else contextlib.redirect_stdout(io.StringIO())
             with sink:
                 ens.addCapsuleRandom(i, count, x0, y0, x1, y1, r, r, nodes, mp, seed=seed,
-                                     min_gap=1.0, check_walls=True)
+                                     min_gap=pl.min_gap, check_walls=True)
     ens.initialize()
     for i, pl in enumerate(plans):
         if pl.gaussian is not None:
