@@ -242,6 +242,32 @@ int sfg_mlp_train(sfg_mlp* m, const float* d_x, const float* d_t, int n, int bat
                   float* losses, void* stream);
 int sfg_mlp_step_count(sfg_mlp* m, int* steps);
 
+/* Learned multi-direct forcing in the step.  On every channel with
+ * ibm_iterations = K >= 3 and capsules, replaces the first K-2 correction
+ * sweeps of ImmersedBoundary::multiDirectForcing (immersed_boundary.cpp:
+ * 231-286) by the network's prediction of their summed correction (seed),
+ * spread like a sweep; the last plain sweep follows.  The no-slip residual
+ * max |U_prev - U_interp| over the channel's markers, taken at that sweep's
+ * interpolation, gates the result: above residual_threshold (lu/step) the
+ * channel redoes the plain K-1 sweeps from its membrane-force spread, so its
+ * result is the plain one.  The network's current parameters are copied into
+ * the context; net == NULL turns the learned form off.  The reference has no
+ * counterpart (it always runs the plain sweeps). */
+int sfg_set_mdf_model(sfg_context* ctx, sfg_mlp* net, double residual_threshold);
+/* Last step's residuals of a channel (learned gate; plain iteration's last
+ * sweep, 0 when it did not run) and cumulative learned / fallback steps. */
+int sfg_get_mdf_stats(sfg_context* ctx, int channel, float* resid_learned, float* resid_plain,
+                      long long* learned_steps, long long* fallbacks);
+/* Training data: when enabled, every step records for each marker the
+ * network inputs (with the velocity interpolated at the plain iteration's
+ * first sweep) and the label, the correction summed over the sweeps before
+ * the last one, in the marker's local frame (learned steps record the
+ * seed).  sfg_get_harvest copies the last step's records:
+ * features [M][8], labels [M][2], valid [M] (M = all markers of the context,
+ * capsule-major).  Any pointer may be NULL. */
+int sfg_set_harvest(sfg_context* ctx, int enabled);
+int sfg_get_harvest(sfg_context* ctx, float* features, float* labels, int* valid);
+
 /* ---- diagnostics ---------------------------------------------------------- */
 int sfg_num_channels(const sfg_context* ctx, int* n);
 int sfg_channel_counts(const sfg_context* ctx, int channel, int* num_capsules, int* num_markers);
@@ -264,7 +290,8 @@ enum sfg_phase {
     SFG_PHASE_LATTICE = 5,      /* "LBM step" (+ fused scalar step)           */
     SFG_PHASE_BOOKKEEPING = 6,  /* per-step flags                             */
     SFG_PHASE_INTERP_MOVE = 7,  /* "IBM interpolate" + marker move            */
-    SFG_NUM_PHASES = 8
+    SFG_PHASE_MDF_LEARNED = 8,  /* learned forcing: interpolation + network   */
+    SFG_NUM_PHASES = 9
 };
 int sfg_set_profiling(sfg_context* ctx, int on);
 int sfg_get_phase_times(sfg_context* ctx, float* ms, int n);

@@ -160,7 +160,8 @@ def features(pos, nxt, prv, rest_prev, rest_next, u_interp, u_target, dF_prev, L
     u_interp : velocity interpolated after the membrane-force spread;
     u_target : the marker's velocity from the previous step (the multi-direct
                forcing target, immersed_boundary.cpp:255);
-    dF_prev  : the marker's total forcing correction of the previous step.
+    dF_prev  : the marker's forcing correction of the previous step before
+               its last sweep.
 
     Tangent t = normalised (e_prev + e_next), normal n = (-t_y, t_x);
     features = [slip.t, slip.n, dF_prev.t, dF_prev.n, stretch, curvature,

@@ -120,10 +120,15 @@ SIGNATURES = {
     "sfg_mlp_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float,
                                 _P(C.c_float), C.c_void_p]),
     "sfg_mlp_step_count": (C.c_int, [C.c_void_p, _P(C.c_int)]),
+    "sfg_set_mdf_model": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double]),
+    "sfg_get_mdf_stats": (C.c_int, [C.c_void_p, C.c_int, _P(C.c_float), _P(C.c_float),
+                                    _P(C.c_longlong), _P(C.c_longlong)]),
+    "sfg_set_harvest": (C.c_int, [C.c_void_p, C.c_int]),
+    "sfg_get_harvest": (C.c_int, [C.c_void_p, _P(C.c_float), _P(C.c_float), _P(C.c_int)]),
 }
 
 PHASES = ["membrane", "contact", "ibm_tiles", "ibm_spread", "mdf_interp", "lattice",
-          "bookkeeping", "interp_move"]
+          "bookkeeping", "interp_move", "mdf_learned"]
 
 
 def lib():

@@ -29,6 +29,7 @@ UNITS = [
     ("spread_noalloc.cu", []),
     ("scan.cu", []),
     ("mlp.cu", []),
+    ("learned_step.cu", ["--fmad=false"]),
     ("context.cu", []),
 ]
 HOST_UNITS = [("host_setup.cpp", ["-ffp-contract=off"])]

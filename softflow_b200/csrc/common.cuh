@@ -66,6 +66,9 @@ struct ChannelDev {
     double rep_epsilon, rep_sigma, rep_r_cut, rep_damping, rep_friction;
     int rep_power;
     int brute_contact;          // <= 100 markers: all pairs, one-sided
+    // learned multi-direct forcing
+    int learned;                // 1: network seed + one sweep, plain sweeps as fallback
+    float mdf_threshold;        // no-slip residual (lu/step) above which it falls back
 };
 
 // Per-capsule constants (reference Capsule members, capsule.h:77-142).
@@ -84,11 +87,36 @@ struct RowItem {
     int chan, y, x0, len;
 };
 
+// Multi-direct forcing launch modes.
+//   MDF_PLAIN   : the reference sweeps; on a learned channel only when its
+//                 gate residual exceeded the threshold (fallback), restarting
+//                 from the force after the membrane spread (acc0);
+//   MDF_SEED    : spread of the network's correction (learned channels);
+//   MDF_LEARNED : the one plain sweep after the seed (learned channels); its
+//                 interpolation gives the gate residual, its spread finishes
+//                 the step's force unless the channel falls back.
+enum MdfMode : int { MDF_PLAIN = 0, MDF_SEED = 1, MDF_LEARNED = 2 };
+
+// A learned channel falls back when its residual is above the threshold or
+// not a number (the residual is kept as the bits of a non-negative float).
+__device__ __forceinline__ bool mdf_fallback(unsigned resid_bits, float thr) {
+    return !(__uint_as_float(resid_bits) <= thr);
+}
+
+// Whether a channel takes part in a correction sweep (sweep >= 1) of the
+// given mode.
+__device__ __forceinline__ bool mdf_active(const ChannelDev& ch, int mode,
+                                           const unsigned* resid_gate, int chan) {
+    if (mode != MDF_PLAIN) return ch.learned != 0;
+    return !ch.learned || mdf_fallback(resid_gate[chan], ch.mdf_threshold);
+}
+
 // Status word bits written by kernels (host reads them after a sync).
 enum StatusBits : unsigned {
     ST_NAN_MARKER = 1u,         // non-finite marker position seen
     ST_LIST_OVERFLOW = 2u,      // a per-tile marker list exceeded its capacity
     ST_CAPSULE_TOO_BIG = 4u,    // a capsule exceeded the per-warp node capacity
+    ST_TENSOR_TIMEOUT = 8u,     // a tensor-core completion wait gave up
 };
 
 }  // namespace sfg

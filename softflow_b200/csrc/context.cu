@@ -10,6 +10,7 @@
 #include "../../include/softflow_gpu.h"
 #include "lattice.cuh"
 #include "sfg_internal.h"
+#include "mlp.cuh"
 
 using namespace sfg;
 
@@ -46,10 +47,17 @@ struct ChanHost {
 };
 
 __global__ void k_step_flags(const ChannelDev* __restrict__ chans, int nch, int* stepped,
-                             int* adr_pending, int* c_fresh, unsigned* step_ctr) {
+                             int* adr_pending, int* c_fresh, unsigned* step_ctr,
+                             const unsigned* __restrict__ resid_gate,
+                             long long* __restrict__ learned_steps,
+                             long long* __restrict__ fallbacks) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c == 0) *step_ctr += 1u;
     if (c >= nch) return;
+    if (chans[c].learned && chans[c].cap_end > chans[c].cap_begin) {
+        learned_steps[c] += 1;
+        if (mdf_fallback(resid_gate[c], chans[c].mdf_threshold)) fallbacks[c] += 1;
+    }
     if (chans[c].adr) {
         if (adr_pending[c]) c_fresh[c] = 0;
         adr_pending[c] = 1;
@@ -173,6 +181,16 @@ struct sfg_context {
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     bool use_graphs = true;
     bool force_scalar_lattice = false;  // diagnostics: use the one-cell-per-thread kernel
+    // learned multi-direct forcing
+    void* d_model = nullptr;            // mlp::ModelDev (the context's own copy)
+    bool any_learned = false;
+    int learned_grid = 592;
+    long long* d_learned_steps = nullptr;  // [nch]
+    long long* d_fallbacks = nullptr;      // [nch]
+    bool harvest = false;
+    float* d_hfeat = nullptr;           // [M][8]
+    float* d_hlab = nullptr;            // [M][2]
+    int* d_hvalid = nullptr;            // [M]
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int launches = 0;
     // per-phase timing (profiling mode runs the step eagerly)
@@ -246,7 +264,10 @@ static void free_all(sfg_context* c) {
     F(c->tb.tile_chan); F(c->tb.tile_flag); F(c->tb.tile_cnt); F(c->tb.cursor);
     F(c->tb.slot_scan); F(c->tb.list_off); F(c->tb.slot_tile); F(c->tb.n_slots);
     F(c->tb.list); F(c->tb.scan_tmp); F(c->tb.acc); F(c->tb.gsnap); F(c->tb.capped);
-    F(c->tb.fluid_touched);
+    F(c->tb.fluid_touched); F(c->tb.acc0); F(c->tb.resid_gate); F(c->tb.resid_plain);
+    F(c->mb.u0); F(c->mb.dFsum); F(c->mb.dFprev);
+    F(c->d_model); F(c->d_learned_steps); F(c->d_fallbacks);
+    F(c->d_hfeat); F(c->d_hlab); F(c->d_hvalid);
     F(c->cb.cell_of); F(c->cb.cell_cnt); F(c->cb.cell_start); F(c->cb.cursor); F(c->cb.list);
     F(c->cb.scan_tmp);
     F(c->d_phi); F(c->d_stepped); F(c->d_adr_pending); F(c->d_c_fresh); F(c->d_status);
@@ -576,6 +597,23 @@ extern "C" int sfg_initialize(sfg_context* c) {
     CU(dalloc(&tb.fluid_touched, nch));
     CU(cudaMemset(tb.capped, 0, sizeof(int) * nch));
     CU(cudaMemset(tb.fluid_touched, 0, sizeof(int) * nch));
+    CU(dalloc(&tb.resid_gate, nch));
+    CU(dalloc(&tb.resid_plain, nch));
+    CU(cudaMemset(tb.resid_gate, 0, sizeof(unsigned) * nch));
+    CU(cudaMemset(tb.resid_plain, 0, sizeof(unsigned) * nch));
+    CU(dalloc(&c->d_learned_steps, nch));
+    CU(dalloc(&c->d_fallbacks, nch));
+    CU(cudaMemset(c->d_learned_steps, 0, sizeof(long long) * nch));
+    CU(cudaMemset(c->d_fallbacks, 0, sizeof(long long) * nch));
+    // forcing state of the learned form (zero before the first step)
+    CU(dalloc(&c->mb.u0, M));
+    CU(dalloc(&c->mb.dFsum, M));
+    CU(dalloc(&c->mb.dFprev, M));
+    if (M > 0) {
+        CU(cudaMemset(c->mb.u0, 0, sizeof(double2) * M));
+        CU(cudaMemset(c->mb.dFsum, 0, sizeof(double2) * M));
+        CU(cudaMemset(c->mb.dFprev, 0, sizeof(double2) * M));
+    }
 
     // contact cells
     CU(dalloc(&c->cb.cell_of, M));
@@ -609,6 +647,7 @@ extern "C" int sfg_initialize(sfg_context* c) {
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
     c->spread_grid = std::max(1, std::min((tb.max_slots + 7) / 8, nsm * 4));
     c->persistent_ctas = nsm * lattice_ctas_per_sm(c->precision, c->any_adr);
+    c->learned_grid = nsm * 4;
     CU(cudaStreamSynchronize(c->stream));
     c->initialized = true;
     c->steps = 0;
@@ -639,6 +678,8 @@ static int enqueue_step_t(sfg_context* c, int p) {
     if (c->M > 0) {
         cudaMemsetAsync(c->tb.capped, 0, sizeof(int) * nch, st);
         cudaMemsetAsync(c->tb.fluid_touched, 0, sizeof(int) * nch, st);
+        cudaMemsetAsync(c->tb.resid_gate, 0, sizeof(unsigned) * nch, st);
+        cudaMemsetAsync(c->tb.resid_plain, 0, sizeof(unsigned) * nch, st);
         launch_membrane(c->d_caps, c->NC, c->mb, c->d_has_prev, c->maxn, c->d_status, st);
         mark(c, SFG_PHASE_MEMBRANE);
         launch_contact(c->d_chans, c->M, c->mb, c->cb, c->ncells, st);
@@ -646,17 +687,39 @@ static int enqueue_step_t(sfg_context* c, int p) {
         launch_tiles(c->d_chans, c->d_caps, c->M, c->mb, c->tb, c->tb.T, p, c->d_phi, c->d_status,
                      st);
         mark(c, SFG_PHASE_IBM_TILES);
-        launch_spread<R>(c->d_chans, c->mb, c->tb, p, c->d_phi, 0, c->spread_grid, c->d_status, st);
+        launch_spread<R>(c->d_chans, c->mb, c->tb, p, 0, MDF_PLAIN, c->spread_grid, c->d_status,
+                         st);
         mark(c, SFG_PHASE_IBM_SPREAD);
         launches += 1 + (c->ncells > 0 ? 7 : 1) + 9 + 1;
-        for (int k = 1; k < c->Kmax; ++k) {
-            launch_mdf_interp<S, R>(c->d_chans, c->M, c->mb, static_cast<const S*>(c->f[p]), c->tb,
-                                    p, c->d_phi, k, st);
+        const S* fp = static_cast<const S*>(c->f[p]);
+        if (c->any_learned) {
+            // seed, one plain sweep, gate; the plain sweeps below run only for
+            // channels above the threshold
+            launch_mdf_learned<S, R>(c->d_chans, c->d_caps, c->M, c->mb, fp, c->tb, p,
+                                     c->d_model, c->learned_grid, c->d_status, st);
+            mark(c, SFG_PHASE_MDF_LEARNED);
+            launch_spread<R>(c->d_chans, c->mb, c->tb, p, 1, MDF_SEED, c->spread_grid,
+                             c->d_status, st);
+            mark(c, SFG_PHASE_IBM_SPREAD);
+            launch_mdf_interp<S, R>(c->d_chans, c->M, c->mb, fp, c->tb, p, 2, MDF_LEARNED, st);
             mark(c, SFG_PHASE_MDF_INTERP);
-            launch_spread<R>(c->d_chans, c->mb, c->tb, p, c->d_phi, k, c->spread_grid, c->d_status,
-                             st);
+            launch_spread<R>(c->d_chans, c->mb, c->tb, p, 2, MDF_LEARNED, c->spread_grid,
+                             c->d_status, st);
+            mark(c, SFG_PHASE_IBM_SPREAD);
+            launches += 4;
+        }
+        for (int k = 1; k < c->Kmax; ++k) {
+            launch_mdf_interp<S, R>(c->d_chans, c->M, c->mb, fp, c->tb, p, k, MDF_PLAIN, st);
+            mark(c, SFG_PHASE_MDF_INTERP);
+            launch_spread<R>(c->d_chans, c->mb, c->tb, p, k, MDF_PLAIN, c->spread_grid,
+                             c->d_status, st);
             mark(c, SFG_PHASE_IBM_SPREAD);
             launches += 2;
+        }
+        if (c->harvest) {
+            launch_harvest(c->d_chans, c->d_caps, c->M, c->mb, c->d_hfeat, c->d_hlab, c->d_hvalid,
+                           st);
+            launches += 1;
         }
     }
     LatticeLaunch L{c->d_items, c->n_items, c->d_chans, c->f[p], c->f[1 - p], c->g[p],
@@ -670,7 +733,8 @@ static int enqueue_step_t(sfg_context* c, int p) {
     mark(c, SFG_PHASE_LATTICE);
     k_step_flags<<<(nch + 127) / 128, 128, 0, st>>>(c->d_chans, nch, c->d_stepped,
                                                     c->d_adr_pending, c->d_c_fresh,
-                                                    c->d_step_ctr);
+                                                    c->d_step_ctr, c->tb.resid_gate,
+                                                    c->d_learned_steps, c->d_fallbacks);
     mark(c, SFG_PHASE_BOOKKEEPING);
     launches += 2;
     if (c->M > 0) {
@@ -758,6 +822,112 @@ extern "C" int sfg_synchronize(sfg_context* c, unsigned* status_out) {
 extern "C" int sfg_last_step_ms(sfg_context* c, float* ms) {
     if (!c || !ms) return fail(SFG_ERR_ARG, "sfg_last_step_ms: null argument");
     CU(cudaEventElapsedTime(ms, c->ev0, c->ev1));
+    return SFG_OK;
+}
+
+// ------------------------------------------------------------------------
+// learned multi-direct forcing
+// ------------------------------------------------------------------------
+int sfg_mlp_model_device(sfg_mlp* m, const void** model, cudaStream_t st);
+
+static void drop_graphs(sfg_context* c) {
+    for (int i = 0; i < 2; ++i) {
+        if (c->gexec[i]) cudaGraphExecDestroy(c->gexec[i]);
+        c->gexec[i] = nullptr;
+    }
+}
+
+extern "C" int sfg_set_mdf_model(sfg_context* c, sfg_mlp* net, double residual_threshold) {
+    if (!c) return fail(SFG_ERR_ARG, "sfg_set_mdf_model: null context");
+    if (!c->initialized) return fail(SFG_ERR_STATE, "sfg_set_mdf_model: context not initialized");
+    if (net && !(residual_threshold >= 0.0))
+        return fail(SFG_ERR_ARG, "sfg_set_mdf_model: the threshold must be >= 0");
+    CU(cudaSetDevice(c->device));
+    CU(cudaStreamSynchronize(c->stream));
+    bool any = false;
+    if (net) {
+        static bool prepared[64] = {false};
+        if (c->device >= 0 && c->device < 64 && !prepared[c->device]) {
+            CU(prepare_mdf_learned());
+            prepared[c->device] = true;
+        }
+        const void* md = nullptr;
+        int rc = sfg_mlp_model_device(net, &md, c->stream);
+        if (rc) return rc;
+        if (!c->d_model) CU(cudaMalloc(&c->d_model, sizeof(sfg::mlp::ModelDev)));
+        CU(cudaMemcpyAsync(c->d_model, md, sizeof(sfg::mlp::ModelDev), cudaMemcpyDeviceToDevice,
+                           c->stream));
+        if (!c->tb.acc0 && c->M > 0)
+            CU(dalloc(&c->tb.acc0, (size_t)c->tb.max_slots * 2 * TILE_CELLS));
+    }
+    for (auto& h : c->ch) {
+        const bool on = net && h.d.ibm_iterations >= 3 && h.d.cap_end > h.d.cap_begin;
+        h.d.learned = on ? 1 : 0;
+        h.d.mdf_threshold = (float)residual_threshold;
+        any = any || on;
+    }
+    std::vector<ChannelDev> dv;
+    for (auto& h : c->ch) dv.push_back(h.d);
+    CU(cudaMemcpyAsync(c->d_chans, dv.data(), sizeof(ChannelDev) * dv.size(),
+                       cudaMemcpyHostToDevice, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    c->any_learned = any;
+    drop_graphs(c);
+    return SFG_OK;
+}
+
+extern "C" int sfg_get_mdf_stats(sfg_context* c, int channel, float* resid_learned,
+                                 float* resid_plain, long long* learned_steps,
+                                 long long* fallbacks) {
+    if (!c) return fail(SFG_ERR_ARG, "sfg_get_mdf_stats: null context");
+    if (!c->initialized) return fail(SFG_ERR_STATE, "sfg_get_mdf_stats: context not initialized");
+    if (channel < 0 || channel >= (int)c->ch.size())
+        return fail(SFG_ERR_ARG, "sfg_get_mdf_stats: bad channel");
+    CU(cudaSetDevice(c->device));
+    CU(cudaStreamSynchronize(c->stream));
+    unsigned rg = 0, rp = 0;
+    long long ls = 0, fb = 0;
+    CU(cudaMemcpy(&rg, c->tb.resid_gate + channel, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(&rp, c->tb.resid_plain + channel, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(&ls, c->d_learned_steps + channel, sizeof(long long), cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(&fb, c->d_fallbacks + channel, sizeof(long long), cudaMemcpyDeviceToHost));
+    float a, b;
+    std::memcpy(&a, &rg, sizeof(float));
+    std::memcpy(&b, &rp, sizeof(float));
+    if (resid_learned) *resid_learned = a;
+    if (resid_plain) *resid_plain = b;
+    if (learned_steps) *learned_steps = ls;
+    if (fallbacks) *fallbacks = fb;
+    return SFG_OK;
+}
+
+extern "C" int sfg_set_harvest(sfg_context* c, int enabled) {
+    if (!c) return fail(SFG_ERR_ARG, "sfg_set_harvest: null context");
+    if (!c->initialized) return fail(SFG_ERR_STATE, "sfg_set_harvest: context not initialized");
+    CU(cudaSetDevice(c->device));
+    CU(cudaStreamSynchronize(c->stream));
+    if (enabled && c->M > 0 && !c->d_hfeat) {
+        CU(dalloc(&c->d_hfeat, 8LL * c->M));
+        CU(dalloc(&c->d_hlab, 2LL * c->M));
+        CU(dalloc(&c->d_hvalid, c->M));
+        CU(cudaMemset(c->d_hvalid, 0, sizeof(int) * c->M));
+    }
+    c->harvest = enabled != 0 && c->M > 0;
+    drop_graphs(c);
+    return SFG_OK;
+}
+
+extern "C" int sfg_get_harvest(sfg_context* c, float* features, float* labels, int* valid) {
+    if (!c) return fail(SFG_ERR_ARG, "sfg_get_harvest: null context");
+    if (!c->harvest || !c->d_hfeat)
+        return fail(SFG_ERR_STATE, "sfg_get_harvest: harvesting is not enabled");
+    CU(cudaSetDevice(c->device));
+    CU(cudaStreamSynchronize(c->stream));
+    if (features)
+        CU(cudaMemcpy(features, c->d_hfeat, sizeof(float) * 8 * c->M, cudaMemcpyDeviceToHost));
+    if (labels)
+        CU(cudaMemcpy(labels, c->d_hlab, sizeof(float) * 2 * c->M, cudaMemcpyDeviceToHost));
+    if (valid) CU(cudaMemcpy(valid, c->d_hvalid, sizeof(int) * c->M, cudaMemcpyDeviceToHost));
     return SFG_OK;
 }
 

@@ -1,0 +1,134 @@
+// ibm_interp.cuh -- interpolation of the lattice velocity at a marker with
+// the force accumulated so far, and the per-marker inputs of the learned
+// multi-direct forcing network.  Shared by the plain forcing sweeps and the
+// learned seed so that both interpolate identically.
+#pragma once
+#include "markers.cuh"
+#include "lattice.cuh"
+
+namespace sfg {
+
+// Lattice velocity at a cell for interpolation: moments of the populations
+// plus half the given force, zero on SOLID wall rows (lattice_field.cpp:28-73).
+template <typename S, typename R>
+__device__ __forceinline__ void cell_rho_j(const ChannelDev& ch, const S* __restrict__ f, int jx,
+                                           int jy, double& rho, double& jxo, double& jyo,
+                                           bool& solid) {
+    solid = !ch.periodic_y && (jy == 0 || jy == ch.ny - 1);
+    if (solid) { rho = 0.0; jxo = 0.0; jyo = 0.0; return; }
+    const long long n = (long long)jy * ch.pitch + jx;
+    R v[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) v[q] = PopIO<S, R>::load(f + ch.f_off + q * ch.plane + n, q);
+    R r, a, b;
+    cell_moments(v, r, a, b);
+    rho = (double)r;
+    jxo = (double)a;
+    jyo = (double)b;
+}
+
+__device__ __forceinline__ size_t tile_cell_index(const ChannelDev& ch, const int* tile_slot,
+                                                  int jx, int jy) {
+    const int t = ch.tile_base + (jy / TILE_H) * ch.tiles_x + (jx / TILE_W);
+    const int s = tile_slot[t];
+    return (size_t)s * 2 * TILE_CELLS + (jy % TILE_H) * TILE_W + (jx % TILE_W);
+}
+
+// u = (j + F/2)/rho at the marker's 4 x 4 stencil with the accumulated force
+// acc (immersed_boundary.cpp:174-229 with the stencil weights of the step;
+// SOLID rows and rho <= 1e-15 contribute zero).
+template <typename S, typename R>
+__device__ __forceinline__ double2 interp_u_acc(const ChannelDev& ch, const MarkerBufs& mb, int m,
+                                               const S* __restrict__ f,
+                                               const int* __restrict__ tile_slot,
+                                               const double* __restrict__ acc) {
+    const int ix0 = mb.ix0[m], iy0 = mb.iy0[m];
+    double ux = 0.0, uy = 0.0;
+    for (int iy = iy0 - 1; iy <= iy0 + 2; ++iy) {
+        for (int ix = ix0 - 1; ix <= ix0 + 2; ++ix) {
+            int jx = ix;
+            if (jx < 0) jx += ch.nx;
+            if (jx >= ch.nx) jx -= ch.nx;
+            const int jy = iy;
+            if (jy < 0 || jy >= ch.ny || jx < 0 || jx >= ch.nx) continue;
+            const double w = mb.wx[4 * m + (ix - ix0 + 1)] * mb.wy[4 * m + (iy - iy0 + 1)];
+            if (w > 1e-15) {
+                double rho, jxm, jym;
+                bool solid;
+                cell_rho_j<S, R>(ch, f, jx, jy, rho, jxm, jym, solid);
+                double cu = 0.0, cv = 0.0;
+                if (!solid && rho > 1e-15) {
+                    const size_t ci = tile_cell_index(ch, tile_slot, jx, jy);
+                    cu = (jxm + 0.5 * acc[ci]) / rho;
+                    cv = (jym + 0.5 * acc[ci + TILE_CELLS]) / rho;
+                }
+                ux += cu * w;
+                uy += cv * w;
+            }
+        }
+    }
+    return make_double2(ux, uy);
+}
+
+// Density at the node nearest to the marker, 1 outside the lattice rows
+// (immersed_boundary.cpp:262-270).
+template <typename S, typename R>
+__device__ __forceinline__ double rho_nearest(const ChannelDev& ch, const S* __restrict__ f,
+                                              double2 p) {
+    double rho_local = 1.0;
+    int ixr = (int)(p.x + 0.5), iyr = (int)(p.y + 0.5);
+    if (ixr < 0) ixr += ch.nx;
+    if (ixr >= ch.nx) ixr -= ch.nx;
+    if (iyr >= 0 && iyr < ch.ny && ixr >= 0 && ixr < ch.nx) {
+        double jxm, jym;
+        bool solid;
+        cell_rho_j<S, R>(ch, f, ixr, iyr, rho_local, jxm, jym, solid);
+    }
+    return rho_local;
+}
+
+// Inputs of the forcing network in the marker's local frame (tangent t along
+// e_prev + e_next, normal n = (-t_y, t_x)):
+//   [slip.t, slip.n, dF_prev.t, dF_prev.n, stretch, curvature, u_target.t,
+//    u_target.n], slip = u_interp - u_target, u_target = the marker velocity
+//   of the previous step (the forcing target, immersed_boundary.cpp:255),
+//   stretch = (|e_prev| + |e_next|) / (L0_prev + L0_next) - 1,
+//   curvature = atan2(e_prev x e_next, e_prev . e_next) / (0.5 (|e_prev| + |e_next|)).
+__device__ __forceinline__ void mdf_features(const ChannelDev& ch, const CapsuleDev& cp,
+                                             const MarkerBufs& mb, int m, double2 u_interp,
+                                             float* feat, double2& t, double2& nrm) {
+    const int k = m - cp.off, n = cp.n;
+    const int kp = cp.off + (k - 1 + n) % n, kn = cp.off + (k + 1) % n;
+    const double Lx = (double)ch.nx;
+    const double2 p = mb.pos[m];
+    const double2 ep = min_image_d(p, mb.pos[kp], Lx);
+    const double2 en = min_image_d(mb.pos[kn], p, Lx);
+    const double tx = ep.x + en.x, ty = ep.y + en.y;
+    const double tl = sqrt(tx * tx + ty * ty);
+    t = tl > 0.0 ? make_double2(tx / tl, ty / tl) : make_double2(1.0, 0.0);
+    nrm = make_double2(-t.y, t.x);
+    const double lp = norm_d(ep), ln = norm_d(en);
+    const double stretch = (lp + ln) / (mb.rest_len[kp] + mb.rest_len[m]) - 1.0;
+    const double curv = atan2(ep.x * en.y - ep.y * en.x, ep.x * en.x + ep.y * en.y) /
+                        (0.5 * (lp + ln));
+    const double2 ut = mb.vel[m];
+    const double2 dp = mb.dFprev[m];
+    const double sx = u_interp.x - ut.x, sy = u_interp.y - ut.y;
+    feat[0] = (float)(sx * t.x + sy * t.y);
+    feat[1] = (float)(sx * nrm.x + sy * nrm.y);
+    feat[2] = (float)(dp.x * t.x + dp.y * t.y);
+    feat[3] = (float)(dp.x * nrm.x + dp.y * nrm.y);
+    feat[4] = (float)stretch;
+    feat[5] = (float)curv;
+    feat[6] = (float)(ut.x * t.x + ut.y * t.y);
+    feat[7] = (float)(ut.x * nrm.x + ut.y * nrm.y);
+}
+
+// Per-channel maximum of a non-negative residual kept as float bits (NaN
+// becomes the largest value, so it triggers the fallback).
+__device__ __forceinline__ void atomic_max_resid(unsigned* slot, double r) {
+    const float rf = (float)r;
+    atomicMax(slot, isnan(rf) ? 0x7fc00000u : __float_as_uint(rf));
+}
+
+}  // namespace sfg

@@ -1,0 +1,146 @@
+// learned_step.cu -- the learned form of multi-direct forcing inside the step.
+//
+// After the membrane-force spread, k_mdf_learned interpolates the velocity at
+// every marker of a learned channel (the same interpolation as the plain
+// sweeps), forms the network inputs in the marker's local frame, runs the
+// network on the tensor cores for 128 markers per tile, and writes the
+// predicted correction back in the lattice frame.  The predictor is
+// the odd part of the network in (slip, previous correction): the plain
+// iteration's correction is linear in the slip field and vanishes with it.  The step then
+// spreads it (seed), runs one plain sweep, and falls back to the plain
+// iteration on channels whose no-slip residual is above the threshold.
+//
+// The network predicts the correction that the plain iteration of K sweeps
+// has accumulated before its last sweep (sweeps 1..K-2).  With an exact
+// prediction the seed reproduces the plain state before the last sweep (the
+// force G that the collision uses), and the one plain sweep that follows is
+// the plain iteration's last sweep: the step equals the plain step.
+//
+// k_harvest writes the inputs and that correction for every marker after
+// the plain iteration: the network's training data.
+#include "ibm_interp.cuh"
+#include "mlp.cuh"
+#include "sfg_internal.h"
+
+namespace sfg {
+
+template <typename S, typename R>
+__global__ void __launch_bounds__(mlp::ROWS)
+k_mdf_learned(const ChannelDev* __restrict__ chans, const CapsuleDev* __restrict__ caps, int M,
+              MarkerBufs mb, const S* __restrict__ f, const int* __restrict__ tile_slot,
+              const double* __restrict__ acc, const mlp::ModelDev* __restrict__ model,
+              unsigned* __restrict__ status) {
+    using namespace mlp;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    FwdSmem& s = *reinterpret_cast<FwdSmem*>(smem_raw);
+    load_model(s, model);
+    start_tiles(s, 128);
+    uint32_t phase = 0;
+    const int ntiles = (M + ROWS - 1) / ROWS;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int m = tile * ROWS + threadIdx.x;
+        bool active = false;
+        if (m < M) {
+            const ChannelDev& ch0 = chans[mb.mk_chan[m]];
+            active = ch0.learned && ch0.ibm_iterations > 1 && mb.valid[m];
+        }
+        if (!__syncthreads_or(active)) continue;  // uniform: no learned marker in the tile
+        float feat[N_IN];
+        double2 u0 = make_double2(0.0, 0.0), t = make_double2(1.0, 0.0),
+                nrm = make_double2(0.0, 1.0);
+        if (active) {
+            const ChannelDev& ch = chans[mb.mk_chan[m]];
+            u0 = interp_u_acc<S, R>(ch, mb, m, f, tile_slot, acc);
+            mdf_features(ch, caps[mb.mk_cap[m]], mb, m, u0, feat, t, nrm);
+        } else {
+#pragma unroll
+            for (int k = 0; k < N_IN; ++k) feat[k] = 0.0f;
+        }
+        // odd predictor: (N(x) - N(Px)) / 2 with P negating the slip and the
+        // previous correction, so no slip and no previous correction give no
+        // correction, as in the plain iteration
+        put_input_row(s, feat, active);
+        float y[2], ym[2];
+        if (!forward_tile(s, s.taddr, phase, y)) break;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) feat[k] = -feat[k];
+        put_input_row(s, feat, active);
+        if (!forward_tile(s, s.taddr, phase, ym)) break;
+        if (active) {
+            const double a = 0.5 * (double)((y[0] - ym[0]) * s.out_std[0]);
+            const double b = 0.5 * (double)((y[1] - ym[1]) * s.out_std[1]);
+            const double2 d = make_double2(a * t.x + b * nrm.x, a * t.y + b * nrm.y);
+            mb.dF[m] = d;
+            mb.dFsum[m] = d;
+            mb.u0[m] = u0;
+        }
+    }
+    if (finish_tiles(s, phase, 128) && threadIdx.x == 0) atomicOr(status, ST_TENSOR_TIMEOUT);
+}
+
+__global__ void k_harvest(const ChannelDev* __restrict__ chans, const CapsuleDev* __restrict__ caps,
+                          int M, MarkerBufs mb, float* __restrict__ feat,
+                          float* __restrict__ label, int* __restrict__ valid) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    const ChannelDev& ch = chans[mb.mk_chan[m]];
+    const bool ok = ch.ibm_iterations > 1 && mb.valid[m];
+    float fe[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    float la[2] = {0, 0};
+    if (ok) {
+        double2 t, nrm;
+        mdf_features(ch, caps[mb.mk_cap[m]], mb, m, mb.u0[m], fe, t, nrm);
+        // label: the correction accumulated before the last sweep (the sum
+        // minus that sweep's dF), which the seed stands in for
+        const double2 d = make_double2(mb.dFsum[m].x - mb.dF[m].x, mb.dFsum[m].y - mb.dF[m].y);
+        la[0] = (float)(d.x * t.x + d.y * t.y);
+        la[1] = (float)(d.x * nrm.x + d.y * nrm.y);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) feat[(size_t)m * 8 + k] = fe[k];
+    label[(size_t)m * 2 + 0] = la[0];
+    label[(size_t)m * 2 + 1] = la[1];
+    valid[m] = ok ? 1 : 0;
+}
+
+cudaError_t prepare_mdf_learned() {
+    const int smem = (int)sizeof(mlp::FwdSmem);
+    cudaError_t e = cudaFuncSetAttribute(k_mdf_learned<double, double>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_mdf_learned<float, float>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_mdf_learned<__half, float>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    return e;
+}
+
+template <typename S, typename R>
+void launch_mdf_learned(const ChannelDev* chans, const CapsuleDev* caps, int M,
+                        const MarkerBufs& mb, const S* f, TileBufs& tb, int parity,
+                        const void* model, int grid, unsigned* status, cudaStream_t st) {
+    if (M <= 0) return;
+    const int tiles = (M + mlp::ROWS - 1) / mlp::ROWS;
+    const int g = tiles < grid ? tiles : grid;
+    k_mdf_learned<S, R><<<g, mlp::ROWS, sizeof(mlp::FwdSmem), st>>>(
+        chans, caps, M, mb, f, tb.tile_slot[parity], tb.acc,
+        static_cast<const mlp::ModelDev*>(model), status);
+}
+
+void launch_harvest(const ChannelDev* chans, const CapsuleDev* caps, int M, const MarkerBufs& mb,
+                    float* feat, float* label, int* valid, cudaStream_t st) {
+    if (M <= 0) return;
+    k_harvest<<<(M + 127) / 128, 128, 0, st>>>(chans, caps, M, mb, feat, label, valid);
+}
+
+#define SFG_INST(S, R)                                                                        \
+    template void launch_mdf_learned<S, R>(const ChannelDev*, const CapsuleDev*, int,          \
+                                           const MarkerBufs&, const S*, TileBufs&, int,        \
+                                           const void*, int, unsigned*, cudaStream_t);
+SFG_INST(double, double)
+SFG_INST(float, float)
+SFG_INST(__half, float)
+#undef SFG_INST
+
+}  // namespace sfg

@@ -14,6 +14,7 @@
 #include "markers.cuh"
 #include "lattice.cuh"
 #include "sfg_internal.h"
+#include "ibm_interp.cuh"
 
 namespace sfg {
 
@@ -521,8 +522,9 @@ __global__ void __launch_bounds__(SPREAD_WARPS * 32)
 k_spread(const ChannelDev* __restrict__ chans, const int* __restrict__ tile_chan,
          const int* __restrict__ n_slots_p, const int* __restrict__ slot_tile,
          const int* __restrict__ tile_cnt, const int* __restrict__ list_off,
-         int* __restrict__ list, MarkerBufs mb, double* __restrict__ acc, R* __restrict__ gsnap,
-         R* __restrict__ fin, int sweep, int* __restrict__ capped,
+         int* __restrict__ list, MarkerBufs mb, double* __restrict__ acc,
+         double* __restrict__ acc0, R* __restrict__ gsnap, R* __restrict__ fin, int sweep,
+         int mode, const unsigned* __restrict__ resid_gate, int* __restrict__ capped,
          int* __restrict__ fluid_touched, unsigned* status) {
     __shared__ double s_acc[SPREAD_WARPS][2][TILE_CELLS];
     __shared__ int s_list[SPREAD_WARPS][SPREAD_LCAP];
@@ -539,13 +541,21 @@ k_spread(const ChannelDev* __restrict__ chans, const int* __restrict__ tile_chan
         const ChannelDev& ch = chans[chan];
         const int K = ch.ibm_iterations > 1 ? ch.ibm_iterations : 1;
         if (sweep >= K) continue;  // warp-uniform
+        if (sweep > 0 && !mdf_active(ch, mode, resid_gate, chan)) continue;  // sweep 0: all
         const int nx = ch.nx, ny = ch.ny;
         const int local = t - ch.tile_base;
         const int x0 = (local % ch.tiles_x) * TILE_W, y0 = (local / ch.tiles_x) * TILE_H;
         int cnt = tile_cnt[t];
         const int off = list_off[t];
         const int* lst;
-        if (cnt <= SPREAD_LCAP) {
+        // the lists are sorted by the step's first spread (sweep 0) and
+        // written back; later sweeps read them in order
+        const bool do_sort = (sweep == 0);
+        if (cnt <= SPREAD_LCAP && !do_sort) {
+            for (int i = lane; i < cnt; i += 32) sl[i] = list[off + i];
+            __syncwarp();
+            lst = sl;
+        } else if (cnt <= SPREAD_LCAP) {
             int pow2 = 1;
             while (pow2 < cnt) pow2 <<= 1;
             for (int i = lane; i < pow2; i += 32) sl[i] = i < cnt ? list[off + i] : INT_MAX;
@@ -561,13 +571,14 @@ k_spread(const ChannelDev* __restrict__ chans, const int* __restrict__ tile_chan
                     }
                     __syncwarp();
                 }
+            for (int i = lane; i < cnt; i += 32) list[off + i] = sl[i];
             lst = sl;
         } else {
             if (cnt > SPREAD_LIST_MAX) {
                 if (lane == 0) atomicOr(status, (unsigned)ST_LIST_OVERFLOW);
                 cnt = SPREAD_LIST_MAX;
             }
-            if (lane == 0) {  // long lists are rare: sort in place
+            if (lane == 0 && do_sort) {  // long lists are rare: sort in place
                 int* a = list + off;
                 for (int i = 1; i < cnt; ++i) {
                     const int v = a[i];
@@ -580,10 +591,12 @@ k_spread(const ChannelDev* __restrict__ chans, const int* __restrict__ tile_chan
             lst = list + off;
         }
         const size_t base = (size_t)slot * 2 * TILE_CELLS;
-        const bool last = (sweep == K - 1);
+        const bool last = mode == MDF_LEARNED ? true : (mode == MDF_SEED ? false : sweep == K - 1);
+        // a learned channel's fallback restarts from the membrane-only force
+        const double* src = (mode == MDF_PLAIN && ch.learned && sweep == 1) ? acc0 : acc;
         for (int c = lane; c < TILE_CELLS; c += 32) {
-            const double vx = sweep > 0 ? acc[base + c] : 0.0;
-            const double vy = sweep > 0 ? acc[base + TILE_CELLS + c] : 0.0;
+            const double vx = sweep > 0 ? src[base + c] : 0.0;
+            const double vy = sweep > 0 ? src[base + TILE_CELLS + c] : 0.0;
             ax[c] = vx;
             ay[c] = vy;
             if (last && K > 1) {
@@ -617,9 +630,14 @@ k_spread(const ChannelDev* __restrict__ chans, const int* __restrict__ tile_chan
             __syncwarp();
         }
         if (!last) {
+            const bool keep0 = (sweep == 0 && ch.learned);
             for (int c = lane; c < TILE_CELLS; c += 32) {
                 acc[base + c] = ax[c];
                 acc[base + TILE_CELLS + c] = ay[c];
+                if (keep0) {
+                    acc0[base + c] = ax[c];
+                    acc0[base + TILE_CELLS + c] = ay[c];
+                }
             }
             __syncwarp();
             continue;
@@ -663,82 +681,42 @@ k_spread(const ChannelDev* __restrict__ chans, const int* __restrict__ tile_chan
     }
 }
 
-// Lattice velocity at a cell for interpolation: moments of the populations
-// plus half the given force, zero on SOLID wall rows (lattice_field.cpp:28-73).
-template <typename S, typename R>
-__device__ __forceinline__ void cell_rho_j(const ChannelDev& ch, const S* __restrict__ f, int jx,
-                                           int jy, double& rho, double& jxo, double& jyo,
-                                           bool& solid) {
-    solid = !ch.periodic_y && (jy == 0 || jy == ch.ny - 1);
-    if (solid) { rho = 0.0; jxo = 0.0; jyo = 0.0; return; }
-    const long long n = (long long)jy * ch.pitch + jx;
-    R v[9];
-#pragma unroll
-    for (int q = 0; q < 9; ++q) v[q] = PopIO<S, R>::load(f + ch.f_off + q * ch.plane + n, q);
-    R r, a, b;
-    cell_moments(v, r, a, b);
-    rho = (double)r;
-    jxo = (double)a;
-    jyo = (double)b;
-}
-
-__device__ __forceinline__ size_t tile_cell_index(const ChannelDev& ch, const int* tile_slot,
-                                                  int jx, int jy) {
-    const int t = ch.tile_base + (jy / TILE_H) * ch.tiles_x + (jx / TILE_W);
-    const int s = tile_slot[t];
-    return (size_t)s * 2 * TILE_CELLS + (jy % TILE_H) * TILE_W + (jx % TILE_W);
-}
-
-// MDF correction of one sweep (immersed_boundary.cpp:355-394): interpolate
+// MDF correction of one sweep (immersed_boundary.cpp:231-286): interpolate
 // u = (j + F/2)/rho with the force spread so far, then
-// dF = 2 rho(nearest node) (U_prev - U_interp).
+// dF = 2 rho(nearest node) (U_prev - U_interp).  Also keeps the step's total
+// correction (dFsum), the first sweep's interpolation (u0) and the no-slip
+// residual max |U_prev - U_interp| per channel: at the learned form's sweep
+// (resid_gate) and at a plain iteration's last sweep (resid_plain).
 template <typename S, typename R>
 __global__ void k_mdf_interp(const ChannelDev* __restrict__ chans, int M, MarkerBufs mb,
                              const S* __restrict__ f, const int* __restrict__ tile_slot,
-                             const double* __restrict__ acc, const double* __restrict__ phi_tbl,
-                             int sweep) {
+                             const double* __restrict__ acc, const double* __restrict__ acc0,
+                             int sweep, int mode, unsigned* __restrict__ resid_gate,
+                             unsigned* __restrict__ resid_plain) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
-    const ChannelDev& ch = chans[mb.mk_chan[m]];
+    const int chan = mb.mk_chan[m];
+    const ChannelDev& ch = chans[chan];
     if (sweep >= ch.ibm_iterations || !mb.valid[m]) return;
-    const double2 p = mb.pos[m];
-    const int ix0 = mb.ix0[m], iy0 = mb.iy0[m];
-    double ux = 0.0, uy = 0.0;
-    for (int iy = iy0 - 1; iy <= iy0 + 2; ++iy) {
-        for (int ix = ix0 - 1; ix <= ix0 + 2; ++ix) {
-            int jx = ix;
-            if (jx < 0) jx += ch.nx;
-            if (jx >= ch.nx) jx -= ch.nx;
-            const int jy = iy;
-            if (jy < 0 || jy >= ch.ny || jx < 0 || jx >= ch.nx) continue;
-            const double w = mb.wx[4 * m + (ix - ix0 + 1)] * mb.wy[4 * m + (iy - iy0 + 1)];
-            if (w > 1e-15) {
-                double rho, jxm, jym;
-                bool solid;
-                cell_rho_j<S, R>(ch, f, jx, jy, rho, jxm, jym, solid);
-                double cu = 0.0, cv = 0.0;
-                if (!solid && rho > 1e-15) {
-                    const size_t ci = tile_cell_index(ch, tile_slot, jx, jy);
-                    cu = (jxm + 0.5 * acc[ci]) / rho;
-                    cv = (jym + 0.5 * acc[ci + TILE_CELLS]) / rho;
-                }
-                ux += cu * w;
-                uy += cv * w;
-            }
-        }
-    }
-    double rho_local = 1.0;
-    int ixr = (int)(p.x + 0.5), iyr = (int)(p.y + 0.5);
-    if (ixr < 0) ixr += ch.nx;
-    if (ixr >= ch.nx) ixr -= ch.nx;
-    if (iyr >= 0 && iyr < ch.ny && ixr >= 0 && ixr < ch.nx) {
-        double jxm, jym;
-        bool solid;
-        cell_rho_j<S, R>(ch, f, ixr, iyr, rho_local, jxm, jym, solid);
-    }
+    if (!mdf_active(ch, mode, resid_gate, chan)) return;
+    const double* base = (mode == MDF_PLAIN && ch.learned && sweep == 1) ? acc0 : acc;
+    const double2 u = interp_u_acc<S, R>(ch, mb, m, f, tile_slot, base);
+    const double rho_local = rho_nearest<S, R>(ch, f, mb.pos[m]);
     const double2 v = mb.vel[m];
-    const double dux = v.x - ux, duy = v.y - uy;
-    mb.dF[m] = make_double2(dux * (2.0 * rho_local), duy * (2.0 * rho_local));
+    const double dux = v.x - u.x, duy = v.y - u.y;
+    const double2 d = make_double2(dux * (2.0 * rho_local), duy * (2.0 * rho_local));
+    mb.dF[m] = d;
+    if (mode == MDF_PLAIN && sweep == 1) {
+        mb.u0[m] = u;
+        mb.dFsum[m] = d;
+    } else {
+        const double2 s0 = mb.dFsum[m];
+        mb.dFsum[m] = make_double2(s0.x + d.x, s0.y + d.y);
+    }
+    if (mode == MDF_LEARNED)
+        atomic_max_resid(&resid_gate[chan], sqrt(dux * dux + duy * duy));
+    else if (sweep == ch.ibm_iterations - 1)
+        atomic_max_resid(&resid_plain[chan], sqrt(dux * dux + duy * duy));
 }
 
 // Interpolate the new velocity and move the markers (simulation.cpp:656-675,
@@ -779,6 +757,11 @@ __global__ void k_interp_move(const ChannelDev* __restrict__ chans, int M, Marke
         }
     }
     mb.vel[m] = make_double2(ux, uy);
+    // the step's correction before its last sweep (the network's label, or
+    // on a learned step its seed) becomes the next step's network input
+    mb.dFprev[m] = (mb.valid[m] && ch.ibm_iterations > 1)
+                       ? make_double2(mb.dFsum[m].x - mb.dF[m].x, mb.dFsum[m].y - mb.dF[m].y)
+                       : make_double2(0.0, 0.0);
     p.x = p.x + ux * ch.dt;
     p.y = p.y + uy * ch.dt;
     const double Lx = (double)ch.nx;
@@ -857,25 +840,23 @@ void launch_tiles(const ChannelDev* chans, const CapsuleDev* caps, int M, const 
 
 template <typename R>
 void launch_spread(const ChannelDev* chans, const MarkerBufs& mb, TileBufs& tb, int parity,
-                   const double* phi_tbl, int sweep, int grid, unsigned* status, cudaStream_t st) {
-    (void)phi_tbl;
+                   int sweep, int mode, int grid, unsigned* status, cudaStream_t st) {
     k_spread<R><<<grid, SPREAD_WARPS * 32, 0, st>>>(
         chans, tb.tile_chan, tb.n_slots, tb.slot_tile, tb.tile_cnt, tb.list_off, tb.list, mb,
-        tb.acc, static_cast<R*>(tb.gsnap), static_cast<R*>(tb.fin[parity]), sweep, tb.capped,
-        tb.fluid_touched, status);
+        tb.acc, tb.acc0, static_cast<R*>(tb.gsnap), static_cast<R*>(tb.fin[parity]), sweep, mode,
+        tb.resid_gate, tb.capped, tb.fluid_touched, status);
 }
-template void launch_spread<double>(const ChannelDev*, const MarkerBufs&, TileBufs&, int,
-                                    const double*, int, int, unsigned*, cudaStream_t);
-template void launch_spread<float>(const ChannelDev*, const MarkerBufs&, TileBufs&, int,
-                                   const double*, int, int, unsigned*, cudaStream_t);
+template void launch_spread<double>(const ChannelDev*, const MarkerBufs&, TileBufs&, int, int,
+                                    int, int, unsigned*, cudaStream_t);
+template void launch_spread<float>(const ChannelDev*, const MarkerBufs&, TileBufs&, int, int, int,
+                                   int, unsigned*, cudaStream_t);
 
 template <typename S, typename R>
 void launch_mdf_interp(const ChannelDev* chans, int M, const MarkerBufs& mb, const S* f,
-                       TileBufs& tb, int parity, const double* phi_tbl, int sweep,
-                       cudaStream_t st) {
+                       TileBufs& tb, int parity, int sweep, int mode, cudaStream_t st) {
     const int B = 128, G = (M + B - 1) / B;
-    k_mdf_interp<S, R><<<G, B, 0, st>>>(chans, M, mb, f, tb.tile_slot[parity], tb.acc, phi_tbl,
-                                        sweep);
+    k_mdf_interp<S, R><<<G, B, 0, st>>>(chans, M, mb, f, tb.tile_slot[parity], tb.acc, tb.acc0,
+                                        sweep, mode, tb.resid_gate, tb.resid_plain);
 }
 
 template <typename S, typename R>
@@ -888,7 +869,7 @@ void launch_interp_move(const ChannelDev* chans, int M, const MarkerBufs& mb, co
 
 #define SFG_INST(S, R)                                                                          \
     template void launch_mdf_interp<S, R>(const ChannelDev*, int, const MarkerBufs&, const S*,  \
-                                          TileBufs&, int, const double*, int, cudaStream_t);    \
+                                          TileBufs&, int, int, int, cudaStream_t);              \
     template void launch_interp_move<S, R>(const ChannelDev*, int, const MarkerBufs&, const S*, \
                                            TileBufs&, int, const double*, cudaStream_t);
 SFG_INST(double, double)

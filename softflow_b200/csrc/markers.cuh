@@ -30,6 +30,10 @@ struct MarkerBufs {
     int* pair_count;    // contact pairs visited per marker (bookkeeping)
     double* wx;         // [M][4] phi(x - ix) for ix = ix0-1 .. ix0+2 (this step)
     double* wy;         // [M][4] phi(y - iy) for iy = iy0-1 .. iy0+2
+    // multi-direct forcing state of the learned form and its training data
+    double2* u0;        // velocity interpolated after the membrane-force spread
+    double2* dFsum;     // forcing correction of this step summed over its sweeps
+    double2* dFprev;    // previous step's correction before its last sweep
 };
 
 // ---------------- Peskin 4-point delta via the 1024-bin table --------------

@@ -34,6 +34,9 @@ struct TileBufs {
     void* fin[2] = {nullptr, nullptr};
     int* capped = nullptr;      // [nchan]
     int* fluid_touched = nullptr;
+    double* acc0 = nullptr;     // [max_slots][2][TILE_CELLS] force after the membrane spread
+    unsigned* resid_gate = nullptr;   // [nchan] learned form's no-slip residual (float bits)
+    unsigned* resid_plain = nullptr;  // [nchan] plain iteration's last-sweep residual
 };
 
 // Exclusive prefix sum of n ints (three kernels, graph-capturable);
@@ -51,12 +54,26 @@ void launch_contact(const ChannelDev* chans, int M, const MarkerBufs& mb, Contac
 void launch_tiles(const ChannelDev* chans, const CapsuleDev* caps, int M, const MarkerBufs& mb,
                   TileBufs& tb, int T, int parity, const double* phi_tbl, unsigned* status,
                   cudaStream_t st);
+// Spread of sweep `sweep` in forcing mode `mode` (MdfMode); sweep 0 spreads
+// the membrane and contact forces of every channel.
 template <typename R>
 void launch_spread(const ChannelDev* chans, const MarkerBufs& mb, TileBufs& tb, int parity,
-                   const double* phi_tbl, int sweep, int grid, unsigned* status, cudaStream_t st);
+                   int sweep, int mode, int grid, unsigned* status, cudaStream_t st);
 template <typename S, typename R>
 void launch_mdf_interp(const ChannelDev* chans, int M, const MarkerBufs& mb, const S* f,
-                       TileBufs& tb, int parity, const double* phi_tbl, int sweep, cudaStream_t st);
+                       TileBufs& tb, int parity, int sweep, int mode, cudaStream_t st);
+// Learned forcing: interpolation after the membrane spread, network inputs,
+// tensor-core inference, rotation back to the lattice frame -> dF, dFsum, u0
+// of every marker of a learned channel.  `model` is a mlp::ModelDev.
+template <typename S, typename R>
+void launch_mdf_learned(const ChannelDev* chans, const CapsuleDev* caps, int M,
+                        const MarkerBufs& mb, const S* f, TileBufs& tb, int parity,
+                        const void* model, int grid, unsigned* status, cudaStream_t st);
+// Training data of the step: inputs [M x 8], labels [M x 2] (the step's total
+// correction in the local frame), valid [M].
+void launch_harvest(const ChannelDev* chans, const CapsuleDev* caps, int M, const MarkerBufs& mb,
+                    float* feat, float* label, int* valid, cudaStream_t st);
+cudaError_t prepare_mdf_learned();
 template <typename S, typename R>
 void launch_interp_move(const ChannelDev* chans, int M, const MarkerBufs& mb, const S* f,
                         TileBufs& tb, int parity, const double* phi_tbl, cudaStream_t st);

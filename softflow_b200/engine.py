@@ -664,6 +664,48 @@ class Ensemble:
     def context(self) -> _Context:
         return self._need()
 
+    # ---- learned multi-direct forcing
+    def setLearnedMDF(self, net=None, threshold: float = 1e-4):
+        """Use the network `net` (softflow_b200.learned.MDFNetwork) to seed
+        the forcing correction, followed by one plain sweep, on every channel
+        with ibm_iterations >= 3; a channel whose no-slip residual exceeds
+        `threshold` (lu/step) redoes the plain sweeps.  net=None restores the
+        plain sweeps everywhere."""
+        ctx = self._need()
+        L.check(ctx._lib.sfg_set_mdf_model(ctx._h, net.handle if net is not None else None,
+                                           float(threshold)))
+        self._learned_net = net     # keeps the trainer object alive
+
+    def mdfStats(self, chan: int = 0) -> dict:
+        """Last step's no-slip residuals (learned gate, plain iteration) and
+        the cumulative learned / fallback step counts of a channel."""
+        ctx = self._need()
+        a, b = C.c_float(), C.c_float()
+        ls, fb = C.c_longlong(), C.c_longlong()
+        L.check(ctx._lib.sfg_get_mdf_stats(ctx._h, int(chan), C.byref(a), C.byref(b),
+                                           C.byref(ls), C.byref(fb)))
+        return dict(resid_learned=float(a.value), resid_plain=float(b.value),
+                    learned_steps=int(ls.value), fallbacks=int(fb.value))
+
+    def setHarvest(self, enabled: bool = True):
+        ctx = self._need()
+        L.check(ctx._lib.sfg_set_harvest(ctx._h, int(bool(enabled))))
+
+    def num_markers(self) -> int:
+        return sum(r.rest.num_nodes for ch in self._chans for r in ch.caps)
+
+    def harvest(self):
+        """(features [M, 8], labels [M, 2], valid [M] bool) of the last step."""
+        ctx = self._need()
+        M = self.num_markers()
+        feat = np.zeros((M, 8), np.float32)
+        lab = np.zeros((M, 2), np.float32)
+        val = np.zeros(M, np.int32)
+        L.check(ctx._lib.sfg_get_harvest(ctx._h, feat.ctypes.data_as(C.POINTER(C.c_float)),
+                                         lab.ctypes.data_as(C.POINTER(C.c_float)),
+                                         val.ctypes.data_as(C.POINTER(C.c_int))))
+        return feat, lab, val.astype(bool)
+
     def close(self):
         if self._ctx is not None:
             self._ctx.close()

@@ -10,8 +10,9 @@ mean-squared-error loss.
 
 Inputs per marker (local frame of the membrane: tangent t, normal n):
 slip = u_interp - u_target (t, n), previous-step forcing correction (t, n),
-stretch, curvature, u_target (t, n).  Output: the total multi-direct forcing
-correction of the step (t, n), i.e. the sum of the correction sweeps.
+stretch, curvature, u_target (t, n).  Output: the multi-direct forcing
+correction (t, n) that the plain iteration of K sweeps accumulates before its
+last sweep; the step spreads it as a seed and then runs that last sweep.
 
 Device buffers for training data are torch CUDA tensors (torch supplies
 device memory and streams only).
@@ -174,3 +175,97 @@ class MDFNetwork:
         s = C.c_int()
         L.check(self._lib.sfg_mlp_step_count(self._h, C.byref(s)))
         return int(s.value)
+
+
+# --------------------------------------------------------------- training data
+
+def harvest(ens, records: int = 1, every: int = 1, warmup: int = 0, at=None):
+    """Runs an initialized ensemble with the plain forcing sweeps and returns
+    (features, labels) of all valid markers: at the given step numbers `at`
+    (1-based, increasing), or at `records` steps spaced by `every` after
+    `warmup` steps."""
+    ens.setLearnedMDF(None)
+    if at is None:
+        at = [warmup + every * (i + 1) for i in range(int(records))]
+    ens.setHarvest(False)
+    feats, labs = [], []
+    done = 0
+    try:
+        for s_at in at:
+            if s_at - 1 > done:
+                ens.run(s_at - 1 - done)
+            ens.setHarvest(True)
+            ens.run(1)
+            done = s_at
+            f, l, v = ens.harvest()
+            v &= np.isfinite(f).all(1) & np.isfinite(l).all(1)
+            feats.append(f[v])
+            labs.append(l[v])
+            ens.setHarvest(False)
+    finally:
+        ens.setHarvest(False)
+    return np.concatenate(feats), np.concatenate(labs)
+
+
+def _geometric_steps(first: int, last: int, n: int):
+    """n distinct step numbers from first to last, spaced geometrically."""
+    v = np.unique(np.round(np.geomspace(first, last, n)).astype(int))
+    while len(v) < n:
+        v = np.unique(np.concatenate([v, v[-1:] + np.arange(1, n - len(v) + 1)]))
+    return [int(x) for x in v[:n]]
+
+
+def training_set(samples: int = 2_000_000, device: int = 0, precision: str = "fp32",
+                 c1_fraction: float = 0.1):
+    """Training data from plain runs of the single 400 x 80 channel with 30
+    capsules and of the 256-channel ensemble (synthetic, seeded placement):
+    records at steps spaced geometrically from the first step (the start-up
+    transient) to step 4000 (single channel) or 1500 (ensemble; beyond that
+    a few of its channels approach the divergence the plain method shows
+    there).  Returns (X, Y) with at most `samples` rows."""
+    from . import workloads as W
+    c1 = W.build(W.plan_c1(precision), precision, device)
+    rec1 = max(1, int(samples * c1_fraction) // max(c1.num_markers(), 1))
+    X1, Y1 = harvest(c1, at=_geometric_steps(1, 4000, rec1))
+    c1.close()
+    c3 = W.build(W.plan_c3(precision), precision, device)
+    rec3 = max(1, int(np.ceil((samples - X1.shape[0]) / max(c3.num_markers(), 1))))
+    X3, Y3 = harvest(c3, at=_geometric_steps(1, 1500, rec3))
+    c3.close()
+    X = np.concatenate([X1, X3])[:samples]
+    Y = np.concatenate([Y1, Y3])[:samples]
+    return X, Y
+
+
+# inputs that change sign with the slip field (slip and previous correction)
+ODD_INPUTS = (0, 1, 2, 3)
+
+
+def mirror(X, Y=None):
+    """P x: the inputs with the slip and the previous correction negated (and
+    -y for the labels).  The step evaluates the odd part (N(x) - N(Px)) / 2."""
+    Xm = np.array(X, dtype=np.float32, copy=True)
+    Xm[:, list(ODD_INPUTS)] *= -1.0
+    return Xm if Y is None else (Xm, -np.asarray(Y, dtype=np.float32))
+
+
+def predict(net: "MDFNetwork", X) -> np.ndarray:
+    """The step's predictor on host data: (N(x) - N(Px)) / 2."""
+    a = net.forward(X).cpu().numpy()
+    b = net.forward(mirror(X)).cpu().numpy()
+    return 0.5 * (a - b)
+
+
+def train_network(X, Y, device: int = 0, epochs: int = 8, batch: int = 8192, lr: float = 1e-3,
+                  seed: int = 1):
+    """Trains a fresh network with Adam on the tensor cores on the samples and
+    their mirror images (P x, -y), so that the network is close to odd and
+    its odd part, which the step evaluates, keeps what it learned; fits the
+    normalisation to the mirrored set.  Returns (network, batch losses)."""
+    Xm, Ym = mirror(X, Y)
+    XA = np.concatenate([np.asarray(X, np.float32), Xm])
+    YA = np.concatenate([np.asarray(Y, np.float32), Ym])
+    net = MDFNetwork(device, seed=seed)
+    net.fit_normalization(XA, YA)
+    losses = net.train(XA, YA, epochs=epochs, batch=batch, lr=lr, seed=seed)
+    return net, losses
