@@ -54,6 +54,10 @@ def parse():
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the per-channel plain form")
+    ap.add_argument("--mdf", default="auto", choices=["auto", "learned", "plain"],
+                    help="forcing form of the timed run (auto: learned on the ensemble)")
+    ap.add_argument("--mdf-threshold", type=float, default=1e-4,
+                    help="no-slip residual (lu/step) above which a learned channel falls back")
     return ap.parse_args()
 
 
@@ -184,7 +188,22 @@ def run_product(args, world, rank, local, pg):
     import softflow_b200 as S
     from softflow_b200 import workloads as W
     plans = make_plans(args.workload, args.precision, world, rank)
+    learned = args.mdf == "learned" or (args.mdf == "auto" and args.workload == "c3")
+    learn_info = None
+    net = None
+    if learned:
+        # the network, trained here on plain runs (untimed, seeded)
+        from softflow_b200.learned import training_set, train_network
+        t0 = time.perf_counter()
+        X, Y = training_set(2_000_000, device=local)
+        net, losses = train_network(X, Y, device=local, epochs=8, seed=1)
+        learn_info = {"samples": int(X.shape[0]), "adam_steps": int(losses.size),
+                      "loss_first": float(losses[0]), "loss_last": float(losses[-1]),
+                      "setup_s": time.perf_counter() - t0}
+        del X, Y
     ens = W.build(plans, precision=args.precision, device=local)
+    if learned:
+        ens.setLearnedMDF(net, threshold=args.mdf_threshold)
     ctx = ens.context()
     cells, caps, markers, scal = W.totals(plans, ens)
     nch = len(plans)
@@ -192,17 +211,29 @@ def run_product(args, world, rank, local, pg):
     # warm-up (graphs are built on the first call)
     ctx.step(args.warmup)
     ctx.synchronize()
+    stats0 = [ens.mdfStats(c) for c in range(nch)] if learned else None
 
+    import torch
     clocks = ClockSampler(local)
     clocks.start()
     barrier(pg, local)
+    torch.cuda.nvtx.range_push("timed")
     ctx.step(args.steps)
     ctx.synchronize()
+    torch.cuda.nvtx.range_pop()
     ms = ctx.last_step_ms()
     barrier(pg, local)
     clk = clocks.stop()
     ms_max = allmax(pg, ms)
     launches = ctx.launches_per_step()
+    if learned:
+        st = [ens.mdfStats(c) for c in range(nch)]
+        ls = sum(a["learned_steps"] - b["learned_steps"] for a, b in zip(st, stats0))
+        fb = sum(a["fallbacks"] - b["fallbacks"] for a, b in zip(st, stats0))
+        learn_info.update({"threshold": args.mdf_threshold,
+                           "fallback_fraction": fb / ls if ls else None,
+                           "gate_residual_median": float(np.median([a["resid_learned"] for a in st])),
+                           "gate_residual_max": float(np.max([a["resid_learned"] for a in st]))})
 
     sec = ms_max / 1e3
     cap_steps = caps * args.steps * world / sec
@@ -227,6 +258,25 @@ def run_product(args, world, rank, local, pg):
     # e2e: host-resident initial state, per-step marker readback
     e2e = run_e2e(args, plans, ens, pg, local)
 
+    # the same ensemble with the plain forcing sweeps (same steps, same clock)
+    batched_plain = None
+    if learned:
+        ens.close()
+        ensp = W.build(plans, precision=args.precision, device=local)
+        cp = ensp.context()
+        cp.step(args.warmup)
+        cp.synchronize()
+        cp.step(args.steps)
+        cp.synchronize()
+        pms = allmax(pg, cp.last_step_ms())
+        batched_plain = {"value": caps * args.steps * world / (pms / 1e3),
+                         "unit": "capsule-steps/s", "ms_per_step": pms / args.steps,
+                         "form": "same ensemble and precision, plain forcing sweeps",
+                         "gate_residual_median_plain": float(np.median(
+                             [ensp.mdfStats(c)["resid_plain"] for c in range(nch)]))}
+        ensp.close()
+        ens = None
+
     # plain per-channel form (each channel its own context, run one after the other)
     plain = None
     if args.workload == "c3" and not args.no_plain:
@@ -248,6 +298,9 @@ def run_product(args, world, rank, local, pg):
         "config": {"workload": args.workload, "channels": nch, "fluid_cells": cells,
                    "capsules": caps, "markers": markers, "precision": args.precision,
                    "mdf_sweeps": max(p.params.ibm_iterations for p in plans),
+                   "mdf": ("learned: network seed for sweeps 1..K-2, last plain sweep, "
+                           f"plain fallback above {args.mdf_threshold:g} lu/step")
+                          if learned else "plain",
                    "l2": "state larger than L2 (no flush needed)" if alg_bytes > 126e6
                          else "state fits L2 (L2-resident workload)",
                    "parallelism": (f"channel shards x{world} (256 distinct channels per rank)"
@@ -264,10 +317,15 @@ def run_product(args, world, rank, local, pg):
         "e2e": e2e,
         "clocks": clk,
     }
+    if learn_info is not None:
+        out["learned_mdf"] = learn_info
+    if batched_plain is not None:
+        out["batched_plain"] = batched_plain
     if plain is not None:
         out["plain"] = plain
         out["batched_vs_plain"] = cap_steps / world / plain["value"] if plain["value"] else None
-    ens.close()
+    if ens is not None:
+        ens.close()
     return out
 
 

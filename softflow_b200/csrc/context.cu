@@ -191,6 +191,9 @@ struct sfg_context {
     float* d_hfeat = nullptr;           // [M][8]
     float* d_hlab = nullptr;            // [M][2]
     int* d_hvalid = nullptr;            // [M]
+    int* d_plain_needed = nullptr;      // [1] see TileBufs::plain_needed
+    float* d_feat = nullptr;            // [M][8] network inputs of the step
+    double2* d_frame = nullptr;         // [M] local tangent of each marker
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int launches = 0;
     // per-phase timing (profiling mode runs the step eagerly)
@@ -264,10 +267,10 @@ static void free_all(sfg_context* c) {
     F(c->tb.tile_chan); F(c->tb.tile_flag); F(c->tb.tile_cnt); F(c->tb.cursor);
     F(c->tb.slot_scan); F(c->tb.list_off); F(c->tb.slot_tile); F(c->tb.n_slots);
     F(c->tb.list); F(c->tb.scan_tmp); F(c->tb.acc); F(c->tb.gsnap); F(c->tb.capped);
-    F(c->tb.fluid_touched); F(c->tb.acc0); F(c->tb.resid_gate); F(c->tb.resid_plain);
+    F(c->tb.fluid_touched); F(c->tb.acc0); F(c->tb.mom); F(c->tb.resid_gate); F(c->tb.resid_plain);
     F(c->mb.u0); F(c->mb.dFsum); F(c->mb.dFprev);
     F(c->d_model); F(c->d_learned_steps); F(c->d_fallbacks);
-    F(c->d_hfeat); F(c->d_hlab); F(c->d_hvalid);
+    F(c->d_hfeat); F(c->d_hlab); F(c->d_hvalid); F(c->d_feat); F(c->d_frame); F(c->d_plain_needed);
     F(c->cb.cell_of); F(c->cb.cell_cnt); F(c->cb.cell_start); F(c->cb.cursor); F(c->cb.list);
     F(c->cb.scan_tmp);
     F(c->d_phi); F(c->d_stepped); F(c->d_adr_pending); F(c->d_c_fresh); F(c->d_status);
@@ -480,6 +483,7 @@ extern "C" int sfg_initialize(sfg_context* c) {
     if (membrane_smem_bytes(c->maxn) > 227 * 1024)
         return fail(SFG_ERR_CAPACITY, "sfg_initialize: capsules with more than 640 nodes");
     if (c->maxn > 0) CU(prepare_membrane(c->maxn));
+    CU(prepare_spread());
 
     std::vector<ChannelDev> dch(nch);
     for (int i = 0; i < nch; ++i) dch[i] = c->ch[i].d;
@@ -593,6 +597,7 @@ extern "C" int sfg_initialize(sfg_context* c) {
     CU(dalloc(&tb.scan_tmp, scan_tmp_ints(T)));
     CU(dalloc(&tb.acc, (size_t)tb.max_slots * 2 * TILE_CELLS));
     CU(cudaMalloc(&tb.gsnap, (size_t)tb.max_slots * 2 * TILE_CELLS * c->real_size()));
+    if (c->Kmax > 1) CU(cudaMalloc(&tb.mom, (size_t)tb.max_slots * TILE_CELLS * 4 * c->real_size()));
     CU(dalloc(&tb.capped, nch));
     CU(dalloc(&tb.fluid_touched, nch));
     CU(cudaMemset(tb.capped, 0, sizeof(int) * nch));
@@ -692,21 +697,28 @@ static int enqueue_step_t(sfg_context* c, int p) {
         mark(c, SFG_PHASE_IBM_SPREAD);
         launches += 1 + (c->ncells > 0 ? 7 : 1) + 9 + 1;
         const S* fp = static_cast<const S*>(c->f[p]);
+        if (c->Kmax > 1) {
+            launch_tile_moments<S, R>(c->d_chans, fp, c->tb, c->spread_grid, st);
+            mark(c, SFG_PHASE_MDF_INTERP);
+            launches += 1;
+        }
         if (c->any_learned) {
             // seed, one plain sweep, gate; the plain sweeps below run only for
             // channels above the threshold
             launch_mdf_learned<S, R>(c->d_chans, c->d_caps, c->M, c->mb, fp, c->tb, p,
-                                     c->d_model, c->learned_grid, c->d_status, st);
+                                     c->d_model, c->d_feat, c->d_frame, c->learned_grid,
+                                     c->d_status, st);
             mark(c, SFG_PHASE_MDF_LEARNED);
             launch_spread<R>(c->d_chans, c->mb, c->tb, p, 1, MDF_SEED, c->spread_grid,
                              c->d_status, st);
             mark(c, SFG_PHASE_IBM_SPREAD);
             launch_mdf_interp<S, R>(c->d_chans, c->M, c->mb, fp, c->tb, p, 2, MDF_LEARNED, st);
             mark(c, SFG_PHASE_MDF_INTERP);
+            launch_plain_needed(c->d_chans, nch, c->tb, st);
             launch_spread<R>(c->d_chans, c->mb, c->tb, p, 2, MDF_LEARNED, c->spread_grid,
                              c->d_status, st);
             mark(c, SFG_PHASE_IBM_SPREAD);
-            launches += 4;
+            launches += 6;
         }
         for (int k = 1; k < c->Kmax; ++k) {
             launch_mdf_interp<S, R>(c->d_chans, c->M, c->mb, fp, c->tb, p, k, MDF_PLAIN, st);
@@ -859,6 +871,11 @@ extern "C" int sfg_set_mdf_model(sfg_context* c, sfg_mlp* net, double residual_t
                            c->stream));
         if (!c->tb.acc0 && c->M > 0)
             CU(dalloc(&c->tb.acc0, (size_t)c->tb.max_slots * 2 * TILE_CELLS));
+        if (!c->d_plain_needed) CU(dalloc(&c->d_plain_needed, 1));
+        if (!c->d_feat && c->M > 0) {
+            CU(dalloc(&c->d_feat, 8LL * c->M));
+            CU(dalloc(&c->d_frame, c->M));
+        }
     }
     for (auto& h : c->ch) {
         const bool on = net && h.d.ibm_iterations >= 3 && h.d.cap_end > h.d.cap_begin;
@@ -872,6 +889,7 @@ extern "C" int sfg_set_mdf_model(sfg_context* c, sfg_mlp* net, double residual_t
                        cudaMemcpyHostToDevice, c->stream));
     CU(cudaStreamSynchronize(c->stream));
     c->any_learned = any;
+    c->tb.plain_needed = any ? c->d_plain_needed : nullptr;
     drop_graphs(c);
     return SFG_OK;
 }

@@ -37,11 +37,11 @@ __device__ __forceinline__ size_t tile_cell_index(const ChannelDev& ch, const in
 // u = (j + F/2)/rho at the marker's 4 x 4 stencil with the accumulated force
 // acc (immersed_boundary.cpp:174-229 with the stencil weights of the step;
 // SOLID rows and rho <= 1e-15 contribute zero).
-template <typename S, typename R>
+template <typename S, typename R, typename A = double>
 __device__ __forceinline__ double2 interp_u_acc(const ChannelDev& ch, const MarkerBufs& mb, int m,
                                                const S* __restrict__ f,
                                                const int* __restrict__ tile_slot,
-                                               const double* __restrict__ acc) {
+                                               const A* __restrict__ acc) {
     const int ix0 = mb.ix0[m], iy0 = mb.iy0[m];
     double ux = 0.0, uy = 0.0;
     for (int iy = iy0 - 1; iy <= iy0 + 2; ++iy) {
@@ -59,8 +59,8 @@ __device__ __forceinline__ double2 interp_u_acc(const ChannelDev& ch, const Mark
                 double cu = 0.0, cv = 0.0;
                 if (!solid && rho > 1e-15) {
                     const size_t ci = tile_cell_index(ch, tile_slot, jx, jy);
-                    cu = (jxm + 0.5 * acc[ci]) / rho;
-                    cv = (jym + 0.5 * acc[ci + TILE_CELLS]) / rho;
+                    cu = (jxm + 0.5 * (double)acc[ci]) / rho;
+                    cv = (jym + 0.5 * (double)acc[ci + TILE_CELLS]) / rho;
                 }
                 ux += cu * w;
                 uy += cv * w;
@@ -68,6 +68,71 @@ __device__ __forceinline__ double2 interp_u_acc(const ChannelDev& ch, const Mark
         }
     }
     return make_double2(ux, uy);
+}
+
+// Moments (rho, jx, jy) of a force tile's cells, computed once per step
+// (k_tile_moments) because the populations do not change during the forcing
+// sweeps: [slot][TILE_CELLS] records of R, rho = 0 on SOLID rows (where the
+// reference's interpolation and density lookup give 0) and outside the
+// channel.
+template <typename R> struct Mom4;
+template <> struct Mom4<double> { using T = double4; };
+template <> struct Mom4<float> { using T = float4; };
+
+__device__ __forceinline__ size_t tile_cell_mom(const ChannelDev& ch, const int* tile_slot, int jx,
+                                                int jy) {
+    const int t = ch.tile_base + (jy / TILE_H) * ch.tiles_x + (jx / TILE_W);
+    return (size_t)tile_slot[t] * TILE_CELLS + (jy % TILE_H) * TILE_W + (jx % TILE_W);
+}
+
+// interp_u_acc with the step's tile moments: the same terms in the same
+// order, so the same result bit for bit.
+template <typename R>
+__device__ __forceinline__ double2 interp_u_mom(const ChannelDev& ch, const MarkerBufs& mb, int m,
+                                               const int* __restrict__ tile_slot,
+                                               const typename Mom4<R>::T* __restrict__ mom,
+                                               const double* __restrict__ acc) {
+    const int ix0 = mb.ix0[m], iy0 = mb.iy0[m];
+    double ux = 0.0, uy = 0.0;
+#pragma unroll
+    for (int sy = 0; sy < 4; ++sy) {
+#pragma unroll
+        for (int sx = 0; sx < 4; ++sx) {
+            int jx = ix0 - 1 + sx;
+            const int jy = iy0 - 1 + sy;
+            if (jx < 0) jx += ch.nx;
+            if (jx >= ch.nx) jx -= ch.nx;
+            if (jy < 0 || jy >= ch.ny || jx < 0 || jx >= ch.nx) continue;
+            const double w = mb.wx[4 * m + sx] * mb.wy[4 * m + sy];
+            if (w > 1e-15) {
+                const size_t cm = tile_cell_mom(ch, tile_slot, jx, jy);
+                const auto q = mom[cm];
+                const double rho = (double)q.x;
+                double cu = 0.0, cv = 0.0;
+                if (rho > 1e-15) {
+                    const size_t ci = (cm / TILE_CELLS) * 2 * TILE_CELLS + cm % TILE_CELLS;
+                    cu = ((double)q.y + 0.5 * acc[ci]) / rho;
+                    cv = ((double)q.z + 0.5 * acc[ci + TILE_CELLS]) / rho;
+                }
+                ux += cu * w;
+                uy += cv * w;
+            }
+        }
+    }
+    return make_double2(ux, uy);
+}
+
+// rho_nearest with the tile moments (the nearest node lies in the stencil).
+template <typename R>
+__device__ __forceinline__ double rho_nearest_mom(const ChannelDev& ch, const int* tile_slot,
+                                                  const typename Mom4<R>::T* __restrict__ mom,
+                                                  double2 p) {
+    int ixr = (int)(p.x + 0.5), iyr = (int)(p.y + 0.5);
+    if (ixr < 0) ixr += ch.nx;
+    if (ixr >= ch.nx) ixr -= ch.nx;
+    if (iyr >= 0 && iyr < ch.ny && ixr >= 0 && ixr < ch.nx)
+        return (double)mom[tile_cell_mom(ch, tile_slot, ixr, iyr)].x;
+    return 1.0;
 }
 
 // Density at the node nearest to the marker, 1 outside the lattice rows

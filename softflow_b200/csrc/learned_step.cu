@@ -1,10 +1,10 @@
 // learned_step.cu -- the learned form of multi-direct forcing inside the step.
 //
-// After the membrane-force spread, k_mdf_learned interpolates the velocity at
-// every marker of a learned channel (the same interpolation as the plain
-// sweeps), forms the network inputs in the marker's local frame, runs the
-// network on the tensor cores for 128 markers per tile, and writes the
-// predicted correction back in the lattice frame.  The predictor is
+// After the membrane-force spread, k_mdf_features interpolates the velocity
+// at every marker of a learned channel (the same interpolation as the plain
+// sweeps) and forms the network inputs in the marker's local frame;
+// k_mdf_seed runs the network on the tensor cores for 128 markers per tile
+// and writes the predicted correction back in the lattice frame.  The predictor is
 // the odd part of the network in (slip, previous correction): the plain
 // iteration's correction is linear in the slip field and vanishes with it.  The step then
 // spreads it (seed), runs one plain sweep, and falls back to the plain
@@ -24,12 +24,44 @@
 
 namespace sfg {
 
-template <typename S, typename R>
+__device__ __forceinline__ bool learned_marker(const ChannelDev* __restrict__ chans,
+                                               const MarkerBufs& mb, int m) {
+    const ChannelDev& ch = chans[mb.mk_chan[m]];
+    return ch.learned && ch.ibm_iterations > 1 && mb.valid[m];
+}
+
+// Interpolation after the membrane spread (with the step's tile moments) and
+// the network inputs of every marker of a learned channel: u0, feat [M][8] and
+// the local tangent frame [M].
+template <typename R>
+__global__ void k_mdf_features(const ChannelDev* __restrict__ chans,
+                               const CapsuleDev* __restrict__ caps, int M, MarkerBufs mb,
+                               const int* __restrict__ tile_slot,
+                               const typename Mom4<R>::T* __restrict__ mom,
+                               const double* __restrict__ acc, float* __restrict__ feat,
+                               double2* __restrict__ frame) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M || !learned_marker(chans, mb, m)) return;
+    const ChannelDev& ch = chans[mb.mk_chan[m]];
+    const double2 u0 = interp_u_mom<R>(ch, mb, m, tile_slot, mom, acc);
+    float fe[8];
+    double2 t, nrm;
+    mdf_features(ch, caps[mb.mk_cap[m]], mb, m, u0, fe, t, nrm);
+    float4* out = reinterpret_cast<float4*>(feat + 8 * (size_t)m);
+    out[0] = make_float4(fe[0], fe[1], fe[2], fe[3]);
+    out[1] = make_float4(fe[4], fe[5], fe[6], fe[7]);
+    frame[m] = t;
+    mb.u0[m] = u0;
+}
+
+// The network's seed for 128 markers per tile on the tensor cores.  The
+// predictor is the odd part (N(x) - N(Px)) / 2, P negating the slip and the
+// previous correction: no slip and no previous correction give no
+// correction, as in the plain iteration.
 __global__ void __launch_bounds__(mlp::ROWS)
-k_mdf_learned(const ChannelDev* __restrict__ chans, const CapsuleDev* __restrict__ caps, int M,
-              MarkerBufs mb, const S* __restrict__ f, const int* __restrict__ tile_slot,
-              const double* __restrict__ acc, const mlp::ModelDev* __restrict__ model,
-              unsigned* __restrict__ status) {
+k_mdf_seed(const ChannelDev* __restrict__ chans, int M, MarkerBufs mb,
+           const float* __restrict__ feat, const double2* __restrict__ frame,
+           const mlp::ModelDev* __restrict__ model, unsigned* __restrict__ status) {
     using namespace mlp;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     FwdSmem& s = *reinterpret_cast<FwdSmem*>(smem_raw);
@@ -39,40 +71,32 @@ k_mdf_learned(const ChannelDev* __restrict__ chans, const CapsuleDev* __restrict
     const int ntiles = (M + ROWS - 1) / ROWS;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int m = tile * ROWS + threadIdx.x;
-        bool active = false;
-        if (m < M) {
-            const ChannelDev& ch0 = chans[mb.mk_chan[m]];
-            active = ch0.learned && ch0.ibm_iterations > 1 && mb.valid[m];
-        }
+        const bool active = m < M && learned_marker(chans, mb, m);
         if (!__syncthreads_or(active)) continue;  // uniform: no learned marker in the tile
-        float feat[N_IN];
-        double2 u0 = make_double2(0.0, 0.0), t = make_double2(1.0, 0.0),
-                nrm = make_double2(0.0, 1.0);
+        float fe[N_IN];
         if (active) {
-            const ChannelDev& ch = chans[mb.mk_chan[m]];
-            u0 = interp_u_acc<S, R>(ch, mb, m, f, tile_slot, acc);
-            mdf_features(ch, caps[mb.mk_cap[m]], mb, m, u0, feat, t, nrm);
+            const float4* in = reinterpret_cast<const float4*>(feat + 8 * (size_t)m);
+            const float4 a = in[0], b = in[1];
+            fe[0] = a.x; fe[1] = a.y; fe[2] = a.z; fe[3] = a.w;
+            fe[4] = b.x; fe[5] = b.y; fe[6] = b.z; fe[7] = b.w;
         } else {
 #pragma unroll
-            for (int k = 0; k < N_IN; ++k) feat[k] = 0.0f;
+            for (int k = 0; k < N_IN; ++k) fe[k] = 0.0f;
         }
-        // odd predictor: (N(x) - N(Px)) / 2 with P negating the slip and the
-        // previous correction, so no slip and no previous correction give no
-        // correction, as in the plain iteration
-        put_input_row(s, feat, active);
+        put_input_row(s, fe, active);
         float y[2], ym[2];
         if (!forward_tile(s, s.taddr, phase, y)) break;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) feat[k] = -feat[k];
-        put_input_row(s, feat, active);
+        for (int k = 0; k < 4; ++k) fe[k] = -fe[k];
+        put_input_row(s, fe, active);
         if (!forward_tile(s, s.taddr, phase, ym)) break;
         if (active) {
             const double a = 0.5 * (double)((y[0] - ym[0]) * s.out_std[0]);
             const double b = 0.5 * (double)((y[1] - ym[1]) * s.out_std[1]);
-            const double2 d = make_double2(a * t.x + b * nrm.x, a * t.y + b * nrm.y);
+            const double2 t = frame[m];
+            const double2 d = make_double2(a * t.x - b * t.y, a * t.y + b * t.x);
             mb.dF[m] = d;
             mb.dFsum[m] = d;
-            mb.u0[m] = u0;
         }
     }
     if (finish_tiles(s, phase, 128) && threadIdx.x == 0) atomicOr(status, ST_TENSOR_TIMEOUT);
@@ -104,28 +128,24 @@ __global__ void k_harvest(const ChannelDev* __restrict__ chans, const CapsuleDev
 }
 
 cudaError_t prepare_mdf_learned() {
-    const int smem = (int)sizeof(mlp::FwdSmem);
-    cudaError_t e = cudaFuncSetAttribute(k_mdf_learned<double, double>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_mdf_learned<float, float>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_mdf_learned<__half, float>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    return e;
+    return cudaFuncSetAttribute(k_mdf_seed, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(mlp::FwdSmem));
 }
 
 template <typename S, typename R>
 void launch_mdf_learned(const ChannelDev* chans, const CapsuleDev* caps, int M,
                         const MarkerBufs& mb, const S* f, TileBufs& tb, int parity,
-                        const void* model, int grid, unsigned* status, cudaStream_t st) {
+                        const void* model, float* feat, double2* frame, int grid,
+                        unsigned* status, cudaStream_t st) {
     if (M <= 0) return;
+    (void)f;
+    k_mdf_features<R><<<(M + 127) / 128, 128, 0, st>>>(
+        chans, caps, M, mb, tb.tile_slot[parity], static_cast<const typename Mom4<R>::T*>(tb.mom),
+        tb.acc, feat, frame);
     const int tiles = (M + mlp::ROWS - 1) / mlp::ROWS;
     const int g = tiles < grid ? tiles : grid;
-    k_mdf_learned<S, R><<<g, mlp::ROWS, sizeof(mlp::FwdSmem), st>>>(
-        chans, caps, M, mb, f, tb.tile_slot[parity], tb.acc,
-        static_cast<const mlp::ModelDev*>(model), status);
+    k_mdf_seed<<<g, mlp::ROWS, sizeof(mlp::FwdSmem), st>>>(
+        chans, M, mb, feat, frame, static_cast<const mlp::ModelDev*>(model), status);
 }
 
 void launch_harvest(const ChannelDev* chans, const CapsuleDev* caps, int M, const MarkerBufs& mb,
@@ -137,7 +157,8 @@ void launch_harvest(const ChannelDev* chans, const CapsuleDev* caps, int M, cons
 #define SFG_INST(S, R)                                                                        \
     template void launch_mdf_learned<S, R>(const ChannelDev*, const CapsuleDev*, int,          \
                                            const MarkerBufs&, const S*, TileBufs&, int,        \
-                                           const void*, int, unsigned*, cudaStream_t);
+                                           const void*, float*, double2*, int, unsigned*,      \
+                                           cudaStream_t);
 SFG_INST(double, double)
 SFG_INST(float, float)
 SFG_INST(__half, float)

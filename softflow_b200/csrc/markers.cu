@@ -505,8 +505,20 @@ __device__ __forceinline__ bool stencil_ix(int jx, int ix0, int nx, int& ix) {
 }
 
 constexpr int SPREAD_WARPS = 8;       // force tiles processed per CTA (one per warp)
-constexpr int SPREAD_LCAP = 384;      // list entries sorted in shared memory per warp
+constexpr int SPREAD_LCAP = 256;      // list entries sorted in shared memory per warp
+                                      // (a power of two: the bitonic sort pads to one)
 constexpr int SPREAD_LIST_MAX = 4096; // longer lists are clamped and flagged
+
+// Shared memory of one spread warp: the tile's accumulators, its sorted
+// marker list and a staging chunk of 32 markers.
+struct SpreadWarpSmem {
+    double ax[TILE_CELLS], ay[TILE_CELLS];
+    double fx[32], fy[32], ds[32];
+    double wx[32][4], wy[32][4];
+    int ix[32], iy[32], ok[32];
+    int list[SPREAD_LCAP];
+};
+constexpr size_t SPREAD_SMEM = sizeof(SpreadWarpSmem) * SPREAD_WARPS;
 
 // Deterministic spread into force tiles for MDF sweep `sweep`.  Sweep 0
 // spreads the membrane + contact forces (immersed_boundary.cpp:25-100);
@@ -524,14 +536,16 @@ k_spread(const ChannelDev* __restrict__ chans, const int* __restrict__ tile_chan
          const int* __restrict__ tile_cnt, const int* __restrict__ list_off,
          int* __restrict__ list, MarkerBufs mb, double* __restrict__ acc,
          double* __restrict__ acc0, R* __restrict__ gsnap, R* __restrict__ fin, int sweep,
-         int mode, const unsigned* __restrict__ resid_gate, int* __restrict__ capped,
+         int mode, const unsigned* __restrict__ resid_gate,
+         const int* __restrict__ plain_needed, int* __restrict__ capped,
          int* __restrict__ fluid_touched, unsigned* status) {
-    __shared__ double s_acc[SPREAD_WARPS][2][TILE_CELLS];
-    __shared__ int s_list[SPREAD_WARPS][SPREAD_LCAP];
+    if (sweep > 0 && mode == MDF_PLAIN && plain_needed && !*plain_needed) return;
+    extern __shared__ __align__(16) unsigned char spread_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double* ax = s_acc[warp][0];
-    double* ay = s_acc[warp][1];
-    int* sl = s_list[warp];
+    SpreadWarpSmem& W = reinterpret_cast<SpreadWarpSmem*>(spread_smem)[warp];
+    double* ax = W.ax;
+    double* ay = W.ay;
+    int* sl = W.list;
     const int n_slots = *n_slots_p;
     const int sx = lane & 3, sy = (lane >> 2) & 3;
     for (int slot = blockIdx.x * SPREAD_WARPS + warp; slot < n_slots;
@@ -605,29 +619,48 @@ k_spread(const ChannelDev* __restrict__ chans, const int* __restrict__ tile_chan
             }
         }
         __syncwarp();
-        for (int i = 0; i < cnt; ++i) {
-            const int m = lst[i];
-            if (lane < 16) {
+        // markers in list order, staged 32 at a time: each lane loads one
+        // marker's force, stencil origin, ds and weights (the loads of a
+        // chunk are in flight together), then the half-warp adds them in
+        // order, one stencil point per lane
+        for (int c0 = 0; c0 < cnt; c0 += 32) {
+            const int nb = cnt - c0 < 32 ? cnt - c0 : 32;
+            if (lane < nb) {
+                const int m = lst[c0 + lane];
                 const double2 fo = sweep == 0 ? mb.frc[m] : mb.dF[m];
-                if (!(isnan(fo.x) || isnan(fo.y))) {
-                    const int iy = mb.iy0[m] - 1 + sy;
-                    int jx = mb.ix0[m] - 1 + sx;
+                W.fx[lane] = fo.x;
+                W.fy[lane] = fo.y;
+                W.ok[lane] = !(isnan(fo.x) || isnan(fo.y));
+                W.ix[lane] = mb.ix0[m];
+                W.iy[lane] = mb.iy0[m];
+                W.ds[lane] = mb.ds[m];
+                const double2* wx2 = reinterpret_cast<const double2*>(mb.wx + 4 * (size_t)m);
+                const double2* wy2 = reinterpret_cast<const double2*>(mb.wy + 4 * (size_t)m);
+                const double2 a0 = wx2[0], a1 = wx2[1], b0 = wy2[0], b1 = wy2[1];
+                W.wx[lane][0] = a0.x; W.wx[lane][1] = a0.y; W.wx[lane][2] = a1.x; W.wx[lane][3] = a1.y;
+                W.wy[lane][0] = b0.x; W.wy[lane][1] = b0.y; W.wy[lane][2] = b1.x; W.wy[lane][3] = b1.y;
+            }
+            __syncwarp();
+            for (int j = 0; j < nb; ++j) {
+                if (lane < 16 && W.ok[j]) {
+                    const int iy = W.iy[j] - 1 + sy;
+                    int jx = W.ix[j] - 1 + sx;
                     if (jx < 0) jx += nx;
                     if (jx >= nx) jx -= nx;
                     const int cxl = jx - x0, cyl = iy - y0;
                     if (iy >= 0 && iy < ny && cxl >= 0 && cxl < TILE_W && cyl >= 0 &&
                         cyl < TILE_H) {
-                        const double w = mb.wx[4 * m + sx] * mb.wy[4 * m + sy];
+                        const double w = W.wx[j][sx] * W.wy[j][sy];
                         if (w > 1e-15) {
-                            const double ds = mb.ds[m];
+                            const double ds = W.ds[j];
                             const int c = cyl * TILE_W + cxl;
-                            ax[c] += fo.x * w * ds;
-                            ay[c] += fo.y * w * ds;
+                            ax[c] += W.fx[j] * w * ds;
+                            ay[c] += W.fy[j] * w * ds;
                         }
                     }
                 }
+                __syncwarp();
             }
-            __syncwarp();
         }
         if (!last) {
             const bool keep0 = (sweep == 0 && ch.learned);
@@ -689,10 +722,13 @@ k_spread(const ChannelDev* __restrict__ chans, const int* __restrict__ tile_chan
 // (resid_gate) and at a plain iteration's last sweep (resid_plain).
 template <typename S, typename R>
 __global__ void k_mdf_interp(const ChannelDev* __restrict__ chans, int M, MarkerBufs mb,
-                             const S* __restrict__ f, const int* __restrict__ tile_slot,
+                             const int* __restrict__ tile_slot,
+                             const typename Mom4<R>::T* __restrict__ mom,
                              const double* __restrict__ acc, const double* __restrict__ acc0,
                              int sweep, int mode, unsigned* __restrict__ resid_gate,
-                             unsigned* __restrict__ resid_plain) {
+                             unsigned* __restrict__ resid_plain,
+                             const int* __restrict__ plain_needed) {
+    if (mode == MDF_PLAIN && plain_needed && !*plain_needed) return;  // no channel needs it
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
     const int chan = mb.mk_chan[m];
@@ -700,8 +736,8 @@ __global__ void k_mdf_interp(const ChannelDev* __restrict__ chans, int M, Marker
     if (sweep >= ch.ibm_iterations || !mb.valid[m]) return;
     if (!mdf_active(ch, mode, resid_gate, chan)) return;
     const double* base = (mode == MDF_PLAIN && ch.learned && sweep == 1) ? acc0 : acc;
-    const double2 u = interp_u_acc<S, R>(ch, mb, m, f, tile_slot, base);
-    const double rho_local = rho_nearest<S, R>(ch, f, mb.pos[m]);
+    const double2 u = interp_u_mom<R>(ch, mb, m, tile_slot, mom, base);
+    const double rho_local = rho_nearest_mom<R>(ch, tile_slot, mom, mb.pos[m]);
     const double2 v = mb.vel[m];
     const double dux = v.x - u.x, duy = v.y - u.y;
     const double2 d = make_double2(dux * (2.0 * rho_local), duy * (2.0 * rho_local));
@@ -719,6 +755,67 @@ __global__ void k_mdf_interp(const ChannelDev* __restrict__ chans, int M, Marker
         atomic_max_resid(&resid_plain[chan], sqrt(dux * dux + duy * duy));
 }
 
+// Whether any channel needs the plain correction sweeps this step: a forcing
+// channel that is not learned, or a learned one whose gate residual is above
+// its threshold.  One CTA; runs after the learned sweep's interpolation.
+__global__ void k_plain_needed(const ChannelDev* __restrict__ chans, int nch,
+                               const unsigned* __restrict__ resid_gate, int* __restrict__ flag) {
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    int mine = 0;
+    for (int c = threadIdx.x; c < nch; c += blockDim.x) {
+        const ChannelDev& ch = chans[c];
+        if (ch.cap_end > ch.cap_begin && ch.ibm_iterations > 1 &&
+            (!ch.learned || mdf_fallback(resid_gate[c], ch.mdf_threshold)))
+            mine = 1;
+    }
+    if (mine) any = 1;
+    __syncthreads();
+    if (threadIdx.x == 0) *flag = any;
+}
+
+void launch_plain_needed(const ChannelDev* chans, int nch, TileBufs& tb, cudaStream_t st) {
+    k_plain_needed<<<1, 256, 0, st>>>(chans, nch, tb.resid_gate, tb.plain_needed);
+}
+
+// (rho, jx, jy) of every cell of the step's force tiles, one warp per tile
+// (rows of 32 cells: coalesced population loads).
+template <typename S, typename R>
+__global__ void k_tile_moments(const ChannelDev* __restrict__ chans,
+                               const int* __restrict__ tile_chan, const int* __restrict__ n_slots_p,
+                               const int* __restrict__ slot_tile, const S* __restrict__ f,
+                               typename Mom4<R>::T* __restrict__ mom) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int n_slots = *n_slots_p;
+    for (int slot = warp; slot < n_slots; slot += nwarps) {
+        const int t = slot_tile[slot];
+        const ChannelDev& ch = chans[tile_chan[t]];
+        const int local = t - ch.tile_base;
+        const int x0 = (local % ch.tiles_x) * TILE_W, y0 = (local / ch.tiles_x) * TILE_H;
+        const int jx = x0 + lane;
+#pragma unroll
+        for (int r = 0; r < TILE_H; ++r) {
+            const int jy = y0 + r;
+            typename Mom4<R>::T q;
+            q.x = 0; q.y = 0; q.z = 0; q.w = 0;
+            if (jx < ch.nx && jy < ch.ny) {
+                double rho, jxm, jym;
+                bool solid;
+                cell_rho_j<S, R>(ch, f, jx, jy, rho, jxm, jym, solid);
+                if (!solid) {
+                    q.x = (R)rho;
+                    q.y = (R)jxm;
+                    q.z = (R)jym;
+                }
+            }
+            mom[(size_t)slot * TILE_CELLS + r * TILE_W + lane] = q;
+        }
+    }
+}
+
 // Interpolate the new velocity and move the markers (simulation.cpp:656-675,
 // capsule.cpp:267-297).
 template <typename S, typename R>
@@ -729,33 +826,9 @@ __global__ void k_interp_move(const ChannelDev* __restrict__ chans, int M, Marke
     if (m >= M) return;
     const ChannelDev& ch = chans[mb.mk_chan[m]];
     double2 p = mb.pos[m];
-    double ux = 0.0, uy = 0.0;
-    if (mb.valid[m]) {
-        const int ix0 = mb.ix0[m], iy0 = mb.iy0[m];
-        for (int iy = iy0 - 1; iy <= iy0 + 2; ++iy) {
-            for (int ix = ix0 - 1; ix <= ix0 + 2; ++ix) {
-                int jx = ix;
-                if (jx < 0) jx += ch.nx;
-                if (jx >= ch.nx) jx -= ch.nx;
-                const int jy = iy;
-                if (jy < 0 || jy >= ch.ny || jx < 0 || jx >= ch.nx) continue;
-                const double w = mb.wx[4 * m + (ix - ix0 + 1)] * mb.wy[4 * m + (iy - iy0 + 1)];
-                if (w > 1e-15) {
-                    double rho, jxm, jym;
-                    bool solid;
-                    cell_rho_j<S, R>(ch, f, jx, jy, rho, jxm, jym, solid);
-                    double cu = 0.0, cv = 0.0;
-                    if (!solid && rho > 1e-15) {
-                        const size_t ci = tile_cell_index(ch, tile_slot, jx, jy);
-                        cu = (jxm + 0.5 * (double)fin[ci]) / rho;
-                        cv = (jym + 0.5 * (double)fin[ci + TILE_CELLS]) / rho;
-                    }
-                    ux += cu * w;
-                    uy += cv * w;
-                }
-            }
-        }
-    }
+    double2 u = make_double2(0.0, 0.0);
+    if (mb.valid[m]) u = interp_u_acc<S, R, R>(ch, mb, m, f, tile_slot, fin);
+    const double ux = u.x, uy = u.y;
     mb.vel[m] = make_double2(ux, uy);
     // the step's correction before its last sweep (the network's label, or
     // on a learned step its seed) becomes the next step's network input
@@ -788,6 +861,16 @@ __global__ void k_interp_move(const ChannelDev* __restrict__ chans, int M, Marke
 
 size_t membrane_smem_bytes(int maxn) {
     return (size_t)MEM_WARPS * MEM_DOUBLES_PER_NODE * maxn * sizeof(double);
+}
+
+cudaError_t prepare_spread() {
+    cudaError_t e = cudaFuncSetAttribute(k_spread<double>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)SPREAD_SMEM);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_spread<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)SPREAD_SMEM);
+    return e;
 }
 
 cudaError_t prepare_membrane(int maxn) {
@@ -841,10 +924,10 @@ void launch_tiles(const ChannelDev* chans, const CapsuleDev* caps, int M, const 
 template <typename R>
 void launch_spread(const ChannelDev* chans, const MarkerBufs& mb, TileBufs& tb, int parity,
                    int sweep, int mode, int grid, unsigned* status, cudaStream_t st) {
-    k_spread<R><<<grid, SPREAD_WARPS * 32, 0, st>>>(
+    k_spread<R><<<grid, SPREAD_WARPS * 32, SPREAD_SMEM, st>>>(
         chans, tb.tile_chan, tb.n_slots, tb.slot_tile, tb.tile_cnt, tb.list_off, tb.list, mb,
         tb.acc, tb.acc0, static_cast<R*>(tb.gsnap), static_cast<R*>(tb.fin[parity]), sweep, mode,
-        tb.resid_gate, tb.capped, tb.fluid_touched, status);
+        tb.resid_gate, tb.plain_needed, tb.capped, tb.fluid_touched, status);
 }
 template void launch_spread<double>(const ChannelDev*, const MarkerBufs&, TileBufs&, int, int,
                                     int, int, unsigned*, cudaStream_t);
@@ -854,9 +937,19 @@ template void launch_spread<float>(const ChannelDev*, const MarkerBufs&, TileBuf
 template <typename S, typename R>
 void launch_mdf_interp(const ChannelDev* chans, int M, const MarkerBufs& mb, const S* f,
                        TileBufs& tb, int parity, int sweep, int mode, cudaStream_t st) {
+    (void)f;
     const int B = 128, G = (M + B - 1) / B;
-    k_mdf_interp<S, R><<<G, B, 0, st>>>(chans, M, mb, f, tb.tile_slot[parity], tb.acc, tb.acc0,
-                                        sweep, mode, tb.resid_gate, tb.resid_plain);
+    k_mdf_interp<S, R><<<G, B, 0, st>>>(chans, M, mb, tb.tile_slot[parity],
+                                        static_cast<const typename Mom4<R>::T*>(tb.mom), tb.acc,
+                                        tb.acc0, sweep, mode, tb.resid_gate, tb.resid_plain,
+                                        tb.plain_needed);
+}
+
+template <typename S, typename R>
+void launch_tile_moments(const ChannelDev* chans, const S* f, TileBufs& tb, int grid,
+                         cudaStream_t st) {
+    k_tile_moments<S, R><<<grid, 256, 0, st>>>(chans, tb.tile_chan, tb.n_slots, tb.slot_tile, f,
+                                               static_cast<typename Mom4<R>::T*>(tb.mom));
 }
 
 template <typename S, typename R>
@@ -870,6 +963,8 @@ void launch_interp_move(const ChannelDev* chans, int M, const MarkerBufs& mb, co
 #define SFG_INST(S, R)                                                                          \
     template void launch_mdf_interp<S, R>(const ChannelDev*, int, const MarkerBufs&, const S*,  \
                                           TileBufs&, int, int, int, cudaStream_t);              \
+    template void launch_tile_moments<S, R>(const ChannelDev*, const S*, TileBufs&, int,       \
+                                            cudaStream_t);                                      \
     template void launch_interp_move<S, R>(const ChannelDev*, int, const MarkerBufs&, const S*, \
                                            TileBufs&, int, const double*, cudaStream_t);
 SFG_INST(double, double)

@@ -35,6 +35,9 @@ struct TileBufs {
     int* capped = nullptr;      // [nchan]
     int* fluid_touched = nullptr;
     double* acc0 = nullptr;     // [max_slots][2][TILE_CELLS] force after the membrane spread
+    void* mom = nullptr;        // [max_slots][TILE_CELLS] (rho, jx, jy, 0) of R (step's moments)
+    int* plain_needed = nullptr;  // [1] set when some channel needs the plain sweeps; null
+                                  // (always run them) unless a channel is learned
     unsigned* resid_gate = nullptr;   // [nchan] learned form's no-slip residual (float bits)
     unsigned* resid_plain = nullptr;  // [nchan] plain iteration's last-sweep residual
 };
@@ -47,6 +50,8 @@ size_t scan_tmp_ints(int n);
 // Capsules of up to maxn nodes; > 48 KB of shared memory needs opting in.
 size_t membrane_smem_bytes(int maxn);
 cudaError_t prepare_membrane(int maxn);
+// Opts the spread kernels into their shared-memory size (once per device).
+cudaError_t prepare_spread();
 void launch_membrane(const CapsuleDev* caps, int ncaps, const MarkerBufs& mb, int* has_prev,
                      int maxn, unsigned* status, cudaStream_t st);
 void launch_contact(const ChannelDev* chans, int M, const MarkerBufs& mb, ContactBufs& cb,
@@ -62,18 +67,26 @@ void launch_spread(const ChannelDev* chans, const MarkerBufs& mb, TileBufs& tb, 
 template <typename S, typename R>
 void launch_mdf_interp(const ChannelDev* chans, int M, const MarkerBufs& mb, const S* f,
                        TileBufs& tb, int parity, int sweep, int mode, cudaStream_t st);
-// Learned forcing: interpolation after the membrane spread, network inputs,
-// tensor-core inference, rotation back to the lattice frame -> dF, dFsum, u0
-// of every marker of a learned channel.  `model` is a mlp::ModelDev.
+// Learned forcing: interpolation after the membrane spread and network
+// inputs (feat [M][8], frame [M]), then tensor-core inference and rotation
+// back to the lattice frame -> dF, dFsum, u0 of every marker of a learned
+// channel.  `model` is a mlp::ModelDev.
 template <typename S, typename R>
 void launch_mdf_learned(const ChannelDev* chans, const CapsuleDev* caps, int M,
                         const MarkerBufs& mb, const S* f, TileBufs& tb, int parity,
-                        const void* model, int grid, unsigned* status, cudaStream_t st);
+                        const void* model, float* feat, double2* frame, int grid,
+                        unsigned* status, cudaStream_t st);
 // Training data of the step: inputs [M x 8], labels [M x 2] (the step's total
 // correction in the local frame), valid [M].
 void launch_harvest(const ChannelDev* chans, const CapsuleDev* caps, int M, const MarkerBufs& mb,
                     float* feat, float* label, int* valid, cudaStream_t st);
 cudaError_t prepare_mdf_learned();
+// Sets tb.plain_needed from the gate residuals (learned contexts).
+void launch_plain_needed(const ChannelDev* chans, int nch, TileBufs& tb, cudaStream_t st);
+// Moments of the step's force tiles (before the first forcing sweep).
+template <typename S, typename R>
+void launch_tile_moments(const ChannelDev* chans, const S* f, TileBufs& tb, int grid,
+                         cudaStream_t st);
 template <typename S, typename R>
 void launch_interp_move(const ChannelDev* chans, int M, const MarkerBufs& mb, const S* f,
                         TileBufs& tb, int parity, const double* phi_tbl, cudaStream_t st);

@@ -100,7 +100,7 @@ __global__ void k_sa_fill(int nx, int ny, int tiles_x, int M, SpreadScratch sc) 
 }
 
 constexpr int SA_WARPS = 8;
-constexpr int SA_LCAP = 384;
+constexpr int SA_LCAP = 256;  // a power of two: the bitonic sort pads to one
 
 __global__ void __launch_bounds__(SA_WARPS * 32)
 k_sa_gather(int nx, int ny, int tiles_x, int T, const double2* __restrict__ pos,
