@@ -18,6 +18,19 @@ __device__ __forceinline__ void cell_moments(const R f[9], R& rho, R& jx, R& jy)
     jy = f[2] - f[4] + f[5] + f[6] - f[7] - f[8];
 }
 
+// Moments in the lattice kernels' representation: populations (FP64) or
+// deviations d = f - w (FP32 arithmetic: rho = 1 + sum d, j = sum e d).
+template <typename R>
+__device__ __forceinline__ void lattice_moments(const R c[9], R& rho, R& jx, R& jy) {
+    cell_moments(c, rho, jx, jy);
+}
+template <>
+__device__ __forceinline__ void lattice_moments<float>(const float c[9], float& rho, float& jx,
+                                                       float& jy) {
+    cell_moments(c, rho, jx, jy);
+    rho += 1.f;
+}
+
 // u = (j + F/2) / rho, zero for rho <= 1e-15 (lattice_field.cpp:229-237).
 template <typename R>
 __device__ __forceinline__ void cell_velocity(R rho, R jx, R jy, R Gx, R Gy, R& ux, R& uy) {
@@ -157,11 +170,18 @@ __device__ __forceinline__ void collide_mrt(R f[9], R r, R vx, R vy, R fx, R fy,
 // (1/cs^2 = 3, 1/(2 cs^4) = 4.5, reciprocals of the inverse-transform
 // denominators) instead of the reference's evaluation order.
 // ---------------------------------------------------------------------------
+// FP32-arithmetic forms work on the deviations d = f - w (the lattice
+// kernels' representation for FP32 and FP16 storage): the collision reads d
+// and writes d, so no value near a weight is ever formed or rounded.
+
+// MRT on deviations: M w = (1, -2, 1, 0, ..., 0), so the conserved moment is
+// rho - 1 and the two energy equilibria shift by the rest state:
+// e_eq + 2 = -2 (rho - 1) + 3 rho u^2, eps_eq - 1 = (rho - 1) - 3 rho u^2.
 template <>
 __device__ __forceinline__ void collide_mrt<float>(float f[9], float r, float vx, float vy,
                                                    float fx, float fy, float sn, float s1,
                                                    float s2, float s4) {
-    const float m0 = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
+    const float m0 = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];  // rho - 1
     const float a = f[1] + f[2] + f[3] + f[4];
     const float d = f[5] + f[6] + f[7] + f[8];
     float m1 = -4.f * f[0] - a + 2.f * d;
@@ -174,8 +194,9 @@ __device__ __forceinline__ void collide_mrt<float>(float f[9], float r, float vx
     float m8 = f[5] - f[6] + f[7] - f[8];
     const float uu = vx * vx + vy * vy;
     const float uF = vx * fx + vy * fy;
-    m1 = m1 - s1 * (m1 - (-2.f * r + 3.f * r * uu)) + (1.f - 0.5f * s1) * (6.f * uF);
-    m2 = m2 - s2 * (m2 - (r - 3.f * r * uu)) - (1.f - 0.5f * s2) * (6.f * uF);
+    const float ru3 = 3.f * r * uu;
+    m1 = m1 - s1 * (m1 - (-2.f * m0 + ru3)) + (1.f - 0.5f * s1) * (6.f * uF);
+    m2 = m2 - s2 * (m2 - (m0 - ru3)) - (1.f - 0.5f * s2) * (6.f * uF);
     m4 = m4 - s4 * (m4 + r * vx) - (1.f - 0.5f * s4) * fx;
     m6 = m6 - s4 * (m6 + r * vy) - (1.f - 0.5f * s4) * fy;
     m7 = m7 - sn * (m7 - r * (vx * vx - vy * vy)) + (1.f - 0.5f * sn) * (2.f * (vx * fx - vy * fy));
@@ -197,40 +218,73 @@ __device__ __forceinline__ void collide_mrt<float>(float f[9], float r, float vx
     f[8] = bD + px - py - 0.25f * m8;
 }
 
+// Regularized BGK on deviations, by opposite direction pairs.  The
+// non-equilibrium first moment and stress come from the moments minus their
+// values for the
+// second-order equilibrium (sum e feq = rho u, sum e e feq = rho/3 I +
+// rho u u), and every pair (e, -e) shares the even part of the update
+// (equilibrium, stress projection, second-order Guo term) while the odd part
+// (3 e.u, 3 e.j_neq, 3 e.F) changes sign.
 template <>
 __device__ __forceinline__ void collide_regularized<float>(float f[9], float rho, float ux,
                                                            float uy, float Fx, float Fy,
                                                            float omega) {
-    const float uu15 = 1.5f * (ux * ux + uy * uy);
-    float fe[9];
-    float jx = 0.f, jy = 0.f, pxx = 0.f, pxy = 0.f, pyy = 0.f;
-#pragma unroll
-    for (int q = 0; q < 9; ++q) {
-        const float cx = float(cx_of(q)), cy = float(cy_of(q));
-        const float eu = cx * ux + cy * uy;
-        fe[q] = float(w_of(q)) * rho * (1.f + 3.f * eu + 4.5f * eu * eu - uu15);
-        const float fneq = f[q] - fe[q];
-        if (cx_of(q) != 0) { jx += cx * fneq; pxx += fneq; }
-        if (cy_of(q) != 0) { jy += cy * fneq; pyy += fneq; }
-        if (cx_of(q) * cy_of(q) != 0) pxy += cx * cy * fneq;
-    }
+    // f holds deviations d = f - w: sum_{cx!=0} w = 1/3 and the odd weight
+    // moments vanish
+    const float* d = f;
+    const float drho = d[0] + d[1] + d[2] + d[3] + d[4] + d[5] + d[6] + d[7] + d[8];
+    const float jx = d[1] - d[3] + d[5] - d[6] - d[7] + d[8];
+    const float jy = d[2] - d[4] + d[5] + d[6] - d[7] - d[8];
+    const float sxx = d[1] + d[3] + d[5] + d[6] + d[7] + d[8];
+    const float syy = d[2] + d[4] + d[5] + d[6] + d[7] + d[8];
+    const float sxy = d[5] - d[6] + d[7] - d[8];
+    const float rux = rho * ux, ruy = rho * uy;
+    const float jnx = jx - rux, jny = jy - ruy;
+    const float dr3 = drho * (1.f / 3.f);
+    const float pxx = sxx - dr3 - rux * ux;
+    const float pyy = syy - dr3 - ruy * uy;
+    const float pxy = sxy - rux * uy;
     const float om1 = 1.f - omega, guo = 1.f - 0.5f * omega;
-    // Q:Pi/(2 cs^4) with Q = e e - cs^2 I
-    const float trP = (pxx + pyy) * (1.f / 3.f);
-#pragma unroll
-    for (int q = 0; q < 9; ++q) {
-        const int icx = cx_of(q), icy = cy_of(q);
-        const float cx = float(icx), cy = float(icy), w = float(w_of(q));
-        float qp = -trP;
-        if (icx) qp += pxx;
-        if (icy) qp += pyy;
-        if (icx * icy) qp += 2.f * cx * cy * pxy;
-        const float fneq_reg = w * (3.f * (cx * jx + cy * jy) + 4.5f * qp);
-        const float eu = cx * ux + cy * uy;
-        const float Fi = guo * w * ((3.f * (cx - ux) + 9.f * eu * cx) * Fx +
-                                    (3.f * (cy - uy) + 9.f * eu * cy) * Fy);
-        f[q] = fe[q] + om1 * fneq_reg + Fi;
-    }
+    const float bm = -1.5f * (ux * ux + uy * uy);
+    const float uF3 = 3.f * (ux * Fx + uy * Fy);
+    const float trP3 = (pxx + pyy) * (1.f / 3.f);
+    const float ane = 4.5f * om1, aj = 3.f * om1, g3 = 3.f * guo, g9 = 9.f * guo;
+    f[0] = (4.f / 9.f) * (drho + rho * bm - ane * trP3 - guo * uF3);
+    auto pair = [&](int q, int o, float eu, float eF, float ej, float QP, float w) {
+        const float E = w * (drho + rho * (bm + 4.5f * eu * eu) + ane * QP + g9 * eu * eF -
+                             guo * uF3);
+        const float O = w * (3.f * rho * eu + aj * ej + g3 * eF);
+        f[q] = E + O;
+        f[o] = E - O;
+    };
+    pair(1, 3, ux, Fx, jnx, pxx - trP3, 1.f / 9.f);
+    pair(2, 4, uy, Fy, jny, pyy - trP3, 1.f / 9.f);
+    pair(5, 7, ux + uy, Fx + Fy, jnx + jny, pxx + pyy + 2.f * pxy - trP3, 1.f / 36.f);
+    pair(6, 8, uy - ux, Fy - Fx, jny - jnx, pxx + pyy - 2.f * pxy - trP3, 1.f / 36.f);
+}
+
+// BGK on deviations, by opposite direction pairs:
+// d' = (1 - omega) d + omega (feq - w) + F with
+// feq - w = w ((rho - 1) + rho (-1.5 u^2 + 4.5 (e.u)^2) + 3 rho e.u).
+template <>
+__device__ __forceinline__ void collide_bgk<float>(float f[9], float r, float vx, float vy,
+                                                   float fx, float fy, float om) {
+    const float drho = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
+    const float om1 = 1.f - om, guo = 1.f - 0.5f * om;
+    const float bm = -1.5f * (vx * vx + vy * vy);
+    const float uF3 = 3.f * (vx * fx + vy * fy);
+    const float g3 = 3.f * guo, g9 = 9.f * guo, orr = om * r;
+    f[0] = om1 * f[0] + (4.f / 9.f) * (om * drho + orr * bm - guo * uF3);
+    auto pair = [&](int q, int o, float eu, float eF, float w) {
+        const float E = w * (om * drho + orr * (bm + 4.5f * eu * eu) + g9 * eu * eF - guo * uF3);
+        const float O = w * (3.f * orr * eu + g3 * eF);
+        f[q] = om1 * f[q] + (E + O);
+        f[o] = om1 * f[o] + (E - O);
+    };
+    pair(1, 3, vx, fx, 1.f / 9.f);
+    pair(2, 4, vy, fy, 1.f / 9.f);
+    pair(5, 7, vx + vy, fx + fy, 1.f / 36.f);
+    pair(6, 8, vy - vx, fy - fx, 1.f / 36.f);
 }
 
 // Passive-scalar BGK collision with the first-order equilibrium

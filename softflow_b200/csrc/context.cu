@@ -650,7 +650,7 @@ extern "C" int sfg_initialize(sfg_context* c) {
 
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-    c->spread_grid = std::max(1, std::min((tb.max_slots + 7) / 8, nsm * 4));
+    c->spread_grid = std::max(1, std::min((tb.max_slots + 7) / 8, nsm * spread_blocks_per_sm()));
     c->persistent_ctas = nsm * lattice_ctas_per_sm(c->precision, c->any_adr);
     c->learned_grid = nsm * 4;
     CU(cudaStreamSynchronize(c->stream));

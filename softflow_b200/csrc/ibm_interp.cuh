@@ -19,9 +19,9 @@ __device__ __forceinline__ void cell_rho_j(const ChannelDev& ch, const S* __rest
     const long long n = (long long)jy * ch.pitch + jx;
     R v[9];
 #pragma unroll
-    for (int q = 0; q < 9; ++q) v[q] = PopIO<S, R>::load(f + ch.f_off + q * ch.plane + n, q);
+    for (int q = 0; q < 9; ++q) v[q] = PopIO<S, R>::ld(f + ch.f_off + q * ch.plane + n, q);
     R r, a, b;
-    cell_moments(v, r, a, b);
+    lattice_moments(v, r, a, b);
     rho = (double)r;
     jxo = (double)a;
     jyo = (double)b;

@@ -45,17 +45,29 @@ __device__ __forceinline__ __half f2h_stochastic(float v, uint32_t r) {
 
 template <typename S, typename R>
 struct PopIO;
+// load / store: populations f (fill, import, export).  ld / st_sr: the
+// lattice kernels' working representation -- f for FP64, the deviation
+// d = f - w for FP32 arithmetic (FP32 and FP16 storage both keep d).
 template <>
 struct PopIO<double, double> {
+    static __device__ __forceinline__ double ld(const double* p, int) { return __ldg(p); }
+    static __device__ __forceinline__ void st_sr(double* p, int, double v, uint32_t) { *p = v; }
     static __device__ __forceinline__ double load(const double* p, int) { return __ldg(p); }
     static __device__ __forceinline__ void store(double* p, int, double v) { *p = v; }
-    static __device__ __forceinline__ void store_sr(double* p, int, double v, uint32_t) { *p = v; }
 };
+// FP32 storage keeps the deviation f - w (the populations stay close to
+// their weights, so the stored deviation carries far more significant bits
+// than f itself).
 template <>
 struct PopIO<float, float> {
-    static __device__ __forceinline__ float load(const float* p, int) { return __ldg(p); }
-    static __device__ __forceinline__ void store(float* p, int, float v) { *p = v; }
-    static __device__ __forceinline__ void store_sr(float* p, int, float v, uint32_t) { *p = v; }
+    static __device__ __forceinline__ float load(const float* p, int q) {
+        return float(w_of(q)) + __ldg(p);
+    }
+    static __device__ __forceinline__ void store(float* p, int q, float v) {
+        *p = v - float(w_of(q));
+    }
+    static __device__ __forceinline__ float ld(const float* p, int) { return __ldg(p); }
+    static __device__ __forceinline__ void st_sr(float* p, int, float v, uint32_t) { *p = v; }
 };
 template <>
 struct PopIO<__half, float> {
@@ -65,10 +77,13 @@ struct PopIO<__half, float> {
     static __device__ __forceinline__ void store(__half* p, int q, float v) {
         *p = __float2half_rn((v - float(w_of(q))) * FP16S_SCALE);
     }
+    static __device__ __forceinline__ float ld(const __half* p, int) {
+        return __half2float(__ldg(p)) * FP16S_UNSCALE;
+    }
     // r: per-cell seed; each direction draws its own 13 dither bits
-    static __device__ __forceinline__ void store_sr(__half* p, int q, float v, uint32_t r) {
+    static __device__ __forceinline__ void st_sr(__half* p, int q, float v, uint32_t r) {
         const uint32_t d = (r + (uint32_t)q * 0x9E3779B9u) * 1664525u + 1013904223u;
-        *p = f2h_stochastic((v - float(w_of(q))) * FP16S_SCALE, d >> 19);
+        *p = f2h_stochastic(v * FP16S_SCALE, d >> 19);
     }
 };
 
@@ -180,7 +195,7 @@ __device__ __forceinline__ Nbr neighbours(int x, int y, int nx, int ny, int mode
 
 // Push the nine post-collision values of cell (x, y): to the downstream
 // neighbour, or reflected into the own cell when that neighbour is a wall.
-template <typename S, typename R>
+template <typename S, typename R, bool POP = true>
 __device__ __forceinline__ void push_cell(S* __restrict__ fd, const R f[9], int x, int y, int n,
                                           int pitch, int plane, const Nbr& b, uint32_t seed) {
 #pragma unroll
@@ -189,10 +204,10 @@ __device__ __forceinline__ void push_cell(S* __restrict__ fd, const R f[9], int 
         const bool wall = (cy > 0 && b.wall_p) || (cy < 0 && b.wall_m);
         const int xd = cx == 0 ? x : (cx > 0 ? b.xp : b.xm);
         const int yd = cy == 0 ? y : (cy > 0 ? b.yp : b.ym);
-        if (!wall)
-            PopIO<S, R>::store_sr(fd + q * plane + yd * pitch + xd, q, f[q], seed);
-        else
-            PopIO<S, R>::store_sr(fd + opp_of(q) * plane + n, opp_of(q), f[q], seed);
+        S* p = wall ? fd + opp_of(q) * plane + n : fd + q * plane + yd * pitch + xd;
+        const int qs = wall ? opp_of(q) : q;
+        if (POP) PopIO<S, R>::st_sr(p, qs, f[q], seed);
+        else *p = (S)f[q];
     }
 }
 
@@ -215,9 +230,9 @@ k_lattice_step(const RowItem* __restrict__ items, int n_items, const ChannelDev*
     const S* __restrict__ fs = src + ch.f_off + n;
     R f[9];
 #pragma unroll
-    for (int q = 0; q < 9; ++q) f[q] = PopIO<S, R>::load(fs + q * plane, q);
+    for (int q = 0; q < 9; ++q) f[q] = PopIO<S, R>::ld(fs + q * plane, q);
     R rho, jx, jy;
-    cell_moments(f, rho, jx, jy);
+    lattice_moments(f, rho, jx, jy);
     const int st = stepped[it.chan];
     const CellForces<R> cf = cell_forces<R>(ch, x, y, tv, st);
     R ux, uy;
@@ -251,7 +266,7 @@ k_lattice_step(const RowItem* __restrict__ items, int n_items, const ChannelDev*
             collide_scalar(g, C, vx, vy, R(ch.omega_s));
             const int gmode = ch.periodic_y ? (ch.adr_periodic_y ? 1 : 2) : 0;
             const Nbr gb = gmode == (ch.periodic_y ? 1 : 0) ? b : neighbours(x, y, nx, ny, gmode);
-            push_cell<R, R>(gdst + ch.g_off, g, x, y, n, pitch, plane, gb, 0u);
+            push_cell<R, R, false>(gdst + ch.g_off, g, x, y, n, pitch, plane, gb, 0u);
         }
     }
 }
@@ -327,15 +342,40 @@ template <typename S, typename R>
 struct Enc {
     static __device__ __forceinline__ R dec(S s, int) { return (R)s; }
     static __device__ __forceinline__ S enc(R v, int, uint32_t) { return (S)v; }
+    static __device__ __forceinline__ void enc4(const R v[4], int, uint32_t, S e[4]) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) e[i] = (S)v[i];
+    }
 };
+
 template <>
-struct Enc<__half, float> {
-    static __device__ __forceinline__ float dec(__half s, int q) {
-        return float(w_of(q)) + __half2float(s) * FP16S_UNSCALE;
+struct Enc<__half, float> {   // working representation: deviations d = f - w
+    static __device__ __forceinline__ float dec(__half s, int) {
+        return __half2float(s) * FP16S_UNSCALE;
     }
     static __device__ __forceinline__ __half enc(float v, int q, uint32_t r) {
         const uint32_t d = (r + (uint32_t)q * 0x9E3779B9u) * 1664525u + 1013904223u;
-        return f2h_stochastic((v - float(w_of(q))) * FP16S_SCALE, d >> 19);
+        return f2h_stochastic(v * FP16S_SCALE, d >> 19);
+    }
+    // Four consecutive cells of direction q with the hardware's stochastic
+    // rounding (cvt.rs.f16x2.f32: the first operand goes to the high half and
+    // takes random bits 16-28, the second the low half and bits 0-12).
+    static __device__ __forceinline__ void enc4(const float v[4], int q, uint32_t r,
+                                                __half e[4]) {
+        uint32_t p[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            uint32_t h = r + (uint32_t)q * 0x9E3779B9u + (uint32_t)k * 0x7F4A7C15u;
+            h ^= h >> 15;
+            h *= 0x2C1B3C6Du;
+            h ^= h >> 12;
+            const float lo = v[2 * k] * FP16S_SCALE, hi = v[2 * k + 1] * FP16S_SCALE;
+            asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(p[k]) : "f"(hi), "f"(lo), "r"(h));
+        }
+        e[0] = __ushort_as_half((unsigned short)(p[0] & 0xFFFFu));
+        e[1] = __ushort_as_half((unsigned short)(p[0] >> 16));
+        e[2] = __ushort_as_half((unsigned short)(p[1] & 0xFFFFu));
+        e[3] = __ushort_as_half((unsigned short)(p[1] >> 16));
     }
 };
 
@@ -397,7 +437,9 @@ __device__ __forceinline__ void store_plane4(S* __restrict__ row, const S v[4], 
     }
 }
 
-template <typename S, typename R>
+// POP: f are lattice populations (stored through the population codec);
+// otherwise raw values (the scalar's distributions).
+template <typename S, typename R, bool POP = true>
 __device__ __forceinline__ void push_vec4(S* __restrict__ fd, R f[9][4], int x, int x0, int len,
                                           int nx, int y, int ym, int yp, bool wall_m, bool wall_p,
                                           int pitch, int plane, bool active, int lane,
@@ -408,8 +450,12 @@ __device__ __forceinline__ void push_vec4(S* __restrict__ fd, R f[9][4], int x, 
         const bool wall = (cy > 0 && wall_p) || (cy < 0 && wall_m);
         const int qq = wall ? opp_of(q) : q;
         S e[4];
+        if (POP) {
+            Enc<S, R>::enc4(f[q], qq, seed, e);
+        } else {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) e[i] = Enc<S, R>::enc(f[q][i], qq, seed + 0x632BE5ABu * i);
+            for (int i = 0; i < 4; ++i) e[i] = (S)f[q][i];
+        }
         if (wall) {
             store_plane4<S>(fd + qq * plane + y * pitch, e, 0, x, x0, len, nx, active, lane,
                             last_lane);
@@ -543,7 +589,7 @@ __device__ __forceinline__ void lattice_run4(const RowItem& it, const ChannelDev
 #pragma unroll
         for (int q = 0; q < 9; ++q) c[q] = f[q][i];
         R r, a, bj;
-        cell_moments(c, r, a, bj);
+        lattice_moments(c, r, a, bj);
         if (active) {
             const CellForces<R> cf = run_forces<R>(ch, rt, i, tv, st);
             R ux, uy;
@@ -592,7 +638,7 @@ __device__ __forceinline__ void lattice_run4(const RowItem& it, const ChannelDev
             }
             const int gmode = ch.periodic_y ? (ch.adr_periodic_y ? 1 : 2) : 0;
             const Nbr gb = neighbours(0, y, nx, ny, gmode);
-            push_vec4<R, R>(gdst + ch.g_off, g, x, x0, it.len, nx, y, gb.ym, gb.yp, gb.wall_m,
+            push_vec4<R, R, false>(gdst + ch.g_off, g, x, x0, it.len, nx, y, gb.ym, gb.yp, gb.wall_m,
                             gb.wall_p, pitch, plane, active, lane, last_lane, 0u);
         }
     }
@@ -658,9 +704,9 @@ k_scalar_flush(const RowItem* __restrict__ items, int n_items, const ChannelDev*
     const S* fs = src + ch.f_off + n;
     R f[9];
 #pragma unroll
-    for (int q = 0; q < 9; ++q) f[q] = PopIO<S, R>::load(fs + q * plane, q);
+    for (int q = 0; q < 9; ++q) f[q] = PopIO<S, R>::ld(fs + q * plane, q);
     R rho, jx, jy;
-    cell_moments(f, rho, jx, jy);
+    lattice_moments(f, rho, jx, jy);
     // the force of the last completed step (its "cur" tile set)
     const CellForces<R> cf = cell_forces<R>(ch, x, y, tv_last, 1);
     R g[9];
@@ -674,7 +720,7 @@ k_scalar_flush(const RowItem* __restrict__ items, int n_items, const ChannelDev*
     cell_velocity(rho, jx, jy, cf.Fx, cf.Fy, vx, vy);
     collide_scalar(g, C, vx, vy, R(ch.omega_s));
     const int gmode = ch.periodic_y ? (ch.adr_periodic_y ? 1 : 2) : 0;
-    push_cell<R, R>(gdst + ch.g_off, g, x, y, n, pitch, plane, neighbours(x, y, nx, ny, gmode),
+    push_cell<R, R, false>(gdst + ch.g_off, g, x, y, n, pitch, plane, neighbours(x, y, nx, ny, gmode),
                     0u);
 }
 
@@ -763,9 +809,9 @@ __global__ void k_macro_export(const S* __restrict__ in, ChannelDev ch, TileView
         R f[9];
         const long long n = (long long)y * ch.pitch + x;
 #pragma unroll
-        for (int q = 0; q < 9; ++q) f[q] = PopIO<S, R>::load(in + ch.f_off + q * ch.plane + n, q);
+        for (int q = 0; q < 9; ++q) f[q] = PopIO<S, R>::ld(in + ch.f_off + q * ch.plane + n, q);
         R rho, jx, jy, ux, uy;
-        cell_moments(f, rho, jx, jy);
+        lattice_moments(f, rho, jx, jy);
         cell_velocity(rho, jx, jy, Fx, Fy, ux, uy);
         rho_o[i] = (double)rho;
         ux_o[i] = (double)ux;

@@ -510,12 +510,13 @@ constexpr int SPREAD_LCAP = 256;      // list entries sorted in shared memory pe
 constexpr int SPREAD_LIST_MAX = 4096; // longer lists are clamped and flagged
 
 // Shared memory of one spread warp: the tile's accumulators, its sorted
-// marker list and a staging chunk of 32 markers.
+// marker list and a staging chunk of markers.
+constexpr int SPREAD_CHUNK = 16;      // markers staged at a time per warp
 struct SpreadWarpSmem {
     double ax[TILE_CELLS], ay[TILE_CELLS];
-    double fx[32], fy[32], ds[32];
-    double wx[32][4], wy[32][4];
-    int ix[32], iy[32], ok[32];
+    double fx[SPREAD_CHUNK], fy[SPREAD_CHUNK], ds[SPREAD_CHUNK];
+    double wx[SPREAD_CHUNK][4], wy[SPREAD_CHUNK][4];
+    int ix[SPREAD_CHUNK], iy[SPREAD_CHUNK], ok[SPREAD_CHUNK];
     int list[SPREAD_LCAP];
 };
 constexpr size_t SPREAD_SMEM = sizeof(SpreadWarpSmem) * SPREAD_WARPS;
@@ -547,7 +548,6 @@ k_spread(const ChannelDev* __restrict__ chans, const int* __restrict__ tile_chan
     double* ay = W.ay;
     int* sl = W.list;
     const int n_slots = *n_slots_p;
-    const int sx = lane & 3, sy = (lane >> 2) & 3;
     for (int slot = blockIdx.x * SPREAD_WARPS + warp; slot < n_slots;
          slot += gridDim.x * SPREAD_WARPS) {
         const int t = slot_tile[slot];
@@ -619,12 +619,15 @@ k_spread(const ChannelDev* __restrict__ chans, const int* __restrict__ tile_chan
             }
         }
         __syncwarp();
-        // markers in list order, staged 32 at a time: each lane loads one
-        // marker's force, stencil origin, ds and weights (the loads of a
-        // chunk are in flight together), then the half-warp adds them in
-        // order, one stencil point per lane
-        for (int c0 = 0; c0 < cnt; c0 += 32) {
-            const int nb = cnt - c0 < 32 ? cnt - c0 : 32;
+        // Markers in list order, staged SPREAD_CHUNK at a time (the loads of
+        // a chunk are in flight together).  Lane l owns column x0 + l of the
+        // tile; for each marker it adds to its own cells, so every cell
+        // still receives its terms in list order while lanes never share a
+        // cell (no warp synchronisation between markers).
+        const int xg = x0 + lane;
+        for (int c0 = 0; c0 < cnt; c0 += SPREAD_CHUNK) {
+            const int nb = cnt - c0 < SPREAD_CHUNK ? cnt - c0 : SPREAD_CHUNK;
+            __syncwarp();
             if (lane < nb) {
                 const int m = lst[c0 + lane];
                 const double2 fo = sweep == 0 ? mb.frc[m] : mb.dF[m];
@@ -641,27 +644,35 @@ k_spread(const ChannelDev* __restrict__ chans, const int* __restrict__ tile_chan
                 W.wy[lane][0] = b0.x; W.wy[lane][1] = b0.y; W.wy[lane][2] = b1.x; W.wy[lane][3] = b1.y;
             }
             __syncwarp();
-            for (int j = 0; j < nb; ++j) {
-                if (lane < 16 && W.ok[j]) {
-                    const int iy = W.iy[j] - 1 + sy;
-                    int jx = W.ix[j] - 1 + sx;
-                    if (jx < 0) jx += nx;
-                    if (jx >= nx) jx -= nx;
-                    const int cxl = jx - x0, cyl = iy - y0;
-                    if (iy >= 0 && iy < ny && cxl >= 0 && cxl < TILE_W && cyl >= 0 &&
-                        cyl < TILE_H) {
-                        const double w = W.wx[j][sx] * W.wy[j][sy];
-                        if (w > 1e-15) {
-                            const double ds = W.ds[j];
-                            const int c = cyl * TILE_W + cxl;
-                            ax[c] += W.fx[j] * w * ds;
-                            ay[c] += W.fy[j] * w * ds;
+            if (xg < nx) {
+                for (int j = 0; j < nb; ++j) {
+                    if (!W.ok[j]) continue;
+                    // stencil column sx with wrap(ix0 - 1 + sx) == xg
+                    int d = xg - W.ix[j] + 1;
+                    if (d < 0) d += nx;
+                    if (d < 0) d += nx;
+                    if (d >= nx) d -= nx;
+                    if (d >= 4) continue;
+                    const double wxs = W.wx[j][d];
+                    const double ds = W.ds[j], fx = W.fx[j], fy = W.fy[j];
+                    const int iyb = W.iy[j] - 1;
+#pragma unroll
+                    for (int sy = 0; sy < 4; ++sy) {
+                        const int iy = iyb + sy;
+                        const int cyl = iy - y0;
+                        if (iy >= 0 && iy < ny && cyl >= 0 && cyl < TILE_H) {
+                            const double w = wxs * W.wy[j][sy];
+                            if (w > 1e-15) {
+                                const int c = cyl * TILE_W + lane;
+                                ax[c] += fx * w * ds;
+                                ay[c] += fy * w * ds;
+                            }
                         }
                     }
                 }
-                __syncwarp();
             }
         }
+        __syncwarp();
         if (!last) {
             const bool keep0 = (sweep == 0 && ch.learned);
             for (int c = lane; c < TILE_CELLS; c += 32) {
@@ -861,6 +872,14 @@ __global__ void k_interp_move(const ChannelDev* __restrict__ chans, int M, Marke
 
 size_t membrane_smem_bytes(int maxn) {
     return (size_t)MEM_WARPS * MEM_DOUBLES_PER_NODE * maxn * sizeof(double);
+}
+
+int spread_blocks_per_sm() {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_spread<float>, SPREAD_WARPS * 32,
+                                                      SPREAD_SMEM) != cudaSuccess || b < 1)
+        b = 1;
+    return b;
 }
 
 cudaError_t prepare_spread() {
