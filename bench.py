@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the per-channel plain form")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch shapes (no autotuner trials)")
     ap.add_argument("--mdf", default="auto", choices=["auto", "learned", "plain"],
                     help="forcing form of the timed run (auto: learned on the ensemble)")
     ap.add_argument("--mdf-threshold", type=float, default=1e-4,
@@ -208,7 +210,9 @@ def run_product(args, world, rank, local, pg):
     cells, caps, markers, scal = W.totals(plans, ens)
     nch = len(plans)
 
-    # warm-up (graphs are built on the first call)
+    # launch shapes chosen by the autotuner on real steps, then the warm-up
+    # (graphs are built on the first call); both untimed
+    tuned = ens.autotune(steps_per_trial=5) if not args.no_autotune else ens.launchConfig()
     ctx.step(args.warmup)
     ctx.synchronize()
     stats0 = [ens.mdfStats(c) for c in range(nch)] if learned else None
@@ -303,6 +307,7 @@ def run_product(args, world, rank, local, pg):
                           if learned else "plain",
                    "l2": "state larger than L2 (no flush needed)" if alg_bytes > 126e6
                          else "state fits L2 (L2-resident workload)",
+                   "launch_shapes": tuned,
                    "parallelism": (f"channel shards x{world} (256 distinct channels per rank)"
                                    if args.workload == "c3" else f"replicas x{world}")},
         "mlups": mlups,

@@ -268,6 +268,17 @@ int sfg_get_mdf_stats(sfg_context* ctx, int channel, float* resid_learned, float
 int sfg_set_harvest(sfg_context* ctx, int enabled);
 int sfg_get_harvest(sfg_context* ctx, float* features, float* labels, int* valid);
 
+/* ---- launch shapes ------------------------------------------------------
+ * sfg_autotune times whole steps (CUDA events) for each candidate launch
+ * shape -- CTAs per SM of the persistent lattice kernel, of the spread and of
+ * the learned seed, and the block size of the per-marker kernels -- one
+ * tunable at a time, and keeps the fastest.  The trials are real steps: the
+ * context advances by *steps_run steps (call it in place of warm-up steps).
+ * No reference counterpart (the reference has no launch shapes). */
+int sfg_autotune(sfg_context* ctx, int steps_per_trial, int* steps_run);
+int sfg_get_launch_config(sfg_context* ctx, int* lattice_ctas_per_sm, int* spread_ctas_per_sm,
+                          int* marker_block, int* learned_ctas_per_sm);
+
 /* ---- diagnostics ---------------------------------------------------------- */
 int sfg_num_channels(const sfg_context* ctx, int* n);
 int sfg_channel_counts(const sfg_context* ctx, int channel, int* num_capsules, int* num_markers);

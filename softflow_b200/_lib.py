@@ -123,6 +123,9 @@ SIGNATURES = {
     "sfg_set_mdf_model": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double]),
     "sfg_get_mdf_stats": (C.c_int, [C.c_void_p, C.c_int, _P(C.c_float), _P(C.c_float),
                                     _P(C.c_longlong), _P(C.c_longlong)]),
+    "sfg_autotune": (C.c_int, [C.c_void_p, C.c_int, _P(C.c_int)]),
+    "sfg_get_launch_config": (C.c_int, [C.c_void_p, _P(C.c_int), _P(C.c_int), _P(C.c_int),
+                                        _P(C.c_int)]),
     "sfg_set_harvest": (C.c_int, [C.c_void_p, C.c_int]),
     "sfg_get_harvest": (C.c_int, [C.c_void_p, _P(C.c_float), _P(C.c_float), _P(C.c_int)]),
 }

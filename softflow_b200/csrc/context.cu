@@ -185,6 +185,10 @@ struct sfg_context {
     void* d_model = nullptr;            // mlp::ModelDev (the context's own copy)
     bool any_learned = false;
     int learned_grid = 592;
+    // launch shapes (sfg_autotune): CTAs per SM of the persistent lattice
+    // kernel, the spread and the learned seed; 0 = the largest resident count
+    int nsm = 148;
+    int lattice_cps = 0, spread_cps = 0, learned_cps = 4;
     long long* d_learned_steps = nullptr;  // [nch]
     long long* d_fallbacks = nullptr;      // [nch]
     bool harvest = false;
@@ -267,7 +271,7 @@ static void free_all(sfg_context* c) {
     F(c->tb.tile_chan); F(c->tb.tile_flag); F(c->tb.tile_cnt); F(c->tb.cursor);
     F(c->tb.slot_scan); F(c->tb.list_off); F(c->tb.slot_tile); F(c->tb.n_slots);
     F(c->tb.list); F(c->tb.scan_tmp); F(c->tb.acc); F(c->tb.gsnap); F(c->tb.capped);
-    F(c->tb.fluid_touched); F(c->tb.acc0); F(c->tb.mom); F(c->tb.resid_gate); F(c->tb.resid_plain);
+    F(c->tb.fluid_touched); F(c->tb.acc0); F(c->tb.mom); F(c->tb.slot_info); F(c->tb.spread_ctr); F(c->tb.resid_gate); F(c->tb.resid_plain);
     F(c->mb.u0); F(c->mb.dFsum); F(c->mb.dFprev);
     F(c->d_model); F(c->d_learned_steps); F(c->d_fallbacks);
     F(c->d_hfeat); F(c->d_hlab); F(c->d_hvalid); F(c->d_feat); F(c->d_frame); F(c->d_plain_needed);
@@ -343,6 +347,17 @@ static cudaError_t dalloc(T** p, size_t n) {
 // ------------------------------------------------------------------------
 // initialize
 // ------------------------------------------------------------------------
+// Grid sizes from the tuned CTAs-per-SM counts (0 = the resident maximum).
+static void apply_launch_config(sfg_context* c) {
+    const int lat_max = lattice_ctas_per_sm(c->precision, c->any_adr);
+    const int spr_max = spread_blocks_per_sm();
+    const int lat = c->lattice_cps > 0 ? std::min(c->lattice_cps, lat_max) : lat_max;
+    const int spr = c->spread_cps > 0 ? std::min(c->spread_cps, spr_max) : spr_max;
+    c->persistent_ctas = c->nsm * lat;
+    c->spread_grid = std::max(1, std::min((c->tb.max_slots + 7) / 8, c->nsm * spr));
+    c->learned_grid = c->nsm * std::max(1, std::min(c->learned_cps, 4));
+}
+
 extern "C" int sfg_initialize(sfg_context* c) {
     if (!c) return fail(SFG_ERR_ARG, "sfg_initialize: null context");
     if (c->initialized) return fail(SFG_ERR_STATE, "sfg_initialize: already initialized");
@@ -591,6 +606,9 @@ extern "C" int sfg_initialize(sfg_context* c) {
         CU(cudaMalloc(&tb.fin[i], (size_t)tb.max_slots * 2 * TILE_CELLS * c->real_size()));
     }
     CU(dalloc(&tb.slot_tile, tb.max_slots));
+    CU(dalloc(&tb.slot_info, tb.max_slots));
+    tb.n_spread_ctr = c->Kmax + 3;
+    CU(dalloc(&tb.spread_ctr, tb.n_spread_ctr));
     CU(dalloc(&tb.n_slots, 1));
     CU(cudaMemset(tb.n_slots, 0, sizeof(int)));
     CU(dalloc(&tb.list, 8LL * M));
@@ -650,9 +668,8 @@ extern "C" int sfg_initialize(sfg_context* c) {
 
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-    c->spread_grid = std::max(1, std::min((tb.max_slots + 7) / 8, nsm * spread_blocks_per_sm()));
-    c->persistent_ctas = nsm * lattice_ctas_per_sm(c->precision, c->any_adr);
-    c->learned_grid = nsm * 4;
+    c->nsm = nsm;
+    apply_launch_config(c);
     CU(cudaStreamSynchronize(c->stream));
     c->initialized = true;
     c->steps = 0;
@@ -685,6 +702,7 @@ static int enqueue_step_t(sfg_context* c, int p) {
         cudaMemsetAsync(c->tb.fluid_touched, 0, sizeof(int) * nch, st);
         cudaMemsetAsync(c->tb.resid_gate, 0, sizeof(unsigned) * nch, st);
         cudaMemsetAsync(c->tb.resid_plain, 0, sizeof(unsigned) * nch, st);
+        cudaMemsetAsync(c->tb.spread_ctr, 0, sizeof(int) * c->tb.n_spread_ctr, st);
         launch_membrane(c->d_caps, c->NC, c->mb, c->d_has_prev, c->maxn, c->d_status, st);
         mark(c, SFG_PHASE_MEMBRANE);
         launch_contact(c->d_chans, c->M, c->mb, c->cb, c->ncells, st);
@@ -692,8 +710,8 @@ static int enqueue_step_t(sfg_context* c, int p) {
         launch_tiles(c->d_chans, c->d_caps, c->M, c->mb, c->tb, c->tb.T, p, c->d_phi, c->d_status,
                      st);
         mark(c, SFG_PHASE_IBM_TILES);
-        launch_spread<R>(c->d_chans, c->mb, c->tb, p, 0, MDF_PLAIN, c->spread_grid, c->d_status,
-                         st);
+        launch_spread<R>(c->d_chans, c->mb, c->tb, p, 0, MDF_PLAIN, 0, c->spread_grid,
+                         c->d_status, st);
         mark(c, SFG_PHASE_IBM_SPREAD);
         launches += 1 + (c->ncells > 0 ? 7 : 1) + 9 + 1;
         const S* fp = static_cast<const S*>(c->f[p]);
@@ -709,13 +727,13 @@ static int enqueue_step_t(sfg_context* c, int p) {
                                      c->d_model, c->d_feat, c->d_frame, c->learned_grid,
                                      c->d_status, st);
             mark(c, SFG_PHASE_MDF_LEARNED);
-            launch_spread<R>(c->d_chans, c->mb, c->tb, p, 1, MDF_SEED, c->spread_grid,
+            launch_spread<R>(c->d_chans, c->mb, c->tb, p, 1, MDF_SEED, 1, c->spread_grid,
                              c->d_status, st);
             mark(c, SFG_PHASE_IBM_SPREAD);
             launch_mdf_interp<S, R>(c->d_chans, c->M, c->mb, fp, c->tb, p, 2, MDF_LEARNED, st);
             mark(c, SFG_PHASE_MDF_INTERP);
             launch_plain_needed(c->d_chans, nch, c->tb, st);
-            launch_spread<R>(c->d_chans, c->mb, c->tb, p, 2, MDF_LEARNED, c->spread_grid,
+            launch_spread<R>(c->d_chans, c->mb, c->tb, p, 2, MDF_LEARNED, 2, c->spread_grid,
                              c->d_status, st);
             mark(c, SFG_PHASE_IBM_SPREAD);
             launches += 6;
@@ -723,7 +741,7 @@ static int enqueue_step_t(sfg_context* c, int p) {
         for (int k = 1; k < c->Kmax; ++k) {
             launch_mdf_interp<S, R>(c->d_chans, c->M, c->mb, fp, c->tb, p, k, MDF_PLAIN, st);
             mark(c, SFG_PHASE_MDF_INTERP);
-            launch_spread<R>(c->d_chans, c->mb, c->tb, p, k, MDF_PLAIN, c->spread_grid,
+            launch_spread<R>(c->d_chans, c->mb, c->tb, p, k, MDF_PLAIN, 2 + k, c->spread_grid,
                              c->d_status, st);
             mark(c, SFG_PHASE_IBM_SPREAD);
             launches += 2;
@@ -847,6 +865,89 @@ static void drop_graphs(sfg_context* c) {
         if (c->gexec[i]) cudaGraphExecDestroy(c->gexec[i]);
         c->gexec[i] = nullptr;
     }
+}
+
+// ------------------------------------------------------------------------
+// launch-shape autotuner
+// ------------------------------------------------------------------------
+static int time_steps(sfg_context* c, int n, float* ms_per_step) {
+    drop_graphs(c);
+    int rc = sfg_step(c, 2);
+    if (rc) return rc;
+    CU(cudaStreamSynchronize(c->stream));
+    if ((rc = sfg_step(c, n))) return rc;
+    CU(cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    *ms_per_step = ms / (float)n;
+    return SFG_OK;
+}
+
+extern "C" int sfg_autotune(sfg_context* c, int steps_per_trial, int* steps_run) {
+    if (!c) return fail(SFG_ERR_ARG, "sfg_autotune: null context");
+    if (!c->initialized) return fail(SFG_ERR_STATE, "sfg_autotune: context not initialized");
+    if (steps_per_trial < 1) return fail(SFG_ERR_ARG, "sfg_autotune: steps_per_trial < 1");
+    CU(cudaSetDevice(c->device));
+    const bool prof = c->profiling;
+    c->profiling = false;
+    int run = 0;
+    // coordinate descent over the tunables, each trial timed on real steps
+    struct Knob {
+        int* v;
+        std::vector<int> cand;
+    };
+    std::vector<Knob> knobs;
+    const int lat_max = lattice_ctas_per_sm(c->precision, c->any_adr);
+    const int spr_max = spread_blocks_per_sm();
+    std::vector<int> lat, spr;
+    for (int k = 1; k <= lat_max; ++k) lat.push_back(k);
+    for (int k = 1; k <= spr_max; ++k) spr.push_back(k);
+    knobs.push_back({&c->lattice_cps, lat});
+    if (c->M > 0) {
+        knobs.push_back({&c->spread_cps, spr});
+        knobs.push_back({&c->tb.marker_block, {64, 128, 256}});
+        if (c->any_learned) knobs.push_back({&c->learned_cps, {1, 2, 4}});
+    }
+    if (c->lattice_cps == 0) c->lattice_cps = lat_max;
+    if (c->spread_cps == 0) c->spread_cps = spr_max;
+    for (auto& k : knobs) {
+        int best = *k.v;
+        float best_ms = 1e30f;
+        for (int v : k.cand) {
+            *k.v = v;
+            apply_launch_config(c);
+            float ms = 0.f;
+            int rc = time_steps(c, steps_per_trial, &ms);
+            run += 2 + steps_per_trial;
+            if (rc) {
+                c->profiling = prof;
+                return rc;
+            }
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = v;
+            }
+        }
+        *k.v = best;
+        apply_launch_config(c);
+    }
+    drop_graphs(c);
+    c->profiling = prof;
+    if (steps_run) *steps_run = run;
+    return SFG_OK;
+}
+
+extern "C" int sfg_get_launch_config(sfg_context* c, int* lattice_cps, int* spread_cps,
+                                     int* marker_block, int* learned_cps) {
+    if (!c) return fail(SFG_ERR_ARG, "sfg_get_launch_config: null context");
+    // the chosen counts (the spread grid is further capped by the slot count)
+    const int lat_max = lattice_ctas_per_sm(c->precision, c->any_adr);
+    const int spr_max = spread_blocks_per_sm();
+    if (lattice_cps) *lattice_cps = c->lattice_cps > 0 ? std::min(c->lattice_cps, lat_max) : lat_max;
+    if (spread_cps) *spread_cps = c->spread_cps > 0 ? std::min(c->spread_cps, spr_max) : spr_max;
+    if (marker_block) *marker_block = c->tb.marker_block;
+    if (learned_cps) *learned_cps = std::max(1, std::min(c->learned_cps, 4));
+    return SFG_OK;
 }
 
 extern "C" int sfg_set_mdf_model(sfg_context* c, sfg_mlp* net, double residual_threshold) {

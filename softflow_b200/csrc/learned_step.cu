@@ -139,7 +139,7 @@ void launch_mdf_learned(const ChannelDev* chans, const CapsuleDev* caps, int M,
                         unsigned* status, cudaStream_t st) {
     if (M <= 0) return;
     (void)f;
-    k_mdf_features<R><<<(M + 127) / 128, 128, 0, st>>>(
+    k_mdf_features<R><<<(M + tb.marker_block - 1) / tb.marker_block, tb.marker_block, 0, st>>>(
         chans, caps, M, mb, tb.tile_slot[parity], static_cast<const typename Mom4<R>::T*>(tb.mom),
         tb.acc, feat, frame);
     const int tiles = (M + mlp::ROWS - 1) / mlp::ROWS;

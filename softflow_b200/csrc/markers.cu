@@ -468,14 +468,33 @@ __global__ void k_ibm_prep(const ChannelDev* __restrict__ chans,
     }
 }
 
+// Slot map of the step, and per slot the record the spread reads first
+// (SlotInfo: tile, channel, tile origin, list length and offset, nx, ny), so
+// that a spread warp starts a slot with one 32-byte load.
 __global__ void k_tile_slots(int T, const int* __restrict__ tile_flag,
                              const int* __restrict__ slot_scan, int* __restrict__ tile_slot,
-                             int* __restrict__ slot_tile) {
+                             int* __restrict__ slot_tile, const ChannelDev* __restrict__ chans,
+                             const int* __restrict__ tile_chan, const int* __restrict__ tile_cnt,
+                             const int* __restrict__ list_off, SlotInfo* __restrict__ info) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= T) return;
     if (tile_flag[t]) {
-        tile_slot[t] = slot_scan[t];
-        slot_tile[slot_scan[t]] = t;
+        const int s = slot_scan[t];
+        tile_slot[t] = s;
+        slot_tile[s] = t;
+        const int chan = tile_chan[t];
+        const ChannelDev& ch = chans[chan];
+        const int local = t - ch.tile_base;
+        SlotInfo si;
+        si.tile = t;
+        si.chan = chan;
+        si.x0 = (local % ch.tiles_x) * TILE_W;
+        si.y0 = (local / ch.tiles_x) * TILE_H;
+        si.cnt = tile_cnt[t];
+        si.off = list_off[t];
+        si.nx = ch.nx;
+        si.ny = ch.ny;
+        info[s] = si;
     } else {
         tile_slot[t] = -1;
     }
@@ -509,16 +528,23 @@ constexpr int SPREAD_LCAP = 256;      // list entries sorted in shared memory pe
                                       // (a power of two: the bitonic sort pads to one)
 constexpr int SPREAD_LIST_MAX = 4096; // longer lists are clamped and flagged
 
-// Shared memory of one spread warp: the tile's accumulators, its sorted
-// marker list and a staging chunk of markers.
-constexpr int SPREAD_CHUNK = 16;      // markers staged at a time per warp
+// Shared memory of one spread warp: the tile's accumulators, the sort buffer
+// of its marker list (sweep 0) sharing storage with the stencil terms of a
+// chunk of markers.
+constexpr int SPREAD_CHUNK = 8;       // markers per chunk (staged, then two per product pass)
 struct SpreadWarpSmem {
     double ax[TILE_CELLS], ay[TILE_CELLS];
-    double fx[SPREAD_CHUNK], fy[SPREAD_CHUNK], ds[SPREAD_CHUNK];
+    union {
+        int list[SPREAD_LCAP];                 // sweep 0: the bitonic sort of the list
+        double2 p[SPREAD_CHUNK][16];           // stencil terms of a chunk of markers
+    } u;
+    double2 f[SPREAD_CHUNK];                   // staged marker data of the chunk
+    double ds[SPREAD_CHUNK];
     double wx[SPREAD_CHUNK][4], wy[SPREAD_CHUNK][4];
-    int ix[SPREAD_CHUNK], iy[SPREAD_CHUNK], ok[SPREAD_CHUNK];
-    int list[SPREAD_LCAP];
+    int ix[SPREAD_CHUNK], iy[SPREAD_CHUNK];
+    unsigned mask[SPREAD_CHUNK];               // stencil points that add (bit sy*4+sx)
 };
+static_assert(sizeof(int) * SPREAD_LCAP <= sizeof(double2) * SPREAD_CHUNK * 16, "union");
 constexpr size_t SPREAD_SMEM = sizeof(SpreadWarpSmem) * SPREAD_WARPS;
 
 // Deterministic spread into force tiles for MDF sweep `sweep`.  Sweep 0
@@ -532,9 +558,8 @@ constexpr size_t SPREAD_SMEM = sizeof(SpreadWarpSmem) * SPREAD_WARPS;
 // (simulation.cpp:540-609), writing the final tile force `fin` (type R).
 template <typename R>
 __global__ void __launch_bounds__(SPREAD_WARPS * 32)
-k_spread(const ChannelDev* __restrict__ chans, const int* __restrict__ tile_chan,
-         const int* __restrict__ n_slots_p, const int* __restrict__ slot_tile,
-         const int* __restrict__ tile_cnt, const int* __restrict__ list_off,
+k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot_info,
+         const int* __restrict__ n_slots_p, int* __restrict__ slot_ctr,
          int* __restrict__ list, MarkerBufs mb, double* __restrict__ acc,
          double* __restrict__ acc0, R* __restrict__ gsnap, R* __restrict__ fin, int sweep,
          int mode, const unsigned* __restrict__ resid_gate,
@@ -546,29 +571,38 @@ k_spread(const ChannelDev* __restrict__ chans, const int* __restrict__ tile_chan
     SpreadWarpSmem& W = reinterpret_cast<SpreadWarpSmem*>(spread_smem)[warp];
     double* ax = W.ax;
     double* ay = W.ay;
-    int* sl = W.list;
+    int* sl = W.u.list;
     const int n_slots = *n_slots_p;
-    for (int slot = blockIdx.x * SPREAD_WARPS + warp; slot < n_slots;
-         slot += gridDim.x * SPREAD_WARPS) {
-        const int t = slot_tile[slot];
-        const int chan = tile_chan[t];
+    // slots are claimed one at a time (balances uneven list lengths); the
+    // next slot's record is fetched while the current one is processed
+    auto claim = [&]() {
+        int v = 0;
+        if (lane == 0) v = atomicAdd(slot_ctr, 1);
+        return __shfl_sync(0xffffffffu, v, 0);
+    };
+    int next = claim();
+    SlotInfo nfo{};
+    if (next < n_slots) nfo = slot_info[next];
+    while (next < n_slots) {
+        const int slot = next;
+        const SlotInfo si = nfo;
+        next = claim();
+        if (next < n_slots) nfo = slot_info[next];
+        const int chan = si.chan;
         const ChannelDev& ch = chans[chan];
         const int K = ch.ibm_iterations > 1 ? ch.ibm_iterations : 1;
         if (sweep >= K) continue;  // warp-uniform
         if (sweep > 0 && !mdf_active(ch, mode, resid_gate, chan)) continue;  // sweep 0: all
-        const int nx = ch.nx, ny = ch.ny;
-        const int local = t - ch.tile_base;
-        const int x0 = (local % ch.tiles_x) * TILE_W, y0 = (local / ch.tiles_x) * TILE_H;
-        int cnt = tile_cnt[t];
-        const int off = list_off[t];
+        const int nx = si.nx, ny = si.ny;
+        const int x0 = si.x0, y0 = si.y0;
+        int cnt = si.cnt;
+        const int off = si.off;
         const int* lst;
         // the lists are sorted by the step's first spread (sweep 0) and
         // written back; later sweeps read them in order
         const bool do_sort = (sweep == 0);
         if (cnt <= SPREAD_LCAP && !do_sort) {
-            for (int i = lane; i < cnt; i += 32) sl[i] = list[off + i];
-            __syncwarp();
-            lst = sl;
+            lst = list + off;
         } else if (cnt <= SPREAD_LCAP) {
             int pow2 = 1;
             while (pow2 < cnt) pow2 <<= 1;
@@ -586,7 +620,8 @@ k_spread(const ChannelDev* __restrict__ chans, const int* __restrict__ tile_chan
                     __syncwarp();
                 }
             for (int i = lane; i < cnt; i += 32) list[off + i] = sl[i];
-            lst = sl;
+            __syncwarp();
+            lst = list + off;   // the sort buffer is reused for the stencil terms
         } else {
             if (cnt > SPREAD_LIST_MAX) {
                 if (lane == 0) atomicOr(status, (unsigned)ST_LIST_OVERFLOW);
@@ -619,54 +654,96 @@ k_spread(const ChannelDev* __restrict__ chans, const int* __restrict__ tile_chan
             }
         }
         __syncwarp();
-        // Markers in list order, staged SPREAD_CHUNK at a time (the loads of
-        // a chunk are in flight together).  Lane l owns column x0 + l of the
-        // tile; for each marker it adds to its own cells, so every cell
-        // still receives its terms in list order while lanes never share a
-        // cell (no warp synchronisation between markers).
+        // Markers in list order, SPREAD_CHUNK at a time.  Lane j < SPREAD_CHUNK
+        // loads marker j of the next chunk into registers while the current
+        // chunk is processed, then stages it in shared memory.  Two passes per
+        // chunk:
+        // 1. the stencil terms (f w) ds, all lanes busy: half-warp h takes
+        //    markers h, h+2, ..., lane & 15 the stencil point; the points
+        //    that add (cell in the tile and the lattice, w > 1e-15, finite
+        //    force) form the marker's mask;
+        // 2. the ordered additions: lane l owns column x0 + l of the tile and
+        //    adds each marker's terms for its column in list order, so every
+        //    cell receives its terms in the reference's order while lanes
+        //    never share a cell.
         const int xg = x0 + lane;
+        const int pt = lane & 15, psx = pt & 3, psy = pt >> 2;
+        double2 rf = make_double2(0.0, 0.0), rw0 = rf, rw1 = rf, rv0 = rf, rv1 = rf;
+        double rds = 0.0;
+        int rix = 0, riy = 0;
+        auto fetch = [&](int c) {
+            if (lane < SPREAD_CHUNK && c + lane < cnt) {
+                const int m = lst[c + lane];
+                rf = sweep == 0 ? mb.frc[m] : mb.dF[m];
+                rix = mb.ix0[m];
+                riy = mb.iy0[m];
+                rds = mb.ds[m];
+                const double2* wx2 = reinterpret_cast<const double2*>(mb.wx + 4 * (size_t)m);
+                const double2* wy2 = reinterpret_cast<const double2*>(mb.wy + 4 * (size_t)m);
+                rw0 = wx2[0]; rw1 = wx2[1]; rv0 = wy2[0]; rv1 = wy2[1];
+            }
+        };
+        fetch(0);
         for (int c0 = 0; c0 < cnt; c0 += SPREAD_CHUNK) {
             const int nb = cnt - c0 < SPREAD_CHUNK ? cnt - c0 : SPREAD_CHUNK;
             __syncwarp();
             if (lane < nb) {
-                const int m = lst[c0 + lane];
-                const double2 fo = sweep == 0 ? mb.frc[m] : mb.dF[m];
-                W.fx[lane] = fo.x;
-                W.fy[lane] = fo.y;
-                W.ok[lane] = !(isnan(fo.x) || isnan(fo.y));
-                W.ix[lane] = mb.ix0[m];
-                W.iy[lane] = mb.iy0[m];
-                W.ds[lane] = mb.ds[m];
-                const double2* wx2 = reinterpret_cast<const double2*>(mb.wx + 4 * (size_t)m);
-                const double2* wy2 = reinterpret_cast<const double2*>(mb.wy + 4 * (size_t)m);
-                const double2 a0 = wx2[0], a1 = wx2[1], b0 = wy2[0], b1 = wy2[1];
-                W.wx[lane][0] = a0.x; W.wx[lane][1] = a0.y; W.wx[lane][2] = a1.x; W.wx[lane][3] = a1.y;
-                W.wy[lane][0] = b0.x; W.wy[lane][1] = b0.y; W.wy[lane][2] = b1.x; W.wy[lane][3] = b1.y;
+                W.f[lane] = rf;
+                W.ds[lane] = rds;
+                W.ix[lane] = rix;
+                W.iy[lane] = riy;
+                W.wx[lane][0] = rw0.x; W.wx[lane][1] = rw0.y; W.wx[lane][2] = rw1.x; W.wx[lane][3] = rw1.y;
+                W.wy[lane][0] = rv0.x; W.wy[lane][1] = rv0.y; W.wy[lane][2] = rv1.x; W.wy[lane][3] = rv1.y;
+            }
+            __syncwarp();
+            fetch(c0 + SPREAD_CHUNK);   // in flight during the two passes
+            for (int jp = 0; jp < nb; jp += 2) {   // warp-uniform: two markers per pass
+                const int j = jp + (lane >> 4);
+                const bool live = j < nb;
+                const int js = live ? j : jp;
+                const double2 fo = W.f[js];
+                int jx = W.ix[js] - 1 + psx;
+                if (jx < 0) jx += nx;
+                if (jx >= nx) jx -= nx;
+                const int iy = W.iy[js] - 1 + psy;
+                const int cxl = jx - x0, cyl = iy - y0;
+                double2 pv = make_double2(0.0, 0.0);
+                bool ok = live && !(isnan(fo.x) || isnan(fo.y)) && iy >= 0 && iy < ny &&
+                          cxl >= 0 && cxl < TILE_W && cyl >= 0 && cyl < TILE_H;
+                if (ok) {
+                    const double w = W.wx[js][psx] * W.wy[js][psy];
+                    ok = w > 1e-15;
+                    if (ok) {
+                        const double ds = W.ds[js];
+                        pv.x = fo.x * w * ds;
+                        pv.y = fo.y * w * ds;
+                    }
+                }
+                const unsigned bits = __ballot_sync(0xffffffffu, ok);
+                if (live) {
+                    W.u.p[j][pt] = pv;
+                    if (pt == 0) W.mask[j] = (bits >> (lane & 16)) & 0xFFFFu;
+                }
             }
             __syncwarp();
             if (xg < nx) {
                 for (int j = 0; j < nb; ++j) {
-                    if (!W.ok[j]) continue;
+                    const unsigned msk = W.mask[j];
+                    if (!msk) continue;
                     // stencil column sx with wrap(ix0 - 1 + sx) == xg
                     int d = xg - W.ix[j] + 1;
                     if (d < 0) d += nx;
                     if (d < 0) d += nx;
                     if (d >= nx) d -= nx;
                     if (d >= 4) continue;
-                    const double wxs = W.wx[j][d];
-                    const double ds = W.ds[j], fx = W.fx[j], fy = W.fy[j];
-                    const int iyb = W.iy[j] - 1;
+                    const int rb = W.iy[j] - 1 - y0;
 #pragma unroll
                     for (int sy = 0; sy < 4; ++sy) {
-                        const int iy = iyb + sy;
-                        const int cyl = iy - y0;
-                        if (iy >= 0 && iy < ny && cyl >= 0 && cyl < TILE_H) {
-                            const double w = wxs * W.wy[j][sy];
-                            if (w > 1e-15) {
-                                const int c = cyl * TILE_W + lane;
-                                ax[c] += fx * w * ds;
-                                ay[c] += fy * w * ds;
-                            }
+                        if ((msk >> (sy * 4 + d)) & 1u) {
+                            const int c = (rb + sy) * TILE_W + lane;
+                            const double2 pv = W.u.p[j][sy * 4 + d];
+                            ax[c] += pv.x;
+                            ay[c] += pv.y;
                         }
                     }
                 }
@@ -794,18 +871,17 @@ void launch_plain_needed(const ChannelDev* chans, int nch, TileBufs& tb, cudaStr
 // (rows of 32 cells: coalesced population loads).
 template <typename S, typename R>
 __global__ void k_tile_moments(const ChannelDev* __restrict__ chans,
-                               const int* __restrict__ tile_chan, const int* __restrict__ n_slots_p,
-                               const int* __restrict__ slot_tile, const S* __restrict__ f,
+                               const SlotInfo* __restrict__ slot_info,
+                               const int* __restrict__ n_slots_p, const S* __restrict__ f,
                                typename Mom4<R>::T* __restrict__ mom) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     const int n_slots = *n_slots_p;
     for (int slot = warp; slot < n_slots; slot += nwarps) {
-        const int t = slot_tile[slot];
-        const ChannelDev& ch = chans[tile_chan[t]];
-        const int local = t - ch.tile_base;
-        const int x0 = (local % ch.tiles_x) * TILE_W, y0 = (local / ch.tiles_x) * TILE_H;
+        const SlotInfo si = slot_info[slot];
+        const ChannelDev& ch = chans[si.chan];
+        const int x0 = si.x0, y0 = si.y0;
         const int jx = x0 + lane;
 #pragma unroll
         for (int r = 0; r < TILE_H; ++r) {
@@ -936,28 +1012,31 @@ void launch_tiles(const ChannelDev* chans, const CapsuleDev* caps, int M, const 
     scan_exclusive(tb.tile_flag, tb.slot_scan, T, tb.scan_tmp, tb.n_slots, st);
     scan_exclusive(tb.tile_cnt, tb.list_off, T, tb.scan_tmp, nullptr, st);
     k_tile_slots<<<(T + B - 1) / B, B, 0, st>>>(T, tb.tile_flag, tb.slot_scan,
-                                                tb.tile_slot[parity], tb.slot_tile);
+                                                tb.tile_slot[parity], tb.slot_tile, chans,
+                                                tb.tile_chan, tb.tile_cnt, tb.list_off,
+                                                tb.slot_info);
     k_tile_fill<<<G, B, 0, st>>>(chans, M, mb, tb.list_off, tb.cursor, tb.list);
 }
 
 template <typename R>
 void launch_spread(const ChannelDev* chans, const MarkerBufs& mb, TileBufs& tb, int parity,
-                   int sweep, int mode, int grid, unsigned* status, cudaStream_t st) {
+                   int sweep, int mode, int launch_idx, int grid, unsigned* status,
+                   cudaStream_t st) {
     k_spread<R><<<grid, SPREAD_WARPS * 32, SPREAD_SMEM, st>>>(
-        chans, tb.tile_chan, tb.n_slots, tb.slot_tile, tb.tile_cnt, tb.list_off, tb.list, mb,
+        chans, tb.slot_info, tb.n_slots, tb.spread_ctr + launch_idx, tb.list, mb,
         tb.acc, tb.acc0, static_cast<R*>(tb.gsnap), static_cast<R*>(tb.fin[parity]), sweep, mode,
         tb.resid_gate, tb.plain_needed, tb.capped, tb.fluid_touched, status);
 }
 template void launch_spread<double>(const ChannelDev*, const MarkerBufs&, TileBufs&, int, int,
-                                    int, int, unsigned*, cudaStream_t);
+                                    int, int, int, unsigned*, cudaStream_t);
 template void launch_spread<float>(const ChannelDev*, const MarkerBufs&, TileBufs&, int, int, int,
-                                   int, unsigned*, cudaStream_t);
+                                   int, int, unsigned*, cudaStream_t);
 
 template <typename S, typename R>
 void launch_mdf_interp(const ChannelDev* chans, int M, const MarkerBufs& mb, const S* f,
                        TileBufs& tb, int parity, int sweep, int mode, cudaStream_t st) {
     (void)f;
-    const int B = 128, G = (M + B - 1) / B;
+    const int B = tb.marker_block, G = (M + B - 1) / B;
     k_mdf_interp<S, R><<<G, B, 0, st>>>(chans, M, mb, tb.tile_slot[parity],
                                         static_cast<const typename Mom4<R>::T*>(tb.mom), tb.acc,
                                         tb.acc0, sweep, mode, tb.resid_gate, tb.resid_plain,
@@ -967,14 +1046,14 @@ void launch_mdf_interp(const ChannelDev* chans, int M, const MarkerBufs& mb, con
 template <typename S, typename R>
 void launch_tile_moments(const ChannelDev* chans, const S* f, TileBufs& tb, int grid,
                          cudaStream_t st) {
-    k_tile_moments<S, R><<<grid, 256, 0, st>>>(chans, tb.tile_chan, tb.n_slots, tb.slot_tile, f,
+    k_tile_moments<S, R><<<grid, 256, 0, st>>>(chans, tb.slot_info, tb.n_slots, f,
                                                static_cast<typename Mom4<R>::T*>(tb.mom));
 }
 
 template <typename S, typename R>
 void launch_interp_move(const ChannelDev* chans, int M, const MarkerBufs& mb, const S* f,
                         TileBufs& tb, int parity, const double* phi_tbl, cudaStream_t st) {
-    const int B = 128, G = (M + B - 1) / B;
+    const int B = tb.marker_block, G = (M + B - 1) / B;
     k_interp_move<S, R><<<G, B, 0, st>>>(chans, M, mb, f, tb.tile_slot[parity],
                                          static_cast<const R*>(tb.fin[parity]), phi_tbl);
 }

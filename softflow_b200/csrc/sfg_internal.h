@@ -15,6 +15,11 @@ struct ContactBufs {
     int* scan_tmp = nullptr;
 };
 
+// Per-slot record of the step's force tiles (written by k_tile_slots).
+struct SlotInfo {
+    int tile, chan, x0, y0, cnt, off, nx, ny;
+};
+
 struct TileBufs {
     int T = 0;                  // force tiles over all channels
     int max_slots = 0;
@@ -36,6 +41,11 @@ struct TileBufs {
     int* fluid_touched = nullptr;
     double* acc0 = nullptr;     // [max_slots][2][TILE_CELLS] force after the membrane spread
     void* mom = nullptr;        // [max_slots][TILE_CELLS] (rho, jx, jy, 0) of R (step's moments)
+    int marker_block = 128;         // block size of the per-marker kernels (tuned)
+    SlotInfo* slot_info = nullptr;  // [max_slots]
+    int* spread_ctr = nullptr;      // [n_spread_ctr] slot counters, one per spread launch of a
+                                    // step (zeroed at the start of the step)
+    int n_spread_ctr = 0;
     int* plain_needed = nullptr;  // [1] set when some channel needs the plain sweeps; null
                                   // (always run them) unless a channel is learned
     unsigned* resid_gate = nullptr;   // [nchan] learned form's no-slip residual (float bits)
@@ -62,10 +72,12 @@ void launch_tiles(const ChannelDev* chans, const CapsuleDev* caps, int M, const 
                   TileBufs& tb, int T, int parity, const double* phi_tbl, unsigned* status,
                   cudaStream_t st);
 // Spread of sweep `sweep` in forcing mode `mode` (MdfMode); sweep 0 spreads
-// the membrane and contact forces of every channel.
+// the membrane and contact forces of every channel.  launch_idx: the
+// launch's slot counter in tb.spread_ctr (distinct per launch of a step).
 template <typename R>
 void launch_spread(const ChannelDev* chans, const MarkerBufs& mb, TileBufs& tb, int parity,
-                   int sweep, int mode, int grid, unsigned* status, cudaStream_t st);
+                   int sweep, int mode, int launch_idx, int grid, unsigned* status,
+                   cudaStream_t st);
 template <typename S, typename R>
 void launch_mdf_interp(const ChannelDev* chans, int M, const MarkerBufs& mb, const S* f,
                        TileBufs& tb, int parity, int sweep, int mode, cudaStream_t st);

@@ -664,6 +664,26 @@ class Ensemble:
     def context(self) -> _Context:
         return self._need()
 
+    # ---- launch shapes
+    def autotune(self, steps_per_trial: int = 5) -> dict:
+        """Times candidate launch shapes on real steps and keeps the fastest;
+        the ensemble advances by the returned number of steps."""
+        ctx = self._need()
+        n = C.c_int()
+        L.check(ctx._lib.sfg_autotune(ctx._h, int(steps_per_trial), C.byref(n)))
+        ctx.synchronize()
+        self._steps += int(n.value)
+        cfg = self.launchConfig()
+        cfg["steps_run"] = int(n.value)
+        return cfg
+
+    def launchConfig(self) -> dict:
+        ctx = self._need()
+        v = [C.c_int() for _ in range(4)]
+        L.check(ctx._lib.sfg_get_launch_config(ctx._h, *[C.byref(x) for x in v]))
+        return dict(lattice_ctas_per_sm=v[0].value, spread_ctas_per_sm=v[1].value,
+                    marker_block=v[2].value, learned_ctas_per_sm=v[3].value)
+
     # ---- learned multi-direct forcing
     def setLearnedMDF(self, net=None, threshold: float = 1e-4):
         """Use the network `net` (softflow_b200.learned.MDFNetwork) to seed
