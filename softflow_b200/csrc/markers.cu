@@ -529,22 +529,16 @@ constexpr int SPREAD_LCAP = 256;      // list entries sorted in shared memory pe
 constexpr int SPREAD_LIST_MAX = 4096; // longer lists are clamped and flagged
 
 // Shared memory of one spread warp: the tile's accumulators, the sort buffer
-// of its marker list (sweep 0) sharing storage with the stencil terms of a
-// chunk of markers.
-constexpr int SPREAD_CHUNK = 8;       // markers per chunk (staged, then two per product pass)
+// of its marker list (sweep 0) and a staged chunk of markers.
+constexpr int SPREAD_CHUNK = 16;      // markers staged per chunk
 struct SpreadWarpSmem {
     double ax[TILE_CELLS], ay[TILE_CELLS];
-    union {
-        int list[SPREAD_LCAP];                 // sweep 0: the bitonic sort of the list
-        double2 p[SPREAD_CHUNK][16];           // stencil terms of a chunk of markers
-    } u;
+    int list[SPREAD_LCAP];                     // sweep 0: the bitonic sort of long lists
     double2 f[SPREAD_CHUNK];                   // staged marker data of the chunk
     double ds[SPREAD_CHUNK];
     double wx[SPREAD_CHUNK][4], wy[SPREAD_CHUNK][4];
-    int ix[SPREAD_CHUNK], iy[SPREAD_CHUNK];
-    unsigned mask[SPREAD_CHUNK];               // stencil points that add (bit sy*4+sx)
+    int ix[SPREAD_CHUNK], iy[SPREAD_CHUNK], ok[SPREAD_CHUNK];
 };
-static_assert(sizeof(int) * SPREAD_LCAP <= sizeof(double2) * SPREAD_CHUNK * 16, "union");
 constexpr size_t SPREAD_SMEM = sizeof(SpreadWarpSmem) * SPREAD_WARPS;
 
 // Deterministic spread into force tiles for MDF sweep `sweep`.  Sweep 0
@@ -571,7 +565,7 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
     SpreadWarpSmem& W = reinterpret_cast<SpreadWarpSmem*>(spread_smem)[warp];
     double* ax = W.ax;
     double* ay = W.ay;
-    int* sl = W.u.list;
+    int* sl = W.list;
     const int n_slots = *n_slots_p;
     // slots are claimed one at a time (balances uneven list lengths); the
     // next slot's record is fetched while the current one is processed
@@ -603,6 +597,20 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
         const bool do_sort = (sweep == 0);
         if (cnt <= SPREAD_LCAP && !do_sort) {
             lst = list + off;
+        } else if (cnt <= 32) {
+            // bitonic sort across the warp's registers (ascending by lane)
+            int v = lane < cnt ? list[off + lane] : INT_MAX;
+#pragma unroll
+            for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    const int o = __shfl_xor_sync(0xffffffffu, v, j);
+                    const bool take_min = ((lane & j) == 0) == ((lane & k) == 0);
+                    v = take_min ? min(v, o) : max(v, o);
+                }
+            if (lane < cnt) list[off + lane] = v;
+            __syncwarp();
+            lst = list + off;
         } else if (cnt <= SPREAD_LCAP) {
             int pow2 = 1;
             while (pow2 < cnt) pow2 <<= 1;
@@ -621,7 +629,7 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
                 }
             for (int i = lane; i < cnt; i += 32) list[off + i] = sl[i];
             __syncwarp();
-            lst = list + off;   // the sort buffer is reused for the stencil terms
+            lst = list + off;
         } else {
             if (cnt > SPREAD_LIST_MAX) {
                 if (lane == 0) atomicOr(status, (unsigned)ST_LIST_OVERFLOW);
@@ -654,20 +662,16 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
             }
         }
         __syncwarp();
-        // Markers in list order, SPREAD_CHUNK at a time.  Lane j < SPREAD_CHUNK
+        // Markers in list order, SPREAD_CHUNK at a time: lane j < SPREAD_CHUNK
         // loads marker j of the next chunk into registers while the current
-        // chunk is processed, then stages it in shared memory.  Two passes per
-        // chunk:
-        // 1. the stencil terms (f w) ds, all lanes busy: half-warp h takes
-        //    markers h, h+2, ..., lane & 15 the stencil point; the points
-        //    that add (cell in the tile and the lattice, w > 1e-15, finite
-        //    force) form the marker's mask;
-        // 2. the ordered additions: lane l owns column x0 + l of the tile and
-        //    adds each marker's terms for its column in list order, so every
-        //    cell receives its terms in the reference's order while lanes
-        //    never share a cell.
-        const int xg = x0 + lane;
-        const int pt = lane & 15, psx = pt & 3, psy = pt >> 2;
+        // chunk is added, then stages it in shared memory.  Lane (a, b) =
+        // (lane & 7, lane >> 3) owns the tile cells whose local column is
+        // a mod 8 and row b mod 4; the 4 x 4 stencil of a marker has 4
+        // consecutive columns and rows, so its 16 points fall on 16 distinct
+        // lanes.  Each lane adds its own point's term to its own cell, marker
+        // after marker, so every cell receives its terms in the reference's
+        // order with no synchronisation between markers.
+        const int la = lane & 7, lb = lane >> 3;
         double2 rf = make_double2(0.0, 0.0), rw0 = rf, rw1 = rf, rv0 = rf, rv1 = rf;
         double rds = 0.0;
         int rix = 0, riy = 0;
@@ -689,6 +693,7 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
             __syncwarp();
             if (lane < nb) {
                 W.f[lane] = rf;
+                W.ok[lane] = !(isnan(rf.x) || isnan(rf.y));
                 W.ds[lane] = rds;
                 W.ix[lane] = rix;
                 W.iy[lane] = riy;
@@ -696,55 +701,63 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
                 W.wy[lane][0] = rv0.x; W.wy[lane][1] = rv0.y; W.wy[lane][2] = rv1.x; W.wy[lane][3] = rv1.y;
             }
             __syncwarp();
-            fetch(c0 + SPREAD_CHUNK);   // in flight during the two passes
-            for (int jp = 0; jp < nb; jp += 2) {   // warp-uniform: two markers per pass
-                const int j = jp + (lane >> 4);
-                const bool live = j < nb;
-                const int js = live ? j : jp;
-                const double2 fo = W.f[js];
-                int jx = W.ix[js] - 1 + psx;
-                if (jx < 0) jx += nx;
-                if (jx >= nx) jx -= nx;
-                const int iy = W.iy[js] - 1 + psy;
-                const int cxl = jx - x0, cyl = iy - y0;
-                double2 pv = make_double2(0.0, 0.0);
-                bool ok = live && !(isnan(fo.x) || isnan(fo.y)) && iy >= 0 && iy < ny &&
-                          cxl >= 0 && cxl < TILE_W && cyl >= 0 && cyl < TILE_H;
-                if (ok) {
-                    const double w = W.wx[js][psx] * W.wy[js][psy];
-                    ok = w > 1e-15;
-                    if (ok) {
-                        const double ds = W.ds[js];
-                        pv.x = fo.x * w * ds;
-                        pv.y = fo.y * w * ds;
+            fetch(c0 + SPREAD_CHUNK);   // in flight while this chunk is added
+            for (int j = 0; j < nb; ++j) {
+                if (!W.ok[j]) continue;  // warp-uniform
+                const int jx0 = W.ix[j] - 1;
+                if (nx <= TILE_W) {
+                    // one tile holds both sides of the periodic seam: two
+                    // stencil columns can share a residue, so apply every one
+                    const int r0n = W.iy[j] - 1 - y0;
+                    const int syn = (lb - r0n) & 3;
+                    const int cyn = r0n + syn;
+                    if (cyn >= 0 && cyn < TILE_H && cyn + y0 >= 0 && cyn + y0 < ny) {
+                        for (int k = 0; k < 4; ++k) {
+                            int jx = jx0 + k;
+                            if (jx < 0) jx += nx;
+                            if (jx >= nx) jx -= nx;
+                            const int cl = jx - x0;
+                            if (cl < 0 || cl >= TILE_W || (cl & 7) != la) continue;
+                            const double w = W.wx[j][k] * W.wy[j][syn];
+                            if (w > 1e-15) {
+                                const double ds = W.ds[j];
+                                const double2 fo = W.f[j];
+                                const int c = cyn * TILE_W + cl;
+                                ax[c] += fo.x * w * ds;
+                                ay[c] += fo.y * w * ds;
+                            }
+                        }
+                    }
+                    continue;
+                }
+                // this lane's stencil column sx: wrap(ix0 - 1 + sx) in the tile
+                // with local column a mod 8 (at most one of the 4 when the tile
+                // does not hold both sides of the seam)
+                int sx = -1, cxl = 0;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    int jx = jx0 + k;
+                    if (jx < 0) jx += nx;
+                    if (jx >= nx) jx -= nx;
+                    const int cl = jx - x0;
+                    if (cl >= 0 && cl < TILE_W && (cl & 7) == la) {
+                        sx = k;
+                        cxl = cl;
                     }
                 }
-                const unsigned bits = __ballot_sync(0xffffffffu, ok);
-                if (live) {
-                    W.u.p[j][pt] = pv;
-                    if (pt == 0) W.mask[j] = (bits >> (lane & 16)) & 0xFFFFu;
-                }
-            }
-            __syncwarp();
-            if (xg < nx) {
-                for (int j = 0; j < nb; ++j) {
-                    const unsigned msk = W.mask[j];
-                    if (!msk) continue;
-                    // stencil column sx with wrap(ix0 - 1 + sx) == xg
-                    int d = xg - W.ix[j] + 1;
-                    if (d < 0) d += nx;
-                    if (d < 0) d += nx;
-                    if (d >= nx) d -= nx;
-                    if (d >= 4) continue;
-                    const int rb = W.iy[j] - 1 - y0;
-#pragma unroll
-                    for (int sy = 0; sy < 4; ++sy) {
-                        if ((msk >> (sy * 4 + d)) & 1u) {
-                            const int c = (rb + sy) * TILE_W + lane;
-                            const double2 pv = W.u.p[j][sy * 4 + d];
-                            ax[c] += pv.x;
-                            ay[c] += pv.y;
-                        }
+                // and its row sy: local row b mod 4 (exactly one of the 4)
+                const int r0 = W.iy[j] - 1 - y0;
+                const int sy = (lb - r0) & 3;
+                const int cyl = r0 + sy;
+                const int iy = cyl + y0;
+                if (sx >= 0 && cyl >= 0 && cyl < TILE_H && iy >= 0 && iy < ny) {
+                    const double w = W.wx[j][sx] * W.wy[j][sy];
+                    if (w > 1e-15) {
+                        const double ds = W.ds[j];
+                        const double2 fo = W.f[j];
+                        const int c = cyl * TILE_W + cxl;
+                        ax[c] += fo.x * w * ds;
+                        ay[c] += fo.y * w * ds;
                     }
                 }
             }

@@ -50,6 +50,13 @@ CASES = {
                         capsules=[("add", 1.5, 15.3, 5.0, 32,
                                    dict(model=O.NEO_HOOKEAN, G_s=0.05))],
                         conc=None),
+    # a channel narrower than one 32-wide force tile: the stencil of a capsule
+    # across the seam covers columns 8, 9, 0, 1 of the same tile
+    "narrow_seam": dict(spec=dict(nx=10, ny=24, collision=O.BGK, tau=0.8, body_fx=2e-5,
+                                  ibm_iterations=3),
+                        capsules=[("add", 0.7, 11.6, 2.0, 12,
+                                   dict(model=O.NEO_HOOKEAN, G_s=0.05))],
+                        conc=None),
     # config 2 in miniature: MRT, WLC + Helfrich and Skalak, scalar transport
     "mini_c2": dict(spec=dict(nx=128, ny=64, collision=O.MRT, tau=0.8, body_fx=1e-5,
                               scalar_enabled=1, scalar_D=0.05),

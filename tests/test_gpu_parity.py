@@ -48,7 +48,8 @@ def test_fp64_lattice_bit_exact(sfg, oracle_mod, name, steps):
         assert np.array_equal(a[k], b[k]), k
 
 
-@pytest.mark.parametrize("name,steps", [("seam_single", 60), ("c1", 40), ("c1_plain", 40),
+@pytest.mark.parametrize("name,steps", [("seam_single", 60), ("narrow_seam", 60), ("c1", 40),
+                                        ("c1_plain", 40),
                                         ("mini_c2", 40), ("contact_brute", 60)])
 def test_fp64_coupled(sfg, oracle_mod, name, steps):
     case = CASES[name]
@@ -71,7 +72,7 @@ def test_fp64_coupled(sfg, oracle_mod, name, steps):
         assert rel_l2(C, o.concentration()) < 1e-9
 
 
-@pytest.mark.parametrize("name", ["seam_single", "c1_plain"])
+@pytest.mark.parametrize("name", ["seam_single", "narrow_seam", "c1_plain"])
 def test_fp64_single_capsule_first_steps_bit_exact(sfg, oracle_mod, name):
     """Without contact (pow) or Helfrich (atan2), a step is reproduced bit for
     bit: membrane forces, ds, spreading, MDF, collision, interpolation, move."""
@@ -81,7 +82,7 @@ def test_fp64_single_capsule_first_steps_bit_exact(sfg, oracle_mod, name):
     o.step(1)
     sim.run(1)
     a, b = _state(sim), _ostate(o)
-    if name == "seam_single":
+    if name in ("seam_single", "narrow_seam"):
         for k in ("Fx", "Fy", "ux", "uy", "rho", "pos", "vel", "frc"):
             assert np.array_equal(a[k], b[k]), k
 
