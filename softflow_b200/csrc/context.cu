@@ -272,7 +272,7 @@ static void free_all(sfg_context* c) {
     F(c->tb.slot_scan); F(c->tb.list_off); F(c->tb.slot_tile); F(c->tb.n_slots);
     F(c->tb.list); F(c->tb.scan_tmp); F(c->tb.acc); F(c->tb.gsnap); F(c->tb.capped);
     F(c->tb.fluid_touched); F(c->tb.acc0); F(c->tb.mom); F(c->tb.slot_info); F(c->tb.spread_ctr); F(c->tb.resid_gate); F(c->tb.resid_plain);
-    F(c->mb.u0); F(c->mb.dFsum); F(c->mb.dFprev);
+    F(c->mb.u0); F(c->mb.dFsum); F(c->mb.dFprev); F(c->mb.slot8);
     F(c->d_model); F(c->d_learned_steps); F(c->d_fallbacks);
     F(c->d_hfeat); F(c->d_hlab); F(c->d_hvalid); F(c->d_feat); F(c->d_frame); F(c->d_plain_needed);
     F(c->cb.cell_of); F(c->cb.cell_cnt); F(c->cb.cell_start); F(c->cb.cursor); F(c->cb.list);
@@ -632,6 +632,7 @@ extern "C" int sfg_initialize(sfg_context* c) {
     CU(dalloc(&c->mb.u0, M));
     CU(dalloc(&c->mb.dFsum, M));
     CU(dalloc(&c->mb.dFprev, M));
+    CU(dalloc(&c->mb.slot8, 8LL * M));
     if (M > 0) {
         CU(cudaMemset(c->mb.u0, 0, sizeof(double2) * M));
         CU(cudaMemset(c->mb.dFsum, 0, sizeof(double2) * M));

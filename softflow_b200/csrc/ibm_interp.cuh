@@ -27,22 +27,33 @@ __device__ __forceinline__ void cell_rho_j(const ChannelDev& ch, const S* __rest
     jyo = (double)b;
 }
 
-__device__ __forceinline__ size_t tile_cell_index(const ChannelDev& ch, const int* tile_slot,
-                                                  int jx, int jy) {
-    const int t = ch.tile_base + (jy / TILE_H) * ch.tiles_x + (jx / TILE_W);
-    const int s = tile_slot[t];
-    return (size_t)s * 2 * TILE_CELLS + (jy % TILE_H) * TILE_W + (jx % TILE_W);
-}
-
 // u = (j + F/2)/rho at the marker's 4 x 4 stencil with the accumulated force
 // acc (immersed_boundary.cpp:174-229 with the stencil weights of the step;
 // SOLID rows and rho <= 1e-15 contribute zero).
+// Slot of stencil cell (sx, jy) from the marker's slot record (k_tile_fill).
+struct StencilSlots {
+    int s[8];
+    int ty0;
+    __device__ __forceinline__ StencilSlots(const MarkerBufs& mb, int m, int iy0) {
+        const int4* p = reinterpret_cast<const int4*>(mb.slot8 + 8 * (size_t)m);
+        const int4 a = p[0], b = p[1];
+        s[0] = a.x; s[1] = a.y; s[2] = a.z; s[3] = a.w;
+        s[4] = b.x; s[5] = b.y; s[6] = b.z; s[7] = b.w;
+        ty0 = max(iy0 - 1, 0) / TILE_H;
+    }
+    __device__ __forceinline__ int slot(int sx, int jy) const {
+        return s[(jy / TILE_H != ty0 ? 4 : 0) + sx];
+    }
+};
+
 template <typename S, typename R, typename A = double>
 __device__ __forceinline__ double2 interp_u_acc(const ChannelDev& ch, const MarkerBufs& mb, int m,
                                                const S* __restrict__ f,
                                                const int* __restrict__ tile_slot,
                                                const A* __restrict__ acc) {
+    (void)tile_slot;
     const int ix0 = mb.ix0[m], iy0 = mb.iy0[m];
+    const StencilSlots ss(mb, m, iy0);
     double ux = 0.0, uy = 0.0;
     for (int iy = iy0 - 1; iy <= iy0 + 2; ++iy) {
         for (int ix = ix0 - 1; ix <= ix0 + 2; ++ix) {
@@ -58,7 +69,8 @@ __device__ __forceinline__ double2 interp_u_acc(const ChannelDev& ch, const Mark
                 cell_rho_j<S, R>(ch, f, jx, jy, rho, jxm, jym, solid);
                 double cu = 0.0, cv = 0.0;
                 if (!solid && rho > 1e-15) {
-                    const size_t ci = tile_cell_index(ch, tile_slot, jx, jy);
+                    const size_t ci = (size_t)ss.slot(ix - ix0 + 1, jy) * 2 * TILE_CELLS +
+                                      (jy % TILE_H) * TILE_W + (jx % TILE_W);
                     cu = (jxm + 0.5 * (double)acc[ci]) / rho;
                     cv = (jym + 0.5 * (double)acc[ci + TILE_CELLS]) / rho;
                 }
@@ -79,12 +91,6 @@ template <typename R> struct Mom4;
 template <> struct Mom4<double> { using T = double4; };
 template <> struct Mom4<float> { using T = float4; };
 
-__device__ __forceinline__ size_t tile_cell_mom(const ChannelDev& ch, const int* tile_slot, int jx,
-                                                int jy) {
-    const int t = ch.tile_base + (jy / TILE_H) * ch.tiles_x + (jx / TILE_W);
-    return (size_t)tile_slot[t] * TILE_CELLS + (jy % TILE_H) * TILE_W + (jx % TILE_W);
-}
-
 // interp_u_acc with the step's tile moments: the same terms in the same
 // order, so the same result bit for bit.
 template <typename R>
@@ -92,7 +98,9 @@ __device__ __forceinline__ double2 interp_u_mom(const ChannelDev& ch, const Mark
                                                const int* __restrict__ tile_slot,
                                                const typename Mom4<R>::T* __restrict__ mom,
                                                const double* __restrict__ acc) {
+    (void)tile_slot;
     const int ix0 = mb.ix0[m], iy0 = mb.iy0[m];
+    const StencilSlots ss(mb, m, iy0);
     double ux = 0.0, uy = 0.0;
 #pragma unroll
     for (int sy = 0; sy < 4; ++sy) {
@@ -105,7 +113,8 @@ __device__ __forceinline__ double2 interp_u_mom(const ChannelDev& ch, const Mark
             if (jy < 0 || jy >= ch.ny || jx < 0 || jx >= ch.nx) continue;
             const double w = mb.wx[4 * m + sx] * mb.wy[4 * m + sy];
             if (w > 1e-15) {
-                const size_t cm = tile_cell_mom(ch, tile_slot, jx, jy);
+                const size_t cm = (size_t)ss.slot(sx, jy) * TILE_CELLS + (jy % TILE_H) * TILE_W +
+                                  (jx % TILE_W);
                 const auto q = mom[cm];
                 const double rho = (double)q.x;
                 double cu = 0.0, cv = 0.0;
@@ -124,14 +133,20 @@ __device__ __forceinline__ double2 interp_u_mom(const ChannelDev& ch, const Mark
 
 // rho_nearest with the tile moments (the nearest node lies in the stencil).
 template <typename R>
-__device__ __forceinline__ double rho_nearest_mom(const ChannelDev& ch, const int* tile_slot,
-                                                  const typename Mom4<R>::T* __restrict__ mom,
+__device__ __forceinline__ double rho_nearest_mom(const ChannelDev& ch, const MarkerBufs& mb,
+                                                  int m, const typename Mom4<R>::T* __restrict__ mom,
                                                   double2 p) {
     int ixr = (int)(p.x + 0.5), iyr = (int)(p.y + 0.5);
     if (ixr < 0) ixr += ch.nx;
     if (ixr >= ch.nx) ixr -= ch.nx;
-    if (iyr >= 0 && iyr < ch.ny && ixr >= 0 && ixr < ch.nx)
-        return (double)mom[tile_cell_mom(ch, tile_slot, ixr, iyr)].x;
+    if (iyr >= 0 && iyr < ch.ny && ixr >= 0 && ixr < ch.nx) {
+        // the nearest node is stencil column 1 or 2 (x - floor(x) < 1)
+        const int ix0 = mb.ix0[m];
+        const int sx = (int)(p.x + 0.5) - ix0 + 1;
+        const StencilSlots ss(mb, m, mb.iy0[m]);
+        return (double)mom[(size_t)ss.slot(sx, iyr) * TILE_CELLS + (iyr % TILE_H) * TILE_W +
+                           (ixr % TILE_W)].x;
+    }
     return 1.0;
 }
 

@@ -502,13 +502,31 @@ __global__ void k_tile_slots(int T, const int* __restrict__ tile_flag,
 
 __global__ void k_tile_fill(const ChannelDev* __restrict__ chans, int M, MarkerBufs mb,
                             const int* __restrict__ list_off, int* __restrict__ cursor,
-                            int* __restrict__ list) {
+                            int* __restrict__ list, const int* __restrict__ tile_slot) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M || !mb.valid[m]) return;
     const ChannelDev& ch = chans[mb.mk_chan[m]];
+    const int ix0 = mb.ix0[m], iy0 = mb.iy0[m];
     int t[8];
-    const int nt = stencil_tiles(ch, mb.ix0[m], mb.iy0[m], t);
+    const int nt = stencil_tiles(ch, ix0, iy0, t);
     for (int a = 0; a < nt; ++a) list[list_off[t[a]] + atomicAdd(&cursor[t[a]], 1)] = m;
+    // the slot of every stencil cell, by row tile and stencil column, for the
+    // interpolations of the step (one 32-byte record instead of 16 lookups)
+    int s8[8];
+    const int ty0 = max(iy0 - 1, 0) / TILE_H, ty1 = min(iy0 + 2, ch.ny - 1) / TILE_H;
+#pragma unroll
+    for (int sx = 0; sx < 4; ++sx) {
+        int jx = ix0 - 1 + sx;
+        if (jx < 0) jx += ch.nx;
+        if (jx >= ch.nx) jx -= ch.nx;
+        const bool in = jx >= 0 && jx < ch.nx;
+        const int tx = in ? jx / TILE_W : 0;
+        s8[sx] = in ? tile_slot[ch.tile_base + ty0 * ch.tiles_x + tx] : -1;
+        s8[4 + sx] = in ? tile_slot[ch.tile_base + ty1 * ch.tiles_x + tx] : -1;
+    }
+    int4* o = reinterpret_cast<int4*>(mb.slot8 + 8 * (size_t)m);
+    o[0] = make_int4(s8[0], s8[1], s8[2], s8[3]);
+    o[1] = make_int4(s8[4], s8[5], s8[6], s8[7]);
 }
 
 // Stencil column of lattice column jx for a marker with origin ix0 (the
@@ -838,7 +856,7 @@ __global__ void k_mdf_interp(const ChannelDev* __restrict__ chans, int M, Marker
     if (!mdf_active(ch, mode, resid_gate, chan)) return;
     const double* base = (mode == MDF_PLAIN && ch.learned && sweep == 1) ? acc0 : acc;
     const double2 u = interp_u_mom<R>(ch, mb, m, tile_slot, mom, base);
-    const double rho_local = rho_nearest_mom<R>(ch, tile_slot, mom, mb.pos[m]);
+    const double rho_local = rho_nearest_mom<R>(ch, mb, m, mom, mb.pos[m]);
     const double2 v = mb.vel[m];
     const double dux = v.x - u.x, duy = v.y - u.y;
     const double2 d = make_double2(dux * (2.0 * rho_local), duy * (2.0 * rho_local));
@@ -1028,7 +1046,8 @@ void launch_tiles(const ChannelDev* chans, const CapsuleDev* caps, int M, const 
                                                 tb.tile_slot[parity], tb.slot_tile, chans,
                                                 tb.tile_chan, tb.tile_cnt, tb.list_off,
                                                 tb.slot_info);
-    k_tile_fill<<<G, B, 0, st>>>(chans, M, mb, tb.list_off, tb.cursor, tb.list);
+    k_tile_fill<<<G, B, 0, st>>>(chans, M, mb, tb.list_off, tb.cursor, tb.list,
+                                 tb.tile_slot[parity]);
 }
 
 template <typename R>

@@ -34,6 +34,9 @@ struct MarkerBufs {
     double2* u0;        // velocity interpolated after the membrane-force spread
     double2* dFsum;     // forcing correction of this step summed over its sweeps
     double2* dFprev;    // previous step's correction before its last sweep
+    // force-tile slots of the marker's stencil, this step: [M][2][4] =
+    // [row tile (of the first / last stencil row)][stencil column sx]
+    int* slot8;
 };
 
 // ---------------- Peskin 4-point delta via the 1024-bin table --------------
