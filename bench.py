@@ -42,6 +42,12 @@ if ROOT not in sys.path:
 
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM = 6650.0
+# DRAM bytes (read + write) per fluid cell of one lattice-kernel launch,
+# from one ncu capture of the same workload and precision (named beside each
+# figure); the bench cannot run ncu on itself, so it reports these.
+MEASURED_TRAFFIC = {
+    ("c3", "fp16s"): (508.8e6 / 12_479_984, "profiles/k_lattice_step4_c3_fp16s.md"),
+}
 
 
 def parse():
@@ -116,16 +122,60 @@ def make_plans(workload, precision, world=1, rank=0):
 
 # --------------------------------------------------------------- clocks ----
 class ClockSampler:
+    """SM clock and clock-event reasons of this rank's GPU while the timed
+    region runs.  NVML is polled every 10 ms from a thread (the timed region
+    of the default run lasts a fraction of a second); where NVML cannot be
+    loaded, nvidia-smi is polled every 200 ms instead.  Reading only: no
+    setting of the GPU is changed."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits (nvml.h: nvmlClocksEventReason*)
+    REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8,
+                   "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
         self.path = None
+        self.thread = None
+        self.rows = []
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
     def start(self):
+        import threading
+        try:
+            nv, h = self._nvml_handle()
+        except Exception:
+            nv = None
+        if nv is not None:
+            self.stop_evt = threading.Event()
+            mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons",
+                                  None) or nv.nvmlDeviceGetCurrentClocksThrottleReasons
+
+            def poll():
+                while True:
+                    try:
+                        self.rows.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                          mx, int(get_reasons(h))))
+                    except Exception:
+                        pass
+                    if self.stop_evt.wait(0.01):
+                        break
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
@@ -136,7 +186,24 @@ class ClockSampler:
         except Exception:
             self.proc = None
 
+    def _summary(self, sm, mx, reasons, source):
+        if not sm:
+            return None
+        sm = sorted(sm)
+        return {"sm_mhz": sm[len(sm) // 2], "sm_min_mhz": sm[0], "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm), "source": source}
+
     def stop(self):
+        if self.thread is not None:
+            self.stop_evt.set()
+            self.thread.join(timeout=5)
+            reasons = set()
+            for _, _, bits in self.rows:
+                for n, b in self.REASON_BITS.items():
+                    if bits & b:
+                        reasons.add(n)
+            mx = max((r[1] for r in self.rows), default=None)
+            return self._summary([r[0] for r in self.rows], mx, reasons, "nvml, 10 ms")
         if self.proc is None:
             return None
         self.proc.terminate()
@@ -161,10 +228,7 @@ class ClockSampler:
             for n, v in zip(names, r[5:9]):
                 if v.lower().startswith("active"):
                     reasons.add(n)
-        sm.sort()
-        med = sm[len(sm) // 2] if sm else None
-        return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(rows)}
+        return self._summary(sm, mx, reasons, "nvidia-smi, 200 ms")
 
 
 def peaks():
@@ -257,6 +321,10 @@ def run_product(args, world, rank, local, pg):
         args.precision)
     achieved = alg_bytes / (lat_ms / 1e3) / 1e9 if lat_ms > 0 else 0.0
     peak, peak_kind = peaks()
+    traffic, traffic_src = None, None
+    if (args.workload, args.precision) in MEASURED_TRAFFIC and scal == 0:
+        per_cell, traffic_src = MEASURED_TRAFFIC[(args.workload, args.precision)]
+        traffic = per_cell * cells
     total_phase = sum(phases.values()) or 1.0
 
     # e2e: host-resident initial state, per-step marker readback
@@ -318,7 +386,8 @@ def run_product(args, world, rank, local, pg):
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind,
                      "share_of_step": phases["lattice"] / total_phase,
-                     "algorithmic_bytes_per_launch": alg_bytes, "traffic": None},
+                     "algorithmic_bytes_per_launch": alg_bytes,
+                     "traffic": traffic, "traffic_source": traffic_src},
         "e2e": e2e,
         "clocks": clk,
     }
