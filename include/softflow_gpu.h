@@ -279,6 +279,63 @@ int sfg_autotune(sfg_context* ctx, int steps_per_trial, int* steps_run);
 int sfg_get_launch_config(sfg_context* ctx, int* lattice_ctas_per_sm, int* spread_ctas_per_sm,
                           int* marker_block, int* learned_ctas_per_sm);
 
+/* ---- thermo: device-side reductions of the state -------------------------
+ * One record per channel, reduced on the device over the state after the
+ * last step.  Cell sums run in a fixed tree order (run-to-run identical;
+ * they differ from the reference's row-major serial sums by rounding only);
+ * minima, maxima, counts and the capsule sums are exact. */
+typedef struct sfg_thermo_record {
+    /* sqrt(max |u|^2) over non-SOLID cells: Simulation::getMaxSpeed
+     * (simulation.cpp:892-907), the thermo line's u_max (setup.py:1969) */
+    double max_speed;
+    /* over non-SOLID cells, as GlobalStatsWriter::writeTimestep
+     * (global_stats_writer.cpp:52-81): mean rho, mean |u|, sum 0.5 rho |u|^2,
+     * smallest and largest rho */
+    double mean_rho, mean_velocity, kinetic_energy, min_rho, max_rho;
+    /* sum of the concentration over all cells (0 without the scalar):
+     * total_dissolved_mass (global_stats_writer.cpp:92-103) */
+    double total_scalar;
+    /* Taylor deformation over the channel's capsules, summed in capsule
+     * order (global_stats_writer.cpp:84-90); 0 without capsules */
+    double mean_deformation, max_deformation;
+    long long fluid_cells;      /* non-SOLID cells */
+    /* y * nx + x of the first cell in row-major order whose rho or u is not
+     * finite (Simulation::checkStability, simulation.cpp:818-845), or -1 */
+    long long first_nonfinite;
+    long long capped_nodes;     /* as sfg_get_capped_count */
+    int num_capsules;
+    int reserved;
+} sfg_thermo_record;
+
+/* Geometry of one capsule (FP64, the reference's evaluation order):
+ * Capsule::centroid, area, perimeter, deformationIndex, inclinationAngle
+ * (capsule.cpp:159-266). */
+typedef struct sfg_capsule_stats {
+    double cx, cy, area, perimeter, deformation, inclination;
+} sfg_capsule_stats;
+
+/* Thermo of every channel (chans [num_channels], may be NULL) and the
+ * geometry of every capsule (caps [total capsules, channel-major], may be
+ * NULL), synchronous.  Runs a pending scalar step first, as every host read
+ * of the scalar does. */
+int sfg_thermo(sfg_context* ctx, sfg_thermo_record* chans, sfg_capsule_stats* caps);
+
+/* Called by sfg_run after every thermo interval with the records of
+ * sfg_thermo; a nonzero return stops the run after that interval. */
+typedef int (*sfg_thermo_fn)(long long step, const sfg_thermo_record* chans, int num_channels,
+                             const sfg_capsule_stats* caps, int num_capsules, void* user);
+
+/* Runs nsteps steps in one call: the multi-step loop of Simulation::run
+ * (simulation.cpp:788-800) and of the Python driver's run loop
+ * (setup.py:1957-1969), with the per-interval thermo (max speed, capsule
+ * deformation) reduced on the device.  Every thermo_every steps and after
+ * the last step (thermo_every <= 0: only after the last step) the records are
+ * copied to the host and passed to cb (may be NULL).  *steps_done (may be
+ * NULL) receives the steps run, fewer than nsteps when cb stopped the run.
+ * Returns after the last interval has finished on the device. */
+int sfg_run(sfg_context* ctx, int nsteps, int thermo_every, sfg_thermo_fn cb, void* user,
+            int* steps_done);
+
 /* ---- diagnostics ---------------------------------------------------------- */
 int sfg_num_channels(const sfg_context* ctx, int* n);
 int sfg_channel_counts(const sfg_context* ctx, int channel, int* num_capsules, int* num_markers);

@@ -150,6 +150,8 @@ def _load(path: str, prefix: str):
         "last_capped": (C.c_int, [C.c_void_p]),
         "capsule_area": (C.c_double, [C.c_void_p, C.c_int]),
         "capsule_perimeter": (C.c_double, [C.c_void_p, C.c_int]),
+        "capsule_deformation": (C.c_double, [C.c_void_p, C.c_int]),
+        "capsule_inclination": (C.c_double, [C.c_void_p, C.c_int]),
         "capsule_centroid": (None, [C.c_void_p, C.c_int, d, d]),
         "set_concentration": (None, [C.c_void_p, d]),
         "phi": (C.c_double, [C.c_double]),
@@ -297,6 +299,12 @@ class OracleSim:
 
     def capsule_perimeter(self, c):
         return self._fn["capsule_perimeter"](self._h, c)
+
+    def capsule_deformation(self, c):
+        return self._fn["capsule_deformation"](self._h, c)
+
+    def capsule_inclination(self, c):
+        return self._fn["capsule_inclination"](self._h, c)
 
     def capsule_centroid(self, c):
         x, y = C.c_double(), C.c_double()

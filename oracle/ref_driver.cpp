@@ -277,6 +277,8 @@ double* sfr_g(void* h) {
 int sfr_last_capped(void* h) { return static_cast<RefSim*>(h)->last_capped; }
 double sfr_capsule_area(void* h, int c) { return static_cast<RefSim*>(h)->caps[c].area(); }
 double sfr_capsule_perimeter(void* h, int c) { return static_cast<RefSim*>(h)->caps[c].perimeter(); }
+double sfr_capsule_deformation(void* h, int c) { return static_cast<RefSim*>(h)->caps[c].deformationIndex(); }
+double sfr_capsule_inclination(void* h, int c) { return static_cast<RefSim*>(h)->caps[c].inclinationAngle(); }
 void sfr_capsule_centroid(void* h, int c, double* x, double* y) {
     Vec2d r = static_cast<RefSim*>(h)->caps[c].centroid();
     *x = r.x;

@@ -478,6 +478,64 @@ static v2 cap_centroid(const sfo_sim* s, const capsule_t* c) {
     return vdiv(cc, (double)c->n);
 }
 
+/* reference capsule.cpp:209-247: central second moments of area of the
+ * polygon on nodes unwrapped across the periodic x boundary */
+static void cap_moments(const sfo_sim* s, const capsule_t* c, double* mxx, double* myy,
+                        double* mxy) {
+    const int n = c->n;
+    v2* p = (v2*)malloc(sizeof(v2) * (n > 0 ? n : 1));
+    p[0] = NODE(c, 0);
+    for (int i = 1; i < n; ++i) p[i] = vadd(p[i - 1], min_image(c, NODE(c, i), NODE(c, i - 1)));
+    double A = 0.0, cx = 0.0, cy = 0.0;
+    for (int i = 0; i < n; ++i) {
+        v2 a = p[i], b = p[(i + 1) % n];
+        double cr = a.x * b.y - b.x * a.y;
+        A += cr;
+        cx += (a.x + b.x) * cr;
+        cy += (a.y + b.y) * cr;
+    }
+    A *= 0.5;
+    *mxx = *myy = *mxy = 0.0;
+    if (fabs(A) < 1e-15) { free(p); return; }
+    cx /= (6.0 * A);
+    cy /= (6.0 * A);
+    for (int i = 0; i < n; ++i) {
+        double x0 = p[i].x - cx, y0 = p[i].y - cy;
+        v2 q = p[(i + 1) % n];
+        double x1 = q.x - cx, y1 = q.y - cy;
+        double cr = x0 * y1 - x1 * y0;
+        *mxx += (x0 * x0 + x0 * x1 + x1 * x1) * cr;
+        *myy += (y0 * y0 + y0 * y1 + y1 * y1) * cr;
+        *mxy += (x0 * y1 + 2.0 * x0 * y0 + 2.0 * x1 * y1 + x1 * y0) * cr;
+    }
+    double sgn = (A > 0.0) ? 1.0 : -1.0;
+    *mxx *= sgn / 12.0;
+    *myy *= sgn / 12.0;
+    *mxy *= sgn / 24.0;
+    free(p);
+}
+
+/* reference capsule.cpp:249-258 (Taylor deformation of the equivalent ellipse) */
+static double cap_deformation(const sfo_sim* s, const capsule_t* c) {
+    if (c->n < 3) return 0.0;
+    double mxx, myy, mxy;
+    cap_moments(s, c, &mxx, &myy, &mxy);
+    double tr = 0.5 * (mxx + myy);
+    double dd = sqrt(0.25 * (mxx - myy) * (mxx - myy) + mxy * mxy);
+    double J1 = tr + dd, t2 = tr - dd;
+    double J2 = (t2 < 0.0) ? 0.0 : t2;
+    double s1 = sqrt(J1), s2 = sqrt(J2);
+    return (s1 + s2 > 1e-15) ? (s1 - s2) / (s1 + s2) : 0.0;
+}
+
+/* reference capsule.cpp:260-266 */
+static double cap_inclination(const sfo_sim* s, const capsule_t* c) {
+    if (c->n < 3) return 0.0;
+    double mxx, myy, mxy;
+    cap_moments(s, c, &mxx, &myy, &mxy);
+    return 0.5 * atan2(2.0 * mxy, mxx - myy);
+}
+
 static void grow_markers(sfo_sim* s, int need) {
     if (need <= s->cap_M) return;
     int cap = s->cap_M ? s->cap_M : 64;
@@ -1122,6 +1180,8 @@ int sfo_has_prev(const sfo_sim* s, int c) { return s->caps[c].has_prev; }
 double sfo_capsule_area(const sfo_sim* s, int c) { return cap_area(s, &s->caps[c]); }
 double sfo_capsule_perimeter(const sfo_sim* s, int c) { return cap_perimeter(s, &s->caps[c]); }
 double sfo_capsule_rest_area(const sfo_sim* s, int c) { return s->caps[c].rest_area; }
+double sfo_capsule_deformation(const sfo_sim* s, int c) { return cap_deformation(s, &s->caps[c]); }
+double sfo_capsule_inclination(const sfo_sim* s, int c) { return cap_inclination(s, &s->caps[c]); }
 void sfo_capsule_centroid(const sfo_sim* s, int c, double* cx, double* cy) {
     v2 r = cap_centroid(s, &s->caps[c]);
     *cx = r.x; *cy = r.y;

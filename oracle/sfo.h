@@ -111,6 +111,10 @@ int sfo_has_prev(const sfo_sim* s, int capsule);
 /* Capsule geometry (reference capsule.cpp:159-204). */
 double sfo_capsule_area(const sfo_sim* s, int c);
 double sfo_capsule_perimeter(const sfo_sim* s, int c);
+/* Taylor deformation D and inclination of the equivalent ellipse
+ * (Capsule::deformationIndex / inclinationAngle, capsule.cpp:209-266). */
+double sfo_capsule_deformation(const sfo_sim* s, int c);
+double sfo_capsule_inclination(const sfo_sim* s, int c);
 void sfo_capsule_centroid(const sfo_sim* s, int c, double* cx, double* cy);
 double sfo_capsule_rest_area(const sfo_sim* s, int c);
 

@@ -52,6 +52,25 @@ class CapsuleRestC(C.Structure):
     ]
 
 
+class ThermoRecordC(C.Structure):
+    """sfg_thermo_record: per-channel reductions of the state."""
+    _fields_ = [
+        ("max_speed", C.c_double), ("mean_rho", C.c_double), ("mean_velocity", C.c_double),
+        ("kinetic_energy", C.c_double), ("min_rho", C.c_double), ("max_rho", C.c_double),
+        ("total_scalar", C.c_double), ("mean_deformation", C.c_double),
+        ("max_deformation", C.c_double), ("fluid_cells", C.c_longlong),
+        ("first_nonfinite", C.c_longlong), ("capped_nodes", C.c_longlong),
+        ("num_capsules", C.c_int), ("reserved", C.c_int),
+    ]
+
+
+# sfg_capsule_stats: six doubles per capsule
+CAPSULE_STATS_FIELDS = ("cx", "cy", "area", "perimeter", "deformation", "inclination")
+
+THERMO_FN = C.CFUNCTYPE(C.c_int, C.c_longlong, C.POINTER(ThermoRecordC), C.c_int,
+                        C.POINTER(C.c_double), C.c_int, C.c_void_p)
+
+
 class SoftFlowGpuError(RuntimeError):
     """Raised when a C-ABI call returns a nonzero status."""
 
@@ -124,6 +143,8 @@ SIGNATURES = {
     "sfg_get_mdf_stats": (C.c_int, [C.c_void_p, C.c_int, _P(C.c_float), _P(C.c_float),
                                     _P(C.c_longlong), _P(C.c_longlong)]),
     "sfg_autotune": (C.c_int, [C.c_void_p, C.c_int, _P(C.c_int)]),
+    "sfg_thermo": (C.c_int, [C.c_void_p, _P(ThermoRecordC), _D]),
+    "sfg_run": (C.c_int, [C.c_void_p, C.c_int, C.c_int, THERMO_FN, C.c_void_p, _P(C.c_int)]),
     "sfg_get_launch_config": (C.c_int, [C.c_void_p, _P(C.c_int), _P(C.c_int), _P(C.c_int),
                                         _P(C.c_int)]),
     "sfg_set_harvest": (C.c_int, [C.c_void_p, C.c_int]),

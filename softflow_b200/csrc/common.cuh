@@ -82,6 +82,35 @@ struct CapsuleDev {
     int periodic_nx;
 };
 
+// Partial thermo sums of one block of cells (see k_thermo_cells).
+constexpr int THERMO_THREADS = 256;
+struct ThermoPart {
+    double sum_rho, min_rho, max_rho, max_v2, sum_vel, ke, sum_c;
+    long long count, first_bad;
+};
+constexpr long long THERMO_NONE = 0x7fffffffffffffffLL;
+
+__device__ __forceinline__ void thermo_init(ThermoPart& p) {
+    p.sum_rho = p.sum_vel = p.ke = p.sum_c = p.max_v2 = 0.0;
+    p.min_rho = 1e30;
+    p.max_rho = -1e30;
+    p.count = 0;
+    p.first_bad = THERMO_NONE;
+}
+
+// Comparisons as the reference writes them: a NaN never replaces a value.
+__device__ __forceinline__ void thermo_merge(ThermoPart& a, const ThermoPart& b) {
+    a.sum_rho = __dadd_rn(a.sum_rho, b.sum_rho);
+    a.sum_vel = __dadd_rn(a.sum_vel, b.sum_vel);
+    a.ke = __dadd_rn(a.ke, b.ke);
+    a.sum_c = __dadd_rn(a.sum_c, b.sum_c);
+    if (b.min_rho < a.min_rho) a.min_rho = b.min_rho;
+    if (b.max_rho > a.max_rho) a.max_rho = b.max_rho;
+    if (b.max_v2 > a.max_v2) a.max_v2 = b.max_v2;
+    a.count += b.count;
+    if (b.first_bad < a.first_bad) a.first_bad = b.first_bad;
+}
+
 // Work item of the lattice kernels: one row segment of one channel.
 struct RowItem {
     int chan, y, x0, len;

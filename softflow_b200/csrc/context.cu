@@ -198,6 +198,13 @@ struct sfg_context {
     int* d_plain_needed = nullptr;      // [1] see TileBufs::plain_needed
     float* d_feat = nullptr;            // [M][8] network inputs of the step
     double2* d_frame = nullptr;         // [M] local tangent of each marker
+    // thermo reductions (allocated on first use)
+    ThermoPart* d_thermo_parts = nullptr;  // [nch][thermo_bpc]
+    int thermo_bpc = 0;                    // blocks per channel (from the largest channel)
+    double* d_cap_stats = nullptr;         // [NC][6]
+    sfg_thermo_record* d_thermo = nullptr;        // [nch]
+    sfg_thermo_record* h_thermo = nullptr;        // pinned [nch]
+    double* h_cap_stats = nullptr;         // pinned [NC][6]
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int launches = 0;
     // per-phase timing (profiling mode runs the step eagerly)
@@ -280,6 +287,11 @@ static void free_all(sfg_context* c) {
     F(c->d_phi); F(c->d_stepped); F(c->d_adr_pending); F(c->d_c_fresh); F(c->d_status);
     F(c->d_step_ctr);
     F(c->d_io);
+    F(c->d_thermo_parts); F(c->d_cap_stats); F(c->d_thermo);
+    if (c->h_thermo) cudaFreeHost(c->h_thermo);
+    if (c->h_cap_stats) cudaFreeHost(c->h_cap_stats);
+    c->d_thermo_parts = nullptr; c->d_cap_stats = nullptr; c->d_thermo = nullptr;
+    c->h_thermo = nullptr; c->h_cap_stats = nullptr;
 }
 
 extern "C" int sfg_destroy(sfg_context* c) {
@@ -1239,6 +1251,144 @@ extern "C" int sfg_get_concentration(sfg_context* c, int chi, double* C, double*
     if (C) CU(cudaMemcpyAsync(C, o, N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if (g) CU(cudaMemcpyAsync(g, o + N, 9 * N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CU(cudaStreamSynchronize(c->stream));
+    return SFG_OK;
+}
+
+// ------------------------------------------------------------------------
+// thermo: device-side reductions and the multi-step run
+// ------------------------------------------------------------------------
+// One thread per channel: combines the channel's block partials in block
+// order, sums the capsule deformations in capsule order
+// (global_stats_writer.cpp:84-90) and counts the capped cells as
+// sfg_get_capped_count does.
+__global__ void k_thermo_final(const ChannelDev* __restrict__ chans, int nch, int bpc,
+                               const ThermoPart* __restrict__ parts,
+                               const double* __restrict__ cap_stats, const int* __restrict__ capped,
+                               const int* __restrict__ fluid_touched, int stepped,
+                               sfg_thermo_record* __restrict__ out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nch) return;
+    const ChannelDev& ch = chans[c];
+    ThermoPart p;
+    thermo_init(p);
+    for (int b = 0; b < bpc; ++b) thermo_merge(p, parts[(long long)c * bpc + b]);
+    sfg_thermo_record t;
+    const double n = (double)p.count;
+    t.max_speed = __dsqrt_rn(p.max_v2);
+    t.mean_rho = p.count > 0 ? __ddiv_rn(p.sum_rho, n) : 0.0;
+    t.mean_velocity = p.count > 0 ? __ddiv_rn(p.sum_vel, n) : 0.0;
+    t.kinetic_energy = p.ke;
+    t.min_rho = p.min_rho;
+    t.max_rho = p.max_rho;
+    t.total_scalar = p.sum_c;
+    t.fluid_cells = p.count;
+    t.first_nonfinite = p.first_bad == THERMO_NONE ? -1 : p.first_bad;
+    const int nc = ch.cap_end - ch.cap_begin;
+    double mean_def = 0.0, max_def = 0.0;
+    for (int k = ch.cap_begin; k < ch.cap_end; ++k) {
+        const double D = cap_stats[6LL * k + 4];
+        mean_def = __dadd_rn(mean_def, D);
+        if (D > max_def) max_def = D;
+    }
+    if (nc > 0) mean_def = __ddiv_rn(mean_def, (double)nc);
+    t.mean_deformation = mean_def;
+    t.max_deformation = max_def;
+    t.num_capsules = nc;
+    t.reserved = 0;
+    long long cap_n = 0;
+    if (stepped && capped != nullptr) {
+        cap_n = capped[c];
+        const double bx = 0.0 + ch.body_fx, by = 0.0 + ch.body_fy, Fm = ch.max_force;
+        if (__dadd_rn(__dmul_rn(bx, bx), __dmul_rn(by, by)) > __dmul_rn(Fm, Fm))
+            cap_n += p.count - fluid_touched[c];
+    }
+    t.capped_nodes = cap_n;
+    out[c] = t;
+}
+
+// Enqueues the thermo reductions of the current state on the context stream
+// and the copies of their results into the pinned host records.
+static int enqueue_thermo(sfg_context* c) {
+    const int nch = (int)c->ch.size();
+    if (!c->d_thermo) {
+        long long maxN = 1;
+        for (const ChanHost& h : c->ch) maxN = std::max(maxN, (long long)h.d.nx * h.d.ny);
+        // about 16 cells per thread on the largest channel, at most 512 blocks
+        c->thermo_bpc = (int)std::min<long long>(512, std::max<long long>(1, (maxN + 4095) / 4096));
+        CU(cudaMalloc(&c->d_thermo_parts, sizeof(ThermoPart) * (size_t)nch * c->thermo_bpc));
+        CU(cudaMalloc(&c->d_thermo, sizeof(sfg_thermo_record) * nch));
+        CU(cudaMallocHost(&c->h_thermo, sizeof(sfg_thermo_record) * nch));
+        if (c->NC > 0) {
+            CU(cudaMalloc(&c->d_cap_stats, sizeof(double) * 6 * c->NC));
+            CU(cudaMallocHost(&c->h_cap_stats, sizeof(double) * 6 * c->NC));
+        }
+    }
+    int rc = flush_scalar(c);
+    if (rc) return rc;
+    const int p = (int)(c->steps & 1);
+    const TileViewArgs tv = last_view(c);
+    const int stepped = c->steps > 0;
+    const void* g = c->any_adr ? c->g[c->g_cur] : nullptr;
+    if (c->precision == SFG_FP64)
+        launch_thermo_cells<double, double>(c->f[p], g, c->d_chans, nch, c->thermo_bpc, tv, stepped, c->d_thermo_parts, c->stream);
+    else if (c->precision == SFG_FP32)
+        launch_thermo_cells<float, float>(c->f[p], g, c->d_chans, nch, c->thermo_bpc, tv, stepped, c->d_thermo_parts, c->stream);
+    else
+        launch_thermo_cells<__half, float>(c->f[p], g, c->d_chans, nch, c->thermo_bpc, tv, stepped, c->d_thermo_parts, c->stream);
+    if (c->NC > 0) launch_capsule_stats(c->d_caps, c->NC, c->mb.pos, c->d_cap_stats, c->stream);
+    k_thermo_final<<<(nch + 127) / 128, 128, 0, c->stream>>>(
+        c->d_chans, nch, c->thermo_bpc, c->d_thermo_parts, c->d_cap_stats, c->tb.capped,
+        c->tb.fluid_touched, stepped, c->d_thermo);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(c->h_thermo, c->d_thermo, sizeof(sfg_thermo_record) * nch, cudaMemcpyDeviceToHost,
+                       c->stream));
+    if (c->NC > 0)
+        CU(cudaMemcpyAsync(c->h_cap_stats, c->d_cap_stats, sizeof(double) * 6 * c->NC,
+                           cudaMemcpyDeviceToHost, c->stream));
+    return SFG_OK;
+}
+
+extern "C" int sfg_thermo(sfg_context* c, sfg_thermo_record* chans, sfg_capsule_stats* caps) {
+    if (!c) return fail(SFG_ERR_ARG, "sfg_thermo: null context");
+    if (!c->initialized) return fail(SFG_ERR_STATE, "sfg_thermo: context not initialized");
+    CU(cudaSetDevice(c->device));
+    int rc = enqueue_thermo(c);
+    if (rc) return rc;
+    if ((rc = sfg_synchronize(c, nullptr))) return rc;
+    const int nch = (int)c->ch.size();
+    if (chans) std::memcpy(chans, c->h_thermo, sizeof(sfg_thermo_record) * nch);
+    if (caps && c->NC > 0) std::memcpy(caps, c->h_cap_stats, sizeof(double) * 6 * c->NC);
+    return SFG_OK;
+}
+
+extern "C" int sfg_run(sfg_context* c, int nsteps, int thermo_every, sfg_thermo_fn cb, void* user,
+                       int* steps_done) {
+    if (steps_done) *steps_done = 0;
+    if (!c) return fail(SFG_ERR_ARG, "sfg_run: null context");
+    if (!c->initialized) return fail(SFG_ERR_STATE, "sfg_run: context not initialized");
+    if (nsteps < 0) return fail(SFG_ERR_ARG, "sfg_run: negative step count");
+    CU(cudaSetDevice(c->device));
+    int rc;
+    if (cb == nullptr) {
+        if ((rc = sfg_step(c, nsteps))) return rc;
+        if ((rc = sfg_synchronize(c, nullptr))) return rc;
+        if (steps_done) *steps_done = nsteps;
+        return SFG_OK;
+    }
+    const int every = thermo_every > 0 ? thermo_every : std::max(nsteps, 1);
+    const int nch = (int)c->ch.size();
+    int done = 0;
+    while (done < nsteps) {
+        const int n = std::min(every, nsteps - done);
+        if ((rc = sfg_step(c, n))) return rc;
+        done += n;
+        if (steps_done) *steps_done = done;
+        if ((rc = enqueue_thermo(c))) return rc;
+        if ((rc = sfg_synchronize(c, nullptr))) return rc;
+        if (cb(c->steps, c->h_thermo, nch, reinterpret_cast<const sfg_capsule_stats*>(c->h_cap_stats),
+               c->NC, user) != 0)
+            break;
+    }
     return SFG_OK;
 }
 

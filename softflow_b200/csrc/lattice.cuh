@@ -762,9 +762,50 @@ __global__ void k_pop_export(const S* __restrict__ in, double* __restrict__ out,
     }
 }
 
-// Macroscopic fields of the current state with the force of the last step
-// (reference LatticeField::computeMacroscopic, lattice_field.cpp:28-73).
-// Also exports that force field.
+// Macroscopic state of cell (x, y): rho and u of the current populations with
+// the force of the last step, as the reference's LatticeField::
+// computeMacroscopic leaves them (lattice_field.cpp:28-73; rho = u = 0 on
+// SOLID cells), and that force.  Returns whether the cell is SOLID.
+template <typename S, typename R>
+__device__ __forceinline__ bool cell_macro(const S* __restrict__ in, const ChannelDev& ch,
+                                           const TileView& tv_last, int stepped, int x, int y,
+                                           R& rho, R& ux, R& uy, R& Fx, R& Fy) {
+    const bool solid = !ch.periodic_y && (y == 0 || y == ch.ny - 1);
+    // last step's force (the "cur" tile set of that step)
+    if (!stepped) {
+        Fx = R(0);
+        Fy = R(0);
+    } else {
+        CellForces<R> cf = cell_forces<R>(ch, x, y, tv_last, 1);
+        Fx = cf.Fx;
+        Fy = cf.Fy;
+        if (solid) {
+            bool touched = false;
+            if (ch.cap_end > ch.cap_begin && tv_last.cur_slot != nullptr) {
+                const int t = ch.tile_base + (y / TILE_H) * ch.tiles_x + (x / TILE_W);
+                touched = tv_last.cur_slot[t] >= 0;
+            }
+            if (!touched) {
+                Fx = R(0);
+                Fy = R(0);
+            }
+        }
+    }
+    if (solid) {
+        rho = ux = uy = R(0);
+        return true;
+    }
+    R f[9];
+    const long long n = (long long)y * ch.pitch + x;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) f[q] = PopIO<S, R>::ld(in + ch.f_off + q * ch.plane + n, q);
+    R jx, jy;
+    lattice_moments(f, rho, jx, jy);
+    cell_velocity(rho, jx, jy, Fx, Fy, ux, uy);
+    return false;
+}
+
+// Macroscopic fields and the last step's force field of one channel.
 template <typename S, typename R>
 __global__ void k_macro_export(const S* __restrict__ in, ChannelDev ch, TileView tv_last,
                                int stepped, double* __restrict__ rho_o, double* __restrict__ ux_o,
@@ -774,49 +815,72 @@ __global__ void k_macro_export(const S* __restrict__ in, ChannelDev ch, TileView
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
          i += (long long)gridDim.x * blockDim.x) {
         const int y = (int)(i / ch.nx), x = (int)(i % ch.nx);
-        const bool solid = !ch.periodic_y && (y == 0 || y == ch.ny - 1);
-        // last step's force (the "cur" tile set of that step)
-        R Fx, Fy;
-        if (!stepped) {
-            Fx = R(0);
-            Fy = R(0);
-        } else {
-            CellForces<R> cf = cell_forces<R>(ch, x, y, tv_last, 1);
-            Fx = cf.Fx;
-            Fy = cf.Fy;
-            if (solid) {
-                bool touched = false;
-                if (ch.cap_end > ch.cap_begin && tv_last.cur_slot != nullptr) {
-                    const int t = ch.tile_base + (y / TILE_H) * ch.tiles_x + (x / TILE_W);
-                    touched = tv_last.cur_slot[t] >= 0;
-                }
-                if (!touched) {
-                    Fx = R(0);
-                    Fy = R(0);
-                }
-            }
-        }
+        R rho, ux, uy, Fx, Fy;
+        cell_macro<S, R>(in, ch, tv_last, stepped, x, y, rho, ux, uy, Fx, Fy);
         if (Fx_o) {
             Fx_o[i] = (double)Fx;
             Fy_o[i] = (double)Fy;
         }
-        if (solid) {
-            rho_o[i] = 0.0;
-            ux_o[i] = 0.0;
-            uy_o[i] = 0.0;
-            continue;
-        }
-        R f[9];
-        const long long n = (long long)y * ch.pitch + x;
-#pragma unroll
-        for (int q = 0; q < 9; ++q) f[q] = PopIO<S, R>::ld(in + ch.f_off + q * ch.plane + n, q);
-        R rho, jx, jy, ux, uy;
-        lattice_moments(f, rho, jx, jy);
-        cell_velocity(rho, jx, jy, Fx, Fy, ux, uy);
         rho_o[i] = (double)rho;
         ux_o[i] = (double)ux;
         uy_o[i] = (double)uy;
     }
+}
+
+// ---------------- thermo reductions over the cells --------------------------
+// Partial sums of one block (GlobalStatsWriter::writeTimestep,
+// global_stats_writer.cpp:52-81, and Simulation::getMaxSpeed /
+// checkStability, simulation.cpp:818-907, over non-SOLID cells).  The double
+// products and sums use explicit round-to-nearest intrinsics, so no FMA
+// contraction changes them in either translation unit; rho and u are those
+// of k_macro_export to the bit.
+
+// Grid (blocks per channel, channels).  Thread t of block b visits cells
+// b * 256 + t + k * (256 * blocks per channel) in order; the block's
+// partials are combined in a fixed tree, so the result depends only on the
+// channel sizes.  parts[channel * gridDim.x + b].
+template <typename S, typename R>
+__global__ void __launch_bounds__(THERMO_THREADS)
+k_thermo_cells(const S* __restrict__ in, const R* __restrict__ g, const ChannelDev* __restrict__ chans,
+               TileView tv_last, int stepped, ThermoPart* __restrict__ parts) {
+    __shared__ ThermoPart sp[THERMO_THREADS];
+    const ChannelDev& ch = chans[blockIdx.y];
+    ThermoPart p;
+    thermo_init(p);
+    const long long N = (long long)ch.nx * ch.ny;
+    for (long long i = blockIdx.x * (long long)THERMO_THREADS + threadIdx.x; i < N;
+         i += (long long)gridDim.x * THERMO_THREADS) {
+        const int y = (int)(i / ch.nx), x = (int)(i % ch.nx);
+        R rho, ux, uy, Fx, Fy;
+        if (!cell_macro<S, R>(in, ch, tv_last, stepped, x, y, rho, ux, uy, Fx, Fy)) {
+            const double r = (double)rho, vx = (double)ux, vy = (double)uy;
+            if (isnan(r) || isinf(r) || isnan(vx) || isinf(vx) || isnan(vy) || isinf(vy))
+                if (i < p.first_bad) p.first_bad = i;
+            const double v2 = __dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy));
+            p.sum_rho = __dadd_rn(p.sum_rho, r);
+            if (r < p.min_rho) p.min_rho = r;
+            if (r > p.max_rho) p.max_rho = r;
+            if (v2 > p.max_v2) p.max_v2 = v2;
+            p.sum_vel = __dadd_rn(p.sum_vel, __dsqrt_rn(v2));
+            p.ke = __dadd_rn(p.ke, __dmul_rn(__dmul_rn(0.5, r), v2));
+            ++p.count;
+        }
+        if (g != nullptr && ch.adr) {
+            const long long n = (long long)y * ch.pitch + x;
+            R v[9];
+#pragma unroll
+            for (int q = 0; q < 9; ++q) v[q] = g[ch.g_off + q * ch.plane + n];
+            const R c = v[0] + v[1] + v[2] + v[3] + v[4] + v[5] + v[6] + v[7] + v[8];
+            p.sum_c = __dadd_rn(p.sum_c, (double)c);
+        }
+    }
+    sp[threadIdx.x] = p;
+    __syncthreads();
+    for (int s = THERMO_THREADS / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) thermo_merge(sp[threadIdx.x], sp[threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) parts[(long long)blockIdx.y * gridDim.x + blockIdx.x] = sp[0];
 }
 
 }  // namespace sfg

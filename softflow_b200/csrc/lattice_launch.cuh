@@ -99,6 +99,15 @@ void launch_macro_export(const void* in, const ChannelDev& ch, const TileViewArg
 }
 
 template <typename S, typename R>
+void launch_thermo_cells(const void* in, const void* g, const ChannelDev* chans, int nch,
+                         int blocks_per_chan, const TileViewArgs& tv_last, int stepped,
+                         ThermoPart* parts, cudaStream_t st) {
+    k_thermo_cells<S, R><<<dim3(blocks_per_chan, nch), THERMO_THREADS, 0, st>>>(
+        static_cast<const S*>(in), static_cast<const R*>(g), chans, to_view(tv_last), stepped,
+        parts);
+}
+
+template <typename S, typename R>
 int lattice_ctas_per_sm_t(bool adr) {
     // the generic-collision instance has the largest footprint
     int n = 0;
@@ -121,6 +130,8 @@ int lattice_ctas_per_sm_t(bool adr) {
     template void launch_pop_export<S, R>(const void*, double*, const ChannelDev&, cudaStream_t); \
     template void launch_macro_export<S, R>(const void*, const ChannelDev&, const TileViewArgs&,  \
                                             int, double*, double*, double*, double*, double*,     \
-                                            cudaStream_t);
+                                            cudaStream_t);                                        \
+    template void launch_thermo_cells<S, R>(const void*, const void*, const ChannelDev*, int, int, \
+                                            const TileViewArgs&, int, ThermoPart*, cudaStream_t);
 
 }  // namespace sfg

@@ -999,6 +999,126 @@ cudaError_t prepare_spread() {
     return e;
 }
 
+// ---------------- capsule geometry (thermo) ---------------------------------
+// One thread per capsule, FP64 in the reference's serial order:
+// Capsule::centroid, area, perimeter, secondMoments, deformationIndex and
+// inclinationAngle (capsule.cpp:159-266).  Unwrapped nodes are regenerated
+// on the fly (p_0 = X_0, p_i = p_{i-1} + minImage(X_i - X_{i-1})).
+__device__ __forceinline__ double2 unwrap_next(const double2* X, int i, double2 p, double Lx) {
+    const double2 d = min_image_d(X[i], X[i - 1], Lx);
+    return make_double2(p.x + d.x, p.y + d.y);
+}
+
+__device__ void capsule_moments(const double2* X, int n, double Lx, double& mxx, double& myy,
+                                double& mxy) {
+    // capsule.cpp:209-247
+    double A = 0.0, cx = 0.0, cy = 0.0;
+    double2 a = X[0];
+    const double2 p0 = a;
+    for (int i = 0; i < n; ++i) {
+        const double2 b = (i + 1 < n) ? unwrap_next(X, i + 1, a, Lx) : p0;
+        const double cr = a.x * b.y - b.x * a.y;
+        A += cr;
+        cx += (a.x + b.x) * cr;
+        cy += (a.y + b.y) * cr;
+        a = b;
+    }
+    A *= 0.5;
+    mxx = myy = mxy = 0.0;
+    if (fabs(A) < 1e-15) return;
+    cx /= (6.0 * A);
+    cy /= (6.0 * A);
+    a = p0;
+    for (int i = 0; i < n; ++i) {
+        const double2 q = (i + 1 < n) ? unwrap_next(X, i + 1, a, Lx) : p0;
+        const double x0 = a.x - cx, y0 = a.y - cy;
+        const double x1 = q.x - cx, y1 = q.y - cy;
+        const double cr = x0 * y1 - x1 * y0;
+        mxx += (x0 * x0 + x0 * x1 + x1 * x1) * cr;
+        myy += (y0 * y0 + y0 * y1 + y1 * y1) * cr;
+        mxy += (x0 * y1 + 2.0 * x0 * y0 + 2.0 * x1 * y1 + x1 * y0) * cr;
+        a = q;
+    }
+    const double sgn = (A > 0.0) ? 1.0 : -1.0;
+    mxx *= sgn / 12.0;
+    myy *= sgn / 12.0;
+    mxy *= sgn / 24.0;
+}
+
+__global__ void k_capsule_stats(const CapsuleDev* __restrict__ caps, int ncaps,
+                                const double2* __restrict__ pos, double* __restrict__ out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncaps) return;
+    const CapsuleDev cd = caps[c];
+    const double2* X = pos + cd.off;
+    const int n = cd.n;
+    const double Lx = (double)cd.periodic_nx;
+    double* o = out + 6LL * c;
+    // centroid (capsule.cpp:159-172)
+    double2 cen = make_double2(0.0, 0.0);
+    if (cd.periodic_nx > 0 && n > 0) {
+        const double2 ref = X[0];
+        double2 sum = ref;
+        for (int i = 1; i < n; ++i) {
+            const double2 d = min_image_d(X[i], ref, Lx);
+            sum.x += ref.x + d.x;
+            sum.y += ref.y + d.y;
+        }
+        cen = make_double2(sum.x / (double)n, sum.y / (double)n);
+    } else if (n > 0) {
+        for (int i = 0; i < n; ++i) {
+            cen.x += X[i].x;
+            cen.y += X[i].y;
+        }
+        cen = make_double2(cen.x / (double)n, cen.y / (double)n);
+    }
+    // area (capsule.cpp:174-195)
+    double A = 0.0;
+    if (cd.periodic_nx > 0 && n > 0) {
+        double2 a = X[0];
+        const double2 p0 = a;
+        for (int i = 0; i < n; ++i) {
+            const double2 b = (i + 1 < n) ? unwrap_next(X, i + 1, a, Lx) : p0;
+            A += a.x * b.y - a.y * b.x;
+            a = b;
+        }
+    } else {
+        for (int i = 0; i < n; ++i) {
+            const double2 a = X[i], b = X[(i + 1) % n];
+            A += a.x * b.y - a.y * b.x;
+        }
+    }
+    // perimeter (capsule.cpp:197-204)
+    double P = 0.0;
+    for (int i = 0; i < n; ++i) P += norm_d(min_image_d(X[(i + 1) % n], X[i], Lx));
+    // deformation index and inclination (capsule.cpp:249-266)
+    double D = 0.0, th = 0.0;
+    if (n >= 3) {
+        double mxx, myy, mxy;
+        capsule_moments(X, n, Lx, mxx, myy, mxy);
+        const double tr = 0.5 * (mxx + myy);
+        const double dd = sqrt(0.25 * (mxx - myy) * (mxx - myy) + mxy * mxy);
+        const double J1 = tr + dd;
+        const double t2 = tr - dd;
+        const double J2 = (t2 < 0.0) ? 0.0 : t2;
+        const double s1 = sqrt(J1), s2 = sqrt(J2);
+        D = (s1 + s2 > 1e-15) ? (s1 - s2) / (s1 + s2) : 0.0;
+        th = 0.5 * atan2(2.0 * mxy, mxx - myy);
+    }
+    o[0] = cen.x;
+    o[1] = cen.y;
+    o[2] = 0.5 * fabs(A);
+    o[3] = P;
+    o[4] = D;
+    o[5] = th;
+}
+
+void launch_capsule_stats(const CapsuleDev* caps, int ncaps, const double2* pos, double* out,
+                          cudaStream_t st) {
+    if (ncaps == 0) return;
+    k_capsule_stats<<<(ncaps + 127) / 128, 128, 0, st>>>(caps, ncaps, pos, out);
+}
+
 cudaError_t prepare_membrane(int maxn) {
     const size_t smem = membrane_smem_bytes(maxn);
     if (smem <= 48 * 1024) return cudaSuccess;

@@ -149,5 +149,14 @@ template <typename S, typename R>
 void launch_macro_export(const void* in, const ChannelDev& ch, const TileViewArgs& tv_last,
                          int stepped, double* rho, double* ux, double* uy, double* Fx, double* Fy,
                          cudaStream_t st);
+// Per-block partial thermo sums of every channel (parts [nch][blocks_per_chan]).
+template <typename S, typename R>
+void launch_thermo_cells(const void* in, const void* g, const ChannelDev* chans, int nch,
+                         int blocks_per_chan, const TileViewArgs& tv_last, int stepped,
+                         ThermoPart* parts, cudaStream_t st);
+// Geometry of every capsule: out [ncaps][6] = centroid x, y, area, perimeter,
+// deformation, inclination.
+void launch_capsule_stats(const CapsuleDev* caps, int ncaps, const double2* pos, double* out,
+                          cudaStream_t st);
 
 }  // namespace sfg

@@ -24,6 +24,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 import math
+import sys
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence
 
@@ -146,6 +147,11 @@ class SimulationParams:
     membrane: MembraneParams = field(default_factory=MembraneParams)
     repulsion: RepulsionParams = field(default_factory=RepulsionParams)
     scalar: ScalarParams = field(default_factory=ScalarParams)
+    # stability monitoring (parameters.h:315-319)
+    enable_stability_checks: bool = True
+    max_density_deviation: float = 0.1
+    max_velocity: float = 0.1
+    stability_check_interval: int = 1000
     precision: str = "fp32"
     device: int = 0
 
@@ -272,6 +278,10 @@ class _Context:
         lib = L.lib()
         self._lib = lib
         self.precision = precision
+        self.num_channels = len(channels)
+        self.num_capsules = sum(len(ch.caps) for ch in channels)
+        self._version = 0
+        self._thermo_cache = None
         h = C.c_void_p()
         L.check(lib.sfg_create(int(device), L.PRECISIONS[precision], C.byref(h)))
         self._h = h
@@ -304,6 +314,49 @@ class _Context:
 
     def step(self, n: int):
         L.check(self._lib.sfg_step(self._h, int(n)))
+        self.touch()
+
+    def touch(self):
+        """Marks the device state as changed (drops cached reductions)."""
+        self._version += 1
+        self._thermo_cache = None
+
+    def thermo(self):
+        """Device-side reductions of the current state (sfg_thermo): a list
+        of per-channel dicts and the [capsules][6] geometry array (centroid
+        x, y, area, perimeter, deformation, inclination).  Cached until the
+        state changes."""
+        if self._thermo_cache is not None:
+            return self._thermo_cache
+        recs = (L.ThermoRecordC * max(self.num_channels, 1))()
+        caps = np.zeros((max(self.num_capsules, 1), 6))
+        L.check(self._lib.sfg_thermo(self._h, recs, L.dptr(caps)))
+        out = [thermo_dict(recs[i]) for i in range(self.num_channels)]
+        self._thermo_cache = (out, caps[:self.num_capsules])
+        return self._thermo_cache
+
+    def run(self, n: int, every: int, fn) -> int:
+        """sfg_run: n steps; fn(step, records, caps) after every `every`
+        steps and after the last; a true return stops the run."""
+        def cb(step, recs, nch, caps, ncaps, user):
+            try:
+                r = [thermo_dict(recs[i]) for i in range(nch)]
+                c = (np.ctypeslib.as_array(caps, shape=(ncaps, 6)).copy() if ncaps
+                     else np.zeros((0, 6)))
+                return 1 if fn(int(step), r, c) else 0
+            except Exception as e:          # stop the run; re-raised below
+                errors.append(e)
+                return 1
+        errors = []
+        done = C.c_int(0)
+        cfn = L.THERMO_FN(cb)
+        try:
+            L.check(self._lib.sfg_run(self._h, int(n), int(every), cfn, None, C.byref(done)))
+        finally:
+            self.touch()
+        if errors:
+            raise errors[0]
+        return int(done.value)
 
     def synchronize(self) -> int:
         st = C.c_uint(0)
@@ -336,6 +389,10 @@ class _Context:
         s = C.c_void_p()
         L.check(self._lib.sfg_get_stream(self._h, C.byref(s)))
         return s.value or 0
+
+
+def thermo_dict(r) -> dict:
+    return {k: getattr(r, k) for k, _ in L.ThermoRecordC._fields_ if k != "reserved"}
 
 
 class FieldView:
@@ -391,6 +448,7 @@ class FieldView:
         if a.size != 9 * self.nx * self.ny:
             raise ValueError("populations must have 9*ny*nx entries")
         L.check(self._ctx._lib.sfg_set_populations(self._ctx._h, self._ch, L.dptr(a)))
+        self._ctx.touch()
 
     def getRho(self, x, y):
         return float(self.density()[y, x])
@@ -430,49 +488,36 @@ class CapsuleView:
     def nodeForce(self, k):
         return tuple(self._slice(self._s.forces())[k])
 
+    def _stats(self):
+        return self._s._ctx.thermo()[1][self._s._cap_base + self._i]
+
+    # Geometry reduced on the device (sfg_thermo), FP64 in the reference's
+    # serial order: Capsule::centroid, area, perimeter, deformationIndex,
+    # inclinationAngle (capsule.cpp:159-266).
     def centroid(self):
-        return _centroid_periodic(self.node_positions_array(), self._s._nx)
+        st = self._stats()
+        return (float(st[0]), float(st[1]))
 
     def area(self):
-        """|shoelace area| on min-image-unwrapped nodes (capsule.cpp:175-195)."""
-        p = self.node_positions_array()
-        Lx = float(self._s._nx)
-        uw = [(float(p[0, 0]), float(p[0, 1]))]
-        for i in range(1, len(p)):
-            dx = float(p[i, 0]) - float(p[i - 1, 0])
-            dy = float(p[i, 1]) - float(p[i - 1, 1])
-            if dx > 0.5 * Lx:
-                dx -= Lx
-            if dx < -0.5 * Lx:
-                dx += Lx
-            uw.append((uw[-1][0] + dx, uw[-1][1] + dy))
-        A = 0.0
-        for i in range(len(uw)):
-            a, b = uw[i], uw[(i + 1) % len(uw)]
-            A += a[0] * b[1] - a[1] * b[0]
-        return 0.5 * abs(A)
+        return float(self._stats()[2])
 
     def perimeter(self):
-        p = self.node_positions_array()
-        Lx = float(self._s._nx)
-        P = 0.0
-        for i in range(len(p)):
-            j = (i + 1) % len(p)
-            dx = float(p[j, 0]) - float(p[i, 0])
-            dy = float(p[j, 1]) - float(p[i, 1])
-            if dx > 0.5 * Lx:
-                dx -= Lx
-            if dx < -0.5 * Lx:
-                dx += Lx
-            P += math.sqrt(dx * dx + dy * dy)
-        return P
+        return float(self._stats()[3])
+
+    def deformationIndex(self):
+        return float(self._stats()[4])
+
+    def inclinationAngle(self):
+        return float(self._stats()[5])
 
 
 class CapsuleSystemView:
     """Marker state of one channel (reference CapsuleSystem, capsule-major)."""
 
-    def __init__(self, ctx: _Context, chan: int, recs: List[_CapsuleRec], nx: int):
+    def __init__(self, ctx: _Context, chan: int, recs: List[_CapsuleRec], nx: int,
+                 cap_base: int = 0):
         self._ctx, self._ch, self._nx = ctx, chan, nx
+        self._cap_base = cap_base
         self._counts = [r.rest.num_nodes for r in recs]
         self._types = [r.type_id for r in recs]
         self._offsets = np.concatenate([[0], np.cumsum(self._counts)]).astype(int)
@@ -512,6 +557,7 @@ class CapsuleSystemView:
         p = None if pos is None else np.ascontiguousarray(pos, dtype=np.float64).ravel()
         v = None if vel is None else np.ascontiguousarray(vel, dtype=np.float64).ravel()
         L.check(self._ctx._lib.sfg_set_markers(self._ctx._h, self._ch, L.dptr(p), L.dptr(v)))
+        self._ctx.touch()
 
     def contact_counts(self):
         c = np.zeros(max(self.M, 1), dtype=np.int32)
@@ -545,6 +591,7 @@ class ScalarView:
         if a.size != self.nx * self.ny:
             raise ValueError("concentration must have ny*nx entries")
         L.check(self._ctx._lib.sfg_set_concentration(self._ctx._h, self._ch, L.dptr(a)))
+        self._ctx.touch()
 
     def setRegion(self, x0, y0, x1, y1, concentration, species=0):
         Cf = self.concentration()
@@ -618,11 +665,41 @@ class Ensemble:
         self._need().step(1)
         self._steps += 1
 
-    def run(self, num_steps: int):
+    def run(self, num_steps: int, thermo_every: int = 0, callback=None) -> int:
+        """Advances every channel by num_steps steps in C++ (sfg_run / sfg_step
+        in CUDA graphs; no Python per step).
+
+        callback(step, records, capsule_stats) -> bool, if given, is called
+        after every thermo_every steps and after the last one with the
+        device-reduced thermo (see thermo()); a true return stops the run.
+        Without a callback, the stability check of Simulation::step
+        (simulation.cpp:729-733) runs where the reference runs it: after the
+        step whose count before the step is a multiple of
+        stability_check_interval.  Returns the steps run."""
         ctx = self._need()
-        ctx.step(num_steps)
-        self._steps += int(num_steps)
+        num_steps = int(num_steps)
+        if callback is not None:
+            done = ctx.run(num_steps, int(thermo_every), callback)
+            self._steps += done
+            return done
+        ivs = sorted({c.params.stability_check_interval for c in self._chans
+                      if c.params.enable_stability_checks and c.params.stability_check_interval > 0})
+        done = 0
+        while done < num_steps:
+            # next step (0-based count before the step) that is checked
+            s0 = self._steps
+            nxt = min((-(-s0 // iv)) * iv for iv in ivs) if ivs else None
+            n = num_steps - done if nxt is None else min(num_steps - done, nxt - s0 + 1)
+            ctx.step(n)
+            self._steps += n
+            done += n
+            if nxt is not None and self._steps - 1 == nxt:
+                for k, c in enumerate(self._chans):
+                    iv = c.params.stability_check_interval
+                    if c.params.enable_stability_checks and iv > 0 and nxt % iv == 0:
+                        self.checkStability(k, step=nxt)
         ctx.synchronize()
+        return done
 
     def synchronize(self) -> int:
         return self._need().synchronize()
@@ -638,8 +715,9 @@ class Ensemble:
         return FieldView(self._need(), chan, p.nx, p.ny)
 
     def capsules(self, chan: int = 0) -> CapsuleSystemView:
+        base = sum(len(c.caps) for c in self._chans[:chan])
         return CapsuleSystemView(self._need(), chan, self._chans[chan].caps,
-                                 self._chans[chan].params.nx)
+                                 self._chans[chan].params.nx, base)
 
     def advectionDiffusion(self, chan: int = 0) -> Optional[ScalarView]:
         p = self._chans[chan].params
@@ -652,14 +730,59 @@ class Ensemble:
         L.check(self._need()._lib.sfg_get_capped_count(self._ctx._h, chan, C.byref(v)))
         return v.value
 
+    def thermo(self, chan: Optional[int] = None):
+        """Device-side reductions of the state after the last step (one
+        launch set for every channel, sfg_thermo): max_speed, mean_rho,
+        mean_velocity, kinetic_energy, min_rho, max_rho, total_scalar,
+        mean_deformation, max_deformation, fluid_cells, first_nonfinite,
+        capped_nodes, num_capsules.  One dict for `chan`, else a list."""
+        recs = self._need().thermo()[0]
+        return recs if chan is None else recs[chan]
+
     def getMaxSpeed(self, chan: int = 0) -> float:
-        """max |u| over non-SOLID cells (simulation.cpp:892-907)."""
-        rho, ux, uy, _, _ = self.field(chan).macroscopic()
+        """max |u| over non-SOLID cells (simulation.cpp:892-907), reduced on
+        the device."""
+        return float(self.thermo(chan)["max_speed"])
+
+    def checkStability(self, chan: int = 0, step: Optional[int] = None) -> dict:
+        """Simulation::checkStability (simulation.cpp:817-889) from the
+        device reductions: warnings for a non-finite cell (the first in
+        row-major order), a density deviation above max_density_deviation
+        (the extreme rho), a speed above max_velocity, and the capped-cell
+        notice, printed to stderr as the reference does.  Returns the
+        findings."""
         p = self._chans[chan].params
-        sp = ux * ux + uy * uy
-        if not p.fluid.periodic_y:
-            sp = sp[1:-1]
-        return float(math.sqrt(float(sp.max()))) if sp.size else 0.0
+        t = self.thermo(chan)
+        step = self._steps if step is None else step
+        nx = p.nx
+        out = {"nonfinite": None, "worst_rho": None, "worst_velocity": None,
+               "capped_nodes": int(t["capped_nodes"])}
+        if t["first_nonfinite"] >= 0:
+            i = int(t["first_nonfinite"])
+            out["nonfinite"] = (i % nx, i // nx)
+            print(f"*** STABILITY WARNING: NaN/Inf detected at step {step} at "
+                  f"({i % nx},{i // nx})", file=sys.stderr)
+        rho0 = p.fluid.rho0
+        dev_lo = abs(t["min_rho"] - rho0) / rho0
+        dev_hi = abs(t["max_rho"] - rho0) / rho0
+        # the reference's scan stops at the first non-finite cell; the
+        # whole-field extremes are only reported for a finite field
+        finite = out["nonfinite"] is None
+        if finite and max(dev_lo, dev_hi) > p.max_density_deviation:
+            worst = t["min_rho"] if dev_lo > dev_hi else t["max_rho"]
+            out["worst_rho"] = worst
+            print(f"*** STABILITY WARNING: density deviation at step {step} \u2014 rho = "
+                  f"{worst:g} (rho0 = {rho0:g}, deviation = "
+                  f"{abs(worst - rho0) / rho0 * 100.0:g}%)", file=sys.stderr)
+        if finite and t["max_speed"] > p.max_velocity:
+            out["worst_velocity"] = t["max_speed"]
+            print(f"*** STABILITY WARNING: high velocity at step {step} \u2014 |u| = "
+                  f"{t['max_speed']:g} (limit = {p.max_velocity:g}, Ma = "
+                  f"{t['max_speed'] / math.sqrt(1.0 / 3.0):g})", file=sys.stderr)
+        if t["capped_nodes"] > 0:
+            print(f"*** STABILITY NOTICE: max_lattice_force cap rescaled {t['capped_nodes']} "
+                  f"fluid nodes at step {step} (cap = {p.max_lattice_force:g})", file=sys.stderr)
+        return out
 
     def context(self) -> _Context:
         return self._need()
@@ -671,6 +794,7 @@ class Ensemble:
         ctx = self._need()
         n = C.c_int()
         L.check(ctx._lib.sfg_autotune(ctx._h, int(steps_per_trial), C.byref(n)))
+        ctx.touch()
         ctx.synchronize()
         self._steps += int(n.value)
         cfg = self.launchConfig()

@@ -36,6 +36,12 @@ def main():
             out.update(f=o.f()[:, rows])
         else:
             out.update(pos=o.positions(), vel=o.velocities(), force=o.forces())
+            # Capsule::centroid / area / perimeter / deformationIndex /
+            # inclinationAngle of the reference (capsule.cpp:159-266)
+            n = o.num_capsules
+            out.update(geom=np.array([[*o.capsule_centroid(c), o.capsule_area(c),
+                                       o.capsule_perimeter(c), o.capsule_deformation(c),
+                                       o.capsule_inclination(c)] for c in range(n)]))
         if case["conc"] is not None:
             out.update(C=o.concentration())
         path = os.path.join(HERE, f"{name}.npz")

@@ -55,3 +55,45 @@ def test_peskin_table_matches_reference(oracle_mod):
         pytest.skip("reference build absent")
     for r in np.linspace(-2.5, 2.5, 1001):
         assert O.phi(float(r), "sfo") == O.phi(float(r), "ref")
+
+
+@pytest.mark.parametrize("name", [n for n in NAMES if CASES[n]["capsules"]])
+def test_oracle_capsule_geometry_matches_reference_golden(oracle_mod, name):
+    """Capsule::centroid / area / perimeter / deformationIndex /
+    inclinationAngle (capsule.cpp:159-266) of the restatement against the
+    reference's values in the fixtures, bit for bit."""
+    g = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    o = build_oracle(CASES[name])
+    o.step(int(g["steps"]))
+    geom = np.array([[*o.capsule_centroid(c), o.capsule_area(c), o.capsule_perimeter(c),
+                      o.capsule_deformation(c), o.capsule_inclination(c)]
+                     for c in range(o.num_capsules)])
+    assert np.array_equal(geom, g["geom"])
+    assert (g["geom"][:, 4] > 0).any()      # the capsules have deformed
+
+
+def test_oracle_stats_restatement():
+    """The serial reductions of oracle/stats.py on a small field with SOLID
+    rows, a NaN cell and known extremes."""
+    from oracle import stats as OS
+    ny, nx = 5, 4
+    rng = np.random.default_rng(3)
+    rho = 1.0 + 0.01 * rng.standard_normal((ny, nx))
+    ux = 0.02 * rng.standard_normal((ny, nx))
+    uy = 0.02 * rng.standard_normal((ny, nx))
+    solid = OS.solid_mask(nx, ny, False)
+    rho[solid] = ux[solid] = uy[solid] = 0.0
+    st = OS.global_stats(rho, ux, uy, solid, [0.1, 0.3])
+    f = ~solid
+    assert st["fluid_cells"] == f.sum()
+    assert st["max_velocity"] == OS.max_speed(ux, uy, solid)
+    assert np.isclose(st["max_velocity"], np.sqrt((ux[f] ** 2 + uy[f] ** 2).max()), rtol=0, atol=0)
+    assert np.isclose(st["mean_rho"], rho[f].mean(), rtol=1e-14)
+    assert st["min_rho"] == rho[f].min() and st["max_rho"] == rho[f].max()
+    assert np.isclose(st["total_kinetic_energy"], (0.5 * rho * (ux ** 2 + uy ** 2))[f].sum(),
+                      rtol=1e-14)
+    assert st["mean_deformation"] == 0.2 and st["max_deformation"] == 0.3
+    assert OS.first_nonfinite(rho, ux, uy, solid) == -1
+    ux[3, 1] = np.nan
+    ux[2, 2] = np.inf
+    assert OS.first_nonfinite(rho, ux, uy, solid) == 2 * nx + 2
