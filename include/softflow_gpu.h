@@ -166,6 +166,18 @@ int sfg_get_all_markers(sfg_context* ctx, double* pos, double* vel);
 /* Concentration field and equilibrium populations g = w C
  * (AdvectionDiffusion::setRegion semantics, advection_diffusion.cpp:59-71). */
 int sfg_set_concentration(sfg_context* ctx, int channel, const double* C);
+/* Declares, before the first step, that the populations set with
+ * sfg_set_populations are a saved state after a step: the first collision
+ * then takes the uniform (capped) body force as the previous step's force
+ * in u = (j + F/2) / rho, as the reference's restored u includes it
+ * (Checkpoint::load restores rho and u, io/checkpoint.cpp:249-255).  The
+ * previous step's spread (capsule) force is not part of a saved state and
+ * counts as zero there. */
+int sfg_mark_restored(sfg_context* ctx);
+/* Scalar state restored from a saved state: concentration C [ny][nx] and
+ * populations g [9][ny][nx] as they were (Checkpoint::load,
+ * io/checkpoint.cpp:312-330). */
+int sfg_set_scalar_state(sfg_context* ctx, int channel, const double* C, const double* g);
 /* Concentration (and, if g != NULL, the scalar populations [9][ny][nx]). */
 int sfg_get_concentration(sfg_context* ctx, int channel, double* C, double* g);
 /* Cells whose force was capped in the last step (Simulation::
@@ -336,7 +348,35 @@ typedef int (*sfg_thermo_fn)(long long step, const sfg_thermo_record* chans, int
 int sfg_run(sfg_context* ctx, int nsteps, int thermo_every, sfg_thermo_fn cb, void* user,
             int* steps_done);
 
+/* ---- output: VTK files of a channel --------------------------------------
+ * Written on the host from the device state of the last step (pulled by the
+ * call), with the file names, layout and "%.6e" formatting of the
+ * reference's VTKWriter: XML ImageData <dir>/fluid/fluid_%06d.vti and
+ * PolyData <dir>/particles/particles_%06d.vtp, or with legacy != 0 the
+ * legacy files <dir>/fluid_%06d.vtk and <dir>/particles_%06d.vtk
+ * (vtk_writer.cpp:75-209, 230-471, 549-929).  fields selects the fluid
+ * arrays (FluidOutputFields, io/output_config.h:10-21); SFG_VTK_DEFAULT is the
+ * reference's default set. */
+enum sfg_vtk_field {
+    SFG_VTK_DENSITY = 1, SFG_VTK_VELOCITY = 2, SFG_VTK_VELOCITY_MAG = 4,
+    SFG_VTK_PRESSURE = 8, SFG_VTK_VORTICITY = 16, SFG_VTK_STRAIN_RATE = 32,
+    SFG_VTK_IBM_FORCE = 64, SFG_VTK_NODE_TYPE = 128, SFG_VTK_CONCENTRATION = 256,
+    SFG_VTK_DEFAULT = 1 | 2 | 4 | 8 | 128 | 256
+};
+int sfg_write_vtk_fluid(sfg_context* ctx, int channel, const char* output_dir, int step,
+                        int legacy, unsigned fields);
+/* Capsule polygons split at the periodic seam as the reference does;
+ * type_ids [capsules of the channel] (may be NULL: type 0). */
+int sfg_write_vtk_capsules(sfg_context* ctx, int channel, const char* output_dir, int step,
+                           int legacy, const int* type_ids);
+
 /* ---- diagnostics ---------------------------------------------------------- */
+/* The parameters a channel was added with. */
+int sfg_get_channel_params(const sfg_context* ctx, int channel, sfg_channel_params* out);
+/* Nodes of each capsule of a channel (nodes [capsules of the channel]). */
+int sfg_get_capsule_nodes(const sfg_context* ctx, int channel, int* nodes);
+/* Index of the channel's first capsule in the context-wide capsule order. */
+int sfg_get_capsule_base(const sfg_context* ctx, int channel, int* first_capsule);
 int sfg_num_channels(const sfg_context* ctx, int* n);
 int sfg_channel_counts(const sfg_context* ctx, int channel, int* num_capsules, int* num_markers);
 int sfg_step_count(const sfg_context* ctx, long long* steps);

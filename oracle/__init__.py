@@ -167,6 +167,12 @@ def _load(path: str, prefix: str):
         fn.argtypes = args
         fns[name] = fn
     if prefix == "sfr_":
+        lib.sfr_write_vtk.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int]
+        lib.sfr_write_vtk.restype = None
+        lib.sfr_write_global_stats.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_double]
+        lib.sfr_write_global_stats.restype = None
+        fns["write_vtk"] = lib.sfr_write_vtk
+        fns["write_global_stats"] = lib.sfr_write_global_stats
         lib.sfr_set_threads.argtypes = [C.c_int]
         lib.sfr_set_threads.restype = None
         lib.sfr_get_threads.restype = C.c_int
@@ -310,6 +316,15 @@ class OracleSim:
         x, y = C.c_double(), C.c_double()
         self._fn["capsule_centroid"](self._h, c, C.byref(x), C.byref(y))
         return x.value, y.value
+
+    def write_vtk(self, directory: str, step: int, legacy: bool):
+        """The reference's VTKWriter on the current state (reference build
+        only)."""
+        self._fn["write_vtk"](self._h, directory.encode(), int(step), int(bool(legacy)))
+
+    def write_global_stats(self, directory: str, step: int, time: float):
+        """One row of the reference's GlobalStatsWriter (reference build only)."""
+        self._fn["write_global_stats"](self._h, directory.encode(), int(step), float(time))
 
     def _view(self, name, n):
         ptr = self._fn[name](self._h)

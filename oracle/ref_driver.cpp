@@ -18,6 +18,8 @@
 #include "coupling/immersed_boundary.h"
 #include "membrane/capsule_system.h"
 #include "membrane/repulsion.h"
+#include "io/vtk_writer.h"
+#include "io/global_stats_writer.h"
 
 #include <omp.h>
 
@@ -285,6 +287,25 @@ void sfr_capsule_centroid(void* h, int c, double* x, double* y) {
     *y = r.y;
 }
 double sfr_phi(double r) { return PeskinDelta::phi(r); }
+
+// The reference's VTK writer on the current state (default fields, periodic
+// x as Simulation's constructor sets it, simulation.cpp:177-186).
+void sfr_write_vtk(void* h, const char* dir, int step, int legacy) {
+    auto* s = static_cast<RefSim*>(h);
+    VTKWriter w(dir);
+    w.setPeriodicX(s->p.nx);
+    w.setLegacyMode(legacy != 0);
+    if (s->adr) w.setAdvectionDiffusion(s->adr.get());
+    w.writeFluidField(s->lbm->field(), step);
+    w.writeCapsules(s->caps, step);
+}
+
+// One row of the reference's global_stats.csv on the current state.
+void sfr_write_global_stats(void* h, const char* dir, int step, double time) {
+    auto* s = static_cast<RefSim*>(h);
+    GlobalStatsWriter w(dir);
+    w.writeTimestep(s->lbm->field(), s->caps, step, time, s->adr.get());
+}
 
 // OpenMP thread count of the reference loops.  One thread makes the
 // reference's spread (per-thread buffers, dynamic schedule) reproducible.

@@ -144,6 +144,15 @@ SIGNATURES = {
                                     _P(C.c_longlong), _P(C.c_longlong)]),
     "sfg_autotune": (C.c_int, [C.c_void_p, C.c_int, _P(C.c_int)]),
     "sfg_thermo": (C.c_int, [C.c_void_p, _P(ThermoRecordC), _D]),
+    "sfg_write_vtk_fluid": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p, C.c_int, C.c_int,
+                                      C.c_uint]),
+    "sfg_write_vtk_capsules": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p, C.c_int, C.c_int,
+                                         _I]),
+    "sfg_set_scalar_state": (C.c_int, [C.c_void_p, C.c_int, _D, _D]),
+    "sfg_mark_restored": (C.c_int, [C.c_void_p]),
+    "sfg_get_channel_params": (C.c_int, [C.c_void_p, C.c_int, _P(ChannelParamsC)]),
+    "sfg_get_capsule_nodes": (C.c_int, [C.c_void_p, C.c_int, _I]),
+    "sfg_get_capsule_base": (C.c_int, [C.c_void_p, C.c_int, _I]),
     "sfg_run": (C.c_int, [C.c_void_p, C.c_int, C.c_int, THERMO_FN, C.c_void_p, _P(C.c_int)]),
     "sfg_get_launch_config": (C.c_int, [C.c_void_p, _P(C.c_int), _P(C.c_int), _P(C.c_int),
                                         _P(C.c_int)]),

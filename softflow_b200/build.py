@@ -32,7 +32,7 @@ UNITS = [
     ("learned_step.cu", ["--fmad=false"]),
     ("context.cu", []),
 ]
-HOST_UNITS = [("host_setup.cpp", ["-ffp-contract=off"])]
+HOST_UNITS = [("host_setup.cpp", ["-ffp-contract=off"]), ("host_io.cpp", ["-ffp-contract=off"])]
 
 
 def _nvcc() -> str:

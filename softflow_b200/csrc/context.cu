@@ -105,6 +105,27 @@ __global__ void k_scalar_set(const double* __restrict__ C, R* __restrict__ g0, R
     }
 }
 
+// Scalar state from a saved state: populations g [9][ny][nx] into both
+// buffers and the concentration field the next collision reads.
+template <typename R>
+__global__ void k_scalar_import(const double* __restrict__ C, const double* __restrict__ g,
+                                R* __restrict__ g0, R* __restrict__ g1, R* __restrict__ cf,
+                                ChannelDev ch) {
+    const long long N = (long long)ch.nx * ch.ny;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(i / ch.nx), x = (int)(i % ch.nx);
+        const long long n = (long long)y * ch.pitch + x;
+        cf[ch.cell_off + n] = (R)C[i];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            const R v = (R)g[q * N + i];
+            g0[ch.g_off + q * ch.plane + n] = v;
+            g1[ch.g_off + q * ch.plane + n] = v;
+        }
+    }
+}
+
 template <typename R>
 __global__ void k_scalar_export(const R* __restrict__ g, ChannelDev ch, double* __restrict__ C,
                                 double* __restrict__ gout) {
@@ -176,6 +197,7 @@ struct sfg_context {
     int shared_collision = -1;
 
     long long steps = 0;
+    bool restored = false;              // state restored before the first step
     bool adr_pending_h = false;
     int g_cur = 0;
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
@@ -1135,7 +1157,7 @@ extern "C" int sfg_get_macroscopic(sfg_context* c, int chi, double* rho, double*
     if ((rc = ensure_io(c, 5 * N))) return rc;
     const int p = (int)(c->steps & 1);
     const TileViewArgs tv = last_view(c);
-    const int stepped = c->steps > 0;
+    const int stepped = c->steps > 0 || c->restored;
     double* o = c->d_io;
     if (c->precision == SFG_FP64)
         launch_macro_export<double, double>(c->f[p], d, tv, stepped, o, o + N, o + 2 * N, o + 3 * N, o + 4 * N, c->stream);
@@ -1234,6 +1256,42 @@ extern "C" int sfg_set_concentration(sfg_context* c, int chi, const double* C) {
     return SFG_OK;
 }
 
+extern "C" int sfg_set_scalar_state(sfg_context* c, int chi, const double* C, const double* g) {
+    int rc = check_chan(c, chi, "sfg_set_scalar_state");
+    if (rc) return rc;
+    if (!C || !g) return fail(SFG_ERR_ARG, "sfg_set_scalar_state: null input");
+    const ChannelDev& d = c->ch[chi].d;
+    if (!d.adr) return fail(SFG_ERR_STATE, "sfg_set_scalar_state: scalar transport is off");
+    if ((rc = flush_scalar(c))) return rc;
+    const size_t N = (size_t)d.nx * d.ny;
+    if ((rc = ensure_io(c, 10 * N))) return rc;
+    CU(cudaMemcpyAsync(c->d_io, C, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CU(cudaMemcpyAsync(c->d_io + N, g, 9 * N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (c->precision == SFG_FP64)
+        k_scalar_import<double><<<io_blocks(N), 256, 0, c->stream>>>(c->d_io, c->d_io + N, (double*)c->g[0], (double*)c->g[1], (double*)c->cfield, d);
+    else
+        k_scalar_import<float><<<io_blocks(N), 256, 0, c->stream>>>(c->d_io, c->d_io + N, (float*)c->g[0], (float*)c->g[1], (float*)c->cfield, d);
+    const int one = 1;
+    CU(cudaMemcpyAsync(c->d_c_fresh + chi, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(c->stream));
+    return SFG_OK;
+}
+
+extern "C" int sfg_mark_restored(sfg_context* c) {
+    if (!c) return fail(SFG_ERR_ARG, "sfg_mark_restored: null context");
+    if (!c->initialized) return fail(SFG_ERR_STATE, "sfg_mark_restored: context not initialized");
+    if (c->steps != 0)
+        return fail(SFG_ERR_STATE, "sfg_mark_restored: only before the first step");
+    CU(cudaSetDevice(c->device));
+    const int nch = (int)c->ch.size();
+    std::vector<int> ones(nch, 1);
+    CU(cudaMemcpyAsync(c->d_stepped, ones.data(), sizeof(int) * nch, cudaMemcpyHostToDevice, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    c->restored = true;
+    return SFG_OK;
+}
+
 extern "C" int sfg_get_concentration(sfg_context* c, int chi, double* C, double* g) {
     int rc = check_chan(c, chi, "sfg_get_concentration");
     if (rc) return rc;
@@ -1327,7 +1385,7 @@ static int enqueue_thermo(sfg_context* c) {
     if (rc) return rc;
     const int p = (int)(c->steps & 1);
     const TileViewArgs tv = last_view(c);
-    const int stepped = c->steps > 0;
+    const int stepped = c->steps > 0 || c->restored;
     const void* g = c->any_adr ? c->g[c->g_cur] : nullptr;
     if (c->precision == SFG_FP64)
         launch_thermo_cells<double, double>(c->f[p], g, c->d_chans, nch, c->thermo_bpc, tv, stepped, c->d_thermo_parts, c->stream);
@@ -1434,6 +1492,30 @@ extern "C" int sfg_channel_counts(const sfg_context* c, int chi, int* ncaps, int
     for (const auto& cp : c->ch[chi].caps) m += cp.rest.num_nodes;
     if (ncaps) *ncaps = (int)c->ch[chi].caps.size();
     if (nmk) *nmk = m;
+    return SFG_OK;
+}
+
+extern "C" int sfg_get_channel_params(const sfg_context* c, int chi, sfg_channel_params* out) {
+    if (!c || !out || chi < 0 || chi >= (int)c->ch.size())
+        return fail(SFG_ERR_ARG, "sfg_get_channel_params: bad argument");
+    *out = c->ch[chi].p;
+    return SFG_OK;
+}
+
+extern "C" int sfg_get_capsule_nodes(const sfg_context* c, int chi, int* nodes) {
+    if (!c || !nodes || chi < 0 || chi >= (int)c->ch.size())
+        return fail(SFG_ERR_ARG, "sfg_get_capsule_nodes: bad argument");
+    int k = 0;
+    for (const auto& cp : c->ch[chi].caps) nodes[k++] = cp.rest.num_nodes;
+    return SFG_OK;
+}
+
+extern "C" int sfg_get_capsule_base(const sfg_context* c, int chi, int* first_capsule) {
+    if (!c || !first_capsule || chi < 0 || chi >= (int)c->ch.size())
+        return fail(SFG_ERR_ARG, "sfg_get_capsule_base: bad argument");
+    int k = 0;
+    for (int i = 0; i < chi; ++i) k += (int)c->ch[i].caps.size();
+    *first_capsule = k;
     return SFG_OK;
 }
 

@@ -24,6 +24,7 @@ from __future__ import annotations
 import ctypes as C
 import enum
 import math
+import os
 import sys
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence
@@ -147,6 +148,18 @@ class SimulationParams:
     membrane: MembraneParams = field(default_factory=MembraneParams)
     repulsion: RepulsionParams = field(default_factory=RepulsionParams)
     scalar: ScalarParams = field(default_factory=ScalarParams)
+    # output (parameters.h:302-313).  output_dir None writes no files (the
+    # reference's default is "output"); set it to get the reference's
+    # per-step output schedule in run().
+    output_dir: Optional[str] = None
+    output_interval: int = 100
+    vtk_dump_every: int = 0
+    csv_dump_every: int = 0
+    probe_dump_every: int = 10
+    stats_dump_every: int = 100
+    checkpoint_interval: int = 0
+    vtk_format: str = "ascii"
+    probes: List[tuple] = field(default_factory=list)
     # stability monitoring (parameters.h:315-319)
     enable_stability_checks: bool = True
     max_density_deviation: float = 0.1
@@ -682,24 +695,41 @@ class Ensemble:
             done = ctx.run(num_steps, int(thermo_every), callback)
             self._steps += done
             return done
-        ivs = sorted({c.params.stability_check_interval for c in self._chans
-                      if c.params.enable_stability_checks and c.params.stability_check_interval > 0})
+        events = self._scheduled()
         done = 0
         while done < num_steps:
-            # next step (0-based count before the step) that is checked
+            # next step (counted before the step, as the reference's
+            # step_count_) at which some per-step task runs
             s0 = self._steps
-            nxt = min((-(-s0 // iv)) * iv for iv in ivs) if ivs else None
+            nxt = None
+            for iv, first, _ in events:
+                k = max(s0, first)
+                m = -(-k // iv) * iv
+                nxt = m if nxt is None else min(nxt, m)
             n = num_steps - done if nxt is None else min(num_steps - done, nxt - s0 + 1)
             ctx.step(n)
             self._steps += n
             done += n
             if nxt is not None and self._steps - 1 == nxt:
-                for k, c in enumerate(self._chans):
-                    iv = c.params.stability_check_interval
-                    if c.params.enable_stability_checks and iv > 0 and nxt % iv == 0:
-                        self.checkStability(k, step=nxt)
+                for iv, first, fn in events:
+                    if nxt >= first and nxt % iv == 0:
+                        fn(nxt)
         ctx.synchronize()
+        self._finish_run()
         return done
+
+    def _scheduled(self):
+        """Per-step tasks of Simulation::step after the physics
+        (simulation.cpp:729-787) as (interval, first step, fn(step))."""
+        ev = []
+        for k, c in enumerate(self._chans):
+            iv = c.params.stability_check_interval
+            if c.params.enable_stability_checks and iv > 0:
+                ev.append((iv, 0, lambda s, k=k: self.checkStability(k, step=s)))
+        return ev
+
+    def _finish_run(self):
+        pass
 
     def synchronize(self) -> int:
         return self._need().synchronize()
@@ -880,3 +910,77 @@ class Simulation(Ensemble):
 
     def setChannelWalls(self, enabled: bool = True):
         super().setChannelWalls(0, enabled)
+
+    def setStepCallback(self, fn):
+        """fn(sim, step) after every step (Simulation::setStepCallback; step
+        counted before the step, simulation.cpp:781-784).  Costs one host
+        round trip per step."""
+        self._step_callback = fn
+
+    def _writers(self):
+        from . import output as O
+        if getattr(self, "_out", None) is None:
+            p = self._params
+            d = p.output_dir
+            self._out = {"vtk": O.VTKWriter(d, legacy=(p.vtk_format == "legacy")),
+                         "csv": O.CSVWriter(d), "probe": O.FluidProbeWriter(d),
+                         "stats": O.GlobalStatsWriter(d)}
+            for i, j, label in p.probes:
+                self._out["probe"].addProbe(i, j, label)
+        return self._out
+
+    def _scheduled(self):
+        ev = super()._scheduled()
+        p = self._params
+        if p.output_dir:
+            w = self._writers()
+            t = lambda s: s * p.dt  # noqa: E731
+            vtk_iv = p.vtk_dump_every if p.vtk_dump_every > 0 else p.output_interval
+            csv_iv = p.csv_dump_every if p.csv_dump_every > 0 else p.output_interval
+
+            def vtk(s):
+                w["vtk"].writeFluidField(self, s)
+                w["vtk"].writeCapsules(self, s)
+                w["vtk"].recordTimestep(s, t(s))
+            if vtk_iv > 0:
+                ev.append((vtk_iv, 0, vtk))
+            if csv_iv > 0:
+                ev.append((csv_iv, 0, lambda s: w["csv"].writeTimestep(self, s, t(s))))
+            if p.probe_dump_every > 0 and p.probes:
+                ev.append((p.probe_dump_every, 0,
+                           lambda s: w["probe"].writeTimestep(self, s, t(s))))
+            if p.stats_dump_every > 0:
+                ev.append((p.stats_dump_every, 0,
+                           lambda s: w["stats"].writeTimestep(self, s, t(s))))
+            if p.checkpoint_interval > 0:
+                from .output import Checkpoint
+
+                def ckpt(s):
+                    # named and stamped with the step count before the
+                    # increment, as the reference does (simulation.cpp:
+                    # 773-779); the file holds the state after the step
+                    Checkpoint.save(self, os.path.join(p.output_dir, f"checkpoint_{s}.sfck"),
+                                    step=s)
+                ev.append((p.checkpoint_interval, 1, ckpt))
+        cb = getattr(self, "_step_callback", None)
+        if cb is not None:
+            ev.append((1, 0, lambda s: cb(self, s)))
+        return ev
+
+    def _finish_run(self):
+        """Simulation::finalize (simulation.cpp:802-817): PVD collections,
+        writers closed."""
+        out = getattr(self, "_out", None)
+        if out is not None:
+            out["vtk"].writePVDFiles()
+            for k in ("csv", "probe", "stats"):
+                out[k].close()
+            self._out = None
+
+    def saveCheckpoint(self, filename: str) -> str:
+        from .output import Checkpoint
+        return Checkpoint.save(self, filename)
+
+    def loadCheckpoint(self, filename: str) -> int:
+        from .output import Checkpoint
+        return Checkpoint.load(self, filename)

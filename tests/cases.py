@@ -21,6 +21,11 @@ def gaussian_conc(cx, cy, sigma):
     return f
 
 
+def diffusion_conc(nx, ny):
+    """Initial concentration of the diffusion fixtures: a Gaussian in x."""
+    return np.exp(-((np.arange(nx)[None, :] - nx / 2.0) ** 2) / (2 * 64.0)) * np.ones((ny, 1))
+
+
 SKALAK_C1 = dict(model=O.SKALAK, G_s=0.06, C_skalak=10.0, k_bend=0.0)
 WLC_HELF = dict(model=O.WLC, G_s=0.06, use_helfrich=1, k_bend=0.01)
 

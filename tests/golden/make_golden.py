@@ -18,7 +18,11 @@ sys.path.insert(0, os.path.dirname(HERE))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 import oracle  # noqa: E402
-from cases import CASES, build_oracle, fluid_rows  # noqa: E402
+from cases import CASES, build_oracle, diffusion_conc, fluid_rows  # noqa: E402
+
+# Output files of the reference's own writers (VTKWriter, GlobalStatsWriter)
+# on states the GPU path reproduces bit for bit in FP64.
+OUTPUT_RUNS = [("bgk_small", 300), ("seam_single", 40), ("diffusion", 200)]
 
 RUNS = [("bgk_small", 300), ("mrt_small", 300), ("reg_small", 300), ("mini_c2", 30),
         ("contact_brute", 60), ("seam_single", 40), ("c1", 10)]
@@ -49,5 +53,36 @@ def main():
         print(path, os.path.getsize(path))
 
 
+def outputs():
+    """tests/golden/output/<case>_<steps>.npz: the bytes of every file the
+    reference's writers produce for the state after <steps> steps (XML and
+    legacy VTK, one global_stats.csv row at time = steps)."""
+    import tempfile
+    oracle.build(ref=True)
+    os.makedirs(os.path.join(HERE, "output"), exist_ok=True)
+    for name, steps in OUTPUT_RUNS:
+        case = dict(CASES[name])
+        if name == "diffusion":
+            case["conc"] = diffusion_conc
+        o = build_oracle(case, impl="ref")
+        o.step(steps)
+        files = {}
+        with tempfile.TemporaryDirectory() as td:
+            for legacy in (False, True):
+                d = os.path.join(td, "legacy" if legacy else "xml")
+                o.write_vtk(d, steps, legacy)
+            o.write_global_stats(os.path.join(td, "stats"), steps, float(steps))
+            for root, _, fns in os.walk(td):
+                for fn in fns:
+                    full = os.path.join(root, fn)
+                    rel = os.path.relpath(full, td)
+                    with open(full, "rb") as fh:
+                        files[rel] = np.frombuffer(fh.read(), dtype=np.uint8)
+        path = os.path.join(HERE, "output", f"{name}_{steps}.npz")
+        np.savez_compressed(path, **{k.replace("/", "|"): v for k, v in files.items()})
+        print(path, os.path.getsize(path), sorted(files))
+
+
 if __name__ == "__main__":
     main()
+    outputs()
