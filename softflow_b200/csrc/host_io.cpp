@@ -348,6 +348,58 @@ extern "C" int sfg_write_vtk_capsules(sfg_context* ctx, int channel, const char*
             for (const auto& cp : copies)
                 for (int k = off[cp.capsule]; k < off[cp.capsule + 1]; ++k) std::fprintf(fp, "%.6e\n", 0.0);
         }
+        // per-polygon quantities (vtk_writer.cpp:821-913)
+        std::fprintf(fp, "CELL_DATA %d\n", total_polys);
+        std::fprintf(fp, "SCALARS capsule_id_cell int 1\n");
+        std::fprintf(fp, "LOOKUP_TABLE default\n");
+        for (const auto& cp : copies) std::fprintf(fp, "%d\n", cp.capsule);
+        std::fprintf(fp, "SCALARS cell_type int 1\n");
+        std::fprintf(fp, "LOOKUP_TABLE default\n");
+        for (const auto& cp : copies) std::fprintf(fp, "%d\n", tid(cp.capsule));
+        std::fprintf(fp, "SCALARS deformation_index double 1\n");
+        std::fprintf(fp, "LOOKUP_TABLE default\n");
+        for (const auto& cp : copies) std::fprintf(fp, "%.6e\n", st[(size_t)base + cp.capsule].deformation);
+        std::vector<double> avx(ncaps), avy(ncaps), ftx(ncaps), fty(ncaps);
+        for (int c = 0; c < ncaps; ++c) {
+            double ax = 0.0, ay = 0.0, fx = 0.0, fy = 0.0;
+            for (int k = off[c]; k < off[c + 1]; ++k) {
+                ax += vel[2 * (size_t)k];
+                ay += vel[2 * (size_t)k + 1];
+                fx += frc[2 * (size_t)k];
+                fy += frc[2 * (size_t)k + 1];
+            }
+            avx[c] = ax / nodes[c];
+            avy[c] = ay / nodes[c];
+            ftx[c] = fx;
+            fty[c] = fy;
+        }
+        std::fprintf(fp, "VECTORS particle_velocity double\n");
+        for (const auto& cp : copies) std::fprintf(fp, "%.6e %.6e 0\n", avx[cp.capsule], avy[cp.capsule]);
+        std::fprintf(fp, "VECTORS particle_force double\n");
+        for (const auto& cp : copies) std::fprintf(fp, "%.6e %.6e 0\n", ftx[cp.capsule], fty[cp.capsule]);
+        std::fprintf(fp, "SCALARS particle_speed double 1\n");
+        std::fprintf(fp, "LOOKUP_TABLE default\n");
+        for (const auto& cp : copies) {
+            const double ax = avx[cp.capsule], ay = avy[cp.capsule];
+            std::fprintf(fp, "%.6e\n", std::sqrt(ax * ax + ay * ay));
+        }
+        std::fprintf(fp, "SCALARS particle_area double 1\n");
+        std::fprintf(fp, "LOOKUP_TABLE default\n");
+        for (const auto& cp : copies) std::fprintf(fp, "%.6e\n", st[(size_t)base + cp.capsule].area);
+        std::fprintf(fp, "SCALARS particle_perimeter double 1\n");
+        std::fprintf(fp, "LOOKUP_TABLE default\n");
+        for (const auto& cp : copies) std::fprintf(fp, "%.6e\n", st[(size_t)base + cp.capsule].perimeter);
+        if (scalar) {
+            // no capsule chemistry on this path: nothing released or
+            // absorbed, infinite reservoirs (-1), no surface coverage
+            const char* names[4] = {"scalar_released", "scalar_absorbed", "Mp", "gamma_mean"};
+            const double vals[4] = {0.0, 0.0, -1.0, 0.0};
+            for (int a = 0; a < 4; ++a) {
+                std::fprintf(fp, "SCALARS %s double 1\n", names[a]);
+                std::fprintf(fp, "LOOKUP_TABLE default\n");
+                for (size_t k = 0; k < copies.size(); ++k) std::fprintf(fp, "%.6e\n", vals[a]);
+            }
+        }
         std::fflush(fp);
         std::fclose(fp);
         return SFG_OK;
