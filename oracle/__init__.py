@@ -28,6 +28,7 @@ REF_FAST_LIB = os.path.join(HERE, "_ref", "libsfref_fast.so")
 
 BGK, MRT, REGULARIZED = 0, 1, 2
 HOOKEAN, NEO_HOOKEAN, SKALAK, WLC = 0, 1, 2, 3
+INLET_OUTLET, PERIODIC, CLOSED = 0, 1, 2
 
 
 class _Params(C.Structure):
@@ -42,6 +43,9 @@ class _Params(C.Structure):
         ("rep_power", C.c_int), ("rep_damping_normal", C.c_double), ("rep_friction", C.c_double),
         ("scalar_enabled", C.c_int), ("scalar_D", C.c_double),
         ("scalar_periodic_y", C.c_int), ("scalar_inlet", C.c_double),
+        ("boundary_type", C.c_int), ("inlet_velocity", C.c_double),
+        ("outlet_density", C.c_double), ("top_wall_velocity", C.c_double),
+        ("bottom_wall_velocity", C.c_double),
     ]
 
 
@@ -82,6 +86,12 @@ class ChannelSpec:
     scalar_D: float = 0.01
     scalar_periodic_y: int = 0
     scalar_inlet: float = 0.0
+    # BoundaryType (types.h:58-62): 0 INLET_OUTLET, 1 PERIODIC, 2 CLOSED
+    boundary_type: int = 1
+    inlet_velocity: float = 0.02
+    outlet_density: float = 1.0
+    top_wall_velocity: float = 0.0
+    bottom_wall_velocity: float = 0.0
 
     def to_c(self) -> _Params:
         return _Params(**{f.name: getattr(self, f.name) for f in fields(self)})

@@ -104,7 +104,11 @@ void* sfr_create(const sf_params* in) {
     p.max_lattice_force = in->max_lattice_force;
     p.fluid.tau = in->tau;
     p.fluid.rho0 = in->rho0;
-    p.fluid.boundary_type = BoundaryType::PERIODIC;
+    p.fluid.boundary_type = static_cast<BoundaryType>(in->boundary_type);
+    p.fluid.inlet_velocity = in->inlet_velocity;
+    p.fluid.outlet_density = in->outlet_density;
+    p.fluid.top_wall_velocity = in->top_wall_velocity;
+    p.fluid.bottom_wall_velocity = in->bottom_wall_velocity;
     p.fluid.periodic_y = in->periodic_y != 0;
     p.fluid.body_force_x = in->body_fx;
     p.fluid.body_force_y = in->body_fy;
@@ -126,8 +130,10 @@ void* sfr_create(const sf_params* in) {
     // Simulation constructor (simulation.cpp:125-140)
     s->lbm = std::make_unique<LBMSolver>(p);
     s->rep = std::make_unique<RepulsionForce>(p.repulsion);
-    s->rep->setPeriodicX(static_cast<Real>(p.nx));
-    s->caps.setPeriodicX(p.nx);
+    if (p.fluid.boundary_type == BoundaryType::PERIODIC) {      // simulation.cpp:129-132
+        s->rep->setPeriodicX(static_cast<Real>(p.nx));
+        s->caps.setPeriodicX(p.nx);
+    }
     if (p.scalar.enabled) s->adr = std::make_unique<AdvectionDiffusion>(p.nx, p.ny, p.scalar);
     return s;
 }
@@ -181,7 +187,8 @@ void sfr_initialize(void* h) {
     auto* s = static_cast<RefSim*>(h);
     s->lbm->initialize();                      // simulation.cpp:436
     if (s->adr) s->adr->initialize(0.0);       // :446-448
-    s->caps.setPeriodicX(s->p.nx);             // :456-458
+    if (s->p.fluid.boundary_type == BoundaryType::PERIODIC)
+        s->caps.setPeriodicX(s->p.nx);             // :456-458
     sync_markers(s);
 }
 
@@ -293,7 +300,7 @@ double sfr_phi(double r) { return PeskinDelta::phi(r); }
 void sfr_write_vtk(void* h, const char* dir, int step, int legacy) {
     auto* s = static_cast<RefSim*>(h);
     VTKWriter w(dir);
-    w.setPeriodicX(s->p.nx);
+    if (s->p.fluid.boundary_type == BoundaryType::PERIODIC) w.setPeriodicX(s->p.nx);
     w.setLegacyMode(legacy != 0);
     if (s->adr) w.setAdvectionDiffusion(s->adr.get());
     w.writeFluidField(s->lbm->field(), step);

@@ -24,7 +24,8 @@ static const int CY[Q] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
 static const int OPP[Q] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
 static const double PI_ = 3.14159265358979323846;
 
-enum { CT_FLUID = 0, CT_SOLID = 1 };
+enum { CT_FLUID = 0, CT_SOLID = 1, CT_INLET = 2, CT_OUTLET = 3 };
+enum { BT_INLET_OUTLET = 0, BT_PERIODIC = 1, BT_CLOSED = 2 };
 
 typedef struct { double x, y; } v2;
 static inline v2 vadd(v2 a, v2 b) { v2 r = {a.x + b.x, a.y + b.y}; return r; }
@@ -79,6 +80,11 @@ void sf_params_default(sf_params* p) {
     p->dt = 1.0;
     p->rep_epsilon = 0.05; p->rep_sigma = 1.0; p->rep_r_cut = 3.5; p->rep_power = 4;
     p->scalar_D = 0.01;
+    p->boundary_type = BT_PERIODIC;
+    p->inlet_velocity = 0.02;
+    p->outlet_density = 1.0;
+    p->top_wall_velocity = 0.0;
+    p->bottom_wall_velocity = 0.0;
 }
 
 /* Defaults of reference MembraneParams (parameters.h:82-136). */
@@ -318,7 +324,7 @@ static void collide_mrt(sfo_sim* s) {
  * 212-235): out-of-range sources fall back to the node itself. */
 static void stream(sfo_sim* s) {
     const int nx = s->nx, ny = s->ny, N = s->N;
-    const int px = 1, py = s->p.periodic_y;
+    const int px = s->p.boundary_type == BT_PERIODIC, py = s->p.periodic_y;
     for (int q = 0; q < Q; ++q) {
         for (int y = 0; y < ny; ++y) {
             for (int x = 0; x < nx; ++x) {
@@ -343,7 +349,7 @@ static void bounce_back(sfo_sim* s) {
         int x = n % nx, y = n / nx;
         for (int q = 1; q < Q; ++q) {
             int xn = x - CX[q], yn = y - CY[q];
-            xn = (xn + nx) % nx;
+            if (s->p.boundary_type == BT_PERIODIC) xn = (xn + nx) % nx;
             if (s->p.periodic_y) yn = (yn + ny) % ny;
             if (xn < 0 || xn >= nx || yn < 0 || yn >= ny) continue;
             if (s->flags[yn * nx + xn] == CT_SOLID) continue;
@@ -352,13 +358,80 @@ static void bounce_back(sfo_sim* s) {
     }
 }
 
-/* reference lbm_solver.cpp:172-207 (collide -> stream -> BB -> macroscopic) */
+/* Moving top / bottom walls after the halfway bounce-back (reference
+ * moving_wall.cpp:14-64): the reflected population of each link into a wall
+ * row loses 2 w_q rho_n (e_q . u_wall) / cs^2, rho_n of the fluid node from
+ * the last macroscopic update. */
+static void moving_wall_row(sfo_sim* s, int yw, double vel) {
+    const int nx = s->nx, ny = s->ny, N = s->N;
+    const double cs2 = 1.0 / 3.0;
+    for (int x = 0; x < nx; ++x) {
+        if (s->flags[yw * nx + x] != CT_SOLID) continue;
+        for (int q = 1; q < Q; ++q) {
+            int xn = x - CX[q], yn = yw - CY[q];
+            if (s->p.boundary_type == BT_PERIODIC) xn = (xn + nx) % nx;
+            if (xn < 0 || xn >= nx || yn < 0 || yn >= ny) continue;
+            if (s->flags[yn * nx + xn] == CT_SOLID) continue;
+            double rho = s->rho[yn * nx + xn];
+            double eu_wall = CX[q] * vel;
+            s->f[OPP[q] * N + yn * nx + xn] = s->f[q * N + yw * nx + x]
+                - 2.0 * W[q] * rho * eu_wall / cs2;
+        }
+    }
+}
+
+static void moving_walls(sfo_sim* s) {
+    if (fabs(s->p.bottom_wall_velocity) > 1e-15) moving_wall_row(s, 0, s->p.bottom_wall_velocity);
+    if (fabs(s->p.top_wall_velocity) > 1e-15) moving_wall_row(s, s->ny - 1, s->p.top_wall_velocity);
+}
+
+/* Zou-He velocity inlet (parabolic profile) on the INLET column and
+ * pressure outlet on the OUTLET column, in the order of the reference's
+ * node lists (zou_he_boundary.cpp:17-85: inlet nodes, then outlet nodes,
+ * each by increasing y). */
+static void zou_he(sfo_sim* s) {
+    const int nx = s->nx, ny = s->ny, N = s->N;
+#define F(x, y, q) s->f[(q) * N + (y) * nx + (x)]
+    for (int y = 0; y < ny; ++y) {
+        const int x = 0;
+        if (s->flags[y * nx + x] != CT_INLET) continue;
+        double y_center = (double)ny * 0.5;
+        double H = (double)(ny - 2);
+        double y_norm = ((double)y - y_center) / (H * 0.5);
+        double ux = s->p.inlet_velocity * (1.0 - y_norm * y_norm);
+        double uy = 0.0;
+        double f0 = F(x, y, 0), f2 = F(x, y, 2), f3 = F(x, y, 3);
+        double f4 = F(x, y, 4), f6 = F(x, y, 6), f7 = F(x, y, 7);
+        double rho = (f0 + f2 + f4 + 2.0 * (f3 + f6 + f7)) / (1.0 - ux);
+        F(x, y, 1) = f3 + (2.0 / 3.0) * rho * ux;
+        F(x, y, 5) = f7 + 0.5 * (f4 - f2) + (1.0 / 6.0) * rho * ux + 0.5 * rho * uy;
+        F(x, y, 8) = f6 - 0.5 * (f4 - f2) + (1.0 / 6.0) * rho * ux - 0.5 * rho * uy;
+    }
+    for (int y = 0; y < ny; ++y) {
+        const int x = nx - 1;
+        if (s->flags[y * nx + x] != CT_OUTLET) continue;
+        double rho = s->p.outlet_density;
+        double f0 = F(x, y, 0), f1 = F(x, y, 1), f2 = F(x, y, 2);
+        double f4 = F(x, y, 4), f5 = F(x, y, 5), f8 = F(x, y, 8);
+        double ux = -1.0 + (f0 + f2 + f4 + 2.0 * (f1 + f5 + f8)) / rho;
+        double uy = 0.0;
+        F(x, y, 3) = f1 - (2.0 / 3.0) * rho * ux;
+        F(x, y, 7) = f5 - 0.5 * (f4 - f2) - (1.0 / 6.0) * rho * ux - 0.5 * rho * uy;
+        F(x, y, 6) = f8 + 0.5 * (f4 - f2) - (1.0 / 6.0) * rho * ux + 0.5 * rho * uy;
+    }
+#undef F
+}
+
+/* reference lbm_solver.cpp:172-207 (collide -> stream -> BB -> moving wall
+ * -> Zou-He -> macroscopic) */
 static void lbm_step(sfo_sim* s) {
     if (s->p.collision == SF_REGULARIZED) collide_regularized(s);
     else if (s->p.collision == SF_MRT) collide_mrt(s);
     else collide_bgk(s);
     stream(s);
     bounce_back(s);
+    moving_walls(s);
+    if (s->p.boundary_type == BT_INLET_OUTLET) zou_he(s);
     sfo_compute_macroscopic(s);
 }
 
@@ -1080,8 +1153,17 @@ void sfo_initialize(sfo_sim* s) {
     const int nx = s->nx, ny = s->ny, N = s->N;
     /* lbm_solver.cpp:130-170 */
     for (int n = 0; n < N; ++n) s->flags[n] = CT_FLUID;
-    if (!s->p.periodic_y) {
-        for (int x = 0; x < nx; ++x) { s->flags[x] = CT_SOLID; s->flags[(ny - 1) * nx + x] = CT_SOLID; }
+    for (int x = 0; x < nx; ++x) { s->flags[x] = CT_SOLID; s->flags[(ny - 1) * nx + x] = CT_SOLID; }
+    if (s->p.boundary_type == BT_INLET_OUTLET) {
+        for (int y = 1; y < ny - 1; ++y) {
+            s->flags[y * nx] = CT_INLET;
+            s->flags[y * nx + nx - 1] = CT_OUTLET;
+        }
+    } else if (s->p.boundary_type == BT_CLOSED) {
+        for (int y = 0; y < ny; ++y) { s->flags[y * nx] = CT_SOLID; s->flags[y * nx + nx - 1] = CT_SOLID; }
+    }
+    if (s->p.periodic_y) {
+        for (int x = 0; x < nx; ++x) { s->flags[x] = CT_FLUID; s->flags[(ny - 1) * nx + x] = CT_FLUID; }
     }
     for (int n = 0; n < N; ++n) {
         s->rho[n] = s->p.rho0; s->ux[n] = 0.0; s->uy[n] = 0.0;

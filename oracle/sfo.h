@@ -13,7 +13,9 @@
  * tests/test_oracle_vs_reference.py against the reference sources compiled
  * by oracle/Makefile).
  *
- * Scope: periodic-x channel (rows 0 and ny-1 SOLID, or periodic-y), BGK /
+ * Scope: periodic-x channel (rows 0 and ny-1 SOLID, or periodic-y), a
+ * closed box, or a Zou-He inlet / outlet channel, with optional moving top /
+ * bottom walls; BGK /
  * MRT / regularized collision with Guo forcing, body force + force cap,
  * Peskin 4-point IBM spread / interpolate / multi-direct forcing, circular
  * capsules with Hookean / Neo-Hookean / Skalak / WLC stretching,
@@ -54,6 +56,13 @@ typedef struct sf_params {
     double scalar_D;
     int scalar_periodic_y;
     double scalar_inlet;
+    /* fluid boundaries (FluidParams, parameters.h:44-46, 87-88):
+     * boundary_type as BoundaryType (types.h:58-62): 0 INLET_OUTLET
+     * (Zou-He velocity inlet at x = 0, pressure outlet at x = nx-1),
+     * 1 PERIODIC, 2 CLOSED; moving top / bottom walls */
+    int boundary_type;
+    double inlet_velocity, outlet_density;
+    double top_wall_velocity, bottom_wall_velocity;
 } sf_params;
 
 /* Membrane parameters (reference MembraneParams, circle shape only). */

@@ -75,6 +75,31 @@ CASES = {
                           capsules=[("add", 10.0, 20.0, 4.0, 0, dict(model=O.HOOKEAN)),
                                     ("add", 19.5, 21.0, 4.0, 0, dict(model=O.NEO_HOOKEAN))],
                           conc=None),
+    # Zou-He velocity inlet / pressure outlet channels (the reference's
+    # default BoundaryType::INLET_OUTLET), no body force
+    "zouhe_bgk": dict(spec=dict(nx=64, ny=20, collision=O.BGK, tau=0.8,
+                                boundary_type=O.INLET_OUTLET, inlet_velocity=0.03,
+                                outlet_density=1.0),
+                      capsules=[], conc=None),
+    "zouhe_mrt": dict(spec=dict(nx=48, ny=26, collision=O.MRT, tau=0.7,
+                                boundary_type=O.INLET_OUTLET, inlet_velocity=0.02,
+                                outlet_density=0.995, body_fx=1e-6),
+                      capsules=[], conc=None),
+    "zouhe_reg": dict(spec=dict(nx=40, ny=18, collision=O.REGULARIZED, tau=0.9,
+                                boundary_type=O.INLET_OUTLET, inlet_velocity=0.04,
+                                outlet_density=1.0, bottom_wall_velocity=0.01),
+                      capsules=[], conc=None),
+    # lid-driven cavity: closed box, moving top wall
+    "cavity": dict(spec=dict(nx=32, ny=32, collision=O.BGK, tau=0.7,
+                             boundary_type=O.CLOSED, top_wall_velocity=0.05),
+                   capsules=[], conc=None),
+    # plane Couette flow with a capsule (periodic x, walls moving apart)
+    "shear_capsule": dict(spec=dict(nx=64, ny=34, collision=O.BGK, tau=0.8,
+                                    top_wall_velocity=0.01, bottom_wall_velocity=-0.01,
+                                    ibm_iterations=3),
+                          capsules=[("add", 32.0, 17.0, 6.0, 36,
+                                     dict(model=O.SKALAK, G_s=0.05, C_skalak=10.0))],
+                          conc=None),
     # pure diffusion (reference tests/verification/test_pure_diffusion.cpp)
     "diffusion": dict(spec=dict(nx=256, ny=8, collision=O.BGK, tau=0.6, periodic_y=1,
                                 scalar_enabled=1, scalar_D=0.05, scalar_periodic_y=1),

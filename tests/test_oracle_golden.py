@@ -11,7 +11,8 @@ import oracle as O
 from cases import CASES, build_oracle, fluid_rows
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-NAMES = ["bgk_small", "mrt_small", "reg_small", "mini_c2", "contact_brute", "seam_single", "c1"]
+NAMES = ["bgk_small", "mrt_small", "reg_small", "mini_c2", "contact_brute", "seam_single", "c1",
+         "zouhe_bgk", "zouhe_reg", "cavity", "shear_capsule"]
 
 
 @pytest.mark.parametrize("name", NAMES)
@@ -97,3 +98,22 @@ def test_oracle_stats_restatement():
     ux[3, 1] = np.nan
     ux[2, 2] = np.inf
     assert OS.first_nonfinite(rho, ux, uy, solid) == 2 * nx + 2
+
+
+BOUNDARY_CASES = [("zouhe_bgk", 300), ("zouhe_mrt", 300), ("zouhe_reg", 300), ("cavity", 400),
+                  ("shear_capsule", 60)]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build absent")
+@pytest.mark.parametrize("name,steps", BOUNDARY_CASES)
+def test_oracle_boundaries_match_live_reference(oracle_mod, name, steps):
+    """Zou-He inlet / outlet (zou_he_boundary.cpp), closed box, moving walls
+    (moving_wall.cpp): the restatement against the reference's own
+    LBMSolver, bit for bit."""
+    case = CASES[name]
+    a = build_oracle(case, "sfo")
+    b = build_oracle(case, "ref")
+    a.step(steps)
+    b.step(steps)
+    for k in ("f", "ux", "uy", "rho", "positions", "velocities"):
+        assert np.array_equal(getattr(a, k)(), getattr(b, k)()), k
