@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define SFG_ABI_VERSION 1
+#define SFG_ABI_VERSION 2
 
 enum sfg_status {
     SFG_OK = 0,
@@ -53,8 +53,9 @@ enum sfg_collision { SFG_BGK = 0, SFG_MRT = 1, SFG_REGULARIZED = 2 };
 enum sfg_membrane_model { SFG_HOOKEAN = 0, SFG_NEO_HOOKEAN = 1, SFG_SKALAK = 2, SFG_WLC = 3 };
 
 /* Channel parameters: the fields of the reference SimulationParams that the
- * path reads (src/core/parameters.h:41-342), for a channel periodic in x
- * with SOLID rows 0 and ny-1 (or periodic in y). */
+ * path reads (src/core/parameters.h:41-342): SOLID rows 0 and ny-1 (or
+ * periodic in y); periodic in x, a Zou-He inlet / outlet pair of columns,
+ * or SOLID columns (closed box). */
 typedef struct sfg_channel_params {
     int nx, ny;
     int collision;              /* sfg_collision                               */
@@ -72,7 +73,19 @@ typedef struct sfg_channel_params {
     double scalar_D;
     int scalar_periodic_y;
     double scalar_inlet;
+    /* fluid boundaries (FluidParams, parameters.h:44-46, 87-88):
+     * boundary_type is sfg_boundary; inlet_velocity is the centre-line
+     * speed of the parabolic Zou-He inlet profile, outlet_density the Zou-He
+     * outlet pressure (zou_he_boundary.cpp:17-85); moving top / bottom wall
+     * speeds along x (moving_wall.cpp:14-64).  Channels other than PERIODIC
+     * carry no capsules and no scalar here. */
+    int boundary_type;
+    double inlet_velocity, outlet_density;
+    double top_wall_velocity, bottom_wall_velocity;
 } sfg_channel_params;
+
+/* BoundaryType (reference core/types.h:58-62). */
+enum sfg_boundary { SFG_INLET_OUTLET = 0, SFG_PERIODIC = 1, SFG_CLOSED = 2 };
 
 /* Membrane parameters (reference MembraneParams, parameters.h:82-136). */
 typedef struct sfg_membrane_params {

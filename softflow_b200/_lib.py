@@ -32,6 +32,9 @@ class ChannelParamsC(C.Structure):
         ("rep_power", C.c_int), ("rep_damping_normal", C.c_double), ("rep_friction", C.c_double),
         ("scalar_enabled", C.c_int), ("scalar_D", C.c_double),
         ("scalar_periodic_y", C.c_int), ("scalar_inlet", C.c_double),
+        ("boundary_type", C.c_int), ("inlet_velocity", C.c_double),
+        ("outlet_density", C.c_double), ("top_wall_velocity", C.c_double),
+        ("bottom_wall_velocity", C.c_double),
     ]
 
 

@@ -69,7 +69,30 @@ struct ChannelDev {
     // learned multi-direct forcing
     int learned;                // 1: network seed + one sweep, plain sweeps as fallback
     float mdf_threshold;        // no-slip residual (lu/step) above which it falls back
+    // fluid boundaries: x columns as BoundaryType (0 Zou-He inlet / outlet,
+    // 1 periodic, 2 SOLID); Zou-He inlet centre-line speed and outlet
+    // density; moving top / bottom wall speeds (0 when at rest)
+    int bc_x;
+    int bc_active;              // needs the boundary-aware lattice kernel
+    double u_in, rho_out, u_top, u_bot;
 };
+
+// Cell types of a channel (reference CellType, core/types.h:48-56), as
+// LBMSolver::initialize sets them (lbm_solver.cpp:130-160): rows 0 and ny-1
+// SOLID unless periodic in y; Zou-He channels have an INLET column at x = 0
+// and an OUTLET column at x = nx-1 (rows 1..ny-2); closed boxes SOLID
+// columns 0 and nx-1.
+enum CellKind : int { CK_FLUID = 0, CK_SOLID = 1, CK_INLET = 2, CK_OUTLET = 3 };
+__host__ __device__ __forceinline__ int cell_kind(const ChannelDev& ch, int x, int y) {
+    if (y == 0 || y == ch.ny - 1) return ch.periodic_y ? CK_FLUID : CK_SOLID;
+    if (ch.bc_x == 0) {
+        if (x == 0) return CK_INLET;
+        if (x == ch.nx - 1) return CK_OUTLET;
+    } else if (ch.bc_x == 2) {
+        if (x == 0 || x == ch.nx - 1) return CK_SOLID;
+    }
+    return CK_FLUID;
+}
 
 // Per-capsule constants (reference Capsule members, capsule.h:77-142).
 struct CapsuleDev {
@@ -86,7 +109,7 @@ struct CapsuleDev {
 constexpr int THERMO_THREADS = 256;
 struct ThermoPart {
     double sum_rho, min_rho, max_rho, max_v2, sum_vel, ke, sum_c;
-    long long count, first_bad;
+    long long count, first_bad, fluid;
 };
 constexpr long long THERMO_NONE = 0x7fffffffffffffffLL;
 
@@ -95,6 +118,7 @@ __device__ __forceinline__ void thermo_init(ThermoPart& p) {
     p.min_rho = 1e30;
     p.max_rho = -1e30;
     p.count = 0;
+    p.fluid = 0;
     p.first_bad = THERMO_NONE;
 }
 
@@ -108,6 +132,7 @@ __device__ __forceinline__ void thermo_merge(ThermoPart& a, const ThermoPart& b)
     if (b.max_rho > a.max_rho) a.max_rho = b.max_rho;
     if (b.max_v2 > a.max_v2) a.max_v2 = b.max_v2;
     a.count += b.count;
+    a.fluid += b.fluid;
     if (b.first_bad < a.first_bad) a.first_bad = b.first_bad;
 }
 

@@ -173,6 +173,9 @@ struct sfg_context {
     RowItem* d_items4 = nullptr;
     int n_items4 = 0;
     bool use_vec4 = false;
+    bool any_bc = false;                // boundary-aware lattice kernel in use
+    RowItem* d_zh_rows = nullptr;       // Zou-He rows (channel, y)
+    int n_zh = 0;
     void* f[2] = {nullptr, nullptr};
     void* g[2] = {nullptr, nullptr};
     void* cfield = nullptr;
@@ -309,6 +312,8 @@ static void free_all(sfg_context* c) {
     F(c->d_phi); F(c->d_stepped); F(c->d_adr_pending); F(c->d_c_fresh); F(c->d_status);
     F(c->d_step_ctr);
     F(c->d_io);
+    F(c->d_zh_rows);
+    c->d_zh_rows = nullptr;
     F(c->d_thermo_parts); F(c->d_cap_stats); F(c->d_thermo);
     if (c->h_thermo) cudaFreeHost(c->h_thermo);
     if (c->h_cap_stats) cudaFreeHost(c->h_cap_stats);
@@ -339,6 +344,19 @@ extern "C" int sfg_add_channel(sfg_context* c, const sfg_channel_params* p, int*
     if (p->scalar_enabled && !(p->scalar_D > 0.0))
         return fail(SFG_ERR_ARG, "sfg_add_channel: scalar diffusivity must be positive");
     if (p->rep_r_cut <= 0.0) return fail(SFG_ERR_ARG, "sfg_add_channel: r_cut must be positive");
+    if (p->boundary_type < 0 || p->boundary_type > 2)
+        return fail(SFG_ERR_ARG, "sfg_add_channel: unknown boundary type");
+    if (p->boundary_type == SFG_INLET_OUTLET && p->ny < 3)
+        return fail(SFG_ERR_ARG, "sfg_add_channel: a Zou-He channel needs ny >= 3");
+    if (p->boundary_type == SFG_INLET_OUTLET && !(p->outlet_density > 0.0))
+        return fail(SFG_ERR_ARG, "sfg_add_channel: outlet density must be positive");
+    {
+        const bool moving = std::fabs(p->top_wall_velocity) > 1e-15 ||
+                            std::fabs(p->bottom_wall_velocity) > 1e-15;
+        if (p->scalar_enabled && (p->boundary_type != SFG_PERIODIC || moving))
+            return fail(SFG_ERR_ARG, "sfg_add_channel: the scalar is supported on periodic "
+                                     "channels with resting walls only");
+    }
     ChanHost h;
     h.p = *p;
     c->ch.push_back(h);
@@ -355,6 +373,8 @@ extern "C" int sfg_add_capsule(sfg_context* c, int channel, const sfg_membrane_p
     if (c->initialized) return fail(SFG_ERR_STATE, "sfg_add_capsule: context already initialized");
     if (channel < 0 || channel >= (int)c->ch.size())
         return fail(SFG_ERR_ARG, "sfg_add_capsule: bad channel");
+    if (c->ch[channel].p.boundary_type != SFG_PERIODIC)
+        return fail(SFG_ERR_ARG, "sfg_add_capsule: capsules need a channel periodic in x");
     if (rest->num_nodes < 3) return fail(SFG_ERR_ARG, "sfg_add_capsule: need >= 3 nodes");
     if (mp->use_helfrich && (!rest_ang || !rest_ds))
         return fail(SFG_ERR_ARG, "sfg_add_capsule: Helfrich bending needs rest angles");
@@ -400,12 +420,13 @@ extern "C" int sfg_initialize(sfg_context* c) {
     const int nch = (int)c->ch.size();
     long long cell_off = 0;
     int tile_base = 0, cell_base = 0, cap_base = 0, mk_base = 0;
-    std::vector<RowItem> items, items4;
+    std::vector<RowItem> items, items4, zh_rows;
     std::vector<CapsuleDev> caps;
     bool all_vec4 = true;
     std::vector<double> pos, rest_len, rest_ang, rest_ds;
     std::vector<int> mk_cap, mk_chan, tile_chan;
     c->any_adr = false;
+    c->any_bc = false;
     c->maxn = 0;
     c->Kmax = 1;
     for (int ci = 0; ci < nch; ++ci) {
@@ -443,6 +464,14 @@ extern "C" int sfg_initialize(sfg_context* c) {
             d.F_uni_y = fy;
         }
         d.dt = p.dt;
+        d.bc_x = p.boundary_type;
+        d.u_in = p.inlet_velocity;
+        d.rho_out = p.outlet_density;
+        d.u_top = p.top_wall_velocity;
+        d.u_bot = p.bottom_wall_velocity;
+        d.bc_active = (p.boundary_type != SFG_PERIODIC ||
+                       (!p.periodic_y && (std::fabs(p.top_wall_velocity) > 1e-15 ||
+                                          std::fabs(p.bottom_wall_velocity) > 1e-15))) ? 1 : 0;
         d.adr = p.scalar_enabled ? 1 : 0;
         d.adr_periodic_y = p.scalar_periodic_y ? 1 : 0;
         d.omega_s = 1.0 / (3.0 * p.scalar_D + 0.5);
@@ -521,7 +550,12 @@ extern "C" int sfg_initialize(sfg_context* c) {
         for (int y = y0; y < y1; ++y)
             for (int x0 = 0; x0 < p.nx; x0 += VEC_RUN)
                 items4.push_back({ci, y, x0, std::min(VEC_RUN, p.nx - x0)});
-        h.fluid_cells = (long long)p.nx * (y1 - y0);
+        h.fluid_cells = 0;
+        for (int y = 0; y < p.ny; ++y)
+            for (int x = 0; x < p.nx; ++x) h.fluid_cells += cell_kind(d, x, y) == CK_FLUID;
+        if (d.bc_active) c->any_bc = true;
+        if (d.bc_x == SFG_INLET_OUTLET)
+            for (int y = 1; y < p.ny - 1; ++y) zh_rows.push_back({ci, y, 0, 1});
         h.d = d;
     }
     c->M = mk_base;
@@ -540,7 +574,16 @@ extern "C" int sfg_initialize(sfg_context* c) {
     CU(cudaMemcpy(c->d_chans, dch.data(), sizeof(ChannelDev) * nch, cudaMemcpyHostToDevice));
     CU(dalloc(&c->d_items, items.size()));
     CU(cudaMemcpy(c->d_items, items.data(), sizeof(RowItem) * items.size(), cudaMemcpyHostToDevice));
-    c->use_vec4 = all_vec4 && !c->force_scalar_lattice;
+    c->use_vec4 = all_vec4 && !c->force_scalar_lattice && !c->any_bc;
+    if (c->any_bc && c->any_adr)
+        return fail(SFG_ERR_ARG, "sfg_initialize: the scalar cannot share a context with "
+                                 "Zou-He, closed or moving-wall channels");
+    c->n_zh = (int)zh_rows.size();
+    if (c->n_zh > 0) {
+        CU(dalloc(&c->d_zh_rows, zh_rows.size()));
+        CU(cudaMemcpy(c->d_zh_rows, zh_rows.data(), sizeof(RowItem) * zh_rows.size(),
+                      cudaMemcpyHostToDevice));
+    }
     c->shared_collision = c->ch[0].p.collision;
     for (const ChanHost& h : c->ch)
         if (h.p.collision != c->shared_collision) c->shared_collision = -1;
@@ -790,7 +833,9 @@ static int enqueue_step_t(sfg_context* c, int p) {
     LatticeLaunch L{c->d_items, c->n_items, c->d_chans, c->f[p], c->f[1 - p], c->g[p],
                     c->g[1 - p], c->cfield, c->d_stepped, c->d_adr_pending, c->d_c_fresh,
                     c->d_step_ctr, c->any_adr, c->d_items4, c->n_items4, c->use_vec4,
-                    c->persistent_ctas, c->shared_collision};
+                    c->persistent_ctas, c->shared_collision, c->any_bc, c->d_zh_rows,
+                    c->n_zh};
+    if (c->any_bc && c->n_zh > 0) launches += 1;
     TileViewArgs tv{c->M > 0 ? c->tb.tile_slot[p] : nullptr,
                     c->M > 0 ? c->tb.tile_slot[1 - p] : nullptr, c->tb.fin[p], c->tb.gsnap,
                     c->tb.fin[1 - p]};
@@ -1358,7 +1403,7 @@ __global__ void k_thermo_final(const ChannelDev* __restrict__ chans, int nch, in
         cap_n = capped[c];
         const double bx = 0.0 + ch.body_fx, by = 0.0 + ch.body_fy, Fm = ch.max_force;
         if (__dadd_rn(__dmul_rn(bx, bx), __dmul_rn(by, by)) > __dmul_rn(Fm, Fm))
-            cap_n += p.count - fluid_touched[c];
+            cap_n += p.fluid - fluid_touched[c];
     }
     t.capped_nodes = cap_n;
     out[c] = t;

@@ -272,6 +272,143 @@ k_lattice_step(const RowItem* __restrict__ items, int n_items, const ChannelDev*
 }
 
 // ---------------------------------------------------------------------------
+// Lattice step of contexts with fluid boundaries other than the periodic
+// channel with resting walls: Zou-He inlet / outlet columns, closed boxes,
+// moving top / bottom walls (reference lbm_solver.cpp:172-207 with
+// moving_wall.cpp:14-64 and the INLET / OUTLET cell types).  One cell per
+// thread, push scheme:
+//   * SOLID cells do nothing; INLET / OUTLET cells do not collide (the
+//     reference collides FLUID cells only) and push their populations as
+//     they are;
+//   * a population bound for a SOLID cell is reflected into the own cell
+//     (halfway bounce-back); bound for a moving wall row it loses
+//     2 w_q rho (e_q . u_wall) / cs^2, rho the cell's own density;
+//   * without periodic x a population leaving the lattice is dropped (the
+//     reference's pull falls back to the node itself there, and Zou-He
+//     overwrites exactly those populations afterwards: k_zou_he).
+// The working representation (f in FP64, f - w otherwise) reflects the same
+// way since w_q = w_opp(q).
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ R wall_correction(int q, R rho, double vel) {
+    // 2.0 * w[q] * rho * eu_wall / cs2 in the reference's order
+    const R eu = R((double)cx_of(q) * vel);
+    const R cs2 = R(1.0) / R(3.0);
+    return R(2.0) * R(w_of(q)) * rho * eu / cs2;
+}
+
+template <typename S, typename R>
+__global__ void __launch_bounds__(256)
+k_lattice_step_bc(const RowItem* __restrict__ items, int n_items,
+                  const ChannelDev* __restrict__ chans, const S* __restrict__ src,
+                  S* __restrict__ dst, TileView tv, const int* __restrict__ stepped,
+                  const unsigned* __restrict__ step_ctr) {
+    const int item = blockIdx.x * ITEMS_PER_CTA + (threadIdx.x >> 5);
+    if (item >= n_items) return;
+    const RowItem it = items[item];
+    const int lane = threadIdx.x & 31;
+    if (lane >= it.len) return;
+    const ChannelDev& ch = chans[it.chan];
+    const int nx = ch.nx, ny = ch.ny, pitch = ch.pitch, plane = (int)ch.plane;
+    const int x = it.x0 + lane, y = it.y;
+    const int kind = cell_kind(ch, x, y);
+    if (kind == CK_SOLID) return;
+    const int n = y * pitch + x;
+    const S* __restrict__ fs = src + ch.f_off + n;
+    R f[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) f[q] = PopIO<S, R>::ld(fs + q * plane, q);
+    R rho, jx, jy;
+    lattice_moments(f, rho, jx, jy);
+    if (kind == CK_FLUID) {
+        const CellForces<R> cf = cell_forces<R>(ch, x, y, tv, stepped[it.chan]);
+        R ux, uy;
+        cell_velocity(rho, jx, jy, cf.Gx, cf.Gy, ux, uy);
+        const int coll = ch.collision;
+        if (coll == 2) {
+            collide_regularized(f, rho, ux, uy, cf.Fx, cf.Fy, R(ch.omega));
+        } else if (coll == 1) {
+            collide_mrt(f, rho, ux, uy, cf.Fx, cf.Fy, R(ch.omega), R(ch.mrt_se),
+                        R(ch.mrt_s_eps), R(ch.mrt_sq));
+        } else {
+            collide_bgk(f, rho, ux, uy, cf.Fx, cf.Fy, R(ch.omega));
+        }
+    }
+    const uint32_t seed = mix32((uint32_t)(ch.cell_off + n) ^ mix32(*step_ctr + 0x51ED270Bu));
+    S* __restrict__ fd = dst + ch.f_off;
+    const bool per_x = ch.bc_x == 1;
+    const bool mw_bot = !ch.periodic_y && fabs(ch.u_bot) > 1e-15;
+    const bool mw_top = !ch.periodic_y && fabs(ch.u_top) > 1e-15;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        int xt = x + cx_of(q), yt = y + cy_of(q);
+        if (per_x) xt = xt < 0 ? xt + nx : (xt >= nx ? xt - nx : xt);
+        else if (xt < 0 || xt >= nx) continue;
+        if (ch.periodic_y) yt = yt < 0 ? yt + ny : (yt >= ny ? yt - ny : yt);
+        if (cell_kind(ch, xt, yt) == CK_SOLID) {
+            R v = f[q];
+            if (yt == 0 && mw_bot) v = v - wall_correction<R>(q, rho, ch.u_bot);
+            else if (yt == ny - 1 && mw_top) v = v - wall_correction<R>(q, rho, ch.u_top);
+            PopIO<S, R>::st_sr(fd + opp_of(q) * plane + n, opp_of(q), v, seed);
+        } else {
+            PopIO<S, R>::st_sr(fd + q * plane + yt * pitch + xt, q, f[q], seed);
+        }
+    }
+}
+
+// Zou-He velocity inlet (parabolic profile) at x = 0 and pressure outlet at
+// x = nx-1 on the streamed populations (reference zou_he_boundary.cpp:17-85),
+// one thread per row item (chan, y).  The expressions keep the reference's
+// order; in FP32 arithmetic they act on deviations f - w, where the known
+// weights sum to 1 and opposite weights cancel.
+template <typename S, typename R>
+__global__ void k_zou_he(const RowItem* __restrict__ rows, int n_rows,
+                         const ChannelDev* __restrict__ chans, S* __restrict__ dst,
+                         const unsigned* __restrict__ step_ctr) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_rows) return;
+    const RowItem it = rows[i];
+    const ChannelDev& ch = chans[it.chan];
+    const int y = it.y, ny = ch.ny, plane = (int)ch.plane;
+    const R base = sizeof(R) == sizeof(double) ? R(0) : R(1);
+    S* __restrict__ fd = dst + ch.f_off;
+    const uint32_t seed = mix32((uint32_t)(ch.cell_off + y) ^ mix32(*step_ctr + 0x2E5BF271u));
+    {   // inlet
+        const int n = y * ch.pitch;
+        R f0 = PopIO<S, R>::ld(fd + 0 * plane + n, 0), f2 = PopIO<S, R>::ld(fd + 2 * plane + n, 2);
+        R f3 = PopIO<S, R>::ld(fd + 3 * plane + n, 3), f4 = PopIO<S, R>::ld(fd + 4 * plane + n, 4);
+        R f6 = PopIO<S, R>::ld(fd + 6 * plane + n, 6), f7 = PopIO<S, R>::ld(fd + 7 * plane + n, 7);
+        const double y_center = (double)ny * 0.5;
+        const double H = (double)(ny - 2);
+        const double y_norm = ((double)y - y_center) / (H * 0.5);
+        const R ux = R(ch.u_in * (1.0 - y_norm * y_norm));
+        const R uy = R(0);
+        const R rho = (base + (f0 + f2 + f4 + R(2.0) * (f3 + f6 + f7))) / (R(1.0) - ux);
+        const R f1 = f3 + (R(2.0) / R(3.0)) * rho * ux;
+        const R f5 = f7 + R(0.5) * (f4 - f2) + (R(1.0) / R(6.0)) * rho * ux + R(0.5) * rho * uy;
+        const R f8 = f6 - R(0.5) * (f4 - f2) + (R(1.0) / R(6.0)) * rho * ux - R(0.5) * rho * uy;
+        PopIO<S, R>::st_sr(fd + 1 * plane + n, 1, f1, seed);
+        PopIO<S, R>::st_sr(fd + 5 * plane + n, 5, f5, seed ^ 0x5bd1e995u);
+        PopIO<S, R>::st_sr(fd + 8 * plane + n, 8, f8, seed ^ 0x27d4eb2fu);
+    }
+    {   // outlet
+        const int n = y * ch.pitch + ch.nx - 1;
+        const R rho = R(ch.rho_out);
+        R f0 = PopIO<S, R>::ld(fd + 0 * plane + n, 0), f1 = PopIO<S, R>::ld(fd + 1 * plane + n, 1);
+        R f2 = PopIO<S, R>::ld(fd + 2 * plane + n, 2), f4 = PopIO<S, R>::ld(fd + 4 * plane + n, 4);
+        R f5 = PopIO<S, R>::ld(fd + 5 * plane + n, 5), f8 = PopIO<S, R>::ld(fd + 8 * plane + n, 8);
+        const R ux = R(-1.0) + (base + (f0 + f2 + f4 + R(2.0) * (f1 + f5 + f8))) / rho;
+        const R uy = R(0);
+        const R f3 = f1 - (R(2.0) / R(3.0)) * rho * ux;
+        const R f7 = f5 - R(0.5) * (f4 - f2) - (R(1.0) / R(6.0)) * rho * ux - R(0.5) * rho * uy;
+        const R f6 = f8 + R(0.5) * (f4 - f2) - (R(1.0) / R(6.0)) * rho * ux + R(0.5) * rho * uy;
+        PopIO<S, R>::st_sr(fd + 3 * plane + n, 3, f3, seed ^ 0x165667b1u);
+        PopIO<S, R>::st_sr(fd + 7 * plane + n, 7, f7, seed ^ 0xd3a2646cu);
+        PopIO<S, R>::st_sr(fd + 6 * plane + n, 6, f6, seed ^ 0xfd7046c5u);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Vectorised lattice step: each lane owns 4 consecutive cells of a row, loads
 // every population plane with one aligned vector load (16 B for FP32, 8 B for
 // FP16-shifted, 2 x 16 B for FP64), collides the 4 cells, and stores.  Planes
@@ -770,8 +907,10 @@ template <typename S, typename R>
 __device__ __forceinline__ bool cell_macro(const S* __restrict__ in, const ChannelDev& ch,
                                            const TileView& tv_last, int stepped, int x, int y,
                                            R& rho, R& ux, R& uy, R& Fx, R& Fy) {
-    const bool solid = !ch.periodic_y && (y == 0 || y == ch.ny - 1);
-    // last step's force (the "cur" tile set of that step)
+    const int kind = cell_kind(ch, x, y);
+    const bool solid = kind == CK_SOLID;
+    // last step's force (the "cur" tile set of that step); the body force
+    // is on FLUID cells only (simulation.cpp:556-560)
     if (!stepped) {
         Fx = R(0);
         Fy = R(0);
@@ -779,7 +918,7 @@ __device__ __forceinline__ bool cell_macro(const S* __restrict__ in, const Chann
         CellForces<R> cf = cell_forces<R>(ch, x, y, tv_last, 1);
         Fx = cf.Fx;
         Fy = cf.Fy;
-        if (solid) {
+        if (kind != CK_FLUID) {
             bool touched = false;
             if (ch.cap_end > ch.cap_begin && tv_last.cur_slot != nullptr) {
                 const int t = ch.tile_base + (y / TILE_H) * ch.tiles_x + (x / TILE_W);
@@ -853,6 +992,7 @@ k_thermo_cells(const S* __restrict__ in, const R* __restrict__ g, const ChannelD
         const int y = (int)(i / ch.nx), x = (int)(i % ch.nx);
         R rho, ux, uy, Fx, Fy;
         if (!cell_macro<S, R>(in, ch, tv_last, stepped, x, y, rho, ux, uy, Fx, Fy)) {
+            if (cell_kind(ch, x, y) == CK_FLUID) ++p.fluid;
             const double r = (double)rho, vx = (double)ux, vy = (double)uy;
             if (isnan(r) || isinf(r) || isnan(vx) || isinf(vx) || isnan(vy) || isinf(vy))
                 if (i < p.first_bad) p.first_bad = i;

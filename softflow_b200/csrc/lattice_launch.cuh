@@ -41,6 +41,20 @@ static void launch_step4_coll(const LatticeLaunch& L, const TileViewArgs& tv, in
 
 template <typename S, typename R>
 void launch_lattice_step(const LatticeLaunch& L, const TileViewArgs& tv, cudaStream_t st) {
+    if (L.any_bc) {
+        // boundary-aware kernel (no scalar transport in such contexts), then
+        // the Zou-He columns on the streamed populations
+        if (L.n_items == 0) return;
+        k_lattice_step_bc<S, R><<<(L.n_items + ITEMS_PER_CTA - 1) / ITEMS_PER_CTA,
+                                  32 * ITEMS_PER_CTA, 0, st>>>(
+            L.items, L.n_items, L.chans, static_cast<const S*>(L.src), static_cast<S*>(L.dst),
+            to_view(tv), L.stepped, L.step_ctr);
+        if (L.n_zh > 0)
+            k_zou_he<S, R><<<(L.n_zh + 127) / 128, 128, 0, st>>>(L.zh_rows, L.n_zh, L.chans,
+                                                                 static_cast<S*>(L.dst),
+                                                                 L.step_ctr);
+        return;
+    }
     if (L.use_vec4) {
         if (L.n_items4 == 0) return;
         const int grid = std::max(1, std::min(L.persistent_ctas,

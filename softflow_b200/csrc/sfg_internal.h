@@ -125,6 +125,9 @@ struct LatticeLaunch {
     bool use_vec4;              // every channel has nx % 4 == 0
     int persistent_ctas;        // grid of the persistent vectorised kernel
     int collision;              // shared collision model of all channels, -1 if mixed
+    bool any_bc = false;        // some channel has Zou-He / closed columns or moving walls
+    const RowItem* zh_rows = nullptr;  // (channel, y) rows of the Zou-He columns
+    int n_zh = 0;
 };
 struct TileViewArgs {
     const int* cur_slot;

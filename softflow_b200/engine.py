@@ -76,6 +76,10 @@ class FluidParams:
     mrt_s_eps: float = 1.4
     mrt_sq: float = 1.4
     periodic_y: bool = False
+    inlet_velocity: float = 0.02
+    outlet_density: float = 1.0
+    top_wall_velocity: float = 0.0
+    bottom_wall_velocity: float = 0.0
 
 
 @dataclass
@@ -173,10 +177,6 @@ class SimulationParams:
 
     def to_c(self) -> L.ChannelParamsC:
         f = self.fluid
-        if f.boundary_type != BoundaryType.PERIODIC:
-            raise NotImplementedError(
-                "only BoundaryType.PERIODIC channels are on this path (Zou-He inlet/outlet "
-                "and closed boxes are not implemented)")
         coll = CollisionModel.MRT if f.use_mrt else CollisionModel(f.collision_model)
         if self.scalar.enabled and self.scalar.n_species != 1:
             raise NotImplementedError("one scalar species is supported")
@@ -193,7 +193,10 @@ class SimulationParams:
             scalar_D=(self.scalar.diffusivity[0] if self.scalar.diffusivity else 0.01),
             scalar_periodic_y=int(bool(self.scalar.periodic_y)),
             scalar_inlet=(self.scalar.inlet_concentration[0]
-                          if self.scalar.inlet_concentration else 0.0))
+                          if self.scalar.inlet_concentration else 0.0),
+            boundary_type=int(f.boundary_type), inlet_velocity=f.inlet_velocity,
+            outlet_density=f.outlet_density, top_wall_velocity=f.top_wall_velocity,
+            bottom_wall_velocity=f.bottom_wall_velocity)
 
 
 @dataclass

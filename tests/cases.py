@@ -132,7 +132,10 @@ def gpu_params(case, precision):
     p.dt = sp["dt"]
     p.ibm_iterations = sp["ibm_iterations"]
     p.max_lattice_force = sp["max_lattice_force"]
-    p.fluid.boundary_type = S.BoundaryType.PERIODIC
+    p.fluid.boundary_type = S.BoundaryType(sp["boundary_type"])
+    p.fluid.inlet_velocity, p.fluid.outlet_density = sp["inlet_velocity"], sp["outlet_density"]
+    p.fluid.top_wall_velocity = sp["top_wall_velocity"]
+    p.fluid.bottom_wall_velocity = sp["bottom_wall_velocity"]
     p.fluid.tau, p.fluid.rho0 = sp["tau"], sp["rho0"]
     p.fluid.collision_model = S.CollisionModel(sp["collision"])
     p.fluid.mrt_se, p.fluid.mrt_s_eps, p.fluid.mrt_sq = sp["mrt_se"], sp["mrt_s_eps"], sp["mrt_sq"]
