@@ -45,7 +45,7 @@ class _Params(C.Structure):
         ("scalar_periodic_y", C.c_int), ("scalar_inlet", C.c_double),
         ("boundary_type", C.c_int), ("inlet_velocity", C.c_double),
         ("outlet_density", C.c_double), ("top_wall_velocity", C.c_double),
-        ("bottom_wall_velocity", C.c_double),
+        ("bottom_wall_velocity", C.c_double), ("use_interpolated_bb", C.c_int),
     ]
 
 
@@ -92,6 +92,7 @@ class ChannelSpec:
     outlet_density: float = 1.0
     top_wall_velocity: float = 0.0
     bottom_wall_velocity: float = 0.0
+    use_interpolated_bb: int = 0
 
     def to_c(self) -> _Params:
         return _Params(**{f.name: getattr(self, f.name) for f in fields(self)})
@@ -149,6 +150,9 @@ def _load(path: str, prefix: str):
                                          C.POINTER(_Membrane), C.c_int, C.c_int, C.c_double,
                                          C.c_int, C.c_int]),
         "initialize": (None, [C.c_void_p]),
+        "add_circle_pillar": (None, [C.c_void_p, C.c_double, C.c_double, C.c_double]),
+        "add_rect_pillar": (None, [C.c_void_p, C.c_double, C.c_double, C.c_double,
+                                   C.c_double]),
         "step": (None, [C.c_void_p, C.c_int]),
         "num_capsules": (C.c_int, [C.c_void_p]),
         "num_markers": (C.c_int, [C.c_void_p]),
@@ -237,6 +241,12 @@ class OracleSim:
         return self._fn["add_capsule_random"](self._h, count, x0, y0, x1, y1, rmin, rmax, nn,
                                               C.byref(mc), type_, seed, min_gap, max_attempts,
                                               int(check_walls))
+
+    def add_circle_pillar(self, cx, cy, r):
+        self._fn["add_circle_pillar"](self._h, cx, cy, r)
+
+    def add_rect_pillar(self, x0, y0, x1, y1):
+        self._fn["add_rect_pillar"](self._h, x0, y0, x1, y1)
 
     def initialize(self):
         self._fn["initialize"](self._h)

@@ -19,6 +19,7 @@
 #include "membrane/capsule_system.h"
 #include "membrane/repulsion.h"
 #include "io/vtk_writer.h"
+#include "geometry/channel_builder.h"
 #include "io/global_stats_writer.h"
 
 #include <omp.h>
@@ -44,6 +45,7 @@ struct RefSim {
     std::vector<double> pos, vel, frc, prev_len;
     std::vector<int> offsets;
     std::vector<double> C_mirror;
+    std::unique_ptr<ChannelBuilder> builder;   // Simulation::setChannelBuilder
 };
 
 MembraneParams to_mp(const sf_membrane* m) {
@@ -109,6 +111,7 @@ void* sfr_create(const sf_params* in) {
     p.fluid.outlet_density = in->outlet_density;
     p.fluid.top_wall_velocity = in->top_wall_velocity;
     p.fluid.bottom_wall_velocity = in->bottom_wall_velocity;
+    p.fluid.use_interpolated_bb = in->use_interpolated_bb != 0;
     p.fluid.periodic_y = in->periodic_y != 0;
     p.fluid.body_force_x = in->body_fx;
     p.fluid.body_force_y = in->body_fy;
@@ -183,9 +186,27 @@ int sfr_add_capsule_random(void* h, int count, double x0, double y0, double x1, 
     return placed;
 }
 
+void sfr_add_circle_pillar(void* h, double cx, double cy, double r) {
+    auto* s = static_cast<RefSim*>(h);
+    if (!s->builder) s->builder = std::make_unique<ChannelBuilder>(s->p.nx, s->p.ny);
+    s->builder->addCirclePillar(cx, cy, r);
+}
+
+void sfr_add_rect_pillar(void* h, double x0, double y0, double x1, double y1) {
+    auto* s = static_cast<RefSim*>(h);
+    if (!s->builder) s->builder = std::make_unique<ChannelBuilder>(s->p.nx, s->p.ny);
+    s->builder->addRectPillar(x0, y0, x1, y1);
+}
+
 void sfr_initialize(void* h) {
     auto* s = static_cast<RefSim*>(h);
+    if (s->builder) {                          // simulation.cpp:430-434
+        s->builder->setBoundaryType(s->p.fluid.boundary_type);
+        s->builder->applyToField(s->lbm->field());
+    }
     s->lbm->initialize();                      // simulation.cpp:436
+    if (s->builder && s->p.fluid.use_interpolated_bb)   // :439-442
+        s->lbm->setObstacles(s->builder->getObstacles());
     if (s->adr) s->adr->initialize(0.0);       // :446-448
     if (s->p.fluid.boundary_type == BoundaryType::PERIODIC)
         s->caps.setPeriodicX(s->p.nx);             // :456-458

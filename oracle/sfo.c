@@ -45,8 +45,16 @@ typedef struct {
     int periodic_nx;
 } capsule_t;
 
+/* circle (a, b) radius c, or rectangle [a, c] x [b, d] */
+typedef struct { int rect; double a, b, c, d; } obstacle_t;
+typedef struct { int x, y, q; double qf; } ibb_link_t;
+
 struct sfo_sim {
     sf_params p;
+    int nobs;
+    obstacle_t obs[64];
+    int nlinks;
+    ibb_link_t* links;
     int nx, ny, N;
     double *f, *ftmp, *rho, *ux, *uy, *Fx, *Fy;
     int* flags;
@@ -85,6 +93,7 @@ void sf_params_default(sf_params* p) {
     p->outlet_density = 1.0;
     p->top_wall_velocity = 0.0;
     p->bottom_wall_velocity = 0.0;
+    p->use_interpolated_bb = 0;
 }
 
 /* Defaults of reference MembraneParams (parameters.h:82-136). */
@@ -169,7 +178,7 @@ void sfo_destroy(sfo_sim* s) {
     free(s->Fx); free(s->Fy); free(s->flags); free(s->g); free(s->gtmp); free(s->C);
     free(s->caps); free(s->pos); free(s->vel); free(s->frc);
     free(s->rest_len); free(s->rest_ang); free(s->rest_ds); free(s->prev_len);
-    free(s->offsets); free(s->pair_count); free(s->pair_list);
+    free(s->offsets); free(s->pair_count); free(s->pair_list); free(s->links);
     free(s);
 }
 
@@ -385,6 +394,88 @@ static void moving_walls(sfo_sim* s) {
     if (fabs(s->p.top_wall_velocity) > 1e-15) moving_wall_row(s, s->ny - 1, s->p.top_wall_velocity);
 }
 
+/* Obstacle::contains of CircleObstacle / RectObstacle
+ * (geometry/circle_obstacle.h:11-15, rect_obstacle.h:9-16). */
+static int obstacle_contains(const obstacle_t* o, double x, double y) {
+    if (o->rect) return x >= o->a && x <= o->c && y >= o->b && y <= o->d;
+    double dx = x - o->a, dy = y - o->b;
+    return (dx * dx + dy * dy) <= o->c * o->c;
+}
+
+void sfo_add_circle_pillar(sfo_sim* s, double cx, double cy, double radius) {
+    obstacle_t o = {0, cx, cy, radius, 0.0};
+    if (s->nobs < 64) s->obs[s->nobs++] = o;
+}
+
+void sfo_add_rect_pillar(sfo_sim* s, double x0, double y0, double x1, double y1) {
+    obstacle_t o = {1, x0 < x1 ? x0 : x1, y0 < y1 ? y0 : y1, x0 > x1 ? x0 : x1, y0 > y1 ? y0 : y1};
+    if (s->nobs < 64) s->obs[s->nobs++] = o;
+}
+
+/* InterpolatedBounceBack::initialize (interpolated_bounce_back.cpp:7-54):
+ * every link of a non-SOLID node into a SOLID node, with the wall distance
+ * found by bisection against the obstacles (1 where none is crossed). */
+static void ibb_build(sfo_sim* s) {
+    const int nx = s->nx, ny = s->ny;
+    s->nlinks = 0;
+    int cap = 64;
+    s->links = (ibb_link_t*)realloc(s->links, sizeof(ibb_link_t) * cap);
+    for (int y = 0; y < ny; ++y) {
+        for (int x = 0; x < nx; ++x) {
+            if (s->flags[y * nx + x] == CT_SOLID) continue;
+            for (int q = 1; q < Q; ++q) {
+                int xn = x + CX[q], yn = y + CY[q];
+                if (xn < 0 || xn >= nx || yn < 0 || yn >= ny) continue;
+                if (s->flags[yn * nx + xn] != CT_SOLID) continue;
+                double x0 = (double)x, y0 = (double)y, dx = (double)CX[q], dy = (double)CY[q];
+                double min_q = 1.0;
+                for (int k = 0; k < s->nobs; ++k) {
+                    double lo = 0.0, hi = 1.0;
+                    for (int it = 0; it < 20; ++it) {
+                        double mid = 0.5 * (lo + hi);
+                        double xm = x0 + mid * dx, ym = y0 + mid * dy;
+                        if (obstacle_contains(&s->obs[k], xm, ym)) hi = mid;
+                        else lo = mid;
+                    }
+                    if (hi < min_q) min_q = hi;
+                }
+                if (s->nlinks == cap) {
+                    cap *= 2;
+                    s->links = (ibb_link_t*)realloc(s->links, sizeof(ibb_link_t) * cap);
+                }
+                ibb_link_t l = {x, y, q, min_q};
+                s->links[s->nlinks++] = l;
+            }
+        }
+    }
+}
+
+/* InterpolatedBounceBack::apply (interpolated_bounce_back.cpp:56-96), links
+ * in their build order. */
+static void ibb_apply(sfo_sim* s) {
+    const int nx = s->nx, ny = s->ny, N = s->N;
+    const int pnx = s->p.boundary_type == BT_PERIODIC ? nx : 0;
+    for (int i = 0; i < s->nlinks; ++i) {
+        const ibb_link_t* l = &s->links[i];
+        int x = l->x, y = l->y, q = l->q, opp = OPP[q];
+        double qf = l->qf;
+        if (qf < 0.5) {
+            int xu = x - CX[q], yu = y - CY[q];
+            if (pnx > 0) xu = ((xu % pnx) + pnx) % pnx;
+            if (xu >= 0 && xu < nx && yu >= 0 && yu < ny) {
+                s->f[opp * N + y * nx + x] = 2.0 * qf * s->f[q * N + y * nx + x]
+                    + (1.0 - 2.0 * qf) * s->f[q * N + yu * nx + xu];
+            } else {
+                s->f[opp * N + y * nx + x] = s->f[q * N + y * nx + x];
+            }
+        } else {
+            double inv2q = 1.0 / (2.0 * qf);
+            s->f[opp * N + y * nx + x] = inv2q * s->f[q * N + y * nx + x]
+                + (1.0 - inv2q) * s->f[opp * N + y * nx + x];
+        }
+    }
+}
+
 /* Zou-He velocity inlet (parabolic profile) on the INLET column and
  * pressure outlet on the OUTLET column, in the order of the reference's
  * node lists (zou_he_boundary.cpp:17-85: inlet nodes, then outlet nodes,
@@ -431,6 +522,7 @@ static void lbm_step(sfo_sim* s) {
     stream(s);
     bounce_back(s);
     moving_walls(s);
+    if (s->nlinks > 0) ibb_apply(s);
     if (s->p.boundary_type == BT_INLET_OUTLET) zou_he(s);
     sfo_compute_macroscopic(s);
 }
@@ -1153,6 +1245,14 @@ void sfo_initialize(sfo_sim* s) {
     const int nx = s->nx, ny = s->ny, N = s->N;
     /* lbm_solver.cpp:130-170 */
     for (int n = 0; n < N; ++n) s->flags[n] = CT_FLUID;
+    /* ChannelBuilder::applyToField (channel_builder.cpp:6-36): pillars */
+    for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x)
+            for (int k = 0; k < s->nobs; ++k)
+                if (obstacle_contains(&s->obs[k], (double)x, (double)y)) {
+                    s->flags[y * nx + x] = CT_SOLID;
+                    break;
+                }
     for (int x = 0; x < nx; ++x) { s->flags[x] = CT_SOLID; s->flags[(ny - 1) * nx + x] = CT_SOLID; }
     if (s->p.boundary_type == BT_INLET_OUTLET) {
         for (int y = 1; y < ny - 1; ++y) {
@@ -1172,6 +1272,9 @@ void sfo_initialize(sfo_sim* s) {
     memset(s->Fx, 0, sizeof(double) * N);
     memset(s->Fy, 0, sizeof(double) * N);
     sfo_compute_macroscopic(s);
+    /* simulation.cpp:439-442: links only with a channel builder */
+    s->nlinks = 0;
+    if (s->nobs > 0 && s->p.use_interpolated_bb) ibb_build(s);
     /* advection_diffusion.cpp:46-57 with initial concentration 0 */
     memset(s->g, 0, sizeof(double) * N * Q);
     memset(s->C, 0, sizeof(double) * N);

@@ -63,6 +63,9 @@ typedef struct sf_params {
     int boundary_type;
     double inlet_velocity, outlet_density;
     double top_wall_velocity, bottom_wall_velocity;
+    /* Bouzidi interpolated bounce-back at obstacle links
+     * (FluidParams::use_interpolated_bb, parameters.h:89) */
+    int use_interpolated_bb;
 } sf_params;
 
 /* Membrane parameters (reference MembraneParams, circle shape only). */
@@ -83,6 +86,12 @@ void sf_membrane_default(sf_membrane* m);
 
 sfo_sim* sfo_create(const sf_params* p);
 void sfo_destroy(sfo_sim* s);
+
+/* Pillars of the channel geometry (ChannelBuilder::addCirclePillar /
+ * addRectPillar, geometry/channel_builder.h:25-33), before sfo_initialize.
+ * A channel with pillars has a ChannelBuilder in the reference's sense. */
+void sfo_add_circle_pillar(sfo_sim* s, double cx, double cy, double radius);
+void sfo_add_rect_pillar(sfo_sim* s, double x0, double y0, double x1, double y1);
 
 /* Capsule construction (reference capsule.cpp:7-141), returns its index. */
 int sfo_add_capsule(sfo_sim* s, double cx, double cy, double radius, int nn,

@@ -93,6 +93,21 @@ CASES = {
     "cavity": dict(spec=dict(nx=32, ny=32, collision=O.BGK, tau=0.7,
                              boundary_type=O.CLOSED, top_wall_velocity=0.05),
                    capsules=[], conc=None),
+    # pillars (ChannelBuilder): flow past a cylinder and a rectangle in a
+    # periodic channel and in a Zou-He channel, halfway and interpolated
+    # (Bouzidi) bounce-back
+    "pillars_bb": dict(spec=dict(nx=80, ny=30, collision=O.BGK, tau=0.8, body_fx=2e-5),
+                       capsules=[], conc=None,
+                       pillars=[("circle", 20.3, 14.6, 5.2), ("rect", 50.0, 8.0, 58.5, 20.0)]),
+    "pillars_ibb": dict(spec=dict(nx=80, ny=30, collision=O.REGULARIZED, tau=0.8, body_fx=2e-5,
+                                  use_interpolated_bb=1),
+                        capsules=[], conc=None,
+                        pillars=[("circle", 20.3, 14.6, 5.2), ("rect", 50.0, 8.0, 58.5, 20.0)]),
+    "pillars_zouhe": dict(spec=dict(nx=72, ny=28, collision=O.MRT, tau=0.7,
+                                    boundary_type=O.INLET_OUTLET, inlet_velocity=0.03,
+                                    use_interpolated_bb=1),
+                          capsules=[], conc=None,
+                          pillars=[("circle", 24.0, 13.3, 4.7), ("circle", 45.5, 9.0, 3.1)]),
     # plane Couette flow with a capsule (periodic x, walls moving apart)
     "shear_capsule": dict(spec=dict(nx=64, ny=34, collision=O.BGK, tau=0.8,
                                     top_wall_velocity=0.01, bottom_wall_velocity=-0.01,
@@ -109,6 +124,11 @@ CASES = {
 
 def build_oracle(case, impl="sfo"):
     s = O.OracleSim(O.ChannelSpec(**case["spec"]), impl)
+    for ob in case.get("pillars", []):
+        if ob[0] == "circle":
+            s.add_circle_pillar(*ob[1:])
+        else:
+            s.add_rect_pillar(*ob[1:])
     for c in case["capsules"]:
         if c[0] == "add":
             _, cx, cy, r, nn, mk = c

@@ -26,7 +26,8 @@ OUTPUT_RUNS = [("bgk_small", 300), ("seam_single", 40), ("diffusion", 200)]
 
 RUNS = [("bgk_small", 300), ("mrt_small", 300), ("reg_small", 300), ("mini_c2", 30),
         ("contact_brute", 60), ("seam_single", 40), ("c1", 10),
-        ("zouhe_bgk", 300), ("zouhe_reg", 300), ("cavity", 400), ("shear_capsule", 60)]
+        ("zouhe_bgk", 300), ("zouhe_reg", 300), ("cavity", 400), ("shear_capsule", 60),
+        ("pillars_ibb", 300), ("pillars_zouhe", 300)]
 
 
 def main():

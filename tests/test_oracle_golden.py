@@ -12,7 +12,7 @@ from cases import CASES, build_oracle, fluid_rows
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 NAMES = ["bgk_small", "mrt_small", "reg_small", "mini_c2", "contact_brute", "seam_single", "c1",
-         "zouhe_bgk", "zouhe_reg", "cavity", "shear_capsule"]
+         "zouhe_bgk", "zouhe_reg", "cavity", "shear_capsule", "pillars_ibb", "pillars_zouhe"]
 
 
 @pytest.mark.parametrize("name", NAMES)
@@ -116,4 +116,19 @@ def test_oracle_boundaries_match_live_reference(oracle_mod, name, steps):
     a.step(steps)
     b.step(steps)
     for k in ("f", "ux", "uy", "rho", "positions", "velocities"):
+        assert np.array_equal(getattr(a, k)(), getattr(b, k)()), k
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build absent")
+@pytest.mark.parametrize("name,steps", [("pillars_bb", 300), ("pillars_ibb", 300),
+                                        ("pillars_zouhe", 300)])
+def test_oracle_pillars_match_live_reference(oracle_mod, name, steps):
+    """ChannelBuilder pillars (channel_builder.cpp) with halfway and
+    interpolated bounce-back (interpolated_bounce_back.cpp): bit for bit."""
+    case = CASES[name]
+    a = build_oracle(case, "sfo")
+    b = build_oracle(case, "ref")
+    a.step(steps)
+    b.step(steps)
+    for k in ("f", "ux", "uy", "rho"):
         assert np.array_equal(getattr(a, k)(), getattr(b, k)()), k
