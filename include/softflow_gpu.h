@@ -82,6 +82,10 @@ typedef struct sfg_channel_params {
     int boundary_type;
     double inlet_velocity, outlet_density;
     double top_wall_velocity, bottom_wall_velocity;
+    /* Bouzidi interpolated bounce-back on the links of a channel with
+     * pillars (FluidParams::use_interpolated_bb, parameters.h:89;
+     * interpolated_bounce_back.cpp); no effect without pillars */
+    int use_interpolated_bb;
 } sfg_channel_params;
 
 /* BoundaryType (reference core/types.h:58-62). */
@@ -151,6 +155,17 @@ int sfg_add_channel(sfg_context* ctx, const sfg_channel_params* p, int* channel_
 int sfg_add_capsule(sfg_context* ctx, int channel, const sfg_membrane_params* mp,
                     const sfg_capsule_rest* rest, const double* pos, const double* rest_len,
                     const double* rest_ang, const double* rest_ds, int* capsule_out);
+
+/* Adds a pillar to a channel's geometry (before sfg_initialize): kind 0 a
+ * circle of centre (a, b) and radius c, kind 1 the rectangle spanned by
+ * (a, b) and (c, d).  Replaces ChannelBuilder::addCirclePillar /
+ * addRectPillar with Simulation::setChannelBuilder (geometry/
+ * channel_builder.h:25-33, simulation.cpp:211-213, 430-442): lattice nodes
+ * inside a pillar are SOLID (halfway bounce-back, or interpolated with
+ * use_interpolated_bb).  Channels with pillars carry no capsules here. */
+enum sfg_pillar { SFG_PILLAR_CIRCLE = 0, SFG_PILLAR_RECT = 1 };
+int sfg_add_pillar(sfg_context* ctx, int channel, int kind, double a, double b, double c,
+                   double d);
 
 /* Allocates device state and sets every channel to equilibrium at rho0 with
  * u = 0 (LBMSolver::initialize, lbm_solver.cpp:130-170; scalar initialised to

@@ -8,6 +8,7 @@ is the host-side mirror of the reference engine API.
 from .engine import (  # noqa: F401
     BoundaryType,
     CapsuleShape,
+    ChannelBuilder,
     CollisionModel,
     Ensemble,
     FluidParams,
@@ -22,7 +23,7 @@ from .engine import (  # noqa: F401
 from ._lib import SoftFlowGpuError, lib as load_library  # noqa: F401
 
 __all__ = [
-    "BoundaryType", "CapsuleShape", "CollisionModel", "Ensemble", "FluidParams",
+    "BoundaryType", "CapsuleShape", "ChannelBuilder", "CollisionModel", "Ensemble", "FluidParams",
     "MembraneModel", "MembraneParams", "RepulsionParams", "ScalarParams", "Simulation",
     "SimulationParams", "SoftFlowGpuError", "build_circle_capsule", "load_library",
 ]

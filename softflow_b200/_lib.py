@@ -34,7 +34,7 @@ class ChannelParamsC(C.Structure):
         ("scalar_periodic_y", C.c_int), ("scalar_inlet", C.c_double),
         ("boundary_type", C.c_int), ("inlet_velocity", C.c_double),
         ("outlet_density", C.c_double), ("top_wall_velocity", C.c_double),
-        ("bottom_wall_velocity", C.c_double),
+        ("bottom_wall_velocity", C.c_double), ("use_interpolated_bb", C.c_int),
     ]
 
 
@@ -147,6 +147,8 @@ SIGNATURES = {
                                     _P(C.c_longlong), _P(C.c_longlong)]),
     "sfg_autotune": (C.c_int, [C.c_void_p, C.c_int, _P(C.c_int)]),
     "sfg_thermo": (C.c_int, [C.c_void_p, _P(ThermoRecordC), _D]),
+    "sfg_add_pillar": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double,
+                                 C.c_double, C.c_double]),
     "sfg_write_vtk_fluid": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p, C.c_int, C.c_int,
                                       C.c_uint]),
     "sfg_write_vtk_capsules": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p, C.c_int, C.c_int,

@@ -75,15 +75,21 @@ struct ChannelDev {
     int bc_x;
     int bc_active;              // needs the boundary-aware lattice kernel
     double u_in, rho_out, u_top, u_bot;
+    const unsigned char* mask;  // device cell types [ny][nx] of a channel with
+                                // pillars, null otherwise
 };
 
 // Cell types of a channel (reference CellType, core/types.h:48-56), as
 // LBMSolver::initialize sets them (lbm_solver.cpp:130-160): rows 0 and ny-1
 // SOLID unless periodic in y; Zou-He channels have an INLET column at x = 0
 // and an OUTLET column at x = nx-1 (rows 1..ny-2); closed boxes SOLID
-// columns 0 and nx-1.
+// columns 0 and nx-1.  Channels with pillars read the types from a mask
+// built on the host (device code only; host code uses the mask array).
 enum CellKind : int { CK_FLUID = 0, CK_SOLID = 1, CK_INLET = 2, CK_OUTLET = 3 };
 __host__ __device__ __forceinline__ int cell_kind(const ChannelDev& ch, int x, int y) {
+#ifdef __CUDA_ARCH__
+    if (ch.mask != nullptr) return ch.mask[y * ch.nx + x];
+#endif
     if (y == 0 || y == ch.ny - 1) return ch.periodic_y ? CK_FLUID : CK_SOLID;
     if (ch.bc_x == 0) {
         if (x == 0) return CK_INLET;
@@ -103,6 +109,14 @@ struct CapsuleDev {
     double k_bend, k_area, k_perimeter, gamma_visc, eta_membrane;
     double rest_area, rest_perimeter;
     int periodic_nx;
+};
+
+// One interpolated bounce-back link (reference InterpolatedBounceBack::Link):
+// non-SOLID node (x, y) of channel chan whose direction q points into a
+// SOLID node, wall at the fraction qf of the link.
+struct IbbLink {
+    int chan, x, y, q;
+    double qf;
 };
 
 // Partial thermo sums of one block of cells (see k_thermo_cells).

@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/softflow_gpu.h"
@@ -39,12 +40,87 @@ struct CapsuleHost {
     std::vector<double> pos, rest_len, rest_ang, rest_ds;
 };
 
+struct Pillar {
+    int rect;            // 0 circle (a, b) radius c; 1 rectangle [a, c] x [b, d]
+    double a, b, c, d;
+};
+
 struct ChanHost {
     sfg_channel_params p;
     ChannelDev d;
     std::vector<CapsuleHost> caps;
+    std::vector<Pillar> pillars;
     long long fluid_cells = 0;
 };
+
+// Obstacle::contains of CircleObstacle / RectObstacle
+// (geometry/circle_obstacle.h:11-15, rect_obstacle.h:9-16).
+bool pillar_contains(const Pillar& o, double x, double y) {
+    if (o.rect) return x >= o.a && x <= o.c && y >= o.b && y <= o.d;
+    const double dx = x - o.a, dy = y - o.b;
+    return (dx * dx + dy * dy) <= o.c * o.c;
+}
+
+// Cell types of a channel with pillars: ChannelBuilder::applyToField
+// (channel_builder.cpp:6-36) followed by LBMSolver::initialize's rows and
+// columns (lbm_solver.cpp:130-160).
+std::vector<unsigned char> pillar_mask(const sfg_channel_params& p,
+                                       const std::vector<Pillar>& pillars) {
+    const int nx = p.nx, ny = p.ny;
+    std::vector<unsigned char> m((size_t)nx * ny, 0);
+    for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x)
+            for (const Pillar& o : pillars)
+                if (pillar_contains(o, (double)x, (double)y)) {
+                    m[(size_t)y * nx + x] = 1;
+                    break;
+                }
+    for (int x = 0; x < nx; ++x) m[x] = m[(size_t)(ny - 1) * nx + x] = 1;
+    if (p.boundary_type == SFG_INLET_OUTLET) {
+        for (int y = 1; y < ny - 1; ++y) {
+            m[(size_t)y * nx] = 2;
+            m[(size_t)y * nx + nx - 1] = 3;
+        }
+    } else if (p.boundary_type == SFG_CLOSED) {
+        for (int y = 0; y < ny; ++y) m[(size_t)y * nx] = m[(size_t)y * nx + nx - 1] = 1;
+    }
+    if (p.periodic_y)
+        for (int x = 0; x < nx; ++x) m[x] = m[(size_t)(ny - 1) * nx + x] = 0;
+    return m;
+}
+
+// InterpolatedBounceBack::initialize (interpolated_bounce_back.cpp:7-54):
+// links of non-SOLID nodes into SOLID nodes in (y, x, q) order, the wall
+// fraction by 20 bisection steps against every pillar (1 if none is hit).
+void build_ibb_links(int chan, const sfg_channel_params& p, const std::vector<unsigned char>& m,
+                     const std::vector<Pillar>& pillars, std::vector<IbbLink>& out) {
+    static const int CXh[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
+    static const int CYh[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
+    const int nx = p.nx, ny = p.ny;
+    for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x) {
+            if (m[(size_t)y * nx + x] == 1) continue;
+            for (int q = 1; q < 9; ++q) {
+                const int xn = x + CXh[q], yn = y + CYh[q];
+                if (xn < 0 || xn >= nx || yn < 0 || yn >= ny) continue;
+                if (m[(size_t)yn * nx + xn] != 1) continue;
+                const double x0 = (double)x, y0 = (double)y;
+                const double dx = (double)CXh[q], dy = (double)CYh[q];
+                double min_q = 1.0;
+                for (const Pillar& o : pillars) {
+                    double lo = 0.0, hi = 1.0;
+                    for (int it = 0; it < 20; ++it) {
+                        const double mid = 0.5 * (lo + hi);
+                        const double xm = x0 + mid * dx, ym = y0 + mid * dy;
+                        if (pillar_contains(o, xm, ym)) hi = mid;
+                        else lo = mid;
+                    }
+                    if (hi < min_q) min_q = hi;
+                }
+                out.push_back({chan, x, y, q, min_q});
+            }
+        }
+}
 
 __global__ void k_step_flags(const ChannelDev* __restrict__ chans, int nch, int* stepped,
                              int* adr_pending, int* c_fresh, unsigned* step_ctr,
@@ -176,6 +252,9 @@ struct sfg_context {
     bool any_bc = false;                // boundary-aware lattice kernel in use
     RowItem* d_zh_rows = nullptr;       // Zou-He rows (channel, y)
     int n_zh = 0;
+    unsigned char* d_masks = nullptr;   // cell types of channels with pillars
+    IbbLink* d_ibb = nullptr;           // interpolated bounce-back links by level
+    std::vector<int> ibb_level_start;   // [levels + 1]
     void* f[2] = {nullptr, nullptr};
     void* g[2] = {nullptr, nullptr};
     void* cfield = nullptr;
@@ -314,6 +393,10 @@ static void free_all(sfg_context* c) {
     F(c->d_io);
     F(c->d_zh_rows);
     c->d_zh_rows = nullptr;
+    F(c->d_masks);
+    F(c->d_ibb);
+    c->d_masks = nullptr;
+    c->d_ibb = nullptr;
     F(c->d_thermo_parts); F(c->d_cap_stats); F(c->d_thermo);
     if (c->h_thermo) cudaFreeHost(c->h_thermo);
     if (c->h_cap_stats) cudaFreeHost(c->h_cap_stats);
@@ -364,6 +447,28 @@ extern "C" int sfg_add_channel(sfg_context* c, const sfg_channel_params* p, int*
     return SFG_OK;
 }
 
+extern "C" int sfg_add_pillar(sfg_context* c, int channel, int kind, double a, double b,
+                              double cc, double d) {
+    if (!c) return fail(SFG_ERR_ARG, "sfg_add_pillar: null context");
+    if (c->initialized) return fail(SFG_ERR_STATE, "sfg_add_pillar: context already initialized");
+    if (channel < 0 || channel >= (int)c->ch.size())
+        return fail(SFG_ERR_ARG, "sfg_add_pillar: bad channel");
+    if (kind != SFG_PILLAR_CIRCLE && kind != SFG_PILLAR_RECT)
+        return fail(SFG_ERR_ARG, "sfg_add_pillar: unknown pillar kind");
+    if (!c->ch[channel].caps.empty())
+        return fail(SFG_ERR_ARG, "sfg_add_pillar: pillars cannot share a channel with capsules");
+    if (c->ch[channel].p.scalar_enabled)
+        return fail(SFG_ERR_ARG, "sfg_add_pillar: pillars cannot share a channel with the scalar");
+    Pillar o;
+    if (kind == SFG_PILLAR_CIRCLE) {
+        o = {0, a, b, cc, 0.0};
+    } else {   // RectObstacle normalises its corners (rect_obstacle.h:9-11)
+        o = {1, std::min(a, cc), std::min(b, d), std::max(a, cc), std::max(b, d)};
+    }
+    c->ch[channel].pillars.push_back(o);
+    return SFG_OK;
+}
+
 extern "C" int sfg_add_capsule(sfg_context* c, int channel, const sfg_membrane_params* mp,
                                const sfg_capsule_rest* rest, const double* pos,
                                const double* rest_len, const double* rest_ang,
@@ -375,6 +480,8 @@ extern "C" int sfg_add_capsule(sfg_context* c, int channel, const sfg_membrane_p
         return fail(SFG_ERR_ARG, "sfg_add_capsule: bad channel");
     if (c->ch[channel].p.boundary_type != SFG_PERIODIC)
         return fail(SFG_ERR_ARG, "sfg_add_capsule: capsules need a channel periodic in x");
+    if (!c->ch[channel].pillars.empty())
+        return fail(SFG_ERR_ARG, "sfg_add_capsule: capsules cannot share a channel with pillars");
     if (rest->num_nodes < 3) return fail(SFG_ERR_ARG, "sfg_add_capsule: need >= 3 nodes");
     if (mp->use_helfrich && (!rest_ang || !rest_ds))
         return fail(SFG_ERR_ARG, "sfg_add_capsule: Helfrich bending needs rest angles");
@@ -421,6 +528,9 @@ extern "C" int sfg_initialize(sfg_context* c) {
     long long cell_off = 0;
     int tile_base = 0, cell_base = 0, cap_base = 0, mk_base = 0;
     std::vector<RowItem> items, items4, zh_rows;
+    std::vector<unsigned char> masks;
+    std::vector<long long> mask_off;
+    std::vector<IbbLink> links;
     std::vector<CapsuleDev> caps;
     bool all_vec4 = true;
     std::vector<double> pos, rest_len, rest_ang, rest_ds;
@@ -551,8 +661,18 @@ extern "C" int sfg_initialize(sfg_context* c) {
             for (int x0 = 0; x0 < p.nx; x0 += VEC_RUN)
                 items4.push_back({ci, y, x0, std::min(VEC_RUN, p.nx - x0)});
         h.fluid_cells = 0;
-        for (int y = 0; y < p.ny; ++y)
-            for (int x = 0; x < p.nx; ++x) h.fluid_cells += cell_kind(d, x, y) == CK_FLUID;
+        if (!h.pillars.empty()) {
+            const std::vector<unsigned char> m = pillar_mask(p, h.pillars);
+            for (unsigned char k : m) h.fluid_cells += k == CK_FLUID;
+            mask_off.push_back((long long)masks.size());
+            masks.insert(masks.end(), m.begin(), m.end());
+            d.bc_active = 1;
+            if (p.use_interpolated_bb) build_ibb_links(ci, p, m, h.pillars, links);
+        } else {
+            mask_off.push_back(-1);
+            for (int y = 0; y < p.ny; ++y)
+                for (int x = 0; x < p.nx; ++x) h.fluid_cells += cell_kind(d, x, y) == CK_FLUID;
+        }
         if (d.bc_active) c->any_bc = true;
         if (d.bc_x == SFG_INLET_OUTLET)
             for (int y = 1; y < p.ny - 1; ++y) zh_rows.push_back({ci, y, 0, 1});
@@ -568,6 +688,60 @@ extern "C" int sfg_initialize(sfg_context* c) {
     if (c->maxn > 0) CU(prepare_membrane(c->maxn));
     CU(prepare_spread());
 
+    if (!masks.empty()) {
+        CU(dalloc(&c->d_masks, masks.size()));
+        CU(cudaMemcpy(c->d_masks, masks.data(), masks.size(), cudaMemcpyHostToDevice));
+        for (int i = 0; i < nch; ++i)
+            if (mask_off[i] >= 0) c->ch[i].d.mask = c->d_masks + mask_off[i];
+    }
+    c->ibb_level_start.clear();
+    if (!links.empty()) {
+        // levels: a link runs after every earlier link that writes what it
+        // reads or reads what it writes (the reference applies them in order)
+        std::unordered_map<long long, int> max_w, max_r;
+        std::vector<int> level(links.size());
+        int nlev = 0;
+        auto key = [&](const IbbLink& l, int x, int y, int q) {
+            return ((long long)l.chan << 40) | ((long long)(y * c->ch[l.chan].p.nx + x) << 4) | q;
+        };
+        static const int CXh[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
+        static const int CYh[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
+        static const int OPh[9] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
+        for (size_t i = 0; i < links.size(); ++i) {
+            const IbbLink& l = links[i];
+            const int nx = c->ch[l.chan].p.nx, ny = c->ch[l.chan].p.ny;
+            std::vector<long long> reads = {key(l, l.x, l.y, l.q), key(l, l.x, l.y, OPh[l.q])};
+            int xu = l.x - CXh[l.q];
+            const int yu = l.y - CYh[l.q];
+            if (c->ch[l.chan].p.boundary_type == SFG_PERIODIC) xu = ((xu % nx) + nx) % nx;
+            if (xu >= 0 && xu < nx && yu >= 0 && yu < ny) reads.push_back(key(l, xu, yu, l.q));
+            const long long w = key(l, l.x, l.y, OPh[l.q]);
+            int lv = 0;
+            for (long long r : reads) {
+                auto it = max_w.find(r);
+                if (it != max_w.end()) lv = std::max(lv, it->second + 1);
+            }
+            auto ir = max_r.find(w);
+            if (ir != max_r.end()) lv = std::max(lv, ir->second + 1);
+            auto iw = max_w.find(w);
+            if (iw != max_w.end()) lv = std::max(lv, iw->second + 1);
+            level[i] = lv;
+            nlev = std::max(nlev, lv + 1);
+            for (long long r : reads) max_r[r] = std::max(max_r.count(r) ? max_r[r] : 0, lv);
+            max_w[w] = lv;
+        }
+        std::vector<IbbLink> sorted;
+        sorted.reserve(links.size());
+        c->ibb_level_start.push_back(0);
+        for (int lv = 0; lv < nlev; ++lv) {
+            for (size_t i = 0; i < links.size(); ++i)
+                if (level[i] == lv) sorted.push_back(links[i]);
+            c->ibb_level_start.push_back((int)sorted.size());
+        }
+        CU(dalloc(&c->d_ibb, sorted.size()));
+        CU(cudaMemcpy(c->d_ibb, sorted.data(), sizeof(IbbLink) * sorted.size(),
+                      cudaMemcpyHostToDevice));
+    }
     std::vector<ChannelDev> dch(nch);
     for (int i = 0; i < nch; ++i) dch[i] = c->ch[i].d;
     CU(dalloc(&c->d_chans, nch));
@@ -834,8 +1008,10 @@ static int enqueue_step_t(sfg_context* c, int p) {
                     c->g[1 - p], c->cfield, c->d_stepped, c->d_adr_pending, c->d_c_fresh,
                     c->d_step_ctr, c->any_adr, c->d_items4, c->n_items4, c->use_vec4,
                     c->persistent_ctas, c->shared_collision, c->any_bc, c->d_zh_rows,
-                    c->n_zh};
+                    c->n_zh, c->d_ibb, c->ibb_level_start.data(),
+                    (int)c->ibb_level_start.size() - 1};
     if (c->any_bc && c->n_zh > 0) launches += 1;
+    if (c->any_bc && c->ibb_level_start.size() > 1) launches += (int)c->ibb_level_start.size() - 1;
     TileViewArgs tv{c->M > 0 ? c->tb.tile_slot[p] : nullptr,
                     c->M > 0 ? c->tb.tile_slot[1 - p] : nullptr, c->tb.fin[p], c->tb.gsnap,
                     c->tb.fin[1 - p]};

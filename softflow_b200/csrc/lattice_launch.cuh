@@ -49,6 +49,13 @@ void launch_lattice_step(const LatticeLaunch& L, const TileViewArgs& tv, cudaStr
                                   32 * ITEMS_PER_CTA, 0, st>>>(
             L.items, L.n_items, L.chans, static_cast<const S*>(L.src), static_cast<S*>(L.dst),
             to_view(tv), L.stepped, L.step_ctr);
+        for (int lv = 0; lv < L.n_ibb_levels; ++lv) {
+            const int a = L.ibb_level_start[lv], n = L.ibb_level_start[lv + 1] - a;
+            if (n > 0)
+                k_ibb<S, R><<<(n + 127) / 128, 128, 0, st>>>(L.ibb + a, n, L.chans,
+                                                             static_cast<S*>(L.dst),
+                                                             L.step_ctr);
+        }
         if (L.n_zh > 0)
             k_zou_he<S, R><<<(L.n_zh + 127) / 128, 128, 0, st>>>(L.zh_rows, L.n_zh, L.chans,
                                                                  static_cast<S*>(L.dst),

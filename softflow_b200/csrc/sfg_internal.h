@@ -128,6 +128,9 @@ struct LatticeLaunch {
     bool any_bc = false;        // some channel has Zou-He / closed columns or moving walls
     const RowItem* zh_rows = nullptr;  // (channel, y) rows of the Zou-He columns
     int n_zh = 0;
+    const IbbLink* ibb = nullptr;      // interpolated bounce-back links, by level
+    const int* ibb_level_start = nullptr;  // host array [n_ibb_levels + 1]
+    int n_ibb_levels = 0;
 };
 struct TileViewArgs {
     const int* cur_slot;

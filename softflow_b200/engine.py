@@ -80,6 +80,7 @@ class FluidParams:
     outlet_density: float = 1.0
     top_wall_velocity: float = 0.0
     bottom_wall_velocity: float = 0.0
+    use_interpolated_bb: bool = False
 
 
 @dataclass
@@ -196,7 +197,8 @@ class SimulationParams:
                           if self.scalar.inlet_concentration else 0.0),
             boundary_type=int(f.boundary_type), inlet_velocity=f.inlet_velocity,
             outlet_density=f.outlet_density, top_wall_velocity=f.top_wall_velocity,
-            bottom_wall_velocity=f.bottom_wall_velocity)
+            bottom_wall_velocity=f.bottom_wall_velocity,
+            use_interpolated_bb=int(bool(f.use_interpolated_bb)))
 
 
 @dataclass
@@ -247,11 +249,62 @@ def _centroid_periodic(pos: np.ndarray, nx: int):
     return sx / n, sy / n
 
 
+class ChannelBuilder:
+    """Channel geometry (reference ChannelBuilder, geometry/channel_builder.h:
+    14-62; bindings.cpp:634-654): circular and rectangular pillars.  Walls
+    and the boundary type come from the simulation parameters, as the
+    reference's LBMSolver::initialize re-applies them."""
+
+    def __init__(self, nx: int, ny: int):
+        self.nx, self.ny = int(nx), int(ny)
+        self.pillars: List[tuple] = []
+        self._walls = False
+        self._bt = BoundaryType.INLET_OUTLET
+
+    def addWalls(self):
+        self._walls = True
+        return self
+
+    def addCirclePillar(self, cx: float, cy: float, radius: float):
+        self.pillars.append((0, float(cx), float(cy), float(radius), 0.0))
+        return self
+
+    def addRectPillar(self, x0: float, y0: float, x1: float, y1: float):
+        self.pillars.append((1, float(x0), float(y0), float(x1), float(y1)))
+        return self
+
+    def setBoundaryType(self, bt):
+        self._bt = BoundaryType(bt)
+        return self
+
+    def getBoundaryType(self):
+        return self._bt
+
+    def hasTopWall(self):
+        return self._walls
+
+    def hasBottomWall(self):
+        return self._walls
+
+    def getNx(self):
+        return self.nx
+
+    def getNy(self):
+        return self.ny
+
+    def wallBottom(self):
+        return 0.0
+
+    def wallTop(self):
+        return float(self.ny - 1)
+
+
 class _Channel:
     def __init__(self, params: SimulationParams):
         self.params = params
         self.cparams = params.to_c()
         self.caps: List[_CapsuleRec] = []
+        self.pillars: List[tuple] = []
         self.walls_in_placement = False
 
     def add_capsule(self, center, radius, num_nodes=0, mparams=None, type_id=0):
@@ -306,6 +359,8 @@ class _Context:
             for ch in channels:
                 idx = C.c_int()
                 L.check(lib.sfg_add_channel(h, C.byref(ch.cparams), C.byref(idx)))
+                for pl in ch.pillars:
+                    L.check(lib.sfg_add_pillar(h, idx.value, *pl))
                 for rec in ch.caps:
                     mpc = rec.mp.to_c()
                     L.check(lib.sfg_add_capsule(h, idx.value, C.byref(mpc), C.byref(rec.rest),
@@ -662,6 +717,13 @@ class Ensemble:
         (simulation.cpp:250-256), as the declarative Python API does."""
         self._chans[chan].walls_in_placement = bool(enabled)
 
+    def setChannelBuilder(self, chan: int, builder: "ChannelBuilder"):
+        """Simulation::setChannelBuilder (simulation.cpp:211-213): the
+        builder's pillars become SOLID nodes of the channel (with Bouzidi
+        links when fluid.use_interpolated_bb)."""
+        self._pre_init()
+        self._chans[chan].pillars = list(builder.pillars)
+
     def _pre_init(self):
         if self._ctx is not None:
             raise RuntimeError("capsules must be added before initialize()")
@@ -913,6 +975,9 @@ class Simulation(Ensemble):
 
     def setChannelWalls(self, enabled: bool = True):
         super().setChannelWalls(0, enabled)
+
+    def setChannelBuilder(self, builder: "ChannelBuilder"):
+        super().setChannelBuilder(0, builder)
 
     def setStepCallback(self, fn):
         """fn(sim, step) after every step (Simulation::setStepCallback; step

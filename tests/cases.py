@@ -156,6 +156,7 @@ def gpu_params(case, precision):
     p.fluid.inlet_velocity, p.fluid.outlet_density = sp["inlet_velocity"], sp["outlet_density"]
     p.fluid.top_wall_velocity = sp["top_wall_velocity"]
     p.fluid.bottom_wall_velocity = sp["bottom_wall_velocity"]
+    p.fluid.use_interpolated_bb = bool(sp["use_interpolated_bb"])
     p.fluid.tau, p.fluid.rho0 = sp["tau"], sp["rho0"]
     p.fluid.collision_model = S.CollisionModel(sp["collision"])
     p.fluid.mrt_se, p.fluid.mrt_s_eps, p.fluid.mrt_sq = sp["mrt_se"], sp["mrt_s_eps"], sp["mrt_sq"]
@@ -200,6 +201,15 @@ def add_case_capsules(ens, chan, case):
 def build_gpu(case, precision="fp32"):
     import softflow_b200 as S
     sim = S.Simulation(gpu_params(case, precision))
+    if case.get("pillars"):
+        sp = case["spec"]
+        b = S.ChannelBuilder(sp["nx"], sp["ny"])
+        for ob in case["pillars"]:
+            if ob[0] == "circle":
+                b.addCirclePillar(*ob[1:])
+            else:
+                b.addRectPillar(*ob[1:])
+        sim.setChannelBuilder(b)
     add_case_capsules(sim, 0, case)
     sim.initialize()
     if case["conc"] is not None:

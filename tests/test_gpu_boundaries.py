@@ -21,11 +21,15 @@ pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 BOUNDARY = [("zouhe_bgk", 300), ("zouhe_mrt", 300), ("zouhe_reg", 300), ("cavity", 400),
-            ("shear_capsule", 60)]
+            ("shear_capsule", 60), ("pillars_bb", 300), ("pillars_ibb", 300),
+            ("pillars_zouhe", 300)]
 
 
-def _open_mask(case):
-    """Non-SOLID cells (CellType as LBMSolver::initialize sets it)."""
+def _open_mask(case, o=None):
+    """Non-SOLID cells (CellType as LBMSolver::initialize sets it); with
+    pillars, the cells where the oracle's density is not zeroed."""
+    if case.get("pillars"):
+        return o.rho() != 0.0
     sp = case["spec"]
     nx, ny = sp["nx"], sp["ny"]
     m = np.ones((ny, nx), dtype=bool)
@@ -46,7 +50,7 @@ def test_fp64_boundaries_bit_exact(sfg, oracle_mod, name, steps):
     sim = build_gpu(case, "fp64")
     sim.run(steps)
     fld = sim.field()
-    m = _open_mask(case)
+    m = _open_mask(case, o)
     f = fld.distributions()
     assert np.array_equal(f[:, m], o.f()[:, m])
     rho, ux, uy, _, _ = fld.macroscopic()
@@ -58,7 +62,8 @@ def test_fp64_boundaries_bit_exact(sfg, oracle_mod, name, steps):
     assert np.abs(ux).max() > 1e-3          # the boundaries drive a flow
 
 
-@pytest.mark.parametrize("name", ["zouhe_bgk", "zouhe_reg", "cavity", "shear_capsule"])
+@pytest.mark.parametrize("name", ["zouhe_bgk", "zouhe_reg", "cavity", "shear_capsule",
+                                  "pillars_ibb", "pillars_zouhe"])
 def test_fp64_boundaries_match_reference_golden(sfg, name):
     """Against the reference's own outputs (tests/golden/make_golden.py)."""
     g = np.load(os.path.join(GOLDEN, f"{name}.npz"))
@@ -74,7 +79,8 @@ def test_fp64_boundaries_match_reference_golden(sfg, name):
 
 @pytest.mark.parametrize("precision,tol", [("fp32", 1e-4), ("fp16s", 5e-3)])
 @pytest.mark.parametrize("name,steps", [("zouhe_bgk", 300), ("zouhe_mrt", 300),
-                                        ("cavity", 400), ("shear_capsule", 60)])
+                                        ("cavity", 400), ("shear_capsule", 60),
+                                        ("pillars_ibb", 300)])
 def test_reduced_precision_boundaries(sfg, oracle_mod, precision, tol, name, steps):
     case = CASES[name]
     o = build_oracle(case)
@@ -82,7 +88,7 @@ def test_reduced_precision_boundaries(sfg, oracle_mod, precision, tol, name, ste
     sim = build_gpu(case, precision)
     sim.run(steps)
     fld = sim.field()
-    m = _open_mask(case)
+    m = _open_mask(case, o)
     ex = rel_l2(fld.velocity_x()[m], o.ux()[m])
     ey = rel_l2(fld.velocity_y()[m], o.uy()[m])
     print(f"{name} {precision}: rel L2 ux {ex:.3e}, uy {ey:.3e}")
@@ -122,6 +128,12 @@ def test_boundary_channel_restrictions(sfg):
     q.scalar.enabled = True
     with pytest.raises(S.SoftFlowGpuError, match="scalar"):
         S.Simulation(q).initialize()
+    r = gpu_params(CASES["pillars_bb"], "fp32")
+    sim = S.Simulation(r)
+    sim.setChannelBuilder(S.ChannelBuilder(r.nx, r.ny).addCirclePillar(20.0, 15.0, 4.0))
+    sim.addCapsule((50.0, 15.0), 3.0, 24)
+    with pytest.raises(S.SoftFlowGpuError, match="pillars"):
+        sim.initialize()
 
 
 def test_body_force_on_fluid_cells_only(sfg, oracle_mod):
