@@ -354,6 +354,18 @@ k_lattice_step_bc(const RowItem* __restrict__ items, int n_items,
             PopIO<S, R>::st_sr(fd + q * plane + yt * pitch + xt, q, f[q], seed);
         }
     }
+    if (!per_x) {
+        // a direction whose source lies outside the lattice keeps the node's
+        // own value, as the reference's pull falls back to the node itself
+        // (lbm_solver.cpp:86-96); Zou-He overwrites these at the INLET /
+        // OUTLET columns, but interpolated bounce-back reads them first
+#pragma unroll
+        for (int q = 1; q < 9; ++q) {
+            const int xs = x - cx_of(q);
+            if (xs < 0 || xs >= nx)
+                PopIO<S, R>::st_sr(fd + q * plane + n, q, f[q], seed);
+        }
+    }
 }
 
 // Bouzidi interpolated bounce-back on the streamed populations (reference
