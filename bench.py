@@ -12,9 +12,11 @@ steps per second); MLUPS and marker-updates/s are reported beside it.
 value     device time (CUDA events on the context stream) of K steps with the
           state resident in HBM; max over ranks; whole-job aggregate.
 e2e       the same K steps through the public API from host buffers: the
-          initial populations and markers are uploaded from pinned host memory
-          inside the timed region, and every step reads all marker positions
-          back to the host.
+          initial populations are uploaded from pinned host memory inside the
+          timed region, and every step's marker positions and velocities land
+          in pinned host memory (sfg_get_all_markers_async: copied on a second
+          stream while the next step runs; the host takes step s's markers
+          before enqueuing step s + 2).
 roofline  the lattice kernel (fused collide + stream + bounce-back + lagged
           scalar step), timed live with CUDA events in a profiling pass;
           algorithmic bytes = one read + one write of 9 populations per fluid
@@ -424,13 +426,21 @@ def run_e2e(args, plans, ens, pg, local):
     lib.sfg_get_all_markers(ctx._h, L.dptr(pos_h.numpy()), L.dptr(vel_h.numpy()))
     h2d = sum(p.numel() * 8 for p in pops)
     d2h_step = 2 * 8 * 2 * M
+    # two pinned landing buffers: step s's markers are copied to the host while
+    # step s + 1 runs; the host takes step s's markers before enqueuing s + 2
+    pos_b = [pos_h, torch.empty_like(pos_h).pin_memory()]
+    vel_b = [vel_h, torch.empty_like(vel_h).pin_memory()]
     barrier(pg, local)
     t0 = time.perf_counter()
     for i in range(len(plans)):
         L.check(lib.sfg_set_populations(ctx._h, i, L.dptr(pops[i].numpy())))
     for s in range(args.steps):
         L.check(lib.sfg_step(ctx._h, 1))
-        L.check(lib.sfg_get_all_markers(ctx._h, L.dptr(pos_h.numpy()), L.dptr(vel_h.numpy())))
+        if s >= 1:
+            L.check(lib.sfg_wait_markers(ctx._h, (s - 1) % 2))   # step s - 1 on the host
+        L.check(lib.sfg_get_all_markers_async(ctx._h, s % 2, L.dptr(pos_b[s % 2].numpy()),
+                                              L.dptr(vel_b[s % 2].numpy())))
+    L.check(lib.sfg_wait_markers(ctx._h, (args.steps - 1) % 2))
     ctx.synchronize()
     t1 = time.perf_counter()
     sec = allmax(pg, t1 - t0)
@@ -439,7 +449,8 @@ def run_e2e(args, plans, ens, pg, local):
     return {"value": caps * args.steps * world / sec, "unit": "capsule-steps/s",
             "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h_step,
             "note": "initial state uploaded from pinned host memory inside the timed region; "
-                    "every step reads all marker positions and velocities back"}
+                    "every step's marker positions and velocities land in pinned host "
+                    "memory (copied on a second stream while the next step runs)"}
 
 
 def run_plain(args, plans, local, max_channels=256, steps=None):

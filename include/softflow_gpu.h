@@ -191,6 +191,16 @@ int sfg_get_markers(sfg_context* ctx, int channel, double* pos, double* vel, dou
 int sfg_set_markers(sfg_context* ctx, int channel, const double* pos, const double* vel);
 /* Marker positions / velocities of every channel at once (channel-major). */
 int sfg_get_all_markers(sfg_context* ctx, double* pos, double* vel);
+/* The same copy without waiting, for a host loop that consumes every step's
+ * markers while the next steps run: a snapshot after the steps enqueued so
+ * far is taken on the context stream and copied to pos / vel (page-locked
+ * host memory, [M][2] each, either may be NULL) on a separate copy stream.
+ * slot (0 or 1) selects one of two snapshot buffers; the host buffers must
+ * stay valid and unread until sfg_wait_markers(slot) returns.  Reusing a
+ * slot first waits for its previous copy.  No reference counterpart (the
+ * reference's host owns the markers). */
+int sfg_get_all_markers_async(sfg_context* ctx, int slot, double* pos, double* vel);
+int sfg_wait_markers(sfg_context* ctx, int slot);
 /* Concentration field and equilibrium populations g = w C
  * (AdvectionDiffusion::setRegion semantics, advection_diffusion.cpp:59-71). */
 int sfg_set_concentration(sfg_context* ctx, int channel, const double* C);

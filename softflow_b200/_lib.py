@@ -147,6 +147,8 @@ SIGNATURES = {
                                     _P(C.c_longlong), _P(C.c_longlong)]),
     "sfg_autotune": (C.c_int, [C.c_void_p, C.c_int, _P(C.c_int)]),
     "sfg_thermo": (C.c_int, [C.c_void_p, _P(ThermoRecordC), _D]),
+    "sfg_get_all_markers_async": (C.c_int, [C.c_void_p, C.c_int, _D, _D]),
+    "sfg_wait_markers": (C.c_int, [C.c_void_p, C.c_int]),
     "sfg_add_pillar": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double,
                                  C.c_double, C.c_double]),
     "sfg_write_vtk_fluid": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p, C.c_int, C.c_int,

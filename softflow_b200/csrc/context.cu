@@ -252,6 +252,13 @@ struct sfg_context {
     bool any_bc = false;                // boundary-aware lattice kernel in use
     RowItem* d_zh_rows = nullptr;       // Zou-He rows (channel, y)
     int n_zh = 0;
+    // pipelined marker output: snapshots on the context stream, copied to
+    // the host on a copy stream while later steps run
+    cudaStream_t copy_stream = nullptr;
+    double* d_snap[2] = {nullptr, nullptr};       // [M][2] positions, then [M][2] velocities
+    cudaEvent_t ev_snap[2] = {nullptr, nullptr};
+    cudaEvent_t ev_copy[2] = {nullptr, nullptr};
+    bool copy_pending[2] = {false, false};
     unsigned char* d_masks = nullptr;   // cell types of channels with pillars
     IbbLink* d_ibb = nullptr;           // interpolated bounce-back links by level
     std::vector<int> ibb_level_start;   // [levels + 1]
@@ -395,6 +402,17 @@ static void free_all(sfg_context* c) {
     c->d_zh_rows = nullptr;
     F(c->d_masks);
     F(c->d_ibb);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+    for (int i = 0; i < 2; ++i) {
+        F(c->d_snap[i]);
+        c->d_snap[i] = nullptr;
+        if (c->ev_snap[i]) cudaEventDestroy(c->ev_snap[i]);
+        if (c->ev_copy[i]) cudaEventDestroy(c->ev_copy[i]);
+        c->ev_snap[i] = c->ev_copy[i] = nullptr;
+        c->copy_pending[i] = false;
+    }
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    c->copy_stream = nullptr;
     c->d_masks = nullptr;
     c->d_ibb = nullptr;
     F(c->d_thermo_parts); F(c->d_cap_stats); F(c->d_thermo);
@@ -1406,6 +1424,49 @@ extern "C" int sfg_get_markers(sfg_context* c, int chi, double* pos, double* vel
         if (force) CU(cudaMemcpyAsync(force, c->mb.frc + d.mk_begin, sizeof(double2) * n, cudaMemcpyDeviceToHost, c->stream));
     }
     CU(cudaStreamSynchronize(c->stream));
+    return SFG_OK;
+}
+
+extern "C" int sfg_wait_markers(sfg_context* c, int slot) {
+    if (!c || slot < 0 || slot > 1) return fail(SFG_ERR_ARG, "sfg_wait_markers: bad argument");
+    if (!c->copy_pending[slot]) return SFG_OK;
+    CU(cudaSetDevice(c->device));
+    CU(cudaEventSynchronize(c->ev_copy[slot]));
+    c->copy_pending[slot] = false;
+    return SFG_OK;
+}
+
+extern "C" int sfg_get_all_markers_async(sfg_context* c, int slot, double* pos, double* vel) {
+    if (!c || slot < 0 || slot > 1)
+        return fail(SFG_ERR_ARG, "sfg_get_all_markers_async: bad argument");
+    if (!c->initialized)
+        return fail(SFG_ERR_STATE, "sfg_get_all_markers_async: context not initialized");
+    if (c->M == 0) return SFG_OK;
+    CU(cudaSetDevice(c->device));
+    if (!c->copy_stream) {
+        CU(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        for (int i = 0; i < 2; ++i) {
+            CU(cudaMalloc(&c->d_snap[i], sizeof(double) * 4 * (size_t)c->M));
+            CU(cudaEventCreateWithFlags(&c->ev_snap[i], cudaEventDisableTiming));
+            CU(cudaEventCreateWithFlags(&c->ev_copy[i], cudaEventDisableTiming));
+        }
+    }
+    // the slot's previous copy must have left its snapshot buffer
+    int rc = sfg_wait_markers(c, slot);
+    if (rc) return rc;
+    double* snap = c->d_snap[slot];
+    const size_t bytes = sizeof(double2) * (size_t)c->M;
+    CU(cudaMemcpyAsync(snap, c->mb.pos, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    CU(cudaMemcpyAsync(snap + 2 * (size_t)c->M, c->mb.vel, bytes, cudaMemcpyDeviceToDevice,
+                       c->stream));
+    CU(cudaEventRecord(c->ev_snap[slot], c->stream));
+    CU(cudaStreamWaitEvent(c->copy_stream, c->ev_snap[slot], 0));
+    if (pos) CU(cudaMemcpyAsync(pos, snap, bytes, cudaMemcpyDeviceToHost, c->copy_stream));
+    if (vel)
+        CU(cudaMemcpyAsync(vel, snap + 2 * (size_t)c->M, bytes, cudaMemcpyDeviceToHost,
+                           c->copy_stream));
+    CU(cudaEventRecord(c->ev_copy[slot], c->copy_stream));
+    c->copy_pending[slot] = true;
     return SFG_OK;
 }
 

@@ -155,3 +155,34 @@ def test_stability_check_schedule(sfg, capsys):
     steps = [int(line.split("at step ")[1].split()[0])
              for line in err.splitlines() if "high velocity" in line]
     assert steps == [0, 5, 10]
+
+
+def test_async_marker_readback(sfg):
+    """sfg_get_all_markers_async: every step's snapshot, landed through the
+    copy stream while later steps run, equals the synchronous read."""
+    import ctypes as C
+    import torch
+    from softflow_b200 import _lib as L
+    case = CASES["c1"]
+    a = build_gpu(case, "fp32")
+    b = build_gpu(case, "fp32")
+    M = a.capsules().totalNodes()
+    bufs = [(torch.zeros(2 * M, dtype=torch.float64).pin_memory(),
+             torch.zeros(2 * M, dtype=torch.float64).pin_memory()) for _ in range(2)]
+    ca, cb = a.context(), b.context()
+    got = []
+    for s in range(6):
+        L.check(ca._lib.sfg_step(ca._h, 1))
+        if s >= 1:
+            L.check(ca._lib.sfg_wait_markers(ca._h, (s - 1) % 2))
+            got.append(bufs[(s - 1) % 2][0].numpy().copy())
+        p, v = bufs[s % 2]
+        L.check(ca._lib.sfg_get_all_markers_async(ca._h, s % 2, L.dptr(p.numpy()),
+                                                  L.dptr(v.numpy())))
+    L.check(ca._lib.sfg_wait_markers(ca._h, 5 % 2))
+    got.append(bufs[5 % 2][0].numpy().copy())
+    for s in range(6):
+        b.run(1)
+        pos = np.zeros(2 * M)
+        L.check(cb._lib.sfg_get_all_markers(cb._h, L.dptr(pos), None))
+        assert np.array_equal(got[s], pos), s
