@@ -49,6 +49,29 @@ class _Params(C.Structure):
     ]
 
 
+class _Chemistry(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("n_release", "n_absorb", "n_k_leach", "n_C_eq", "n_M_p",
+                                       "n_k_adsorb", "n_k_desorb", "n_Gamma_max")] + \
+               [(n, C.c_double * 8) for n in ("release", "absorb", "k_leach", "C_eq",
+                                              "M_p_initial", "k_adsorb", "k_desorb",
+                                              "Gamma_max")]
+
+
+def chemistry_struct(**vectors) -> _Chemistry:
+    """Per capsule type vectors (lists) keyed release, absorb, k_leach, C_eq,
+    M_p_initial, k_adsorb, k_desorb, Gamma_max; missing keys are empty."""
+    counts = {"release": "n_release", "absorb": "n_absorb", "k_leach": "n_k_leach",
+              "C_eq": "n_C_eq", "M_p_initial": "n_M_p", "k_adsorb": "n_k_adsorb",
+              "k_desorb": "n_k_desorb", "Gamma_max": "n_Gamma_max"}
+    c = _Chemistry()
+    for k, v in vectors.items():
+        setattr(c, counts[k], len(v))
+        arr = getattr(c, k)
+        for i, x in enumerate(v):
+            arr[i] = float(x)
+    return c
+
+
 class _Membrane(C.Structure):
     _fields_ = [
         ("model", C.c_int), ("k_stretch", C.c_double), ("G_s", C.c_double),
@@ -151,6 +174,8 @@ def _load(path: str, prefix: str):
                                          C.c_int, C.c_int]),
         "initialize": (None, [C.c_void_p]),
         "add_circle_pillar": (None, [C.c_void_p, C.c_double, C.c_double, C.c_double]),
+        "set_chemistry": (None, [C.c_void_p, C.POINTER(_Chemistry)]),
+        "chemistry_state": (None, [C.c_void_p, d, d, d, d]),
         "add_rect_pillar": (None, [C.c_void_p, C.c_double, C.c_double, C.c_double,
                                    C.c_double]),
         "step": (None, [C.c_void_p, C.c_int]),
@@ -241,6 +266,19 @@ class OracleSim:
         return self._fn["add_capsule_random"](self._h, count, x0, y0, x1, y1, rmin, rmax, nn,
                                               C.byref(mc), type_, seed, min_gap, max_attempts,
                                               int(check_walls))
+
+    def set_chemistry(self, **vectors):
+        self._chem = chemistry_struct(**vectors)
+        self._fn["set_chemistry"](self._h, C.byref(self._chem))
+
+    def chemistry_state(self):
+        """(released [caps], absorbed [caps], Mp [caps], gamma [markers])."""
+        n, M = self.num_capsules, self.num_markers
+        out = [np.zeros(max(n, 1)), np.zeros(max(n, 1)), np.zeros(max(n, 1)),
+               np.zeros(max(M, 1))]
+        dp = C.POINTER(C.c_double)
+        self._fn["chemistry_state"](self._h, *[a.ctypes.data_as(dp) for a in out])
+        return out[0][:n], out[1][:n], out[2][:n], out[3][:M]
 
     def add_circle_pillar(self, cx, cy, r):
         self._fn["add_circle_pillar"](self._h, cx, cy, r)

@@ -46,6 +46,10 @@ struct RefSim {
     std::vector<int> offsets;
     std::vector<double> C_mirror;
     std::unique_ptr<ChannelBuilder> builder;   // Simulation::setChannelBuilder
+    // Simulation::scalar_release_rates_ / scalar_absorption_rates_ and the
+    // kinetic vectors of ScalarParams (simulation.cpp:925-945)
+    bool chem_on = false;
+    std::vector<Real> release_rates, absorption_rates;
 };
 
 MembraneParams to_mp(const sf_membrane* m) {
@@ -265,7 +269,17 @@ static void one_step(RefSim* s) {
         s->last_capped = capped;
     }
     s->lbm->step();
-    if (s->adr) s->adr->step(field);
+    if (s->adr) {
+        s->adr->step(field);
+        if (s->chem_on) {                     // simulation.cpp:640-653
+            bool has_physics = !s->p.scalar.k_leach.empty() || !s->p.scalar.k_adsorb.empty();
+            if (has_physics)
+                s->adr->applyChemistry(s->caps, s->release_rates, s->absorption_rates,
+                                       s->p.scalar);
+            else if (!s->release_rates.empty() || !s->absorption_rates.empty())
+                s->adr->applySourceSink(s->caps, s->release_rates, s->absorption_rates);
+        }
+    }
     s->ibm.interpolateVelocity(field, s->caps);
     s->caps.moveAllNodes(s->p.dt);
     if (!s->p.fluid.periodic_y) {
@@ -315,6 +329,33 @@ void sfr_capsule_centroid(void* h, int c, double* x, double* y) {
     *y = r.y;
 }
 double sfr_phi(double r) { return PeskinDelta::phi(r); }
+
+void sfr_set_chemistry(void* h, const sf_chemistry* c) {
+    auto* s = static_cast<RefSim*>(h);
+    auto vec = [](const double* v, int n) { return std::vector<Real>(v, v + n); };
+    s->release_rates = vec(c->release, c->n_release);
+    s->absorption_rates = vec(c->absorb, c->n_absorb);
+    s->p.scalar.k_leach = vec(c->k_leach, c->n_k_leach);
+    s->p.scalar.C_eq = vec(c->C_eq, c->n_C_eq);
+    s->p.scalar.M_p_initial = vec(c->M_p_initial, c->n_M_p);
+    s->p.scalar.k_adsorb = vec(c->k_adsorb, c->n_k_adsorb);
+    s->p.scalar.k_desorb = vec(c->k_desorb, c->n_k_desorb);
+    s->p.scalar.Gamma_max = vec(c->Gamma_max, c->n_Gamma_max);
+    s->chem_on = true;
+}
+
+void sfr_chemistry_state(void* h, double* released, double* absorbed, double* Mp,
+                         double* gamma) {
+    auto* s = static_cast<RefSim*>(h);
+    int k = 0;
+    for (int c = 0; c < s->caps.numCapsules(); ++c) {
+        if (released) released[c] = s->adr ? s->adr->getCapsuleReleased(c) : 0.0;
+        if (absorbed) absorbed[c] = s->adr ? s->adr->getCapsuleAbsorbed(c) : 0.0;
+        if (Mp) Mp[c] = s->adr ? s->adr->getCapsuleMp(c) : -1.0;
+        for (int i = 0; i < s->caps[c].numNodes(); ++i, ++k)
+            if (gamma) gamma[k] = s->adr ? s->adr->getNodeGamma(c, i) : 0.0;
+    }
+}
 
 // The reference's VTK writer on the current state (default fields, periodic
 // x as Simulation's constructor sets it, simulation.cpp:177-186).

@@ -55,6 +55,9 @@ struct sfo_sim {
     obstacle_t obs[64];
     int nlinks;
     ibb_link_t* links;
+    int chem_on;
+    sf_chemistry chem;
+    double *released, *absorbed, *Mp, *gamma;
     int nx, ny, N;
     double *f, *ftmp, *rho, *ux, *uy, *Fx, *Fy;
     int* flags;
@@ -179,6 +182,7 @@ void sfo_destroy(sfo_sim* s) {
     free(s->caps); free(s->pos); free(s->vel); free(s->frc);
     free(s->rest_len); free(s->rest_ang); free(s->rest_ds); free(s->prev_len);
     free(s->offsets); free(s->pair_count); free(s->pair_list); free(s->links);
+    free(s->released); free(s->absorbed); free(s->Mp); free(s->gamma);
     free(s);
 }
 
@@ -578,6 +582,166 @@ static void adr_step(sfo_sim* s) {
         double C = 0.0;
         for (int q = 0; q < Q; ++q) C += s->g[(size_t)n * Q + q];
         s->C[n] = C;
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* Capsule chemistry (reference advection_diffusion.cpp:225-437)        */
+/* ------------------------------------------------------------------ */
+
+void sfo_set_chemistry(sfo_sim* s, const sf_chemistry* c) {
+    s->chem = *c;
+    s->chem_on = 1;
+}
+
+void sfo_chemistry_state(const sfo_sim* s, double* released, double* absorbed, double* Mp,
+                         double* gamma) {
+    for (int c = 0; c < s->ncaps; ++c) {
+        if (released) released[c] = s->released ? s->released[c] : 0.0;
+        if (absorbed) absorbed[c] = s->absorbed ? s->absorbed[c] : 0.0;
+        if (Mp) Mp[c] = s->Mp ? s->Mp[c] : -1.0;
+    }
+    if (gamma)
+        for (int k = 0; k < s->M; ++k) gamma[k] = s->gamma ? s->gamma[k] : 0.0;
+}
+
+static inline double chem_get(const double* v, int n, int type, double dflt) {
+    return type < n ? v[type] : dflt;
+}
+
+/* per-capsule arrays as the first call sizes them (:231-234, :300-316) */
+static void chem_init(sfo_sim* s) {
+    if (s->released) return;
+    s->released = (double*)calloc(s->ncaps > 0 ? s->ncaps : 1, sizeof(double));
+    s->absorbed = (double*)calloc(s->ncaps > 0 ? s->ncaps : 1, sizeof(double));
+    s->Mp = (double*)calloc(s->ncaps > 0 ? s->ncaps : 1, sizeof(double));
+    s->gamma = (double*)calloc(s->M > 0 ? s->M : 1, sizeof(double));
+    for (int c = 0; c < s->ncaps; ++c) {
+        int type = s->caps[c].type;
+        s->Mp[c] = -1.0;
+        if (type < s->chem.n_M_p && s->chem.M_p_initial[type] > 0.0)
+            s->Mp[c] = s->chem.M_p_initial[type];
+    }
+}
+
+/* constant rates at the nearest node (:225-271) */
+static void chem_source_sink(sfo_sim* s) {
+    const int nx = s->nx, ny = s->ny;
+    for (int c = 0; c < s->ncaps; ++c) {
+        const capsule_t* cp = &s->caps[c];
+        int type = cp->type;
+        double release = chem_get(s->chem.release, s->chem.n_release, type, 0.0);
+        double absorb = chem_get(s->chem.absorb, s->chem.n_absorb, type, 0.0);
+        for (int ni = 0; ni < cp->n; ++ni) {
+            v2 pos = s->pos[cp->off + ni];
+            int ix = (int)(pos.x + 0.5);
+            int iy = (int)(pos.y + 0.5);
+            ix = ix < 0 ? 0 : (ix > nx - 1 ? nx - 1 : ix);
+            iy = iy < 0 ? 0 : (iy > ny - 1 ? ny - 1 : iy);
+            int n = iy * nx + ix;
+            s->C[n] += release;
+            s->released[c] += release;
+            double actual = (s->C[n] < absorb) ? s->C[n] : absorb;   /* std::min */
+            s->C[n] -= actual;
+            s->absorbed[c] += actual;
+            for (int q = 0; q < Q; ++q) s->g[(size_t)n * Q + q] = W[q] * s->C[n];
+        }
+    }
+}
+
+/* leaching, Langmuir adsorption, Peskin-weighted exchange (:273-437) */
+static void chem_physics(sfo_sim* s) {
+    const int nx = s->nx, ny = s->ny, Lx = nx;
+    for (int c = 0; c < s->ncaps; ++c) {
+        const capsule_t* cp = &s->caps[c];
+        int type = cp->type, Nn = cp->n;
+        double k_L = chem_get(s->chem.k_leach, s->chem.n_k_leach, type, 0.0);
+        double Ceq = chem_get(s->chem.C_eq, s->chem.n_C_eq, type, 0.0);
+        double k_a = chem_get(s->chem.k_adsorb, s->chem.n_k_adsorb, type, 0.0);
+        double k_d = chem_get(s->chem.k_desorb, s->chem.n_k_desorb, type, 0.0);
+        double Gmax = chem_get(s->chem.Gamma_max, s->chem.n_Gamma_max, type, 1.0);
+        double const_release = chem_get(s->chem.release, s->chem.n_release, type, 0.0);
+        double const_absorb = chem_get(s->chem.absorb, s->chem.n_absorb, type, 0.0);
+        for (int k = 0; k < Nn; ++k) {
+            v2 pos = s->pos[cp->off + k];
+            int kp = (k + 1) % Nn, km = (k - 1 + Nn) % Nn;
+            v2 pp = s->pos[cp->off + kp], pm = s->pos[cp->off + km];
+            double dxp = pp.x - pos.x, dyp = pp.y - pos.y;
+            double dxm = pos.x - pm.x, dym = pos.y - pm.y;
+            double ds = 0.5 * (sqrt(dxp * dxp + dyp * dyp) + sqrt(dxm * dxm + dym * dym));
+            if (ds < 1e-12) ds = 1.0;
+            int ix0 = (int)floor(pos.x), iy0 = (int)floor(pos.y);
+            double C_surf = 0.0;
+            for (int dy = -1; dy <= 2; ++dy) {
+                int jy = iy0 + dy;
+                if (jy < 0 || jy >= ny) continue;
+                for (int dx = -1; dx <= 2; ++dx) {
+                    int jx = ix0 + dx;
+                    jx = ((jx % Lx) + Lx) % Lx;
+                    double rx = pos.x - (double)(ix0 + dx);
+                    double ry = pos.y - (double)jy;
+                    double w = phi_tab(s->phi_tbl, rx) * phi_tab(s->phi_tbl, ry);
+                    C_surf += s->C[jy * nx + jx] * w;
+                }
+            }
+            double dC_leach = 0.0;
+            if (k_L > 0.0) {
+                dC_leach = k_L * (Ceq - C_surf);
+                if (s->Mp[c] >= 0.0) {
+                    if (dC_leach > 0.0) {
+                        double available_per_ds = s->Mp[c] / ds;
+                        dC_leach = (available_per_ds < dC_leach) ? available_per_ds : dC_leach;
+                        s->Mp[c] -= dC_leach * ds;
+                        if (s->Mp[c] < 0.0) s->Mp[c] = 0.0;
+                    }
+                }
+            } else {
+                double absorb_now = (C_surf < const_absorb) ? C_surf : const_absorb;
+                dC_leach = const_release - absorb_now;
+            }
+            double dC_adsorb = 0.0;
+            if (k_a > 0.0 || k_d > 0.0) {
+                double* G = &s->gamma[cp->off + k];
+                double dGamma = k_a * C_surf * (1.0 - *G / Gmax) - k_d * *G;
+                double t = *G + dGamma;
+                t = (t < Gmax) ? t : Gmax;              /* std::min(Gmax, t) */
+                *G = (0.0 < t) ? t : 0.0;               /* std::max(0.0, t) */
+                dC_adsorb = -dGamma;
+            }
+            double total_flux = dC_leach + dC_adsorb;
+            if (total_flux == 0.0) continue;
+            for (int dy = -1; dy <= 2; ++dy) {
+                int jy = iy0 + dy;
+                if (jy < 0 || jy >= ny) continue;
+                for (int dx = -1; dx <= 2; ++dx) {
+                    int jx = ix0 + dx;
+                    jx = ((jx % Lx) + Lx) % Lx;
+                    double rx = pos.x - (double)(ix0 + dx);
+                    double ry = pos.y - (double)jy;
+                    double w = phi_tab(s->phi_tbl, rx) * phi_tab(s->phi_tbl, ry);
+                    if (w < 1e-15) continue;
+                    int n = jy * nx + jx;
+                    s->C[n] += total_flux * w * ds;
+                    if (s->C[n] < 0.0) s->C[n] = 0.0;
+                    for (int q = 0; q < Q; ++q) s->g[(size_t)n * Q + q] = W[q] * s->C[n];
+                }
+            }
+            if (total_flux > 0.0) s->released[c] += total_flux * ds;
+            else s->absorbed[c] -= total_flux * ds;
+        }
+    }
+}
+
+/* simulation.cpp:640-653 */
+static void chemistry(sfo_sim* s) {
+    if (!s->chem_on) return;
+    int has_physics = s->chem.n_k_leach > 0 || s->chem.n_k_adsorb > 0;
+    if (has_physics) {
+        chem_init(s);
+        chem_physics(s);
+    } else if (s->chem.n_release > 0 || s->chem.n_absorb > 0) {
+        chem_init(s);
+        chem_source_sink(s);
     }
 }
 
@@ -1312,7 +1476,7 @@ static void one_step(sfo_sim* s) {
         s->last_capped = capped;
     }
     lbm_step(s);                                              /* 7 */
-    if (s->p.scalar_enabled) adr_step(s);                     /* 7c */
+    if (s->p.scalar_enabled) { adr_step(s); chemistry(s); }  /* 7c */
     for (int c = 0; c < s->ncaps; ++c) {                      /* 8 */
         const capsule_t* cp = &s->caps[c];
         for (int k = 0; k < cp->n; ++k) s->vel[cp->off + k] = interp_point(s, NODE(cp, k));

@@ -93,6 +93,24 @@ void sfo_destroy(sfo_sim* s);
 void sfo_add_circle_pillar(sfo_sim* s, double cx, double cy, double radius);
 void sfo_add_rect_pillar(sfo_sim* s, double x0, double y0, double x1, double y1);
 
+/* Capsule chemistry of the scalar (AdvectionDiffusion::applySourceSink /
+ * applyChemistry, advection_diffusion.cpp:225-437): per capsule type up to 8
+ * entries; a count of 0 is an empty vector, which selects the reference's
+ * branches (simulation.cpp:640-653: physics kinetics when k_leach or
+ * k_adsorb is non-empty, else the constant rates when either is set). */
+#define SF_CHEM_TYPES 8
+typedef struct sf_chemistry {
+    int n_release, n_absorb, n_k_leach, n_C_eq, n_M_p, n_k_adsorb, n_k_desorb, n_Gamma_max;
+    double release[SF_CHEM_TYPES], absorb[SF_CHEM_TYPES], k_leach[SF_CHEM_TYPES];
+    double C_eq[SF_CHEM_TYPES], M_p_initial[SF_CHEM_TYPES], k_adsorb[SF_CHEM_TYPES];
+    double k_desorb[SF_CHEM_TYPES], Gamma_max[SF_CHEM_TYPES];
+} sf_chemistry;
+void sfo_set_chemistry(sfo_sim* s, const sf_chemistry* c);
+/* Per capsule: cumulative released / absorbed amounts and the reservoir
+ * mass (-1: infinite); per marker: the surface coverage Gamma. */
+void sfo_chemistry_state(const sfo_sim* s, double* released, double* absorbed, double* Mp,
+                         double* gamma);
+
 /* Capsule construction (reference capsule.cpp:7-141), returns its index. */
 int sfo_add_capsule(sfo_sim* s, double cx, double cy, double radius, int nn,
                     const sf_membrane* m, int type);

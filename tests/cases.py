@@ -115,6 +115,27 @@ CASES = {
                           capsules=[("add", 32.0, 17.0, 6.0, 36,
                                      dict(model=O.SKALAK, G_s=0.05, C_skalak=10.0))],
                           conc=None),
+    # capsule chemistry of the scalar: constant release / absorption at the
+    # nearest node, and Fick leaching from finite reservoirs with Langmuir
+    # adsorption; capsules of two types, two of them close enough for their
+    # stencils to overlap (the reference applies capsules in order)
+    "chem_source": dict(spec=dict(nx=96, ny=48, collision=O.BGK, tau=0.8, body_fx=1e-5,
+                                  scalar_enabled=1, scalar_D=0.05),
+                        capsules=[("add", 30.0, 20.0, 4.0, 24, SKALAK_C1, 0),
+                                  ("add", 39.2, 21.0, 4.0, 24, SKALAK_C1, 1),
+                                  ("add", 70.0, 30.0, 5.0, 32, SKALAK_C1, 0)],
+                        conc=gaussian_conc(48.0, 24.0, 12.0),
+                        chem=dict(release=[0.002, 0.0], absorb=[0.0, 0.001])),
+    "chem_physics": dict(spec=dict(nx=96, ny=48, collision=O.BGK, tau=0.8, body_fx=1e-5,
+                                   scalar_enabled=1, scalar_D=0.05),
+                         capsules=[("add", 30.0, 20.0, 4.0, 24, SKALAK_C1, 0),
+                                   ("add", 39.2, 21.0, 4.0, 24, SKALAK_C1, 1),
+                                   ("add", 70.0, 30.0, 5.0, 32, SKALAK_C1, 0)],
+                         conc=gaussian_conc(48.0, 24.0, 12.0),
+                         chem=dict(k_leach=[0.05, 0.0], C_eq=[1.0, 0.0],
+                                   M_p_initial=[0.02, 0.0], k_adsorb=[0.0, 0.02],
+                                   k_desorb=[0.0, 0.001], Gamma_max=[1.0, 0.5],
+                                   release=[0.0, 0.0005])),
     # pure diffusion (reference tests/verification/test_pure_diffusion.cpp)
     "diffusion": dict(spec=dict(nx=256, ny=8, collision=O.BGK, tau=0.6, periodic_y=1,
                                 scalar_enabled=1, scalar_D=0.05, scalar_periodic_y=1),
@@ -131,12 +152,14 @@ def build_oracle(case, impl="sfo"):
             s.add_rect_pillar(*ob[1:])
     for c in case["capsules"]:
         if c[0] == "add":
-            _, cx, cy, r, nn, mk = c
-            s.add_capsule(cx, cy, r, nn, O.Membrane(**mk))
+            _, cx, cy, r, nn, mk = c[:6]
+            s.add_capsule(cx, cy, r, nn, O.Membrane(**mk), c[6] if len(c) > 6 else 0)
         else:
             _, count, x0, y0, x1, y1, rmin, rmax, nn, mk, seed, gap, walls = c
             s.add_capsule_random(count, x0, y0, x1, y1, rmin, rmax, nn, O.Membrane(**mk),
                                  seed=seed, min_gap=gap, check_walls=walls)
+    if case.get("chem"):
+        s.set_chemistry(**case["chem"])
     s.initialize()
     if case["conc"] is not None:
         sp = case["spec"]

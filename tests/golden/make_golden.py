@@ -27,7 +27,8 @@ OUTPUT_RUNS = [("bgk_small", 300), ("seam_single", 40), ("diffusion", 200)]
 RUNS = [("bgk_small", 300), ("mrt_small", 300), ("reg_small", 300), ("mini_c2", 30),
         ("contact_brute", 60), ("seam_single", 40), ("c1", 10),
         ("zouhe_bgk", 300), ("zouhe_reg", 300), ("cavity", 400), ("shear_capsule", 60),
-        ("pillars_ibb", 300), ("pillars_zouhe", 300)]
+        ("pillars_ibb", 300), ("pillars_zouhe", 300), ("chem_source", 60),
+        ("chem_physics", 60)]
 
 
 def main():
@@ -50,6 +51,9 @@ def main():
                                        o.capsule_inclination(c)] for c in range(n)]))
         if case["conc"] is not None:
             out.update(C=o.concentration())
+        if case.get("chem"):
+            rel, ab, mp, gam = o.chemistry_state()
+            out.update(released=rel, absorbed=ab, Mp=mp, gamma=gam, g=o.g())
         path = os.path.join(HERE, f"{name}.npz")
         np.savez_compressed(path, **out)
         print(path, os.path.getsize(path))

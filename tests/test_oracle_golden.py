@@ -12,7 +12,8 @@ from cases import CASES, build_oracle, fluid_rows
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 NAMES = ["bgk_small", "mrt_small", "reg_small", "mini_c2", "contact_brute", "seam_single", "c1",
-         "zouhe_bgk", "zouhe_reg", "cavity", "shear_capsule", "pillars_ibb", "pillars_zouhe"]
+         "zouhe_bgk", "zouhe_reg", "cavity", "shear_capsule", "pillars_ibb", "pillars_zouhe",
+         "chem_source", "chem_physics"]
 
 
 @pytest.mark.parametrize("name", NAMES)
@@ -32,6 +33,9 @@ def test_oracle_matches_reference_golden(oracle_mod, name):
         assert np.array_equal(o.forces(), g["force"])
     if "C" in g:
         assert np.array_equal(o.concentration(), g["C"])
+    if "released" in g:
+        for k, v in zip(("released", "absorbed", "Mp", "gamma"), o.chemistry_state()):
+            assert np.array_equal(v, g[k]), k
 
 
 @pytest.mark.skipif(not O.ref_available(), reason="reference build absent")
@@ -132,3 +136,22 @@ def test_oracle_pillars_match_live_reference(oracle_mod, name, steps):
     b.step(steps)
     for k in ("f", "ux", "uy", "rho"):
         assert np.array_equal(getattr(a, k)(), getattr(b, k)()), k
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build absent")
+@pytest.mark.parametrize("name,steps", [("chem_source", 60), ("chem_physics", 60)])
+def test_oracle_chemistry_matches_live_reference(oracle_mod, name, steps):
+    """Capsule chemistry of the scalar (applySourceSink / applyChemistry,
+    advection_diffusion.cpp:225-437): concentration, scalar populations and
+    the per-capsule / per-node chemistry state, bit for bit."""
+    case = CASES[name]
+    a = build_oracle(case, "sfo")
+    b = build_oracle(case, "ref")
+    a.step(steps)
+    b.step(steps)
+    for k in ("concentration", "g", "ux", "positions"):
+        assert np.array_equal(getattr(a, k)(), getattr(b, k)()), k
+    for x, y in zip(a.chemistry_state(), b.chemistry_state()):
+        assert np.array_equal(x, y)
+    rel, ab, mp, gam = a.chemistry_state()
+    assert (rel > 0).any() and (ab > 0).any()
