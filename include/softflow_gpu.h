@@ -167,6 +167,35 @@ enum sfg_pillar { SFG_PILLAR_CIRCLE = 0, SFG_PILLAR_RECT = 1 };
 int sfg_add_pillar(sfg_context* ctx, int channel, int kind, double a, double b, double c,
                    double d);
 
+/* Capsule chemistry of the scalar, before sfg_initialize (the channel needs
+ * the scalar): AdvectionDiffusion::applySourceSink / applyChemistry
+ * (advection_diffusion.cpp:225-437) after every scalar step, as
+ * Simulation::step calls them (simulation.cpp:640-653).  Vectors are per
+ * capsule type (at most SFG_CHEM_TYPES entries); a count of 0 is an empty
+ * vector, which selects the reference's branches: Fick leaching from
+ * finite reservoirs and Langmuir adsorption with Peskin-weighted exchange
+ * when k_leach or k_adsorb is non-empty, else constant release /
+ * absorption at the nearest node when either rate vector is non-empty.
+ * Capsules are applied in order; capsules whose stencils overlap run one
+ * after the other, so results equal the reference's serial loop. */
+#define SFG_CHEM_TYPES 8
+typedef struct sfg_chemistry {
+    int n_release, n_absorb, n_k_leach, n_C_eq, n_M_p, n_k_adsorb, n_k_desorb, n_Gamma_max;
+    double release[SFG_CHEM_TYPES], absorb[SFG_CHEM_TYPES], k_leach[SFG_CHEM_TYPES];
+    double C_eq[SFG_CHEM_TYPES], M_p_initial[SFG_CHEM_TYPES], k_adsorb[SFG_CHEM_TYPES];
+    double k_desorb[SFG_CHEM_TYPES], Gamma_max[SFG_CHEM_TYPES];
+} sfg_chemistry;
+int sfg_set_chemistry(sfg_context* ctx, int channel, const sfg_chemistry* chem);
+/* Type id of a capsule (Capsule::getTypeId), index within its channel,
+ * before sfg_initialize; 0 by default. */
+int sfg_set_capsule_type(sfg_context* ctx, int channel, int capsule, int type);
+/* Chemistry state of a channel: per capsule the cumulative released and
+ * absorbed amounts and the reservoir mass (-1: infinite), per marker the
+ * surface coverage (AdvectionDiffusion::getCapsuleReleased / Absorbed / Mp,
+ * getNodeGamma).  Any pointer may be NULL. */
+int sfg_get_chemistry_state(sfg_context* ctx, int channel, double* released, double* absorbed,
+                            double* Mp, double* gamma);
+
 /* Allocates device state and sets every channel to equilibrium at rho0 with
  * u = 0 (LBMSolver::initialize, lbm_solver.cpp:130-170; scalar initialised to
  * zero, advection_diffusion.cpp:46-57). */

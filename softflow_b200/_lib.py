@@ -74,6 +74,15 @@ THERMO_FN = C.CFUNCTYPE(C.c_int, C.c_longlong, C.POINTER(ThermoRecordC), C.c_int
                         C.POINTER(C.c_double), C.c_int, C.c_void_p)
 
 
+class ChemistryC(C.Structure):
+    """sfg_chemistry: per capsule type vectors (8 entries, counts 0..8)."""
+    _fields_ = [(n, C.c_int) for n in ("n_release", "n_absorb", "n_k_leach", "n_C_eq", "n_M_p",
+                                       "n_k_adsorb", "n_k_desorb", "n_Gamma_max")] + \
+               [(n, C.c_double * 8) for n in ("release", "absorb", "k_leach", "C_eq",
+                                              "M_p_initial", "k_adsorb", "k_desorb",
+                                              "Gamma_max")]
+
+
 class SoftFlowGpuError(RuntimeError):
     """Raised when a C-ABI call returns a nonzero status."""
 
@@ -149,6 +158,9 @@ SIGNATURES = {
     "sfg_thermo": (C.c_int, [C.c_void_p, _P(ThermoRecordC), _D]),
     "sfg_get_all_markers_async": (C.c_int, [C.c_void_p, C.c_int, _D, _D]),
     "sfg_wait_markers": (C.c_int, [C.c_void_p, C.c_int]),
+    "sfg_set_chemistry": (C.c_int, [C.c_void_p, C.c_int, _P(ChemistryC)]),
+    "sfg_set_capsule_type": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    "sfg_get_chemistry_state": (C.c_int, [C.c_void_p, C.c_int, _D, _D, _D, _D]),
     "sfg_add_pillar": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double,
                                  C.c_double, C.c_double]),
     "sfg_write_vtk_fluid": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p, C.c_int, C.c_int,

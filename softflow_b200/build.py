@@ -30,6 +30,7 @@ UNITS = [
     ("scan.cu", []),
     ("mlp.cu", []),
     ("learned_step.cu", ["--fmad=false"]),
+    ("chemistry.cu", ["--fmad=false"]),
     ("context.cu", []),
 ]
 HOST_UNITS = [("host_setup.cpp", ["-ffp-contract=off"]), ("host_io.cpp", ["-ffp-contract=off"])]

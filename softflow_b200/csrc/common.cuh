@@ -77,6 +77,8 @@ struct ChannelDev {
     double u_in, rho_out, u_top, u_bot;
     const unsigned char* mask;  // device cell types [ny][nx] of a channel with
                                 // pillars, null otherwise
+    int chem;                   // capsule chemistry after the scalar step
+    int adr_now;                // scalar step inside its own step (not lagged)
 };
 
 // Cell types of a channel (reference CellType, core/types.h:48-56), as
@@ -103,6 +105,7 @@ __host__ __device__ __forceinline__ int cell_kind(const ChannelDev& ch, int x, i
 // Per-capsule constants (reference Capsule members, capsule.h:77-142).
 struct CapsuleDev {
     int off, n, chan, model;
+    int type;                   // Capsule::getTypeId (chemistry parameters)
     int use_helfrich;
     double k_stretch, G_s, C_skalak;
     double wlc_L_max_ratio, wlc_kBT_p, wlc_k_pow;

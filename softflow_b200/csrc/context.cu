@@ -35,6 +35,7 @@ static int fail(int code, const std::string& msg) {
 namespace {
 
 struct CapsuleHost {
+    int type = 0;
     sfg_membrane_params mp;
     sfg_capsule_rest rest;
     std::vector<double> pos, rest_len, rest_ang, rest_ds;
@@ -50,6 +51,8 @@ struct ChanHost {
     ChannelDev d;
     std::vector<CapsuleHost> caps;
     std::vector<Pillar> pillars;
+    bool has_chem = false;
+    sfg_chemistry chem{};
     long long fluid_cells = 0;
 };
 
@@ -135,8 +138,12 @@ __global__ void k_step_flags(const ChannelDev* __restrict__ chans, int nch, int*
         if (mdf_fallback(resid_gate[c], chans[c].mdf_threshold)) fallbacks[c] += 1;
     }
     if (chans[c].adr) {
-        if (adr_pending[c]) c_fresh[c] = 0;
-        adr_pending[c] = 1;
+        if (chans[c].adr_now) {
+            c_fresh[c] = 0;          // this step's scalar step has run
+        } else {
+            if (adr_pending[c]) c_fresh[c] = 0;
+            adr_pending[c] = 1;
+        }
     }
     stepped[c] = 1;
 }
@@ -204,7 +211,8 @@ __global__ void k_scalar_import(const double* __restrict__ C, const double* __re
 
 template <typename R>
 __global__ void k_scalar_export(const R* __restrict__ g, ChannelDev ch, double* __restrict__ C,
-                                double* __restrict__ gout) {
+                                double* __restrict__ gout, const R* __restrict__ cfield,
+                                const unsigned char* __restrict__ cov) {
     const long long N = (long long)ch.nx * ch.ny;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
          i += (long long)gridDim.x * blockDim.x) {
@@ -214,7 +222,8 @@ __global__ void k_scalar_export(const R* __restrict__ g, ChannelDev ch, double* 
 #pragma unroll
         for (int q = 0; q < 9; ++q) v[q] = g[ch.g_off + q * ch.plane + n];
         const R s = v[0] + v[1] + v[2] + v[3] + v[4] + v[5] + v[6] + v[7] + v[8];
-        C[i] = (double)s;
+        // a concentration the capsule chemistry overwrote is the stored one
+        C[i] = (cov != nullptr && cov[ch.cell_off + n]) ? (double)cfield[ch.cell_off + n] : (double)s;
         if (gout)
             for (int q = 0; q < 9; ++q) gout[q * N + i] = (double)v[q];
     }
@@ -259,6 +268,14 @@ struct sfg_context {
     cudaEvent_t ev_snap[2] = {nullptr, nullptr};
     cudaEvent_t ev_copy[2] = {nullptr, nullptr};
     bool copy_pending[2] = {false, false};
+    // capsule chemistry of the scalar
+    bool any_chem = false;              // also: the scalar step runs inside its step
+    sfg_chemistry* d_chem = nullptr;    // [nch]
+    double *d_released = nullptr, *d_absorbed = nullptr, *d_Mp = nullptr;   // [NC]
+    double* d_gamma = nullptr;          // [M]
+    unsigned char* d_cov = nullptr;     // [cells] stored concentration in cfield
+    int* d_waves = nullptr;             // [2 NC]
+    void* d_boxes = nullptr;            // [NC] footprints
     unsigned char* d_masks = nullptr;   // cell types of channels with pillars
     IbbLink* d_ibb = nullptr;           // interpolated bounce-back links by level
     std::vector<int> ibb_level_start;   // [levels + 1]
@@ -402,6 +419,10 @@ static void free_all(sfg_context* c) {
     c->d_zh_rows = nullptr;
     F(c->d_masks);
     F(c->d_ibb);
+    F(c->d_chem); F(c->d_released); F(c->d_absorbed); F(c->d_Mp); F(c->d_gamma);
+    F(c->d_cov); F(c->d_waves); F(c->d_boxes);
+    c->d_chem = nullptr; c->d_released = c->d_absorbed = c->d_Mp = c->d_gamma = nullptr;
+    c->d_cov = nullptr; c->d_waves = nullptr; c->d_boxes = nullptr;
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     for (int i = 0; i < 2; ++i) {
         F(c->d_snap[i]);
@@ -462,6 +483,61 @@ extern "C" int sfg_add_channel(sfg_context* c, const sfg_channel_params* p, int*
     h.p = *p;
     c->ch.push_back(h);
     if (out) *out = (int)c->ch.size() - 1;
+    return SFG_OK;
+}
+
+extern "C" int sfg_set_chemistry(sfg_context* c, int channel, const sfg_chemistry* chem) {
+    if (!c || !chem) return fail(SFG_ERR_ARG, "sfg_set_chemistry: null argument");
+    if (c->initialized) return fail(SFG_ERR_STATE, "sfg_set_chemistry: context already initialized");
+    if (channel < 0 || channel >= (int)c->ch.size())
+        return fail(SFG_ERR_ARG, "sfg_set_chemistry: bad channel");
+    if (!c->ch[channel].p.scalar_enabled)
+        return fail(SFG_ERR_STATE, "sfg_set_chemistry: the channel has no scalar");
+    const int counts[8] = {chem->n_release, chem->n_absorb, chem->n_k_leach, chem->n_C_eq,
+                           chem->n_M_p, chem->n_k_adsorb, chem->n_k_desorb, chem->n_Gamma_max};
+    for (int k : counts)
+        if (k < 0 || k > SFG_CHEM_TYPES)
+            return fail(SFG_ERR_ARG, "sfg_set_chemistry: vector lengths must be 0..8");
+    c->ch[channel].chem = *chem;
+    c->ch[channel].has_chem = true;
+    return SFG_OK;
+}
+
+extern "C" int sfg_set_capsule_type(sfg_context* c, int channel, int capsule, int type) {
+    if (!c) return fail(SFG_ERR_ARG, "sfg_set_capsule_type: null context");
+    if (c->initialized)
+        return fail(SFG_ERR_STATE, "sfg_set_capsule_type: context already initialized");
+    if (channel < 0 || channel >= (int)c->ch.size() || capsule < 0 ||
+        capsule >= (int)c->ch[channel].caps.size() || type < 0)
+        return fail(SFG_ERR_ARG, "sfg_set_capsule_type: bad argument");
+    c->ch[channel].caps[capsule].type = type;
+    return SFG_OK;
+}
+
+extern "C" int sfg_get_chemistry_state(sfg_context* c, int chi, double* released,
+                                       double* absorbed, double* Mp, double* gamma) {
+    if (!c || chi < 0 || chi >= (int)c->ch.size())
+        return fail(SFG_ERR_ARG, "sfg_get_chemistry_state: bad channel");
+    if (!c->initialized)
+        return fail(SFG_ERR_STATE, "sfg_get_chemistry_state: context not initialized");
+    const ChannelDev& d = c->ch[chi].d;
+    const int nc = d.cap_end - d.cap_begin, nm = d.mk_end - d.mk_begin;
+    CU(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < nc; ++i) {
+        if (released) released[i] = 0.0;
+        if (absorbed) absorbed[i] = 0.0;
+        if (Mp) Mp[i] = -1.0;
+    }
+    for (int i = 0; i < nm; ++i)
+        if (gamma) gamma[i] = 0.0;
+    if (!c->any_chem || !c->ch[chi].has_chem) return SFG_OK;
+    if (nc > 0) {
+        if (released) CU(cudaMemcpy(released, c->d_released + d.cap_begin, sizeof(double) * nc, cudaMemcpyDeviceToHost));
+        if (absorbed) CU(cudaMemcpy(absorbed, c->d_absorbed + d.cap_begin, sizeof(double) * nc, cudaMemcpyDeviceToHost));
+        if (Mp) CU(cudaMemcpy(Mp, c->d_Mp + d.cap_begin, sizeof(double) * nc, cudaMemcpyDeviceToHost));
+    }
+    if (nm > 0 && gamma)
+        CU(cudaMemcpy(gamma, c->d_gamma + d.mk_begin, sizeof(double) * nm, cudaMemcpyDeviceToHost));
     return SFG_OK;
 }
 
@@ -555,6 +631,7 @@ extern "C" int sfg_initialize(sfg_context* c) {
     std::vector<int> mk_cap, mk_chan, tile_chan;
     c->any_adr = false;
     c->any_bc = false;
+    c->any_chem = false;
     c->maxn = 0;
     c->Kmax = 1;
     for (int ci = 0; ci < nch; ++ci) {
@@ -604,6 +681,8 @@ extern "C" int sfg_initialize(sfg_context* c) {
         d.adr_periodic_y = p.scalar_periodic_y ? 1 : 0;
         d.omega_s = 1.0 / (3.0 * p.scalar_D + 0.5);
         c->any_adr |= d.adr != 0;
+        d.chem = h.has_chem ? 1 : 0;
+        c->any_chem |= h.has_chem;
         d.tiles_x = (p.nx + TILE_W - 1) / TILE_W;
         d.tiles_y = (p.ny + TILE_H - 1) / TILE_H;
         d.tile_base = tile_base;
@@ -633,6 +712,7 @@ extern "C" int sfg_initialize(sfg_context* c) {
             cd.rest_area = cp.rest.rest_area;
             cd.rest_perimeter = cp.rest.rest_perimeter;
             cd.periodic_nx = p.nx;
+            cd.type = cp.type;
             caps.push_back(cd);
             c->maxn = std::max(c->maxn, cd.n);
             for (int k = 0; k < cd.n; ++k) {
@@ -760,6 +840,8 @@ extern "C" int sfg_initialize(sfg_context* c) {
         CU(cudaMemcpy(c->d_ibb, sorted.data(), sizeof(IbbLink) * sorted.size(),
                       cudaMemcpyHostToDevice));
     }
+    // with capsule chemistry the scalar step runs inside its own step
+    for (int i = 0; i < nch; ++i) c->ch[i].d.adr_now = (c->any_chem && c->ch[i].d.adr) ? 1 : 0;
     std::vector<ChannelDev> dch(nch);
     for (int i = 0; i < nch; ++i) dch[i] = c->ch[i].d;
     CU(dalloc(&c->d_chans, nch));
@@ -794,6 +876,10 @@ extern "C" int sfg_initialize(sfg_context* c) {
         }
         CU(cudaMalloc(&c->cfield, (size_t)cell_off * c->real_size()));
         CU(cudaMemset(c->cfield, 0, (size_t)cell_off * c->real_size()));
+        if (c->any_chem) {
+            CU(cudaMalloc(&c->d_cov, (size_t)cell_off));
+            CU(cudaMemset(c->d_cov, 0, (size_t)cell_off));
+        }
     }
     for (int ci = 0; ci < nch; ++ci) {
         const ChannelDev& d = c->ch[ci].d;
@@ -840,6 +926,32 @@ extern "C" int sfg_initialize(sfg_context* c) {
     CU(dalloc(&c->mb.wy, 4LL * M));
     CU(dalloc(&c->d_caps, c->NC));
     CU(dalloc(&c->d_has_prev, c->NC));
+    if (c->any_chem) {
+        // chemistry state as the reference sizes it at its first call
+        // (advection_diffusion.cpp:300-316): nothing released or absorbed,
+        // reservoirs infinite (-1) unless M_p_initial[type] > 0, no coverage
+        std::vector<sfg_chemistry> chp(nch);
+        for (int i = 0; i < nch; ++i) chp[i] = c->ch[i].chem;
+        CU(dalloc(&c->d_chem, nch));
+        CU(cudaMemcpy(c->d_chem, chp.data(), sizeof(sfg_chemistry) * nch, cudaMemcpyHostToDevice));
+        const int NCc = std::max(c->NC, 1);
+        CU(dalloc(&c->d_released, NCc));
+        CU(dalloc(&c->d_absorbed, NCc));
+        CU(dalloc(&c->d_Mp, NCc));
+        CU(dalloc(&c->d_gamma, std::max(M, 1)));
+        CU(dalloc(&c->d_waves, 2 * NCc));
+        CU(cudaMalloc(&c->d_boxes, chem_box_bytes() * NCc));
+        CU(cudaMemset(c->d_released, 0, sizeof(double) * NCc));
+        CU(cudaMemset(c->d_absorbed, 0, sizeof(double) * NCc));
+        CU(cudaMemset(c->d_gamma, 0, sizeof(double) * std::max(M, 1)));
+        std::vector<double> mp(NCc, -1.0);
+        for (int k = 0; k < c->NC; ++k) {
+            const sfg_chemistry& ck = c->ch[caps[k].chan].chem;
+            const int t = caps[k].type;
+            if (t >= 0 && t < ck.n_M_p && ck.M_p_initial[t] > 0.0) mp[k] = ck.M_p_initial[t];
+        }
+        CU(cudaMemcpy(c->d_Mp, mp.data(), sizeof(double) * NCc, cudaMemcpyHostToDevice));
+    }
     if (M > 0) {
         CU(cudaMemcpy(c->mb.pos, pos.data(), sizeof(double) * 2 * M, cudaMemcpyHostToDevice));
         CU(cudaMemset(c->mb.vel, 0, sizeof(double2) * M));
@@ -1024,7 +1136,7 @@ static int enqueue_step_t(sfg_context* c, int p) {
     }
     LatticeLaunch L{c->d_items, c->n_items, c->d_chans, c->f[p], c->f[1 - p], c->g[p],
                     c->g[1 - p], c->cfield, c->d_stepped, c->d_adr_pending, c->d_c_fresh,
-                    c->d_step_ctr, c->any_adr, c->d_items4, c->n_items4, c->use_vec4,
+                    c->d_step_ctr, c->any_adr && !c->any_chem, c->d_items4, c->n_items4, c->use_vec4,
                     c->persistent_ctas, c->shared_collision, c->any_bc, c->d_zh_rows,
                     c->n_zh, c->d_ibb, c->ibb_level_start.data(),
                     (int)c->ibb_level_start.size() - 1};
@@ -1034,6 +1146,16 @@ static int enqueue_step_t(sfg_context* c, int p) {
                     c->M > 0 ? c->tb.tile_slot[1 - p] : nullptr, c->tb.fin[p], c->tb.gsnap,
                     c->tb.fin[1 - p]};
     launch_lattice_step<S, R>(L, tv, st);
+    if (c->any_chem) {
+        // this step's scalar step, then the capsule chemistry
+        // (simulation.cpp:636-653), before the markers move
+        launch_scalar_now<S, R>(L, tv, c->d_cov, st);
+        launch_chemistry<R>(c->d_chans, nch, c->d_chem, c->d_caps, c->mb.pos, c->d_phi,
+                            c->g[1 - p], c->g[p], c->cfield, c->d_cov, c->d_released,
+                            c->d_absorbed, c->d_Mp, c->d_gamma, c->d_waves, c->d_boxes,
+                            std::max(c->NC, 1), c->d_status, st);
+        launches += 2;
+    }
     mark(c, SFG_PHASE_LATTICE);
     k_step_flags<<<(nch + 127) / 128, 128, 0, st>>>(c->d_chans, nch, c->d_stepped,
                                                     c->d_adr_pending, c->d_c_fresh,
@@ -1099,8 +1221,12 @@ extern "C" int sfg_step(sfg_context* c, int nsteps) {
             enqueue_step(c, p);
         }
         if (c->any_adr) {
-            if (c->adr_pending_h) c->g_cur = 1 - p;
-            c->adr_pending_h = true;
+            if (c->any_chem) {
+                c->g_cur = 1 - p;    // scalar step done inside the step
+            } else {
+                if (c->adr_pending_h) c->g_cur = 1 - p;
+                c->adr_pending_h = true;
+            }
         }
         ++c->steps;
     }
@@ -1533,6 +1659,7 @@ extern "C" int sfg_set_concentration(sfg_context* c, int chi, const double* C) {
         k_scalar_set<float><<<io_blocks(N), 256, 0, c->stream>>>(c->d_io, (float*)c->g[0], (float*)c->g[1], (float*)c->cfield, d);
     const int one = 1;
     CU(cudaMemcpyAsync(c->d_c_fresh + chi, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    if (c->d_cov) CU(cudaMemsetAsync(c->d_cov + d.cell_off, 0, (size_t)d.plane, c->stream));
     CU(cudaGetLastError());
     CU(cudaStreamSynchronize(c->stream));
     return SFG_OK;
@@ -1555,6 +1682,7 @@ extern "C" int sfg_set_scalar_state(sfg_context* c, int chi, const double* C, co
         k_scalar_import<float><<<io_blocks(N), 256, 0, c->stream>>>(c->d_io, c->d_io + N, (float*)c->g[0], (float*)c->g[1], (float*)c->cfield, d);
     const int one = 1;
     CU(cudaMemcpyAsync(c->d_c_fresh + chi, &one, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    if (c->d_cov) CU(cudaMemsetAsync(c->d_cov + d.cell_off, 0, (size_t)d.plane, c->stream));
     CU(cudaGetLastError());
     CU(cudaStreamSynchronize(c->stream));
     return SFG_OK;
@@ -1584,9 +1712,9 @@ extern "C" int sfg_get_concentration(sfg_context* c, int chi, double* C, double*
     if ((rc = ensure_io(c, 10 * N))) return rc;
     double* o = c->d_io;
     if (c->precision == SFG_FP64)
-        k_scalar_export<double><<<io_blocks(N), 256, 0, c->stream>>>((const double*)c->g[c->g_cur], d, o, g ? o + N : nullptr);
+        k_scalar_export<double><<<io_blocks(N), 256, 0, c->stream>>>((const double*)c->g[c->g_cur], d, o, g ? o + N : nullptr, (const double*)c->cfield, c->d_cov);
     else
-        k_scalar_export<float><<<io_blocks(N), 256, 0, c->stream>>>((const float*)c->g[c->g_cur], d, o, g ? o + N : nullptr);
+        k_scalar_export<float><<<io_blocks(N), 256, 0, c->stream>>>((const float*)c->g[c->g_cur], d, o, g ? o + N : nullptr, (const float*)c->cfield, c->d_cov);
     CU(cudaGetLastError());
     if (C) CU(cudaMemcpyAsync(C, o, N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if (g) CU(cudaMemcpyAsync(g, o + N, 9 * N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -1670,11 +1798,11 @@ static int enqueue_thermo(sfg_context* c) {
     const int stepped = c->steps > 0 || c->restored;
     const void* g = c->any_adr ? c->g[c->g_cur] : nullptr;
     if (c->precision == SFG_FP64)
-        launch_thermo_cells<double, double>(c->f[p], g, c->d_chans, nch, c->thermo_bpc, tv, stepped, c->d_thermo_parts, c->stream);
+        launch_thermo_cells<double, double>(c->f[p], g, c->d_chans, nch, c->thermo_bpc, tv, stepped, c->d_thermo_parts, c->cfield, c->d_cov, c->stream);
     else if (c->precision == SFG_FP32)
-        launch_thermo_cells<float, float>(c->f[p], g, c->d_chans, nch, c->thermo_bpc, tv, stepped, c->d_thermo_parts, c->stream);
+        launch_thermo_cells<float, float>(c->f[p], g, c->d_chans, nch, c->thermo_bpc, tv, stepped, c->d_thermo_parts, c->cfield, c->d_cov, c->stream);
     else
-        launch_thermo_cells<__half, float>(c->f[p], g, c->d_chans, nch, c->thermo_bpc, tv, stepped, c->d_thermo_parts, c->stream);
+        launch_thermo_cells<__half, float>(c->f[p], g, c->d_chans, nch, c->thermo_bpc, tv, stepped, c->d_thermo_parts, c->cfield, c->d_cov, c->stream);
     if (c->NC > 0) launch_capsule_stats(c->d_caps, c->NC, c->mb.pos, c->d_cap_stats, c->stream);
     k_thermo_final<<<(nch + 127) / 128, 128, 0, c->stream>>>(
         c->d_chans, nch, c->thermo_bpc, c->d_thermo_parts, c->d_cap_stats, c->tb.capped,

@@ -914,6 +914,52 @@ k_scalar_flush(const RowItem* __restrict__ items, int n_items, const ChannelDev*
                     0u);
 }
 
+// Scalar step of this step right after its lattice step, for contexts with
+// capsule chemistry (the chemistry follows it within the step, as in
+// Simulation::step, simulation.cpp:636-653).  src: the streamed populations
+// of this step; tv: this step's forces.  The concentration of a node whose
+// value the chemistry overwrote (cov) is the stored one; the flag is
+// consumed here.
+template <typename S, typename R>
+__global__ void __launch_bounds__(256)
+k_scalar_now(const RowItem* __restrict__ items, int n_items, const ChannelDev* __restrict__ chans,
+             const S* __restrict__ src, const R* __restrict__ gsrc, R* __restrict__ gdst,
+             const R* __restrict__ cfield, unsigned char* __restrict__ cov, TileView tv,
+             const int* __restrict__ c_fresh) {
+    const int item = blockIdx.x * ITEMS_PER_CTA + (threadIdx.x >> 5);
+    if (item >= n_items) return;
+    const RowItem it = items[item];
+    const int lane = threadIdx.x & 31;
+    if (lane >= it.len) return;
+    const ChannelDev& ch = chans[it.chan];
+    if (!ch.adr) return;
+    const int nx = ch.nx, ny = ch.ny, pitch = ch.pitch, plane = (int)ch.plane;
+    const int x = it.x0 + lane, y = it.y;
+    const int n = y * pitch + x;
+    const S* fs = src + ch.f_off + n;
+    R f[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) f[q] = PopIO<S, R>::ld(fs + q * plane, q);
+    R rho, jx, jy;
+    lattice_moments(f, rho, jx, jy);
+    const CellForces<R> cf = cell_forces<R>(ch, x, y, tv, 1);
+    R g[9];
+    const R* gp = gsrc + ch.g_off + n;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) g[q] = gp[q * plane];
+    R C;
+    const bool stored = c_fresh[it.chan] || (cov != nullptr && cov[ch.cell_off + n]);
+    if (stored) C = cfield[ch.cell_off + n];
+    else C = g[0] + g[1] + g[2] + g[3] + g[4] + g[5] + g[6] + g[7] + g[8];
+    if (cov != nullptr) cov[ch.cell_off + n] = 0;
+    R vx, vy;
+    cell_velocity(rho, jx, jy, cf.Fx, cf.Fy, vx, vy);
+    collide_scalar(g, C, vx, vy, R(ch.omega_s));
+    const int gmode = ch.periodic_y ? (ch.adr_periodic_y ? 1 : 2) : 0;
+    push_cell<R, R, false>(gdst + ch.g_off, g, x, y, n, pitch, plane,
+                           neighbours(x, y, nx, ny, gmode), 0u);
+}
+
 // ---- host <-> device population transfer (canonical FP64 [9][ny][nx]) ----
 
 template <typename S, typename R>
@@ -1034,7 +1080,8 @@ __global__ void k_macro_export(const S* __restrict__ in, ChannelDev ch, TileView
 template <typename S, typename R>
 __global__ void __launch_bounds__(THERMO_THREADS)
 k_thermo_cells(const S* __restrict__ in, const R* __restrict__ g, const ChannelDev* __restrict__ chans,
-               TileView tv_last, int stepped, ThermoPart* __restrict__ parts) {
+               TileView tv_last, int stepped, ThermoPart* __restrict__ parts,
+               const R* __restrict__ cfield, const unsigned char* __restrict__ cov) {
     __shared__ ThermoPart sp[THERMO_THREADS];
     const ChannelDev& ch = chans[blockIdx.y];
     ThermoPart p;
@@ -1064,7 +1111,9 @@ k_thermo_cells(const S* __restrict__ in, const R* __restrict__ g, const ChannelD
 #pragma unroll
             for (int q = 0; q < 9; ++q) v[q] = g[ch.g_off + q * ch.plane + n];
             const R c = v[0] + v[1] + v[2] + v[3] + v[4] + v[5] + v[6] + v[7] + v[8];
-            p.sum_c = __dadd_rn(p.sum_c, (double)c);
+            const double cc = (cov != nullptr && cov[ch.cell_off + n])
+                                  ? (double)cfield[ch.cell_off + n] : (double)c;
+            p.sum_c = __dadd_rn(p.sum_c, cc);
         }
     }
     sp[threadIdx.x] = p;

@@ -86,6 +86,16 @@ void launch_lattice_step(const LatticeLaunch& L, const TileViewArgs& tv, cudaStr
 }
 
 template <typename S, typename R>
+void launch_scalar_now(const LatticeLaunch& L, const TileViewArgs& tv, unsigned char* cov,
+                       cudaStream_t st) {
+    if (L.n_items == 0) return;
+    k_scalar_now<S, R><<<(L.n_items + ITEMS_PER_CTA - 1) / ITEMS_PER_CTA, 32 * ITEMS_PER_CTA, 0,
+                         st>>>(L.items, L.n_items, L.chans, static_cast<const S*>(L.dst),
+                               static_cast<const R*>(L.gsrc), static_cast<R*>(L.gdst),
+                               static_cast<const R*>(L.cfield), cov, to_view(tv), L.c_fresh);
+}
+
+template <typename S, typename R>
 void launch_scalar_flush(const LatticeLaunch& L, const TileViewArgs& tv_last, cudaStream_t st) {
     if (L.n_items == 0 || !L.any_adr) return;
     k_scalar_flush<S, R><<<(L.n_items + ITEMS_PER_CTA - 1) / ITEMS_PER_CTA,
@@ -122,10 +132,11 @@ void launch_macro_export(const void* in, const ChannelDev& ch, const TileViewArg
 template <typename S, typename R>
 void launch_thermo_cells(const void* in, const void* g, const ChannelDev* chans, int nch,
                          int blocks_per_chan, const TileViewArgs& tv_last, int stepped,
-                         ThermoPart* parts, cudaStream_t st) {
+                         ThermoPart* parts, const void* cfield, const unsigned char* cov,
+                         cudaStream_t st) {
     k_thermo_cells<S, R><<<dim3(blocks_per_chan, nch), THERMO_THREADS, 0, st>>>(
         static_cast<const S*>(in), static_cast<const R*>(g), chans, to_view(tv_last), stepped,
-        parts);
+        parts, static_cast<const R*>(cfield), cov);
 }
 
 template <typename S, typename R>
@@ -147,12 +158,15 @@ int lattice_ctas_per_sm_t(bool adr) {
                                             cudaStream_t);                                        \
     template void launch_scalar_flush<S, R>(const LatticeLaunch&, const TileViewArgs&,           \
                                             cudaStream_t);                                        \
+    template void launch_scalar_now<S, R>(const LatticeLaunch&, const TileViewArgs&,             \
+                                          unsigned char*, cudaStream_t);                          \
     template void launch_pop_import<S, R>(const double*, void*, const ChannelDev&, cudaStream_t); \
     template void launch_pop_export<S, R>(const void*, double*, const ChannelDev&, cudaStream_t); \
     template void launch_macro_export<S, R>(const void*, const ChannelDev&, const TileViewArgs&,  \
                                             int, double*, double*, double*, double*, double*,     \
                                             cudaStream_t);                                        \
     template void launch_thermo_cells<S, R>(const void*, const void*, const ChannelDev*, int, int, \
-                                            const TileViewArgs&, int, ThermoPart*, cudaStream_t);
+                                            const TileViewArgs&, int, ThermoPart*, const void*,   \
+                                            const unsigned char*, cudaStream_t);
 
 }  // namespace sfg

@@ -1,6 +1,7 @@
 // sfg_internal.h -- device buffer bundles and launch wrappers shared by the
 // translation units of libsoftflow_b200.so (not part of the C ABI).
 #pragma once
+#include "../../include/softflow_gpu.h"
 #include "common.cuh"
 #include "markers.cuh"
 
@@ -147,6 +148,19 @@ template <typename S, typename R>
 void launch_lattice_step(const LatticeLaunch& L, const TileViewArgs& tv, cudaStream_t st);
 template <typename S, typename R>
 void launch_scalar_flush(const LatticeLaunch& L, const TileViewArgs& tv_last, cudaStream_t st);
+// Scalar step of the current step on its streamed populations (L.dst) and
+// forces (contexts with capsule chemistry).
+template <typename S, typename R>
+void launch_scalar_now(const LatticeLaunch& L, const TileViewArgs& tv, unsigned char* cov,
+                       cudaStream_t st);
+// Capsule chemistry of every channel that has it (chemistry.cu).
+size_t chem_box_bytes();
+template <typename R>
+void launch_chemistry(const ChannelDev* chans, int nch, const sfg_chemistry* params,
+                      const CapsuleDev* caps, const double2* pos, const double* phi, void* g_new,
+                      void* g_old, void* cfield, unsigned char* cov, double* released,
+                      double* absorbed, double* Mp, double* gamma, int* wave_buf,
+                      void* box_buf, int box_cap, unsigned* status, cudaStream_t st);
 template <typename S, typename R>
 void launch_pop_import(const double* in, void* out, const ChannelDev& ch, cudaStream_t st);
 template <typename S, typename R>
@@ -159,7 +173,8 @@ void launch_macro_export(const void* in, const ChannelDev& ch, const TileViewArg
 template <typename S, typename R>
 void launch_thermo_cells(const void* in, const void* g, const ChannelDev* chans, int nch,
                          int blocks_per_chan, const TileViewArgs& tv_last, int stepped,
-                         ThermoPart* parts, cudaStream_t st);
+                         ThermoPart* parts, const void* cfield, const unsigned char* cov,
+                         cudaStream_t st);
 // Geometry of every capsule: out [ncaps][6] = centroid x, y, area, perimeter,
 // deformation, inclination.
 void launch_capsule_stats(const CapsuleDev* caps, int ncaps, const double2* pos, double* out,

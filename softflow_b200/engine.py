@@ -137,6 +137,14 @@ class ScalarParams:
     diffusivity: List[float] = field(default_factory=lambda: [0.01])
     inlet_concentration: List[float] = field(default_factory=lambda: [0.0])
     periodic_y: bool = False
+    # capsule chemistry kinetics per capsule type (parameters.h:214-228);
+    # empty vectors select the constant release / absorption rates
+    k_leach: List[float] = field(default_factory=list)
+    C_eq: List[float] = field(default_factory=list)
+    M_p_initial: List[float] = field(default_factory=list)
+    k_adsorb: List[float] = field(default_factory=list)
+    k_desorb: List[float] = field(default_factory=list)
+    Gamma_max: List[float] = field(default_factory=list)
 
 
 @dataclass
@@ -306,6 +314,30 @@ class _Channel:
         self.caps: List[_CapsuleRec] = []
         self.pillars: List[tuple] = []
         self.walls_in_placement = False
+        self.release_rates: List[float] = []
+        self.absorption_rates: List[float] = []
+
+    def chemistry(self) -> Optional[L.ChemistryC]:
+        """sfg_chemistry of the channel, or None when no vector is set
+        (Simulation::step then runs no chemistry, simulation.cpp:640-653)."""
+        sc = self.params.scalar
+        vecs = {"release": self.release_rates, "absorb": self.absorption_rates,
+                "k_leach": sc.k_leach, "C_eq": sc.C_eq, "M_p_initial": sc.M_p_initial,
+                "k_adsorb": sc.k_adsorb, "k_desorb": sc.k_desorb, "Gamma_max": sc.Gamma_max}
+        if not any(len(v) for v in vecs.values()):
+            return None
+        counts = {"release": "n_release", "absorb": "n_absorb", "k_leach": "n_k_leach",
+                  "C_eq": "n_C_eq", "M_p_initial": "n_M_p", "k_adsorb": "n_k_adsorb",
+                  "k_desorb": "n_k_desorb", "Gamma_max": "n_Gamma_max"}
+        c = L.ChemistryC()
+        for k, v in vecs.items():
+            if len(v) > 8:
+                raise ValueError(f"at most 8 capsule types ({k})")
+            setattr(c, counts[k], len(v))
+            arr = getattr(c, k)
+            for i, x in enumerate(v):
+                arr[i] = float(x)
+        return c
 
     def add_capsule(self, center, radius, num_nodes=0, mparams=None, type_id=0):
         mp = mparams if mparams is not None else self.params.membrane
@@ -366,6 +398,13 @@ class _Context:
                     L.check(lib.sfg_add_capsule(h, idx.value, C.byref(mpc), C.byref(rec.rest),
                                                 L.dptr(rec.pos), L.dptr(rec.rest_len),
                                                 L.dptr(rec.rest_ang), L.dptr(rec.rest_ds), None))
+                for k, rec in enumerate(ch.caps):
+                    if rec.type_id:
+                        L.check(lib.sfg_set_capsule_type(h, idx.value, k, int(rec.type_id)))
+                chem = ch.chemistry()
+                if chem is not None:
+                    self._chem_keep = getattr(self, "_chem_keep", []) + [chem]
+                    L.check(lib.sfg_set_chemistry(h, idx.value, C.byref(chem)))
             L.check(lib.sfg_initialize(h))
         except Exception:
             lib.sfg_destroy(h)
@@ -643,6 +682,30 @@ class ScalarView:
     def __init__(self, ctx: _Context, chan: int, nx: int, ny: int):
         self._ctx, self._ch, self.nx, self.ny = ctx, chan, nx, ny
 
+    def _chem(self):
+        lib, h = self._ctx._lib, self._ctx._h
+        nc, nm = C.c_int(), C.c_int()
+        L.check(lib.sfg_channel_counts(h, self._ch, C.byref(nc), C.byref(nm)))
+        out = [np.zeros(max(nc.value, 1)) for _ in range(3)] + [np.zeros(max(nm.value, 1))]
+        L.check(lib.sfg_get_chemistry_state(h, self._ch, *[L.dptr(a) for a in out]))
+        nodes = (C.c_int * max(nc.value, 1))()
+        L.check(lib.sfg_get_capsule_nodes(h, self._ch, nodes))
+        return out, list(nodes)[:nc.value]
+
+    # chemistry state (AdvectionDiffusion accessors, advection_diffusion.h:75-103)
+    def getCapsuleReleased(self, capsule_id: int) -> float:
+        return float(self._chem()[0][0][capsule_id])
+
+    def getCapsuleAbsorbed(self, capsule_id: int) -> float:
+        return float(self._chem()[0][1][capsule_id])
+
+    def getCapsuleMp(self, capsule_id: int) -> float:
+        return float(self._chem()[0][2][capsule_id])
+
+    def getNodeGamma(self, capsule_id: int, node: int) -> float:
+        (st, nodes) = self._chem()
+        return float(st[3][sum(nodes[:capsule_id]) + node])
+
     def concentration(self, species: int = 0):
         Cf = np.zeros(self.nx * self.ny)
         L.check(self._ctx._lib.sfg_get_concentration(self._ctx._h, self._ch, L.dptr(Cf), None))
@@ -716,6 +779,34 @@ class Ensemble:
         """Apply the channel-builder wall test in random placement
         (simulation.cpp:250-256), as the declarative Python API does."""
         self._chans[chan].walls_in_placement = bool(enabled)
+
+    def setScalarReleaseRate(self, chan: int, capsule_type: int, rate: float):
+        """Simulation::setScalarReleaseRate (simulation.cpp:929-935)."""
+        self._pre_init()
+        v = self._chans[chan].release_rates
+        if capsule_type >= len(v):
+            v.extend([0.0] * (capsule_type + 1 - len(v)))
+        v[capsule_type] = float(rate)
+
+    def setScalarAbsorptionRate(self, chan: int, capsule_type: int, rate: float):
+        """Simulation::setScalarAbsorptionRate (simulation.cpp:936-942)."""
+        self._pre_init()
+        v = self._chans[chan].absorption_rates
+        if capsule_type >= len(v):
+            v.extend([0.0] * (capsule_type + 1 - len(v)))
+        v[capsule_type] = float(rate)
+
+    def chemistryState(self, chan: int = 0):
+        """(released [capsules], absorbed [capsules], Mp [capsules],
+        gamma [markers]) of a channel (AdvectionDiffusion's per-capsule and
+        per-node chemistry state)."""
+        ctx = self._need()
+        n = len(self._chans[chan].caps)
+        m = sum(r.rest.num_nodes for r in self._chans[chan].caps)
+        out = [np.zeros(max(n, 1)), np.zeros(max(n, 1)), np.zeros(max(n, 1)),
+               np.zeros(max(m, 1))]
+        L.check(ctx._lib.sfg_get_chemistry_state(ctx._h, chan, *[L.dptr(a) for a in out]))
+        return out[0][:n], out[1][:n], out[2][:n], out[3][:m]
 
     def setChannelBuilder(self, chan: int, builder: "ChannelBuilder"):
         """Simulation::setChannelBuilder (simulation.cpp:211-213): the
@@ -978,6 +1069,12 @@ class Simulation(Ensemble):
 
     def setChannelBuilder(self, builder: "ChannelBuilder"):
         super().setChannelBuilder(0, builder)
+
+    def setScalarReleaseRate(self, capsule_type: int, rate: float):
+        super().setScalarReleaseRate(0, capsule_type, rate)
+
+    def setScalarAbsorptionRate(self, capsule_type: int, rate: float):
+        super().setScalarAbsorptionRate(0, capsule_type, rate)
 
     def setStepCallback(self, fn):
         """fn(sim, step) after every step (Simulation::setStepCallback; step

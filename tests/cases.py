@@ -193,6 +193,8 @@ def gpu_params(case, precision):
     p.scalar.diffusivity = [sp["scalar_D"]]
     p.scalar.periodic_y = bool(sp["scalar_periodic_y"])
     p.scalar.inlet_concentration = [sp["scalar_inlet"]]
+    for k in ("k_leach", "C_eq", "M_p_initial", "k_adsorb", "k_desorb", "Gamma_max"):
+        setattr(p.scalar, k, list((case.get("chem") or {}).get(k, [])))
     p.precision = precision
     return p
 
@@ -212,8 +214,9 @@ def add_case_capsules(ens, chan, case):
     import softflow_b200 as S
     for c in case["capsules"]:
         if c[0] == "add":
-            _, cx, cy, r, nn, mk = c
-            S.Ensemble.addCapsule(ens, chan, (cx, cy), r, nn, gpu_membrane(mk))
+            _, cx, cy, r, nn, mk = c[:6]
+            S.Ensemble.addCapsule(ens, chan, (cx, cy), r, nn, gpu_membrane(mk),
+                                  c[6] if len(c) > 6 else 0)
         else:
             _, count, x0, y0, x1, y1, rmin, rmax, nn, mk, seed, gap, walls = c
             S.Ensemble.addCapsuleRandom(ens, chan, count, x0, y0, x1, y1, rmin, rmax, nn,
@@ -234,6 +237,11 @@ def build_gpu(case, precision="fp32"):
                 b.addRectPillar(*ob[1:])
         sim.setChannelBuilder(b)
     add_case_capsules(sim, 0, case)
+    chem = case.get("chem") or {}
+    for t, r in enumerate(chem.get("release", [])):
+        sim.setScalarReleaseRate(t, r)
+    for t, r in enumerate(chem.get("absorb", [])):
+        sim.setScalarAbsorptionRate(t, r)
     sim.initialize()
     if case["conc"] is not None:
         sp = case["spec"]
