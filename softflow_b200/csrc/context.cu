@@ -261,6 +261,10 @@ struct sfg_context {
     bool any_bc = false;                // boundary-aware lattice kernel in use
     RowItem* d_zh_rows = nullptr;       // Zou-He rows (channel, y)
     int n_zh = 0;
+    // independent launch groups at the start of a step (contact cell list,
+    // force tiles + tile moments) run on side streams, joined by events
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_contact = nullptr, ev_tiles = nullptr, ev_mom = nullptr;
     // pipelined marker output: snapshots on the context stream, copied to
     // the host on a copy stream while later steps run
     cudaStream_t copy_stream = nullptr;
@@ -434,6 +438,17 @@ static void free_all(sfg_context* c) {
     }
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     c->copy_stream = nullptr;
+    for (int i = 0; i < 2; ++i) {
+        if (c->side[i]) {
+            cudaStreamSynchronize(c->side[i]);
+            cudaStreamDestroy(c->side[i]);
+        }
+        c->side[i] = nullptr;
+    }
+    for (cudaEvent_t* e : {&c->ev_fork, &c->ev_contact, &c->ev_tiles, &c->ev_mom}) {
+        if (*e) cudaEventDestroy(*e);
+        *e = nullptr;
+    }
     c->d_masks = nullptr;
     c->d_ibb = nullptr;
     F(c->d_thermo_parts); F(c->d_cap_stats); F(c->d_thermo);
@@ -1053,6 +1068,11 @@ extern "C" int sfg_initialize(sfg_context* c) {
     c->nsm = nsm;
     apply_launch_config(c);
     CU(cudaStreamSynchronize(c->stream));
+    if (c->M > 0 && !c->side[0]) {
+        for (int i = 0; i < 2; ++i) CU(cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking));
+        for (cudaEvent_t* e : {&c->ev_fork, &c->ev_contact, &c->ev_tiles, &c->ev_mom})
+            CU(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
     c->initialized = true;
     c->steps = 0;
     return SFG_OK;
@@ -1085,22 +1105,49 @@ static int enqueue_step_t(sfg_context* c, int p) {
         cudaMemsetAsync(c->tb.resid_gate, 0, sizeof(unsigned) * nch, st);
         cudaMemsetAsync(c->tb.resid_plain, 0, sizeof(unsigned) * nch, st);
         cudaMemsetAsync(c->tb.spread_ctr, 0, sizeof(int) * c->tb.n_spread_ctr, st);
-        launch_membrane(c->d_caps, c->NC, c->mb, c->d_has_prev, c->maxn, c->d_status, st);
-        mark(c, SFG_PHASE_MEMBRANE);
-        launch_contact(c->d_chans, c->M, c->mb, c->cb, c->ncells, st);
-        mark(c, SFG_PHASE_CONTACT);
-        launch_tiles(c->d_chans, c->d_caps, c->M, c->mb, c->tb, c->tb.T, p, c->d_phi, c->d_status,
-                     st);
-        mark(c, SFG_PHASE_IBM_TILES);
-        launch_spread<R>(c->d_chans, c->mb, c->tb, p, 0, MDF_PLAIN, 0, c->spread_grid,
-                         c->d_status, st);
-        mark(c, SFG_PHASE_IBM_SPREAD);
-        launches += 1 + (c->ncells > 0 ? 7 : 1) + 9 + 1;
         const S* fp = static_cast<const S*>(c->f[p]);
-        if (c->Kmax > 1) {
-            launch_tile_moments<S, R>(c->d_chans, fp, c->tb, c->spread_grid, st);
-            mark(c, SFG_PHASE_MDF_INTERP);
-            launches += 1;
+        // The contact cell list and the force tiles read positions only, the
+        // tile moments the populations: with profiling off they run beside
+        // the membrane forces on side streams and join before their users.
+        const bool par = !c->profiling && c->side[0] != nullptr;
+        if (par) {
+            CU(cudaEventRecord(c->ev_fork, st));
+            CU(cudaStreamWaitEvent(c->side[0], c->ev_fork, 0));
+            CU(cudaStreamWaitEvent(c->side[1], c->ev_fork, 0));
+            launch_contact_prep(c->d_chans, c->M, c->mb, c->cb, c->ncells, c->side[0]);
+            CU(cudaEventRecord(c->ev_contact, c->side[0]));
+            launch_tiles(c->d_chans, c->d_caps, c->M, c->mb, c->tb, c->tb.T, p, c->d_phi,
+                         c->d_status, c->side[1]);
+            CU(cudaEventRecord(c->ev_tiles, c->side[1]));
+            if (c->Kmax > 1) {
+                launch_tile_moments<S, R>(c->d_chans, fp, c->tb, c->spread_grid, c->side[1]);
+                CU(cudaEventRecord(c->ev_mom, c->side[1]));
+            }
+            launch_membrane(c->d_caps, c->NC, c->mb, c->d_has_prev, c->maxn, c->d_status, st);
+            CU(cudaStreamWaitEvent(st, c->ev_contact, 0));
+            launch_contact_force(c->d_chans, c->M, c->mb, c->cb, st);
+            CU(cudaStreamWaitEvent(st, c->ev_tiles, 0));
+            launch_spread<R>(c->d_chans, c->mb, c->tb, p, 0, MDF_PLAIN, 0, c->spread_grid,
+                             c->d_status, st);
+            if (c->Kmax > 1) CU(cudaStreamWaitEvent(st, c->ev_mom, 0));
+            launches += 1 + (c->ncells > 0 ? 7 : 1) + 9 + 1 + (c->Kmax > 1 ? 1 : 0);
+        } else {
+            launch_membrane(c->d_caps, c->NC, c->mb, c->d_has_prev, c->maxn, c->d_status, st);
+            mark(c, SFG_PHASE_MEMBRANE);
+            launch_contact(c->d_chans, c->M, c->mb, c->cb, c->ncells, st);
+            mark(c, SFG_PHASE_CONTACT);
+            launch_tiles(c->d_chans, c->d_caps, c->M, c->mb, c->tb, c->tb.T, p, c->d_phi,
+                         c->d_status, st);
+            mark(c, SFG_PHASE_IBM_TILES);
+            launch_spread<R>(c->d_chans, c->mb, c->tb, p, 0, MDF_PLAIN, 0, c->spread_grid,
+                             c->d_status, st);
+            mark(c, SFG_PHASE_IBM_SPREAD);
+            launches += 1 + (c->ncells > 0 ? 7 : 1) + 9 + 1;
+            if (c->Kmax > 1) {
+                launch_tile_moments<S, R>(c->d_chans, fp, c->tb, c->spread_grid, st);
+                mark(c, SFG_PHASE_MDF_INTERP);
+                launches += 1;
+            }
         }
         if (c->any_learned) {
             // seed, one plain sweep, gate; the plain sweeps below run only for

@@ -1136,6 +1136,20 @@ void launch_membrane(const CapsuleDev* caps, int ncaps, const MarkerBufs& mb, in
 
 void launch_contact(const ChannelDev* chans, int M, const MarkerBufs& mb, ContactBufs& cb,
                     int ncells, cudaStream_t st) {
+    launch_contact_prep(chans, M, mb, cb, ncells, st);
+    launch_contact_force(chans, M, mb, cb, st);
+}
+
+void launch_contact_force(const ChannelDev* chans, int M, const MarkerBufs& mb, ContactBufs& cb,
+                          cudaStream_t st) {
+    if (M == 0) return;
+    const int B = 256, G = (M + B - 1) / B;
+    k_contact_force<<<G, B, 0, st>>>(chans, M, mb, cb.cell_of, cb.cell_start, cb.cell_cnt,
+                                     cb.list);
+}
+
+void launch_contact_prep(const ChannelDev* chans, int M, const MarkerBufs& mb, ContactBufs& cb,
+                         int ncells, cudaStream_t st) {
     if (M == 0) return;
     const int B = 256, G = (M + B - 1) / B;
     if (ncells > 0) {
@@ -1148,8 +1162,6 @@ void launch_contact(const ChannelDev* chans, int M, const MarkerBufs& mb, Contac
         k_contact_sort<<<(ncells + B - 1) / B, B, 0, st>>>(ncells, cb.cell_start, cb.cell_cnt,
                                                            cb.list);
     }
-    k_contact_force<<<G, B, 0, st>>>(chans, M, mb, cb.cell_of, cb.cell_start, cb.cell_cnt,
-                                     cb.list);
 }
 
 void launch_tiles(const ChannelDev* chans, const CapsuleDev* caps, int M, const MarkerBufs& mb,

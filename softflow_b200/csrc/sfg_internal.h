@@ -69,6 +69,12 @@ void launch_membrane(const CapsuleDev* caps, int ncaps, const MarkerBufs& mb, in
                      int maxn, unsigned* status, cudaStream_t st);
 void launch_contact(const ChannelDev* chans, int M, const MarkerBufs& mb, ContactBufs& cb,
                     int ncells, cudaStream_t st);
+// The cell list (binning, scan, fill, sort: positions only) and the pair
+// forces (added to the membrane forces) as separate launch groups.
+void launch_contact_prep(const ChannelDev* chans, int M, const MarkerBufs& mb, ContactBufs& cb,
+                         int ncells, cudaStream_t st);
+void launch_contact_force(const ChannelDev* chans, int M, const MarkerBufs& mb, ContactBufs& cb,
+                          cudaStream_t st);
 void launch_tiles(const ChannelDev* chans, const CapsuleDev* caps, int M, const MarkerBufs& mb,
                   TileBufs& tb, int T, int parity, const double* phi_tbl, unsigned* status,
                   cudaStream_t st);
