@@ -132,3 +132,140 @@ def test_autotuned_launch_shapes_keep_results(sfg, learned):
     b.run(7)
     assert np.array_equal(a.field().distributions(), b.field().distributions())
     assert np.array_equal(a.capsules().positions(), b.capsules().positions())
+
+
+def _feq(rho, ux, uy):
+    """Second-order equilibrium of reference lattice.h:35-39, [9][ny][nx]."""
+    W = np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4)
+    CX = np.array([0, 1, 0, -1, 0, 1, -1, -1, 1])
+    CY = np.array([0, 0, 1, 0, -1, 1, 1, -1, -1])
+    cs2 = 1.0 / 3.0
+    out = np.empty((9,) + rho.shape)
+    uu = ux * ux + uy * uy
+    for q in range(9):
+        eu = CX[q] * ux + CY[q] * uy
+        out[q] = W[q] * rho * (1.0 + eu / cs2 + eu * eu / (2 * cs2 * cs2) - uu / (2 * cs2))
+    return out
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 0.02), ("fp32", 0.02), ("fp16s", 0.03)])
+def test_taylor_green_decay(sfg, precision, tol):
+    """test_taylor_green.cpp:36-104: a 64 x 64 doubly periodic Taylor-Green
+    vortex (U0 0.04, BGK tau 0.8) loses kinetic energy as exp(-2 nu k^2 t):
+    after one e-fold of the amplitude E(t)/E(0) is exp(-2) within 2 %."""
+    import softflow_b200 as S
+    nx = ny = 64
+    p = S.SimulationParams(nx=nx, ny=ny, precision=precision)
+    p.fluid.boundary_type = S.BoundaryType.PERIODIC
+    p.fluid.periodic_y = True
+    p.fluid.collision_model = S.CollisionModel.BGK
+    p.fluid.tau = 0.8
+    p.enable_stability_checks = False
+    sim = S.Simulation(p)
+    sim.initialize()
+    U0, kx, ky = 0.04, 2 * math.pi / nx, 2 * math.pi / ny
+    y, x = np.mgrid[0:ny, 0:nx].astype(float)
+    ux = -U0 * np.cos(kx * x) * np.sin(ky * y)
+    uy = U0 * np.sin(kx * x) * np.cos(ky * y)
+    rho = 1.0 - (U0 * U0 / (4.0 / 3.0)) * (np.cos(2 * kx * x) + np.cos(2 * ky * y))
+    sim.field().set_distributions(_feq(rho, ux, uy))
+    E0 = 0.5 * float((ux * ux + uy * uy).sum())
+    nu = (p.fluid.tau - 0.5) / 3.0
+    n = int(1.0 / (nu * (kx * kx + ky * ky)))
+    sim.run(n)
+    f = sim.field()
+    Et = 0.5 * float((f.velocity_x() ** 2 + f.velocity_y() ** 2).sum())
+    err = abs(Et / E0 - math.exp(-2.0)) / math.exp(-2.0)
+    print(f"Taylor-Green {precision}: E(t)/E(0) {Et / E0:.6f}, rel err {err:.3e}")
+    assert err < tol
+
+
+def test_tank_treading_frequency(sfg):
+    """test_capsule_shear.cpp:15-150: a Skalak capsule (R 5) in plane Couette
+    flow (walls at +-0.02, 80 x 64, regularized tau 0.8) tank-treads at
+    f = gamma_dot / (4 pi) (Keller-Skalak, 2D) within 10 %: zero crossings of
+    node 0's height above the centroid over the second half of the record."""
+    import softflow_b200 as S
+    p = S.SimulationParams(nx=80, ny=64, precision="fp32")
+    p.fluid.boundary_type = S.BoundaryType.PERIODIC
+    p.fluid.collision_model = S.CollisionModel.REGULARIZED
+    p.fluid.tau = 0.8
+    Uw = 0.02
+    p.fluid.top_wall_velocity, p.fluid.bottom_wall_velocity = Uw, -Uw
+    p.enable_stability_checks = False
+    mp = S.MembraneParams(model=S.MembraneModel.SKALAK, G_s=0.002, C_skalak=10.0,
+                          k_bend=0.001, k_area=0.02, k_perimeter=0.005, gamma_visc=0.0,
+                          eta_membrane=0.0)
+    sim = S.Simulation(p)
+    R = 5.0
+    sim.addCapsule((p.nx / 2.0, p.ny / 2.0), R, max(12, math.ceil(2 * math.pi * R / 0.75)), mp)
+    sim.initialize()
+    H = p.ny - 2
+    gdot = 2.0 * Uw / H
+    sim.run(8000)
+    ry = []
+    f_meas = None
+    caps = sim.capsules()
+    for s in range(0, 200000, 50):
+        sim.run(50)
+        pos = caps.positions()
+        ry.append(float(pos[0, 1] - pos[:, 1].mean()))
+        if len(ry) > 200:
+            i0 = len(ry) // 2
+            tail = np.array(ry[i0:])
+            crossings = int(np.sum((tail[:-1] < 0) & (tail[1:] >= 0)) +
+                            np.sum((tail[:-1] > 0) & (tail[1:] <= 0)))
+            if crossings >= 6:
+                T = (len(ry) - i0) * 50 / (crossings / 2.0)
+                f_meas = 1.0 / T
+                break
+    assert f_meas is not None, "fewer than three tank-treading periods"
+    f_exp = gdot / (4.0 * math.pi)
+    rel = abs(f_meas - f_exp) / f_exp
+    print(f"tank-treading: f {f_meas:.4e}, Keller-Skalak {f_exp:.4e}, rel {rel:.3f}")
+    assert rel < 0.10
+
+
+@pytest.mark.parametrize("k_a,k_d,Gmax", [(0.0, 0.0, 1.0), (0.02, 0.005, 0.1)])
+def test_chemistry_mass_balance(sfg, k_a, k_d, Gmax):
+    """test_chemistry_mass_balance.cpp: a capsule at rest in a doubly
+    periodic box leaches from a finite reservoir (and adsorbs): reservoir +
+    sum C + sum Gamma ds stays constant to 1e-10 relative over 200 steps."""
+    import softflow_b200 as S
+    nx, ny = 128, 96
+    p = S.SimulationParams(nx=nx, ny=ny, precision="fp64")
+    p.fluid.boundary_type = S.BoundaryType.PERIODIC
+    p.fluid.periodic_y = True
+    p.fluid.collision_model = S.CollisionModel.BGK
+    p.fluid.tau = 0.6
+    p.enable_stability_checks = False
+    p.scalar.enabled = True
+    p.scalar.diffusivity = [0.01]
+    p.scalar.periodic_y = True
+    p.scalar.k_leach, p.scalar.C_eq, p.scalar.M_p_initial = [0.01], [0.05], [5.0]
+    p.scalar.k_adsorb, p.scalar.k_desorb, p.scalar.Gamma_max = [k_a], [k_d], [Gmax]
+    sim = S.Simulation(p)
+    sim.addCapsule((nx / 2.0, ny / 2.0), 32.0 / (2 * math.pi), 32, S.MembraneParams())
+    sim.initialize()
+
+    def total():
+        rel, ab, mp, gam = sim.chemistryState()
+        pos = sim.capsules().positions()
+        d_next = np.roll(pos, -1, axis=0) - pos
+        d_prev = pos - np.roll(pos, 1, axis=0)
+        ds = 0.5 * (np.hypot(*d_next.T) + np.hypot(*d_prev.T))
+        return (float(mp[mp >= 0].sum()) + float(sim.advectionDiffusion().concentration().sum())
+                + float((gam * ds).sum()))
+
+    t0 = total()
+    assert abs(t0 - 5.0) < 1e-12
+    worst = 0.0
+    for _ in range(20):
+        sim.run(10)
+        worst = max(worst, abs(total() - t0) / t0)
+    rel, ab, mp, gam = sim.chemistryState()
+    print(f"chemistry budget: worst rel err {worst:.3e}, Mp {mp[0]:.4f}")
+    assert worst < 1e-10
+    assert mp[0] < 5.0 - 1e-6
+    if k_a > 0:
+        assert gam.max() > 0
