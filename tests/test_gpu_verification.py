@@ -227,10 +227,15 @@ def test_tank_treading_frequency(sfg):
 
 
 @pytest.mark.parametrize("k_a,k_d,Gmax", [(0.0, 0.0, 1.0), (0.02, 0.005, 0.1)])
-def test_chemistry_mass_balance(sfg, k_a, k_d, Gmax):
+def test_chemistry_mass_balance(sfg, oracle_mod, k_a, k_d, Gmax):
     """test_chemistry_mass_balance.cpp: a capsule at rest in a doubly
     periodic box leaches from a finite reservoir (and adsorbs): reservoir +
-    sum C + sum Gamma ds stays constant to 1e-10 relative over 200 steps."""
+    sum C + sum Gamma ds over 200 steps.  Leaching alone conserves it to
+    1e-10 relative.  With adsorption the scalar step's undershoots (C < 0
+    near the capsule, tau_s 0.53) meet the chemistry's clamp of negative
+    concentrations, so the reference itself loses 1.4e-6 here (its own
+    sources, run on the same full steps); the GPU budget equals the
+    oracle's to rounding."""
     import softflow_b200 as S
     nx, ny = 128, 96
     p = S.SimulationParams(nx=nx, ny=ny, precision="fp64")
@@ -257,15 +262,36 @@ def test_chemistry_mass_balance(sfg, k_a, k_d, Gmax):
         return (float(mp[mp >= 0].sum()) + float(sim.advectionDiffusion().concentration().sum())
                 + float((gam * ds).sum()))
 
+    import oracle as O
+    o = O.OracleSim(O.ChannelSpec(nx=nx, ny=ny, collision=O.BGK, tau=0.6, periodic_y=1,
+                                  scalar_enabled=1, scalar_D=0.01, scalar_periodic_y=1))
+    o.add_capsule(nx / 2.0, ny / 2.0, 32.0 / (2 * math.pi), 32, O.Membrane(), 0)
+    o.set_chemistry(k_leach=[0.01], C_eq=[0.05], M_p_initial=[5.0], k_adsorb=[k_a],
+                    k_desorb=[k_d], Gamma_max=[Gmax])
+    o.initialize()
+
+    def o_total():
+        rel, ab, mp, gam = o.chemistry_state()
+        pos = o.positions()
+        d_next = np.roll(pos, -1, axis=0) - pos
+        d_prev = pos - np.roll(pos, 1, axis=0)
+        ds = 0.5 * (np.hypot(*d_next.T) + np.hypot(*d_prev.T))
+        return (float(mp[mp >= 0].sum()) + float(o.concentration().sum())
+                + float((gam * ds).sum()))
+
     t0 = total()
     assert abs(t0 - 5.0) < 1e-12
-    worst = 0.0
+    worst = worst_o = 0.0
     for _ in range(20):
         sim.run(10)
+        o.step(10)
         worst = max(worst, abs(total() - t0) / t0)
+        worst_o = max(worst_o, abs(o_total() - 5.0) / 5.0)
     rel, ab, mp, gam = sim.chemistryState()
-    print(f"chemistry budget: worst rel err {worst:.3e}, Mp {mp[0]:.4f}")
-    assert worst < 1e-10
+    print(f"chemistry budget: worst rel err {worst:.3e} (oracle {worst_o:.3e}), Mp {mp[0]:.4f}")
     assert mp[0] < 5.0 - 1e-6
-    if k_a > 0:
+    if k_a == 0.0:
+        assert worst < 1e-10
+    else:
         assert gam.max() > 0
+        assert abs(worst - worst_o) <= 1e-12
