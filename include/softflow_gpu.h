@@ -140,6 +140,18 @@ int sfg_place_random(int count, double x0, double y0, double x1, double y1, doub
                      int capacity, double* out_center, double* out_radius, int* n_placed,
                      int* n_attempts);
 
+/* sfg_place_random with the channel's pillars ([n_pillars][5]: kind 0 circle
+ * (a, b) radius c, kind 1 rectangle (a, b)-(c, d)): with check_walls a
+ * candidate whose centre lies closer than r + min_gap to a pillar is
+ * rejected, as Simulation::addCapsuleRandom does with a channel builder
+ * (simulation.cpp:250-262). */
+int sfg_place_random_pillars(int count, double x0, double y0, double x1, double y1,
+                             double rmin, double rmax, int num_nodes, int seed, double min_gap,
+                             int max_attempts, int check_walls, int nx, int ny, int n_existing,
+                             const double* existing_centroid, const double* existing_radius,
+                             int capacity, double* out_center, double* out_radius, int* n_placed,
+                             int* n_attempts, int n_pillars, const double* pillars);
+
 /* ---- context ------------------------------------------------------------ */
 int sfg_create(int device, int precision, sfg_context** out);
 int sfg_destroy(sfg_context* ctx);
@@ -162,7 +174,8 @@ int sfg_add_capsule(sfg_context* ctx, int channel, const sfg_membrane_params* mp
  * addRectPillar with Simulation::setChannelBuilder (geometry/
  * channel_builder.h:25-33, simulation.cpp:211-213, 430-442): lattice nodes
  * inside a pillar are SOLID (halfway bounce-back, or interpolated with
- * use_interpolated_bb).  Channels with pillars carry no capsules here. */
+ * use_interpolated_bb); markers are repelled from the pillars as
+ * RepulsionForce::computeObstacleRepulsion does (repulsion.cpp:180-235). */
 enum sfg_pillar { SFG_PILLAR_CIRCLE = 0, SFG_PILLAR_RECT = 1 };
 int sfg_add_pillar(sfg_context* ctx, int channel, int kind, double a, double b, double c,
                    double d);

@@ -179,6 +179,9 @@ int sfr_add_capsule_random(void* h, int count, double x0, double y0, double x1, 
         if (check_walls) {
             if (cy - r < 0.0 + min_gap || cy + r > static_cast<Real>(s->p.ny - 1) - min_gap)
                 overlap = true;
+            if (s->builder)                            // simulation.cpp:256-261
+                for (const auto& obs : s->builder->getObstacles())
+                    if (obs->signedDistance(cx, cy) < r + min_gap) { overlap = true; break; }
         }
         if (!overlap) {
             s->caps.addCapsule({cx, cy}, r, nn, mp, type);
@@ -238,6 +241,9 @@ static void one_step(RefSim* s) {
     s->caps.clearAllForces();
     s->caps.computeAllMembraneForces();
     s->rep->computeAll(s->caps, 0.5, static_cast<Real>(s->p.ny) - 1.5);
+    if (s->builder)                                // simulation.cpp:494-498
+        for (const auto& obs : s->builder->getObstacles())
+            s->rep->computeObstacleRepulsion(s->caps, *obs);
     if (s->p.ibm_iterations > 1) s->ibm.multiDirectForcing(s->caps, field, s->p.ibm_iterations);
     else s->ibm.spreadForces(s->caps, field);
     {

@@ -406,6 +406,8 @@ static int obstacle_contains(const obstacle_t* o, double x, double y) {
     return (dx * dx + dy * dy) <= o->c * o->c;
 }
 
+static double obstacle_sd(const obstacle_t* o, double x, double y);
+
 void sfo_add_circle_pillar(sfo_sim* s, double cx, double cy, double radius) {
     obstacle_t o = {0, cx, cy, radius, 0.0};
     if (s->nobs < 64) s->obs[s->nobs++] = o;
@@ -1003,6 +1005,8 @@ int sfo_add_capsule_random(sfo_sim* s, int count, double x0, double y0, double x
         }
         if (check_walls) {
             if (cy - r < 0.0 + min_gap || cy + r > (double)(s->ny - 1) - min_gap) overlap = 1;
+            for (int o = 0; o < s->nobs; ++o)                 /* simulation.cpp:256-261 */
+                if (obstacle_sd(&s->obs[o], cx, cy) < r + min_gap) { overlap = 1; break; }
         }
         if (!overlap) {
             sfo_add_capsule(s, cx, cy, r, nn, m, type);
@@ -1180,6 +1184,106 @@ static v2 pair_force(const sfo_sim* s, v2 pa, v2 va, v2 pb, v2 vb) {
         }
     }
     return vadd(vmul(nrm, F_n), F_t);
+}
+
+/* Obstacle::signedDistance / normalAt of CircleObstacle and RectObstacle
+ * (geometry/circle_obstacle.h:17-37, rect_obstacle.h:18-59); std::min and
+ * std::max over initializer lists keep the first extremum. */
+static double first_max3(double a, double b, double c) {
+    double m = a;
+    if (m < b) m = b;
+    if (m < c) m = c;
+    return m;
+}
+static double first_min4(double a, double b, double c, double d) {
+    double m = a;
+    if (b < m) m = b;
+    if (c < m) m = c;
+    if (d < m) m = d;
+    return m;
+}
+static double obstacle_sd(const obstacle_t* o, double x, double y) {
+    if (!o->rect) {
+        double dx = x - o->a, dy = y - o->b;
+        return sqrt(dx * dx + dy * dy) - o->c;
+    }
+    double dx = first_max3(o->a - x, x - o->c, 0.0);
+    double dy = first_max3(o->b - y, y - o->d, 0.0);
+    double outside = sqrt(dx * dx + dy * dy);
+    if (outside > 1e-15) return outside;
+    return -first_min4(x - o->a, o->c - x, y - o->b, o->d - y);
+}
+static v2 obstacle_normal(const obstacle_t* o, double x, double y) {
+    if (!o->rect) {
+        double dx = x - o->a, dy = y - o->b;
+        double d = sqrt(dx * dx + dy * dy);
+        v2 e = {1.0, 0.0};
+        if (d < 1e-15) return e;
+        v2 n = {dx / d, dy / d};
+        return n;
+    }
+    const double x0 = o->a, y0 = o->b, x1 = o->c, y1 = o->d;
+    double cx = x < x0 ? x0 : (x1 < x ? x1 : x);       /* std::clamp */
+    double cy = y < y0 ? y0 : (y1 < y ? y1 : y);
+    v2 np = {cx, cy};
+    if (cx == x && cy == y) {
+        double dl = x - x0, dr = x1 - x, db = y - y0, dt = y1 - y;
+        double dmin = first_min4(dl, dr, db, dt);
+        if (dmin == dl) { np.x = x0; np.y = y; }
+        else if (dmin == dr) { np.x = x1; np.y = y; }
+        else if (dmin == db) { np.x = x; np.y = y0; }
+        else { np.x = x; np.y = y1; }
+    }
+    double dx = x - np.x, dy = y - np.y;
+    double d = sqrt(dx * dx + dy * dy);
+    v2 n;
+    if (d < 1e-15) {
+        double dl = fabs(x - x0), dr = fabs(x - x1), db = fabs(y - y0), dt = fabs(y - y1);
+        double dmin = first_min4(dl, dr, db, dt);
+        if (dmin == dl) { n.x = -1.0; n.y = 0.0; }
+        else if (dmin == dr) { n.x = 1.0; n.y = 0.0; }
+        else if (dmin == db) { n.x = 0.0; n.y = -1.0; }
+        else { n.x = 0.0; n.y = 1.0; }
+        return n;
+    }
+    n.x = dx / d; n.y = dy / d;
+    return n;
+}
+
+/* RepulsionForce::computeObstacleRepulsion (membrane/repulsion.cpp:180-235)
+ * for every obstacle of the channel builder in order, after the pair and
+ * wall repulsion (engine/simulation.cpp:494-498). */
+static void obstacle_repulsion(sfo_sim* s) {
+    const sf_params* p = &s->p;
+    for (int o = 0; o < s->nobs; ++o) {
+        const obstacle_t* ob = &s->obs[o];
+        for (int k = 0; k < s->M; ++k) {
+            double sd = obstacle_sd(ob, s->pos[k].x, s->pos[k].y);
+            if (sd >= p->rep_r_cut) continue;
+            double r = fabs(sd);
+            if (r < 1e-15) r = 1e-15;
+            v2 nrm = obstacle_normal(ob, s->pos[k].x, s->pos[k].y);
+            double F_rep = p->rep_epsilon * pow(p->rep_sigma / r, (double)p->rep_power);
+            if (sd < 0.0) {
+                s->frc[k] = vadd(s->frc[k], vmul(nrm, F_rep * 10.0));
+                continue;
+            }
+            double F_n = F_rep;
+            v2 F_t = {0.0, 0.0};
+            if (p->rep_damping_normal > 0.0 || p->rep_friction > 0.0) {
+                v2 v = s->vel[k];
+                double v_n = v.x * nrm.x + v.y * nrm.y;
+                F_n = F_rep - p->rep_damping_normal * v_n;
+                if (F_n < 0.0) F_n = 0.0;
+                if (p->rep_friction > 0.0) {
+                    v2 vt = vsub(v, vmul(nrm, v_n));
+                    double vtm = vnorm(vt);
+                    if (vtm > 1e-12) F_t = vmul(vdiv(vt, vtm), -p->rep_friction * F_n);
+                }
+            }
+            s->frc[k] = vadd(s->frc[k], vadd(vmul(nrm, F_n), F_t));
+        }
+    }
 }
 
 static void wall_repulsion(sfo_sim* s, const capsule_t* c, double yb, double yt) {
@@ -1451,6 +1555,7 @@ static void one_step(sfo_sim* s) {
     for (int k = 0; k < s->M; ++k) { s->frc[k].x = 0.0; s->frc[k].y = 0.0; }   /* 1 */
     sfo_compute_membrane_forces(s);                           /* 2 */
     sfo_compute_repulsion(s);                                 /* 3 */
+    obstacle_repulsion(s);
     /* 4: with K > 1 the macroscopic recompute runs even without capsules */
     if (s->p.ibm_iterations > 1) multi_direct_forcing(s, s->p.ibm_iterations);
     else sfo_spread_forces(s);

@@ -106,6 +106,11 @@ SIGNATURES = {
                                    C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int,
                                    C.c_int, C.c_int, C.c_int, C.c_int, _D, _D, C.c_int, _D, _D,
                                    _I, _I]),
+    "sfg_place_random_pillars": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double,
+                                           C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
+                                           C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
+                                           C.c_int, _D, _D, C.c_int, _D, _D, _I, _I, C.c_int,
+                                           _D]),
     "sfg_create": (C.c_int, [C.c_int, C.c_int, _P(C.c_void_p)]),
     "sfg_destroy": (C.c_int, [C.c_void_p]),
     "sfg_add_channel": (C.c_int, [C.c_void_p, _P(ChannelParamsC), _I]),

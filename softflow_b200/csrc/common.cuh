@@ -79,6 +79,8 @@ struct ChannelDev {
                                 // pillars, null otherwise
     int chem;                   // capsule chemistry after the scalar step
     int adr_now;                // scalar step inside its own step (not lagged)
+    const double* pillars;      // [n_pillars][5]: kind (0 circle, 1 rectangle), a, b, c, d
+    int n_pillars;
 };
 
 // Cell types of a channel (reference CellType, core/types.h:48-56), as

@@ -281,6 +281,8 @@ struct sfg_context {
     int* d_waves = nullptr;             // [2 NC]
     void* d_boxes = nullptr;            // [NC] footprints
     unsigned char* d_masks = nullptr;   // cell types of channels with pillars
+    double* d_pillars = nullptr;        // [pillars][5] of every channel
+    bool pillar_repulsion = false;      // some channel has pillars and capsules
     IbbLink* d_ibb = nullptr;           // interpolated bounce-back links by level
     std::vector<int> ibb_level_start;   // [levels + 1]
     void* f[2] = {nullptr, nullptr};
@@ -423,6 +425,8 @@ static void free_all(sfg_context* c) {
     c->d_zh_rows = nullptr;
     F(c->d_masks);
     F(c->d_ibb);
+    F(c->d_pillars);
+    c->d_pillars = nullptr;
     F(c->d_chem); F(c->d_released); F(c->d_absorbed); F(c->d_Mp); F(c->d_gamma);
     F(c->d_cov); F(c->d_waves); F(c->d_boxes);
     c->d_chem = nullptr; c->d_released = c->d_absorbed = c->d_Mp = c->d_gamma = nullptr;
@@ -564,8 +568,7 @@ extern "C" int sfg_add_pillar(sfg_context* c, int channel, int kind, double a, d
         return fail(SFG_ERR_ARG, "sfg_add_pillar: bad channel");
     if (kind != SFG_PILLAR_CIRCLE && kind != SFG_PILLAR_RECT)
         return fail(SFG_ERR_ARG, "sfg_add_pillar: unknown pillar kind");
-    if (!c->ch[channel].caps.empty())
-        return fail(SFG_ERR_ARG, "sfg_add_pillar: pillars cannot share a channel with capsules");
+
     if (c->ch[channel].p.scalar_enabled)
         return fail(SFG_ERR_ARG, "sfg_add_pillar: pillars cannot share a channel with the scalar");
     Pillar o;
@@ -589,8 +592,7 @@ extern "C" int sfg_add_capsule(sfg_context* c, int channel, const sfg_membrane_p
         return fail(SFG_ERR_ARG, "sfg_add_capsule: bad channel");
     if (c->ch[channel].p.boundary_type != SFG_PERIODIC)
         return fail(SFG_ERR_ARG, "sfg_add_capsule: capsules need a channel periodic in x");
-    if (!c->ch[channel].pillars.empty())
-        return fail(SFG_ERR_ARG, "sfg_add_capsule: capsules cannot share a channel with pillars");
+
     if (rest->num_nodes < 3) return fail(SFG_ERR_ARG, "sfg_add_capsule: need >= 3 nodes");
     if (mp->use_helfrich && (!rest_ang || !rest_ds))
         return fail(SFG_ERR_ARG, "sfg_add_capsule: Helfrich bending needs rest angles");
@@ -801,6 +803,30 @@ extern "C" int sfg_initialize(sfg_context* c) {
     if (c->maxn > 0) CU(prepare_membrane(c->maxn));
     CU(prepare_spread());
 
+    {   // pillar shapes for the obstacle repulsion of the markers
+        std::vector<double> pl;
+        std::vector<int> pl_off(nch, 0);
+        c->pillar_repulsion = false;
+        for (int i = 0; i < nch; ++i) {
+            pl_off[i] = (int)pl.size();
+            for (const Pillar& o : c->ch[i].pillars) {
+                pl.push_back((double)o.rect);
+                pl.push_back(o.a);
+                pl.push_back(o.b);
+                pl.push_back(o.c);
+                pl.push_back(o.d);
+            }
+            c->ch[i].d.n_pillars = (int)c->ch[i].pillars.size();
+            if (!c->ch[i].pillars.empty() && !c->ch[i].caps.empty()) c->pillar_repulsion = true;
+        }
+        if (!pl.empty()) {
+            CU(dalloc(&c->d_pillars, pl.size()));
+            CU(cudaMemcpy(c->d_pillars, pl.data(), sizeof(double) * pl.size(),
+                          cudaMemcpyHostToDevice));
+            for (int i = 0; i < nch; ++i)
+                if (c->ch[i].d.n_pillars > 0) c->ch[i].d.pillars = c->d_pillars + pl_off[i];
+        }
+    }
     if (!masks.empty()) {
         CU(dalloc(&c->d_masks, masks.size()));
         CU(cudaMemcpy(c->d_masks, masks.data(), masks.size(), cudaMemcpyHostToDevice));
@@ -1126,6 +1152,10 @@ static int enqueue_step_t(sfg_context* c, int p) {
             launch_membrane(c->d_caps, c->NC, c->mb, c->d_has_prev, c->maxn, c->d_status, st);
             CU(cudaStreamWaitEvent(st, c->ev_contact, 0));
             launch_contact_force(c->d_chans, c->M, c->mb, c->cb, st);
+            if (c->pillar_repulsion) {
+                launch_obstacle_repulsion(c->d_chans, c->M, c->mb, st);
+                launches += 1;
+            }
             CU(cudaStreamWaitEvent(st, c->ev_tiles, 0));
             launch_spread<R>(c->d_chans, c->mb, c->tb, p, 0, MDF_PLAIN, 0, c->spread_grid,
                              c->d_status, st);
@@ -1135,6 +1165,10 @@ static int enqueue_step_t(sfg_context* c, int p) {
             launch_membrane(c->d_caps, c->NC, c->mb, c->d_has_prev, c->maxn, c->d_status, st);
             mark(c, SFG_PHASE_MEMBRANE);
             launch_contact(c->d_chans, c->M, c->mb, c->cb, c->ncells, st);
+            if (c->pillar_repulsion) {
+                launch_obstacle_repulsion(c->d_chans, c->M, c->mb, st);
+                launches += 1;
+            }
             mark(c, SFG_PHASE_CONTACT);
             launch_tiles(c->d_chans, c->d_caps, c->M, c->mb, c->tb, c->tb.T, p, c->d_phi,
                          c->d_status, st);

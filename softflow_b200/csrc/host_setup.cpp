@@ -131,12 +131,53 @@ extern "C" int sfg_build_circle_capsule(double cx, double cy, double radius, int
 
 // Simulation::addCapsuleRandom (simulation.cpp:220-274): the same engine and
 // distributions, so the draws (x, y, r per attempt) are the reference's.
+// Obstacle::signedDistance of CircleObstacle / RectObstacle
+// (geometry/circle_obstacle.h:17-21, rect_obstacle.h:18-26); o = kind, a..d.
+static double pillar_sd(const double* o, double x, double y) {
+    if (o[0] == 0.0) {
+        const double dx = x - o[1], dy = y - o[2];
+        return std::sqrt(dx * dx + dy * dy) - o[3];
+    }
+    auto max3 = [](double a, double b, double c) {
+        double m = a;
+        if (m < b) m = b;
+        if (m < c) m = c;
+        return m;
+    };
+    const double dx = max3(o[1] - x, x - o[3], 0.0);
+    const double dy = max3(o[2] - y, y - o[4], 0.0);
+    const double outside = std::sqrt(dx * dx + dy * dy);
+    if (outside > 1e-15) return outside;
+    double m = x - o[1];
+    if (o[3] - x < m) m = o[3] - x;
+    if (y - o[2] < m) m = y - o[2];
+    if (o[4] - y < m) m = o[4] - y;
+    return -m;
+}
+
 extern "C" int sfg_place_random(int count, double x0, double y0, double x1, double y1,
                                 double rmin, double rmax, int num_nodes, int seed, double min_gap,
                                 int max_attempts, int check_walls, int nx, int ny, int n_existing,
                                 const double* existing_centroid, const double* existing_radius,
                                 int capacity, double* out_center, double* out_radius,
                                 int* n_placed, int* n_attempts) {
+    return sfg_place_random_pillars(count, x0, y0, x1, y1, rmin, rmax, num_nodes, seed, min_gap,
+                                    max_attempts, check_walls, nx, ny, n_existing,
+                                    existing_centroid, existing_radius, capacity, out_center,
+                                    out_radius, n_placed, n_attempts, 0, nullptr);
+}
+
+extern "C" int sfg_place_random_pillars(int count, double x0, double y0, double x1, double y1,
+                                        double rmin, double rmax, int num_nodes, int seed,
+                                        double min_gap, int max_attempts, int check_walls, int nx,
+                                        int ny, int n_existing, const double* existing_centroid,
+                                        const double* existing_radius, int capacity,
+                                        double* out_center, double* out_radius, int* n_placed,
+                                        int* n_attempts, int n_pillars, const double* pillars) {
+    if (n_pillars < 0 || (n_pillars > 0 && !pillars)) {
+        sfg_host::set_error("sfg_place_random_pillars: bad pillar list");
+        return SFG_ERR_ARG;
+    }
     if (count < 0 || (n_existing > 0 && (!existing_centroid || !existing_radius))) {
         sfg_host::set_error("sfg_place_random: bad arguments");
         return SFG_ERR_ARG;
@@ -166,6 +207,12 @@ extern "C" int sfg_place_random(int count, double x0, double y0, double x1, doub
         if (check_walls) {
             if (cy - r < 0.0 + min_gap || cy + r > static_cast<double>(ny - 1) - min_gap)
                 overlap = true;
+            // obstacles of the channel builder (simulation.cpp:256-261)
+            for (int k = 0; k < n_pillars; ++k)
+                if (pillar_sd(pillars + 5 * k, cx, cy) < r + min_gap) {
+                    overlap = true;
+                    break;
+                }
         }
         if (!overlap) {
             if (placed >= capacity) {

@@ -9,12 +9,12 @@
 namespace sfg {
 
 // Lattice velocity at a cell for interpolation: moments of the populations
-// plus half the given force, zero on SOLID wall rows (lattice_field.cpp:28-73).
+// plus half the given force, zero on SOLID cells (lattice_field.cpp:28-73).
 template <typename S, typename R>
 __device__ __forceinline__ void cell_rho_j(const ChannelDev& ch, const S* __restrict__ f, int jx,
                                            int jy, double& rho, double& jxo, double& jyo,
                                            bool& solid) {
-    solid = !ch.periodic_y && (jy == 0 || jy == ch.ny - 1);
+    solid = cell_kind(ch, jx, jy) == CK_SOLID;
     if (solid) { rho = 0.0; jxo = 0.0; jyo = 0.0; return; }
     const long long n = (long long)jy * ch.pitch + jx;
     R v[9];

@@ -802,7 +802,7 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
             const int jx = x0 + (c % TILE_W), jy = y0 + (c / TILE_W);
             double vx = ax[c], vy = ay[c];
             if (jx < nx && jy < ny) {
-                const bool fluid = ch.periodic_y || (jy != 0 && jy != ny - 1);
+                const bool fluid = cell_kind(ch, jx, jy) == CK_FLUID;
                 if (fluid && body) {
                     vx += ch.body_fx;
                     vy += ch.body_fy;
@@ -1132,6 +1132,119 @@ void launch_membrane(const CapsuleDev* caps, int ncaps, const MarkerBufs& mb, in
     const size_t smem = membrane_smem_bytes(maxn);
     const int blocks = (ncaps + MEM_WARPS - 1) / MEM_WARPS;
     k_membrane<<<blocks, MEM_WARPS * 32, smem, st>>>(caps, ncaps, mb, has_prev, maxn, status);
+}
+
+// ---------------- obstacle repulsion (pillars) -------------------------------
+// Obstacle::signedDistance / normalAt of CircleObstacle and RectObstacle
+// (geometry/circle_obstacle.h:17-37, rect_obstacle.h:18-59) with the
+// first-extremum semantics of std::min / std::max over initializer lists.
+__device__ __forceinline__ double max3(double a, double b, double c) {
+    double m = a;
+    if (m < b) m = b;
+    if (m < c) m = c;
+    return m;
+}
+__device__ __forceinline__ double min4(double a, double b, double c, double d) {
+    double m = a;
+    if (b < m) m = b;
+    if (c < m) m = c;
+    if (d < m) m = d;
+    return m;
+}
+
+__device__ void pillar_geometry(const double* o, double x, double y, double& sd, double2& nrm) {
+    if (o[0] == 0.0) {   // circle (a, b) radius c
+        const double dx = x - o[1], dy = y - o[2];
+        const double d = sqrt(dx * dx + dy * dy);
+        sd = d - o[3];
+        nrm = (d < 1e-15) ? make_double2(1.0, 0.0) : make_double2(dx / d, dy / d);
+        return;
+    }
+    const double x0 = o[1], y0 = o[2], x1 = o[3], y1 = o[4];
+    {
+        const double dx = max3(x0 - x, x - x1, 0.0);
+        const double dy = max3(y0 - y, y - y1, 0.0);
+        const double outside = sqrt(dx * dx + dy * dy);
+        sd = (outside > 1e-15) ? outside : -min4(x - x0, x1 - x, y - y0, y1 - y);
+    }
+    // nearestPoint
+    const double cx = (x < x0) ? x0 : ((x1 < x) ? x1 : x);
+    const double cy = (y < y0) ? y0 : ((y1 < y) ? y1 : y);
+    double2 np;
+    if (cx == x && cy == y) {
+        const double dl = x - x0, dr = x1 - x, db = y - y0, dt = y1 - y;
+        const double dmin = min4(dl, dr, db, dt);
+        if (dmin == dl) np = make_double2(x0, y);
+        else if (dmin == dr) np = make_double2(x1, y);
+        else if (dmin == db) np = make_double2(x, y0);
+        else np = make_double2(x, y1);
+    } else {
+        np = make_double2(cx, cy);
+    }
+    const double ddx = x - np.x, ddy = y - np.y;
+    const double d = sqrt(ddx * ddx + ddy * ddy);
+    if (d < 1e-15) {
+        const double dl = fabs(x - x0), dr = fabs(x - x1), db = fabs(y - y0), dt = fabs(y - y1);
+        const double dmin = min4(dl, dr, db, dt);
+        if (dmin == dl) nrm = make_double2(-1.0, 0.0);
+        else if (dmin == dr) nrm = make_double2(1.0, 0.0);
+        else if (dmin == db) nrm = make_double2(0.0, -1.0);
+        else nrm = make_double2(0.0, 1.0);
+    } else {
+        nrm = make_double2(ddx / d, ddy / d);
+    }
+}
+
+// RepulsionForce::computeObstacleRepulsion (repulsion.cpp:180-235) for every
+// pillar of the marker's channel in order, after the pair contact.
+__global__ void k_obstacle_repulsion(const ChannelDev* __restrict__ chans, int M, MarkerBufs mb) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    const ChannelDev& ch = chans[mb.mk_chan[m]];
+    if (ch.n_pillars == 0) return;
+    const double2 p = mb.pos[m], v = mb.vel[m];
+    double2 f = mb.frc[m];
+    const double r_cut = ch.rep_r_cut, eps = ch.rep_epsilon, sigma = ch.rep_sigma;
+    const double gamma_n = ch.rep_damping, mu = ch.rep_friction;
+    for (int k = 0; k < ch.n_pillars; ++k) {
+        double sd;
+        double2 nrm;
+        pillar_geometry(ch.pillars + 5 * k, p.x, p.y, sd, nrm);
+        if (sd >= r_cut) continue;
+        double r = fabs(sd);
+        if (r < 1e-15) r = 1e-15;
+        const double F_rep = eps * pow(sigma / r, (double)ch.rep_power);
+        if (sd < 0.0) {
+            const double s = F_rep * 10.0;
+            f.x += nrm.x * s;
+            f.y += nrm.y * s;
+            continue;
+        }
+        double F_n = F_rep;
+        double2 F_t = make_double2(0.0, 0.0);
+        if (gamma_n > 0.0 || mu > 0.0) {
+            const double v_n = v.x * nrm.x + v.y * nrm.y;
+            F_n = F_rep - gamma_n * v_n;
+            if (F_n < 0.0) F_n = 0.0;
+            if (mu > 0.0) {
+                const double2 v_t = make_double2(v.x - nrm.x * v_n, v.y - nrm.y * v_n);
+                const double v_t_mag = sqrt(v_t.x * v_t.x + v_t.y * v_t.y);
+                if (v_t_mag > 1e-12) {
+                    const double s = -mu * F_n;
+                    F_t = make_double2((v_t.x / v_t_mag) * s, (v_t.y / v_t_mag) * s);
+                }
+            }
+        }
+        f.x += nrm.x * F_n + F_t.x;
+        f.y += nrm.y * F_n + F_t.y;
+    }
+    mb.frc[m] = f;
+}
+
+void launch_obstacle_repulsion(const ChannelDev* chans, int M, const MarkerBufs& mb,
+                               cudaStream_t st) {
+    if (M == 0) return;
+    k_obstacle_repulsion<<<(M + 255) / 256, 256, 0, st>>>(chans, M, mb);
 }
 
 void launch_contact(const ChannelDev* chans, int M, const MarkerBufs& mb, ContactBufs& cb,

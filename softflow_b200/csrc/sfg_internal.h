@@ -75,6 +75,9 @@ void launch_contact_prep(const ChannelDev* chans, int M, const MarkerBufs& mb, C
                          int ncells, cudaStream_t st);
 void launch_contact_force(const ChannelDev* chans, int M, const MarkerBufs& mb, ContactBufs& cb,
                           cudaStream_t st);
+// Repulsion of markers from the pillars of their channel (after the pairs).
+void launch_obstacle_repulsion(const ChannelDev* chans, int M, const MarkerBufs& mb,
+                               cudaStream_t st);
 void launch_tiles(const ChannelDev* chans, const CapsuleDev* caps, int M, const MarkerBufs& mb,
                   TileBufs& tb, int T, int parity, const double* phi_tbl, unsigned* status,
                   cudaStream_t st);

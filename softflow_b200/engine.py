@@ -357,11 +357,13 @@ class _Channel:
         out_c = np.zeros(2 * max(count, 1))
         out_r = np.zeros(max(count, 1))
         placed, attempts = C.c_int(0), C.c_int(0)
-        L.check(L.lib().sfg_place_random(
+        pl = np.array([x for o in self.pillars for x in o], dtype=np.float64)
+        L.check(L.lib().sfg_place_random_pillars(
             int(count), float(x0), float(y0), float(x1), float(y1), float(rmin), float(rmax),
             int(num_nodes), int(seed), float(min_gap), int(max_attempts), int(bool(check_walls)),
             int(self.params.nx), int(self.params.ny), n_ex, L.dptr(cen), L.dptr(rad),
-            int(count), L.dptr(out_c), L.dptr(out_r), C.byref(placed), C.byref(attempts)))
+            int(count), L.dptr(out_c), L.dptr(out_r), C.byref(placed), C.byref(attempts),
+            len(self.pillars), L.dptr(pl) if len(self.pillars) else None))
         for i in range(placed.value):
             self.add_capsule((out_c[2 * i], out_c[2 * i + 1]), out_r[i], num_nodes, mparams,
                              type_id)
@@ -814,6 +816,9 @@ class Ensemble:
         links when fluid.use_interpolated_bb)."""
         self._pre_init()
         self._chans[chan].pillars = list(builder.pillars)
+        # with a channel builder the random placement tests the walls and
+        # the obstacles (simulation.cpp:250-262)
+        self._chans[chan].walls_in_placement = True
 
     def _pre_init(self):
         if self._ctx is not None:

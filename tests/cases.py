@@ -108,6 +108,35 @@ CASES = {
                                     use_interpolated_bb=1),
                           capsules=[], conc=None,
                           pillars=[("circle", 24.0, 13.3, 4.7), ("circle", 45.5, 9.0, 3.1)]),
+    # capsules among pillars: one capsule inside the contact range of a
+    # cylinder, one above a rectangle, three more placed at random with the
+    # pillars rejected (simulation.cpp:256-261); obstacle repulsion with
+    # normal damping and Coulomb friction (repulsion.cpp:180-235)
+    "pillars_capsules": dict(spec=dict(nx=80, ny=30, collision=O.BGK, tau=0.8, body_fx=2e-5,
+                                       rep_damping_normal=0.1, rep_friction=0.2),
+                             pillars=[("circle", 40.0, 15.0, 5.0), ("rect", 55.0, 3.0, 62.0, 11.0)],
+                             capsules=[("add", 30.5, 15.2, 4.0, 24, SKALAK_C1),
+                                       ("add", 58.5, 16.0, 4.0, 24, SKALAK_C1),
+                                       ("random", 3, 0, 5, 80, 25, 3.0, 3.0, 24, SKALAK_C1, 7,
+                                        1.0, True)],
+                             conc=None),
+    # the same with interpolated bounce-back, regularized collision and
+    # three direct-forcing sweeps
+    "pillars_capsules_mdf": dict(spec=dict(nx=80, ny=30, collision=O.REGULARIZED, tau=0.8,
+                                           body_fx=2e-5, use_interpolated_bb=1,
+                                           ibm_iterations=3),
+                                 pillars=[("circle", 40.0, 15.0, 5.0),
+                                          ("rect", 55.0, 3.0, 62.0, 11.0)],
+                                 capsules=[("add", 30.5, 15.2, 4.0, 24, SKALAK_C1),
+                                           ("add", 58.5, 16.0, 4.0, 24, SKALAK_C1)],
+                                 conc=None),
+    # capsules that reach into both pillars at the start: the nodes inside
+    # get the push-out branch of the obstacle repulsion
+    "pillars_overlap": dict(spec=dict(nx=80, ny=30, collision=O.BGK, tau=0.8, body_fx=2e-5),
+                            pillars=[("circle", 40.0, 15.0, 5.0), ("rect", 55.0, 3.0, 62.0, 11.0)],
+                            capsules=[("add", 40.0, 22.5, 3.0, 20, SKALAK_C1),
+                                      ("add", 58.5, 13.5, 3.0, 20, SKALAK_C1)],
+                            conc=None),
     # plane Couette flow with a capsule (periodic x, walls moving apart)
     "shear_capsule": dict(spec=dict(nx=64, ny=34, collision=O.BGK, tau=0.8,
                                     top_wall_velocity=0.01, bottom_wall_velocity=-0.01,

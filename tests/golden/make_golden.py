@@ -6,7 +6,8 @@ build, one OpenMP thread).  Writes tests/golden/*.npz.  The fixtures are
 outputs of the reference itself on seeded inputs; the tests compare the CPU
 restatement (oracle/sfo.c) and the GPU path against them.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # every fixture
+    python tests/golden/make_golden.py NAME ...   # the named cases only
 """
 import os
 import sys
@@ -28,12 +29,14 @@ RUNS = [("bgk_small", 300), ("mrt_small", 300), ("reg_small", 300), ("mini_c2", 
         ("contact_brute", 60), ("seam_single", 40), ("c1", 10),
         ("zouhe_bgk", 300), ("zouhe_reg", 300), ("cavity", 400), ("shear_capsule", 60),
         ("pillars_ibb", 300), ("pillars_zouhe", 300), ("chem_source", 60),
-        ("chem_physics", 60)]
+        ("chem_physics", 60), ("pillars_capsules", 200), ("pillars_capsules_mdf", 200)]
 
 
-def main():
+def main(only=None):
     oracle.build(ref=True)
     for name, steps in RUNS:
+        if only and name not in only:
+            continue
         case = CASES[name]
         o = build_oracle(case, impl="ref")
         o.step(steps)
@@ -90,5 +93,6 @@ def outputs():
 
 
 if __name__ == "__main__":
-    main()
-    outputs()
+    main(sys.argv[1:])
+    if len(sys.argv) == 1:
+        outputs()

@@ -128,12 +128,6 @@ def test_boundary_channel_restrictions(sfg):
     q.scalar.enabled = True
     with pytest.raises(S.SoftFlowGpuError, match="scalar"):
         S.Simulation(q).initialize()
-    r = gpu_params(CASES["pillars_bb"], "fp32")
-    sim = S.Simulation(r)
-    sim.setChannelBuilder(S.ChannelBuilder(r.nx, r.ny).addCirclePillar(20.0, 15.0, 4.0))
-    sim.addCapsule((50.0, 15.0), 3.0, 24)
-    with pytest.raises(S.SoftFlowGpuError, match="pillars"):
-        sim.initialize()
 
 
 def test_body_force_on_fluid_cells_only(sfg, oracle_mod):

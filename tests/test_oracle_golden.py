@@ -13,7 +13,7 @@ from cases import CASES, build_oracle, fluid_rows
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 NAMES = ["bgk_small", "mrt_small", "reg_small", "mini_c2", "contact_brute", "seam_single", "c1",
          "zouhe_bgk", "zouhe_reg", "cavity", "shear_capsule", "pillars_ibb", "pillars_zouhe",
-         "chem_source", "chem_physics"]
+         "chem_source", "chem_physics", "pillars_capsules", "pillars_capsules_mdf"]
 
 
 @pytest.mark.parametrize("name", NAMES)
@@ -135,6 +135,22 @@ def test_oracle_pillars_match_live_reference(oracle_mod, name, steps):
     a.step(steps)
     b.step(steps)
     for k in ("f", "ux", "uy", "rho"):
+        assert np.array_equal(getattr(a, k)(), getattr(b, k)()), k
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference build absent")
+@pytest.mark.parametrize("name,steps", [("pillars_capsules", 200),
+                                        ("pillars_capsules_mdf", 200)])
+def test_oracle_capsules_among_pillars_match_live_reference(oracle_mod, name, steps):
+    """Capsules among pillars: placement that rejects the pillars
+    (simulation.cpp:256-261) and the obstacle repulsion
+    (repulsion.cpp:180-235, after the pair contact), bit for bit."""
+    case = CASES[name]
+    a = build_oracle(case, "sfo")
+    b = build_oracle(case, "ref")
+    a.step(steps)
+    b.step(steps)
+    for k in ("f", "ux", "uy", "rho", "positions", "velocities", "forces"):
         assert np.array_equal(getattr(a, k)(), getattr(b, k)()), k
 
 
