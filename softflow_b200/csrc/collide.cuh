@@ -9,6 +9,75 @@
 
 namespace sfg {
 
+// ---------------------------------------------------------------------------
+// FP32 arithmetic of the lattice kernels, written once for a single cell
+// (V = float) and for two cells packed in one register pair (V = F2: the
+// sm_100 paired FP32 instructions FADD2 / FMUL2 / FFMA2, which round each
+// half exactly like the scalar instruction).  Every operation is explicit
+// (no contraction left to the compiler), so the one-cell and the paired
+// kernels give bit-identical results.
+// ---------------------------------------------------------------------------
+struct F2 {
+    float2 v;
+};
+__device__ __forceinline__ F2 mk2(float a, float b) {
+    F2 r;
+    r.v = make_float2(a, b);
+    return r;
+}
+template <typename V>
+__device__ __forceinline__ V vc(float a);
+template <>
+__device__ __forceinline__ float vc<float>(float a) { return a; }
+template <>
+__device__ __forceinline__ F2 vc<F2>(float a) { return mk2(a, a); }
+
+__device__ __forceinline__ float vadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float vsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float vmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float vfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ F2 vadd(F2 a, F2 b) {
+    F2 r;
+    r.v = __fadd2_rn(a.v, b.v);
+    return r;
+}
+__device__ __forceinline__ F2 vmul(F2 a, F2 b) {
+    F2 r;
+    r.v = __fmul2_rn(a.v, b.v);
+    return r;
+}
+__device__ __forceinline__ F2 vfma(F2 a, F2 b, F2 c) {
+    F2 r;
+    r.v = __ffma2_rn(a.v, b.v, c.v);
+    return r;
+}
+// a - b = fma(b, -1, a), rounded once like the scalar subtraction
+__device__ __forceinline__ F2 vsub(F2 a, F2 b) { return vfma(b, vc<F2>(-1.f), a); }
+
+// Moments of the deviations d = f - w: rho - 1, j and the second-moment sums
+// sxx = sum d cx^2, syy = sum d cy^2, sxy = sum d cx cy, through the
+// opposite-direction sums and differences.
+template <typename V>
+struct DevMoments {
+    V drho, jx, jy, sxx, syy, sxy;
+};
+template <typename V>
+__device__ __forceinline__ DevMoments<V> dev_moments(const V d[9]) {
+    const V a13 = vadd(d[1], d[3]), m13 = vsub(d[1], d[3]);
+    const V a24 = vadd(d[2], d[4]), m24 = vsub(d[2], d[4]);
+    const V a57 = vadd(d[5], d[7]), m57 = vsub(d[5], d[7]);
+    const V a68 = vadd(d[6], d[8]), m68 = vsub(d[6], d[8]);
+    const V sd = vadd(a57, a68);
+    DevMoments<V> m;
+    m.drho = vadd(vadd(d[0], a13), vadd(a24, sd));
+    m.jx = vsub(vadd(m13, m57), m68);
+    m.jy = vadd(vadd(m24, m57), m68);
+    m.sxx = vadd(a13, sd);
+    m.syy = vadd(a24, sd);
+    m.sxy = vsub(a57, a68);
+    return m;
+}
+
 // Moments of one cell in the reference's summation order
 // (lattice_field.cpp:220-227): rho = sum f_q, j = sum f_q e_q, q = 0..8.
 template <typename R>
@@ -27,8 +96,10 @@ __device__ __forceinline__ void lattice_moments(const R c[9], R& rho, R& jx, R& 
 template <>
 __device__ __forceinline__ void lattice_moments<float>(const float c[9], float& rho, float& jx,
                                                        float& jy) {
-    cell_moments(c, rho, jx, jy);
-    rho += 1.f;
+    const DevMoments<float> m = dev_moments(c);
+    rho = vadd(m.drho, 1.f);
+    jx = m.jx;
+    jy = m.jy;
 }
 
 // u = (j + F/2) / rho, zero for rho <= 1e-15 (lattice_field.cpp:229-237).
@@ -43,12 +114,27 @@ __device__ __forceinline__ void cell_velocity(R rho, R jx, R jy, R Gx, R Gy, R& 
     }
 }
 // FP32 form: one correctly rounded reciprocal and two products.
+// FP32 reciprocal of the density: the hardware approximation (relative
+// error below 2^-22, no special-case path; rho stays near 1).
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 template <>
 __device__ __forceinline__ void cell_velocity<float>(float rho, float jx, float jy, float Gx,
                                                      float Gy, float& ux, float& uy) {
-    const float inv = rho > 1e-15f ? __frcp_rn(rho) : 0.0f;
-    ux = (jx + 0.5f * Gx) * inv;
-    uy = (jy + 0.5f * Gy) * inv;
+    const float inv = rho > 1e-15f ? rcp_approx(rho) : 0.0f;
+    ux = vmul(vfma(0.5f, Gx, jx), inv);
+    uy = vmul(vfma(0.5f, Gy, jy), inv);
+}
+// Two cells: the reciprocal per half, the rest paired.
+__device__ __forceinline__ void cell_velocity2(F2 rho, F2 jx, F2 jy, F2 Gx, F2 Gy, F2& ux,
+                                               F2& uy) {
+    const F2 inv = mk2(rho.v.x > 1e-15f ? rcp_approx(rho.v.x) : 0.0f,
+                       rho.v.y > 1e-15f ? rcp_approx(rho.v.y) : 0.0f);
+    ux = vmul(vfma(vc<F2>(0.5f), Gx, jx), inv);
+    uy = vmul(vfma(vc<F2>(0.5f), Gy, jy), inv);
 }
 
 template <typename R>
@@ -168,123 +254,210 @@ __device__ __forceinline__ void collide_mrt(R f[9], R r, R vx, R vy, R fx, R fy,
 // FP32 forms.  The FP32 path is checked against the FP64 oracle with a
 // tolerance, so it uses algebraically equal, division-free expressions
 // (1/cs^2 = 3, 1/(2 cs^4) = 4.5, reciprocals of the inverse-transform
-// denominators) instead of the reference's evaluation order.
+// denominators) instead of the reference's evaluation order.  They work on
+// the deviations d = f - w (the lattice kernels' representation for FP32
+// and FP16 storage), so no value near a weight is ever formed or rounded,
+// and are written for V = float (one cell) and V = F2 (two cells).
 // ---------------------------------------------------------------------------
-// FP32-arithmetic forms work on the deviations d = f - w (the lattice
-// kernels' representation for FP32 and FP16 storage): the collision reads d
-// and writes d, so no value near a weight is ever formed or rounded.
 
-// MRT on deviations: M w = (1, -2, 1, 0, ..., 0), so the conserved moment is
-// rho - 1 and the two energy equilibria shift by the rest state:
-// e_eq + 2 = -2 (rho - 1) + 3 rho u^2, eps_eq - 1 = (rho - 1) - 3 rho u^2.
-template <>
-__device__ __forceinline__ void collide_mrt<float>(float f[9], float r, float vx, float vy,
-                                                   float fx, float fy, float sn, float s1,
-                                                   float s2, float s4) {
-    const float m0 = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];  // rho - 1
-    const float a = f[1] + f[2] + f[3] + f[4];
-    const float d = f[5] + f[6] + f[7] + f[8];
-    float m1 = -4.f * f[0] - a + 2.f * d;
-    float m2 = 4.f * f[0] - 2.f * a + d;
-    const float m3 = f[1] - f[3] + f[5] - f[6] - f[7] + f[8] + fx;   // + Sb3
-    float m4 = -2.f * (f[1] - f[3]) + f[5] - f[6] - f[7] + f[8];
-    const float m5 = f[2] - f[4] + f[5] + f[6] - f[7] - f[8] + fy;   // + Sb5
-    float m6 = -2.f * (f[2] - f[4]) + f[5] + f[6] - f[7] - f[8];
-    float m7 = f[1] - f[2] + f[3] - f[4];
-    float m8 = f[5] - f[6] + f[7] - f[8];
-    const float uu = vx * vx + vy * vy;
-    const float uF = vx * fx + vy * fy;
-    const float ru3 = 3.f * r * uu;
-    m1 = m1 - s1 * (m1 - (-2.f * m0 + ru3)) + (1.f - 0.5f * s1) * (6.f * uF);
-    m2 = m2 - s2 * (m2 - (m0 - ru3)) - (1.f - 0.5f * s2) * (6.f * uF);
-    m4 = m4 - s4 * (m4 + r * vx) - (1.f - 0.5f * s4) * fx;
-    m6 = m6 - s4 * (m6 + r * vy) - (1.f - 0.5f * s4) * fy;
-    m7 = m7 - sn * (m7 - r * (vx * vx - vy * vy)) + (1.f - 0.5f * sn) * (2.f * (vx * fx - vy * fy));
-    m8 = m8 - sn * (m8 - r * vx * vy) + (1.f - 0.5f * sn) * (vx * fy + vy * fx);
-    const float c9 = 1.f / 9.f, c18 = 1.f / 18.f, c36 = 1.f / 36.f, c6 = 1.f / 6.f,
-                c12 = 1.f / 12.f;
-    const float b0 = c9 * m0;
-    const float bA = b0 - c36 * m1 - c18 * m2;   // axis directions
-    const float bD = b0 + c18 * m1 + c36 * m2;   // diagonals
-    f[0] = c9 * (m0 - m1 + m2);
-    f[1] = bA + c6 * (m3 - m4) + 0.25f * m7;
-    f[2] = bA + c6 * (m5 - m6) - 0.25f * m7;
-    f[3] = bA - c6 * (m3 - m4) + 0.25f * m7;
-    f[4] = bA - c6 * (m5 - m6) - 0.25f * m7;
-    const float px = c6 * m3 + c12 * m4, py = c6 * m5 + c12 * m6;
-    f[5] = bD + px + py + 0.25f * m8;
-    f[6] = bD - px + py - 0.25f * m8;
-    f[7] = bD - px - py + 0.25f * m8;
-    f[8] = bD + px - py - 0.25f * m8;
+// Per-channel constants, computed in scalar FP32 with explicit rounding so
+// both forms see the same values.
+template <typename V>
+struct RegConst {
+    V ane, aj, g3, g9, nguo, nane;
+};
+template <typename V>
+__device__ __forceinline__ RegConst<V> reg_const(float omega) {
+    const float om1 = __fsub_rn(1.f, omega), guo = __fmaf_rn(-0.5f, omega, 1.f);
+    const float ane = __fmul_rn(4.5f, om1);
+    RegConst<V> c;
+    c.ane = vc<V>(ane);
+    c.nane = vc<V>(-ane);
+    c.aj = vc<V>(__fmul_rn(3.f, om1));
+    c.g3 = vc<V>(__fmul_rn(3.f, guo));
+    c.g9 = vc<V>(__fmul_rn(9.f, guo));
+    c.nguo = vc<V>(-guo);
+    return c;
+}
+
+template <typename V>
+struct BgkConst {
+    V om, om1, g3, g9, nguo;
+};
+template <typename V>
+__device__ __forceinline__ BgkConst<V> bgk_const(float omega) {
+    const float guo = __fmaf_rn(-0.5f, omega, 1.f);
+    BgkConst<V> c;
+    c.om = vc<V>(omega);
+    c.om1 = vc<V>(__fsub_rn(1.f, omega));
+    c.g3 = vc<V>(__fmul_rn(3.f, guo));
+    c.g9 = vc<V>(__fmul_rn(9.f, guo));
+    c.nguo = vc<V>(-guo);
+    return c;
+}
+
+// MRT rates: sn (stress), s1 (energy), s2 (energy square), s4 (heat flux);
+// h = 1 - s/2 the Guo factors.
+template <typename V>
+struct MrtConst {
+    V ns1, h1, ns2, nh2, ns4, nh4, nsn, hn, hn2;
+};
+template <typename V>
+__device__ __forceinline__ MrtConst<V> mrt_const(float sn, float s1, float s2, float s4) {
+    const float h1 = __fmaf_rn(-0.5f, s1, 1.f), h2 = __fmaf_rn(-0.5f, s2, 1.f);
+    const float h4 = __fmaf_rn(-0.5f, s4, 1.f), hn = __fmaf_rn(-0.5f, sn, 1.f);
+    MrtConst<V> c;
+    c.ns1 = vc<V>(-s1);
+    c.h1 = vc<V>(h1);
+    c.ns2 = vc<V>(-s2);
+    c.nh2 = vc<V>(-h2);
+    c.ns4 = vc<V>(-s4);
+    c.nh4 = vc<V>(-h4);
+    c.nsn = vc<V>(-sn);
+    c.hn = vc<V>(hn);
+    c.hn2 = vc<V>(__fmul_rn(2.f, hn));
+    return c;
 }
 
 // Regularized BGK on deviations, by opposite direction pairs.  The
 // non-equilibrium first moment and stress come from the moments minus their
-// values for the
-// second-order equilibrium (sum e feq = rho u, sum e e feq = rho/3 I +
-// rho u u), and every pair (e, -e) shares the even part of the update
-// (equilibrium, stress projection, second-order Guo term) while the odd part
-// (3 e.u, 3 e.j_neq, 3 e.F) changes sign.
-template <>
-__device__ __forceinline__ void collide_regularized<float>(float f[9], float rho, float ux,
-                                                           float uy, float Fx, float Fy,
-                                                           float omega) {
-    // f holds deviations d = f - w: sum_{cx!=0} w = 1/3 and the odd weight
-    // moments vanish
-    const float* d = f;
-    const float drho = d[0] + d[1] + d[2] + d[3] + d[4] + d[5] + d[6] + d[7] + d[8];
-    const float jx = d[1] - d[3] + d[5] - d[6] - d[7] + d[8];
-    const float jy = d[2] - d[4] + d[5] + d[6] - d[7] - d[8];
-    const float sxx = d[1] + d[3] + d[5] + d[6] + d[7] + d[8];
-    const float syy = d[2] + d[4] + d[5] + d[6] + d[7] + d[8];
-    const float sxy = d[5] - d[6] + d[7] - d[8];
-    const float rux = rho * ux, ruy = rho * uy;
-    const float jnx = jx - rux, jny = jy - ruy;
-    const float dr3 = drho * (1.f / 3.f);
-    const float pxx = sxx - dr3 - rux * ux;
-    const float pyy = syy - dr3 - ruy * uy;
-    const float pxy = sxy - rux * uy;
-    const float om1 = 1.f - omega, guo = 1.f - 0.5f * omega;
-    const float bm = -1.5f * (ux * ux + uy * uy);
-    const float uF3 = 3.f * (ux * Fx + uy * Fy);
-    const float trP3 = (pxx + pyy) * (1.f / 3.f);
-    const float ane = 4.5f * om1, aj = 3.f * om1, g3 = 3.f * guo, g9 = 9.f * guo;
-    f[0] = (4.f / 9.f) * (drho + rho * bm - ane * trP3 - guo * uF3);
-    auto pair = [&](int q, int o, float eu, float eF, float ej, float QP, float w) {
-        const float E = w * (drho + rho * (bm + 4.5f * eu * eu) + ane * QP + g9 * eu * eF -
-                             guo * uF3);
-        const float O = w * (3.f * rho * eu + aj * ej + g3 * eF);
-        f[q] = E + O;
-        f[o] = E - O;
+// values for the second-order equilibrium (sum e feq = rho u,
+// sum e e feq = rho/3 I + rho u u), and every pair (e, -e) shares the even
+// part of the update (equilibrium, stress projection, second-order Guo term)
+// while the odd part (3 e.u, 3 e.j_neq, 3 e.F) changes sign.  Sums over d
+// use sum_{cx != 0} w = 1/3 and the vanishing odd weight moments.
+template <typename V>
+__device__ __forceinline__ void reg_collide_v(V d[9], const DevMoments<V>& m, V rho, V ux, V uy,
+                                              V Fx, V Fy, const RegConst<V>& c) {
+    const V rux = vmul(rho, ux), ruy = vmul(rho, uy);
+    const V jnx = vsub(m.jx, rux), jny = vsub(m.jy, ruy);
+    const V dr3 = vmul(m.drho, vc<V>(1.f / 3.f));
+    const V pxx = vsub(m.sxx, vfma(rux, ux, dr3));
+    const V pyy = vsub(m.syy, vfma(ruy, uy, dr3));
+    const V pxy = vsub(m.sxy, vmul(rux, uy));
+    const V bm = vmul(vfma(ux, ux, vmul(uy, uy)), vc<V>(-1.5f));
+    const V uF3 = vmul(vfma(ux, Fx, vmul(uy, Fy)), vc<V>(3.f));
+    const V sP = vadd(pxx, pyy);
+    const V trP3 = vmul(sP, vc<V>(1.f / 3.f));
+    const V C0 = vfma(c.nguo, uF3, vfma(rho, bm, m.drho));
+    d[0] = vmul(vc<V>(4.f / 9.f), vfma(c.nane, trP3, C0));
+    const V r45 = vmul(rho, vc<V>(4.5f)), r3 = vmul(rho, vc<V>(3.f));
+    auto pair = [&](int q, int o, V eu, V eF, V ej, V QP, float w) {
+        const V E = vmul(vc<V>(w), vfma(c.ane, QP, vfma(eu, vfma(r45, eu, vmul(c.g9, eF)), C0)));
+        const V O = vmul(vc<V>(w), vfma(r3, eu, vfma(c.aj, ej, vmul(c.g3, eF))));
+        d[q] = vadd(E, O);
+        d[o] = vsub(E, O);
     };
-    pair(1, 3, ux, Fx, jnx, pxx - trP3, 1.f / 9.f);
-    pair(2, 4, uy, Fy, jny, pyy - trP3, 1.f / 9.f);
-    pair(5, 7, ux + uy, Fx + Fy, jnx + jny, pxx + pyy + 2.f * pxy - trP3, 1.f / 36.f);
-    pair(6, 8, uy - ux, Fy - Fx, jny - jnx, pxx + pyy - 2.f * pxy - trP3, 1.f / 36.f);
+    pair(1, 3, ux, Fx, jnx, vsub(pxx, trP3), 1.f / 9.f);
+    pair(2, 4, uy, Fy, jny, vsub(pyy, trP3), 1.f / 9.f);
+    pair(5, 7, vadd(ux, uy), vadd(Fx, Fy), vadd(jnx, jny),
+         vsub(vfma(vc<V>(2.f), pxy, sP), trP3), 1.f / 36.f);
+    pair(6, 8, vsub(uy, ux), vsub(Fy, Fx), vsub(jny, jnx),
+         vsub(vfma(vc<V>(-2.f), pxy, sP), trP3), 1.f / 36.f);
 }
 
 // BGK on deviations, by opposite direction pairs:
 // d' = (1 - omega) d + omega (feq - w) + F with
 // feq - w = w ((rho - 1) + rho (-1.5 u^2 + 4.5 (e.u)^2) + 3 rho e.u).
+template <typename V>
+__device__ __forceinline__ void bgk_collide_v(V d[9], V drho, V rho, V ux, V uy, V Fx, V Fy,
+                                              const BgkConst<V>& c) {
+    const V bm = vmul(vfma(ux, ux, vmul(uy, uy)), vc<V>(-1.5f));
+    const V uF3 = vmul(vfma(ux, Fx, vmul(uy, Fy)), vc<V>(3.f));
+    const V orr = vmul(c.om, rho);
+    const V C0 = vfma(c.nguo, uF3, vfma(orr, bm, vmul(c.om, drho)));
+    d[0] = vfma(c.om1, d[0], vmul(vc<V>(4.f / 9.f), C0));
+    const V o45 = vmul(orr, vc<V>(4.5f)), o3 = vmul(orr, vc<V>(3.f));
+    auto pair = [&](int q, int o, V eu, V eF, float w) {
+        const V E = vmul(vc<V>(w), vfma(eu, vfma(o45, eu, vmul(c.g9, eF)), C0));
+        const V O = vmul(vc<V>(w), vfma(o3, eu, vmul(c.g3, eF)));
+        d[q] = vfma(c.om1, d[q], vadd(E, O));
+        d[o] = vfma(c.om1, d[o], vsub(E, O));
+    };
+    pair(1, 3, ux, Fx, 1.f / 9.f);
+    pair(2, 4, uy, Fy, 1.f / 9.f);
+    pair(5, 7, vadd(ux, uy), vadd(Fx, Fy), 1.f / 36.f);
+    pair(6, 8, vsub(uy, ux), vsub(Fy, Fx), 1.f / 36.f);
+}
+
+// MRT on deviations: M w = (1, -2, 1, 0, ..., 0), so the conserved moment is
+// rho - 1 and the two energy equilibria shift by the rest state:
+// e_eq + 2 = -2 (rho - 1) + 3 rho u^2, eps_eq - 1 = (rho - 1) - 3 rho u^2.
+template <typename V>
+__device__ __forceinline__ void mrt_collide_v(V d[9], V rho, V vx, V vy, V fx, V fy,
+                                              const MrtConst<V>& c) {
+    const V a13 = vadd(d[1], d[3]), m13 = vsub(d[1], d[3]);
+    const V a24 = vadd(d[2], d[4]), m24 = vsub(d[2], d[4]);
+    const V a57 = vadd(d[5], d[7]), m57 = vsub(d[5], d[7]);
+    const V a68 = vadd(d[6], d[8]), m68 = vsub(d[6], d[8]);
+    const V sd = vadd(a57, a68), sa = vadd(a13, a24);
+    const V m0 = vadd(vadd(d[0], a13), vadd(a24, sd));          // rho - 1
+    const V jx = vsub(vadd(m13, m57), m68), jy = vadd(vadd(m24, m57), m68);
+    V m1 = vsub(vfma(vc<V>(2.f), sd, vmul(vc<V>(-4.f), d[0])), sa);
+    V m2 = vadd(vfma(vc<V>(-2.f), sa, vmul(vc<V>(4.f), d[0])), sd);
+    const V m3 = vadd(jx, fx);                                   // + Sb3
+    V m4 = vfma(vc<V>(-3.f), m13, jx);
+    const V m5 = vadd(jy, fy);                                   // + Sb5
+    V m6 = vfma(vc<V>(-3.f), m24, jy);
+    V m7 = vsub(a13, a24);
+    V m8 = vsub(a57, a68);
+    const V uu = vfma(vx, vx, vmul(vy, vy));
+    const V uF6 = vmul(vfma(vx, fx, vmul(vy, fy)), vc<V>(6.f));
+    const V ru3 = vmul(vmul(rho, vc<V>(3.f)), uu);
+    m1 = vfma(c.h1, uF6, vfma(c.ns1, vsub(m1, vfma(vc<V>(-2.f), m0, ru3)), m1));
+    m2 = vfma(c.nh2, uF6, vfma(c.ns2, vsub(m2, vsub(m0, ru3)), m2));
+    m4 = vfma(c.nh4, fx, vfma(c.ns4, vfma(rho, vx, m4), m4));
+    m6 = vfma(c.nh4, fy, vfma(c.ns4, vfma(rho, vy, m6), m6));
+    const V A = vsub(vmul(vx, vx), vmul(vy, vy));
+    const V B = vsub(vmul(vx, fx), vmul(vy, fy));
+    m7 = vfma(c.hn2, B, vfma(c.nsn, vsub(m7, vmul(rho, A)), m7));
+    const V Cxy = vmul(vx, vy);
+    const V D = vfma(vx, fy, vmul(vy, fx));
+    m8 = vfma(c.hn, D, vfma(c.nsn, vsub(m8, vmul(rho, Cxy)), m8));
+    const float c9 = 1.f / 9.f, c18 = 1.f / 18.f, c36 = 1.f / 36.f, c6 = 1.f / 6.f,
+                c12 = 1.f / 12.f;
+    const V b0 = vmul(vc<V>(c9), m0);
+    const V bA = vfma(vc<V>(-c18), m2, vfma(vc<V>(-c36), m1, b0));   // axis directions
+    const V bD = vfma(vc<V>(c36), m2, vfma(vc<V>(c18), m1, b0));     // diagonals
+    d[0] = vmul(vc<V>(c9), vadd(vsub(m0, m1), m2));
+    const V t1 = vmul(vc<V>(c6), vsub(m3, m4)), t2 = vmul(vc<V>(c6), vsub(m5, m6));
+    const V q7 = vmul(vc<V>(0.25f), m7);
+    const V bAp = vadd(bA, q7), bAm = vsub(bA, q7);
+    d[1] = vadd(bAp, t1);
+    d[3] = vsub(bAp, t1);
+    d[2] = vadd(bAm, t2);
+    d[4] = vsub(bAm, t2);
+    const V px = vfma(vc<V>(c12), m4, vmul(vc<V>(c6), m3));
+    const V py = vfma(vc<V>(c12), m6, vmul(vc<V>(c6), m5));
+    const V q8 = vmul(vc<V>(0.25f), m8);
+    const V bDp = vadd(bD, q8), bDm = vsub(bD, q8);
+    const V spp = vadd(px, py), smp = vsub(py, px);
+    d[5] = vadd(bDp, spp);
+    d[7] = vsub(bDp, spp);
+    d[6] = vadd(bDm, smp);
+    d[8] = vsub(bDm, smp);
+}
+
+template <>
+__device__ __forceinline__ void collide_mrt<float>(float f[9], float r, float vx, float vy,
+                                                   float fx, float fy, float sn, float s1,
+                                                   float s2, float s4) {
+    mrt_collide_v(f, r, vx, vy, fx, fy, mrt_const<float>(sn, s1, s2, s4));
+}
+
+template <>
+__device__ __forceinline__ void collide_regularized<float>(float f[9], float rho, float ux,
+                                                           float uy, float Fx, float Fy,
+                                                           float omega) {
+    const DevMoments<float> m = dev_moments(f);
+    reg_collide_v(f, m, rho, ux, uy, Fx, Fy, reg_const<float>(omega));
+}
+
 template <>
 __device__ __forceinline__ void collide_bgk<float>(float f[9], float r, float vx, float vy,
                                                    float fx, float fy, float om) {
-    const float drho = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
-    const float om1 = 1.f - om, guo = 1.f - 0.5f * om;
-    const float bm = -1.5f * (vx * vx + vy * vy);
-    const float uF3 = 3.f * (vx * fx + vy * fy);
-    const float g3 = 3.f * guo, g9 = 9.f * guo, orr = om * r;
-    f[0] = om1 * f[0] + (4.f / 9.f) * (om * drho + orr * bm - guo * uF3);
-    auto pair = [&](int q, int o, float eu, float eF, float w) {
-        const float E = w * (om * drho + orr * (bm + 4.5f * eu * eu) + g9 * eu * eF - guo * uF3);
-        const float O = w * (3.f * orr * eu + g3 * eF);
-        f[q] = om1 * f[q] + (E + O);
-        f[o] = om1 * f[o] + (E - O);
-    };
-    pair(1, 3, vx, fx, 1.f / 9.f);
-    pair(2, 4, vy, fy, 1.f / 9.f);
-    pair(5, 7, vx + vy, fx + fy, 1.f / 36.f);
-    pair(6, 8, vy - vx, fy - fx, 1.f / 36.f);
+    const DevMoments<float> m = dev_moments(f);
+    bgk_collide_v(f, m.drho, r, vx, vy, fx, fy, bgk_const<float>(om));
 }
 
 // Passive-scalar BGK collision with the first-order equilibrium

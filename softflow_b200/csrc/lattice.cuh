@@ -11,6 +11,8 @@
 // Storage types: double (FP64), float (FP32), or __half holding f - w
 // (FP16-shifted), with FP32 arithmetic for the last two.
 #pragma once
+#include <type_traits>
+
 #include "collide.cuh"
 
 namespace sfg {
@@ -531,6 +533,10 @@ struct Vec<__half> {
 template <typename S, typename R>
 struct Enc {
     static __device__ __forceinline__ R dec(S s, int) { return (R)s; }
+    static __device__ __forceinline__ void dec4(const S s[4], int, R out[4]) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) out[i] = (R)s[i];
+    }
     static __device__ __forceinline__ S enc(R v, int, uint32_t) { return (S)v; }
     static __device__ __forceinline__ void enc4(const R v[4], int, uint32_t, S e[4]) {
 #pragma unroll
@@ -542,6 +548,16 @@ template <>
 struct Enc<__half, float> {   // working representation: deviations d = f - w
     static __device__ __forceinline__ float dec(__half s, int) {
         return __half2float(s) * FP16S_UNSCALE;
+    }
+    // four values, unscaled two at a time (paired multiply, same rounding)
+    static __device__ __forceinline__ void dec4(const __half s[4], int, float out[4]) {
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const F2 a = vmul(mk2(__half2float(s[2 * k]), __half2float(s[2 * k + 1])),
+                              vc<F2>(FP16S_UNSCALE));
+            out[2 * k] = a.v.x;
+            out[2 * k + 1] = a.v.y;
+        }
     }
     static __device__ __forceinline__ __half enc(float v, int q, uint32_t r) {
         const uint32_t d = (r + (uint32_t)q * 0x9E3779B9u) * 1664525u + 1013904223u;
@@ -559,7 +575,8 @@ struct Enc<__half, float> {   // working representation: deviations d = f - w
             h ^= h >> 15;
             h *= 0x2C1B3C6Du;
             h ^= h >> 12;
-            const float lo = v[2 * k] * FP16S_SCALE, hi = v[2 * k + 1] * FP16S_SCALE;
+            const F2 sc = vmul(mk2(v[2 * k], v[2 * k + 1]), vc<F2>(FP16S_SCALE));
+            const float lo = sc.v.x, hi = sc.v.y;
             asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(p[k]) : "f"(hi), "f"(lo), "r"(h));
         }
         e[0] = __ushort_as_half((unsigned short)(p[0] & 0xFFFFu));
@@ -568,6 +585,84 @@ struct Enc<__half, float> {   // working representation: deviations d = f - w
         e[3] = __ushort_as_half((unsigned short)(p[1] >> 16));
     }
 };
+
+// Odd 32-bit multipliers for the dither words of the paired FP16 encode,
+// one per (direction, pair): murmur3's finaliser of the index, evaluated at
+// compile time.
+__host__ __device__ constexpr uint32_t dither_mult(uint32_t j) {
+    uint32_t x = j * 0x9E3779B9u + 0x632BE5ABu;
+    x ^= x >> 16;
+    x *= 0x85EBCA6Bu;
+    x ^= x >> 13;
+    x *= 0xC2B2AE35u;
+    x ^= x >> 16;
+    return x | 1u;
+}
+
+// FP16-shifted encode of four consecutive cells of direction q into two
+// words (cells 0, 1 and 2, 3; the first cell in the low half).  The hardware
+// stochastic rounding (cvt.rs.f16x2.f32) takes its random bits (0-12 for the
+// low half, 16-28 for the high half) from the cell's seed r times a
+// per-(q, pair) odd multiplier: one instruction per word, and a bijection of
+// r, so every dither field stays exactly uniform (rounding unbiased).  The
+// high word of the product would not be: it is bounded by the multiplier.
+__device__ __forceinline__ void enc4_words(F2 a, F2 b, int q, uint32_t r, uint32_t& w0,
+                                           uint32_t& w1) {
+    const F2 sa = vmul(a, vc<F2>(FP16S_SCALE)), sb = vmul(b, vc<F2>(FP16S_SCALE));
+    const uint32_t h0 = r * dither_mult((uint32_t)(2 * q)),
+                   h1 = r * dither_mult((uint32_t)(2 * q + 1));
+    asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(w0) : "f"(sa.v.y), "f"(sa.v.x), "r"(h0));
+    asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(w1) : "f"(sb.v.y), "f"(sb.v.x), "r"(h1));
+}
+__device__ __forceinline__ void enc4_words(const float v[4], int q, uint32_t r, uint32_t& w0,
+                                           uint32_t& w1) {
+    enc4_words(mk2(v[0], v[1]), mk2(v[2], v[3]), q, r, w0, w1);
+}
+
+// Stores the encoded words of one plane of a run (FP16 storage): w0 holds
+// cells x, x + 1 and w1 cells x + 2, x + 3 of the lane.  dx is the x shift
+// (-1, 0, +1); the shifted forms assemble the target words with byte
+// permutes from the lane's words and one neighbour word.  All lanes of the
+// warp must call this (shuffles).
+__device__ __forceinline__ void store_plane4h(__half* __restrict__ row, uint32_t w0, uint32_t w1,
+                                              int dx, int x, int x0, int len, int nx, bool active,
+                                              int lane, int last_lane) {
+    if (dx == 0) {
+        if (active) *reinterpret_cast<uint2*>(row + x) = make_uint2(w0, w1);
+        return;
+    }
+    if (dx > 0) {
+        const uint32_t prev = __shfl_up_sync(0xffffffffu, w1, 1);
+        if (!active) return;
+        const uint32_t b = __byte_perm(w0, w1, 0x5432);
+        if (lane > 0) {
+            *reinterpret_cast<uint2*>(row + x) = make_uint2(__byte_perm(prev, w0, 0x5432), b);
+        } else {
+            row[x + 1] = __ushort_as_half((unsigned short)(w0 & 0xFFFFu));
+            *reinterpret_cast<uint32_t*>(row + x + 2) = b;
+        }
+        if (lane == last_lane) {
+            int xe = x0 + len;
+            if (xe >= nx) xe -= nx;
+            row[xe] = __ushort_as_half((unsigned short)(w1 >> 16));
+        }
+    } else {
+        const uint32_t next = __shfl_down_sync(0xffffffffu, w0, 1);
+        if (!active) return;
+        const uint32_t a = __byte_perm(w0, w1, 0x5432);
+        if (lane < last_lane) {
+            *reinterpret_cast<uint2*>(row + x) = make_uint2(a, __byte_perm(w1, next, 0x5432));
+        } else {
+            *reinterpret_cast<uint32_t*>(row + x) = a;
+            row[x + 2] = __ushort_as_half((unsigned short)(w1 >> 16));
+        }
+        if (lane == 0) {
+            int xb = x0 - 1;
+            if (xb < 0) xb += nx;
+            row[xb] = __ushort_as_half((unsigned short)(w0 & 0xFFFFu));
+        }
+    }
+}
 
 template <typename S>
 __device__ __forceinline__ S shfl_up1(S v) { return __shfl_up_sync(0xffffffffu, v, 1); }
@@ -639,6 +734,19 @@ __device__ __forceinline__ void push_vec4(S* __restrict__ fd, R f[9][4], int x, 
         const int cx = cx_of(q), cy = cy_of(q);
         const bool wall = (cy > 0 && wall_p) || (cy < 0 && wall_m);
         const int qq = wall ? opp_of(q) : q;
+        if constexpr (POP && std::is_same<S, __half>::value && std::is_same<R, float>::value) {
+            uint32_t w0, w1;
+            enc4_words(f[q], qq, seed, w0, w1);
+            if (wall) {
+                store_plane4h(fd + qq * plane + y * pitch, w0, w1, 0, x, x0, len, nx, active,
+                              lane, last_lane);
+            } else {
+                const int yd = cy == 0 ? y : (cy > 0 ? yp : ym);
+                store_plane4h(fd + q * plane + yd * pitch, w0, w1, cx, x, x0, len, nx, active,
+                              lane, last_lane);
+            }
+            continue;
+        }
         S e[4];
         if (POP) {
             Enc<S, R>::enc4(f[q], qq, seed, e);
@@ -717,6 +825,77 @@ __device__ __forceinline__ CellForces<R> run_forces(const ChannelDev& ch, const 
     return cf;
 }
 
+// Forces of cells (i, i + 1) of a run in FP32, one 8-byte load per
+// component (i is even, the run's first cell a multiple of 4 inside its
+// tile): F (Guo force), G (force in the collision's velocity) and P
+// (previous step's force, for the scalar step), with the rules of
+// run_forces.
+struct PairForces {
+    F2 Fx, Fy, Gx, Gy, Px, Py;
+};
+__device__ __forceinline__ F2 ld2(const float* p) {
+    F2 r;
+    r.v = *reinterpret_cast<const float2*>(p);
+    return r;
+}
+template <bool NEED_P>
+__device__ __forceinline__ PairForces pair_forces(const ChannelDev& ch, const RunTiles& rt, int i,
+                                                  const TileView& tv, int stepped) {
+    PairForces r;
+    const float Fux = float(ch.F_uni_x), Fuy = float(ch.F_uni_y);
+    const float Pux = stepped ? Fux : 0.f, Puy = stepped ? Fuy : 0.f;
+    const bool mdf = ch.ibm_iterations > 1;
+    const int c = rt.cell + i;
+    if (rt.s >= 0) {
+        const float* fin = static_cast<const float*>(tv.cur_fin) + (size_t)rt.s * 2 * TILE_CELLS;
+        r.Fx = ld2(fin + c);
+        r.Fy = ld2(fin + TILE_CELLS + c);
+    } else {
+        r.Fx = vc<F2>(Fux);
+        r.Fy = vc<F2>(Fuy);
+    }
+    if (NEED_P || !mdf) {
+        if (rt.ps >= 0) {
+            const float* pf =
+                static_cast<const float*>(tv.prev_fin) + (size_t)rt.ps * 2 * TILE_CELLS;
+            r.Px = ld2(pf + c);
+            r.Py = ld2(pf + TILE_CELLS + c);
+        } else {
+            r.Px = vc<F2>(Pux);
+            r.Py = vc<F2>(Puy);
+        }
+    }
+    if (mdf) {
+        if (rt.s >= 0) {
+            const float* gs = static_cast<const float*>(tv.cur_G) + (size_t)rt.s * 2 * TILE_CELLS;
+            r.Gx = ld2(gs + c);
+            r.Gy = ld2(gs + TILE_CELLS + c);
+        } else {
+            r.Gx = vc<F2>(0.f);
+            r.Gy = r.Gx;
+        }
+    } else {
+        r.Gx = r.Px;
+        r.Gy = r.Py;
+    }
+    return r;
+}
+
+// Collision of two cells (paired FP32), bit-identical to collide_cell<float>.
+template <int COLL>
+__device__ __forceinline__ void collide_cell2(F2 d[9], const DevMoments<F2>& m, F2 rho, F2 ux,
+                                              F2 uy, F2 Fx, F2 Fy, const ChannelDev& ch) {
+    const int coll = COLL >= 0 ? COLL : ch.collision;
+    if (coll == 2)
+        reg_collide_v(d, m, rho, ux, uy, Fx, Fy, reg_const<F2>(float(ch.omega)));
+    else if (coll == 1)
+        mrt_collide_v(d, rho, ux, uy, Fx, Fy,
+                      mrt_const<F2>(float(ch.omega), float(ch.mrt_se), float(ch.mrt_s_eps),
+                                    float(ch.mrt_sq)));
+    else
+        bgk_collide_v(d, m.drho, rho, ux, uy, Fx, Fy, bgk_const<F2>(float(ch.omega)));
+}
+
 // Forces of 4 consecutive cells (same force tile: x is a multiple of 4).
 template <typename R>
 __device__ __forceinline__ void cell_forces4(const ChannelDev& ch, int x, int y,
@@ -741,6 +920,158 @@ __device__ __forceinline__ void collide_cell(R c[9], R rho, R ux, R uy, R Fx, R 
         collide_bgk(c, rho, ux, uy, Fx, Fy, R(ch.omega));
 }
 
+// Loads and decodes the 4 cells of direction q of a run as two pairs
+// (cells 0, 1 and 2, 3): FP32 storage as one 16-byte load, FP16-shifted
+// storage as one 8-byte load whose half pairs convert and unscale in pairs.
+template <typename S>
+__device__ __forceinline__ void load_pairs(const S* p, F2& a, F2& b);
+template <>
+__device__ __forceinline__ void load_pairs<float>(const float* p, F2& a, F2& b) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    a = mk2(v.x, v.y);
+    b = mk2(v.z, v.w);
+}
+template <>
+__device__ __forceinline__ void load_pairs<__half>(const __half* p, F2& a, F2& b) {
+    const uint2 w = __ldg(reinterpret_cast<const uint2*>(p));
+    F2 u, v;
+    u.v = __half22float2(*reinterpret_cast<const __half2*>(&w.x));
+    v.v = __half22float2(*reinterpret_cast<const __half2*>(&w.y));
+    a = vmul(u, vc<F2>(FP16S_UNSCALE));
+    b = vmul(v, vc<F2>(FP16S_UNSCALE));
+}
+
+// Stores plane q of a run from its two pairs (see push_vec4).
+template <typename S>
+__device__ __forceinline__ void store_pairs(S* row, F2 a, F2 b, int q, uint32_t seed, int dx,
+                                            int x, int x0, int len, int nx, bool active,
+                                            int lane, int last_lane);
+template <>
+__device__ __forceinline__ void store_pairs<__half>(__half* row, F2 a, F2 b, int q,
+                                                    uint32_t seed, int dx, int x, int x0, int len,
+                                                    int nx, bool active, int lane,
+                                                    int last_lane) {
+    uint32_t w0, w1;
+    enc4_words(a, b, q, seed, w0, w1);
+    store_plane4h(row, w0, w1, dx, x, x0, len, nx, active, lane, last_lane);
+}
+template <>
+__device__ __forceinline__ void store_pairs<float>(float* row, F2 a, F2 b, int, uint32_t, int dx,
+                                                   int x, int x0, int len, int nx, bool active,
+                                                   int lane, int last_lane) {
+    const float v[4] = {a.v.x, a.v.y, b.v.x, b.v.y};
+    store_plane4<float>(row, v, dx, x, x0, len, nx, active, lane, last_lane);
+}
+
+// lattice_run4 for FP32 arithmetic (FP32 and FP16-shifted storage): the
+// populations stay in register pairs from the load to the store, two cells
+// per paired instruction.
+template <typename S, bool ADR, int COLL>
+__device__ __forceinline__ void lattice_run4f(const RowItem& it, const ChannelDev& ch, int st,
+                                              const S* __restrict__ src, S* __restrict__ dst,
+                                              const float* __restrict__ gsrc,
+                                              float* __restrict__ gdst,
+                                              const float* __restrict__ cfield,
+                                              const TileView& tv, bool adr_on, bool fresh,
+                                              uint32_t step_mix, int lane) {
+    const bool active = 4 * lane < it.len;
+    const int last_lane = (it.len >> 2) - 1;
+    const int nx = ch.nx, ny = ch.ny, pitch = ch.pitch, plane = (int)ch.plane;
+    const int x0 = it.x0, y = it.y;
+    const int x = x0 + 4 * lane;
+    const int n = y * pitch + (active ? x : x0);
+    F2 d[2][9];   // [pair][direction]
+    {
+        const S* fs = src + ch.f_off + n;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            if (active) {
+                load_pairs<S>(fs + q * plane, d[0][q], d[1][q]);
+            } else {
+                d[0][q] = vc<F2>(0.f);
+                d[1][q] = vc<F2>(0.f);
+            }
+        }
+    }
+    float rho[ADR ? 4 : 1], jx[ADR ? 4 : 1], jy[ADR ? 4 : 1], Px[ADR ? 4 : 1], Py[ADR ? 4 : 1];
+    const RunTiles rt = active ? run_tiles(ch, x, y, tv) : RunTiles{-1, -1, 0};
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+        const DevMoments<F2> m = dev_moments(d[p]);
+        const F2 r = vadd(m.drho, vc<F2>(1.f));
+        if (active) {
+            const PairForces pf = pair_forces<ADR>(ch, rt, 2 * p, tv, st);
+            F2 ux, uy;
+            cell_velocity2(r, m.jx, m.jy, pf.Gx, pf.Gy, ux, uy);
+            collide_cell2<COLL>(d[p], m, r, ux, uy, pf.Fx, pf.Fy, ch);
+            if (ADR) {
+                Px[2 * p] = pf.Px.v.x;
+                Px[2 * p + 1] = pf.Px.v.y;
+                Py[2 * p] = pf.Py.v.x;
+                Py[2 * p + 1] = pf.Py.v.y;
+            }
+        }
+        if (ADR) {
+            rho[2 * p] = r.v.x;
+            rho[2 * p + 1] = r.v.y;
+            jx[2 * p] = m.jx.v.x;
+            jx[2 * p + 1] = m.jx.v.y;
+            jy[2 * p] = m.jy.v.x;
+            jy[2 * p + 1] = m.jy.v.y;
+        }
+    }
+    {
+        const Nbr b = neighbours(0, y, nx, ny, ch.periodic_y ? 1 : 0);
+        const uint32_t seed = mix32((uint32_t)(ch.cell_off + n) ^ step_mix);
+        S* fd = dst + ch.f_off;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            const int cx = cx_of(q), cy = cy_of(q);
+            const bool wall = (cy > 0 && b.wall_p) || (cy < 0 && b.wall_m);
+            const int qq = wall ? opp_of(q) : q;
+            if (wall) {
+                store_pairs<S>(fd + qq * plane + y * pitch, d[0][q], d[1][q], qq, seed, 0, x, x0,
+                               it.len, nx, active, lane, last_lane);
+            } else {
+                const int yd = cy == 0 ? y : (cy > 0 ? b.yp : b.ym);
+                store_pairs<S>(fd + q * plane + yd * pitch, d[0][q], d[1][q], q, seed, cx, x, x0,
+                               it.len, nx, active, lane, last_lane);
+            }
+        }
+    }
+    if (ADR) {
+        if (adr_on) {   // warp-uniform
+            float g[9][4];
+            const float* gp = gsrc + ch.g_off + n;
+#pragma unroll
+            for (int q = 0; q < 9; ++q) {
+                if (active) Vec<float>::load4(gp + q * plane, g[q]);
+                else g[q][0] = g[q][1] = g[q][2] = g[q][3] = 0.f;
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                float c[9];
+#pragma unroll
+                for (int q = 0; q < 9; ++q) c[q] = g[q][i];
+                if (active) {
+                    float C = fresh ? cfield[ch.cell_off + n + i]
+                                    : c[0] + c[1] + c[2] + c[3] + c[4] + c[5] + c[6] + c[7] + c[8];
+                    float vx, vy;
+                    cell_velocity(rho[i], jx[i], jy[i], Px[i], Py[i], vx, vy);
+                    collide_scalar(c, C, vx, vy, float(ch.omega_s));
+                }
+#pragma unroll
+                for (int q = 0; q < 9; ++q) g[q][i] = c[q];
+            }
+            const int gmode = ch.periodic_y ? (ch.adr_periodic_y ? 1 : 2) : 0;
+            const Nbr gb = neighbours(0, y, nx, ny, gmode);
+            push_vec4<float, float, false>(gdst + ch.g_off, g, x, x0, it.len, nx, y, gb.ym,
+                                           gb.yp, gb.wall_m, gb.wall_p, pitch, plane, active,
+                                           lane, last_lane, 0u);
+        }
+    }
+}
+
 template <typename S, typename R, bool ADR, int COLL>
 __device__ __forceinline__ void lattice_run4(const RowItem& it, const ChannelDev& ch, int st,
                                              const S* __restrict__ src, S* __restrict__ dst,
@@ -748,6 +1079,11 @@ __device__ __forceinline__ void lattice_run4(const RowItem& it, const ChannelDev
                                              const R* __restrict__ cfield, const TileView& tv,
                                              bool adr_on, bool fresh, uint32_t step_mix,
                                              int lane) {
+    if constexpr (std::is_same<R, float>::value) {
+        lattice_run4f<S, ADR, COLL>(it, ch, st, src, dst, gsrc, gdst, cfield, tv, adr_on, fresh,
+                                    step_mix, lane);
+        return;
+    }
     const bool active = 4 * lane < it.len;
     const int last_lane = (it.len >> 2) - 1;
     const int nx = ch.nx, ny = ch.ny, pitch = ch.pitch, plane = (int)ch.plane;
@@ -765,8 +1101,7 @@ __device__ __forceinline__ void lattice_run4(const RowItem& it, const ChannelDev
             } else {
                 v[0] = v[1] = v[2] = v[3] = S(0);
             }
-#pragma unroll
-            for (int i = 0; i < 4; ++i) f[q][i] = Enc<S, R>::dec(v[i], q);
+            Enc<S, R>::dec4(v, q, f[q]);
         }
     }
     // per cell: forces, moments and collision; the scalar step keeps only
