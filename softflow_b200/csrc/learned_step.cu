@@ -141,7 +141,7 @@ void launch_mdf_learned(const ChannelDev* chans, const CapsuleDev* caps, int M,
     (void)f;
     k_mdf_features<R><<<(M + tb.marker_block - 1) / tb.marker_block, tb.marker_block, 0, st>>>(
         chans, caps, M, mb, tb.tile_slot[parity], static_cast<const typename Mom4<R>::T*>(tb.mom),
-        tb.acc, feat, frame);
+        tb.acc0, feat, frame);   // a learned channel's sweep-0 force is in acc0
     const int tiles = (M + mlp::ROWS - 1) / mlp::ROWS;
     const int g = tiles < grid ? tiles : grid;
     k_mdf_seed<<<g, mlp::ROWS, sizeof(mlp::FwdSmem), st>>>(

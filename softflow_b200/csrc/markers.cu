@@ -549,13 +549,28 @@ constexpr int SPREAD_LIST_MAX = 4096; // longer lists are clamped and flagged
 // Shared memory of one spread warp: the tile's accumulators, the sort buffer
 // of its marker list (sweep 0) and a staged chunk of markers.
 constexpr int SPREAD_CHUNK = 16;      // markers staged per chunk
-struct SpreadWarpSmem {
-    double ax[TILE_CELLS], ay[TILE_CELLS];
-    int list[SPREAD_LCAP];                     // sweep 0: the bitonic sort of long lists
-    double2 f[SPREAD_CHUNK];                   // staged marker data of the chunk
+// Channels narrower than a tile: the stencil data of each marker.
+struct SpreadChunkNarrow {
+    double2 f[SPREAD_CHUNK];
     double ds[SPREAD_CHUNK];
     double wx[SPREAD_CHUNK][4], wy[SPREAD_CHUNK][4];
     int ix[SPREAD_CHUNK], iy[SPREAD_CHUNK], ok[SPREAD_CHUNK];
+};
+// Otherwise: each marker's 16 stencil contributions (f w ds, in the
+// reference's rounding order), the lanes that own a valid point of it, and
+// its stencil origin in tile coordinates.
+struct SpreadChunkWide {
+    double2 c[SPREAD_CHUNK][16];   // point k + 4 sy
+    unsigned mask[SPREAD_CHUNK];
+    int org[SPREAD_CHUNK];         // (column origin + 64) | (row origin + 64) << 8
+};
+struct SpreadWarpSmem {
+    double ax[TILE_CELLS], ay[TILE_CELLS];
+    union {
+        int list[SPREAD_LCAP];                 // sweep 0: the bitonic sort of long lists
+        SpreadChunkNarrow n;                   // (the sort ends before the first chunk)
+        SpreadChunkWide w;
+    } ck;
 };
 constexpr size_t SPREAD_SMEM = sizeof(SpreadWarpSmem) * SPREAD_WARPS;
 
@@ -583,22 +598,19 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
     SpreadWarpSmem& W = reinterpret_cast<SpreadWarpSmem*>(spread_smem)[warp];
     double* ax = W.ax;
     double* ay = W.ay;
-    int* sl = W.list;
+    int* sl = W.ck.list;
     const int n_slots = *n_slots_p;
-    // slots are claimed one at a time (balances uneven list lengths); the
+    // slots are dealt to the warps in a fixed stride (list lengths are
+    // similar; a shared claim counter serialises on one L2 address); the
     // next slot's record is fetched while the current one is processed
-    auto claim = [&]() {
-        int v = 0;
-        if (lane == 0) v = atomicAdd(slot_ctr, 1);
-        return __shfl_sync(0xffffffffu, v, 0);
-    };
-    int next = claim();
+    const int nwarps = gridDim.x * SPREAD_WARPS;
+    int next = blockIdx.x * SPREAD_WARPS + warp;
     SlotInfo nfo{};
     if (next < n_slots) nfo = slot_info[next];
     while (next < n_slots) {
         const int slot = next;
         const SlotInfo si = nfo;
-        next = claim();
+        next += nwarps;
         if (next < n_slots) nfo = slot_info[next];
         const int chan = si.chan;
         const ChannelDev& ch = chans[chan];
@@ -668,7 +680,10 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
         const size_t base = (size_t)slot * 2 * TILE_CELLS;
         const bool last = mode == MDF_LEARNED ? true : (mode == MDF_SEED ? false : sweep == K - 1);
         // a learned channel's fallback restarts from the membrane-only force
-        const double* src = (mode == MDF_PLAIN && ch.learned && sweep == 1) ? acc0 : acc;
+        // a learned channel's membrane-only force lives in acc0 only: the
+        // seed sweep and a fallback's restart read it there
+        const double* src =
+            (ch.learned && (mode == MDF_SEED || (mode == MDF_PLAIN && sweep == 1))) ? acc0 : acc;
         for (int c = lane; c < TILE_CELLS; c += 32) {
             const double vx = sweep > 0 ? src[base + c] : 0.0;
             const double vy = sweep > 0 ? src[base + TILE_CELLS + c] : 0.0;
@@ -680,16 +695,139 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
             }
         }
         __syncwarp();
-        // Markers in list order, SPREAD_CHUNK at a time: lane j < SPREAD_CHUNK
-        // loads marker j of the next chunk into registers while the current
-        // chunk is added, then stages it in shared memory.  Lane (a, b) =
-        // (lane & 7, lane >> 3) owns the tile cells whose local column is
-        // a mod 8 and row b mod 4; the 4 x 4 stencil of a marker has 4
-        // consecutive columns and rows, so its 16 points fall on 16 distinct
-        // lanes.  Each lane adds its own point's term to its own cell, marker
-        // after marker, so every cell receives its terms in the reference's
-        // order with no synchronisation between markers.
         const int la = lane & 7, lb = lane >> 3;
+        if (nx > TILE_W) {
+            // Markers in list order, SPREAD_CHUNK at a time.  Staging: lanes
+            // j and j + 16 take marker j of the chunk and evaluate its stencil
+            // rows 2h, 2h + 1 (h = lane / 16): the weights w = phi(rx)
+            // phi(ry), the contributions (f w) ds and the lanes owning each
+            // valid point.  Lane (a, b) = (lane & 7, lane >> 3) owns the tile
+            // cells whose local column is a mod 8 and row b mod 4; the 4 x 4
+            // stencil has 4 consecutive columns and rows, so its 16 points
+            // fall on 16 distinct lanes.  Then every lane adds its own point of
+            // each marker to its own cell, marker after marker, so every cell
+            // receives its terms in the reference's order.
+            const int jm = lane & 15, hh = lane >> 4;
+            double2 rf = make_double2(0.0, 0.0), rw0 = rf, rw1 = rf, rv = rf;
+            double rds = 0.0;
+            int rix = 0, riy = 0;
+            auto fetch = [&](int c) {
+                if (c + jm < cnt) {
+                    const int m = lst[c + jm];
+                    rf = sweep == 0 ? mb.frc[m] : mb.dF[m];
+                    rix = mb.ix0[m];
+                    riy = mb.iy0[m];
+                    rds = mb.ds[m];
+                    const double2* wx2 = reinterpret_cast<const double2*>(mb.wx + 4 * (size_t)m);
+                    const double2* wy2 = reinterpret_cast<const double2*>(mb.wy + 4 * (size_t)m);
+                    rw0 = wx2[0];
+                    rw1 = wx2[1];
+                    rv = wy2[hh];
+                }
+            };
+            fetch(0);
+            for (int c0 = 0; c0 < cnt; c0 += SPREAD_CHUNK) {
+                const int nb = cnt - c0 < SPREAD_CHUNK ? cnt - c0 : SPREAD_CHUNK;
+                __syncwarp();
+                unsigned mask = 0u;
+                int o = 0;
+                const int r0 = riy - 1 - y0;
+                if (jm < nb) {
+                    const bool ok = !(isnan(rf.x) || isnan(rf.y));
+                    const double wxk[4] = {rw0.x, rw0.y, rw1.x, rw1.y};
+                    bool vk[4];
+                    bool have = false;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        int jx = rix - 1 + k;
+                        if (jx < 0) jx += nx;
+                        if (jx >= nx) jx -= nx;
+                        const int cl = jx - x0;
+                        vk[k] = jx >= 0 && jx < nx && cl >= 0 && cl < TILE_W;
+                        if (vk[k] && !have) {
+                            o = cl - k;
+                            have = true;
+                        }
+                    }
+#pragma unroll
+                    for (int t = 0; t < 2; ++t) {
+                        const int sy = 2 * hh + t;
+                        const int cyl = r0 + sy, iy = cyl + y0;
+                        const bool vrow = ok && cyl >= 0 && cyl < TILE_H && iy >= 0 && iy < ny;
+                        const double wy = t == 0 ? rv.x : rv.y;
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const double w = wxk[k] * wy;
+                            if (vrow && vk[k] && w > 1e-15) {
+                                W.ck.w.c[jm][k + 4 * sy] =
+                                    make_double2(rf.x * w * rds, rf.y * w * rds);
+                                mask |= 1u << (((o + k) & 7) + 8 * (cyl & 3));
+                            }
+                        }
+                    }
+                }
+                mask |= __shfl_xor_sync(0xffffffffu, mask, 16);
+                if (hh == 0 && jm < nb) {
+                    W.ck.w.mask[jm] = mask;
+                    W.ck.w.org[jm] = (o + 64) | ((r0 + 64) << 8);
+                }
+                __syncwarp();
+                fetch(c0 + SPREAD_CHUNK);   // in flight while this chunk is added
+                // this lane's point of marker j: cell index and contribution
+                auto point = [&](int j, int& c, double2& v) {
+                    const int org = W.ck.w.org[j];
+                    const int oj = (org & 0xFF) - 64, rj = (org >> 8) - 64;
+                    const int k = (la - oj) & 7, sy = (lb - rj) & 3;
+                    v = W.ck.w.c[j][k + 4 * sy];
+                    c = (rj + sy) * TILE_W + oj + k;
+                };
+                int j = 0;
+                // two markers at a time: both cells are read before either is
+                // written, the second addition taking the first's sum when
+                // both points are the same cell (same order, same rounding)
+                for (; j + 1 < nb; j += 2) {
+                    const bool h0 = (W.ck.w.mask[j] >> lane) & 1u;
+                    const bool h1 = (W.ck.w.mask[j + 1] >> lane) & 1u;
+                    int c0i = 0, c1i = 0;
+                    double2 v0 = make_double2(0.0, 0.0), v1 = v0;
+                    if (h0) point(j, c0i, v0);
+                    if (h1) point(j + 1, c1i, v1);
+                    double a0x = 0.0, a0y = 0.0, a1x = 0.0, a1y = 0.0;
+                    if (h0) {
+                        a0x = ax[c0i];
+                        a0y = ay[c0i];
+                    }
+                    if (h1) {
+                        a1x = ax[c1i];
+                        a1y = ay[c1i];
+                    }
+                    if (h0) {
+                        a0x += v0.x;
+                        a0y += v0.y;
+                        ax[c0i] = a0x;
+                        ay[c0i] = a0y;
+                    }
+                    if (h1) {
+                        if (h0 && c1i == c0i) {
+                            a1x = a0x;
+                            a1y = a0y;
+                        }
+                        ax[c1i] = a1x + v1.x;
+                        ay[c1i] = a1y + v1.y;
+                    }
+                }
+                if (j < nb && ((W.ck.w.mask[j] >> lane) & 1u)) {
+                    int c;
+                    double2 v;
+                    point(j, c, v);
+                    ax[c] += v.x;
+                    ay[c] += v.y;
+                }
+            }
+        } else {
+        // One tile holds both sides of the periodic seam: two stencil
+        // columns can share a residue, so a lane applies each of its points.
+        SpreadChunkNarrow& N = W.ck.n;
         double2 rf = make_double2(0.0, 0.0), rw0 = rf, rw1 = rf, rv0 = rf, rv1 = rf;
         double rds = 0.0;
         int rix = 0, riy = 0;
@@ -710,86 +848,48 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
             const int nb = cnt - c0 < SPREAD_CHUNK ? cnt - c0 : SPREAD_CHUNK;
             __syncwarp();
             if (lane < nb) {
-                W.f[lane] = rf;
-                W.ok[lane] = !(isnan(rf.x) || isnan(rf.y));
-                W.ds[lane] = rds;
-                W.ix[lane] = rix;
-                W.iy[lane] = riy;
-                W.wx[lane][0] = rw0.x; W.wx[lane][1] = rw0.y; W.wx[lane][2] = rw1.x; W.wx[lane][3] = rw1.y;
-                W.wy[lane][0] = rv0.x; W.wy[lane][1] = rv0.y; W.wy[lane][2] = rv1.x; W.wy[lane][3] = rv1.y;
+                N.f[lane] = rf;
+                N.ok[lane] = !(isnan(rf.x) || isnan(rf.y));
+                N.ds[lane] = rds;
+                N.ix[lane] = rix;
+                N.iy[lane] = riy;
+                N.wx[lane][0] = rw0.x; N.wx[lane][1] = rw0.y; N.wx[lane][2] = rw1.x; N.wx[lane][3] = rw1.y;
+                N.wy[lane][0] = rv0.x; N.wy[lane][1] = rv0.y; N.wy[lane][2] = rv1.x; N.wy[lane][3] = rv1.y;
             }
             __syncwarp();
             fetch(c0 + SPREAD_CHUNK);   // in flight while this chunk is added
             for (int j = 0; j < nb; ++j) {
-                if (!W.ok[j]) continue;  // warp-uniform
-                const int jx0 = W.ix[j] - 1;
-                if (nx <= TILE_W) {
-                    // one tile holds both sides of the periodic seam: two
-                    // stencil columns can share a residue, so apply every one
-                    const int r0n = W.iy[j] - 1 - y0;
-                    const int syn = (lb - r0n) & 3;
-                    const int cyn = r0n + syn;
-                    if (cyn >= 0 && cyn < TILE_H && cyn + y0 >= 0 && cyn + y0 < ny) {
-                        for (int k = 0; k < 4; ++k) {
-                            int jx = jx0 + k;
-                            if (jx < 0) jx += nx;
-                            if (jx >= nx) jx -= nx;
-                            const int cl = jx - x0;
-                            if (cl < 0 || cl >= TILE_W || (cl & 7) != la) continue;
-                            const double w = W.wx[j][k] * W.wy[j][syn];
-                            if (w > 1e-15) {
-                                const double ds = W.ds[j];
-                                const double2 fo = W.f[j];
-                                const int c = cyn * TILE_W + cl;
-                                ax[c] += fo.x * w * ds;
-                                ay[c] += fo.y * w * ds;
-                            }
+                if (!N.ok[j]) continue;  // warp-uniform
+                const int jx0 = N.ix[j] - 1;
+                const int r0n = N.iy[j] - 1 - y0;
+                const int syn = (lb - r0n) & 3;
+                const int cyn = r0n + syn;
+                if (cyn >= 0 && cyn < TILE_H && cyn + y0 >= 0 && cyn + y0 < ny) {
+                    for (int k = 0; k < 4; ++k) {
+                        int jx = jx0 + k;
+                        if (jx < 0) jx += nx;
+                        if (jx >= nx) jx -= nx;
+                        const int cl = jx - x0;
+                        if (cl < 0 || cl >= TILE_W || (cl & 7) != la) continue;
+                        const double w = N.wx[j][k] * N.wy[j][syn];
+                        if (w > 1e-15) {
+                            const double ds = N.ds[j];
+                            const double2 fo = N.f[j];
+                            const int c = cyn * TILE_W + cl;
+                            ax[c] += fo.x * w * ds;
+                            ay[c] += fo.y * w * ds;
                         }
-                    }
-                    continue;
-                }
-                // this lane's stencil column sx: wrap(ix0 - 1 + sx) in the tile
-                // with local column a mod 8 (at most one of the 4 when the tile
-                // does not hold both sides of the seam)
-                int sx = -1, cxl = 0;
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    int jx = jx0 + k;
-                    if (jx < 0) jx += nx;
-                    if (jx >= nx) jx -= nx;
-                    const int cl = jx - x0;
-                    if (cl >= 0 && cl < TILE_W && (cl & 7) == la) {
-                        sx = k;
-                        cxl = cl;
-                    }
-                }
-                // and its row sy: local row b mod 4 (exactly one of the 4)
-                const int r0 = W.iy[j] - 1 - y0;
-                const int sy = (lb - r0) & 3;
-                const int cyl = r0 + sy;
-                const int iy = cyl + y0;
-                if (sx >= 0 && cyl >= 0 && cyl < TILE_H && iy >= 0 && iy < ny) {
-                    const double w = W.wx[j][sx] * W.wy[j][sy];
-                    if (w > 1e-15) {
-                        const double ds = W.ds[j];
-                        const double2 fo = W.f[j];
-                        const int c = cyl * TILE_W + cxl;
-                        ax[c] += fo.x * w * ds;
-                        ay[c] += fo.y * w * ds;
                     }
                 }
             }
         }
+        }
         __syncwarp();
         if (!last) {
-            const bool keep0 = (sweep == 0 && ch.learned);
+            double* out = (sweep == 0 && ch.learned) ? acc0 : acc;
             for (int c = lane; c < TILE_CELLS; c += 32) {
-                acc[base + c] = ax[c];
-                acc[base + TILE_CELLS + c] = ay[c];
-                if (keep0) {
-                    acc0[base + c] = ax[c];
-                    acc0[base + TILE_CELLS + c] = ay[c];
-                }
+                out[base + c] = ax[c];
+                out[base + TILE_CELLS + c] = ay[c];
             }
             __syncwarp();
             continue;
@@ -816,8 +916,7 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
                 }
                 n_fluid += fluid ? 1 : 0;
             }
-            acc[base + c] = vx;
-            acc[base + TILE_CELLS + c] = vy;
+            // (no sweep reads acc after a channel's last one)
             fin[base + c] = (R)vx;
             fin[base + TILE_CELLS + c] = (R)vy;
         }
