@@ -54,25 +54,61 @@ __device__ __forceinline__ double2 interp_u_acc(const ChannelDev& ch, const Mark
     (void)tile_slot;
     const int ix0 = mb.ix0[m], iy0 = mb.iy0[m];
     const StencilSlots ss(mb, m, iy0);
+    const double2* wx2 = reinterpret_cast<const double2*>(mb.wx + 4 * (size_t)m);
+    const double2* wy2 = reinterpret_cast<const double2*>(mb.wy + 4 * (size_t)m);
+    const double2 wxa = wx2[0], wxb = wx2[1], wya = wy2[0], wyb = wy2[1];
+    const double wxs[4] = {wxa.x, wxa.y, wxb.x, wxb.y};
+    const double wys[4] = {wya.x, wya.y, wyb.x, wyb.y};
+    int jxs[4];
+#pragma unroll
+    for (int sx = 0; sx < 4; ++sx) {
+        int jx = ix0 - 1 + sx;
+        if (jx < 0) jx += ch.nx;
+        if (jx >= ch.nx) jx -= ch.nx;
+        jxs[sx] = jx;
+    }
     double ux = 0.0, uy = 0.0;
-    for (int iy = iy0 - 1; iy <= iy0 + 2; ++iy) {
-        for (int ix = ix0 - 1; ix <= ix0 + 2; ++ix) {
-            int jx = ix;
-            if (jx < 0) jx += ch.nx;
-            if (jx >= ch.nx) jx -= ch.nx;
-            const int jy = iy;
-            if (jy < 0 || jy >= ch.ny || jx < 0 || jx >= ch.nx) continue;
-            const double w = mb.wx[4 * m + (ix - ix0 + 1)] * mb.wy[4 * m + (iy - iy0 + 1)];
+    // one stencil row at a time: the populations and forces of its four
+    // cells are loaded together, then its terms are added in order
+#pragma unroll
+    for (int sy = 0; sy < 4; ++sy) {
+        const int jy = iy0 - 1 + sy;
+        R v[4][9];
+        A fx[4], fy[4];
+        bool in[4], solid[4];
+#pragma unroll
+        for (int sx = 0; sx < 4; ++sx) {
+            const int jx = jxs[sx];
+            in[sx] = jy >= 0 && jy < ch.ny && jx >= 0 && jx < ch.nx;
+            solid[sx] = in[sx] && cell_kind(ch, jx, jy) == CK_SOLID;
+            if (in[sx] && !solid[sx]) {
+                const long long n = (long long)jy * ch.pitch + jx;
+#pragma unroll
+                for (int q = 0; q < 9; ++q)
+                    v[sx][q] = PopIO<S, R>::ld(f + ch.f_off + q * ch.plane + n, q);
+                const size_t ci = (size_t)ss.slot(sx, jy) * 2 * TILE_CELLS +
+                                  (jy % TILE_H) * TILE_W + (jx % TILE_W);
+                fx[sx] = acc[ci];
+                fy[sx] = acc[ci + TILE_CELLS];
+            }
+        }
+#pragma unroll
+        for (int sx = 0; sx < 4; ++sx) {
+            if (!in[sx]) continue;
+            const double w = wxs[sx] * wys[sy];
             if (w > 1e-15) {
-                double rho, jxm, jym;
-                bool solid;
-                cell_rho_j<S, R>(ch, f, jx, jy, rho, jxm, jym, solid);
+                double rho = 0.0, jxm = 0.0, jym = 0.0;
+                if (!solid[sx]) {
+                    R r, a, b;
+                    lattice_moments(v[sx], r, a, b);
+                    rho = (double)r;
+                    jxm = (double)a;
+                    jym = (double)b;
+                }
                 double cu = 0.0, cv = 0.0;
-                if (!solid && rho > 1e-15) {
-                    const size_t ci = (size_t)ss.slot(ix - ix0 + 1, jy) * 2 * TILE_CELLS +
-                                      (jy % TILE_H) * TILE_W + (jx % TILE_W);
-                    cu = (jxm + 0.5 * (double)acc[ci]) / rho;
-                    cv = (jym + 0.5 * (double)acc[ci + TILE_CELLS]) / rho;
+                if (!solid[sx] && rho > 1e-15) {
+                    cu = (jxm + 0.5 * (double)fx[sx]) / rho;
+                    cv = (jym + 0.5 * (double)fy[sx]) / rho;
                 }
                 ux += cu * w;
                 uy += cv * w;
@@ -92,7 +128,11 @@ template <> struct Mom4<double> { using T = double4; };
 template <> struct Mom4<float> { using T = float4; };
 
 // interp_u_acc with the step's tile moments: the same terms in the same
-// order, so the same result bit for bit.
+// order.  The loads of a stencil half (two rows: moments and force of eight
+// cells) are issued together before any of their terms is formed, so a
+// marker waits for two rounds of gathers instead of one per cell.  FP64
+// divides by rho as the reference does (bit for bit); FP32-arithmetic modes
+// multiply by one reciprocal per cell.
 template <typename R>
 __device__ __forceinline__ double2 interp_u_mom(const ChannelDev& ch, const MarkerBufs& mb, int m,
                                                const int* __restrict__ tile_slot,
@@ -101,27 +141,57 @@ __device__ __forceinline__ double2 interp_u_mom(const ChannelDev& ch, const Mark
     (void)tile_slot;
     const int ix0 = mb.ix0[m], iy0 = mb.iy0[m];
     const StencilSlots ss(mb, m, iy0);
+    const double2* wx2 = reinterpret_cast<const double2*>(mb.wx + 4 * (size_t)m);
+    const double2* wy2 = reinterpret_cast<const double2*>(mb.wy + 4 * (size_t)m);
+    const double2 wxa = wx2[0], wxb = wx2[1], wya = wy2[0], wyb = wy2[1];
+    const double wxs[4] = {wxa.x, wxa.y, wxb.x, wxb.y};
+    const double wys[4] = {wya.x, wya.y, wyb.x, wyb.y};
+    int jxs[4];
+#pragma unroll
+    for (int sx = 0; sx < 4; ++sx) {
+        int jx = ix0 - 1 + sx;
+        if (jx < 0) jx += ch.nx;
+        if (jx >= ch.nx) jx -= ch.nx;
+        jxs[sx] = jx;
+    }
     double ux = 0.0, uy = 0.0;
 #pragma unroll
-    for (int sy = 0; sy < 4; ++sy) {
+    for (int half = 0; half < 2; ++half) {
+        typename Mom4<R>::T q[8];
+        double fx[8], fy[8];
+        bool in[8];
 #pragma unroll
-        for (int sx = 0; sx < 4; ++sx) {
-            int jx = ix0 - 1 + sx;
-            const int jy = iy0 - 1 + sy;
-            if (jx < 0) jx += ch.nx;
-            if (jx >= ch.nx) jx -= ch.nx;
-            if (jy < 0 || jy >= ch.ny || jx < 0 || jx >= ch.nx) continue;
-            const double w = mb.wx[4 * m + sx] * mb.wy[4 * m + sy];
+        for (int i = 0; i < 8; ++i) {
+            const int sy = 2 * half + (i >> 2), sx = i & 3;
+            const int jx = jxs[sx], jy = iy0 - 1 + sy;
+            in[i] = jy >= 0 && jy < ch.ny && jx >= 0 && jx < ch.nx;
+            const int sl = in[i] ? ss.slot(sx, jy) : -1;
+            in[i] = in[i] && sl >= 0;
+            if (in[i]) {
+                const int cell = (jy % TILE_H) * TILE_W + (jx % TILE_W);
+                q[i] = mom[(size_t)sl * TILE_CELLS + cell];
+                const size_t ci = (size_t)sl * 2 * TILE_CELLS + cell;
+                fx[i] = acc[ci];
+                fy[i] = acc[ci + TILE_CELLS];
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int sy = 2 * half + (i >> 2), sx = i & 3;
+            if (!in[i]) continue;
+            const double w = wxs[sx] * wys[sy];
             if (w > 1e-15) {
-                const size_t cm = (size_t)ss.slot(sx, jy) * TILE_CELLS + (jy % TILE_H) * TILE_W +
-                                  (jx % TILE_W);
-                const auto q = mom[cm];
-                const double rho = (double)q.x;
+                const double rho = (double)q[i].x;
                 double cu = 0.0, cv = 0.0;
                 if (rho > 1e-15) {
-                    const size_t ci = (cm / TILE_CELLS) * 2 * TILE_CELLS + cm % TILE_CELLS;
-                    cu = ((double)q.y + 0.5 * acc[ci]) / rho;
-                    cv = ((double)q.z + 0.5 * acc[ci + TILE_CELLS]) / rho;
+                    if constexpr (sizeof(R) == 8) {
+                        cu = ((double)q[i].y + 0.5 * fx[i]) / rho;
+                        cv = ((double)q[i].z + 0.5 * fy[i]) / rho;
+                    } else {
+                        const double inv = 1.0 / rho;
+                        cu = ((double)q[i].y + 0.5 * fx[i]) * inv;
+                        cv = ((double)q[i].z + 0.5 * fy[i]) * inv;
+                    }
                 }
                 ux += cu * w;
                 uy += cv * w;
