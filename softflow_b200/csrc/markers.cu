@@ -564,8 +564,15 @@ struct SpreadChunkWide {
     unsigned mask[SPREAD_CHUNK];
     int org[SPREAD_CHUNK];         // (column origin + 64) | (row origin + 64) << 8
 };
+// The tile accumulators keep rows of TILE_W + 4 doubles: the 4 x 4 stencil
+// points of a marker (4 consecutive rows and columns) then fall on 16
+// distinct bank pairs (a row stride of 32 doubles puts all 4 rows on the same
+// banks: 4-way conflicts on every accumulation).
+constexpr int ACC_W = TILE_W + 4;
+constexpr int ACC_CELLS = TILE_H * ACC_W;
+__device__ __forceinline__ int acc_at(int c) { return (c / TILE_W) * ACC_W + (c % TILE_W); }
 struct SpreadWarpSmem {
-    double ax[TILE_CELLS], ay[TILE_CELLS];
+    double ax[ACC_CELLS], ay[ACC_CELLS];
     union {
         int list[SPREAD_LCAP];                 // sweep 0: the bitonic sort of long lists
         SpreadChunkNarrow n;                   // (the sort ends before the first chunk)
@@ -687,8 +694,8 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
         for (int c = lane; c < TILE_CELLS; c += 32) {
             const double vx = sweep > 0 ? src[base + c] : 0.0;
             const double vy = sweep > 0 ? src[base + TILE_CELLS + c] : 0.0;
-            ax[c] = vx;
-            ay[c] = vy;
+            ax[acc_at(c)] = vx;
+            ay[acc_at(c)] = vy;
             if (last && K > 1) {
                 gsnap[base + c] = (R)vx;
                 gsnap[base + TILE_CELLS + c] = (R)vy;
@@ -779,7 +786,7 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
                     const int oj = (org & 0xFF) - 64, rj = (org >> 8) - 64;
                     const int k = (la - oj) & 7, sy = (lb - rj) & 3;
                     v = W.ck.w.c[j][k + 4 * sy];
-                    c = (rj + sy) * TILE_W + oj + k;
+                    c = (rj + sy) * ACC_W + oj + k;
                 };
                 int j = 0;
                 // two markers at a time: both cells are read before either is
@@ -875,7 +882,7 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
                         if (w > 1e-15) {
                             const double ds = N.ds[j];
                             const double2 fo = N.f[j];
-                            const int c = cyn * TILE_W + cl;
+                            const int c = cyn * ACC_W + cl;
                             ax[c] += fo.x * w * ds;
                             ay[c] += fo.y * w * ds;
                         }
@@ -888,8 +895,8 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
         if (!last) {
             double* out = (sweep == 0 && ch.learned) ? acc0 : acc;
             for (int c = lane; c < TILE_CELLS; c += 32) {
-                out[base + c] = ax[c];
-                out[base + TILE_CELLS + c] = ay[c];
+                out[base + c] = ax[acc_at(c)];
+                out[base + TILE_CELLS + c] = ay[acc_at(c)];
             }
             __syncwarp();
             continue;
@@ -900,7 +907,7 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
         const bool body = (ch.body_fx != 0.0 || ch.body_fy != 0.0);
         for (int c = lane; c < TILE_CELLS; c += 32) {
             const int jx = x0 + (c % TILE_W), jy = y0 + (c / TILE_W);
-            double vx = ax[c], vy = ay[c];
+            double vx = ax[acc_at(c)], vy = ay[acc_at(c)];
             if (jx < nx && jy < ny) {
                 const bool fluid = cell_kind(ch, jx, jy) == CK_FLUID;
                 if (fluid && body) {
