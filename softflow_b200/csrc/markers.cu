@@ -560,7 +560,7 @@ struct SpreadChunkNarrow {
 // reference's rounding order), the lanes that own a valid point of it, and
 // its stencil origin in tile coordinates.
 struct SpreadChunkWide {
-    double2 c[SPREAD_CHUNK][16];   // point k + 4 sy
+    double2 c[SPREAD_CHUNK][17];   // point k + 4 sy (padded: conflict-free staging stores)
     unsigned mask[SPREAD_CHUNK];
     int org[SPREAD_CHUNK];         // (column origin + 64) | (row origin + 64) << 8
 };
