@@ -127,10 +127,10 @@ template <typename R> struct Mom4;
 template <> struct Mom4<double> { using T = double4; };
 template <> struct Mom4<float> { using T = float4; };
 
-// interp_u_acc with the step's tile moments: the same terms in the same
-// order.  The loads of a stencil half (two rows: moments and force of eight
-// cells) are issued together before any of their terms is formed, so a
-// marker waits for two rounds of gathers instead of one per cell.  FP64
+// interp_u_acc with the step's tile moments and the accumulated force acc
+// ([slot][TILE_CELLS] (x, y) pairs): the same terms in the same order.  The loads of a stencil row (moments and force of four cells) are
+// issued together before any of their terms is formed, so a marker waits
+// for one round of gathers per row instead of one per cell.  FP64
 // divides by rho as the reference does (bit for bit); FP32-arithmetic modes
 // multiply by one reciprocal per cell.
 template <typename R>
@@ -156,13 +156,13 @@ __device__ __forceinline__ double2 interp_u_mom(const ChannelDev& ch, const Mark
     }
     double ux = 0.0, uy = 0.0;
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {
-        typename Mom4<R>::T q[8];
-        double fx[8], fy[8];
-        bool in[8];
+    for (int half = 0; half < 4; ++half) {
+        typename Mom4<R>::T q[4];
+        double fx[4], fy[4];
+        bool in[4];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int sy = 2 * half + (i >> 2), sx = i & 3;
+        for (int i = 0; i < 4; ++i) {
+            const int sy = half, sx = i;
             const int jx = jxs[sx], jy = iy0 - 1 + sy;
             in[i] = jy >= 0 && jy < ch.ny && jx >= 0 && jx < ch.nx;
             const int sl = in[i] ? ss.slot(sx, jy) : -1;
@@ -170,14 +170,14 @@ __device__ __forceinline__ double2 interp_u_mom(const ChannelDev& ch, const Mark
             if (in[i]) {
                 const int cell = (jy % TILE_H) * TILE_W + (jx % TILE_W);
                 q[i] = mom[(size_t)sl * TILE_CELLS + cell];
-                const size_t ci = (size_t)sl * 2 * TILE_CELLS + cell;
-                fx[i] = acc[ci];
-                fy[i] = acc[ci + TILE_CELLS];
+                const double2 a = reinterpret_cast<const double2*>(acc)[(size_t)sl * TILE_CELLS + cell];
+                fx[i] = a.x;
+                fy[i] = a.y;
             }
         }
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int sy = 2 * half + (i >> 2), sx = i & 3;
+        for (int i = 0; i < 4; ++i) {
+            const int sy = half, sx = i;
             if (!in[i]) continue;
             const double w = wxs[sx] * wys[sy];
             if (w > 1e-15) {

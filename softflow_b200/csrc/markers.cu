@@ -686,14 +686,15 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
         }
         const size_t base = (size_t)slot * 2 * TILE_CELLS;
         const bool last = mode == MDF_LEARNED ? true : (mode == MDF_SEED ? false : sweep == K - 1);
-        // a learned channel's fallback restarts from the membrane-only force
         // a learned channel's membrane-only force lives in acc0 only: the
-        // seed sweep and a fallback's restart read it there
-        const double* src =
-            (ch.learned && (mode == MDF_SEED || (mode == MDF_PLAIN && sweep == 1))) ? acc0 : acc;
+        // seed sweep and a fallback's restart read it there.  The
+        // accumulators hold (x, y) pairs per cell: [slot][TILE_CELLS] double2.
+        const double2* src = reinterpret_cast<const double2*>(
+            (ch.learned && (mode == MDF_SEED || (mode == MDF_PLAIN && sweep == 1))) ? acc0 : acc);
+        const size_t base2 = (size_t)slot * TILE_CELLS;
         for (int c = lane; c < TILE_CELLS; c += 32) {
-            const double vx = sweep > 0 ? src[base + c] : 0.0;
-            const double vy = sweep > 0 ? src[base + TILE_CELLS + c] : 0.0;
+            const double2 a = sweep > 0 ? src[base2 + c] : make_double2(0.0, 0.0);
+            const double vx = a.x, vy = a.y;
             ax[acc_at(c)] = vx;
             ay[acc_at(c)] = vy;
             if (last && K > 1) {
@@ -893,11 +894,9 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
         }
         __syncwarp();
         if (!last) {
-            double* out = (sweep == 0 && ch.learned) ? acc0 : acc;
-            for (int c = lane; c < TILE_CELLS; c += 32) {
-                out[base + c] = ax[acc_at(c)];
-                out[base + TILE_CELLS + c] = ay[acc_at(c)];
-            }
+            double2* out = reinterpret_cast<double2*>((sweep == 0 && ch.learned) ? acc0 : acc);
+            for (int c = lane; c < TILE_CELLS; c += 32)
+                out[base2 + c] = make_double2(ax[acc_at(c)], ay[acc_at(c)]);
             __syncwarp();
             continue;
         }

@@ -35,12 +35,12 @@ struct TileBufs {
     int* n_slots = nullptr;     // [1]
     int* list = nullptr;        // [8 M]
     int* scan_tmp = nullptr;
-    double* acc = nullptr;      // [max_slots][2][TILE_CELLS]
+    double* acc = nullptr;      // [max_slots][TILE_CELLS][2]: (x, y) per cell
     void* gsnap = nullptr;      // [max_slots][2][TILE_CELLS] (R)
     void* fin[2] = {nullptr, nullptr};
     int* capped = nullptr;      // [nchan]
     int* fluid_touched = nullptr;
-    double* acc0 = nullptr;     // [max_slots][2][TILE_CELLS] force after the membrane spread
+    double* acc0 = nullptr;     // [max_slots][TILE_CELLS][2] force after the membrane spread
     void* mom = nullptr;        // [max_slots][TILE_CELLS] (rho, jx, jy, 0) of R (step's moments)
     int marker_block = 128;         // block size of the per-marker kernels (tuned)
     SlotInfo* slot_info = nullptr;  // [max_slots]
