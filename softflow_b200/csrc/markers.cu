@@ -1019,22 +1019,35 @@ __global__ void k_tile_moments(const ChannelDev* __restrict__ chans,
         const ChannelDev& ch = chans[si.chan];
         const int x0 = si.x0, y0 = si.y0;
         const int jx = x0 + lane;
+        // four rows at a time: their 36 population loads are issued together
 #pragma unroll
-        for (int r = 0; r < TILE_H; ++r) {
-            const int jy = y0 + r;
-            typename Mom4<R>::T q;
-            q.x = 0; q.y = 0; q.z = 0; q.w = 0;
-            if (jx < ch.nx && jy < ch.ny) {
-                double rho, jxm, jym;
-                bool solid;
-                cell_rho_j<S, R>(ch, f, jx, jy, rho, jxm, jym, solid);
-                if (!solid) {
-                    q.x = (R)rho;
-                    q.y = (R)jxm;
-                    q.z = (R)jym;
+        for (int rb = 0; rb < TILE_H; rb += 4) {
+            R v[4][9];
+            bool use[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int jy = y0 + rb + i;
+                use[i] = jx < ch.nx && jy < ch.ny && cell_kind(ch, jx, jy) != CK_SOLID;
+                if (use[i]) {
+                    const long long n = (long long)jy * ch.pitch + jx;
+#pragma unroll
+                    for (int q = 0; q < 9; ++q)
+                        v[i][q] = PopIO<S, R>::ld(f + ch.f_off + q * ch.plane + n, q);
                 }
             }
-            mom[(size_t)slot * TILE_CELLS + r * TILE_W + lane] = q;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                typename Mom4<R>::T q;
+                q.x = 0; q.y = 0; q.z = 0; q.w = 0;
+                if (use[i]) {   // cell_rho_j's moments, in its precision
+                    R r, a, b;
+                    lattice_moments(v[i], r, a, b);
+                    q.x = (R)(double)r;
+                    q.y = (R)(double)a;
+                    q.z = (R)(double)b;
+                }
+                mom[(size_t)slot * TILE_CELLS + (rb + i) * TILE_W + lane] = q;
+            }
         }
     }
 }
