@@ -225,6 +225,12 @@ int sfg_synchronize(sfg_context* ctx, unsigned* status_out);
 /* ---- state transfer (synchronous) ---------------------------------------- */
 int sfg_get_populations(sfg_context* ctx, int channel, double* f);
 int sfg_set_populations(sfg_context* ctx, int channel, const double* f);
+/* Every channel's populations in one call: f holds the channels' [9][ny][nx]
+ * FP64 arrays back to back in channel order (the LatticeField::fData()
+ * layout of each, python/bindings.cpp:348-355).  The copies of channel i + 1
+ * overlap the device-side import of channel i (two staging buffers, a copy
+ * stream); synchronous on return like sfg_set_populations. */
+int sfg_set_all_populations(sfg_context* ctx, const double* f);
 /* rho, u and the lattice force of the last step (any pointer may be NULL),
  * as LatticeField::computeMacroscopic leaves them (lattice_field.cpp:28-73). */
 int sfg_get_macroscopic(sfg_context* ctx, int channel, double* rho, double* ux, double* uy,

@@ -121,6 +121,7 @@ SIGNATURES = {
     "sfg_synchronize": (C.c_int, [C.c_void_p, _P(C.c_uint)]),
     "sfg_get_populations": (C.c_int, [C.c_void_p, C.c_int, _D]),
     "sfg_set_populations": (C.c_int, [C.c_void_p, C.c_int, _D]),
+    "sfg_set_all_populations": (C.c_int, [C.c_void_p, _D]),
     "sfg_get_macroscopic": (C.c_int, [C.c_void_p, C.c_int, _D, _D, _D, _D, _D]),
     "sfg_get_markers": (C.c_int, [C.c_void_p, C.c_int, _D, _D, _D]),
     "sfg_set_markers": (C.c_int, [C.c_void_p, C.c_int, _D, _D]),

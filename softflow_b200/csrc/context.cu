@@ -275,6 +275,11 @@ struct sfg_context {
     // pipelined marker output: snapshots on the context stream, copied to
     // the host on a copy stream while later steps run
     cudaStream_t copy_stream = nullptr;
+    // sfg_set_all_populations: upload stream, two staging buffers, events
+    cudaStream_t up_stream = nullptr;
+    double* d_up[2] = {nullptr, nullptr};
+    size_t up_doubles = 0;
+    cudaEvent_t up_copied[2] = {nullptr, nullptr}, up_free[2] = {nullptr, nullptr};
     double* d_snap[2] = {nullptr, nullptr};       // [M][2] positions, then [M][2] velocities
     cudaEvent_t ev_snap[2] = {nullptr, nullptr};
     cudaEvent_t ev_copy[2] = {nullptr, nullptr};
@@ -438,6 +443,18 @@ static void free_all(sfg_context* c) {
     F(c->d_cov); F(c->d_waves); F(c->d_boxes);
     c->d_chem = nullptr; c->d_released = c->d_absorbed = c->d_Mp = c->d_gamma = nullptr;
     c->d_cov = nullptr; c->d_waves = nullptr; c->d_boxes = nullptr;
+    if (c->up_stream) {
+        cudaStreamSynchronize(c->up_stream);
+        cudaStreamDestroy(c->up_stream);
+        c->up_stream = nullptr;
+    }
+    for (int i = 0; i < 2; ++i) {
+        F(c->d_up[i]);
+        c->d_up[i] = nullptr;
+        if (c->up_copied[i]) cudaEventDestroy(c->up_copied[i]);
+        if (c->up_free[i]) cudaEventDestroy(c->up_free[i]);
+        c->up_copied[i] = c->up_free[i] = nullptr;
+    }
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     for (int i = 0; i < 2; ++i) {
         F(c->d_snap[i]);
@@ -1662,6 +1679,56 @@ extern "C" int sfg_set_populations(sfg_context* c, int chi, const double* f) {
         else launch_pop_import<__half, float>(c->d_io, c->f[i], d, c->stream);
     }
     CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(c->stream));
+    return SFG_OK;
+}
+
+extern "C" int sfg_set_all_populations(sfg_context* c, const double* f) {
+    if (!c) return fail(SFG_ERR_ARG, "sfg_set_all_populations: null context");
+    if (!c->initialized)
+        return fail(SFG_ERR_STATE, "sfg_set_all_populations: context not initialized");
+    if (!f) return fail(SFG_ERR_ARG, "sfg_set_all_populations: null input");
+    CU(cudaSetDevice(c->device));
+    const int nch = (int)c->ch.size();
+    size_t maxn = 0;
+    for (int i = 0; i < nch; ++i)
+        maxn = std::max(maxn, (size_t)9 * c->ch[i].d.nx * c->ch[i].d.ny);
+    if (!c->up_stream) {
+        CU(cudaStreamCreateWithFlags(&c->up_stream, cudaStreamNonBlocking));
+        for (int b = 0; b < 2; ++b) {
+            CU(cudaEventCreateWithFlags(&c->up_copied[b], cudaEventDisableTiming));
+            CU(cudaEventCreateWithFlags(&c->up_free[b], cudaEventDisableTiming));
+        }
+    }
+    if (c->up_doubles < maxn) {
+        for (int b = 0; b < 2; ++b) {
+            if (c->d_up[b]) cudaFree(c->d_up[b]);
+            c->d_up[b] = nullptr;
+        }
+        c->up_doubles = 0;
+        for (int b = 0; b < 2; ++b) CU(cudaMalloc(&c->d_up[b], maxn * sizeof(double)));
+        c->up_doubles = maxn;
+    }
+    size_t off = 0;
+    for (int i = 0; i < nch; ++i) {
+        const ChannelDev& d = c->ch[i].d;
+        const size_t n = 9ULL * d.nx * d.ny;
+        const int b = i & 1;
+        // the buffer's previous import (channel i - 2) must have read it
+        if (i >= 2) CU(cudaStreamWaitEvent(c->up_stream, c->up_free[b], 0));
+        CU(cudaMemcpyAsync(c->d_up[b], f + off, n * sizeof(double), cudaMemcpyHostToDevice,
+                           c->up_stream));
+        CU(cudaEventRecord(c->up_copied[b], c->up_stream));
+        CU(cudaStreamWaitEvent(c->stream, c->up_copied[b], 0));
+        for (int k = 0; k < 2; ++k) {
+            if (c->precision == SFG_FP64) launch_pop_import<double, double>(c->d_up[b], c->f[k], d, c->stream);
+            else if (c->precision == SFG_FP32) launch_pop_import<float, float>(c->d_up[b], c->f[k], d, c->stream);
+            else launch_pop_import<__half, float>(c->d_up[b], c->f[k], d, c->stream);
+        }
+        CU(cudaGetLastError());
+        CU(cudaEventRecord(c->up_free[b], c->stream));
+        off += n;
+    }
     CU(cudaStreamSynchronize(c->stream));
     return SFG_OK;
 }

@@ -234,3 +234,28 @@ def test_run_output_schedule(sfg, tmp_path):
     assert csv[0] == "timestep,time,capsule_id,type,cx,cy,vx,vy" and len(csv) == 4
     # stamped with the count before the step, as the reference stamps it
     assert _read_sfck(tmp_path / "checkpoint_20.sfck")["step"] == 20
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp16s"])
+def test_set_all_populations_equals_per_channel(sfg, precision):
+    """sfg_set_all_populations (every channel's FP64 populations back to
+    back, copies overlapped with the import) leaves the same device state as
+    one sfg_set_populations per channel."""
+    from softflow_b200 import _lib as L
+    from softflow_b200 import workloads as W
+    plans = W.plan_c3(precision, n_channels=5)
+    a = W.build(plans, precision)
+    b = W.build(W.plan_c3(precision, n_channels=5), precision)
+    a.run(3)
+    rng = np.random.default_rng(4)
+    fs = []
+    for i in range(len(plans)):
+        f = a.field(i).distributions()
+        fs.append(f + 1e-4 * rng.standard_normal(f.shape))
+    flat = np.concatenate([f.ravel() for f in fs])
+    ctx = b.context()
+    L.check(ctx._lib.sfg_set_all_populations(ctx._h, L.dptr(flat)))
+    for i, f in enumerate(fs):
+        L.check(a.context()._lib.sfg_set_populations(a.context()._h, i, L.dptr(f.ravel().copy())))
+    for i in range(len(plans)):
+        assert np.array_equal(a.field(i).distributions(), b.field(i).distributions())
