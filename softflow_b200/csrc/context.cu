@@ -656,7 +656,7 @@ static void apply_launch_config(sfg_context* c) {
     const int spr = c->spread_cps > 0 ? std::min(c->spread_cps, spr_max) : spr_max;
     c->persistent_ctas = c->nsm * lat;
     c->spread_grid = std::max(1, std::min((c->tb.max_slots + 7) / 8, c->nsm * spr));
-    c->learned_grid = c->nsm * std::max(1, std::min(c->learned_cps, 4));
+    c->learned_grid = c->nsm * std::max(1, std::min(c->learned_cps, 6));
 }
 
 extern "C" int sfg_initialize(sfg_context* c) {
@@ -1476,7 +1476,7 @@ extern "C" int sfg_autotune(sfg_context* c, int steps_per_trial, int* steps_run)
     if (c->M > 0) {
         knobs.push_back({&c->spread_cps, spr});
         knobs.push_back({&c->tb.marker_block, {64, 128, 256}});
-        if (c->any_learned) knobs.push_back({&c->learned_cps, {1, 2, 4}});
+        if (c->any_learned) knobs.push_back({&c->learned_cps, {1, 2, 4, 6}});
     }
     if (c->lattice_cps == 0) c->lattice_cps = lat_max;
     if (c->spread_cps == 0) c->spread_cps = spr_max;
@@ -1516,7 +1516,7 @@ extern "C" int sfg_get_launch_config(sfg_context* c, int* lattice_cps, int* spre
     if (lattice_cps) *lattice_cps = c->lattice_cps > 0 ? std::min(c->lattice_cps, lat_max) : lat_max;
     if (spread_cps) *spread_cps = c->spread_cps > 0 ? std::min(c->spread_cps, spr_max) : spr_max;
     if (marker_block) *marker_block = c->tb.marker_block;
-    if (learned_cps) *learned_cps = std::max(1, std::min(c->learned_cps, 4));
+    if (learned_cps) *learned_cps = std::max(1, std::min(c->learned_cps, 6));
     return SFG_OK;
 }
 

@@ -64,9 +64,9 @@ k_mdf_seed(const ChannelDev* __restrict__ chans, int M, MarkerBufs mb,
            const mlp::ModelDev* __restrict__ model, unsigned* __restrict__ status) {
     using namespace mlp;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    FwdSmem& s = *reinterpret_cast<FwdSmem*>(smem_raw);
+    FwdSmemLean& s = *reinterpret_cast<FwdSmemLean*>(smem_raw);
     load_model(s, model);
-    start_tiles(s, 128);
+    start_tiles(s, LEAN_TMEM_COLS);
     uint32_t phase = 0;
     const int ntiles = (M + ROWS - 1) / ROWS;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -85,11 +85,11 @@ k_mdf_seed(const ChannelDev* __restrict__ chans, int M, MarkerBufs mb,
         }
         put_input_row(s, fe, active);
         float y[2], ym[2];
-        if (!forward_tile(s, s.taddr, phase, y)) break;
+        if (!forward_tile_lean(s, s.taddr, phase, y)) break;
 #pragma unroll
         for (int k = 0; k < 4; ++k) fe[k] = -fe[k];
         put_input_row(s, fe, active);
-        if (!forward_tile(s, s.taddr, phase, ym)) break;
+        if (!forward_tile_lean(s, s.taddr, phase, ym)) break;
         if (active) {
             const double a = 0.5 * (double)((y[0] - ym[0]) * s.out_std[0]);
             const double b = 0.5 * (double)((y[1] - ym[1]) * s.out_std[1]);
@@ -99,7 +99,8 @@ k_mdf_seed(const ChannelDev* __restrict__ chans, int M, MarkerBufs mb,
             mb.dFsum[m] = d;
         }
     }
-    if (finish_tiles(s, phase, 128) && threadIdx.x == 0) atomicOr(status, ST_TENSOR_TIMEOUT);
+    if (finish_tiles(s, phase, LEAN_TMEM_COLS) && threadIdx.x == 0)
+        atomicOr(status, ST_TENSOR_TIMEOUT);
 }
 
 __global__ void k_harvest(const ChannelDev* __restrict__ chans, const CapsuleDev* __restrict__ caps,
@@ -129,7 +130,7 @@ __global__ void k_harvest(const ChannelDev* __restrict__ chans, const CapsuleDev
 
 cudaError_t prepare_mdf_learned() {
     return cudaFuncSetAttribute(k_mdf_seed, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sizeof(mlp::FwdSmem));
+                                (int)sizeof(mlp::FwdSmemLean));
 }
 
 template <typename S, typename R>
@@ -144,7 +145,7 @@ void launch_mdf_learned(const ChannelDev* chans, const CapsuleDev* caps, int M,
         tb.acc0, feat, frame);   // a learned channel's sweep-0 force is in acc0
     const int tiles = (M + mlp::ROWS - 1) / mlp::ROWS;
     const int g = tiles < grid ? tiles : grid;
-    k_mdf_seed<<<g, mlp::ROWS, sizeof(mlp::FwdSmem), st>>>(
+    k_mdf_seed<<<g, mlp::ROWS, sizeof(mlp::FwdSmemLean), st>>>(
         chans, M, mb, feat, frame, static_cast<const mlp::ModelDev*>(model), status);
 }
 

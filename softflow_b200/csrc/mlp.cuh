@@ -179,7 +179,8 @@ struct __align__(1024) FwdSmem {
 };
 
 // Copies the model (already in operand layout) into shared memory.
-__device__ __forceinline__ void load_model(FwdSmem& s, const ModelDev* __restrict__ md) {
+template <typename SM>
+__device__ __forceinline__ void load_model(SM& s, const ModelDev* __restrict__ md) {
     const int t = threadIdx.x;
     const uint4* w1 = reinterpret_cast<const uint4*>(md->W1);
     const uint4* w2 = reinterpret_cast<const uint4*>(md->W2);
@@ -203,7 +204,8 @@ __device__ __forceinline__ void load_model(FwdSmem& s, const ModelDev* __restric
 }
 
 // Writes this thread's row of X: normalised features, 1 (bias), zeros.
-__device__ __forceinline__ void put_input_row(FwdSmem& s, const float* feat, bool valid) {
+template <typename SM>
+__device__ __forceinline__ void put_input_row(SM& s, const float* feat, bool valid) {
     const int r = threadIdx.x;
 #pragma unroll
     for (int k = 0; k < K1; ++k) {
@@ -218,8 +220,8 @@ __device__ __forceinline__ void put_input_row(FwdSmem& s, const float* feat, boo
 // cores, issues the K/16 MMAs from thread 0 and waits for their commit.
 // After a timed-out wait the CTA issues nothing more (s.error, read after
 // the next barrier) and finish_tile waits once more before freeing.
-template <int K>
-__device__ __forceinline__ bool layer(FwdSmem& s, uint32_t tmem_d, const __nv_bfloat16* A,
+template <int K, typename SM>
+__device__ __forceinline__ bool layer(SM& s, uint32_t tmem_d, const __nv_bfloat16* A,
                                       const __nv_bfloat16* B, uint32_t idesc,
                                       uint32_t& phase) {
     fence_async_smem();
@@ -279,8 +281,66 @@ __device__ __forceinline__ bool forward_tile(FwdSmem& s, uint32_t tbase, uint32_
     return true;
 }
 
+// Inference-only image (the network seed): one activation buffer, reused by
+// both hidden layers (layer 2's MMAs have completed before its outputs are
+// written back), and 64 tensor-memory columns, reused by all three layers
+// (each layer's accumulator is read out before the next layer is issued).
+// About 33 KB, so six CTAs fit on an SM (four with FwdSmem).
+struct __align__(1024) FwdSmemLean {
+    __nv_bfloat16 X[ROWS * K1];     // 4 KB
+    __nv_bfloat16 W1[N_H * K1];     // 2 KB
+    __nv_bfloat16 W3[N3 * N_H];     // 2 KB
+    __nv_bfloat16 W2[N_H * N_H];    // 8 KB
+    __nv_bfloat16 H1[ROWS * N_H];   // 16 KB
+    float b2[N_H], b3[N_OUT];
+    float in_mean[N_IN], in_inv_std[N_IN], out_mean[N_OUT], out_std[N_OUT];
+    uint64_t bar;
+    uint32_t taddr;
+    int error;
+};
+constexpr uint32_t LEAN_TMEM_COLS = 64;
+
+// forward_tile on FwdSmemLean (same arithmetic, same outputs).
+__device__ __forceinline__ bool forward_tile_lean(FwdSmemLean& s, uint32_t tbase,
+                                                  uint32_t& phase, float* y) {
+    const int r = threadIdx.x;
+    if (!layer<K1>(s, tbase, s.X, s.W1, idesc_bf16(ROWS, N_H), phase)) return false;
+    {
+        float v[16];
+#pragma unroll
+        for (int c = 0; c < N_H; c += 16) {
+            tmem_ld16(tmem_row(tbase, c), v);
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                s.H1[kmaj(r, c + i, N_H)] = __float2bfloat16_rn(fmaxf(v[i], 0.0f));
+        }
+    }
+    if (!layer<N_H>(s, tbase, s.H1, s.W2, idesc_bf16(ROWS, N_H), phase)) return false;
+    {
+        // layer 2's MMAs have completed (their commit was waited for), so
+        // its operand H1 can take its output; each thread rewrites its row
+        float v[16];
+#pragma unroll
+        for (int c = 0; c < N_H; c += 16) {
+            tmem_ld16(tmem_row(tbase, c), v);
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                s.H1[kmaj(r, c + i, N_H)] = __float2bfloat16_rn(fmaxf(v[i] + s.b2[c + i], 0.0f));
+        }
+    }
+    if (!layer<N_H>(s, tbase, s.H1, s.W3, idesc_bf16(ROWS, N3), phase)) return false;
+    {
+        float v[16];
+        tmem_ld16(tmem_row(tbase, 0), v);
+        y[0] = v[0] + s.b3[0];
+        y[1] = v[1] + s.b3[1];
+    }
+    return true;
+}
+
 // Start of a kernel: barrier init and the tensor-memory allocation (warp 0).
-__device__ __forceinline__ void start_tiles(FwdSmem& s, uint32_t ncols) {
+template <typename SM>
+__device__ __forceinline__ void start_tiles(SM& s, uint32_t ncols) {
     if (threadIdx.x == 0) {
         s.error = 0;
         mbar_init(&s.bar, 1);
@@ -294,7 +354,8 @@ __device__ __forceinline__ void start_tiles(FwdSmem& s, uint32_t ncols) {
 
 // End of a kernel: after a timed-out wait, one more bounded wait for the
 // MMAs in flight; then warp 0 frees the tensor memory.  Returns the error.
-__device__ __forceinline__ int finish_tiles(FwdSmem& s, uint32_t phase, uint32_t ncols) {
+template <typename SM>
+__device__ __forceinline__ int finish_tiles(SM& s, uint32_t phase, uint32_t ncols) {
     tc_fence_before();
     __syncthreads();
     const int err = s.error;
