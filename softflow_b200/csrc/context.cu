@@ -264,13 +264,6 @@ struct sfg_context {
     // independent launch groups at the start of a step (contact cell list,
     // force tiles + tile moments) run on side streams, joined by events
     cudaStream_t side[2] = {nullptr, nullptr};
-    // Step-graph capture: the learned form's fallback sweeps go into a
-    // conditional node whose body runs only when k_plain_needed sets it
-    // (captured on cond_stream); cond_ok turns the form off if the driver
-    // refuses it.
-    bool capturing = false;
-    bool cond_ok = true;
-    cudaStream_t cond_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_contact = nullptr, ev_tiles = nullptr, ev_mom = nullptr;
     // pipelined marker output: snapshots on the context stream, copied to
     // the host on a copy stream while later steps run
@@ -466,11 +459,6 @@ static void free_all(sfg_context* c) {
     }
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     c->copy_stream = nullptr;
-    if (c->cond_stream) {
-        cudaStreamSynchronize(c->cond_stream);
-        cudaStreamDestroy(c->cond_stream);
-        c->cond_stream = nullptr;
-    }
     for (int i = 0; i < 2; ++i) {
         if (c->side[i]) {
             cudaStreamSynchronize(c->side[i]);
@@ -1125,7 +1113,6 @@ extern "C" int sfg_initialize(sfg_context* c) {
     CU(cudaStreamSynchronize(c->stream));
     if (c->M > 0 && !c->side[0]) {
         for (int i = 0; i < 2; ++i) CU(cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking));
-        CU(cudaStreamCreateWithFlags(&c->cond_stream, cudaStreamNonBlocking));
         for (cudaEvent_t* e : {&c->ev_fork, &c->ev_contact, &c->ev_tiles, &c->ev_mom})
             CU(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     }
@@ -1213,8 +1200,6 @@ static int enqueue_step_t(sfg_context* c, int p) {
                 launches += 1;
             }
         }
-        cudaGraphConditionalHandle fb_handle = 0;
-        bool fb_cond = false;
         if (c->any_learned) {
             // seed, one plain sweep, gate; the plain sweeps below run only for
             // channels above the threshold
@@ -1227,60 +1212,19 @@ static int enqueue_step_t(sfg_context* c, int p) {
             mark(c, SFG_PHASE_IBM_SPREAD);
             launch_mdf_interp<S, R>(c->d_chans, c->M, c->mb, fp, c->tb, p, 2, MDF_LEARNED, st);
             mark(c, SFG_PHASE_MDF_INTERP);
-            if (c->capturing && c->cond_ok && c->cond_stream && c->Kmax > 1) {
-                cudaStreamCaptureStatus cs;
-                cudaGraph_t cg = nullptr;
-                const cudaGraphNode_t* deps = nullptr;
-                size_t nd = 0;
-                if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &nd) == cudaSuccess &&
-                    cs == cudaStreamCaptureStatusActive &&
-                    cudaGraphConditionalHandleCreate(&fb_handle, cg, 0,
-                                                     cudaGraphCondAssignDefault) == cudaSuccess)
-                    fb_cond = true;
-            }
-            launch_plain_needed(c->d_chans, nch, c->tb, fb_handle, fb_cond, st);
+            launch_plain_needed(c->d_chans, nch, c->tb, st);
             launch_spread<R>(c->d_chans, c->mb, c->tb, p, 2, MDF_LEARNED, 2, c->spread_grid,
                              c->d_status, st);
             mark(c, SFG_PHASE_IBM_SPREAD);
             launches += 6;
         }
-        if (fb_cond) {
-            // the fallback sweeps as the body of an IF node: skipped unless
-            // some channel's gate residual is above its threshold
-            cudaStreamCaptureStatus cs;
-            cudaGraph_t cg = nullptr;
-            const cudaGraphNode_t* deps = nullptr;
-            size_t nd = 0;
-            CU(cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &nd));
-            cudaGraphNodeParams cp = {};
-            cp.type = cudaGraphNodeTypeConditional;
-            cp.conditional.handle = fb_handle;
-            cp.conditional.type = cudaGraphCondTypeIf;
-            cp.conditional.size = 1;
-            cudaGraphNode_t cnode;
-            CU(cudaGraphAddNode(&cnode, cg, deps, nd, &cp));
-            CU(cudaStreamUpdateCaptureDependencies(st, &cnode, 1,
-                                                   cudaStreamSetCaptureDependencies));
-            CU(cudaStreamBeginCaptureToGraph(c->cond_stream, cp.conditional.phGraph_out[0],
-                                             nullptr, nullptr, 0,
-                                             cudaStreamCaptureModeThreadLocal));
-            for (int k = 1; k < c->Kmax; ++k) {
-                launch_mdf_interp<S, R>(c->d_chans, c->M, c->mb, fp, c->tb, p, k, MDF_PLAIN,
-                                        c->cond_stream);
-                launch_spread<R>(c->d_chans, c->mb, c->tb, p, k, MDF_PLAIN, 2 + k,
-                                 c->spread_grid, c->d_status, c->cond_stream);
-            }
-            cudaGraph_t body = nullptr;
-            CU(cudaStreamEndCapture(c->cond_stream, &body));
-        } else {
-            for (int k = 1; k < c->Kmax; ++k) {
-                launch_mdf_interp<S, R>(c->d_chans, c->M, c->mb, fp, c->tb, p, k, MDF_PLAIN, st);
-                mark(c, SFG_PHASE_MDF_INTERP);
-                launch_spread<R>(c->d_chans, c->mb, c->tb, p, k, MDF_PLAIN, 2 + k,
-                                 c->spread_grid, c->d_status, st);
-                mark(c, SFG_PHASE_IBM_SPREAD);
-                launches += 2;
-            }
+        for (int k = 1; k < c->Kmax; ++k) {
+            launch_mdf_interp<S, R>(c->d_chans, c->M, c->mb, fp, c->tb, p, k, MDF_PLAIN, st);
+            mark(c, SFG_PHASE_MDF_INTERP);
+            launch_spread<R>(c->d_chans, c->mb, c->tb, p, k, MDF_PLAIN, 2 + k, c->spread_grid,
+                             c->d_status, st);
+            mark(c, SFG_PHASE_IBM_SPREAD);
+            launches += 2;
         }
         if (c->harvest) {
             launch_harvest(c->d_chans, c->d_caps, c->M, c->mb, c->d_hfeat, c->d_hlab, c->d_hvalid,
@@ -1337,26 +1281,10 @@ static int build_graphs(sfg_context* c) {
     for (int p = 0; p < 2; ++p) {
         cudaGraph_t g = nullptr;
         CU(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        c->capturing = true;
-        const int rc = enqueue_step(c, p);
-        c->capturing = false;
-        const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
-        cudaError_t e = (rc == SFG_OK && ec == cudaSuccess)
-                            ? cudaGraphInstantiate(&c->gexec[p], g, 0)
-                            : (ec != cudaSuccess ? ec : cudaErrorUnknown);
-        if (g) cudaGraphDestroy(g);
-        if (e != cudaSuccess && c->cond_ok) {
-            // without the conditional node (the fallback kernels then return
-            // at once when no channel needs them)
-            cudaGetLastError();
-            c->cond_ok = false;
-            for (int q = 0; q < 2; ++q)
-                if (c->gexec[q]) {
-                    cudaGraphExecDestroy(c->gexec[q]);
-                    c->gexec[q] = nullptr;
-                }
-            return build_graphs(c);
-        }
+        enqueue_step(c, p);
+        CU(cudaStreamEndCapture(c->stream, &g));
+        cudaError_t e = cudaGraphInstantiate(&c->gexec[p], g, 0);
+        cudaGraphDestroy(g);
         if (e != cudaSuccess)
             return fail(SFG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
     }

@@ -983,8 +983,7 @@ __global__ void k_mdf_interp(const ChannelDev* __restrict__ chans, int M, Marker
 // channel that is not learned, or a learned one whose gate residual is above
 // its threshold.  One CTA; runs after the learned sweep's interpolation.
 __global__ void k_plain_needed(const ChannelDev* __restrict__ chans, int nch,
-                               const unsigned* __restrict__ resid_gate, int* __restrict__ flag,
-                               cudaGraphConditionalHandle cond, int use_cond) {
+                               const unsigned* __restrict__ resid_gate, int* __restrict__ flag) {
     __shared__ int any;
     if (threadIdx.x == 0) any = 0;
     __syncthreads();
@@ -997,17 +996,11 @@ __global__ void k_plain_needed(const ChannelDev* __restrict__ chans, int nch,
     }
     if (mine) any = 1;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        *flag = any;
-        // the step graph's IF node around the fallback sweeps
-        if (use_cond) cudaGraphSetConditional(cond, any ? 1u : 0u);
-    }
+    if (threadIdx.x == 0) *flag = any;
 }
 
-void launch_plain_needed(const ChannelDev* chans, int nch, TileBufs& tb,
-                         cudaGraphConditionalHandle cond, bool use_cond, cudaStream_t st) {
-    k_plain_needed<<<1, 256, 0, st>>>(chans, nch, tb.resid_gate, tb.plain_needed, cond,
-                                      use_cond ? 1 : 0);
+void launch_plain_needed(const ChannelDev* chans, int nch, TileBufs& tb, cudaStream_t st) {
+    k_plain_needed<<<1, 256, 0, st>>>(chans, nch, tb.resid_gate, tb.plain_needed);
 }
 
 // (rho, jx, jy) of every cell of the step's force tiles, one warp per tile

@@ -106,8 +106,7 @@ void launch_harvest(const ChannelDev* chans, const CapsuleDev* caps, int M, cons
                     float* feat, float* label, int* valid, cudaStream_t st);
 cudaError_t prepare_mdf_learned();
 // Sets tb.plain_needed from the gate residuals (learned contexts).
-void launch_plain_needed(const ChannelDev* chans, int nch, TileBufs& tb,
-                         cudaGraphConditionalHandle cond, bool use_cond, cudaStream_t st);
+void launch_plain_needed(const ChannelDev* chans, int nch, TileBufs& tb, cudaStream_t st);
 // Moments of the step's force tiles (before the first forcing sweep).
 template <typename S, typename R>
 void launch_tile_moments(const ChannelDev* chans, const S* f, TileBufs& tb, int grid,
