@@ -627,40 +627,32 @@ __device__ __forceinline__ void enc4_words(const float v[4], int q, uint32_t r, 
 __device__ __forceinline__ void store_plane4h(__half* __restrict__ row, uint32_t w0, uint32_t w1,
                                               int dx, int x, int x0, int len, int nx, bool active,
                                               int lane, int last_lane) {
+    // straight-line code: every store is a single predicated instruction
     if (dx == 0) {
         if (active) *reinterpret_cast<uint2*>(row + x) = make_uint2(w0, w1);
         return;
     }
+    const unsigned short lo0 = (unsigned short)(w0 & 0xFFFFu), hi1 = (unsigned short)(w1 >> 16);
     if (dx > 0) {
         const uint32_t prev = __shfl_up_sync(0xffffffffu, w1, 1);
-        if (!active) return;
-        const uint32_t b = __byte_perm(w0, w1, 0x5432);
-        if (lane > 0) {
-            *reinterpret_cast<uint2*>(row + x) = make_uint2(__byte_perm(prev, w0, 0x5432), b);
-        } else {
-            row[x + 1] = __ushort_as_half((unsigned short)(w0 & 0xFFFFu));
-            *reinterpret_cast<uint32_t*>(row + x + 2) = b;
-        }
-        if (lane == last_lane) {
-            int xe = x0 + len;
-            if (xe >= nx) xe -= nx;
-            row[xe] = __ushort_as_half((unsigned short)(w1 >> 16));
-        }
+        const uint32_t a = __byte_perm(prev, w0, 0x5432), b = __byte_perm(w0, w1, 0x5432);
+        int xe = x0 + len;
+        xe = xe >= nx ? xe - nx : xe;
+        const bool first = lane == 0;
+        if (active && !first) *reinterpret_cast<uint2*>(row + x) = make_uint2(a, b);
+        if (active && first) row[x + 1] = __ushort_as_half(lo0);
+        if (active && first) *reinterpret_cast<uint32_t*>(row + x + 2) = b;
+        if (active && lane == last_lane) row[xe] = __ushort_as_half(hi1);
     } else {
         const uint32_t next = __shfl_down_sync(0xffffffffu, w0, 1);
-        if (!active) return;
-        const uint32_t a = __byte_perm(w0, w1, 0x5432);
-        if (lane < last_lane) {
-            *reinterpret_cast<uint2*>(row + x) = make_uint2(a, __byte_perm(w1, next, 0x5432));
-        } else {
-            *reinterpret_cast<uint32_t*>(row + x) = a;
-            row[x + 2] = __ushort_as_half((unsigned short)(w1 >> 16));
-        }
-        if (lane == 0) {
-            int xb = x0 - 1;
-            if (xb < 0) xb += nx;
-            row[xb] = __ushort_as_half((unsigned short)(w0 & 0xFFFFu));
-        }
+        const uint32_t a = __byte_perm(w0, w1, 0x5432), b = __byte_perm(w1, next, 0x5432);
+        int xb = x0 - 1;
+        xb = xb < 0 ? xb + nx : xb;
+        const bool last = lane == last_lane;
+        if (active && !last) *reinterpret_cast<uint2*>(row + x) = make_uint2(a, b);
+        if (active && last) *reinterpret_cast<uint32_t*>(row + x) = a;
+        if (active && last) row[x + 2] = __ushort_as_half(hi1);
+        if (active && lane == 0) row[xb] = __ushort_as_half(lo0);
     }
 }
 
