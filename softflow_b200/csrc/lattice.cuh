@@ -528,8 +528,9 @@ struct Vec<__half> {
     }
 };
 
-// Storage encoding of one value (identity for FP32/FP64; for FP16-shifted the
-// scaled deviation with stochastic rounding, see PopIO<__half, float>).
+// Storage encoding of the generic 4-cell run (FP64, and the identity for the
+// FP32 deviations).  FP32-arithmetic runs use load_pairs / store_pairs
+// (FP16-shifted: enc4_words) instead.
 template <typename S, typename R>
 struct Enc {
     static __device__ __forceinline__ R dec(S s, int) { return (R)s; }
@@ -544,47 +545,6 @@ struct Enc {
     }
 };
 
-template <>
-struct Enc<__half, float> {   // working representation: deviations d = f - w
-    static __device__ __forceinline__ float dec(__half s, int) {
-        return __half2float(s) * FP16S_UNSCALE;
-    }
-    // four values, unscaled two at a time (paired multiply, same rounding)
-    static __device__ __forceinline__ void dec4(const __half s[4], int, float out[4]) {
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const F2 a = vmul(mk2(__half2float(s[2 * k]), __half2float(s[2 * k + 1])),
-                              vc<F2>(FP16S_UNSCALE));
-            out[2 * k] = a.v.x;
-            out[2 * k + 1] = a.v.y;
-        }
-    }
-    static __device__ __forceinline__ __half enc(float v, int q, uint32_t r) {
-        const uint32_t d = (r + (uint32_t)q * 0x9E3779B9u) * 1664525u + 1013904223u;
-        return f2h_stochastic(v * FP16S_SCALE, d >> 19);
-    }
-    // Four consecutive cells of direction q with the hardware's stochastic
-    // rounding (cvt.rs.f16x2.f32: the first operand goes to the high half and
-    // takes random bits 16-28, the second the low half and bits 0-12).
-    static __device__ __forceinline__ void enc4(const float v[4], int q, uint32_t r,
-                                                __half e[4]) {
-        uint32_t p[2];
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            uint32_t h = r + (uint32_t)q * 0x9E3779B9u + (uint32_t)k * 0x7F4A7C15u;
-            h ^= h >> 15;
-            h *= 0x2C1B3C6Du;
-            h ^= h >> 12;
-            const F2 sc = vmul(mk2(v[2 * k], v[2 * k + 1]), vc<F2>(FP16S_SCALE));
-            const float lo = sc.v.x, hi = sc.v.y;
-            asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(p[k]) : "f"(hi), "f"(lo), "r"(h));
-        }
-        e[0] = __ushort_as_half((unsigned short)(p[0] & 0xFFFFu));
-        e[1] = __ushort_as_half((unsigned short)(p[0] >> 16));
-        e[2] = __ushort_as_half((unsigned short)(p[1] & 0xFFFFu));
-        e[3] = __ushort_as_half((unsigned short)(p[1] >> 16));
-    }
-};
 
 // Odd 32-bit multipliers for the dither words of the paired FP16 encode,
 // one per (direction, pair): murmur3's finaliser of the index, evaluated at
