@@ -639,7 +639,7 @@ static cudaError_t dalloc(T** p, size_t n) {
 // Grid sizes from the tuned CTAs-per-SM counts (0 = the resident maximum).
 static void apply_launch_config(sfg_context* c) {
     const int lat_max = lattice_ctas_per_sm(c->precision, c->any_adr);
-    const int spr_max = spread_blocks_per_sm();
+    const int spr_max = spread_blocks_per_sm(c->precision == SFG_FP64);
     const int lat = c->lattice_cps > 0 ? std::min(c->lattice_cps, lat_max) : lat_max;
     const int spr = c->spread_cps > 0 ? std::min(c->spread_cps, spr_max) : spr_max;
     c->persistent_ctas = c->nsm * lat;
@@ -1396,7 +1396,7 @@ extern "C" int sfg_autotune(sfg_context* c, int steps_per_trial, int* steps_run)
     };
     std::vector<Knob> knobs;
     const int lat_max = lattice_ctas_per_sm(c->precision, c->any_adr);
-    const int spr_max = spread_blocks_per_sm();
+    const int spr_max = spread_blocks_per_sm(c->precision == SFG_FP64);
     std::vector<int> lat, spr;
     for (int k = 1; k <= lat_max; ++k) lat.push_back(k);
     for (int k = 1; k <= spr_max; ++k) spr.push_back(k);
@@ -1440,7 +1440,7 @@ extern "C" int sfg_get_launch_config(sfg_context* c, int* lattice_cps, int* spre
     if (!c) return fail(SFG_ERR_ARG, "sfg_get_launch_config: null context");
     // the chosen counts (the spread grid is further capped by the slot count)
     const int lat_max = lattice_ctas_per_sm(c->precision, c->any_adr);
-    const int spr_max = spread_blocks_per_sm();
+    const int spr_max = spread_blocks_per_sm(c->precision == SFG_FP64);
     if (lattice_cps) *lattice_cps = c->lattice_cps > 0 ? std::min(c->lattice_cps, lat_max) : lat_max;
     if (spread_cps) *spread_cps = c->spread_cps > 0 ? std::min(c->spread_cps, spr_max) : spr_max;
     if (marker_block) *marker_block = c->tb.marker_block;

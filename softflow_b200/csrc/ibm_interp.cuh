@@ -170,9 +170,18 @@ __device__ __forceinline__ double2 interp_u_mom(const ChannelDev& ch, const Mark
             if (in[i]) {
                 const int cell = (jy % TILE_H) * TILE_W + (jx % TILE_W);
                 q[i] = mom[(size_t)sl * TILE_CELLS + cell];
-                const double2 a = reinterpret_cast<const double2*>(acc)[(size_t)sl * TILE_CELLS + cell];
-                fx[i] = a.x;
-                fy[i] = a.y;
+                // (x, y) pairs of R: double2 in FP64 contexts, float2 otherwise
+                if constexpr (sizeof(R) == 8) {
+                    const double2 a =
+                        reinterpret_cast<const double2*>(acc)[(size_t)sl * TILE_CELLS + cell];
+                    fx[i] = a.x;
+                    fy[i] = a.y;
+                } else {
+                    const float2 a =
+                        reinterpret_cast<const float2*>(acc)[(size_t)sl * TILE_CELLS + cell];
+                    fx[i] = (double)a.x;
+                    fy[i] = (double)a.y;
+                }
             }
         }
 #pragma unroll

@@ -559,8 +559,22 @@ struct SpreadChunkNarrow {
 // Otherwise: each marker's 16 stencil contributions (f w ds, in the
 // reference's rounding order), the lanes that own a valid point of it, and
 // its stencil origin in tile coordinates.
+// (x, y) pair of the accumulation type: double2 in FP64 contexts (the
+// reference's arithmetic, bit for bit), float2 in the FP32-arithmetic modes.
+template <typename A> struct APair;
+template <> struct APair<double> {
+    using T = double2;
+    static __device__ __forceinline__ T make(double x, double y) { return make_double2(x, y); }
+};
+template <> struct APair<float> {
+    using T = float2;
+    static __device__ __forceinline__ T make(double x, double y) {
+        return make_float2((float)x, (float)y);
+    }
+};
+template <typename A>
 struct SpreadChunkWide {
-    double2 c[SPREAD_CHUNK][17];   // point k + 4 sy (padded: conflict-free staging stores)
+    typename APair<A>::T c[SPREAD_CHUNK][17];   // point k + 4 sy (padded: conflict-free)
     unsigned mask[SPREAD_CHUNK];
     int org[SPREAD_CHUNK];         // (column origin + 64) | (row origin + 64) << 8
 };
@@ -571,15 +585,17 @@ struct SpreadChunkWide {
 constexpr int ACC_W = TILE_W + 4;
 constexpr int ACC_CELLS = TILE_H * ACC_W;
 __device__ __forceinline__ int acc_at(int c) { return (c / TILE_W) * ACC_W + (c % TILE_W); }
+template <typename A>
 struct SpreadWarpSmem {
-    double ax[ACC_CELLS], ay[ACC_CELLS];
+    A ax[ACC_CELLS], ay[ACC_CELLS];
     union {
         int list[SPREAD_LCAP];                 // sweep 0: the bitonic sort of long lists
         SpreadChunkNarrow n;                   // (the sort ends before the first chunk)
-        SpreadChunkWide w;
+        SpreadChunkWide<A> w;
     } ck;
 };
-constexpr size_t SPREAD_SMEM = sizeof(SpreadWarpSmem) * SPREAD_WARPS;
+template <typename A>
+constexpr size_t spread_smem() { return sizeof(SpreadWarpSmem<A>) * SPREAD_WARPS; }
 
 // Deterministic spread into force tiles for MDF sweep `sweep`.  Sweep 0
 // spreads the membrane + contact forces (immersed_boundary.cpp:25-100);
@@ -590,6 +606,9 @@ constexpr size_t SPREAD_SMEM = sizeof(SpreadWarpSmem) * SPREAD_WARPS;
 // the reference's order.  On a channel's last sweep the warp also adds the
 // body force on FLUID cells, applies the force cap and counts capped cells
 // (simulation.cpp:540-609), writing the final tile force `fin` (type R).
+// The tile accumulates in R: FP64 contexts in double (bit for bit), the
+// FP32-arithmetic modes in float (each contribution rounded once to float,
+// the sums in float; `acc` / `acc0` then hold float pairs).
 template <typename R>
 __global__ void __launch_bounds__(SPREAD_WARPS * 32)
 k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot_info,
@@ -602,9 +621,11 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
     if (sweep > 0 && mode == MDF_PLAIN && plain_needed && !*plain_needed) return;
     extern __shared__ __align__(16) unsigned char spread_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    SpreadWarpSmem& W = reinterpret_cast<SpreadWarpSmem*>(spread_smem)[warp];
-    double* ax = W.ax;
-    double* ay = W.ay;
+    using A = R;
+    using A2 = typename APair<A>::T;
+    SpreadWarpSmem<A>& W = reinterpret_cast<SpreadWarpSmem<A>*>(spread_smem)[warp];
+    A* ax = W.ax;
+    A* ay = W.ay;
     int* sl = W.ck.list;
     const int n_slots = *n_slots_p;
     // slots are dealt to the warps in a fixed stride (list lengths are
@@ -689,12 +710,12 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
         // a learned channel's membrane-only force lives in acc0 only: the
         // seed sweep and a fallback's restart read it there.  The
         // accumulators hold (x, y) pairs per cell: [slot][TILE_CELLS] double2.
-        const double2* src = reinterpret_cast<const double2*>(
+        const A2* src = reinterpret_cast<const A2*>(
             (ch.learned && (mode == MDF_SEED || (mode == MDF_PLAIN && sweep == 1))) ? acc0 : acc);
         const size_t base2 = (size_t)slot * TILE_CELLS;
         for (int c = lane; c < TILE_CELLS; c += 32) {
-            const double2 a = sweep > 0 ? src[base2 + c] : make_double2(0.0, 0.0);
-            const double vx = a.x, vy = a.y;
+            const A2 a = sweep > 0 ? src[base2 + c] : APair<A>::make(0.0, 0.0);
+            const A vx = a.x, vy = a.y;
             ax[acc_at(c)] = vx;
             ay[acc_at(c)] = vy;
             if (last && K > 1) {
@@ -768,7 +789,7 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
                             const double w = wxk[k] * wy;
                             if (vrow && vk[k] && w > 1e-15) {
                                 W.ck.w.c[jm][k + 4 * sy] =
-                                    make_double2(rf.x * w * rds, rf.y * w * rds);
+                                    APair<A>::make(rf.x * w * rds, rf.y * w * rds);
                                 mask |= 1u << (((o + k) & 7) + 8 * (cyl & 3));
                             }
                         }
@@ -782,7 +803,7 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
                 __syncwarp();
                 fetch(c0 + SPREAD_CHUNK);   // in flight while this chunk is added
                 // this lane's point of marker j: cell index and contribution
-                auto point = [&](int j, int& c, double2& v) {
+                auto point = [&](int j, int& c, A2& v) {
                     const int org = W.ck.w.org[j];
                     const int oj = (org & 0xFF) - 64, rj = (org >> 8) - 64;
                     const int k = (la - oj) & 7, sy = (lb - rj) & 3;
@@ -797,10 +818,10 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
                     const bool h0 = (W.ck.w.mask[j] >> lane) & 1u;
                     const bool h1 = (W.ck.w.mask[j + 1] >> lane) & 1u;
                     int c0i = 0, c1i = 0;
-                    double2 v0 = make_double2(0.0, 0.0), v1 = v0;
+                    A2 v0 = APair<A>::make(0.0, 0.0), v1 = v0;
                     if (h0) point(j, c0i, v0);
                     if (h1) point(j + 1, c1i, v1);
-                    double a0x = 0.0, a0y = 0.0, a1x = 0.0, a1y = 0.0;
+                    A a0x = 0, a0y = 0, a1x = 0, a1y = 0;
                     if (h0) {
                         a0x = ax[c0i];
                         a0y = ay[c0i];
@@ -826,7 +847,7 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
                 }
                 if (j < nb && ((W.ck.w.mask[j] >> lane) & 1u)) {
                     int c;
-                    double2 v;
+                    A2 v;
                     point(j, c, v);
                     ax[c] += v.x;
                     ay[c] += v.y;
@@ -884,8 +905,8 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
                             const double ds = N.ds[j];
                             const double2 fo = N.f[j];
                             const int c = cyn * ACC_W + cl;
-                            ax[c] += fo.x * w * ds;
-                            ay[c] += fo.y * w * ds;
+                            ax[c] += (A)(fo.x * w * ds);
+                            ay[c] += (A)(fo.y * w * ds);
                         }
                     }
                 }
@@ -894,9 +915,13 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
         }
         __syncwarp();
         if (!last) {
-            double2* out = reinterpret_cast<double2*>((sweep == 0 && ch.learned) ? acc0 : acc);
-            for (int c = lane; c < TILE_CELLS; c += 32)
-                out[base2 + c] = make_double2(ax[acc_at(c)], ay[acc_at(c)]);
+            A2* out = reinterpret_cast<A2*>((sweep == 0 && ch.learned) ? acc0 : acc);
+            for (int c = lane; c < TILE_CELLS; c += 32) {
+                A2 o;
+                o.x = ax[acc_at(c)];
+                o.y = ay[acc_at(c)];
+                out[base2 + c] = o;
+            }
             __syncwarp();
             continue;
         }
@@ -906,7 +931,7 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
         const bool body = (ch.body_fx != 0.0 || ch.body_fy != 0.0);
         for (int c = lane; c < TILE_CELLS; c += 32) {
             const int jx = x0 + (c % TILE_W), jy = y0 + (c / TILE_W);
-            double vx = ax[acc_at(c)], vy = ay[acc_at(c)];
+            double vx = (double)ax[acc_at(c)], vy = (double)ay[acc_at(c)];
             if (jx < nx && jy < ny) {
                 const bool fluid = cell_kind(ch, jx, jy) == CK_FLUID;
                 if (fluid && body) {
@@ -1099,21 +1124,26 @@ size_t membrane_smem_bytes(int maxn) {
     return (size_t)MEM_WARPS * MEM_DOUBLES_PER_NODE * maxn * sizeof(double);
 }
 
-int spread_blocks_per_sm() {
+int spread_blocks_per_sm(bool fp64) {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_spread<float>, SPREAD_WARPS * 32,
-                                                      SPREAD_SMEM) != cudaSuccess || b < 1)
-        b = 1;
+    const cudaError_t e =
+        fp64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_spread<double>,
+                                                             SPREAD_WARPS * 32,
+                                                             spread_smem<double>())
+             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_spread<float>,
+                                                             SPREAD_WARPS * 32,
+                                                             spread_smem<float>());
+    if (e != cudaSuccess || b < 1) b = 1;
     return b;
 }
 
 cudaError_t prepare_spread() {
     cudaError_t e = cudaFuncSetAttribute(k_spread<double>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)SPREAD_SMEM);
+                                         (int)spread_smem<double>());
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_spread<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)SPREAD_SMEM);
+                                 (int)spread_smem<float>());
     return e;
 }
 
@@ -1417,7 +1447,7 @@ template <typename R>
 void launch_spread(const ChannelDev* chans, const MarkerBufs& mb, TileBufs& tb, int parity,
                    int sweep, int mode, int launch_idx, int grid, unsigned* status,
                    cudaStream_t st) {
-    k_spread<R><<<grid, SPREAD_WARPS * 32, SPREAD_SMEM, st>>>(
+    k_spread<R><<<grid, SPREAD_WARPS * 32, spread_smem<R>(), st>>>(
         chans, tb.slot_info, tb.n_slots, tb.spread_ctr + launch_idx, tb.list, mb,
         tb.acc, tb.acc0, static_cast<R*>(tb.gsnap), static_cast<R*>(tb.fin[parity]), sweep, mode,
         tb.resid_gate, tb.plain_needed, tb.capped, tb.fluid_touched, status);

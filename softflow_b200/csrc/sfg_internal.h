@@ -64,7 +64,7 @@ cudaError_t prepare_membrane(int maxn);
 // Opts the spread kernels into their shared-memory size (once per device).
 cudaError_t prepare_spread();
 // Resident spread CTAs per SM (after prepare_spread).
-int spread_blocks_per_sm();
+int spread_blocks_per_sm(bool fp64);
 void launch_membrane(const CapsuleDev* caps, int ncaps, const MarkerBufs& mb, int* has_prev,
                      int maxn, unsigned* status, cudaStream_t st);
 void launch_contact(const ChannelDev* chans, int M, const MarkerBufs& mb, ContactBufs& cb,
