@@ -609,8 +609,13 @@ constexpr size_t spread_smem() { return sizeof(SpreadWarpSmem<A>) * SPREAD_WARPS
 // The tile accumulates in R: FP64 contexts in double (bit for bit), the
 // FP32-arithmetic modes in float (each contribution rounded once to float,
 // the sums in float; `acc` / `acc0` then hold float pairs).
+// Resident CTAs per SM asked of the compiler: 4 for the float form (64
+// registers; its shared memory allows 6), 3 for the double form.
 template <typename R>
-__global__ void __launch_bounds__(SPREAD_WARPS * 32)
+constexpr int spread_min_ctas() { return sizeof(R) == 4 ? 4 : 3; }
+
+template <typename R>
+__global__ void __launch_bounds__(SPREAD_WARPS * 32, spread_min_ctas<R>())
 k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot_info,
          const int* __restrict__ n_slots_p, int* __restrict__ slot_ctr,
          int* __restrict__ list, MarkerBufs mb, double* __restrict__ acc,
