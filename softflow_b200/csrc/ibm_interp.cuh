@@ -3,6 +3,7 @@
 // multi-direct forcing network.  Shared by the plain forcing sweeps and the
 // learned seed so that both interpolate identically.
 #pragma once
+#include <type_traits>
 #include "markers.cuh"
 #include "lattice.cuh"
 
@@ -139,13 +140,17 @@ __device__ __forceinline__ double2 interp_u_mom(const ChannelDev& ch, const Mark
                                                const typename Mom4<R>::T* __restrict__ mom,
                                                const double* __restrict__ acc) {
     (void)tile_slot;
+    // compute type: double in FP64 contexts (the reference's arithmetic),
+    // float in the FP32-arithmetic modes (fewer registers, more resident
+    // warps for this latency-bound gather)
+    using C = typename std::conditional<sizeof(R) == 8, double, float>::type;
     const int ix0 = mb.ix0[m], iy0 = mb.iy0[m];
     const StencilSlots ss(mb, m, iy0);
     const double2* wx2 = reinterpret_cast<const double2*>(mb.wx + 4 * (size_t)m);
     const double2* wy2 = reinterpret_cast<const double2*>(mb.wy + 4 * (size_t)m);
     const double2 wxa = wx2[0], wxb = wx2[1], wya = wy2[0], wyb = wy2[1];
-    const double wxs[4] = {wxa.x, wxa.y, wxb.x, wxb.y};
-    const double wys[4] = {wya.x, wya.y, wyb.x, wyb.y};
+    const C wxs[4] = {(C)wxa.x, (C)wxa.y, (C)wxb.x, (C)wxb.y};
+    const C wys[4] = {(C)wya.x, (C)wya.y, (C)wyb.x, (C)wyb.y};
     int jxs[4];
 #pragma unroll
     for (int sx = 0; sx < 4; ++sx) {
@@ -154,15 +159,15 @@ __device__ __forceinline__ double2 interp_u_mom(const ChannelDev& ch, const Mark
         if (jx >= ch.nx) jx -= ch.nx;
         jxs[sx] = jx;
     }
-    double ux = 0.0, uy = 0.0;
+    C ux = 0, uy = 0;
 #pragma unroll
-    for (int half = 0; half < 4; ++half) {
+    for (int row = 0; row < 4; ++row) {
         typename Mom4<R>::T q[4];
-        double fx[4], fy[4];
+        C fx[4], fy[4];
         bool in[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const int sy = half, sx = i;
+            const int sy = row, sx = i;
             const int jx = jxs[sx], jy = iy0 - 1 + sy;
             in[i] = jy >= 0 && jy < ch.ny && jx >= 0 && jx < ch.nx;
             const int sl = in[i] ? ss.slot(sx, jy) : -1;
@@ -179,27 +184,27 @@ __device__ __forceinline__ double2 interp_u_mom(const ChannelDev& ch, const Mark
                 } else {
                     const float2 a =
                         reinterpret_cast<const float2*>(acc)[(size_t)sl * TILE_CELLS + cell];
-                    fx[i] = (double)a.x;
-                    fy[i] = (double)a.y;
+                    fx[i] = a.x;
+                    fy[i] = a.y;
                 }
             }
         }
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const int sy = half, sx = i;
+            const int sy = row, sx = i;
             if (!in[i]) continue;
-            const double w = wxs[sx] * wys[sy];
-            if (w > 1e-15) {
-                const double rho = (double)q[i].x;
-                double cu = 0.0, cv = 0.0;
-                if (rho > 1e-15) {
+            const C w = wxs[sx] * wys[sy];
+            if (w > (C)1e-15) {
+                const C rho = (C)q[i].x;
+                C cu = 0, cv = 0;
+                if (rho > (C)1e-15) {
                     if constexpr (sizeof(R) == 8) {
                         cu = ((double)q[i].y + 0.5 * fx[i]) / rho;
                         cv = ((double)q[i].z + 0.5 * fy[i]) / rho;
                     } else {
-                        const double inv = 1.0 / rho;
-                        cu = ((double)q[i].y + 0.5 * fx[i]) * inv;
-                        cv = ((double)q[i].z + 0.5 * fy[i]) * inv;
+                        const float inv = __frcp_rn(rho);
+                        cu = (q[i].y + 0.5f * fx[i]) * inv;
+                        cv = (q[i].z + 0.5f * fy[i]) * inv;
                     }
                 }
                 ux += cu * w;
@@ -207,7 +212,7 @@ __device__ __forceinline__ double2 interp_u_mom(const ChannelDev& ch, const Mark
             }
         }
     }
-    return make_double2(ux, uy);
+    return make_double2((double)ux, (double)uy);
 }
 
 // rho_nearest with the tile moments (the nearest node lies in the stencil).
