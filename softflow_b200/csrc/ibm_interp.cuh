@@ -53,13 +53,16 @@ __device__ __forceinline__ double2 interp_u_acc(const ChannelDev& ch, const Mark
                                                const int* __restrict__ tile_slot,
                                                const A* __restrict__ acc) {
     (void)tile_slot;
+    // compute type: double in FP64 contexts (the reference's arithmetic),
+    // float in the FP32-arithmetic modes
+    using C = typename std::conditional<sizeof(R) == 8, double, float>::type;
     const int ix0 = mb.ix0[m], iy0 = mb.iy0[m];
     const StencilSlots ss(mb, m, iy0);
     const double2* wx2 = reinterpret_cast<const double2*>(mb.wx + 4 * (size_t)m);
     const double2* wy2 = reinterpret_cast<const double2*>(mb.wy + 4 * (size_t)m);
     const double2 wxa = wx2[0], wxb = wx2[1], wya = wy2[0], wyb = wy2[1];
-    const double wxs[4] = {wxa.x, wxa.y, wxb.x, wxb.y};
-    const double wys[4] = {wya.x, wya.y, wyb.x, wyb.y};
+    const C wxs[4] = {(C)wxa.x, (C)wxa.y, (C)wxb.x, (C)wxb.y};
+    const C wys[4] = {(C)wya.x, (C)wya.y, (C)wyb.x, (C)wyb.y};
     int jxs[4];
 #pragma unroll
     for (int sx = 0; sx < 4; ++sx) {
@@ -68,7 +71,7 @@ __device__ __forceinline__ double2 interp_u_acc(const ChannelDev& ch, const Mark
         if (jx >= ch.nx) jx -= ch.nx;
         jxs[sx] = jx;
     }
-    double ux = 0.0, uy = 0.0;
+    C ux = 0, uy = 0;
     // one stencil row at a time: the populations and forces of its four
     // cells are loaded together, then its terms are added in order
 #pragma unroll
@@ -96,27 +99,33 @@ __device__ __forceinline__ double2 interp_u_acc(const ChannelDev& ch, const Mark
 #pragma unroll
         for (int sx = 0; sx < 4; ++sx) {
             if (!in[sx]) continue;
-            const double w = wxs[sx] * wys[sy];
-            if (w > 1e-15) {
-                double rho = 0.0, jxm = 0.0, jym = 0.0;
+            const C w = wxs[sx] * wys[sy];
+            if (w > (C)1e-15) {
+                C rho = 0, jxm = 0, jym = 0;
                 if (!solid[sx]) {
                     R r, a, b;
                     lattice_moments(v[sx], r, a, b);
-                    rho = (double)r;
-                    jxm = (double)a;
-                    jym = (double)b;
+                    rho = (C)r;
+                    jxm = (C)a;
+                    jym = (C)b;
                 }
-                double cu = 0.0, cv = 0.0;
-                if (!solid[sx] && rho > 1e-15) {
-                    cu = (jxm + 0.5 * (double)fx[sx]) / rho;
-                    cv = (jym + 0.5 * (double)fy[sx]) / rho;
+                C cu = 0, cv = 0;
+                if (!solid[sx] && rho > (C)1e-15) {
+                    if constexpr (sizeof(R) == 8) {
+                        cu = (jxm + 0.5 * (double)fx[sx]) / rho;
+                        cv = (jym + 0.5 * (double)fy[sx]) / rho;
+                    } else {
+                        const float inv = __frcp_rn(rho);
+                        cu = (jxm + 0.5f * (float)fx[sx]) * inv;
+                        cv = (jym + 0.5f * (float)fy[sx]) * inv;
+                    }
                 }
                 ux += cu * w;
                 uy += cv * w;
             }
         }
     }
-    return make_double2(ux, uy);
+    return make_double2((double)ux, (double)uy);
 }
 
 // Moments (rho, jx, jy) of a force tile's cells, computed once per step
