@@ -793,8 +793,15 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
                         for (int k = 0; k < 4; ++k) {
                             const double w = wxk[k] * wy;
                             if (vrow && vk[k] && w > 1e-15) {
-                                W.ck.w.c[jm][k + 4 * sy] =
-                                    APair<A>::make(rf.x * w * rds, rf.y * w * rds);
+                                // FP64: (f w) ds in the reference's order; the
+                                // float form rounds f, w, ds once and works in float
+                                if constexpr (sizeof(A) == 8)
+                                    W.ck.w.c[jm][k + 4 * sy] =
+                                        APair<A>::make(rf.x * w * rds, rf.y * w * rds);
+                                else
+                                    W.ck.w.c[jm][k + 4 * sy] = make_float2(
+                                        (float)rf.x * (float)w * (float)rds,
+                                        (float)rf.y * (float)w * (float)rds);
                                 mask |= 1u << (((o + k) & 7) + 8 * (cyl & 3));
                             }
                         }
