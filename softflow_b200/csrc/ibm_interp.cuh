@@ -304,4 +304,18 @@ __device__ __forceinline__ void atomic_max_resid(unsigned* slot, double r) {
     atomicMax(slot, isnan(rf) ? 0x7fc00000u : __float_as_uint(rf));
 }
 
+// atomic_max_resid for the active lanes of a warp (each calls it once, `on`
+// lanes carry a residual; lanes that left the kernel take no part): lanes of
+// one channel are reduced first and one lane per channel updates the slot (the max of non-negative floats is the max of their bit
+// patterns, NaN mapped above every finite value as in atomic_max_resid).
+__device__ __forceinline__ void warp_max_resid(unsigned* slots, int chan, bool on, double r) {
+    const float rf = (float)r;
+    const unsigned v = on ? (isnan(rf) ? 0x7fc00000u : __float_as_uint(rf)) : 0u;
+    const unsigned key = on ? (unsigned)chan : 0xffffffffu;
+    const unsigned peers = __match_any_sync(__activemask(), key);
+    const unsigned m = __reduce_max_sync(peers, v);   // over the lanes of one key
+    const int leader = __ffs(peers) - 1;
+    if (on && (threadIdx.x & 31) == leader) atomicMax(&slots[chan], m);
+}
+
 }  // namespace sfg

@@ -1010,10 +1010,10 @@ __global__ void k_mdf_interp(const ChannelDev* __restrict__ chans, int M, Marker
         const double2 s0 = mb.dFsum[m];
         mb.dFsum[m] = make_double2(s0.x + d.x, s0.y + d.y);
     }
-    if (mode == MDF_LEARNED)
-        atomic_max_resid(&resid_gate[chan], sqrt(dux * dux + duy * duy));
-    else if (sweep == ch.ibm_iterations - 1)
-        atomic_max_resid(&resid_plain[chan], sqrt(dux * dux + duy * duy));
+    // the per-channel residual max, one atomic per channel and warp
+    const bool want = mode == MDF_LEARNED || sweep == ch.ibm_iterations - 1;
+    warp_max_resid(mode == MDF_LEARNED ? resid_gate : resid_plain, chan, want,
+                   sqrt(dux * dux + duy * duy));
 }
 
 // Whether any channel needs the plain correction sweeps this step: a forcing
