@@ -462,9 +462,14 @@ __global__ void k_ibm_prep(const ChannelDev* __restrict__ chans,
     }
     int t[8];
     const int nt = stencil_tiles(ch, ix0, iy0, t);
-    for (int a = 0; a < nt; ++a) {
-        tile_flag[t[a]] = 1;
-        atomicAdd(&tile_cnt[t[a]], 1);
+    // consecutive markers share tiles: one atomic per distinct tile and warp
+    for (int a = 0; a < 8; ++a) {
+        const int key = a < nt ? t[a] : -1;
+        const unsigned peers = __match_any_sync(__activemask(), key);
+        if (key >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) {
+            tile_flag[key] = 1;
+            atomicAdd(&tile_cnt[key], __popc(peers));
+        }
     }
 }
 
@@ -509,7 +514,18 @@ __global__ void k_tile_fill(const ChannelDev* __restrict__ chans, int M, MarkerB
     const int ix0 = mb.ix0[m], iy0 = mb.iy0[m];
     int t[8];
     const int nt = stencil_tiles(ch, ix0, iy0, t);
-    for (int a = 0; a < nt; ++a) list[list_off[t[a]] + atomicAdd(&cursor[t[a]], 1)] = m;
+    // one atomic per distinct tile and warp; the lanes of a tile take
+    // consecutive list entries (the order is restored by the sweep-0 sort)
+    const int lane = threadIdx.x & 31;
+    for (int a = 0; a < 8; ++a) {
+        const int key = a < nt ? t[a] : -1;
+        const unsigned peers = __match_any_sync(__activemask(), key);
+        const int leader = __ffs(peers) - 1;
+        int base = 0;
+        if (key >= 0 && lane == leader) base = atomicAdd(&cursor[key], __popc(peers));
+        base = __shfl_sync(peers, base, leader);
+        if (key >= 0) list[list_off[key] + base + __popc(peers & ((1u << lane) - 1u))] = m;
+    }
     // the slot of every stencil cell, by row tile and stencil column, for the
     // interpolations of the step (one 32-byte record instead of 16 lookups)
     int s8[8];
