@@ -34,6 +34,8 @@ def test_bad_arguments_are_rejected(sfg):
     assert lib.sfg_create(0, 7, C.byref(ctx)) == 1          # SFG_ERR_ARG: unknown precision
     assert b"precision" in lib.sfg_last_error()
     assert lib.sfg_step(None, 1) == 1
+    assert lib.sfg_set_all_populations(None, None) == 1
+    assert b"null context" in lib.sfg_last_error()
 
 
 @pytest.mark.parametrize("model,helfrich,r,n", [(O.SKALAK, 0, 3.0, 24), (O.WLC, 1, 6.0, 48),
@@ -59,6 +61,29 @@ def test_seeded_placement_matches_reference(sfg, oracle_mod):
         add_case_capsules(e, 0, case)
         pos = np.concatenate([c.pos for c in e._chans[0].caps]).reshape(-1, 2)
         assert np.array_equal(pos, build_oracle(case).positions())
+
+
+def test_seeded_placement_among_pillars_matches_reference(sfg, oracle_mod):
+    """Random placement with a channel builder rejects candidates within
+    r + gap of a pillar (simulation.cpp:256-261): the placed capsules are the
+    oracle's (itself checked against the reference in test_oracle_golden)."""
+    import softflow_b200 as S
+    from cases import CASES, add_case_capsules, build_oracle, gpu_params
+    case = CASES["pillars_capsules"]
+    sp = case["spec"]
+    e = S.Ensemble("fp32")
+    e.add_channel(gpu_params(case, "fp32"))
+    b = S.ChannelBuilder(sp["nx"], sp["ny"])
+    for ob in case["pillars"]:
+        if ob[0] == "circle":
+            b.addCirclePillar(*ob[1:])
+        else:
+            b.addRectPillar(*ob[1:])
+    e.setChannelBuilder(0, b)
+    add_case_capsules(e, 0, case)
+    pos = np.concatenate([c.pos for c in e._chans[0].caps]).reshape(-1, 2)
+    assert len(e._chans[0].caps) == 5
+    assert np.array_equal(pos, build_oracle(case).positions())
 
 
 def test_workload_generators_are_deterministic(sfg):
