@@ -44,12 +44,6 @@ if ROOT not in sys.path:
 
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM = 6650.0
-# DRAM bytes (read + write) per fluid cell of one lattice-kernel launch,
-# from one ncu capture of the same workload and precision (named beside each
-# figure); the bench cannot run ncu on itself, so it reports these.
-MEASURED_TRAFFIC = {
-    ("c3", "fp16s"): (504.9e6 / 12_479_984, "profiles/k_lattice_step4_c3_fp16s.md"),
-}
 
 
 def parse():
@@ -251,6 +245,69 @@ def scalar_bytes_per_cell(precision: str) -> int:
     return 144 if precision == "fp64" else 72
 
 
+def lattice_kernel_name(plans, precision):
+    """The lattice kernel instantiation a workload runs (storage, arithmetic,
+    scalar fused or not, collision model)."""
+    st = {"fp64": "double, double", "fp32": "float, float", "fp16s": "__half, float"}[precision]
+    adr = int(any(p.params.scalar.enabled for p in plans))
+    coll = sorted({int(p.params.fluid.collision_model) for p in plans})
+    return f"k_lattice_step4<{st}, {adr}, {'|'.join(map(str, coll))}>"
+
+
+def measure_form(plans, precision, steps, warmup, local, prof_steps=20):
+    """One context holding `plans`: device time of `steps` graph-launched
+    steps after `warmup`, then per-phase CUDA-event times of `prof_steps`
+    eager steps; throughput figures and the lattice kernel's roofline."""
+    from softflow_b200 import workloads as W
+    ens = W.build(plans, precision=precision, device=local)
+    ctx = ens.context()
+    cells, caps, markers, scal = W.totals(plans, ens)
+    ctx.step(warmup)
+    ctx.synchronize()
+    ctx.step(steps)
+    ctx.synchronize()
+    ms = ctx.last_step_ms()
+    ctx.set_profiling(True)
+    ctx.reset_phase_times()
+    ctx.step(prof_steps)
+    ctx.synchronize()
+    phases = ctx.phase_times()
+    ctx.set_profiling(False)
+    ens.close()
+    sec = ms / 1e3
+    lat_ms = phases["lattice"] / prof_steps
+    alg = cells * bytes_per_cell(precision) + scal * scalar_bytes_per_cell(precision)
+    peak, kind = peaks()
+    ach = alg / (lat_ms / 1e3) / 1e9 if lat_ms > 0 else 0.0
+    return {"precision": precision, "ms_per_step": ms / steps,
+            "capsule_steps_per_s": caps * steps / sec, "mlups": cells * steps / sec / 1e6,
+            "marker_updates_per_s": markers * steps / sec,
+            "fluid_cells": cells, "capsules": caps, "markers": markers,
+            "lattice": {"kernel": lattice_kernel_name(plans, precision), "ms": lat_ms,
+                        "algorithmic_bytes": alg, "achieved_gbs": ach, "peak_gbs": peak,
+                        "frac": ach / peak, "peak_source": kind},
+            "phase_ms_per_step": {k: v / prof_steps for k, v in phases.items() if v > 0}}
+
+
+def run_c2_forms(args, local):
+    """Configuration 2 beside the ensemble: its fluid alone in FP32 (the
+    plain stream-collide at 4096 x 1024), and the whole configuration
+    (2,000 capsules, the scalar) in the plain form (FP32) and in FP16-shifted
+    storage."""
+    from softflow_b200 import workloads as W
+    steps = max(args.steps, 50)
+    out = {"lattice_only_fp32": measure_form(W.plan_c2_lattice("fp32"), "fp32", steps,
+                                             args.warmup, local),
+           "coupled_fp32": measure_form(W.plan_c2("fp32"), "fp32", steps, args.warmup, local),
+           "coupled_fp16s": measure_form(W.plan_c2("fp16s"), "fp16s", steps, args.warmup,
+                                         local),
+           "steps": steps,
+           "config": "4096 x 1024 MRT tau 0.8 fx 1e-5; coupled: 1000 WLC + Helfrich "
+                     "(r 6, 48 markers) and 1000 Skalak (r 3, 24 markers) capsules, "
+                     "1 forcing sweep, scalar D 0.05"}
+    return out
+
+
 def run_product(args, world, rank, local, pg):
     import numpy as np
     import softflow_b200 as S
@@ -323,10 +380,6 @@ def run_product(args, world, rank, local, pg):
         args.precision)
     achieved = alg_bytes / (lat_ms / 1e3) / 1e9 if lat_ms > 0 else 0.0
     peak, peak_kind = peaks()
-    traffic, traffic_src = None, None
-    if (args.workload, args.precision) in MEASURED_TRAFFIC and scal == 0:
-        per_cell, traffic_src = MEASURED_TRAFFIC[(args.workload, args.precision)]
-        traffic = per_cell * cells
     total_phase = sum(phases.values()) or 1.0
 
     # e2e: host-resident initial state, per-step marker readback
@@ -348,6 +401,22 @@ def run_product(args, world, rank, local, pg):
                          "form": "same ensemble and precision, plain forcing sweeps",
                          "gate_residual_median_plain": float(np.median(
                              [ensp.mdfStats(c)["resid_plain"] for c in range(nch)]))}
+        # the method's own difference: the learned and the plain forcing from
+        # the same initial state after the same number of steps
+        ensl = W.build(plans, precision=args.precision, device=local)
+        ensl.setLearnedMDF(net, threshold=args.mdf_threshold)
+        ensl.run(args.warmup + args.steps)
+        num = den = 0.0
+        for c, pl in enumerate(plans):
+            rows = slice(1, pl.params.ny - 1)
+            ul = np.stack([ensl.field(c).velocity_x()[rows], ensl.field(c).velocity_y()[rows]])
+            up = np.stack([ensp.field(c).velocity_x()[rows], ensp.field(c).velocity_y()[rows]])
+            num += float(np.sum((ul - up) ** 2))
+            den += float(np.sum(up ** 2))
+        learn_info["learned_vs_plain_velocity_rel_l2"] = math.sqrt(num / den)
+        learn_info["learned_vs_plain_steps"] = args.warmup + args.steps
+        learn_info["gate_residual_median_plain"] = batched_plain["gate_residual_median_plain"]
+        ensl.close()
         ensp.close()
         ens = None
 
@@ -355,6 +424,9 @@ def run_product(args, world, rank, local, pg):
     plain = None
     if args.workload == "c3" and not args.no_plain:
         plain = run_plain(args, plans, local)
+    c2_forms = None
+    if args.workload == "c3" and not args.no_plain and world == 1:
+        c2_forms = run_c2_forms(args, local)
 
     out = {
         "metric": "capsule-steps/s",
@@ -384,12 +456,14 @@ def run_product(args, world, rank, local, pg):
         "marker_updates_per_s": mk_upd,
         "gpu_launches": launches * args.steps,
         "phase_ms_per_step": {k: v / prof_steps for k, v in phases.items()},
-        "roofline": {"kernel": "k_lattice_step", "bound": "hbm", "achieved": achieved,
+        "roofline": {"kernel": lattice_kernel_name(plans, args.precision), "bound": "hbm",
+                     "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind,
                      "share_of_step": phases["lattice"] / total_phase,
                      "algorithmic_bytes_per_launch": alg_bytes,
-                     "traffic": traffic, "traffic_source": traffic_src},
+                     # DRAM bytes need a profiler; the bench does not run one
+                     "traffic": None},
         "e2e": e2e,
         "clocks": clk,
     }
@@ -397,6 +471,8 @@ def run_product(args, world, rank, local, pg):
         out["learned_mdf"] = learn_info
     if batched_plain is not None:
         out["batched_plain"] = batched_plain
+    if c2_forms is not None:
+        out["c2"] = c2_forms
     if plain is not None:
         out["plain"] = plain
         out["batched_vs_plain"] = cap_steps / world / plain["value"] if plain["value"] else None
@@ -435,6 +511,8 @@ def run_e2e(args, plans, ens, pg, local):
     barrier(pg, local)
     t0 = time.perf_counter()
     L.check(lib.sfg_set_all_populations(ctx._h, L.dptr(pops.numpy())))
+    ctx.synchronize()
+    t_up = time.perf_counter()
     for s in range(args.steps):
         L.check(lib.sfg_step(ctx._h, 1))
         if s >= 1:
@@ -445,14 +523,19 @@ def run_e2e(args, plans, ens, pg, local):
     ctx.synchronize()
     t1 = time.perf_counter()
     sec = allmax(pg, t1 - t0)
+    up = allmax(pg, t_up - t0)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     caps = sum(len(c.caps) for c in ens._chans)
     return {"value": caps * args.steps * world / sec, "unit": "capsule-steps/s",
             "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h_step,
-            "note": "initial state uploaded from pinned host memory inside the timed region "
-                    "(sfg_set_all_populations: copies overlapped with the device-side import); "
-                    "every step's marker positions and velocities land in pinned host "
-                    "memory (copied on a second stream while the next step runs)"}
+            "upload_ms": 1e3 * up, "upload_bytes": h2d,
+            "per_step_value": caps * args.steps * world / (sec - up),
+            "per_step_ms": 1e3 * (sec - up) / args.steps,
+            "note": "value: the whole timed region, i.e. the one-off upload of the initial "
+                    "state from pinned host memory (sfg_set_all_populations, FP64 reference "
+                    "layout) followed by the steps; per_step_value: the steps alone, each "
+                    "landing its marker positions and velocities in pinned host memory "
+                    "(copied on a second stream while the next step runs)"}
 
 
 def run_plain(args, plans, local, max_channels=256, steps=None):
@@ -479,113 +562,80 @@ def run_plain(args, plans, local, max_channels=256, steps=None):
 
 
 # ------------------------------------------------------------ CPU side ----
-def oracle_spec(params):
-    import oracle as O
-    f = params.fluid
-    return O.ChannelSpec(
-        nx=params.nx, ny=params.ny, collision=int(f.collision_model), tau=f.tau, rho0=f.rho0,
-        mrt_se=f.mrt_se, mrt_s_eps=f.mrt_s_eps, mrt_sq=f.mrt_sq, body_fx=f.body_force_x,
-        body_fy=f.body_force_y, periodic_y=int(f.periodic_y),
-        max_lattice_force=params.max_lattice_force, ibm_iterations=params.ibm_iterations,
-        dt=params.dt, scalar_enabled=int(params.scalar.enabled),
-        scalar_D=params.scalar.diffusivity[0] if params.scalar.diffusivity else 0.01)
-
-
-def oracle_membrane(mp):
-    import oracle as O
-    return O.Membrane(model=int(mp.model), k_stretch=mp.k_stretch, G_s=mp.G_s,
-                      C_skalak=mp.C_skalak, wlc_L_max_ratio=mp.wlc_L_max_ratio,
-                      wlc_kBT_p=mp.wlc_kBT_p, wlc_k_pow=mp.wlc_k_pow, k_bend=mp.k_bend,
-                      use_helfrich=int(mp.use_helfrich_bending), kappa_0=mp.kappa_0,
-                      k_area=mp.k_area, k_perimeter=mp.k_perimeter,
-                      gamma_visc=mp.gamma_visc, eta_membrane=mp.eta_membrane)
-
-
-def cpu_sims(plans, impl, threads):
-    import io
-    import contextlib
-    import numpy as np
-    import oracle as O
-    sims = []
-    for pl in plans:
-        s = O.OracleSim(oracle_spec(pl.params), impl, fast=(impl == "ref"), threads=threads)
-        with contextlib.redirect_stdout(io.StringIO()):
-            for (count, x0, y0, x1, y1, r, nodes, mp, seed) in pl.placements:
-                s.add_capsule_random(count, x0, y0, x1, y1, r, r, nodes, oracle_membrane(mp),
-                                     seed=seed, min_gap=pl.min_gap, check_walls=True)
-        s.initialize()
-        if pl.gaussian is not None:
-            cx, cy, sg = pl.gaussian
-            p = pl.params
-            y, x = np.mgrid[0:p.ny, 0:p.nx]
-            s.set_concentration(np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2.0 * sg * sg)))
-        sims.append(s)
-    return sims
-
-
 def cpu_kind():
     import oracle as O
     return ("reference", "ref") if os.path.exists(O.REF_FAST_LIB) else ("port", "sfo")
 
 
-def sample_plans(workload, precision):
-    """Bounded CPU sample of the workload."""
+def cpu_sample(workload, precision):
+    """The CPU side's channels: the whole workload (for the ensemble, all 256
+    channels, the same set the GPU runs)."""
     from softflow_b200 import workloads as W
     plans = W.PLANS[workload](precision)
-    if workload == "c3":
-        return plans[:32], "first 32 of 256 channels"
-    return plans, "full workload"
+    what = f"all {len(plans)} channels" if workload == "c3" else "full workload"
+    return plans, what
 
 
-def run_cpu_baseline(workload, precision, steps=None, budget_s=20.0):
+def time_cpu(sims, steps, threads):
+    """Steps every simulation `steps` steps in one call each, one after the
+    other (the sum of per-channel runs), with `threads` OpenMP threads;
+    returns seconds."""
+    for s in sims:
+        s.set_threads(threads)
+    t0 = time.perf_counter()
+    for s in sims:
+        s.step(steps)
+    return time.perf_counter() - t0
+
+
+def run_cpu_baseline(workload, precision, budget_s=15.0):
+    """The reference's own sources (oracle/_ref, Release flags) on the GPU
+    host's cores: all threads on every channel of the workload for a bounded
+    number of steps, and one thread on the same channels for fewer."""
+    from oracle.plans import sims_from_plans
     kind, impl = cpu_kind()
     threads = (os.cpu_count() or 1) if impl == "ref" else 1
-    plans, what = sample_plans(workload, precision)
-    sims = cpu_sims(plans, impl, threads)
+    plans, what = cpu_sample(workload, precision)
+    sims = sims_from_plans(plans, impl, threads)
     caps = sum(s.num_capsules for s in sims)
-    # one step to estimate the cost, then a window of ~budget_s
-    t0 = time.perf_counter()
-    for s in sims:
-        s.step(1)
-    dt1 = max(time.perf_counter() - t0, 1e-6)
-    n = steps or max(1, min(200, int(budget_s / dt1)))
-    t0 = time.perf_counter()
-    for s in sims:
-        s.step(n)
-    sec = time.perf_counter() - t0
-    return {"value": caps * n / sec, "unit": "capsule-steps/s", "cores": threads,
-            "kind": kind, "sample": f"{what}, {n} steps each after 1 warm-up step"}
+    dt1 = max(time_cpu(sims, 1, threads), 1e-6)          # warm-up step, cost estimate
+    n = max(1, min(200, int(budget_s / dt1)))
+    sec = time_cpu(sims, n, threads)
+    out = {"value": caps * n / sec, "unit": "capsule-steps/s", "cores": threads, "kind": kind,
+           "sample": f"{what}, {n} steps per channel in one call each, after 1 warm-up step"}
+    if threads > 1:
+        n1 = max(1, min(n, int(budget_s / (dt1 * threads))))
+        sec1 = time_cpu(sims, n1, 1)
+        out["one_thread"] = {"value": caps * n1 / sec1, "unit": "capsule-steps/s", "cores": 1,
+                             "sample": f"{what}, {n1} steps per channel in one call each"}
+    return out
 
 
 def run_reference_arm(args):
     """The reference's own CPU implementation (oracle/_ref, Release flags,
-    all host threads) on the same workload and metric, one bounded sample
-    (a fixed channel subset) per step."""
+    all host threads) on the same workload, channels and metric as the
+    product arm: every channel stepped `warmup` then `steps` steps in one
+    call each, one channel after the other."""
+    from oracle.plans import sims_from_plans
     kind, impl = cpu_kind()
     threads = (os.cpu_count() or 1) if impl == "ref" else 1
-    plans, what = sample_plans(args.workload, args.precision)
-    if args.workload == "c3":
-        plans, what = plans[:8], "first 8 of 256 channels per step"
-    sims = cpu_sims(plans, impl, threads)
+    plans, what = cpu_sample(args.workload, args.precision)
+    sims = sims_from_plans(plans, impl, threads)
     caps = sum(s.num_capsules for s in sims)
-    for _ in range(args.warmup):
-        for s in sims:
-            s.step(1)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        for s in sims:
-            s.step(1)
-    sec = time.perf_counter() - t0
+    time_cpu(sims, args.warmup, threads)
+    sec = time_cpu(sims, args.steps, threads)
     v = caps * args.steps / sec
+    sample = f"{what}, {args.steps} steps per channel in one call each"
     return {
         "impl": "reference", "metric": "capsule-steps/s", "value": v, "unit": "capsule-steps/s",
         "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
         "data": "synthetic (seeded placement; no datasets)",
-        "config": {"workload": args.workload, "sample": what},
+        "config": {"workload": args.workload, "channels": len(plans), "capsules": caps,
+                   "sample": sample},
         "cpu_baseline": {"value": v, "unit": "capsule-steps/s", "cores": threads, "kind": kind,
-                         "sample": what},
+                         "sample": sample},
         "e2e": {"value": v, "unit": "capsule-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }

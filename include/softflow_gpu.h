@@ -282,7 +282,8 @@ int sfg_get_contact_counts(sfg_context* ctx, int channel, int* counts);
  *   d_offsets    [ncaps + 1] first marker of each ring, d_offsets[ncaps] = M
  *   d_pos        [M][2] marker positions      d_force  [M][2] marker forces
  *   d_Fx, d_Fy   [ny][nx] lattice force; the spread sum is added (F += sum)
- *   num_markers  M
+ *   num_markers  M; must equal d_offsets[ncaps] (markers past the last
+ *                ring are skipped, never read)
  * Deterministic: each cell sums its contributions in ascending marker order
  * (the reference's serial order) without floating-point atomics.  Scratch
  * memory is taken with cudaMallocAsync on the stream and released on it. */

@@ -143,12 +143,11 @@ class Membrane:
         return _Membrane(**{f.name: getattr(self, f.name) for f in fields(self)})
 
 
-def build(ref: bool = False) -> None:
-    """Build the C restatement (and the reference library when asked and its
-    sources are present)."""
-    targets = ["oracle"]
-    if ref:
-        targets.append("ref")
+def build(ref="auto") -> None:
+    """Build the C restatement, and the reference libraries: always when ref
+    is True, never when False, and with "auto" when the Makefile finds the
+    reference tree (REF_SRC, overridable from the environment)."""
+    targets = {True: ["oracle", "ref"], False: ["oracle"]}.get(ref, ["auto"])
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
 
 
@@ -295,6 +294,12 @@ class OracleSim:
 
     def step(self, n: int = 1):
         self._fn["step"](self._h, int(n))
+
+    def set_threads(self, n: int) -> None:
+        """OpenMP threads of the reference build (a setting of its library,
+        shared by every simulation on it); the C restatement is serial."""
+        if self.impl == "ref":
+            self._fn["set_threads"](int(n))
 
     # state views (copies) -------------------------------------------
     def _arr(self, name, n):

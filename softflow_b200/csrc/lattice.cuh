@@ -249,7 +249,7 @@ k_lattice_step(const RowItem* __restrict__ items, int n_items, const ChannelDev*
         collide_bgk(f, rho, ux, uy, cf.Fx, cf.Fy, R(ch.omega));
     }
     const Nbr b = neighbours(x, y, nx, ny, ch.periodic_y ? 1 : 0);
-    const uint32_t seed = mix32((uint32_t)(ch.cell_off + n) ^ mix32(*step_ctr + 0x51ED270Bu));
+    const uint32_t seed = mix32((uint32_t)n ^ mix32(*step_ctr + 0x51ED270Bu));
     push_cell<S, R>(dst + ch.f_off, f, x, y, n, pitch, plane, b, seed);
     if (ADR) {
         // Scalar step of the previous lattice step (it needs that step's
@@ -336,7 +336,7 @@ k_lattice_step_bc(const RowItem* __restrict__ items, int n_items,
             collide_bgk(f, rho, ux, uy, cf.Fx, cf.Fy, R(ch.omega));
         }
     }
-    const uint32_t seed = mix32((uint32_t)(ch.cell_off + n) ^ mix32(*step_ctr + 0x51ED270Bu));
+    const uint32_t seed = mix32((uint32_t)n ^ mix32(*step_ctr + 0x51ED270Bu));
     S* __restrict__ fd = dst + ch.f_off;
     const bool per_x = ch.bc_x == 1;
     const bool mw_bot = !ch.periodic_y && fabs(ch.u_bot) > 1e-15;
@@ -406,7 +406,7 @@ __global__ void k_ibb(const IbbLink* __restrict__ links, int n,
         const R fo = PopIO<S, R>::ld(fd + o * plane + L.y * pitch + L.x, o);
         v = R(inv2q) * fq + R(1.0 - inv2q) * fo;
     }
-    const uint32_t seed = mix32((uint32_t)(ch.cell_off + L.y * pitch + L.x) ^
+    const uint32_t seed = mix32((uint32_t)(L.y * pitch + L.x) ^
                                 mix32(*step_ctr + 0x6A09E667u + (uint32_t)q));
     PopIO<S, R>::st_sr(fd + o * plane + L.y * pitch + L.x, o, v, seed);
 }
@@ -427,7 +427,7 @@ __global__ void k_zou_he(const RowItem* __restrict__ rows, int n_rows,
     const int y = it.y, ny = ch.ny, plane = (int)ch.plane;
     const R base = sizeof(R) == sizeof(double) ? R(0) : R(1);
     S* __restrict__ fd = dst + ch.f_off;
-    const uint32_t seed = mix32((uint32_t)(ch.cell_off + y) ^ mix32(*step_ctr + 0x2E5BF271u));
+    const uint32_t seed = mix32((uint32_t)y ^ mix32(*step_ctr + 0x2E5BF271u));
     {   // inlet
         const int n = y * ch.pitch;
         R f0 = PopIO<S, R>::ld(fd + 0 * plane + n, 0), f2 = PopIO<S, R>::ld(fd + 2 * plane + n, 2);
@@ -974,7 +974,7 @@ __device__ __forceinline__ void lattice_run4f(const RowItem& it, const ChannelDe
     }
     {
         const Nbr b = neighbours(0, y, nx, ny, ch.periodic_y ? 1 : 0);
-        const uint32_t seed = mix32((uint32_t)(ch.cell_off + n) ^ step_mix);
+        const uint32_t seed = mix32((uint32_t)n ^ step_mix);
         S* fd = dst + ch.f_off;
 #pragma unroll
         for (int q = 0; q < 9; ++q) {
@@ -1086,7 +1086,7 @@ __device__ __forceinline__ void lattice_run4(const RowItem& it, const ChannelDev
         for (int q = 0; q < 9; ++q) f[q][i] = c[q];
     }
     const Nbr b = neighbours(0, y, nx, ny, ch.periodic_y ? 1 : 0);
-    const uint32_t seed = mix32((uint32_t)(ch.cell_off + n) ^ step_mix);
+    const uint32_t seed = mix32((uint32_t)n ^ step_mix);
     push_vec4<S, R>(dst + ch.f_off, f, x, x0, it.len, nx, y, b.ym, b.yp, b.wall_m, b.wall_p,
                     pitch, plane, active, lane, last_lane, seed);
     if (ADR) {

@@ -102,5 +102,5 @@ extern "C" int sfg_spread_forces_noalloc(int nx, int ny, int ncaps, const int* d
     if ((rc = scratch_address(&base))) return rc;
     return run_spread(nx, ny, ncaps, d_offsets, d_pos, d_force, d_Fx, d_Fy,
                       carve_spread_scratch(base, num_markers, (int)T), num_markers, (int)T,
-                      tiles_x, phi_table_host(), static_cast<cudaStream_t>(stream));
+                      tiles_x, static_cast<cudaStream_t>(stream));
 }

@@ -63,6 +63,14 @@ __global__ void k_sa_prep(int nx, int ny, int tiles_x, int ncaps, const int* __r
                           SpreadScratch sc) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
+    // num_markers must equal off[ncaps]; a marker beyond the rings (a larger
+    // count) is skipped instead of reading past the caller's arrays
+    if (m >= off[ncaps]) {
+        sc.ds[m] = 0.0;
+        sc.ix0[m] = INT_MIN;
+        sc.iy0[m] = 0;
+        return;
+    }
     const int c = ring_of(off, ncaps, m);
     const int o = off[c], n = off[c + 1] - o, k = m - o;
     const double Lx = (double)nx;
@@ -88,6 +96,29 @@ __global__ void k_sa_prep(int nx, int ny, int tiles_x, int ncaps, const int* __r
     int t[8];
     const int nt = sa_tiles(nx, ny, tiles_x, ix0, iy0, t);
     for (int i = 0; i < nt; ++i) atomicAdd(&sc.tile_cnt[t[i]], 1);
+}
+
+// Clears the per-tile counters and writes the Peskin table
+// (delta_function.h:29-37: phi on 1025 points of [0, 2]) into the scratch.
+// Every operation is exact in double except the square root, which is
+// correctly rounded on the device as in the host library, and the unit is
+// built without contraction, so the table equals the host-built one of the
+// simulation contexts bit for bit.
+__global__ void k_sa_init(int T, SpreadScratch sc) {
+    const int n = T > 1025 ? T : 1025;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (i < T) {
+            sc.tile_cnt[i] = 0;
+            sc.cursor[i] = 0;
+        }
+        if (i <= 1024) {
+            const double ar = 2.0 * static_cast<double>(i) / 1024;
+            double v = 0.0;
+            if (ar <= 1.0) v = 0.125 * (3.0 - 2.0 * ar + sqrt(1.0 + 4.0 * ar - 4.0 * ar * ar));
+            else v = 0.125 * (5.0 - 2.0 * ar - sqrt(-7.0 + 12.0 * ar - 4.0 * ar * ar));
+            sc.phi[i] = v;
+        }
+    }
 }
 
 __global__ void k_sa_fill(int nx, int ny, int tiles_x, int M, SpreadScratch sc) {
@@ -213,52 +244,38 @@ SpreadScratch carve_spread_scratch(void* base, int M, int T) {
     return sc;
 }
 
-// Enqueues the whole spread on `st` with the scratch in `sc`.  The phi table
-// region of the scratch is (re)written from the host-built table here.
+// Enqueues the whole spread on `st` with the scratch in `sc`.  Everything the
+// scratch must start with (zero counters, the Peskin table) is written by
+// k_sa_init on the stream, so the scratch may hold anything on entry.
 int run_spread(int nx, int ny, int ncaps, const int* off, const double* pos, const double* frc,
                double* Fx, double* Fy, SpreadScratch sc, int M, int T, int tiles_x,
-               const double* phi_host, cudaStream_t st) {
-    cudaMemsetAsync(sc.tile_cnt, 0, sizeof(int) * T, st);
-    cudaMemsetAsync(sc.cursor, 0, sizeof(int) * T, st);
-    cudaMemcpyAsync(sc.phi, phi_host, sizeof(double) * 1025, cudaMemcpyHostToDevice, st);
+               cudaStream_t st) {
+    int nsm = 0, dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) {
+        sfg_host::set_error(std::string("spread: ") + cudaGetErrorString(e));
+        return SFG_ERR_CUDA;
+    }
     const int B = 256, G = (M + B - 1) / B;
+    const int Gi = std::min((std::max(T, 1025) + B - 1) / B, nsm * 8);
+    k_sa_init<<<Gi, B, 0, st>>>(T, sc);
     k_sa_prep<<<G, B, 0, st>>>(nx, ny, tiles_x, ncaps, off,
                                reinterpret_cast<const double2*>(pos),
                                reinterpret_cast<const double2*>(frc), M, sc);
     scan_exclusive(sc.tile_cnt, sc.tile_off, T, sc.scan_tmp, nullptr, st);
     k_sa_fill<<<G, B, 0, st>>>(nx, ny, tiles_x, M, sc);
-    int nsm = 148, dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const int grid = std::max(1, std::min((T + SA_WARPS - 1) / SA_WARPS, nsm * 4));
     k_sa_gather<<<grid, SA_WARPS * 32, 0, st>>>(nx, ny, tiles_x, T,
                                                 reinterpret_cast<const double2*>(pos),
                                                 reinterpret_cast<const double2*>(frc), sc.phi, sc,
                                                 Fx, Fy);
-    const cudaError_t e = cudaGetLastError();
+    e = cudaGetLastError();
     if (e != cudaSuccess) {
         sfg_host::set_error(std::string("spread: ") + cudaGetErrorString(e));
         return SFG_ERR_CUDA;
     }
     return SFG_OK;
-}
-
-// Peskin table (delta_function.h:29-37), built once on the host.
-const double* phi_table_host() {
-    static double tbl[1025];
-    static bool done = false;
-    if (!done) {
-        for (int i = 0; i <= 1024; ++i) {
-            const double r = 2.0 * static_cast<double>(i) / 1024;
-            const double ar = r < 0 ? -r : r;
-            double v = 0.0;
-            if (ar <= 1.0) v = 0.125 * (3.0 - 2.0 * ar + std::sqrt(1.0 + 4.0 * ar - 4.0 * ar * ar));
-            else if (ar <= 2.0) v = 0.125 * (5.0 - 2.0 * ar - std::sqrt(-7.0 + 12.0 * ar - 4.0 * ar * ar));
-            tbl[i] = v;
-        }
-        done = true;
-    }
-    return tbl;
 }
 
 int check_spread_args(int nx, int ny, int ncaps, const int* off, const double* pos,
@@ -295,7 +312,7 @@ extern "C" int sfg_spread_forces(int nx, int ny, int ncaps, const int* d_offsets
         return SFG_ERR_CUDA;
     }
     rc = run_spread(nx, ny, ncaps, d_offsets, d_pos, d_force, d_Fx, d_Fy,
-                    carve_spread_scratch(base, M, T), M, T, tiles_x, phi_table_host(), st);
+                    carve_spread_scratch(base, M, T), M, T, tiles_x, st);
     e = cudaFreeAsync(base, st);
     if (rc == SFG_OK && e != cudaSuccess) {
         sfg_host::set_error(std::string("sfg_spread_forces: ") + cudaGetErrorString(e));

@@ -23,8 +23,7 @@ size_t spread_scratch_bytes(int M, int T);
 SpreadScratch carve_spread_scratch(void* base, int M, int T);
 int run_spread(int nx, int ny, int ncaps, const int* off, const double* pos, const double* frc,
                double* Fx, double* Fy, SpreadScratch sc, int M, int T, int tiles_x,
-               const double* phi_host, cudaStream_t st);
-const double* phi_table_host();
+               cudaStream_t st);
 int check_spread_args(int nx, int ny, int ncaps, const int* off, const double* pos,
                       const double* frc, const double* Fx, const double* Fy, const char* who);
 

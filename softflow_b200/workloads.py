@@ -104,6 +104,12 @@ def plan_c2(precision="fp32") -> List[ChannelPlan]:
                         gaussian=(2048.0, 511.5, 20.0))]
 
 
+def plan_c2_lattice(precision="fp32") -> List[ChannelPlan]:
+    """Configuration 2's fluid alone (4096 x 1024 MRT, tau 0.8, fx 1e-5, no
+    capsules, no scalar): the plain stream-collide of the roofline target."""
+    return [ChannelPlan(channel_params(4096, 1024, CollisionModel.MRT, 0.8, 1e-5, 1, precision))]
+
+
 def plan_c3(precision="fp32", n_channels=256, ibm_iterations=5) -> List[ChannelPlan]:
     rng = np.random.default_rng(7)
     plans = []
@@ -122,7 +128,8 @@ def plan_c3(precision="fp32", n_channels=256, ibm_iterations=5) -> List[ChannelP
     return plans
 
 
-PLANS = {"c0": plan_c0, "c1": plan_c1, "c2": plan_c2, "c3": plan_c3}
+PLANS = {"c0": plan_c0, "c1": plan_c1, "c2": plan_c2, "c2_lattice": plan_c2_lattice,
+         "c3": plan_c3}
 
 
 def build(plans: List[ChannelPlan], precision: str = None, device: int = 0,

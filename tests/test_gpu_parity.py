@@ -7,7 +7,7 @@ Tolerances:
            uses pow, whose device implementations differ from glibc by ulps;
            everything else is reproduced bit for bit);
   FP32  -- relative L2 of velocity <= 1e-4 after the stated steps;
-  FP16S -- relative L2 of velocity <= 5e-3;
+  FP16S -- relative L2 of velocity <= 1e-3 (the chosen form's bound);
   integer bookkeeping (capped-cell counts, contact pairs visited per marker)
   is exact.
 """
@@ -117,7 +117,8 @@ def test_fp32_velocity(sfg, oracle_mod, name, steps, tol):
         assert np.max(np.abs(sim.capsules().positions() - o.positions())) < 1e-3
 
 
-@pytest.mark.parametrize("name,steps,tol", [("c0", 2000, 5e-3), ("c1", 200, 5e-3)])
+@pytest.mark.parametrize("name,steps,tol", [("c0", 2000, 1e-3), ("c1", 2000, 1e-3),
+                                            ("mini_c2", 200, 1e-3)])
 def test_fp16s_velocity(sfg, oracle_mod, name, steps, tol):
     case = CASES[name]
     o = build_oracle(case)
@@ -127,7 +128,9 @@ def test_fp16s_velocity(sfg, oracle_mod, name, steps, tol):
     rows = fluid_rows(case)
     u = np.stack([sim.field().velocity_x()[rows], sim.field().velocity_y()[rows]])
     uo = np.stack([o.ux()[rows], o.uy()[rows]])
-    assert rel_l2(u, uo) < tol
+    e = rel_l2(u, uo)
+    print(f"{name} fp16s {steps} steps: velocity rel L2 {e:.3e}")
+    assert e < tol
 
 
 def test_scalar_fp64_bit_exact_lattice_only(sfg, oracle_mod):

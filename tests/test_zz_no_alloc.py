@@ -44,13 +44,23 @@ def _call(name, nx, ny, off, pos, frc):
     return d_Fx.cpu().numpy(), d_Fy.cpu().numpy()
 
 
+RINGS_A = [(1.5, 20.3, 5.0, 32), (40.2, 11.7, 3.0, 24), (44.9, 17.2, 3.0, 24),
+           (80.1, 30.0, 6.0, 48)]
+
+
 def test_noalloc_matches_allocating_spread_twice(sfg, oracle_mod):
+    """Calls in a row on the shared array: a first case, a smaller one, a
+    larger one, then the first case's size again with other forces right
+    after the larger call, so the tile counts and list entries the larger
+    call left in the array lie inside what the last call reads."""
     cases = [
-        (96, 48, [(1.5, 20.3, 5.0, 32), (40.2, 11.7, 3.0, 24), (44.9, 17.2, 3.0, 24),
-                  (80.1, 30.0, 6.0, 48)], 11),
+        (96, 48, RINGS_A, 11),
         (64, 32, [(30.5, 15.5, 4.0, 0), (3.0, 9.0, 3.0, 24)], 12),
+        (160, 64, [(10.5, 12.3, 6.0, 48), (60.2, 40.7, 5.0, 32), (96.0, 20.0, 4.0, 0),
+                   (130.3, 50.1, 3.0, 24), (158.9, 31.7, 5.0, 32)], 14),
+        (96, 48, RINGS_A, 13),
     ]
-    for nx, ny, rings, seed in cases:   # two calls in a row on the shared array
+    for nx, ny, rings, seed in cases:
         off, pos, frc = _inputs(nx, ny, rings, seed)
         ax, ay = _call("sfg_spread_forces", nx, ny, off, pos, frc)
         bx, by = _call("sfg_spread_forces_noalloc", nx, ny, off, pos, frc)
