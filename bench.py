@@ -262,6 +262,7 @@ def measure_form(plans, precision, steps, warmup, local, prof_steps=20):
     ens = W.build(plans, precision=precision, device=local)
     ctx = ens.context()
     cells, caps, markers, scal = W.totals(plans, ens)
+    tuned = ens.autotune(steps_per_trial=5)
     ctx.step(warmup)
     ctx.synchronize()
     ctx.step(steps)
@@ -282,7 +283,7 @@ def measure_form(plans, precision, steps, warmup, local, prof_steps=20):
     return {"precision": precision, "ms_per_step": ms / steps,
             "capsule_steps_per_s": caps * steps / sec, "mlups": cells * steps / sec / 1e6,
             "marker_updates_per_s": markers * steps / sec,
-            "fluid_cells": cells, "capsules": caps, "markers": markers,
+            "fluid_cells": cells, "capsules": caps, "markers": markers, "launch_shapes": tuned,
             "lattice": {"kernel": lattice_kernel_name(plans, precision), "ms": lat_ms,
                         "algorithmic_bytes": alg, "achieved_gbs": ach, "peak_gbs": peak,
                         "frac": ach / peak, "peak_source": kind},
@@ -576,6 +577,43 @@ def cpu_sample(workload, precision):
     return plans, what
 
 
+def host_threads() -> int:
+    """Threads this process may run at once: its CPU affinity, capped by a
+    cgroup CPU quota when one is set (cgroup v2 cpu.max or v1 cfs quota)."""
+    n = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    for quota, period in (("/sys/fs/cgroup/cpu.max", None),
+                          ("/sys/fs/cgroup/cpu/cpu.cfs_quota_us",
+                           "/sys/fs/cgroup/cpu/cpu.cfs_period_us")):
+        try:
+            if period is None:
+                q, p = open(quota).read().split()[:2]
+            else:
+                q, p = open(quota).read().strip(), open(period).read().strip()
+            if q not in ("max", "-1") and int(q) > 0:
+                n = min(n, max(1, int(q) // int(p)))
+            break
+        except Exception:
+            continue
+    return max(1, n)
+
+
+def best_threads(sims, impl):
+    """The reference build's fastest OpenMP thread count on this host: one
+    step of the first 32 channels (each in one call, one after the other) at
+    1, 2, 4, ... threads up to host_threads(), plus that count; the channels
+    are warmed up by it."""
+    top = host_threads() if impl == "ref" else 1
+    cands = sorted({1 << k for k in range(top.bit_length()) if (1 << k) <= top} | {top})
+    sample = sims[:32]
+    time_cpu(sample, 1, cands[-1])
+    best, best_t = cands[-1], None
+    for t in cands:
+        dt = time_cpu(sample, 1, t)
+        if best_t is None or dt < best_t:
+            best, best_t = t, dt
+    return best, cands
+
+
 def time_cpu(sims, steps, threads):
     """Steps every simulation `steps` steps in one call each, one after the
     other (the sum of per-channel runs), with `threads` OpenMP threads;
@@ -594,14 +632,15 @@ def run_cpu_baseline(workload, precision, budget_s=15.0):
     number of steps, and one thread on the same channels for fewer."""
     from oracle.plans import sims_from_plans
     kind, impl = cpu_kind()
-    threads = (os.cpu_count() or 1) if impl == "ref" else 1
     plans, what = cpu_sample(workload, precision)
-    sims = sims_from_plans(plans, impl, threads)
+    sims = sims_from_plans(plans, impl, 1)
     caps = sum(s.num_capsules for s in sims)
+    threads, tried = best_threads(sims, impl)
     dt1 = max(time_cpu(sims, 1, threads), 1e-6)          # warm-up step, cost estimate
     n = max(1, min(200, int(budget_s / dt1)))
     sec = time_cpu(sims, n, threads)
     out = {"value": caps * n / sec, "unit": "capsule-steps/s", "cores": threads, "kind": kind,
+           "threads_tried": tried, "host_threads": host_threads(),
            "sample": f"{what}, {n} steps per channel in one call each, after 1 warm-up step"}
     if threads > 1:
         n1 = max(1, min(n, int(budget_s / (dt1 * threads))))
@@ -618,10 +657,10 @@ def run_reference_arm(args):
     call each, one channel after the other."""
     from oracle.plans import sims_from_plans
     kind, impl = cpu_kind()
-    threads = (os.cpu_count() or 1) if impl == "ref" else 1
     plans, what = cpu_sample(args.workload, args.precision)
-    sims = sims_from_plans(plans, impl, threads)
+    sims = sims_from_plans(plans, impl, 1)
     caps = sum(s.num_capsules for s in sims)
+    threads, tried = best_threads(sims, impl)
     time_cpu(sims, args.warmup, threads)
     sec = time_cpu(sims, args.steps, threads)
     v = caps * args.steps / sec
@@ -635,6 +674,7 @@ def run_reference_arm(args):
         "config": {"workload": args.workload, "channels": len(plans), "capsules": caps,
                    "sample": sample},
         "cpu_baseline": {"value": v, "unit": "capsule-steps/s", "cores": threads, "kind": kind,
+                         "threads_tried": tried, "host_threads": host_threads(),
                          "sample": sample},
         "e2e": {"value": v, "unit": "capsule-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},

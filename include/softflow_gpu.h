@@ -491,10 +491,13 @@ enum sfg_phase {
 int sfg_set_profiling(sfg_context* ctx, int on);
 int sfg_get_phase_times(sfg_context* ctx, float* ms, int n);
 int sfg_reset_phase_times(sfg_context* ctx);
-/* Lattice kernel variant, before sfg_initialize: 0 (default) = four cells per
- * lane with vector loads and stores (used when every channel has nx % 4 == 0),
- * 1 = one cell per thread.  Results are identical; the choice exists for
- * measurements. */
+/* Lattice kernel variant, before sfg_initialize: 0 (default) = the widest
+ * vectorised form the channels allow (eight cells per lane in FP16-shifted
+ * storage without the scalar when every nx % 8 == 0; otherwise four cells per
+ * lane when every nx % 4 == 0), 1 = one cell per thread, 2 = four cells per
+ * lane.  FP64 and FP32 results are identical across variants; FP16-shifted
+ * results differ only in the stochastic rounding's random bits.  The choice
+ * exists for measurements. */
 int sfg_set_lattice_variant(sfg_context* ctx, int variant);
 /* CUDA stream of the context (cudaStream_t), for callers that interleave
  * their own work. */

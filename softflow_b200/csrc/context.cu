@@ -258,6 +258,9 @@ struct sfg_context {
     RowItem* d_items4 = nullptr;
     int n_items4 = 0;
     bool use_vec4 = false;
+    RowItem* d_items8 = nullptr;       // 256-cell runs (FP16-shifted storage)
+    int n_items8 = 0;
+    bool use_vec8 = false;
     bool any_bc = false;                // boundary-aware lattice kernel in use
     RowItem* d_zh_rows = nullptr;       // Zou-He rows (channel, y)
     int n_zh = 0;
@@ -320,6 +323,7 @@ struct sfg_context {
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     bool use_graphs = true;
     bool force_scalar_lattice = false;  // diagnostics: use the one-cell-per-thread kernel
+    bool force_vec4_lattice = false;    // diagnostics: four cells per lane in FP16S too
     // learned multi-direct forcing
     void* d_model = nullptr;            // mlp::ModelDev (the context's own copy)
     bool any_learned = false;
@@ -357,10 +361,10 @@ struct sfg_context {
 };
 
 namespace sfg {
-int lattice_ctas_per_sm(int precision, bool adr) {
-    if (precision == SFG_FP64) return lattice_ctas_per_sm_t<double, double>(adr);
-    if (precision == SFG_FP32) return lattice_ctas_per_sm_t<float, float>(adr);
-    return lattice_ctas_per_sm_t<__half, float>(adr);
+int lattice_ctas_per_sm(int precision, bool adr, bool vec8) {
+    if (precision == SFG_FP64) return lattice_ctas_per_sm_t<double, double>(adr, false);
+    if (precision == SFG_FP32) return lattice_ctas_per_sm_t<float, float>(adr, false);
+    return lattice_ctas_per_sm_t<__half, float>(adr, vec8);
 }
 }  // namespace sfg
 
@@ -408,6 +412,7 @@ static void free_all(sfg_context* c) {
     F(c->d_chans);
     F(c->d_items);
     F(c->d_items4);
+    F(c->d_items8);
     F(c->d_caps);
     F(c->d_has_prev);
     F(c->mb.pos); F(c->mb.vel); F(c->mb.frc); F(c->mb.dF); F(c->mb.ds);
@@ -638,7 +643,7 @@ static cudaError_t dalloc(T** p, size_t n) {
 // ------------------------------------------------------------------------
 // Grid sizes from the tuned CTAs-per-SM counts (0 = the resident maximum).
 static void apply_launch_config(sfg_context* c) {
-    const int lat_max = lattice_ctas_per_sm(c->precision, c->any_adr);
+    const int lat_max = lattice_ctas_per_sm(c->precision, c->any_adr && !c->any_chem, c->use_vec8);
     const int spr_max = spread_blocks_per_sm(c->precision == SFG_FP64);
     const int lat = c->lattice_cps > 0 ? std::min(c->lattice_cps, lat_max) : lat_max;
     const int spr = c->spread_cps > 0 ? std::min(c->spread_cps, spr_max) : spr_max;
@@ -655,12 +660,12 @@ extern "C" int sfg_initialize(sfg_context* c) {
     const int nch = (int)c->ch.size();
     long long cell_off = 0;
     int tile_base = 0, cell_base = 0, cap_base = 0, mk_base = 0;
-    std::vector<RowItem> items, items4, zh_rows;
+    std::vector<RowItem> items, items4, items8, zh_rows;
     std::vector<unsigned char> masks;
     std::vector<long long> mask_off;
     std::vector<IbbLink> links;
     std::vector<CapsuleDev> caps;
-    bool all_vec4 = true;
+    bool all_vec4 = true, all_vec8 = true;
     std::vector<double> pos, rest_len, rest_ang, rest_ds;
     std::vector<int> mk_cap, mk_chan, tile_chan;
     c->any_adr = false;
@@ -789,9 +794,13 @@ extern "C" int sfg_initialize(sfg_context* c) {
             for (int x0 = 0; x0 < p.nx; x0 += ITEM_CELLS)
                 items.push_back({ci, y, x0, std::min(ITEM_CELLS, p.nx - x0)});
         if (p.nx % 4 != 0) all_vec4 = false;
+        if (p.nx % 8 != 0) all_vec8 = false;
         for (int y = y0; y < y1; ++y)
             for (int x0 = 0; x0 < p.nx; x0 += VEC_RUN)
                 items4.push_back({ci, y, x0, std::min(VEC_RUN, p.nx - x0)});
+        for (int y = y0; y < y1; ++y)
+            for (int x0 = 0; x0 < p.nx; x0 += VEC8_RUN)
+                items8.push_back({ci, y, x0, std::min(VEC8_RUN, p.nx - x0)});
         h.fluid_cells = 0;
         if (!h.pillars.empty()) {
             const std::vector<unsigned char> m = pillar_mask(p, h.pillars);
@@ -907,6 +916,7 @@ extern "C" int sfg_initialize(sfg_context* c) {
     CU(dalloc(&c->d_items, items.size()));
     CU(cudaMemcpy(c->d_items, items.data(), sizeof(RowItem) * items.size(), cudaMemcpyHostToDevice));
     c->use_vec4 = all_vec4 && !c->force_scalar_lattice && !c->any_bc;
+    c->use_vec8 = c->use_vec4 && all_vec8 && c->precision == SFG_FP16S && !c->force_vec4_lattice;
     if (c->any_bc && c->any_adr)
         return fail(SFG_ERR_ARG, "sfg_initialize: the scalar cannot share a context with "
                                  "Zou-He, closed or moving-wall channels");
@@ -919,6 +929,10 @@ extern "C" int sfg_initialize(sfg_context* c) {
     c->shared_collision = c->ch[0].p.collision;
     for (const ChanHost& h : c->ch)
         if (h.p.collision != c->shared_collision) c->shared_collision = -1;
+    c->n_items8 = (int)items8.size();
+    CU(dalloc(&c->d_items8, items8.size()));
+    CU(cudaMemcpy(c->d_items8, items8.data(), sizeof(RowItem) * items8.size(),
+                  cudaMemcpyHostToDevice));
     c->n_items4 = (int)items4.size();
     CU(dalloc(&c->d_items4, items4.size()));
     CU(cudaMemcpy(c->d_items4, items4.data(), sizeof(RowItem) * items4.size(),
@@ -1237,7 +1251,7 @@ static int enqueue_step_t(sfg_context* c, int p) {
                     c->d_step_ctr, c->any_adr && !c->any_chem, c->d_items4, c->n_items4, c->use_vec4,
                     c->persistent_ctas, c->shared_collision, c->any_bc, c->d_zh_rows,
                     c->n_zh, c->d_ibb, c->ibb_level_start.data(),
-                    (int)c->ibb_level_start.size() - 1};
+                    (int)c->ibb_level_start.size() - 1, c->d_items8, c->n_items8, c->use_vec8};
     if (c->any_bc && c->n_zh > 0) launches += 1;
     if (c->any_bc && c->ibb_level_start.size() > 1) launches += (int)c->ibb_level_start.size() - 1;
     TileViewArgs tv{c->M > 0 ? c->tb.tile_slot[p] : nullptr,
@@ -1395,7 +1409,7 @@ extern "C" int sfg_autotune(sfg_context* c, int steps_per_trial, int* steps_run)
         std::vector<int> cand;
     };
     std::vector<Knob> knobs;
-    const int lat_max = lattice_ctas_per_sm(c->precision, c->any_adr);
+    const int lat_max = lattice_ctas_per_sm(c->precision, c->any_adr && !c->any_chem, c->use_vec8);
     const int spr_max = spread_blocks_per_sm(c->precision == SFG_FP64);
     std::vector<int> lat, spr;
     for (int k = 1; k <= lat_max; ++k) lat.push_back(k);
@@ -1439,7 +1453,7 @@ extern "C" int sfg_get_launch_config(sfg_context* c, int* lattice_cps, int* spre
                                      int* marker_block, int* learned_cps) {
     if (!c) return fail(SFG_ERR_ARG, "sfg_get_launch_config: null context");
     // the chosen counts (the spread grid is further capped by the slot count)
-    const int lat_max = lattice_ctas_per_sm(c->precision, c->any_adr);
+    const int lat_max = lattice_ctas_per_sm(c->precision, c->any_adr && !c->any_chem, c->use_vec8);
     const int spr_max = spread_blocks_per_sm(c->precision == SFG_FP64);
     if (lattice_cps) *lattice_cps = c->lattice_cps > 0 ? std::min(c->lattice_cps, lat_max) : lat_max;
     if (spread_cps) *spread_cps = c->spread_cps > 0 ? std::min(c->spread_cps, spr_max) : spr_max;
@@ -2110,8 +2124,10 @@ extern "C" int sfg_reset_phase_times(sfg_context* c) {
 extern "C" int sfg_set_lattice_variant(sfg_context* c, int variant) {
     if (!c) return fail(SFG_ERR_ARG, "sfg_set_lattice_variant: null context");
     if (c->initialized) return fail(SFG_ERR_STATE, "sfg_set_lattice_variant: before sfg_initialize");
-    if (variant < 0 || variant > 1) return fail(SFG_ERR_ARG, "sfg_set_lattice_variant: 0 or 1");
+    if (variant < 0 || variant > 2)
+        return fail(SFG_ERR_ARG, "sfg_set_lattice_variant: 0, 1 or 2");
     c->force_scalar_lattice = variant == 1;
+    c->force_vec4_lattice = variant == 2;
     return SFG_OK;
 }
 

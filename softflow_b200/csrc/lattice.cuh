@@ -1121,6 +1121,220 @@ __device__ __forceinline__ void lattice_run4(const RowItem& it, const ChannelDev
     }
 }
 
+// ---------------------------------------------------------------------------
+// FP16-shifted storage, eight cells per lane (256-cell runs).  Each lane
+// moves 16 bytes per plane per load and store, as the FP32 form does with
+// four cells, so the bytes in flight per instruction match FP32 while the
+// per-run work (run record, channel record, force-tile slots, neighbour
+// shuffles, loads and stores) is spread over twice the cells.  The cells
+// are processed as four register pairs: decode (binary16 pair -> FP32 pair),
+// moments, velocity, collision, stochastic encode back into the same word,
+// so the populations stay packed while the next pair is worked on.
+// ---------------------------------------------------------------------------
+constexpr int VEC8_RUN = 256;   // cells per warp work item of the 8-cell form
+
+__device__ __forceinline__ uint32_t u4_get(const uint4& v, int k) {
+    return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
+}
+__device__ __forceinline__ void u4_set(uint4& v, int k, uint32_t w) {
+    if (k == 0) v.x = w;
+    else if (k == 1) v.y = w;
+    else if (k == 2) v.z = w;
+    else v.w = w;
+}
+// binary16 pair (first cell in the low half) -> FP32 deviations
+__device__ __forceinline__ F2 dec_word(uint32_t w) {
+    F2 u;
+    u.v = __half22float2(*reinterpret_cast<const __half2*>(&w));
+    return vmul(u, vc<F2>(FP16S_UNSCALE));
+}
+// FP32 deviations -> binary16 pair, rounded stochastically with the 13-bit
+// fields of `bits` (0-12 for the low half, 16-28 for the high half)
+__device__ __forceinline__ uint32_t enc_word(F2 a, uint32_t bits) {
+    const F2 s = vmul(a, vc<F2>(FP16S_SCALE));
+    uint32_t w;
+    asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(w) : "f"(s.v.y), "f"(s.v.x), "r"(bits));
+    return w;
+}
+
+// Stores the eight encoded cells (four words) of one plane of a 256-cell
+// run: v holds cells x .. x + 7 of the lane, cell x in the low half of v.x.
+// dx is the x shift (-1, 0, +1): the shifted forms build the target's
+// aligned 16-byte block from the lane's words and one word of the
+// neighbouring lane (byte permutes); the run's first and last lanes store
+// the cells at the run's ends singly (the neighbouring runs own the rest of
+// those blocks).  All lanes of the warp must call this (shuffles).
+__device__ __forceinline__ void store_plane8h(__half* __restrict__ row, const uint4 v, int dx,
+                                              int x, int x0, int len, int nx, bool active,
+                                              int lane, int last_lane) {
+    if (dx == 0) {
+        if (active) *reinterpret_cast<uint4*>(row + x) = v;
+        return;
+    }
+    if (dx > 0) {
+        // block x .. x + 7 receives cells x - 1 .. x + 6
+        const uint32_t prev = __shfl_up_sync(0xffffffffu, v.w, 1);
+        const uint32_t a0 = __byte_perm(prev, v.x, 0x5432), a1 = __byte_perm(v.x, v.y, 0x5432),
+                       a2 = __byte_perm(v.y, v.z, 0x5432), a3 = __byte_perm(v.z, v.w, 0x5432);
+        int xe = x0 + len;
+        xe = xe >= nx ? xe - nx : xe;
+        const bool first = lane == 0;
+        if (active && !first) *reinterpret_cast<uint4*>(row + x) = make_uint4(a0, a1, a2, a3);
+        if (active && first) row[x + 1] = __ushort_as_half((unsigned short)(v.x & 0xFFFFu));
+        if (active && first) *reinterpret_cast<uint32_t*>(row + x + 2) = a1;
+        if (active && first) *reinterpret_cast<uint2*>(row + x + 4) = make_uint2(a2, a3);
+        if (active && lane == last_lane) row[xe] = __ushort_as_half((unsigned short)(v.w >> 16));
+    } else {
+        // block x .. x + 7 receives cells x + 1 .. x + 8
+        const uint32_t next = __shfl_down_sync(0xffffffffu, v.x, 1);
+        const uint32_t b0 = __byte_perm(v.x, v.y, 0x5432), b1 = __byte_perm(v.y, v.z, 0x5432),
+                       b2 = __byte_perm(v.z, v.w, 0x5432), b3 = __byte_perm(v.w, next, 0x5432);
+        int xb = x0 - 1;
+        xb = xb < 0 ? xb + nx : xb;
+        const bool last = lane == last_lane;
+        if (active && !last) *reinterpret_cast<uint4*>(row + x) = make_uint4(b0, b1, b2, b3);
+        if (active && last) *reinterpret_cast<uint2*>(row + x) = make_uint2(b0, b1);
+        if (active && last) *reinterpret_cast<uint32_t*>(row + x + 4) = b2;
+        if (active && last) row[x + 6] = __ushort_as_half((unsigned short)(v.w >> 16));
+        if (active && lane == 0) row[xb] = __ushort_as_half((unsigned short)(v.x & 0xFFFFu));
+    }
+}
+
+// Forces of cells c .. c + 3 of a run (c = rt.cell + i, i a multiple of 4),
+// one 16-byte load per component, with the rules of pair_forces for the
+// fluid step without the scalar: F (Guo force) and G (the force in the
+// collision's velocity).
+struct QuadForces {
+    float4 Fx, Fy, Gx, Gy;
+};
+__device__ __forceinline__ float4 ld4f(const float* p) {
+    return __ldg(reinterpret_cast<const float4*>(p));
+}
+__device__ __forceinline__ float4 splat4(float a) { return make_float4(a, a, a, a); }
+__device__ __forceinline__ QuadForces quad_forces(const ChannelDev& ch, const RunTiles& rt, int i,
+                                                  const TileView& tv, int stepped) {
+    QuadForces r;
+    const bool mdf = ch.ibm_iterations > 1;
+    const int c = rt.cell + i;
+    if (rt.s >= 0) {
+        const float* fin = static_cast<const float*>(tv.cur_fin) + (size_t)rt.s * 2 * TILE_CELLS;
+        r.Fx = ld4f(fin + c);
+        r.Fy = ld4f(fin + TILE_CELLS + c);
+    } else {
+        r.Fx = splat4(float(ch.F_uni_x));
+        r.Fy = splat4(float(ch.F_uni_y));
+    }
+    if (mdf) {
+        if (rt.s >= 0) {
+            const float* gs = static_cast<const float*>(tv.cur_G) + (size_t)rt.s * 2 * TILE_CELLS;
+            r.Gx = ld4f(gs + c);
+            r.Gy = ld4f(gs + TILE_CELLS + c);
+        } else {
+            r.Gx = splat4(0.f);
+            r.Gy = r.Gx;
+        }
+    } else if (rt.ps >= 0) {
+        const float* pf = static_cast<const float*>(tv.prev_fin) + (size_t)rt.ps * 2 * TILE_CELLS;
+        r.Gx = ld4f(pf + c);
+        r.Gy = ld4f(pf + TILE_CELLS + c);
+    } else {
+        r.Gx = splat4(stepped ? float(ch.F_uni_x) : 0.f);
+        r.Gy = splat4(stepped ? float(ch.F_uni_y) : 0.f);
+    }
+    return r;
+}
+__device__ __forceinline__ F2 quad_pair(const float4& v, int p) {
+    return p == 0 ? mk2(v.x, v.y) : mk2(v.z, v.w);
+}
+
+// One 256-cell run of the fluid step in FP16-shifted storage (no scalar):
+// collide + push stream + halfway bounce-back, the arithmetic of
+// lattice_run4f (paired FP32 on deviations).  The dither word of the
+// stochastic encode of pair k of plane q is the lane's seed times an odd
+// multiplier per (q, k): a bijection of the seed, so each 13-bit field is
+// uniform.
+template <int COLL>
+__device__ __forceinline__ void lattice_run8h(const RowItem& it, const ChannelDev& ch, int st,
+                                              const __half* __restrict__ src,
+                                              __half* __restrict__ dst, const TileView& tv,
+                                              uint32_t step_mix, int lane) {
+    const bool active = 8 * lane < it.len;
+    const int last_lane = (it.len >> 3) - 1;
+    const int nx = ch.nx, ny = ch.ny, pitch = ch.pitch, plane = (int)ch.plane;
+    const int x0 = it.x0, y = it.y;
+    const int x = x0 + 8 * lane;
+    const int n = y * pitch + (active ? x : x0);
+    uint4 w[9];
+    {
+        const __half* fs = src + ch.f_off + n;
+#pragma unroll
+        for (int q = 0; q < 9; ++q)
+            w[q] = active ? __ldg(reinterpret_cast<const uint4*>(fs + (size_t)q * plane))
+                          : make_uint4(0u, 0u, 0u, 0u);
+    }
+    const RunTiles rt = active ? run_tiles(ch, x, y, tv) : RunTiles{-1, -1, 0};
+    const uint32_t seed = mix32((uint32_t)n ^ step_mix);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const QuadForces qf = quad_forces(ch, rt, 4 * h, tv, st);
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+            const int k = 2 * h + p;
+            F2 d[9];
+#pragma unroll
+            for (int q = 0; q < 9; ++q) d[q] = dec_word(u4_get(w[q], k));
+            const DevMoments<F2> m = dev_moments(d);
+            const F2 r = vadd(m.drho, vc<F2>(1.f));
+            F2 ux, uy;
+            cell_velocity2(r, m.jx, m.jy, quad_pair(qf.Gx, p), quad_pair(qf.Gy, p), ux, uy);
+            collide_cell2<COLL>(d, m, r, ux, uy, quad_pair(qf.Fx, p), quad_pair(qf.Fy, p), ch);
+#pragma unroll
+            for (int q = 0; q < 9; ++q)
+                u4_set(w[q], k, enc_word(d[q], seed * dither_mult((uint32_t)(4 * q + k))));
+        }
+    }
+    const Nbr b = neighbours(0, y, nx, ny, ch.periodic_y ? 1 : 0);
+    __half* fd = dst + ch.f_off;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        const int cx = cx_of(q), cy = cy_of(q);
+        const bool wall = (cy > 0 && b.wall_p) || (cy < 0 && b.wall_m);
+        if (wall) {
+            store_plane8h(fd + opp_of(q) * plane + y * pitch, w[q], 0, x, x0, it.len, nx, active,
+                          lane, last_lane);
+        } else {
+            const int yd = cy == 0 ? y : (cy > 0 ? b.yp : b.ym);
+            store_plane8h(fd + q * plane + yd * pitch, w[q], cx, x, x0, it.len, nx, active, lane,
+                          last_lane);
+        }
+    }
+}
+
+// Persistent 8-cell form (FP16-shifted storage, no scalar): every warp walks
+// a contiguous chunk of 256-cell runs, prefetching the next run record.
+template <int COLL>
+__global__ void __launch_bounds__(256, 2)
+k_lattice_step8h(const RowItem* __restrict__ items, int n_items,
+                 const ChannelDev* __restrict__ chans, const __half* __restrict__ src,
+                 __half* __restrict__ dst, TileView tv, const int* __restrict__ stepped,
+                 const unsigned* __restrict__ step_ctr) {
+    const int lane = threadIdx.x & 31;
+    const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int chunk = (n_items + nwarps - 1) / nwarps;
+    const int i0 = gwarp * chunk;
+    const int i1 = min(n_items, i0 + chunk);
+    if (i0 >= i1) return;                      // warp-uniform
+    const uint32_t step_mix = mix32(*step_ctr + 0x51ED270Bu);
+    RowItem next = items[i0];
+    for (int item = i0; item < i1; ++item) {
+        const RowItem it = next;
+        if (item + 1 < i1) next = items[item + 1];
+        const ChannelDev& ch = chans[it.chan];
+        lattice_run8h<COLL>(it, ch, stepped[it.chan], src, dst, tv, step_mix, lane);
+    }
+}
+
 // Persistent form: every warp walks a contiguous chunk of 128-cell runs,
 // prefetching the next run descriptor, so the dependent loads of a run's
 // metadata overlap the previous run's work.

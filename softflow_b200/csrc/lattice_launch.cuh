@@ -62,6 +62,31 @@ void launch_lattice_step(const LatticeLaunch& L, const TileViewArgs& tv, cudaStr
                                                                  L.step_ctr);
         return;
     }
+    if constexpr (std::is_same<S, __half>::value && std::is_same<R, float>::value) {
+        if (L.use_vec8 && !L.any_adr) {
+            if (L.n_items8 == 0) return;
+            const int grid = std::max(1, std::min(L.persistent_ctas,
+                                                  (L.n_items8 + ITEMS_PER_CTA - 1) / ITEMS_PER_CTA));
+            const TileView v = to_view(tv);
+            const __half* src = static_cast<const __half*>(L.src);
+            __half* dst = static_cast<__half*>(L.dst);
+            switch (L.collision) {
+                case 0: k_lattice_step8h<0><<<grid, 32 * ITEMS_PER_CTA, 0, st>>>(
+                            L.items8, L.n_items8, L.chans, src, dst, v, L.stepped, L.step_ctr);
+                        break;
+                case 1: k_lattice_step8h<1><<<grid, 32 * ITEMS_PER_CTA, 0, st>>>(
+                            L.items8, L.n_items8, L.chans, src, dst, v, L.stepped, L.step_ctr);
+                        break;
+                case 2: k_lattice_step8h<2><<<grid, 32 * ITEMS_PER_CTA, 0, st>>>(
+                            L.items8, L.n_items8, L.chans, src, dst, v, L.stepped, L.step_ctr);
+                        break;
+                default: k_lattice_step8h<-1><<<grid, 32 * ITEMS_PER_CTA, 0, st>>>(
+                             L.items8, L.n_items8, L.chans, src, dst, v, L.stepped, L.step_ctr);
+                         break;
+            }
+            return;
+        }
+    }
     if (L.use_vec4) {
         if (L.n_items4 == 0) return;
         const int grid = std::max(1, std::min(L.persistent_ctas,
@@ -140,9 +165,16 @@ void launch_thermo_cells(const void* in, const void* g, const ChannelDev* chans,
 }
 
 template <typename S, typename R>
-int lattice_ctas_per_sm_t(bool adr) {
+int lattice_ctas_per_sm_t(bool adr, bool vec8) {
     // the generic-collision instance has the largest footprint
     int n = 0;
+    if constexpr (std::is_same<S, __half>::value && std::is_same<R, float>::value) {
+        if (vec8 && !adr) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_lattice_step8h<-1>,
+                                                          32 * ITEMS_PER_CTA, 0);
+            return n > 0 ? n : 1;
+        }
+    }
     if (adr)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_lattice_step4<S, R, true, -1>,
                                                       32 * ITEMS_PER_CTA, 0);
@@ -153,7 +185,7 @@ int lattice_ctas_per_sm_t(bool adr) {
 }
 
 #define SFG_LATTICE_INST(S, R)                                                                   \
-    template int lattice_ctas_per_sm_t<S, R>(bool);                                              \
+    template int lattice_ctas_per_sm_t<S, R>(bool, bool);                                            \
     template void launch_lattice_step<S, R>(const LatticeLaunch&, const TileViewArgs&,           \
                                             cudaStream_t);                                        \
     template void launch_scalar_flush<S, R>(const LatticeLaunch&, const TileViewArgs&,           \

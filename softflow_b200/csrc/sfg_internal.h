@@ -141,6 +141,9 @@ struct LatticeLaunch {
     const IbbLink* ibb = nullptr;      // interpolated bounce-back links, by level
     const int* ibb_level_start = nullptr;  // host array [n_ibb_levels + 1]
     int n_ibb_levels = 0;
+    const RowItem* items8 = nullptr;   // 256-cell runs for the 8-cell FP16-shifted kernel
+    int n_items8 = 0;
+    bool use_vec8 = false;             // FP16-shifted storage, every channel nx % 8 == 0
 };
 struct TileViewArgs {
     const int* cur_slot;
@@ -150,9 +153,9 @@ struct TileViewArgs {
     const void* prev_fin;
 };
 // Resident CTAs per SM of the persistent lattice kernel (occupancy query).
-int lattice_ctas_per_sm(int precision, bool adr);
+int lattice_ctas_per_sm(int precision, bool adr, bool vec8);
 template <typename S, typename R>
-int lattice_ctas_per_sm_t(bool adr);
+int lattice_ctas_per_sm_t(bool adr, bool vec8);
 template <typename S, typename R>
 void launch_lattice_step(const LatticeLaunch& L, const TileViewArgs& tv, cudaStream_t st);
 template <typename S, typename R>
