@@ -246,12 +246,17 @@ def scalar_bytes_per_cell(precision: str) -> int:
 
 
 def lattice_kernel_name(plans, precision):
-    """The lattice kernel instantiation a workload runs (storage, arithmetic,
-    scalar fused or not, collision model)."""
-    st = {"fp64": "double, double", "fp32": "float, float", "fp16s": "__half, float"}[precision]
+    """The lattice kernel instantiation a workload runs: the eight-cell
+    FP16-shifted kernel when the storage is FP16S, there is no scalar and
+    every nx % 8 == 0, otherwise the four-cell kernel (storage, arithmetic,
+    scalar fused or not); the template's last argument is the collision
+    model."""
     adr = int(any(p.params.scalar.enabled for p in plans))
-    coll = sorted({int(p.params.fluid.collision_model) for p in plans})
-    return f"k_lattice_step4<{st}, {adr}, {'|'.join(map(str, coll))}>"
+    coll = "|".join(map(str, sorted({int(p.params.fluid.collision_model) for p in plans})))
+    if precision == "fp16s" and not adr and all(p.params.nx % 8 == 0 for p in plans):
+        return f"k_lattice_step8h<{coll}>"
+    st = {"fp64": "double, double", "fp32": "float, float", "fp16s": "__half, float"}[precision]
+    return f"k_lattice_step4<{st}, {adr}, {coll}>"
 
 
 def measure_form(plans, precision, steps, warmup, local, prof_steps=20):

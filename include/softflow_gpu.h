@@ -346,13 +346,22 @@ int sfg_mlp_step_count(sfg_mlp* m, int* steps);
  * sweeps of ImmersedBoundary::multiDirectForcing (immersed_boundary.cpp:
  * 231-286) by the network's prediction of their summed correction (seed),
  * spread like a sweep; the last plain sweep follows.  The no-slip residual
- * max |U_prev - U_interp| over the channel's markers, taken at that sweep's
- * interpolation, gates the result: above residual_threshold (lu/step) the
- * channel redoes the plain K-1 sweeps from its membrane-force spread, so its
- * result is the plain one.  The network's current parameters are copied into
- * the context; net == NULL turns the learned form off.  The reference has no
+ * after the seed is linear in a scale a of the seed; per channel the step
+ * length a* in [0, step limit] that minimises the squared residual over the
+ * channel's markers scales the seed (see sfg_set_mdf_step_limit).  The
+ * residual max |U_prev - U_interp| over the channel's markers at that step
+ * length gates the result: above residual_threshold (lu/step) the channel
+ * redoes the plain K-1 sweeps from its membrane-force spread, so its result
+ * is the plain one.  The network's current parameters are copied into the
+ * context; net == NULL turns the learned form off.  The reference has no
  * counterpart (it always runs the plain sweeps). */
 int sfg_set_mdf_model(sfg_context* ctx, sfg_mlp* net, double residual_threshold);
+/* Upper limit of the learned form's step length along the network's seed
+ * (default 1, range [0, 4]): 1 shrinks the prediction where that lowers the
+ * residual and never lengthens it.  Limits above 1 lower the residual of a
+ * single step further but destabilise the coupling over longer runs.  No
+ * counterpart in the reference. */
+int sfg_set_mdf_step_limit(sfg_context* ctx, double step_max);
 /* Last step's residuals of a channel (learned gate; plain iteration's last
  * sweep, 0 when it did not run) and cumulative learned / fallback steps. */
 int sfg_get_mdf_stats(sfg_context* ctx, int channel, float* resid_learned, float* resid_plain,
@@ -493,10 +502,13 @@ int sfg_get_phase_times(sfg_context* ctx, float* ms, int n);
 int sfg_reset_phase_times(sfg_context* ctx);
 /* Lattice kernel variant, before sfg_initialize: 0 (default) = the widest
  * vectorised form the channels allow (eight cells per lane in FP16-shifted
- * storage without the scalar when every nx % 8 == 0; otherwise four cells per
- * lane when every nx % 4 == 0), 1 = one cell per thread, 2 = four cells per
- * lane.  FP64 and FP32 results are identical across variants; FP16-shifted
- * results differ only in the stochastic rounding's random bits.  The choice
+ * storage without the scalar when every nx % 8 == 0, otherwise four cells
+ * per lane when every nx % 4 == 0), 1 = one cell per thread, 2 = four cells
+ * per lane, 3 = as 0 with the eight-cell kernel's cells in force tiles
+ * untouched by the step's markers stepped beside the forcing on a side
+ * stream.  FP64 and FP32 results are identical across variants; FP16-shifted
+ * results of the four- and eight-cell forms differ only in the stochastic
+ * rounding's random bits (variants 0 and 3 are identical).  The choice
  * exists for measurements. */
 int sfg_set_lattice_variant(sfg_context* ctx, int variant);
 /* CUDA stream of the context (cudaStream_t), for callers that interleave

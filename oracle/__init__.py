@@ -25,6 +25,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SFO_LIB = os.path.join(HERE, "_build", "libsfo.so")
 REF_LIB = os.path.join(HERE, "_ref", "libsfref.so")
 REF_FAST_LIB = os.path.join(HERE, "_ref", "libsfref_fast.so")
+# the reference's own softflow::Simulation (engine/simulation.cpp) behind the
+# same C entry points (ref_engine.cpp)
+ENGINE_LIB = os.path.join(HERE, "_ref", "libsfengine.so")
 
 BGK, MRT, REGULARIZED = 0, 1, 2
 HOOKEAN, NEO_HOOKEAN, SKALAK, WLC = 0, 1, 2, 3
@@ -204,6 +207,12 @@ def _load(path: str, prefix: str):
         fn.restype = res
         fn.argtypes = args
         fns[name] = fn
+    if prefix == "sfe_":
+        lib.sfe_set_threads.argtypes = [C.c_int]
+        lib.sfe_set_threads.restype = None
+        lib.sfe_get_threads.restype = C.c_int
+        fns["set_threads"] = lib.sfe_set_threads
+        fns["get_threads"] = lib.sfe_get_threads
     if prefix == "sfr_":
         lib.sfr_write_vtk.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int]
         lib.sfr_write_vtk.restype = None
@@ -239,6 +248,10 @@ class OracleSim:
         elif impl == "ref":
             self._lib, self._fn = _load(REF_FAST_LIB if fast else REF_LIB, "sfr_")
             # one thread: the reference spread is order-dependent with more
+            self._fn["set_threads"](threads)
+        elif impl == "engine":
+            # the reference's own Simulation object (deterministic build)
+            self._lib, self._fn = _load(ENGINE_LIB, "sfe_")
             self._fn["set_threads"](threads)
         else:
             raise ValueError(impl)
@@ -298,7 +311,7 @@ class OracleSim:
     def set_threads(self, n: int) -> None:
         """OpenMP threads of the reference build (a setting of its library,
         shared by every simulation on it); the C restatement is serial."""
-        if self.impl == "ref":
+        if self.impl in ("ref", "engine"):
             self._fn["set_threads"](int(n))
 
     # state views (copies) -------------------------------------------

@@ -69,6 +69,7 @@ struct ChannelDev {
     // learned multi-direct forcing
     int learned;                // 1: network seed + one sweep, plain sweeps as fallback
     float mdf_threshold;        // no-slip residual (lu/step) above which it falls back
+    float mdf_step_max;         // largest step length along the network's seed
     // fluid boundaries: x columns as BoundaryType (0 Zou-He inlet / outlet,
     // 1 periodic, 2 SOLID); Zou-He inlet centre-line speed and outlet
     // density; moving top / bottom wall speeds (0 when at rest)
@@ -190,6 +191,7 @@ enum StatusBits : unsigned {
     ST_LIST_OVERFLOW = 2u,      // a per-tile marker list exceeded its capacity
     ST_CAPSULE_TOO_BIG = 4u,    // a capsule exceeded the per-warp node capacity
     ST_TENSOR_TIMEOUT = 8u,     // a tensor-core completion wait gave up
+    ST_LATTICE_RUN = 16u,       // a lattice run record or cell out of range (skipped)
 };
 
 }  // namespace sfg

@@ -266,8 +266,13 @@ struct sfg_context {
     int n_zh = 0;
     // independent launch groups at the start of a step (contact cell list,
     // force tiles + tile moments) run on side streams, joined by events
-    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaStream_t side[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr, ev_contact = nullptr, ev_tiles = nullptr, ev_mom = nullptr;
+    cudaEvent_t ev_lat1 = nullptr;      // the lattice pass over untouched force tiles
+    double mdf_step_max = 1.0;          // learned form: step length limit along the seed
+    bool split_lattice = false;         // that pass beside the forcing (8-cell kernel; off:
+                                        // the concurrent pass slowed the forcing more than it
+                                        // saved on the ensemble)
     // pipelined marker output: snapshots on the context stream, copied to
     // the host on a copy stream while later steps run
     cudaStream_t copy_stream = nullptr;
@@ -423,7 +428,8 @@ static void free_all(sfg_context* c) {
     F(c->tb.slot_scan); F(c->tb.list_off); F(c->tb.slot_tile); F(c->tb.n_slots);
     F(c->tb.list); F(c->tb.scan_tmp); F(c->tb.acc); F(c->tb.gsnap); F(c->tb.capped);
     F(c->tb.fluid_touched); F(c->tb.acc0); F(c->tb.mom); F(c->tb.slot_info); F(c->tb.spread_ctr); F(c->tb.resid_gate); F(c->tb.resid_plain);
-    F(c->mb.u0); F(c->mb.dFsum); F(c->mb.dFprev); F(c->mb.slot8);
+    F(c->mb.u0); F(c->mb.dFsum); F(c->mb.dFprev); F(c->mb.slot8); F(c->mb.dFb); F(c->mb.rho2);
+    F(c->tb.alpha);
     F(c->d_model); F(c->d_learned_steps); F(c->d_fallbacks);
     F(c->d_hfeat); F(c->d_hlab); F(c->d_hvalid); F(c->d_feat); F(c->d_frame); F(c->d_plain_needed);
     F(c->cb.cell_of); F(c->cb.cell_cnt); F(c->cb.cell_start); F(c->cb.cursor); F(c->cb.list);
@@ -464,14 +470,14 @@ static void free_all(sfg_context* c) {
     }
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     c->copy_stream = nullptr;
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < 3; ++i) {
         if (c->side[i]) {
             cudaStreamSynchronize(c->side[i]);
             cudaStreamDestroy(c->side[i]);
         }
         c->side[i] = nullptr;
     }
-    for (cudaEvent_t* e : {&c->ev_fork, &c->ev_contact, &c->ev_tiles, &c->ev_mom}) {
+    for (cudaEvent_t* e : {&c->ev_fork, &c->ev_contact, &c->ev_tiles, &c->ev_mom, &c->ev_lat1}) {
         if (*e) cudaEventDestroy(*e);
         *e = nullptr;
     }
@@ -798,9 +804,13 @@ extern "C" int sfg_initialize(sfg_context* c) {
         for (int y = y0; y < y1; ++y)
             for (int x0 = 0; x0 < p.nx; x0 += VEC_RUN)
                 items4.push_back({ci, y, x0, std::min(VEC_RUN, p.nx - x0)});
-        for (int y = y0; y < y1; ++y)
-            for (int x0 = 0; x0 < p.nx; x0 += VEC8_RUN)
-                items8.push_back({ci, y, x0, std::min(VEC8_RUN, p.nx - x0)});
+        {   // 256-cell runs over the channel's rows in row-major order (a run
+            // continues over row ends; nx % 8 == 0 keeps lanes inside rows)
+            const long long ncell = (long long)(y1 - y0) * p.nx;
+            for (long long o = 0; o < ncell; o += VEC8_RUN)
+                items8.push_back({ci, y0 + (int)(o / p.nx), (int)(o % p.nx),
+                                  (int)std::min<long long>(VEC8_RUN, ncell - o)});
+        }
         h.fluid_cells = 0;
         if (!h.pillars.empty()) {
             const std::vector<unsigned char> m = pillar_mask(p, h.pillars);
@@ -1075,6 +1085,7 @@ extern "C" int sfg_initialize(sfg_context* c) {
     CU(cudaMemset(tb.fluid_touched, 0, sizeof(int) * nch));
     CU(dalloc(&tb.resid_gate, nch));
     CU(dalloc(&tb.resid_plain, nch));
+    CU(dalloc(&tb.alpha, nch));     // written by k_mdf_alpha before each learned spread
     CU(cudaMemset(tb.resid_gate, 0, sizeof(unsigned) * nch));
     CU(cudaMemset(tb.resid_plain, 0, sizeof(unsigned) * nch));
     CU(dalloc(&c->d_learned_steps, nch));
@@ -1085,6 +1096,8 @@ extern "C" int sfg_initialize(sfg_context* c) {
     CU(dalloc(&c->mb.u0, M));
     CU(dalloc(&c->mb.dFsum, M));
     CU(dalloc(&c->mb.dFprev, M));
+    CU(dalloc(&c->mb.dFb, M));
+    CU(dalloc(&c->mb.rho2, M));
     CU(dalloc(&c->mb.slot8, 8LL * M));
     if (M > 0) {
         CU(cudaMemset(c->mb.u0, 0, sizeof(double2) * M));
@@ -1126,8 +1139,8 @@ extern "C" int sfg_initialize(sfg_context* c) {
     apply_launch_config(c);
     CU(cudaStreamSynchronize(c->stream));
     if (c->M > 0 && !c->side[0]) {
-        for (int i = 0; i < 2; ++i) CU(cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking));
-        for (cudaEvent_t* e : {&c->ev_fork, &c->ev_contact, &c->ev_tiles, &c->ev_mom})
+        for (int i = 0; i < 3; ++i) CU(cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking));
+        for (cudaEvent_t* e : {&c->ev_fork, &c->ev_contact, &c->ev_tiles, &c->ev_mom, &c->ev_lat1})
             CU(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     }
     c->initialized = true;
@@ -1156,6 +1169,24 @@ static int enqueue_step_t(sfg_context* c, int p) {
     const int nch = (int)c->ch.size();
     int launches = 0;
     mark(c, -1);
+    LatticeLaunch L{c->d_items, c->n_items, c->d_chans, c->f[p], c->f[1 - p], c->g[p],
+                    c->g[1 - p], c->cfield, c->d_stepped, c->d_adr_pending, c->d_c_fresh,
+                    c->d_step_ctr, c->any_adr && !c->any_chem, c->d_items4, c->n_items4, c->use_vec4,
+                    c->persistent_ctas, c->shared_collision, c->any_bc, c->d_zh_rows,
+                    c->n_zh, c->d_ibb, c->ibb_level_start.data(),
+                    (int)c->ibb_level_start.size() - 1, c->d_items8, c->n_items8, c->use_vec8,
+                    0, nch, c->d_status};
+    TileViewArgs tv{c->M > 0 ? c->tb.tile_slot[p] : nullptr,
+                    c->M > 0 ? c->tb.tile_slot[1 - p] : nullptr, c->tb.fin[p], c->tb.gsnap,
+                    c->tb.fin[1 - p]};
+    // Optionally (lattice variant 3) the 8-cell lattice kernel in two passes:
+    // cells of force tiles that no marker stencil touches this step take the
+    // uniform force and do not depend on the forcing, so that pass runs
+    // beside it on a side stream once the step's slot map exists; the
+    // touched tiles follow the last spread.  The passes write disjoint cells
+    // of the other population buffer.
+    const bool split = c->M > 0 && !c->profiling && c->side[0] != nullptr && c->split_lattice &&
+                       c->use_vec8 && !L.any_adr && !c->any_bc;
     if (c->M > 0) {
         cudaMemsetAsync(c->tb.capped, 0, sizeof(int) * nch, st);
         cudaMemsetAsync(c->tb.fluid_touched, 0, sizeof(int) * nch, st);
@@ -1176,6 +1207,14 @@ static int enqueue_step_t(sfg_context* c, int p) {
             launch_tiles(c->d_chans, c->d_caps, c->M, c->mb, c->tb, c->tb.T, p, c->d_phi,
                          c->d_status, c->side[1]);
             CU(cudaEventRecord(c->ev_tiles, c->side[1]));
+            if (split) {
+                CU(cudaStreamWaitEvent(c->side[2], c->ev_tiles, 0));
+                LatticeLaunch L1 = L;
+                L1.pass = 1;
+                launch_lattice_step<S, R>(L1, tv, c->side[2]);
+                CU(cudaEventRecord(c->ev_lat1, c->side[2]));
+                launches += 1;
+            }
             if (c->Kmax > 1) {
                 launch_tile_moments<S, R>(c->d_chans, fp, c->tb, c->spread_grid, c->side[1]);
                 CU(cudaEventRecord(c->ev_mom, c->side[1]));
@@ -1225,12 +1264,13 @@ static int enqueue_step_t(sfg_context* c, int p) {
                              c->d_status, st);
             mark(c, SFG_PHASE_IBM_SPREAD);
             launch_mdf_interp<S, R>(c->d_chans, c->M, c->mb, fp, c->tb, p, 2, MDF_LEARNED, st);
+            launch_mdf_alpha(c->d_chans, nch, c->mb, c->tb, st);
             mark(c, SFG_PHASE_MDF_INTERP);
             launch_plain_needed(c->d_chans, nch, c->tb, st);
             launch_spread<R>(c->d_chans, c->mb, c->tb, p, 2, MDF_LEARNED, 2, c->spread_grid,
                              c->d_status, st);
             mark(c, SFG_PHASE_IBM_SPREAD);
-            launches += 6;
+            launches += 7;
         }
         for (int k = 1; k < c->Kmax; ++k) {
             launch_mdf_interp<S, R>(c->d_chans, c->M, c->mb, fp, c->tb, p, k, MDF_PLAIN, st);
@@ -1246,18 +1286,15 @@ static int enqueue_step_t(sfg_context* c, int p) {
             launches += 1;
         }
     }
-    LatticeLaunch L{c->d_items, c->n_items, c->d_chans, c->f[p], c->f[1 - p], c->g[p],
-                    c->g[1 - p], c->cfield, c->d_stepped, c->d_adr_pending, c->d_c_fresh,
-                    c->d_step_ctr, c->any_adr && !c->any_chem, c->d_items4, c->n_items4, c->use_vec4,
-                    c->persistent_ctas, c->shared_collision, c->any_bc, c->d_zh_rows,
-                    c->n_zh, c->d_ibb, c->ibb_level_start.data(),
-                    (int)c->ibb_level_start.size() - 1, c->d_items8, c->n_items8, c->use_vec8};
     if (c->any_bc && c->n_zh > 0) launches += 1;
     if (c->any_bc && c->ibb_level_start.size() > 1) launches += (int)c->ibb_level_start.size() - 1;
-    TileViewArgs tv{c->M > 0 ? c->tb.tile_slot[p] : nullptr,
-                    c->M > 0 ? c->tb.tile_slot[1 - p] : nullptr, c->tb.fin[p], c->tb.gsnap,
-                    c->tb.fin[1 - p]};
-    launch_lattice_step<S, R>(L, tv, st);
+    if (split) {
+        L.pass = 2;
+        launch_lattice_step<S, R>(L, tv, st);
+        CU(cudaStreamWaitEvent(st, c->ev_lat1, 0));
+    } else {
+        launch_lattice_step<S, R>(L, tv, st);
+    }
     if (c->any_chem) {
         // this step's scalar step, then the capsule chemistry
         // (simulation.cpp:636-653), before the markers move
@@ -1354,6 +1391,8 @@ extern "C" int sfg_synchronize(sfg_context* c, unsigned* status_out) {
     unsigned st = 0;
     if (c->d_status) CU(cudaMemcpy(&st, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost));
     if (status_out) *status_out = st;
+    if (st & ST_LATTICE_RUN)
+        return fail(SFG_ERR_CUDA, "a lattice run record or cell was out of range (skipped)");
     if (st & (ST_LIST_OVERFLOW | ST_CAPSULE_TOO_BIG))
         return fail(SFG_ERR_CAPACITY,
                     st & ST_LIST_OVERFLOW ? "a force-tile marker list exceeded 4096 entries"
@@ -1494,6 +1533,7 @@ extern "C" int sfg_set_mdf_model(sfg_context* c, sfg_mlp* net, double residual_t
         const bool on = net && h.d.ibm_iterations >= 3 && h.d.cap_end > h.d.cap_begin;
         h.d.learned = on ? 1 : 0;
         h.d.mdf_threshold = (float)residual_threshold;
+        h.d.mdf_step_max = (float)c->mdf_step_max;
         any = any || on;
     }
     std::vector<ChannelDev> dv;
@@ -1504,6 +1544,25 @@ extern "C" int sfg_set_mdf_model(sfg_context* c, sfg_mlp* net, double residual_t
     c->any_learned = any;
     c->tb.plain_needed = any ? c->d_plain_needed : nullptr;
     drop_graphs(c);
+    return SFG_OK;
+}
+
+extern "C" int sfg_set_mdf_step_limit(sfg_context* c, double step_max) {
+    if (!c) return fail(SFG_ERR_ARG, "sfg_set_mdf_step_limit: null context");
+    if (!(step_max >= 0.0 && step_max <= 4.0))
+        return fail(SFG_ERR_ARG, "sfg_set_mdf_step_limit: the limit must be in [0, 4]");
+    c->mdf_step_max = step_max;
+    if (!c->initialized) return SFG_OK;
+    CU(cudaSetDevice(c->device));
+    CU(cudaStreamSynchronize(c->stream));
+    std::vector<ChannelDev> dv;
+    for (auto& h : c->ch) {
+        h.d.mdf_step_max = (float)step_max;
+        dv.push_back(h.d);
+    }
+    CU(cudaMemcpyAsync(c->d_chans, dv.data(), sizeof(ChannelDev) * dv.size(),
+                       cudaMemcpyHostToDevice, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
     return SFG_OK;
 }
 
@@ -2124,10 +2183,11 @@ extern "C" int sfg_reset_phase_times(sfg_context* c) {
 extern "C" int sfg_set_lattice_variant(sfg_context* c, int variant) {
     if (!c) return fail(SFG_ERR_ARG, "sfg_set_lattice_variant: null context");
     if (c->initialized) return fail(SFG_ERR_STATE, "sfg_set_lattice_variant: before sfg_initialize");
-    if (variant < 0 || variant > 2)
-        return fail(SFG_ERR_ARG, "sfg_set_lattice_variant: 0, 1 or 2");
+    if (variant < 0 || variant > 3)
+        return fail(SFG_ERR_ARG, "sfg_set_lattice_variant: 0, 1, 2 or 3");
     c->force_scalar_lattice = variant == 1;
     c->force_vec4_lattice = variant == 2;
+    c->split_lattice = variant == 3;
     return SFG_OK;
 }
 

@@ -1131,7 +1131,8 @@ __device__ __forceinline__ void lattice_run4(const RowItem& it, const ChannelDev
 // moments, velocity, collision, stochastic encode back into the same word,
 // so the populations stay packed while the next pair is worked on.
 // ---------------------------------------------------------------------------
-constexpr int VEC8_RUN = 256;   // cells per warp work item of the 8-cell form
+constexpr int VEC8_RUN = 256;   // cells per warp work item of the 8-cell form (row-major,
+                                // continuing over row ends)
 
 __device__ __forceinline__ uint32_t u4_get(const uint4& v, int k) {
     return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
@@ -1159,44 +1160,47 @@ __device__ __forceinline__ uint32_t enc_word(F2 a, uint32_t bits) {
 
 // Stores the eight encoded cells (four words) of one plane of a 256-cell
 // run: v holds cells x .. x + 7 of the lane, cell x in the low half of v.x.
-// dx is the x shift (-1, 0, +1): the shifted forms build the target's
-// aligned 16-byte block from the lane's words and one word of the
-// neighbouring lane (byte permutes); the run's first and last lanes store
-// the cells at the run's ends singly (the neighbouring runs own the rest of
-// those blocks).  All lanes of the warp must call this (shuffles).
+// CX is the plane's x shift (-1, 0, +1), the same for every lane: the
+// neighbour word it needs is shuffled by all lanes of the warp, whatever
+// their own store does (lanes of one run can sit on different rows, so
+// some reflect the plane at a wall while others push it).  dx is the lane's
+// own shift: CX when it pushes, 0 when it reflects.  The shifted forms build
+// the target's aligned 16-byte block from the lane's words and that
+// neighbour word (byte permutes).  A segment of consecutive active lanes
+// stores the cells at its ends singly: `first` (no active lane of its row
+// before it) leaves the block cell its left neighbour pushes in and, for
+// dx < 0, stores its first cell at xb; `last` (no active lane of its row
+// after it) stores, for dx > 0, its last cell at xe and, for dx < 0, leaves
+// the block cell its right neighbour pushes in.
+template <int CX>
 __device__ __forceinline__ void store_plane8h(__half* __restrict__ row, const uint4 v, int dx,
-                                              int x, int x0, int len, int nx, bool active,
-                                              int lane, int last_lane) {
+                                              int x, int xb, int xe, bool active, bool first,
+                                              bool last) {
+    uint32_t nb = 0u;   // CX > 0: the previous lane's last word; CX < 0: the next lane's first
+    if (CX > 0) nb = __shfl_up_sync(0xffffffffu, v.w, 1);
+    if (CX < 0) nb = __shfl_down_sync(0xffffffffu, v.x, 1);
     if (dx == 0) {
         if (active) *reinterpret_cast<uint4*>(row + x) = v;
         return;
     }
     if (dx > 0) {
         // block x .. x + 7 receives cells x - 1 .. x + 6
-        const uint32_t prev = __shfl_up_sync(0xffffffffu, v.w, 1);
-        const uint32_t a0 = __byte_perm(prev, v.x, 0x5432), a1 = __byte_perm(v.x, v.y, 0x5432),
+        const uint32_t a0 = __byte_perm(nb, v.x, 0x5432), a1 = __byte_perm(v.x, v.y, 0x5432),
                        a2 = __byte_perm(v.y, v.z, 0x5432), a3 = __byte_perm(v.z, v.w, 0x5432);
-        int xe = x0 + len;
-        xe = xe >= nx ? xe - nx : xe;
-        const bool first = lane == 0;
         if (active && !first) *reinterpret_cast<uint4*>(row + x) = make_uint4(a0, a1, a2, a3);
         if (active && first) row[x + 1] = __ushort_as_half((unsigned short)(v.x & 0xFFFFu));
         if (active && first) *reinterpret_cast<uint32_t*>(row + x + 2) = a1;
         if (active && first) *reinterpret_cast<uint2*>(row + x + 4) = make_uint2(a2, a3);
-        if (active && lane == last_lane) row[xe] = __ushort_as_half((unsigned short)(v.w >> 16));
+        if (active && last) row[xe] = __ushort_as_half((unsigned short)(v.w >> 16));
     } else {
         // block x .. x + 7 receives cells x + 1 .. x + 8
-        const uint32_t next = __shfl_down_sync(0xffffffffu, v.x, 1);
         const uint32_t b0 = __byte_perm(v.x, v.y, 0x5432), b1 = __byte_perm(v.y, v.z, 0x5432),
-                       b2 = __byte_perm(v.z, v.w, 0x5432), b3 = __byte_perm(v.w, next, 0x5432);
-        int xb = x0 - 1;
-        xb = xb < 0 ? xb + nx : xb;
-        const bool last = lane == last_lane;
+                       b2 = __byte_perm(v.z, v.w, 0x5432), b3 = __byte_perm(v.w, nb, 0x5432);
         if (active && !last) *reinterpret_cast<uint4*>(row + x) = make_uint4(b0, b1, b2, b3);
         if (active && last) *reinterpret_cast<uint2*>(row + x) = make_uint2(b0, b1);
         if (active && last) *reinterpret_cast<uint32_t*>(row + x + 4) = b2;
         if (active && last) row[x + 6] = __ushort_as_half((unsigned short)(v.w >> 16));
-        if (active && lane == 0) row[xb] = __ushort_as_half((unsigned short)(v.x & 0xFFFFu));
+        if (active && first) row[xb] = __ushort_as_half((unsigned short)(v.x & 0xFFFFu));
     }
 }
 
@@ -1253,17 +1257,44 @@ __device__ __forceinline__ F2 quad_pair(const float4& v, int p) {
 // stochastic encode of pair k of plane q is the lane's seed times an odd
 // multiplier per (q, k): a bijection of the seed, so each 13-bit field is
 // uniform.
+// A run is `len` consecutive fluid cells of one channel in row-major order
+// starting at (x0, y), so it may continue over row ends (each row's nx is a
+// multiple of 8: a lane's eight cells never straddle one): lane i takes
+// cells 8i .. 8i + 7 of the run, on its own row.  A segment of active lanes
+// ends at a row end, where the stream wraps around the periodic row.
+// `pass` selects the lanes (eight cells of one force tile each): 0 all, 1
+// those whose tile has no force slot this step (uniform force: they do not
+// depend on the step's forcing), 2 those whose tile has one.  Passes 1 and 2
+// together write exactly what pass 0 writes.
 template <int COLL>
 __device__ __forceinline__ void lattice_run8h(const RowItem& it, const ChannelDev& ch, int st,
                                               const __half* __restrict__ src,
                                               __half* __restrict__ dst, const TileView& tv,
-                                              uint32_t step_mix, int lane) {
-    const bool active = 8 * lane < it.len;
+                                              uint32_t step_mix, int lane, int pass,
+                                              unsigned* __restrict__ status) {
+    bool in_run = 8 * lane < it.len;
     const int last_lane = (it.len >> 3) - 1;
     const int nx = ch.nx, ny = ch.ny, pitch = ch.pitch, plane = (int)ch.plane;
-    const int x0 = it.x0, y = it.y;
-    const int x = x0 + 8 * lane;
-    const int n = y * pitch + (active ? x : x0);
+    int x = it.x0 + 8 * lane, y = it.y;
+    // row wrap: at most 256 / nx + 1 times for a valid run (bounded; a cell
+    // outside the channel is flagged and skipped)
+    for (int k = 0; k < 40 && nx > 0 && x >= nx; ++k) {
+        x -= nx;
+        ++y;
+    }
+    if (in_run && (nx < 8 || x < 0 || x + 8 > nx || y < 0 || y >= ny)) {
+        atomicOr(status, (unsigned)ST_LATTICE_RUN);
+        in_run = false;
+    }
+    const RunTiles rt = in_run ? run_tiles(ch, x, y, tv) : RunTiles{-1, -1, 0};
+    const bool active = in_run && (pass == 0 || ((rt.s >= 0) == (pass == 2)));
+    const unsigned am = __ballot_sync(0xffffffffu, active);
+    if (am == 0u) return;                      // warp-uniform
+    const bool first = active && (lane == 0 || x == 0 || !((am >> (lane - 1)) & 1u));
+    const bool last = active && (lane == last_lane || x + 8 == nx || !((am >> (lane + 1)) & 1u));
+    const int xb = x == 0 ? nx - 1 : x - 1;    // the row's ends wrap (periodic x)
+    const int xe = x + 8 == nx ? 0 : x + 8;
+    const int n = y * pitch + x;
     uint4 w[9];
     {
         const __half* fs = src + ch.f_off + n;
@@ -1272,7 +1303,6 @@ __device__ __forceinline__ void lattice_run8h(const RowItem& it, const ChannelDe
             w[q] = active ? __ldg(reinterpret_cast<const uint4*>(fs + (size_t)q * plane))
                           : make_uint4(0u, 0u, 0u, 0u);
     }
-    const RunTiles rt = active ? run_tiles(ch, x, y, tv) : RunTiles{-1, -1, 0};
     const uint32_t seed = mix32((uint32_t)n ^ step_mix);
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
@@ -1293,31 +1323,36 @@ __device__ __forceinline__ void lattice_run8h(const RowItem& it, const ChannelDe
                 u4_set(w[q], k, enc_word(d[q], seed * dither_mult((uint32_t)(4 * q + k))));
         }
     }
-    const Nbr b = neighbours(0, y, nx, ny, ch.periodic_y ? 1 : 0);
+    // per-lane rows: a plane bound for a wall row is reflected into the own
+    // cell (dx = 0); every lane still takes part in the plane's shuffle
+    const Nbr b = neighbours(0, in_run ? y : it.y, nx, ny, ch.periodic_y ? 1 : 0);
     __half* fd = dst + ch.f_off;
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
-        const int cx = cx_of(q), cy = cy_of(q);
+        const int cy = cy_of(q);
         const bool wall = (cy > 0 && b.wall_p) || (cy < 0 && b.wall_m);
-        if (wall) {
-            store_plane8h(fd + opp_of(q) * plane + y * pitch, w[q], 0, x, x0, it.len, nx, active,
-                          lane, last_lane);
-        } else {
-            const int yd = cy == 0 ? y : (cy > 0 ? b.yp : b.ym);
-            store_plane8h(fd + q * plane + yd * pitch, w[q], cx, x, x0, it.len, nx, active, lane,
-                          last_lane);
-        }
+        const int yd = wall || cy == 0 ? y : (cy > 0 ? b.yp : b.ym);
+        __half* row = fd + (wall ? opp_of(q) : q) * plane + yd * pitch;
+        const int dx = wall ? 0 : cx_of(q);
+        if (cx_of(q) > 0)
+            store_plane8h<1>(row, w[q], dx, x, xb, xe, active, first, last);
+        else if (cx_of(q) < 0)
+            store_plane8h<-1>(row, w[q], dx, x, xb, xe, active, first, last);
+        else
+            store_plane8h<0>(row, w[q], dx, x, xb, xe, active, first, last);
     }
 }
 
 // Persistent 8-cell form (FP16-shifted storage, no scalar): every warp walks
 // a contiguous chunk of 256-cell runs, prefetching the next run record.
+// `pass` as in lattice_run8h.
 template <int COLL>
 __global__ void __launch_bounds__(256, 2)
 k_lattice_step8h(const RowItem* __restrict__ items, int n_items,
-                 const ChannelDev* __restrict__ chans, const __half* __restrict__ src,
-                 __half* __restrict__ dst, TileView tv, const int* __restrict__ stepped,
-                 const unsigned* __restrict__ step_ctr) {
+                 const ChannelDev* __restrict__ chans, int n_chans,
+                 const __half* __restrict__ src, __half* __restrict__ dst, TileView tv,
+                 const int* __restrict__ stepped, const unsigned* __restrict__ step_ctr,
+                 int pass, unsigned* __restrict__ status) {
     const int lane = threadIdx.x & 31;
     const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -1330,8 +1365,14 @@ k_lattice_step8h(const RowItem* __restrict__ items, int n_items,
     for (int item = i0; item < i1; ++item) {
         const RowItem it = next;
         if (item + 1 < i1) next = items[item + 1];
+        if (it.chan < 0 || it.chan >= n_chans || it.len <= 0 || it.len > VEC8_RUN ||
+            it.x0 < 0) {                       // warp-uniform: a bad record is skipped
+            if (lane == 0) atomicOr(status, (unsigned)ST_LATTICE_RUN);
+            continue;
+        }
         const ChannelDev& ch = chans[it.chan];
-        lattice_run8h<COLL>(it, ch, stepped[it.chan], src, dst, tv, step_mix, lane);
+        lattice_run8h<COLL>(it, ch, stepped[it.chan], src, dst, tv, step_mix, lane, pass,
+                            status);
     }
 }
 

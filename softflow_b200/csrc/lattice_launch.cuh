@@ -72,16 +72,16 @@ void launch_lattice_step(const LatticeLaunch& L, const TileViewArgs& tv, cudaStr
             __half* dst = static_cast<__half*>(L.dst);
             switch (L.collision) {
                 case 0: k_lattice_step8h<0><<<grid, 32 * ITEMS_PER_CTA, 0, st>>>(
-                            L.items8, L.n_items8, L.chans, src, dst, v, L.stepped, L.step_ctr);
+                            L.items8, L.n_items8, L.chans, L.n_chans, src, dst, v, L.stepped, L.step_ctr, L.pass, L.status);
                         break;
                 case 1: k_lattice_step8h<1><<<grid, 32 * ITEMS_PER_CTA, 0, st>>>(
-                            L.items8, L.n_items8, L.chans, src, dst, v, L.stepped, L.step_ctr);
+                            L.items8, L.n_items8, L.chans, L.n_chans, src, dst, v, L.stepped, L.step_ctr, L.pass, L.status);
                         break;
                 case 2: k_lattice_step8h<2><<<grid, 32 * ITEMS_PER_CTA, 0, st>>>(
-                            L.items8, L.n_items8, L.chans, src, dst, v, L.stepped, L.step_ctr);
+                            L.items8, L.n_items8, L.chans, L.n_chans, src, dst, v, L.stepped, L.step_ctr, L.pass, L.status);
                         break;
                 default: k_lattice_step8h<-1><<<grid, 32 * ITEMS_PER_CTA, 0, st>>>(
-                             L.items8, L.n_items8, L.chans, src, dst, v, L.stepped, L.step_ctr);
+                             L.items8, L.n_items8, L.chans, L.n_chans, src, dst, v, L.stepped, L.step_ctr, L.pass, L.status);
                          break;
             }
             return;

@@ -50,6 +50,7 @@ struct TileBufs {
     int* plain_needed = nullptr;  // [1] set when some channel needs the plain sweeps; null
                                   // (always run them) unless a channel is learned
     unsigned* resid_gate = nullptr;   // [nchan] learned form's no-slip residual (float bits)
+    double* alpha = nullptr;          // [nchan] learned form's step length along the seed
     unsigned* resid_plain = nullptr;  // [nchan] plain iteration's last-sweep residual
 };
 
@@ -105,6 +106,10 @@ void launch_mdf_learned(const ChannelDev* chans, const CapsuleDev* caps, int M,
 void launch_harvest(const ChannelDev* chans, const CapsuleDev* caps, int M, const MarkerBufs& mb,
                     float* feat, float* label, int* valid, cudaStream_t st);
 cudaError_t prepare_mdf_learned();
+// Step length along the learned seed per channel, the learned sweep's
+// correction and the gate residual (after the learned sweep's interpolation).
+void launch_mdf_alpha(const ChannelDev* chans, int nch, const MarkerBufs& mb, TileBufs& tb,
+                      cudaStream_t st);
 // Sets tb.plain_needed from the gate residuals (learned contexts).
 void launch_plain_needed(const ChannelDev* chans, int nch, TileBufs& tb, cudaStream_t st);
 // Moments of the step's force tiles (before the first forcing sweep).
@@ -144,6 +149,10 @@ struct LatticeLaunch {
     const RowItem* items8 = nullptr;   // 256-cell runs for the 8-cell FP16-shifted kernel
     int n_items8 = 0;
     bool use_vec8 = false;             // FP16-shifted storage, every channel nx % 8 == 0
+    int pass = 0;                      // 8-cell kernel: 0 all cells, 1 cells of untouched
+                                       // force tiles, 2 cells of touched ones
+    int n_chans = 0;                   // channel count (run records are checked against it)
+    unsigned* status = nullptr;        // status word (ST_* bits)
 };
 struct TileViewArgs {
     const int* cur_slot;

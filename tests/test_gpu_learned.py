@@ -6,8 +6,10 @@
 * harvested features agree with the marker state (frame, stretch,
   curvature and target velocity against oracle/mlp.features; the previous
   correction input equals the last step's label);
-* a network trained on harvested data lowers the no-slip residual of one
-  correction sweep relative to one sweep without it.
+* a network trained on harvested data reproduces the plain correction far
+  better than no seed, and its no-slip residual is no worse than the plain
+  iteration's (a single channel, and the median over 16 ensemble channels
+  from the same states).
 """
 import numpy as np
 import pytest
@@ -93,11 +95,12 @@ def test_harvest_features_consistent(sfg):
 def test_trained_network_reproduces_plain_iteration(sfg):
     """Train on the single channel's own plain runs (5 sweeps).  From one
     state, one step in three forms: plain (4 correction sweeps), learned
-    (network seed for the first 3, then the last sweep) and the same pipeline
-    without the network (zero seed, then one sweep).  The learned seed is
-    close to the plain correction before the last sweep and far closer than
-    the zero seed, and the learned no-slip residual is no worse than the
-    plain form's."""
+    (network seed for the first 3, scaled by the channel's residual-minimising
+    step length, then the last sweep) and the same pipeline without the
+    network (zero seed, then one sweep).  The learned seed is close to the
+    plain correction before the last sweep and far closer than the zero
+    seed, and the learned no-slip residual is no worse than the plain
+    form's."""
     from softflow_b200.learned import MDFNetwork, harvest, train_network
     src = _c1("fp32")
     X, Y = harvest(src, records=300, every=5, warmup=20)
@@ -123,4 +126,32 @@ def test_trained_network_reproduces_plain_iteration(sfg):
           f"residual plain {out['plain'][1]:.3e} learned {out['learned'][1]:.3e} "
           f"zero seed {out['zero'][1]:.3e}")
     assert err["learned"] < 0.5 * err["zero"]
-    assert out["learned"][1] <= 1.25 * out["plain"][1]
+    assert out["learned"][1] <= out["plain"][1]
+
+
+def test_gate_residual_no_worse_than_plain_on_ensemble_sample(sfg):
+    """The first 16 channels of the ensemble (FP16S), two identical plain
+    runs of 200 steps (deterministic: the same state), then one step each:
+    plain (4 correction sweeps) and learned (the network trained on plain
+    runs, 2M samples).  Per channel, the learned form's gate residual
+    against the plain iteration's residual at its last sweep: the median
+    over channels is no larger."""
+    from softflow_b200 import workloads as W
+    from softflow_b200.learned import train_network, training_set
+    X, Y = training_set(2_000_000)
+    net, _ = train_network(X, Y, epochs=8, seed=1)
+    plans = W.plan_c3("fp16s")[:16]
+    a = W.build(plans, "fp16s")
+    b = W.build(W.plan_c3("fp16s")[:16], "fp16s")
+    a.run(200)
+    b.run(200)
+    assert np.array_equal(a.field(3).distributions(), b.field(3).distributions())
+    b.setLearnedMDF(net, threshold=1e9)      # never fall back: the learned sweep's own residual
+    a.run(1)
+    b.run(1)
+    rp = np.array([a.mdfStats(i)["resid_plain"] for i in range(len(plans))])
+    rl = np.array([b.mdfStats(i)["resid_learned"] for i in range(len(plans))])
+    print(f"gate residual median: learned {np.median(rl):.3e}, plain {np.median(rp):.3e}; "
+          f"learned <= plain on {int(np.sum(rl <= rp))} of {len(plans)} channels")
+    assert np.all(rp > 0) and np.all(np.isfinite(rl))
+    assert np.median(rl) <= np.median(rp)

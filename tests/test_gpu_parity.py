@@ -72,6 +72,32 @@ def test_fp64_coupled(sfg, oracle_mod, name, steps):
         assert rel_l2(C, o.concentration()) < 1e-9
 
 
+@pytest.mark.parametrize("name,steps", [("c1", 40), ("mini_c2", 40), ("pillars_capsules", 60),
+                                        ("chem_physics", 40)])
+def test_fp64_against_reference_engine(sfg, oracle_mod, name, steps):
+    """Against the reference's own softflow::Simulation (engine/simulation.cpp
+    compiled unmodified in oracle/_ref/libsfengine.so): its placement, step
+    orchestration, force cap, move and clamp."""
+    import os
+    import oracle as O
+    if not os.path.exists(O.ENGINE_LIB):
+        pytest.skip("reference engine library not built")
+    case = CASES[name]
+    o = build_oracle(case, impl="engine")
+    sim = build_gpu(case, "fp64")
+    assert np.array_equal(sim.capsules().positions(), o.positions())
+    o.step(steps)
+    sim.run(steps)
+    a, b = _state(sim), _ostate(o)
+    rows = fluid_rows(case)
+    for k in ("ux", "uy", "rho"):
+        assert rel_l2(a[k][rows], b[k][rows]) < 1e-9, k
+    assert np.max(np.abs(a["pos"] - b["pos"])) < 1e-9
+    assert rel_l2(a["frc"], b["frc"]) < 1e-8
+    if case["conc"] is not None:
+        assert rel_l2(sim.advectionDiffusion().concentration(), o.concentration()) < 1e-9
+
+
 @pytest.mark.parametrize("name", ["seam_single", "narrow_seam", "c1_plain"])
 def test_fp64_single_capsule_first_steps_bit_exact(sfg, oracle_mod, name):
     """Without contact (pow) or Helfrich (atan2), a step is reproduced bit for
