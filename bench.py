@@ -51,7 +51,8 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
-    ap.add_argument("--workload", default="c3", choices=["c3", "c2", "c1", "c0"])
+    ap.add_argument("--workload", default="c3", choices=["c3", "c2", "c2_lattice", "c1", "c0"],
+                    help="c2_lattice: configuration 2's fluid alone (the plain stream-collide)")
     ap.add_argument("--precision", default="fp16s", choices=["fp16s", "fp32", "fp64"])
     ap.add_argument("--impl", default="product", choices=["product", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -434,10 +435,11 @@ def run_product(args, world, rank, local, pg):
     if args.workload == "c3" and not args.no_plain and world == 1:
         c2_forms = run_c2_forms(args, local)
 
+    metric, value = ("capsule-steps/s", cap_steps) if caps else ("MLUPS", mlups)
     out = {
-        "metric": "capsule-steps/s",
-        "value": cap_steps,
-        "unit": "capsule-steps/s",
+        "metric": metric,
+        "value": value,
+        "unit": metric,
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
@@ -532,10 +534,12 @@ def run_e2e(args, plans, ens, pg, local):
     up = allmax(pg, t_up - t0)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     caps = sum(len(c.caps) for c in ens._chans)
-    return {"value": caps * args.steps * world / sec, "unit": "capsule-steps/s",
+    from softflow_b200 import workloads as W
+    units, unit = (caps, "capsule-steps/s") if caps else (W.totals(plans)[0] / 1e6, "MLUPS")
+    return {"value": units * args.steps * world / sec, "unit": unit,
             "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h_step,
             "upload_ms": 1e3 * up, "upload_bytes": h2d,
-            "per_step_value": caps * args.steps * world / (sec - up),
+            "per_step_value": units * args.steps * world / (sec - up),
             "per_step_ms": 1e3 * (sec - up) / args.steps,
             "note": "value: the whole timed region, i.e. the one-off upload of the initial "
                     "state from pinned host memory (sfg_set_all_populations, FP64 reference "

@@ -346,22 +346,13 @@ int sfg_mlp_step_count(sfg_mlp* m, int* steps);
  * sweeps of ImmersedBoundary::multiDirectForcing (immersed_boundary.cpp:
  * 231-286) by the network's prediction of their summed correction (seed),
  * spread like a sweep; the last plain sweep follows.  The no-slip residual
- * after the seed is linear in a scale a of the seed; per channel the step
- * length a* in [0, step limit] that minimises the squared residual over the
- * channel's markers scales the seed (see sfg_set_mdf_step_limit).  The
- * residual max |U_prev - U_interp| over the channel's markers at that step
- * length gates the result: above residual_threshold (lu/step) the channel
- * redoes the plain K-1 sweeps from its membrane-force spread, so its result
- * is the plain one.  The network's current parameters are copied into the
- * context; net == NULL turns the learned form off.  The reference has no
+ * max |U_prev - U_interp| over the channel's markers, taken at that sweep's
+ * interpolation, gates the result: above residual_threshold (lu/step) the
+ * channel redoes the plain K-1 sweeps from its membrane-force spread, so its
+ * result is the plain one.  The network's current parameters are copied into
+ * the context; net == NULL turns the learned form off.  The reference has no
  * counterpart (it always runs the plain sweeps). */
 int sfg_set_mdf_model(sfg_context* ctx, sfg_mlp* net, double residual_threshold);
-/* Upper limit of the learned form's step length along the network's seed
- * (default 1, range [0, 4]): 1 shrinks the prediction where that lowers the
- * residual and never lengthens it.  Limits above 1 lower the residual of a
- * single step further but destabilise the coupling over longer runs.  No
- * counterpart in the reference. */
-int sfg_set_mdf_step_limit(sfg_context* ctx, double step_max);
 /* Last step's residuals of a channel (learned gate; plain iteration's last
  * sweep, 0 when it did not run) and cumulative learned / fallback steps. */
 int sfg_get_mdf_stats(sfg_context* ctx, int channel, float* resid_learned, float* resid_plain,

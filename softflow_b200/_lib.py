@@ -158,7 +158,6 @@ SIGNATURES = {
                                 _P(C.c_float), C.c_void_p]),
     "sfg_mlp_step_count": (C.c_int, [C.c_void_p, _P(C.c_int)]),
     "sfg_set_mdf_model": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double]),
-    "sfg_set_mdf_step_limit": (C.c_int, [C.c_void_p, C.c_double]),
     "sfg_get_mdf_stats": (C.c_int, [C.c_void_p, C.c_int, _P(C.c_float), _P(C.c_float),
                                     _P(C.c_longlong), _P(C.c_longlong)]),
     "sfg_autotune": (C.c_int, [C.c_void_p, C.c_int, _P(C.c_int)]),

@@ -69,7 +69,6 @@ struct ChannelDev {
     // learned multi-direct forcing
     int learned;                // 1: network seed + one sweep, plain sweeps as fallback
     float mdf_threshold;        // no-slip residual (lu/step) above which it falls back
-    float mdf_step_max;         // largest step length along the network's seed
     // fluid boundaries: x columns as BoundaryType (0 Zou-He inlet / outlet,
     // 1 periodic, 2 SOLID); Zou-He inlet centre-line speed and outlet
     // density; moving top / bottom wall speeds (0 when at rest)

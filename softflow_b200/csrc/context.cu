@@ -269,7 +269,6 @@ struct sfg_context {
     cudaStream_t side[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr, ev_contact = nullptr, ev_tiles = nullptr, ev_mom = nullptr;
     cudaEvent_t ev_lat1 = nullptr;      // the lattice pass over untouched force tiles
-    double mdf_step_max = 1.0;          // learned form: step length limit along the seed
     bool split_lattice = false;         // that pass beside the forcing (8-cell kernel; off:
                                         // the concurrent pass slowed the forcing more than it
                                         // saved on the ensemble)
@@ -428,8 +427,7 @@ static void free_all(sfg_context* c) {
     F(c->tb.slot_scan); F(c->tb.list_off); F(c->tb.slot_tile); F(c->tb.n_slots);
     F(c->tb.list); F(c->tb.scan_tmp); F(c->tb.acc); F(c->tb.gsnap); F(c->tb.capped);
     F(c->tb.fluid_touched); F(c->tb.acc0); F(c->tb.mom); F(c->tb.slot_info); F(c->tb.spread_ctr); F(c->tb.resid_gate); F(c->tb.resid_plain);
-    F(c->mb.u0); F(c->mb.dFsum); F(c->mb.dFprev); F(c->mb.slot8); F(c->mb.dFb); F(c->mb.rho2);
-    F(c->tb.alpha);
+    F(c->mb.u0); F(c->mb.dFsum); F(c->mb.dFprev); F(c->mb.slot8);
     F(c->d_model); F(c->d_learned_steps); F(c->d_fallbacks);
     F(c->d_hfeat); F(c->d_hlab); F(c->d_hvalid); F(c->d_feat); F(c->d_frame); F(c->d_plain_needed);
     F(c->cb.cell_of); F(c->cb.cell_cnt); F(c->cb.cell_start); F(c->cb.cursor); F(c->cb.list);
@@ -1085,7 +1083,6 @@ extern "C" int sfg_initialize(sfg_context* c) {
     CU(cudaMemset(tb.fluid_touched, 0, sizeof(int) * nch));
     CU(dalloc(&tb.resid_gate, nch));
     CU(dalloc(&tb.resid_plain, nch));
-    CU(dalloc(&tb.alpha, nch));     // written by k_mdf_alpha before each learned spread
     CU(cudaMemset(tb.resid_gate, 0, sizeof(unsigned) * nch));
     CU(cudaMemset(tb.resid_plain, 0, sizeof(unsigned) * nch));
     CU(dalloc(&c->d_learned_steps, nch));
@@ -1096,8 +1093,6 @@ extern "C" int sfg_initialize(sfg_context* c) {
     CU(dalloc(&c->mb.u0, M));
     CU(dalloc(&c->mb.dFsum, M));
     CU(dalloc(&c->mb.dFprev, M));
-    CU(dalloc(&c->mb.dFb, M));
-    CU(dalloc(&c->mb.rho2, M));
     CU(dalloc(&c->mb.slot8, 8LL * M));
     if (M > 0) {
         CU(cudaMemset(c->mb.u0, 0, sizeof(double2) * M));
@@ -1264,13 +1259,12 @@ static int enqueue_step_t(sfg_context* c, int p) {
                              c->d_status, st);
             mark(c, SFG_PHASE_IBM_SPREAD);
             launch_mdf_interp<S, R>(c->d_chans, c->M, c->mb, fp, c->tb, p, 2, MDF_LEARNED, st);
-            launch_mdf_alpha(c->d_chans, nch, c->mb, c->tb, st);
             mark(c, SFG_PHASE_MDF_INTERP);
             launch_plain_needed(c->d_chans, nch, c->tb, st);
             launch_spread<R>(c->d_chans, c->mb, c->tb, p, 2, MDF_LEARNED, 2, c->spread_grid,
                              c->d_status, st);
             mark(c, SFG_PHASE_IBM_SPREAD);
-            launches += 7;
+            launches += 6;
         }
         for (int k = 1; k < c->Kmax; ++k) {
             launch_mdf_interp<S, R>(c->d_chans, c->M, c->mb, fp, c->tb, p, k, MDF_PLAIN, st);
@@ -1533,7 +1527,6 @@ extern "C" int sfg_set_mdf_model(sfg_context* c, sfg_mlp* net, double residual_t
         const bool on = net && h.d.ibm_iterations >= 3 && h.d.cap_end > h.d.cap_begin;
         h.d.learned = on ? 1 : 0;
         h.d.mdf_threshold = (float)residual_threshold;
-        h.d.mdf_step_max = (float)c->mdf_step_max;
         any = any || on;
     }
     std::vector<ChannelDev> dv;
@@ -1544,25 +1537,6 @@ extern "C" int sfg_set_mdf_model(sfg_context* c, sfg_mlp* net, double residual_t
     c->any_learned = any;
     c->tb.plain_needed = any ? c->d_plain_needed : nullptr;
     drop_graphs(c);
-    return SFG_OK;
-}
-
-extern "C" int sfg_set_mdf_step_limit(sfg_context* c, double step_max) {
-    if (!c) return fail(SFG_ERR_ARG, "sfg_set_mdf_step_limit: null context");
-    if (!(step_max >= 0.0 && step_max <= 4.0))
-        return fail(SFG_ERR_ARG, "sfg_set_mdf_step_limit: the limit must be in [0, 4]");
-    c->mdf_step_max = step_max;
-    if (!c->initialized) return SFG_OK;
-    CU(cudaSetDevice(c->device));
-    CU(cudaStreamSynchronize(c->stream));
-    std::vector<ChannelDev> dv;
-    for (auto& h : c->ch) {
-        h.d.mdf_step_max = (float)step_max;
-        dv.push_back(h.d);
-    }
-    CU(cudaMemcpyAsync(c->d_chans, dv.data(), sizeof(ChannelDev) * dv.size(),
-                       cudaMemcpyHostToDevice, c->stream));
-    CU(cudaStreamSynchronize(c->stream));
     return SFG_OK;
 }
 

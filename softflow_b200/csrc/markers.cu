@@ -638,7 +638,7 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
          double* __restrict__ acc0, R* __restrict__ gsnap, R* __restrict__ fin, int sweep,
          int mode, const unsigned* __restrict__ resid_gate,
          const int* __restrict__ plain_needed, int* __restrict__ capped,
-         int* __restrict__ fluid_touched, const double* __restrict__ alpha, unsigned* status) {
+         int* __restrict__ fluid_touched, unsigned* status) {
     if (sweep > 0 && mode == MDF_PLAIN && plain_needed && !*plain_needed) return;
     extern __shared__ __align__(16) unsigned char spread_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -734,17 +734,8 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
         const A2* src = reinterpret_cast<const A2*>(
             (ch.learned && (mode == MDF_SEED || (mode == MDF_PLAIN && sweep == 1))) ? acc0 : acc);
         const size_t base2 = (size_t)slot * TILE_CELLS;
-        // the learned sweep starts from the membrane force plus the seed
-        // scaled by the channel's step length a*: acc0 + a* (acc - acc0)
-        const double al = (mode == MDF_LEARNED && alpha) ? alpha[chan] : 1.0;
-        const A2* src0 = reinterpret_cast<const A2*>(acc0);
         for (int c = lane; c < TILE_CELLS; c += 32) {
-            A2 a = sweep > 0 ? src[base2 + c] : APair<A>::make(0.0, 0.0);
-            if (al != 1.0) {                  // warp-uniform
-                const A2 a0 = src0[base2 + c];
-                a.x = a0.x + (A)al * (a.x - a0.x);
-                a.y = a0.y + (A)al * (a.y - a0.y);
-            }
+            const A2 a = sweep > 0 ? src[base2 + c] : APair<A>::make(0.0, 0.0);
             const A vx = a.x, vy = a.y;
             ax[acc_at(c)] = vx;
             ay[acc_at(c)] = vy;
@@ -1028,15 +1019,6 @@ __global__ void k_mdf_interp(const ChannelDev* __restrict__ chans, int M, Marker
     const double dux = v.x - u.x, duy = v.y - u.y;
     const double2 d = make_double2(dux * (2.0 * rho_local), duy * (2.0 * rho_local));
     mb.dF[m] = d;
-    if (mode == MDF_LEARNED) {
-        // the velocity change the seed caused at the marker (force units)
-        // and the nearest-node factor; k_mdf_alpha takes the step length
-        // along the seed, the correction and the gate residual from them
-        const double2 u0 = mb.u0[m];
-        mb.dFb[m] = make_double2((u.x - u0.x) * (2.0 * rho_local), (u.y - u0.y) * (2.0 * rho_local));
-        mb.rho2[m] = 2.0 * rho_local;
-        return;
-    }
     if (mode == MDF_PLAIN && sweep == 1) {
         mb.u0[m] = u;
         mb.dFsum[m] = d;
@@ -1045,90 +1027,9 @@ __global__ void k_mdf_interp(const ChannelDev* __restrict__ chans, int M, Marker
         mb.dFsum[m] = make_double2(s0.x + d.x, s0.y + d.y);
     }
     // the per-channel residual max, one atomic per channel and warp
-    const bool want = sweep == ch.ibm_iterations - 1;
-    warp_max_resid(resid_plain, chan, want, sqrt(dux * dux + duy * duy));
-}
-
-// Step length along the learned seed, per channel (one block each).  After
-// the seed spread the no-slip residual of every marker is linear in a scale
-// a of the seed:
-//   r(a) = r0 - a e,   r0 = U_target - U(membrane force only),
-//                      e  = U(with the seed) - U(membrane force only),
-// (the interpolation is linear in the force; the tile moments do not change
-// during the sweeps), so a* = sum r0 . e / sum |e|^2 minimises sum |r(a)|^2
-// over the channel's markers.  The network's prediction is the search
-// direction, a* the step along it, limited to [0, mdf_step_max] (default 1:
-// the seed is shrunk where that lowers the slip, never lengthened).  The
-// unconstrained step, about 1.4 on the ensemble, drives the slip far below
-// the plain iteration's in one step, but a step beyond the prediction (1.05
-// and more, measured) makes the coupling leave the plain solution within a
-// few hundred steps.  a* = 1 when the seed moves nothing.  Then, per marker, the last sweep's correction 2 rho r(a*), the
-// step's summed correction a* seed + that correction, and the channel's gate
-// residual max |r(a*)|.  Markers in a fixed order and fixed-shape tree sums:
-// deterministic, and a channel's result does not depend on the others.
-constexpr int ALPHA_THREADS = 256;
-__global__ void __launch_bounds__(ALPHA_THREADS)
-k_mdf_alpha(const ChannelDev* __restrict__ chans, MarkerBufs mb, double* __restrict__ alpha,
-            unsigned* __restrict__ resid_gate) {
-    __shared__ double s_a[ALPHA_THREADS], s_b[ALPHA_THREADS];
-    __shared__ unsigned s_r[ALPHA_THREADS];
-    const int c = blockIdx.x, t = threadIdx.x;
-    const ChannelDev& ch = chans[c];
-    if (!(ch.learned && ch.ibm_iterations > 1 && ch.mk_end > ch.mk_begin)) {
-        if (t == 0) alpha[c] = 1.0;
-        return;                                 // block-uniform
-    }
-    double sa = 0.0, sb = 0.0;
-    for (int m = ch.mk_begin + t; m < ch.mk_end; m += ALPHA_THREADS) {
-        const double k = mb.rho2[m];
-        if (!mb.valid[m] || !(k > 0.0)) continue;
-        const double2 a = mb.dF[m], b = mb.dFb[m];
-        const double ex = b.x / k, ey = b.y / k;
-        sa += ((a.x + b.x) / k) * ex + ((a.y + b.y) / k) * ey;
-        sb += ex * ex + ey * ey;
-    }
-    s_a[t] = sa;
-    s_b[t] = sb;
-    __syncthreads();
-    for (int o = ALPHA_THREADS / 2; o > 0; o >>= 1) {
-        if (t < o) {
-            s_a[t] += s_a[t + o];
-            s_b[t] += s_b[t + o];
-        }
-        __syncthreads();
-    }
-    double al = 1.0;
-    if (s_b[0] > 0.0) {
-        const double q = s_a[0] / s_b[0];
-        if (isfinite(q)) al = fmin(fmax(q, 0.0), (double)ch.mdf_step_max);
-    }
-    unsigned rmax = 0u;
-    for (int m = ch.mk_begin + t; m < ch.mk_end; m += ALPHA_THREADS) {
-        const double k = mb.rho2[m];
-        if (!mb.valid[m]) continue;
-        const double2 a = mb.dF[m], b = mb.dFb[m];
-        const double2 F = make_double2(a.x + (1.0 - al) * b.x, a.y + (1.0 - al) * b.y);
-        mb.dF[m] = F;
-        const double2 seed = mb.dFsum[m];
-        mb.dFsum[m] = make_double2(al * seed.x + F.x, al * seed.y + F.y);
-        const float r = k > 0.0 ? (float)(sqrt(F.x * F.x + F.y * F.y) / k) : 0.0f;
-        rmax = max(rmax, isnan(r) ? 0x7fc00000u : __float_as_uint(r));
-    }
-    s_r[t] = rmax;
-    __syncthreads();
-    for (int o = ALPHA_THREADS / 2; o > 0; o >>= 1) {
-        if (t < o) s_r[t] = max(s_r[t], s_r[t + o]);
-        __syncthreads();
-    }
-    if (t == 0) {
-        alpha[c] = al;
-        resid_gate[c] = s_r[0];
-    }
-}
-
-void launch_mdf_alpha(const ChannelDev* chans, int nch, const MarkerBufs& mb, TileBufs& tb,
-                      cudaStream_t st) {
-    if (nch > 0) k_mdf_alpha<<<nch, ALPHA_THREADS, 0, st>>>(chans, mb, tb.alpha, tb.resid_gate);
+    const bool want = mode == MDF_LEARNED || sweep == ch.ibm_iterations - 1;
+    warp_max_resid(mode == MDF_LEARNED ? resid_gate : resid_plain, chan, want,
+                   sqrt(dux * dux + duy * duy));
 }
 
 // Whether any channel needs the plain correction sweeps this step: a forcing
@@ -1577,7 +1478,7 @@ void launch_spread(const ChannelDev* chans, const MarkerBufs& mb, TileBufs& tb, 
     k_spread<R><<<grid, SPREAD_WARPS * 32, spread_smem<R>(), st>>>(
         chans, tb.slot_info, tb.n_slots, tb.spread_ctr + launch_idx, tb.list, mb,
         tb.acc, tb.acc0, static_cast<R*>(tb.gsnap), static_cast<R*>(tb.fin[parity]), sweep, mode,
-        tb.resid_gate, tb.plain_needed, tb.capped, tb.fluid_touched, tb.alpha, status);
+        tb.resid_gate, tb.plain_needed, tb.capped, tb.fluid_touched, status);
 }
 template void launch_spread<double>(const ChannelDev*, const MarkerBufs&, TileBufs&, int, int,
                                     int, int, int, unsigned*, cudaStream_t);

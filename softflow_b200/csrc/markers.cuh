@@ -34,8 +34,6 @@ struct MarkerBufs {
     double2* u0;        // velocity interpolated after the membrane-force spread
     double2* dFsum;     // forcing correction of this step summed over its sweeps
     double2* dFprev;    // previous step's correction before its last sweep
-    double2* dFb;       // learned sweep: 2 rho (U after the seed - U before it)
-    double* rho2;       // learned sweep: 2 rho at the marker's nearest node
     // force-tile slots of the marker's stencil, this step: [M][2][4] =
     // [row tile (of the first / last stencil row)][stencil column sx]
     int* slot8;

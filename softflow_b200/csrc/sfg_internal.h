@@ -50,7 +50,6 @@ struct TileBufs {
     int* plain_needed = nullptr;  // [1] set when some channel needs the plain sweeps; null
                                   // (always run them) unless a channel is learned
     unsigned* resid_gate = nullptr;   // [nchan] learned form's no-slip residual (float bits)
-    double* alpha = nullptr;          // [nchan] learned form's step length along the seed
     unsigned* resid_plain = nullptr;  // [nchan] plain iteration's last-sweep residual
 };
 
@@ -106,10 +105,6 @@ void launch_mdf_learned(const ChannelDev* chans, const CapsuleDev* caps, int M,
 void launch_harvest(const ChannelDev* chans, const CapsuleDev* caps, int M, const MarkerBufs& mb,
                     float* feat, float* label, int* valid, cudaStream_t st);
 cudaError_t prepare_mdf_learned();
-// Step length along the learned seed per channel, the learned sweep's
-// correction and the gate residual (after the learned sweep's interpolation).
-void launch_mdf_alpha(const ChannelDev* chans, int nch, const MarkerBufs& mb, TileBufs& tb,
-                      cudaStream_t st);
 // Sets tb.plain_needed from the gate residuals (learned contexts).
 void launch_plain_needed(const ChannelDev* chans, int nch, TileBufs& tb, cudaStream_t st);
 // Moments of the step's force tiles (before the first forcing sweep).

@@ -1011,13 +1011,6 @@ class Ensemble:
                                            float(threshold)))
         self._learned_net = net     # keeps the trainer object alive
 
-    def setMDFStepLimit(self, step_max: float = 1.0):
-        """Upper limit of the learned form's step length along the network's
-        seed (the residual-minimising step, per channel, is clamped to
-        [0, step_max]; the default 1 never lengthens the prediction)."""
-        ctx = self._need()
-        L.check(ctx._lib.sfg_set_mdf_step_limit(ctx._h, float(step_max)))
-
     def mdfStats(self, chan: int = 0) -> dict:
         """Last step's no-slip residuals (learned gate, plain iteration) and
         the cumulative learned / fallback step counts of a channel."""
