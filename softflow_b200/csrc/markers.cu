@@ -588,11 +588,16 @@ template <> struct APair<float> {
         return make_float2((float)x, (float)y);
     }
 };
+// Markers staged per chunk on the wide path: four lanes per marker, one
+// stencil row each.  A staged point goes to the slot of the lane that owns
+// its cell (lane (a, b) owns the tile cells whose column is a mod 8 and row
+// b mod 4): its contribution and its accumulator index.
+constexpr int WIDE_CHUNK = 8;
 template <typename A>
 struct SpreadChunkWide {
-    typename APair<A>::T c[SPREAD_CHUNK][17];   // point k + 4 sy (padded: conflict-free)
-    unsigned mask[SPREAD_CHUNK];
-    int org[SPREAD_CHUNK];         // (column origin + 64) | (row origin + 64) << 8
+    typename APair<A>::T v[WIDE_CHUNK][33];    // [marker][owner lane] (padded row)
+    unsigned short cell[WIDE_CHUNK][32];       // accumulator index of that point
+    unsigned mask[WIDE_CHUNK];                 // owner lanes holding a point
 };
 // The tile accumulators keep rows of TILE_W + 4 doubles: the 4 x 4 stencil
 // points of a marker (4 consecutive rows and columns) then fall on 16
@@ -747,19 +752,23 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
         __syncwarp();
         const int la = lane & 7, lb = lane >> 3;
         if (nx > TILE_W) {
-            // Markers in list order, SPREAD_CHUNK at a time.  Staging: lanes
-            // j and j + 16 take marker j of the chunk and evaluate its stencil
-            // rows 2h, 2h + 1 (h = lane / 16): the weights w = phi(rx)
-            // phi(ry), the contributions (f w) ds and the lanes owning each
-            // valid point.  Lane (a, b) = (lane & 7, lane >> 3) owns the tile
-            // cells whose local column is a mod 8 and row b mod 4; the 4 x 4
+            // Markers in list order, WIDE_CHUNK at a time.  Staging: lanes
+            // 4j .. 4j + 3 take marker j of the chunk, one stencil row each
+            // (sy = lane & 3), and evaluate its four points: the weight
+            // w = phi(rx) phi(ry), the contribution (f w) ds and the lane that
+            // owns the point's cell, into whose slot the contribution and the
+            // cell's accumulator index go.  Lane (a, b) = (lane & 7, lane >> 3)
+            // owns the tile cells of column a mod 8 and row b mod 4; the 4 x 4
             // stencil has 4 consecutive columns and rows, so its 16 points
             // fall on 16 distinct lanes.  Then every lane adds its own point of
             // each marker to its own cell, marker after marker, so every cell
-            // receives its terms in the reference's order.
-            const int jm = lane & 15, hh = lane >> 4;
-            double2 rf = make_double2(0.0, 0.0), rw0 = rf, rw1 = rf, rv = rf;
-            double rds = 0.0;
+            // receives its terms in the reference's order.  A lane with no
+            // point of a marker adds zero to a padding cell of its own (the
+            // accumulator rows carry four padding columns: 8 x 4 = 32 cells,
+            // one per lane), so the additions carry no branches.
+            const int jm = lane >> 2, sy = lane & 3;
+            double2 rf = make_double2(0.0, 0.0), rw0 = rf, rw1 = rf;
+            double rds = 0.0, rwy = 0.0;
             int rix = 0, riy = 0;
             auto fetch = [&](int c) {
                 if (c + jm < cnt) {
@@ -769,111 +778,79 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
                     riy = mb.iy0[m];
                     rds = mb.ds[m];
                     const double2* wx2 = reinterpret_cast<const double2*>(mb.wx + 4 * (size_t)m);
-                    const double2* wy2 = reinterpret_cast<const double2*>(mb.wy + 4 * (size_t)m);
                     rw0 = wx2[0];
                     rw1 = wx2[1];
-                    rv = wy2[hh];
+                    rwy = mb.wy[4 * (size_t)m + sy];
                 }
             };
+            const int pad = (lane >> 2) * ACC_W + TILE_W + (lane & 3);   // this lane's padding cell
             fetch(0);
-            for (int c0 = 0; c0 < cnt; c0 += SPREAD_CHUNK) {
-                const int nb = cnt - c0 < SPREAD_CHUNK ? cnt - c0 : SPREAD_CHUNK;
+            for (int c0 = 0; c0 < cnt; c0 += WIDE_CHUNK) {
+                const int nb = cnt - c0 < WIDE_CHUNK ? cnt - c0 : WIDE_CHUNK;
                 __syncwarp();
-                unsigned mask = 0u;
-                int o = 0;
-                const int r0 = riy - 1 - y0;
+                unsigned bits = 0u;
                 if (jm < nb) {
                     const bool ok = !(isnan(rf.x) || isnan(rf.y));
+                    const int cyl = riy - 1 + sy - y0, iy = riy - 1 + sy;
+                    const bool vrow = ok && cyl >= 0 && cyl < TILE_H && iy >= 0 && iy < ny;
                     const double wxk[4] = {rw0.x, rw0.y, rw1.x, rw1.y};
-                    bool vk[4];
-                    bool have = false;
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         int jx = rix - 1 + k;
                         if (jx < 0) jx += nx;
                         if (jx >= nx) jx -= nx;
                         const int cl = jx - x0;
-                        vk[k] = jx >= 0 && jx < nx && cl >= 0 && cl < TILE_W;
-                        if (vk[k] && !have) {
-                            o = cl - k;
-                            have = true;
-                        }
-                    }
-#pragma unroll
-                    for (int t = 0; t < 2; ++t) {
-                        const int sy = 2 * hh + t;
-                        const int cyl = r0 + sy, iy = cyl + y0;
-                        const bool vrow = ok && cyl >= 0 && cyl < TILE_H && iy >= 0 && iy < ny;
-                        const double wy = t == 0 ? rv.x : rv.y;
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            const double w = wxk[k] * wy;
-                            if (vrow && vk[k] && w > 1e-15) {
-                                // FP64: (f w) ds in the reference's order; the
-                                // float form rounds f, w, ds once and works in float
-                                if constexpr (sizeof(A) == 8)
-                                    W.ck.w.c[jm][k + 4 * sy] =
-                                        APair<A>::make(rf.x * w * rds, rf.y * w * rds);
-                                else
-                                    W.ck.w.c[jm][k + 4 * sy] = make_float2(
-                                        (float)rf.x * (float)w * (float)rds,
-                                        (float)rf.y * (float)w * (float)rds);
-                                mask |= 1u << (((o + k) & 7) + 8 * (cyl & 3));
-                            }
+                        const double w = wxk[k] * rwy;
+                        if (vrow && jx >= 0 && jx < nx && cl >= 0 && cl < TILE_W && w > 1e-15) {
+                            const int t = (cl & 7) + 8 * (cyl & 3);
+                            // FP64: (f w) ds in the reference's order; the
+                            // float form rounds f, w, ds once and works in float
+                            if constexpr (sizeof(A) == 8)
+                                W.ck.w.v[jm][t] = APair<A>::make(rf.x * w * rds, rf.y * w * rds);
+                            else
+                                W.ck.w.v[jm][t] = make_float2((float)rf.x * (float)w * (float)rds,
+                                                              (float)rf.y * (float)w * (float)rds);
+                            W.ck.w.cell[jm][t] = (unsigned short)(cyl * ACC_W + cl);
+                            bits |= 1u << t;
                         }
                     }
                 }
-                mask |= __shfl_xor_sync(0xffffffffu, mask, 16);
-                if (hh == 0 && jm < nb) {
-                    W.ck.w.mask[jm] = mask;
-                    W.ck.w.org[jm] = (o + 64) | ((r0 + 64) << 8);
-                }
+                bits |= __shfl_xor_sync(0xffffffffu, bits, 1);
+                bits |= __shfl_xor_sync(0xffffffffu, bits, 2);
+                if (sy == 0 && jm < nb) W.ck.w.mask[jm] = bits;
                 __syncwarp();
-                fetch(c0 + SPREAD_CHUNK);   // in flight while this chunk is added
-                // this lane's point of marker j: cell index and contribution
+                fetch(c0 + WIDE_CHUNK);   // in flight while this chunk is added
+                const A2 zero = APair<A>::make(0.0, 0.0);
+                // this lane's point of marker j (or zero into its padding cell)
                 auto point = [&](int j, int& c, A2& v) {
-                    const int org = W.ck.w.org[j];
-                    const int oj = (org & 0xFF) - 64, rj = (org >> 8) - 64;
-                    const int k = (la - oj) & 7, sy = (lb - rj) & 3;
-                    v = W.ck.w.c[j][k + 4 * sy];
-                    c = (rj + sy) * ACC_W + oj + k;
+                    const bool h = (W.ck.w.mask[j] >> lane) & 1u;
+                    const int ci = W.ck.w.cell[j][lane];
+                    const A2 vi = W.ck.w.v[j][lane];
+                    c = h ? ci : pad;
+                    v = h ? vi : zero;
                 };
                 int j = 0;
                 // two markers at a time: both cells are read before either is
                 // written, the second addition taking the first's sum when
                 // both points are the same cell (same order, same rounding)
                 for (; j + 1 < nb; j += 2) {
-                    const bool h0 = (W.ck.w.mask[j] >> lane) & 1u;
-                    const bool h1 = (W.ck.w.mask[j + 1] >> lane) & 1u;
-                    int c0i = 0, c1i = 0;
-                    A2 v0 = APair<A>::make(0.0, 0.0), v1 = v0;
-                    if (h0) point(j, c0i, v0);
-                    if (h1) point(j + 1, c1i, v1);
-                    A a0x = 0, a0y = 0, a1x = 0, a1y = 0;
-                    if (h0) {
-                        a0x = ax[c0i];
-                        a0y = ay[c0i];
-                    }
-                    if (h1) {
-                        a1x = ax[c1i];
-                        a1y = ay[c1i];
-                    }
-                    if (h0) {
-                        a0x += v0.x;
-                        a0y += v0.y;
-                        ax[c0i] = a0x;
-                        ay[c0i] = a0y;
-                    }
-                    if (h1) {
-                        if (h0 && c1i == c0i) {
-                            a1x = a0x;
-                            a1y = a0y;
-                        }
-                        ax[c1i] = a1x + v1.x;
-                        ay[c1i] = a1y + v1.y;
-                    }
+                    int c0i, c1i;
+                    A2 v0, v1;
+                    point(j, c0i, v0);
+                    point(j + 1, c1i, v1);
+                    A a0x = ax[c0i], a0y = ay[c0i];
+                    A a1x = ax[c1i], a1y = ay[c1i];
+                    a0x += v0.x;
+                    a0y += v0.y;
+                    ax[c0i] = a0x;
+                    ay[c0i] = a0y;
+                    const bool same = c1i == c0i;
+                    a1x = same ? a0x : a1x;
+                    a1y = same ? a0y : a1y;
+                    ax[c1i] = a1x + v1.x;
+                    ay[c1i] = a1y + v1.y;
                 }
-                if (j < nb && ((W.ck.w.mask[j] >> lane) & 1u)) {
+                if (j < nb) {
                     int c;
                     A2 v;
                     point(j, c, v);
