@@ -968,6 +968,192 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
     }
 }
 
+// The spread of the FP32-arithmetic modes (FP32 and FP16-shifted storage):
+// the same contributions as k_spread<float> ((float)f (float)w (float)ds for
+// each stencil point with w > 1e-15), summed per cell exactly in fixed point
+// instead of in float.  Integer addition does not depend on the order of the
+// terms, so the lanes of a warp add any markers' points in any order, with
+// 32-bit shared-memory atomics, and the result is the same on every run, in
+// every launch shape and whether a channel runs alone or in an ensemble; the
+// marker lists need no sort.  Each value is v = q 2^-38 with the integer q
+// split into a low part of 20 bits (unsigned, in [0, 2^20)) and a high part
+// (signed): a cell takes at most SPREAD_LIST_MAX + 1 low parts per sweep
+// (below 2^32), and the high parts hold sums up to 2^13 in magnitude, far
+// beyond any lattice force.  The sum is rounded to float once, where it is
+// written out.  FP64 contexts keep k_spread (the reference's serial order,
+// bit for bit).
+constexpr int FX_LO_BITS = 20;
+constexpr float FX_SCALE = 274877906944.0f;          // 2^38
+constexpr float FX_UNSCALE = 1.0f / 274877906944.0f;  // 2^-38 (exact)
+struct SpreadFxWarp {
+    unsigned lo[2][ACC_CELLS];        // x, y; rows of ACC_W cells
+    int hi[2][ACC_CELLS];
+};
+constexpr size_t spread_fx_smem() { return sizeof(SpreadFxWarp) * SPREAD_WARPS; }
+__device__ __forceinline__ long long fx_quant(float v) { return __float2ll_rn(v * FX_SCALE); }
+__device__ __forceinline__ unsigned fx_lo(long long q) {
+    return (unsigned)(q & ((1LL << FX_LO_BITS) - 1));
+}
+__device__ __forceinline__ int fx_hi(long long q) { return (int)(q >> FX_LO_BITS); }
+__device__ __forceinline__ float fx_value(unsigned lo, int hi) {
+    return __ll2float_rn((long long)hi * (1LL << FX_LO_BITS) + (long long)lo) * FX_UNSCALE;
+}
+
+__global__ void __launch_bounds__(SPREAD_WARPS * 32, 4)
+k_spread_fx(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot_info,
+            const int* __restrict__ n_slots_p, const int* __restrict__ list, MarkerBufs mb,
+            double* __restrict__ acc, double* __restrict__ acc0, float* __restrict__ gsnap,
+            float* __restrict__ fin, int sweep, int mode, const unsigned* __restrict__ resid_gate,
+            const int* __restrict__ plain_needed, int* __restrict__ capped,
+            int* __restrict__ fluid_touched, unsigned* status) {
+    if (sweep > 0 && mode == MDF_PLAIN && plain_needed && !*plain_needed) return;
+    extern __shared__ __align__(16) unsigned char spread_fx_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    SpreadFxWarp& W = reinterpret_cast<SpreadFxWarp*>(spread_fx_raw)[warp];
+    const int n_slots = *n_slots_p;
+    const int nwarps = gridDim.x * SPREAD_WARPS;
+    int next = blockIdx.x * SPREAD_WARPS + warp;
+    SlotInfo nfo{};
+    if (next < n_slots) nfo = slot_info[next];
+    while (next < n_slots) {
+        const int slot = next;
+        const SlotInfo si = nfo;
+        next += nwarps;
+        if (next < n_slots) nfo = slot_info[next];
+        const int chan = si.chan;
+        const ChannelDev& ch = chans[chan];
+        const int K = ch.ibm_iterations > 1 ? ch.ibm_iterations : 1;
+        if (sweep >= K) continue;  // warp-uniform
+        if (sweep > 0 && !mdf_active(ch, mode, resid_gate, chan)) continue;  // sweep 0: all
+        const int nx = si.nx, ny = si.ny;
+        const int x0 = si.x0, y0 = si.y0;
+        int cnt = si.cnt;
+        if (cnt > SPREAD_LIST_MAX) {
+            if (lane == 0) atomicOr(status, (unsigned)ST_LIST_OVERFLOW);
+            cnt = SPREAD_LIST_MAX;
+        }
+        const int* lst = list + si.off;
+        const size_t base = (size_t)slot * 2 * TILE_CELLS;
+        const bool last = mode == MDF_LEARNED ? true : (mode == MDF_SEED ? false : sweep == K - 1);
+        // a learned channel's membrane-only force lives in acc0 only (k_spread)
+        const float2* src = reinterpret_cast<const float2*>(
+            (ch.learned && (mode == MDF_SEED || (mode == MDF_PLAIN && sweep == 1))) ? acc0 : acc);
+        const size_t base2 = (size_t)slot * TILE_CELLS;
+        for (int c = lane; c < TILE_CELLS; c += 32) {
+            const float2 a = sweep > 0 ? src[base2 + c] : make_float2(0.f, 0.f);
+            const long long qx = fx_quant(a.x), qy = fx_quant(a.y);
+            const int i = acc_at(c);
+            W.lo[0][i] = fx_lo(qx);
+            W.hi[0][i] = fx_hi(qx);
+            W.lo[1][i] = fx_lo(qy);
+            W.hi[1][i] = fx_hi(qy);
+            if (last && K > 1) {
+                gsnap[base + c] = a.x;
+                gsnap[base + TILE_CELLS + c] = a.y;
+            }
+        }
+        __syncwarp();
+        // four lanes per marker, one stencil row each, eight markers a pass;
+        // the next pass's marker data is loaded before this pass's points
+        const int jm = lane >> 2, sy = lane & 3;
+        struct Mk {
+            double2 f, w0, w1;
+            double ds, wy;
+            int ix, iy;
+        };
+        auto fetch = [&](int c, Mk& k) {
+            if (c + jm < cnt) {
+                const int m = lst[c + jm];
+                k.f = sweep == 0 ? mb.frc[m] : mb.dF[m];
+                k.ix = mb.ix0[m];
+                k.iy = mb.iy0[m];
+                k.ds = mb.ds[m];
+                const double2* wx2 = reinterpret_cast<const double2*>(mb.wx + 4 * (size_t)m);
+                k.w0 = wx2[0];
+                k.w1 = wx2[1];
+                k.wy = mb.wy[4 * (size_t)m + sy];
+            }
+        };
+        Mk cur{}, nxt{};
+        fetch(0, cur);
+        for (int c0 = 0; c0 < cnt; c0 += 8) {
+            fetch(c0 + 8, nxt);
+            if (c0 + jm < cnt) {
+                const bool ok = !(isnan(cur.f.x) || isnan(cur.f.y));
+                const int iy = cur.iy - 1 + sy, cyl = iy - y0;
+                const bool vrow = ok && cyl >= 0 && cyl < TILE_H && iy >= 0 && iy < ny;
+                const double wxk[4] = {cur.w0.x, cur.w0.y, cur.w1.x, cur.w1.y};
+                const float fx = (float)cur.f.x, fy = (float)cur.f.y, ds = (float)cur.ds;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    int jx = cur.ix - 1 + k;
+                    if (jx < 0) jx += nx;
+                    if (jx >= nx) jx -= nx;
+                    const int cl = jx - x0;
+                    const double w = wxk[k] * cur.wy;
+                    if (vrow && jx >= 0 && jx < nx && cl >= 0 && cl < TILE_W && w > 1e-15) {
+                        const float wf = (float)w;
+                        const long long qx = fx_quant(fx * wf * ds), qy = fx_quant(fy * wf * ds);
+                        const int i = cyl * ACC_W + cl;
+                        atomicAdd(&W.lo[0][i], fx_lo(qx));
+                        atomicAdd(&W.hi[0][i], fx_hi(qx));
+                        atomicAdd(&W.lo[1][i], fx_lo(qy));
+                        atomicAdd(&W.hi[1][i], fx_hi(qy));
+                    }
+                }
+            }
+            cur = nxt;
+        }
+        __syncwarp();
+        if (!last) {
+            float2* out = reinterpret_cast<float2*>((sweep == 0 && ch.learned) ? acc0 : acc);
+            for (int c = lane; c < TILE_CELLS; c += 32) {
+                const int i = acc_at(c);
+                out[base2 + c] =
+                    make_float2(fx_value(W.lo[0][i], W.hi[0][i]), fx_value(W.lo[1][i], W.hi[1][i]));
+            }
+            __syncwarp();
+            continue;
+        }
+        // finalize: body force on FLUID cells, then the force cap (as k_spread)
+        int n_cap = 0, n_fluid = 0;
+        const double Fm = ch.max_force, Fm2 = Fm * Fm;
+        const bool body = (ch.body_fx != 0.0 || ch.body_fy != 0.0);
+        for (int c = lane; c < TILE_CELLS; c += 32) {
+            const int jx = x0 + (c % TILE_W), jy = y0 + (c / TILE_W);
+            const int i = acc_at(c);
+            double vx = (double)fx_value(W.lo[0][i], W.hi[0][i]);
+            double vy = (double)fx_value(W.lo[1][i], W.hi[1][i]);
+            if (jx < nx && jy < ny) {
+                const bool fluid = cell_kind(ch, jx, jy) == CK_FLUID;
+                if (fluid && body) {
+                    vx += ch.body_fx;
+                    vy += ch.body_fy;
+                }
+                const double f2 = vx * vx + vy * vy;
+                if (f2 > Fm2) {
+                    const double sc = Fm / sqrt(f2);
+                    vx *= sc;
+                    vy *= sc;
+                    ++n_cap;
+                }
+                n_fluid += fluid ? 1 : 0;
+            }
+            fin[base + c] = (float)vx;
+            fin[base + TILE_CELLS + c] = (float)vy;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            n_cap += __shfl_down_sync(0xffffffffu, n_cap, o);
+            n_fluid += __shfl_down_sync(0xffffffffu, n_fluid, o);
+        }
+        if (lane == 0) {
+            if (n_cap) atomicAdd(&capped[chan], n_cap);
+            if (n_fluid) atomicAdd(&fluid_touched[chan], n_fluid);
+        }
+        __syncwarp();
+    }
+}
+
 // MDF correction of one sweep (immersed_boundary.cpp:231-286): interpolate
 // u = (j + F/2)/rho with the force spread so far, then
 // dF = 2 rho(nearest node) (U_prev - U_interp).  Also keeps the step's total
@@ -1135,9 +1321,9 @@ int spread_blocks_per_sm(bool fp64) {
         fp64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_spread<double>,
                                                              SPREAD_WARPS * 32,
                                                              spread_smem<double>())
-             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_spread<float>,
+             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_spread_fx,
                                                              SPREAD_WARPS * 32,
-                                                             spread_smem<float>());
+                                                             spread_fx_smem());
     if (e != cudaSuccess || b < 1) b = 1;
     return b;
 }
@@ -1147,8 +1333,8 @@ cudaError_t prepare_spread() {
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)spread_smem<double>());
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_spread<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)spread_smem<float>());
+        e = cudaFuncSetAttribute(k_spread_fx, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)spread_fx_smem());
     return e;
 }
 
@@ -1452,10 +1638,17 @@ template <typename R>
 void launch_spread(const ChannelDev* chans, const MarkerBufs& mb, TileBufs& tb, int parity,
                    int sweep, int mode, int launch_idx, int grid, unsigned* status,
                    cudaStream_t st) {
-    k_spread<R><<<grid, SPREAD_WARPS * 32, spread_smem<R>(), st>>>(
-        chans, tb.slot_info, tb.n_slots, tb.spread_ctr + launch_idx, tb.list, mb,
-        tb.acc, tb.acc0, static_cast<R*>(tb.gsnap), static_cast<R*>(tb.fin[parity]), sweep, mode,
-        tb.resid_gate, tb.plain_needed, tb.capped, tb.fluid_touched, status);
+    if constexpr (sizeof(R) == 4) {
+        k_spread_fx<<<grid, SPREAD_WARPS * 32, spread_fx_smem(), st>>>(
+            chans, tb.slot_info, tb.n_slots, tb.list, mb, tb.acc, tb.acc0,
+            static_cast<float*>(tb.gsnap), static_cast<float*>(tb.fin[parity]), sweep, mode,
+            tb.resid_gate, tb.plain_needed, tb.capped, tb.fluid_touched, status);
+    } else {
+        k_spread<R><<<grid, SPREAD_WARPS * 32, spread_smem<R>(), st>>>(
+            chans, tb.slot_info, tb.n_slots, tb.spread_ctr + launch_idx, tb.list, mb, tb.acc,
+            tb.acc0, static_cast<R*>(tb.gsnap), static_cast<R*>(tb.fin[parity]), sweep, mode,
+            tb.resid_gate, tb.plain_needed, tb.capped, tb.fluid_touched, status);
+    }
 }
 template void launch_spread<double>(const ChannelDev*, const MarkerBufs&, TileBufs&, int, int,
                                     int, int, int, unsigned*, cudaStream_t);
