@@ -31,6 +31,13 @@ static_assert(opp_of(5) == 7 && opp_of(6) == 8 && opp_of(7) == 5 && opp_of(8) ==
 constexpr int TILE_W = 32;
 constexpr int TILE_H = 8;
 constexpr int TILE_CELLS = TILE_W * TILE_H;
+// Classes of force tiles by list length for the spread's work order: the
+// passes of 8 markers a tile takes, the last class open-ended.
+constexpr int SLOT_CLASSES = 16;
+__host__ __device__ __forceinline__ int slot_class(int cnt) {
+    const int p = (cnt + 7) >> 3;
+    return p < SLOT_CLASSES - 1 ? p : SLOT_CLASSES - 1;
+}
 
 // Storage precision of the populations.
 enum Precision : int { PREC_FP64 = 0, PREC_FP32 = 1, PREC_FP16S = 2 };

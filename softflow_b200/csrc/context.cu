@@ -426,7 +426,7 @@ static void free_all(sfg_context* c) {
     F(c->tb.tile_chan); F(c->tb.tile_flag); F(c->tb.tile_cnt); F(c->tb.cursor);
     F(c->tb.slot_scan); F(c->tb.list_off); F(c->tb.slot_tile); F(c->tb.n_slots);
     F(c->tb.list); F(c->tb.scan_tmp); F(c->tb.acc); F(c->tb.gsnap); F(c->tb.capped);
-    F(c->tb.fluid_touched); F(c->tb.acc0); F(c->tb.mom); F(c->tb.slot_info); F(c->tb.spread_ctr); F(c->tb.resid_gate); F(c->tb.resid_plain);
+    F(c->tb.fluid_touched); F(c->tb.acc0); F(c->tb.mom); F(c->tb.slot_info); F(c->tb.slot_order); F(c->tb.slot_rank); F(c->tb.cls_cnt); F(c->tb.spread_ctr); F(c->tb.resid_gate); F(c->tb.resid_plain);
     F(c->mb.u0); F(c->mb.dFsum); F(c->mb.dFprev); F(c->mb.slot8);
     F(c->d_model); F(c->d_learned_steps); F(c->d_fallbacks);
     F(c->d_hfeat); F(c->d_hlab); F(c->d_hvalid); F(c->d_feat); F(c->d_frame); F(c->d_plain_needed);
@@ -1068,6 +1068,9 @@ extern "C" int sfg_initialize(sfg_context* c) {
     }
     CU(dalloc(&tb.slot_tile, tb.max_slots));
     CU(dalloc(&tb.slot_info, tb.max_slots));
+    CU(dalloc(&tb.slot_order, tb.max_slots));
+    CU(dalloc(&tb.slot_rank, tb.max_slots));
+    CU(dalloc(&tb.cls_cnt, SLOT_CLASSES));
     tb.n_spread_ctr = c->Kmax + 3;
     CU(dalloc(&tb.spread_ctr, tb.n_spread_ctr));
     CU(dalloc(&tb.n_slots, 1));
@@ -1225,7 +1228,7 @@ static int enqueue_step_t(sfg_context* c, int p) {
             launch_spread<R>(c->d_chans, c->mb, c->tb, p, 0, MDF_PLAIN, 0, c->spread_grid,
                              c->d_status, st);
             if (c->Kmax > 1) CU(cudaStreamWaitEvent(st, c->ev_mom, 0));
-            launches += 1 + (c->ncells > 0 ? 7 : 1) + 9 + 1 + (c->Kmax > 1 ? 1 : 0);
+            launches += 1 + (c->ncells > 0 ? 7 : 1) + 10 + 1 + (c->Kmax > 1 ? 1 : 0);
         } else {
             launch_membrane(c->d_caps, c->NC, c->mb, c->d_has_prev, c->maxn, c->d_status, st);
             mark(c, SFG_PHASE_MEMBRANE);
@@ -1241,7 +1244,7 @@ static int enqueue_step_t(sfg_context* c, int p) {
             launch_spread<R>(c->d_chans, c->mb, c->tb, p, 0, MDF_PLAIN, 0, c->spread_grid,
                              c->d_status, st);
             mark(c, SFG_PHASE_IBM_SPREAD);
-            launches += 1 + (c->ncells > 0 ? 7 : 1) + 9 + 1;
+            launches += 1 + (c->ncells > 0 ? 7 : 1) + 10 + 1;
             if (c->Kmax > 1) {
                 launch_tile_moments<S, R>(c->d_chans, fp, c->tb, c->spread_grid, st);
                 mark(c, SFG_PHASE_MDF_INTERP);

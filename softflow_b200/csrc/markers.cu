@@ -480,7 +480,8 @@ __global__ void k_tile_slots(int T, const int* __restrict__ tile_flag,
                              const int* __restrict__ slot_scan, int* __restrict__ tile_slot,
                              int* __restrict__ slot_tile, const ChannelDev* __restrict__ chans,
                              const int* __restrict__ tile_chan, const int* __restrict__ tile_cnt,
-                             const int* __restrict__ list_off, SlotInfo* __restrict__ info) {
+                             const int* __restrict__ list_off, SlotInfo* __restrict__ info,
+                             int* __restrict__ cls_cnt, int* __restrict__ slot_rank) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= T) return;
     if (tile_flag[t]) {
@@ -500,9 +501,36 @@ __global__ void k_tile_slots(int T, const int* __restrict__ tile_flag,
         si.nx = ch.nx;
         si.ny = ch.ny;
         info[s] = si;
+        // rank within the list-length class: one atomic per class and warp
+        const int cls = slot_class(si.cnt);
+        const unsigned peers = __match_any_sync(__activemask(), cls);
+        const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&cls_cnt[cls], __popc(peers));
+        base = __shfl_sync(peers, base, leader);
+        slot_rank[s] = base + __popc(peers & ((1u << lane) - 1u));
     } else {
         tile_slot[t] = -1;
     }
+}
+
+// The spread's work order: slots by descending class, any order within a
+// class (every slot's result is independent of the warp and of the order).
+__global__ void k_slot_order(const int* __restrict__ n_slots_p, const SlotInfo* __restrict__ info,
+                             const int* __restrict__ cls_cnt, const int* __restrict__ slot_rank,
+                             int* __restrict__ order) {
+    __shared__ int start[SLOT_CLASSES];
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int c = SLOT_CLASSES - 1; c >= 0; --c) {
+            start[c] = acc;
+            acc += cls_cnt[c];
+        }
+    }
+    __syncthreads();
+    const int n = *n_slots_p;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x)
+        order[start[slot_class(info[s].cnt)] + slot_rank[s]] = s;
 }
 
 __global__ void k_tile_fill(const ChannelDev* __restrict__ chans, int M, MarkerBufs mb,
@@ -638,7 +666,8 @@ constexpr int spread_min_ctas() { return sizeof(R) == 4 ? 4 : 3; }
 template <typename R>
 __global__ void __launch_bounds__(SPREAD_WARPS * 32, spread_min_ctas<R>())
 k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot_info,
-         const int* __restrict__ n_slots_p, int* __restrict__ slot_ctr,
+         const int* __restrict__ slot_order, const int* __restrict__ n_slots_p,
+         int* __restrict__ slot_ctr,
          int* __restrict__ list, MarkerBufs mb, double* __restrict__ acc,
          double* __restrict__ acc0, R* __restrict__ gsnap, R* __restrict__ fin, int sweep,
          int mode, const unsigned* __restrict__ resid_gate,
@@ -654,18 +683,28 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
     A* ay = W.ay;
     int* sl = W.ck.list;
     const int n_slots = *n_slots_p;
-    // slots are dealt to the warps in a fixed stride (list lengths are
-    // similar; a shared claim counter serialises on one L2 address); the
-    // next slot's record is fetched while the current one is processed
+    // slots are dealt to the warps in rounds over the work order (longest
+    // lists first, alternating direction, so each warp's share sums to
+    // about the same work; a shared claim counter serialises on one L2
+    // address); the next slot's record is fetched while the current one is
+    // processed
     const int nwarps = gridDim.x * SPREAD_WARPS;
-    int next = blockIdx.x * SPREAD_WARPS + warp;
+    // round k takes work-order positions k nwarps .. (k + 1) nwarps - 1,
+    // the warps in reverse order on odd rounds
+    const int wid = blockIdx.x * SPREAD_WARPS + warp;
+    int round = 0, next = wid;
+    int nslot = next < n_slots ? slot_order[next] : 0;
     SlotInfo nfo{};
-    if (next < n_slots) nfo = slot_info[next];
+    if (next < n_slots) nfo = slot_info[nslot];
     while (next < n_slots) {
-        const int slot = next;
+        const int slot = nslot;
         const SlotInfo si = nfo;
-        next += nwarps;
-        if (next < n_slots) nfo = slot_info[next];
+        ++round;
+        next = round * nwarps + ((round & 1) ? nwarps - 1 - wid : wid);
+        if (next < n_slots) {
+            nslot = slot_order[next];
+            nfo = slot_info[nslot];
+        }
         const int chan = si.chan;
         const ChannelDev& ch = chans[chan];
         const int K = ch.ibm_iterations > 1 ? ch.ibm_iterations : 1;
@@ -979,15 +1018,28 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
 // split into a low part of 20 bits (unsigned, in [0, 2^20)) and a high part
 // (signed): a cell takes at most SPREAD_LIST_MAX + 1 low parts per sweep
 // (below 2^32), and the high parts hold sums up to 2^13 in magnitude, far
-// beyond any lattice force.  The sum is rounded to float once, where it is
-// written out.  FP64 contexts keep k_spread (the reference's serial order,
-// bit for bit).
+// beyond any lattice force.
+//
+// A cell that no stencil point of the tile's markers reaches (with weight
+// above 1e-15) receives nothing in any sweep of the step (the lists do not
+// change between sweeps) and so holds zero throughout; about five in six
+// cells of a tile are such.  The accumulators are therefore read and written
+// only at the touched cells: a sweep adds its sum, rounded to float once, to
+// the previous sweep's value there, and the readers of the accumulators (the
+// interpolations, at the same stencil points) read nothing else.  The last
+// sweep writes every cell of the tile's final force and of the force before
+// that sweep, zero plus the body force where untouched.  The shared
+// accumulators start at zero once per kernel and are cleared again at the
+// touched cells after each tile.  FP64 contexts keep k_spread (the
+// reference's serial order, bit for bit).
 constexpr int FX_LO_BITS = 20;
 constexpr float FX_SCALE = 274877906944.0f;          // 2^38
 constexpr float FX_UNSCALE = 1.0f / 274877906944.0f;  // 2^-38 (exact)
 struct SpreadFxWarp {
     unsigned lo[2][ACC_CELLS];        // x, y; rows of ACC_W cells
     int hi[2][ACC_CELLS];
+    unsigned char hit[ACC_CELLS];     // touched this tile
+    unsigned short idx[TILE_CELLS];   // the touched cells, compacted
 };
 constexpr size_t spread_fx_smem() { return sizeof(SpreadFxWarp) * SPREAD_WARPS; }
 __device__ __forceinline__ long long fx_quant(float v) { return __float2ll_rn(v * FX_SCALE); }
@@ -1001,7 +1053,8 @@ __device__ __forceinline__ float fx_value(unsigned lo, int hi) {
 
 __global__ void __launch_bounds__(SPREAD_WARPS * 32, 4)
 k_spread_fx(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot_info,
-            const int* __restrict__ n_slots_p, const int* __restrict__ list, MarkerBufs mb,
+            const int* __restrict__ slot_order, const int* __restrict__ n_slots_p,
+            const int* __restrict__ list, MarkerBufs mb,
             double* __restrict__ acc, double* __restrict__ acc0, float* __restrict__ gsnap,
             float* __restrict__ fin, int sweep, int mode, const unsigned* __restrict__ resid_gate,
             const int* __restrict__ plain_needed, int* __restrict__ capped,
@@ -1010,16 +1063,30 @@ k_spread_fx(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ s
     extern __shared__ __align__(16) unsigned char spread_fx_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     SpreadFxWarp& W = reinterpret_cast<SpreadFxWarp*>(spread_fx_raw)[warp];
+    for (int i = lane; i < ACC_CELLS; i += 32) {
+        W.lo[0][i] = W.lo[1][i] = 0u;
+        W.hi[0][i] = W.hi[1][i] = 0;
+        W.hit[i] = 0;
+    }
+    __syncwarp();
     const int n_slots = *n_slots_p;
     const int nwarps = gridDim.x * SPREAD_WARPS;
-    int next = blockIdx.x * SPREAD_WARPS + warp;
+    // round k takes work-order positions k nwarps .. (k + 1) nwarps - 1,
+    // the warps in reverse order on odd rounds
+    const int wid = blockIdx.x * SPREAD_WARPS + warp;
+    int round = 0, next = wid;
+    int nslot = next < n_slots ? slot_order[next] : 0;
     SlotInfo nfo{};
-    if (next < n_slots) nfo = slot_info[next];
+    if (next < n_slots) nfo = slot_info[nslot];
     while (next < n_slots) {
-        const int slot = next;
+        const int slot = nslot;
         const SlotInfo si = nfo;
-        next += nwarps;
-        if (next < n_slots) nfo = slot_info[next];
+        ++round;
+        next = round * nwarps + ((round & 1) ? nwarps - 1 - wid : wid);
+        if (next < n_slots) {
+            nslot = slot_order[next];
+            nfo = slot_info[nslot];
+        }
         const int chan = si.chan;
         const ChannelDev& ch = chans[chan];
         const int K = ch.ibm_iterations > 1 ? ch.ibm_iterations : 1;
@@ -1039,20 +1106,6 @@ k_spread_fx(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ s
         const float2* src = reinterpret_cast<const float2*>(
             (ch.learned && (mode == MDF_SEED || (mode == MDF_PLAIN && sweep == 1))) ? acc0 : acc);
         const size_t base2 = (size_t)slot * TILE_CELLS;
-        for (int c = lane; c < TILE_CELLS; c += 32) {
-            const float2 a = sweep > 0 ? src[base2 + c] : make_float2(0.f, 0.f);
-            const long long qx = fx_quant(a.x), qy = fx_quant(a.y);
-            const int i = acc_at(c);
-            W.lo[0][i] = fx_lo(qx);
-            W.hi[0][i] = fx_hi(qx);
-            W.lo[1][i] = fx_lo(qy);
-            W.hi[1][i] = fx_hi(qy);
-            if (last && K > 1) {
-                gsnap[base + c] = a.x;
-                gsnap[base + TILE_CELLS + c] = a.y;
-            }
-        }
-        __syncwarp();
         // four lanes per marker, one stencil row each, eight markers a pass;
         // the next pass's marker data is loaded before this pass's points
         const int jm = lane >> 2, sy = lane & 3;
@@ -1081,7 +1134,7 @@ k_spread_fx(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ s
             if (c0 + jm < cnt) {
                 const bool ok = !(isnan(cur.f.x) || isnan(cur.f.y));
                 const int iy = cur.iy - 1 + sy, cyl = iy - y0;
-                const bool vrow = ok && cyl >= 0 && cyl < TILE_H && iy >= 0 && iy < ny;
+                const bool vrow = cyl >= 0 && cyl < TILE_H && iy >= 0 && iy < ny;
                 const double wxk[4] = {cur.w0.x, cur.w0.y, cur.w1.x, cur.w1.y};
                 const float fx = (float)cur.f.x, fy = (float)cur.f.y, ds = (float)cur.ds;
 #pragma unroll
@@ -1091,10 +1144,14 @@ k_spread_fx(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ s
                     if (jx >= nx) jx -= nx;
                     const int cl = jx - x0;
                     const double w = wxk[k] * cur.wy;
-                    if (vrow && jx >= 0 && jx < nx && cl >= 0 && cl < TILE_W && w > 1e-15) {
+                    // touched: a superset of the points that the
+                    // interpolations read (they test the weight in float)
+                    if (vrow && jx >= 0 && jx < nx && cl >= 0 && cl < TILE_W && w > 0.5e-15) {
+                        const int i = cyl * ACC_W + cl;
+                        W.hit[i] = 1;   // (lanes that meet here all store 1)
+                        if (!ok || !(w > 1e-15)) continue;
                         const float wf = (float)w;
                         const long long qx = fx_quant(fx * wf * ds), qy = fx_quant(fy * wf * ds);
-                        const int i = cyl * ACC_W + cl;
                         atomicAdd(&W.lo[0][i], fx_lo(qx));
                         atomicAdd(&W.hi[0][i], fx_hi(qx));
                         atomicAdd(&W.lo[1][i], fx_lo(qy));
@@ -1106,41 +1163,100 @@ k_spread_fx(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ s
         }
         __syncwarp();
         if (!last) {
+            // the touched cells, compacted row by row
+            int n = 0;
+#pragma unroll
+            for (int r = 0; r < TILE_H; ++r) {
+                const bool h = W.hit[r * ACC_W + lane] != 0;
+                const unsigned b = __ballot_sync(0xffffffffu, h);
+                if (h) W.idx[n + __popc(b & ((1u << lane) - 1u))] = (unsigned short)(r * TILE_W + lane);
+                n += __popc(b);
+            }
+            __syncwarp();
             float2* out = reinterpret_cast<float2*>((sweep == 0 && ch.learned) ? acc0 : acc);
-            for (int c = lane; c < TILE_CELLS; c += 32) {
-                const int i = acc_at(c);
-                out[base2 + c] =
-                    make_float2(fx_value(W.lo[0][i], W.hi[0][i]), fx_value(W.lo[1][i], W.hi[1][i]));
+            for (int k = lane; k < n; k += 32) {
+                const int c = W.idx[k], i = acc_at(c);
+                float2 v = make_float2(fx_value(W.lo[0][i], W.hi[0][i]),
+                                       fx_value(W.lo[1][i], W.hi[1][i]));
+                if (sweep > 0) {
+                    const float2 a = src[base2 + c];
+                    v.x = a.x + v.x;
+                    v.y = a.y + v.y;
+                }
+                out[base2 + c] = v;
+                W.lo[0][i] = W.lo[1][i] = 0u;
+                W.hi[0][i] = W.hi[1][i] = 0;
+                W.hit[i] = 0;
             }
             __syncwarp();
             continue;
         }
-        // finalize: body force on FLUID cells, then the force cap (as k_spread)
+        // finalize every cell, two adjacent cells a lane: the value before
+        // this sweep (zero where untouched) plus this sweep's sum, the body
+        // force on FLUID cells, then the force cap with the capped-cell
+        // count (as k_spread, in float).  Cell kinds follow from the row
+        // alone unless the channel has a cell-type mask or x boundaries.
         int n_cap = 0, n_fluid = 0;
-        const double Fm = ch.max_force, Fm2 = Fm * Fm;
+        const float Fm = (float)ch.max_force, Fm2 = Fm * Fm;
+        const float bfx = (float)ch.body_fx, bfy = (float)ch.body_fy;
         const bool body = (ch.body_fx != 0.0 || ch.body_fy != 0.0);
-        for (int c = lane; c < TILE_CELLS; c += 32) {
-            const int jx = x0 + (c % TILE_W), jy = y0 + (c / TILE_W);
-            const int i = acc_at(c);
-            double vx = (double)fx_value(W.lo[0][i], W.hi[0][i]);
-            double vy = (double)fx_value(W.lo[1][i], W.hi[1][i]);
-            if (jx < nx && jy < ny) {
-                const bool fluid = cell_kind(ch, jx, jy) == CK_FLUID;
-                if (fluid && body) {
-                    vx += ch.body_fx;
-                    vy += ch.body_fy;
+        const bool row_kinds = ch.mask == nullptr && ch.bc_x != 0 && ch.bc_x != 2;
+        const float2 zero = make_float2(0.f, 0.f);
+#pragma unroll 2
+        for (int it = 0; it < TILE_H / 2; ++it) {
+            const int r = 2 * it + (lane >> 4), cx = 2 * (lane & 15);
+            const int c = r * TILE_W + cx, i = r * ACC_W + cx;
+            const int jx = x0 + cx, jy = y0 + r;
+            const bool h0 = W.hit[i] != 0, h1 = W.hit[i + 1] != 0;
+            float2 a0 = zero, a1 = zero, v0 = zero, v1 = zero;
+            if (h0 || h1) {
+                if (sweep > 0) {
+                    const float4 a = *reinterpret_cast<const float4*>(src + base2 + c);
+                    if (h0) a0 = make_float2(a.x, a.y);
+                    if (h1) a1 = make_float2(a.z, a.w);
                 }
-                const double f2 = vx * vx + vy * vy;
-                if (f2 > Fm2) {
-                    const double sc = Fm / sqrt(f2);
-                    vx *= sc;
-                    vy *= sc;
-                    ++n_cap;
+                if (h0) {
+                    v0 = make_float2(a0.x + fx_value(W.lo[0][i], W.hi[0][i]),
+                                     a0.y + fx_value(W.lo[1][i], W.hi[1][i]));
+                    W.lo[0][i] = W.lo[1][i] = 0u;
+                    W.hi[0][i] = W.hi[1][i] = 0;
+                    W.hit[i] = 0;
                 }
-                n_fluid += fluid ? 1 : 0;
+                if (h1) {
+                    v1 = make_float2(a1.x + fx_value(W.lo[0][i + 1], W.hi[0][i + 1]),
+                                     a1.y + fx_value(W.lo[1][i + 1], W.hi[1][i + 1]));
+                    W.lo[0][i + 1] = W.lo[1][i + 1] = 0u;
+                    W.hi[0][i + 1] = W.hi[1][i + 1] = 0;
+                    W.hit[i + 1] = 0;
+                }
             }
-            fin[base + c] = (float)vx;
-            fin[base + TILE_CELLS + c] = (float)vy;
+            if (K > 1) {
+                *reinterpret_cast<float2*>(gsnap + base + c) = make_float2(a0.x, a1.x);
+                *reinterpret_cast<float2*>(gsnap + base + TILE_CELLS + c) = make_float2(a0.y, a1.y);
+            }
+            float2 v[2] = {v0, v1};
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                if (jx + e < nx && jy < ny) {
+                    const bool fluid =
+                        row_kinds ? (ch.periodic_y || (jy != 0 && jy != ny - 1))
+                                  : cell_kind(ch, jx + e, jy) == CK_FLUID;
+                    if (fluid && body) {
+                        v[e].x += bfx;
+                        v[e].y += bfy;
+                    }
+                    const float f2 = v[e].x * v[e].x + v[e].y * v[e].y;
+                    if (f2 > Fm2) {
+                        const float sc = Fm / sqrtf(f2);
+                        v[e].x *= sc;
+                        v[e].y *= sc;
+                        ++n_cap;
+                    }
+                    n_fluid += fluid ? 1 : 0;
+                }
+            }
+            *reinterpret_cast<float2*>(fin + base + c) = make_float2(v[0].x, v[1].x);
+            *reinterpret_cast<float2*>(fin + base + TILE_CELLS + c) = make_float2(v[0].y, v[1].y);
         }
         for (int o = 16; o > 0; o >>= 1) {
             n_cap += __shfl_down_sync(0xffffffffu, n_cap, o);
@@ -1623,13 +1739,16 @@ void launch_tiles(const ChannelDev* chans, const CapsuleDev* caps, int M, const 
     cudaMemsetAsync(tb.tile_flag, 0, sizeof(int) * T, st);
     cudaMemsetAsync(tb.tile_cnt, 0, sizeof(int) * T, st);
     cudaMemsetAsync(tb.cursor, 0, sizeof(int) * T, st);
+    cudaMemsetAsync(tb.cls_cnt, 0, sizeof(int) * SLOT_CLASSES, st);
     k_ibm_prep<<<G, B, 0, st>>>(chans, caps, M, mb, phi_tbl, tb.tile_flag, tb.tile_cnt, status);
     scan_exclusive(tb.tile_flag, tb.slot_scan, T, tb.scan_tmp, tb.n_slots, st);
     scan_exclusive(tb.tile_cnt, tb.list_off, T, tb.scan_tmp, nullptr, st);
     k_tile_slots<<<(T + B - 1) / B, B, 0, st>>>(T, tb.tile_flag, tb.slot_scan,
                                                 tb.tile_slot[parity], tb.slot_tile, chans,
                                                 tb.tile_chan, tb.tile_cnt, tb.list_off,
-                                                tb.slot_info);
+                                                tb.slot_info, tb.cls_cnt, tb.slot_rank);
+    k_slot_order<<<148, 256, 0, st>>>(tb.n_slots, tb.slot_info, tb.cls_cnt, tb.slot_rank,
+                                      tb.slot_order);
     k_tile_fill<<<G, B, 0, st>>>(chans, M, mb, tb.list_off, tb.cursor, tb.list,
                                  tb.tile_slot[parity]);
 }
@@ -1640,12 +1759,13 @@ void launch_spread(const ChannelDev* chans, const MarkerBufs& mb, TileBufs& tb, 
                    cudaStream_t st) {
     if constexpr (sizeof(R) == 4) {
         k_spread_fx<<<grid, SPREAD_WARPS * 32, spread_fx_smem(), st>>>(
-            chans, tb.slot_info, tb.n_slots, tb.list, mb, tb.acc, tb.acc0,
+            chans, tb.slot_info, tb.slot_order, tb.n_slots, tb.list, mb, tb.acc, tb.acc0,
             static_cast<float*>(tb.gsnap), static_cast<float*>(tb.fin[parity]), sweep, mode,
             tb.resid_gate, tb.plain_needed, tb.capped, tb.fluid_touched, status);
     } else {
         k_spread<R><<<grid, SPREAD_WARPS * 32, spread_smem<R>(), st>>>(
-            chans, tb.slot_info, tb.n_slots, tb.spread_ctr + launch_idx, tb.list, mb, tb.acc,
+            chans, tb.slot_info, tb.slot_order, tb.n_slots, tb.spread_ctr + launch_idx, tb.list,
+            mb, tb.acc,
             tb.acc0, static_cast<R*>(tb.gsnap), static_cast<R*>(tb.fin[parity]), sweep, mode,
             tb.resid_gate, tb.plain_needed, tb.capped, tb.fluid_touched, status);
     }

@@ -44,6 +44,12 @@ struct TileBufs {
     void* mom = nullptr;        // [max_slots][TILE_CELLS] (rho, jx, jy, 0) of R (step's moments)
     int marker_block = 128;         // block size of the per-marker kernels (tuned)
     SlotInfo* slot_info = nullptr;  // [max_slots]
+    // The order in which the spread warps take the slots: by descending
+    // class of list length (passes of 8 markers), so that each warp's share
+    // of the step's tiles sums to about the same work.
+    int* slot_order = nullptr;      // [max_slots]
+    int* slot_rank = nullptr;       // [max_slots] rank of the slot within its class
+    int* cls_cnt = nullptr;         // [SLOT_CLASSES] slots per class
     int* spread_ctr = nullptr;      // [n_spread_ctr] slot counters, one per spread launch of a
                                     // step (zeroed at the start of the step)
     int n_spread_ctr = 0;
