@@ -246,6 +246,58 @@ def scalar_bytes_per_cell(precision: str) -> int:
     return 144 if precision == "fp64" else 72
 
 
+SPREAD_ENTRY_BYTES = 100   # per list entry: force 16, arc length 8, origin 8, weights 64, index 4
+SLOT_FINAL_BYTES = 4096    # per force tile, last sweep: final force and force before it, 2 x 2 KB
+
+
+def spread_geometry(ens, plans):
+    """Force tiles (32 x 8), list entries (marker, tile) and touched cells of
+    the markers' 4 x 4 stencils, from the marker positions read back."""
+    import numpy as np
+    slots = entries = touched = 0
+    for i, pl in enumerate(plans):
+        nx, ny = pl.params.nx, pl.params.ny
+        X = np.asarray(ens.capsules(i).positions()).reshape(-1, 2)
+        if len(X) == 0:
+            continue
+        ix = np.floor(X[:, 0]).astype(np.int64)
+        iy = np.floor(X[:, 1]).astype(np.int64)
+        s = np.arange(-1, 3)
+        jx = (ix[:, None, None] + s[None, None, :]) % nx            # [m, 1, 4]
+        jy = iy[:, None, None] + s[None, :, None]                   # [m, 4, 1]
+        jx, jy = np.broadcast_arrays(jx, jy)
+        ok = (jy >= 0) & (jy < ny)
+        cell = np.where(ok, jy * nx + jx, -1)
+        touched += len(np.unique(cell[ok]))
+        tx = (nx + 31) // 32
+        tile = np.sort(np.where(ok, (jy // 8) * tx + jx // 32, -1).reshape(len(X), -1), axis=1)
+        first = np.ones_like(tile, dtype=bool)
+        first[:, 1:] = tile[:, 1:] != tile[:, :-1]
+        entries += int(np.sum(first & (tile >= 0)))           # distinct tiles per marker
+        slots += len(np.unique(tile[tile >= 0]))
+    return slots, entries, touched
+
+
+def spread_roofline(ens, plans, spread_ms, sweeps, peak, peak_kind):
+    """The forcing spread (k_spread_fx on FP32-arithmetic contexts): the
+    algorithmic bytes of the step's `sweeps` launches against their phase
+    time.  Every launch reads each list entry's marker data; the sweeps
+    before the last read (after the first) and write the accumulators at
+    the touched cells; the last writes the tiles' final force and the force
+    before it at every cell."""
+    slots, entries, touched = spread_geometry(ens, plans)
+    alg = sweeps * entries * SPREAD_ENTRY_BYTES + touched * 8 * (2 * sweeps - 2) \
+        + slots * SLOT_FINAL_BYTES
+    ach = alg / (spread_ms / 1e3) / 1e9 if spread_ms > 0 else 0.0
+    return {"kernel": "k_spread_fx", "bound": "latency (gathers, shared atomics)",
+            "launches_per_step": sweeps, "ms_per_step": spread_ms,
+            "force_tiles": slots, "list_entries": entries, "touched_cells": touched,
+            "algorithmic_bytes_per_step": alg, "achieved": ach, "peak": peak, "unit": "GB/s",
+            "frac": ach / peak, "peak_source": peak_kind,
+            "note": "phase time of the profiled pass: the sweeps plus the fallback sweeps "
+                    "that return at once; tiles and cells from the final marker positions"}
+
+
 def lattice_kernel_name(plans, precision):
     """The lattice kernel instantiation a workload runs: the eight-cell
     FP16-shifted kernel when the storage is FP16S, there is no scalar and
@@ -388,6 +440,11 @@ def run_product(args, world, rank, local, pg):
     achieved = alg_bytes / (lat_ms / 1e3) / 1e9 if lat_ms > 0 else 0.0
     peak, peak_kind = peaks()
     total_phase = sum(phases.values()) or 1.0
+    spread = None
+    if args.precision != "fp64" and markers > 0 and phases.get("ibm_spread", 0.0) > 0:
+        K = max(p.params.ibm_iterations for p in plans)
+        spread = spread_roofline(ens, plans, phases["ibm_spread"] / prof_steps,
+                                 3 if (learned and K > 2) else K, peak, peak_kind)
 
     # e2e: host-resident initial state, per-step marker readback
     e2e = run_e2e(args, plans, ens, pg, local)
@@ -472,6 +529,7 @@ def run_product(args, world, rank, local, pg):
                      "algorithmic_bytes_per_launch": alg_bytes,
                      # DRAM bytes need a profiler; the bench does not run one
                      "traffic": None},
+        "spread_roofline": spread,
         "e2e": e2e,
         "clocks": clk,
     }
