@@ -9,25 +9,6 @@
 
 namespace sfg {
 
-// Lattice velocity at a cell for interpolation: moments of the populations
-// plus half the given force, zero on SOLID cells (lattice_field.cpp:28-73).
-template <typename S, typename R>
-__device__ __forceinline__ void cell_rho_j(const ChannelDev& ch, const S* __restrict__ f, int jx,
-                                           int jy, double& rho, double& jxo, double& jyo,
-                                           bool& solid) {
-    solid = cell_kind(ch, jx, jy) == CK_SOLID;
-    if (solid) { rho = 0.0; jxo = 0.0; jyo = 0.0; return; }
-    const long long n = (long long)jy * ch.pitch + jx;
-    R v[9];
-#pragma unroll
-    for (int q = 0; q < 9; ++q) v[q] = PopIO<S, R>::ld(f + ch.f_off + q * ch.plane + n, q);
-    R r, a, b;
-    lattice_moments(v, r, a, b);
-    rho = (double)r;
-    jxo = (double)a;
-    jyo = (double)b;
-}
-
 // u = (j + F/2)/rho at the marker's 4 x 4 stencil with the accumulated force
 // acc (immersed_boundary.cpp:174-229 with the stencil weights of the step;
 // SOLID rows and rho <= 1e-15 contribute zero).
@@ -142,12 +123,17 @@ template <> struct Mom4<float> { using T = float4; };
 // issued together before any of their terms is formed, so a marker waits
 // for one round of gathers per row instead of one per cell.  FP64
 // divides by rho as the reference does (bit for bit); FP32-arithmetic modes
-// multiply by one reciprocal per cell.
-template <typename R>
+// multiply by one reciprocal per cell.  With NEAR, also the density
+// at the node nearest to the marker (immersed_boundary.cpp:262-270: the
+// node (int)(x + 0.5), (int)(y + 0.5), density 1 outside the lattice rows),
+// taken from the stencil's moments already loaded (the node is stencil
+// column and row 1 or 2).
+template <typename R, bool NEAR = false>
 __device__ __forceinline__ double2 interp_u_mom(const ChannelDev& ch, const MarkerBufs& mb, int m,
                                                const int* __restrict__ tile_slot,
                                                const typename Mom4<R>::T* __restrict__ mom,
-                                               const double* __restrict__ acc) {
+                                               const double* __restrict__ acc,
+                                               double& rho_near) {
     (void)tile_slot;
     // compute type: double in FP64 contexts (the reference's arithmetic),
     // float in the FP32-arithmetic modes (fewer registers, more resident
@@ -167,6 +153,24 @@ __device__ __forceinline__ double2 interp_u_mom(const ChannelDev& ch, const Mark
         if (jx < 0) jx += ch.nx;
         if (jx >= ch.nx) jx -= ch.nx;
         jxs[sx] = jx;
+    }
+    // the nearest node's stencil column and row (-1: not wanted, or the
+    // density is 1 outside the lattice rows)
+    int sxn = -1, syn = -1;
+    if (NEAR) {
+        rho_near = 1.0;
+        const double2 p = mb.pos[m];
+        int ixr = (int)(p.x + 0.5);
+        const int iyr = (int)(p.y + 0.5);
+        if (ixr < 0) ixr += ch.nx;
+        if (ixr >= ch.nx) ixr -= ch.nx;
+        if (iyr >= 0 && iyr < ch.ny && ixr >= 0 && ixr < ch.nx) {
+            sxn = (int)(p.x + 0.5) - ix0 + 1;
+            syn = iyr - (iy0 - 1);
+            // (always column and row 1 or 2 for a finite position; a
+            // non-finite one keeps the density 1)
+            if (sxn < 0 || sxn > 3 || syn < 0 || syn > 3) sxn = syn = -1;
+        }
     }
     C ux = 0, uy = 0;
 #pragma unroll
@@ -198,6 +202,11 @@ __device__ __forceinline__ double2 interp_u_mom(const ChannelDev& ch, const Mark
                 }
             }
         }
+        if (NEAR && row == syn) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                if (i == sxn && in[i]) rho_near = (double)q[i].x;
+        }
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const int sy = row, sx = i;
@@ -222,42 +231,6 @@ __device__ __forceinline__ double2 interp_u_mom(const ChannelDev& ch, const Mark
         }
     }
     return make_double2((double)ux, (double)uy);
-}
-
-// rho_nearest with the tile moments (the nearest node lies in the stencil).
-template <typename R>
-__device__ __forceinline__ double rho_nearest_mom(const ChannelDev& ch, const MarkerBufs& mb,
-                                                  int m, const typename Mom4<R>::T* __restrict__ mom,
-                                                  double2 p) {
-    int ixr = (int)(p.x + 0.5), iyr = (int)(p.y + 0.5);
-    if (ixr < 0) ixr += ch.nx;
-    if (ixr >= ch.nx) ixr -= ch.nx;
-    if (iyr >= 0 && iyr < ch.ny && ixr >= 0 && ixr < ch.nx) {
-        // the nearest node is stencil column 1 or 2 (x - floor(x) < 1)
-        const int ix0 = mb.ix0[m];
-        const int sx = (int)(p.x + 0.5) - ix0 + 1;
-        const StencilSlots ss(mb, m, mb.iy0[m]);
-        return (double)mom[(size_t)ss.slot(sx, iyr) * TILE_CELLS + (iyr % TILE_H) * TILE_W +
-                           (ixr % TILE_W)].x;
-    }
-    return 1.0;
-}
-
-// Density at the node nearest to the marker, 1 outside the lattice rows
-// (immersed_boundary.cpp:262-270).
-template <typename S, typename R>
-__device__ __forceinline__ double rho_nearest(const ChannelDev& ch, const S* __restrict__ f,
-                                              double2 p) {
-    double rho_local = 1.0;
-    int ixr = (int)(p.x + 0.5), iyr = (int)(p.y + 0.5);
-    if (ixr < 0) ixr += ch.nx;
-    if (ixr >= ch.nx) ixr -= ch.nx;
-    if (iyr >= 0 && iyr < ch.ny && ixr >= 0 && ixr < ch.nx) {
-        double jxm, jym;
-        bool solid;
-        cell_rho_j<S, R>(ch, f, ixr, iyr, rho_local, jxm, jym, solid);
-    }
-    return rho_local;
 }
 
 // Inputs of the forcing network in the marker's local frame (tangent t along

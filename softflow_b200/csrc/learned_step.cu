@@ -43,7 +43,8 @@ __global__ void k_mdf_features(const ChannelDev* __restrict__ chans,
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M || !learned_marker(chans, mb, m)) return;
     const ChannelDev& ch = chans[mb.mk_chan[m]];
-    const double2 u0 = interp_u_mom<R>(ch, mb, m, tile_slot, mom, acc);
+    double unused;
+    const double2 u0 = interp_u_mom<R>(ch, mb, m, tile_slot, mom, acc, unused);
     float fe[8];
     double2 t, nrm;
     mdf_features(ch, caps[mb.mk_cap[m]], mb, m, u0, fe, t, nrm);

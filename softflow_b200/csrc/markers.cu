@@ -1292,8 +1292,8 @@ __global__ void k_mdf_interp(const ChannelDev* __restrict__ chans, int M, Marker
     if (sweep >= ch.ibm_iterations || !mb.valid[m]) return;
     if (!mdf_active(ch, mode, resid_gate, chan)) return;
     const double* base = (mode == MDF_PLAIN && ch.learned && sweep == 1) ? acc0 : acc;
-    const double2 u = interp_u_mom<R>(ch, mb, m, tile_slot, mom, base);
-    const double rho_local = rho_nearest_mom<R>(ch, mb, m, mom, mb.pos[m]);
+    double rho_local;
+    const double2 u = interp_u_mom<R, true>(ch, mb, m, tile_slot, mom, base, rho_local);
     const double2 v = mb.vel[m];
     const double dux = v.x - u.x, duy = v.y - u.y;
     const double2 d = make_double2(dux * (2.0 * rho_local), duy * (2.0 * rho_local));
@@ -1371,7 +1371,7 @@ __global__ void k_tile_moments(const ChannelDev* __restrict__ chans,
             for (int i = 0; i < 4; ++i) {
                 typename Mom4<R>::T q;
                 q.x = 0; q.y = 0; q.z = 0; q.w = 0;
-                if (use[i]) {   // cell_rho_j's moments, in its precision
+                if (use[i]) {   // the cell's moments, in the working precision
                     R r, a, b;
                     lattice_moments(v[i], r, a, b);
                     q.x = (R)(double)r;
