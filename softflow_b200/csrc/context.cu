@@ -269,6 +269,7 @@ struct sfg_context {
     cudaStream_t side[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr, ev_contact = nullptr, ev_tiles = nullptr, ev_mom = nullptr;
     cudaEvent_t ev_lat1 = nullptr;      // the lattice pass over untouched force tiles
+    cudaEvent_t ev_slots = nullptr;     // the step's slot records exist
     bool split_lattice = false;         // that pass beside the forcing (8-cell kernel; off:
                                         // the concurrent pass slowed the forcing more than it
                                         // saved on the ensemble)
@@ -475,7 +476,7 @@ static void free_all(sfg_context* c) {
         }
         c->side[i] = nullptr;
     }
-    for (cudaEvent_t* e : {&c->ev_fork, &c->ev_contact, &c->ev_tiles, &c->ev_mom, &c->ev_lat1}) {
+    for (cudaEvent_t* e : {&c->ev_fork, &c->ev_contact, &c->ev_tiles, &c->ev_mom, &c->ev_lat1, &c->ev_slots}) {
         if (*e) cudaEventDestroy(*e);
         *e = nullptr;
     }
@@ -1138,7 +1139,7 @@ extern "C" int sfg_initialize(sfg_context* c) {
     CU(cudaStreamSynchronize(c->stream));
     if (c->M > 0 && !c->side[0]) {
         for (int i = 0; i < 3; ++i) CU(cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking));
-        for (cudaEvent_t* e : {&c->ev_fork, &c->ev_contact, &c->ev_tiles, &c->ev_mom, &c->ev_lat1})
+        for (cudaEvent_t* e : {&c->ev_fork, &c->ev_contact, &c->ev_tiles, &c->ev_mom, &c->ev_lat1, &c->ev_slots})
             CU(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     }
     c->initialized = true;
@@ -1203,8 +1204,15 @@ static int enqueue_step_t(sfg_context* c, int p) {
             launch_contact_prep(c->d_chans, c->M, c->mb, c->cb, c->ncells, c->side[0]);
             CU(cudaEventRecord(c->ev_contact, c->side[0]));
             launch_tiles(c->d_chans, c->d_caps, c->M, c->mb, c->tb, c->tb.T, p, c->d_phi,
-                         c->d_status, c->side[1]);
+                         c->d_status, c->side[1], c->Kmax > 1 ? c->ev_slots : nullptr);
             CU(cudaEventRecord(c->ev_tiles, c->side[1]));
+            // the tile moments need the slot records only: they run beside
+            // the work order and the marker lists
+            if (c->Kmax > 1) {
+                CU(cudaStreamWaitEvent(c->side[2], c->ev_slots, 0));
+                launch_tile_moments<S, R>(c->d_chans, fp, c->tb, c->spread_grid, c->side[2]);
+                CU(cudaEventRecord(c->ev_mom, c->side[2]));
+            }
             if (split) {
                 CU(cudaStreamWaitEvent(c->side[2], c->ev_tiles, 0));
                 LatticeLaunch L1 = L;
@@ -1212,10 +1220,6 @@ static int enqueue_step_t(sfg_context* c, int p) {
                 launch_lattice_step<S, R>(L1, tv, c->side[2]);
                 CU(cudaEventRecord(c->ev_lat1, c->side[2]));
                 launches += 1;
-            }
-            if (c->Kmax > 1) {
-                launch_tile_moments<S, R>(c->d_chans, fp, c->tb, c->spread_grid, c->side[1]);
-                CU(cudaEventRecord(c->ev_mom, c->side[1]));
             }
             launch_membrane(c->d_caps, c->NC, c->mb, c->d_has_prev, c->maxn, c->d_status, st);
             CU(cudaStreamWaitEvent(st, c->ev_contact, 0));

@@ -1734,7 +1734,7 @@ void launch_contact_prep(const ChannelDev* chans, int M, const MarkerBufs& mb, C
 
 void launch_tiles(const ChannelDev* chans, const CapsuleDev* caps, int M, const MarkerBufs& mb,
                   TileBufs& tb, int T, int parity, const double* phi_tbl, unsigned* status,
-                  cudaStream_t st) {
+                  cudaStream_t st, cudaEvent_t slots_ready) {
     const int B = 256, G = (M + B - 1) / B;
     cudaMemsetAsync(tb.tile_flag, 0, sizeof(int) * T, st);
     cudaMemsetAsync(tb.tile_cnt, 0, sizeof(int) * T, st);
@@ -1747,6 +1747,7 @@ void launch_tiles(const ChannelDev* chans, const CapsuleDev* caps, int M, const 
                                                 tb.tile_slot[parity], tb.slot_tile, chans,
                                                 tb.tile_chan, tb.tile_cnt, tb.list_off,
                                                 tb.slot_info, tb.cls_cnt, tb.slot_rank);
+    if (slots_ready) cudaEventRecord(slots_ready, st);
     k_slot_order<<<148, 256, 0, st>>>(tb.n_slots, tb.slot_info, tb.cls_cnt, tb.slot_rank,
                                       tb.slot_order);
     k_tile_fill<<<G, B, 0, st>>>(chans, M, mb, tb.list_off, tb.cursor, tb.list,

@@ -84,9 +84,11 @@ void launch_contact_force(const ChannelDev* chans, int M, const MarkerBufs& mb, 
 // Repulsion of markers from the pillars of their channel (after the pairs).
 void launch_obstacle_repulsion(const ChannelDev* chans, int M, const MarkerBufs& mb,
                                cudaStream_t st);
+// `slots_ready` (may be null) is recorded once the slot records exist (the
+// tile moments need no more).
 void launch_tiles(const ChannelDev* chans, const CapsuleDev* caps, int M, const MarkerBufs& mb,
                   TileBufs& tb, int T, int parity, const double* phi_tbl, unsigned* status,
-                  cudaStream_t st);
+                  cudaStream_t st, cudaEvent_t slots_ready = nullptr);
 // Spread of sweep `sweep` in forcing mode `mode` (MdfMode); sweep 0 spreads
 // the membrane and contact forces of every channel.  launch_idx: the
 // launch's slot counter in tb.spread_ctr (distinct per launch of a step).
