@@ -65,9 +65,9 @@ k_mdf_seed(const ChannelDev* __restrict__ chans, int M, MarkerBufs mb,
            const mlp::ModelDev* __restrict__ model, unsigned* __restrict__ status) {
     using namespace mlp;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    FwdSmemLean& s = *reinterpret_cast<FwdSmemLean*>(smem_raw);
+    FwdSmemDual& s = *reinterpret_cast<FwdSmemDual*>(smem_raw);
     load_model(s, model);
-    start_tiles(s, LEAN_TMEM_COLS);
+    start_tiles(s, DUAL_TMEM_COLS);
     uint32_t phase = 0;
     const int ntiles = (M + ROWS - 1) / ROWS;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -84,13 +84,12 @@ k_mdf_seed(const ChannelDev* __restrict__ chans, int M, MarkerBufs mb,
 #pragma unroll
             for (int k = 0; k < N_IN; ++k) fe[k] = 0.0f;
         }
-        put_input_row(s, fe, active);
-        float y[2], ym[2];
-        if (!forward_tile_lean(s, s.taddr, phase, y)) break;
+        put_input_row_dual(s, 0, fe, active);
 #pragma unroll
         for (int k = 0; k < 4; ++k) fe[k] = -fe[k];
-        put_input_row(s, fe, active);
-        if (!forward_tile_lean(s, s.taddr, phase, ym)) break;
+        put_input_row_dual(s, 1, fe, active);
+        float y[2], ym[2];
+        if (!forward_tile_dual(s, s.taddr, phase, y, ym)) break;
         if (active) {
             const double a = 0.5 * (double)((y[0] - ym[0]) * s.out_std[0]);
             const double b = 0.5 * (double)((y[1] - ym[1]) * s.out_std[1]);
@@ -100,7 +99,7 @@ k_mdf_seed(const ChannelDev* __restrict__ chans, int M, MarkerBufs mb,
             mb.dFsum[m] = d;
         }
     }
-    if (finish_tiles(s, phase, LEAN_TMEM_COLS) && threadIdx.x == 0)
+    if (finish_tiles(s, phase, DUAL_TMEM_COLS) && threadIdx.x == 0)
         atomicOr(status, ST_TENSOR_TIMEOUT);
 }
 
@@ -131,7 +130,7 @@ __global__ void k_harvest(const ChannelDev* __restrict__ chans, const CapsuleDev
 
 cudaError_t prepare_mdf_learned() {
     return cudaFuncSetAttribute(k_mdf_seed, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sizeof(mlp::FwdSmemLean));
+                                (int)sizeof(mlp::FwdSmemDual));
 }
 
 template <typename S, typename R>
@@ -146,7 +145,7 @@ void launch_mdf_learned(const ChannelDev* chans, const CapsuleDev* caps, int M,
         tb.acc0, feat, frame);   // a learned channel's sweep-0 force is in acc0
     const int tiles = (M + mlp::ROWS - 1) / mlp::ROWS;
     const int g = tiles < grid ? tiles : grid;
-    k_mdf_seed<<<g, mlp::ROWS, sizeof(mlp::FwdSmemLean), st>>>(
+    k_mdf_seed<<<g, mlp::ROWS, sizeof(mlp::FwdSmemDual), st>>>(
         chans, M, mb, feat, frame, static_cast<const mlp::ModelDev*>(model), status);
 }
 

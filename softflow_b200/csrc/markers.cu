@@ -157,6 +157,15 @@ __global__ void k_membrane(const CapsuleDev* __restrict__ caps, int ncaps, Marke
     __syncwarp();
 
     // ---- ring reductions in the reference's order (capsule.cpp:175-204) ----
+    // The per-edge terms (minimum-image edge vector, edge length) are formed
+    // by the lanes in parallel, with the same expressions; lane 0 then sums
+    // them in the reference's order, so the sums are the same bit for bit.
+    for (int i = lane; i < n; i += 32) {
+        const double2 d = min_image_d(P[(i + 1) % n], P[i], Lx);
+        GN[i] = d;
+        E[i].x = norm_d(d);
+    }
+    __syncwarp();
     double sarea = 0.0, perim = 0.0;
     if (lane == 0) {
         if (Lx > 0.0) {
@@ -164,7 +173,7 @@ __global__ void k_membrane(const CapsuleDev* __restrict__ caps, int ncaps, Marke
             for (int i = 0; i < n; ++i) {
                 double2 nxt;
                 if (i + 1 < n) {
-                    double2 d = min_image_d(P[i + 1], P[i], Lx);
+                    const double2 d = GN[i];
                     nxt = make_double2(cur.x + d.x, cur.y + d.y);
                 } else {
                     nxt = P[0];
@@ -178,7 +187,7 @@ __global__ void k_membrane(const CapsuleDev* __restrict__ caps, int ncaps, Marke
                 sarea += a.x * b.y - a.y * b.x;
             }
         }
-        for (int i = 0; i < n; ++i) perim += norm_d(min_image_d(P[(i + 1) % n], P[i], Lx));
+        for (int i = 0; i < n; ++i) perim += E[i].x;
     }
     sarea = __shfl_sync(0xffffffffu, sarea, 0);
     perim = __shfl_sync(0xffffffffu, perim, 0);

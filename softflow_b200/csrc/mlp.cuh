@@ -281,59 +281,117 @@ __device__ __forceinline__ bool forward_tile(FwdSmem& s, uint32_t tbase, uint32_
     return true;
 }
 
-// Inference-only image (the network seed): one activation buffer, reused by
-// both hidden layers (layer 2's MMAs have completed before its outputs are
-// written back), and 64 tensor-memory columns, reused by all three layers
-// (each layer's accumulator is read out before the next layer is issued).
-// About 33 KB, so six CTAs fit on an SM (four with FwdSmem).
-struct __align__(1024) FwdSmemLean {
-    __nv_bfloat16 X[ROWS * K1];     // 4 KB
-    __nv_bfloat16 W1[N_H * K1];     // 2 KB
-    __nv_bfloat16 W3[N3 * N_H];     // 2 KB
-    __nv_bfloat16 W2[N_H * N_H];    // 8 KB
-    __nv_bfloat16 H1[ROWS * N_H];   // 16 KB
+// The network seed's image: the two inputs of the odd part (x and Px) go
+// through the layers together, 2 x 128 rows a tile, so each layer is one
+// round of MMAs, commit and wait for both instead of two.  Per input, one
+// activation buffer reused by both hidden layers (layer 2's MMAs have
+// completed before its outputs are written back) and 64 tensor-memory
+// columns reused by all three layers (x's in [0, 64), Px's in [64, 128)).
+// Each input's MMAs are those of forward_tile, so the outputs do not depend
+// on the pairing.  About 53 KB: four CTAs per SM, whose 4 x 128 columns fill
+// the tensor memory exactly (more resident CTAs would wait in the
+// allocation; shared memory rules them out).
+struct __align__(1024) FwdSmemDual {
+    __nv_bfloat16 X[2][ROWS * K1];    // 8 KB
+    __nv_bfloat16 W1[N_H * K1];       // 2 KB
+    __nv_bfloat16 W3[N3 * N_H];       // 2 KB
+    __nv_bfloat16 W2[N_H * N_H];      // 8 KB
+    __nv_bfloat16 H1[2][ROWS * N_H];  // 32 KB
     float b2[N_H], b3[N_OUT];
     float in_mean[N_IN], in_inv_std[N_IN], out_mean[N_OUT], out_std[N_OUT];
     uint64_t bar;
     uint32_t taddr;
     int error;
 };
-constexpr uint32_t LEAN_TMEM_COLS = 64;
+constexpr uint32_t DUAL_TMEM_COLS = 128;
 
-// forward_tile on FwdSmemLean (same arithmetic, same outputs).
-__device__ __forceinline__ bool forward_tile_lean(FwdSmemLean& s, uint32_t tbase,
-                                                  uint32_t& phase, float* y) {
+// put_input_row into input buffer `b` of the dual image.
+__device__ __forceinline__ void put_input_row_dual(FwdSmemDual& s, int b, const float* feat,
+                                                   bool valid) {
     const int r = threadIdx.x;
-    if (!layer<K1>(s, tbase, s.X, s.W1, idesc_bf16(ROWS, N_H), phase)) return false;
+#pragma unroll
+    for (int k = 0; k < K1; ++k) {
+        float v = 0.0f;
+        if (valid && k < N_IN) v = (feat[k] - s.in_mean[k]) * s.in_inv_std[k];
+        if (valid && k == N_IN) v = 1.0f;
+        s.X[b][kmaj(r, k, K1)] = __float2bfloat16_rn(v);
+    }
+}
+
+// layer() for both inputs of the dual image: the MMAs of A0 into d0 and of
+// A1 into d1 (same weights B), one commit and one wait.
+template <int K>
+__device__ __forceinline__ bool layer_dual(FwdSmemDual& s, uint32_t d0, uint32_t d1,
+                                           const __nv_bfloat16* A0, const __nv_bfloat16* A1,
+                                           const __nv_bfloat16* B, uint32_t idesc,
+                                           uint32_t& phase) {
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    if (s.error) return false;  // uniform: read after the barrier
+    if (threadIdx.x == 0) {
+        tc_fence_after();
+#pragma unroll
+        for (int kk = 0; kk < K / 16; ++kk)
+            mma(d0, opdesc(A0, K, kk), opdesc(B, K, kk), idesc, kk > 0 ? 1u : 0u);
+#pragma unroll
+        for (int kk = 0; kk < K / 16; ++kk)
+            mma(d1, opdesc(A1, K, kk), opdesc(B, K, kk), idesc, kk > 0 ? 1u : 0u);
+        mma_commit(&s.bar);
+    }
+    if (!mbar_wait(&s.bar, phase)) s.error = 1;
+    phase ^= 1u;
+    tc_fence_after();
+    return true;
+}
+
+// The forward pass of both inputs: outputs of this thread's row in y
+// (input 0) and ym (input 1).
+__device__ __forceinline__ bool forward_tile_dual(FwdSmemDual& s, uint32_t tbase,
+                                                  uint32_t& phase, float* y, float* ym) {
+    const int r = threadIdx.x;
+    const uint32_t t1 = tbase + 64;
+    if (!layer_dual<K1>(s, tbase, t1, s.X[0], s.X[1], s.W1, idesc_bf16(ROWS, N_H), phase))
+        return false;
     {
         float v[16];
 #pragma unroll
-        for (int c = 0; c < N_H; c += 16) {
-            tmem_ld16(tmem_row(tbase, c), v);
+        for (int b = 0; b < 2; ++b)
 #pragma unroll
-            for (int i = 0; i < 16; ++i)
-                s.H1[kmaj(r, c + i, N_H)] = __float2bfloat16_rn(fmaxf(v[i], 0.0f));
-        }
+            for (int c = 0; c < N_H; c += 16) {
+                tmem_ld16(tmem_row(b ? t1 : tbase, c), v);
+#pragma unroll
+                for (int i = 0; i < 16; ++i)
+                    s.H1[b][kmaj(r, c + i, N_H)] = __float2bfloat16_rn(fmaxf(v[i], 0.0f));
+            }
     }
-    if (!layer<N_H>(s, tbase, s.H1, s.W2, idesc_bf16(ROWS, N_H), phase)) return false;
+    if (!layer_dual<N_H>(s, tbase, t1, s.H1[0], s.H1[1], s.W2, idesc_bf16(ROWS, N_H), phase))
+        return false;
     {
         // layer 2's MMAs have completed (their commit was waited for), so
-        // its operand H1 can take its output; each thread rewrites its row
+        // its operands H1 can take its outputs; each thread rewrites its row
         float v[16];
 #pragma unroll
-        for (int c = 0; c < N_H; c += 16) {
-            tmem_ld16(tmem_row(tbase, c), v);
+        for (int b = 0; b < 2; ++b)
 #pragma unroll
-            for (int i = 0; i < 16; ++i)
-                s.H1[kmaj(r, c + i, N_H)] = __float2bfloat16_rn(fmaxf(v[i] + s.b2[c + i], 0.0f));
-        }
+            for (int c = 0; c < N_H; c += 16) {
+                tmem_ld16(tmem_row(b ? t1 : tbase, c), v);
+#pragma unroll
+                for (int i = 0; i < 16; ++i)
+                    s.H1[b][kmaj(r, c + i, N_H)] =
+                        __float2bfloat16_rn(fmaxf(v[i] + s.b2[c + i], 0.0f));
+            }
     }
-    if (!layer<N_H>(s, tbase, s.H1, s.W3, idesc_bf16(ROWS, N3), phase)) return false;
+    if (!layer_dual<N_H>(s, tbase, t1, s.H1[0], s.H1[1], s.W3, idesc_bf16(ROWS, N3), phase))
+        return false;
     {
         float v[16];
         tmem_ld16(tmem_row(tbase, 0), v);
         y[0] = v[0] + s.b3[0];
         y[1] = v[1] + s.b3[1];
+        tmem_ld16(tmem_row(t1, 0), v);
+        ym[0] = v[0] + s.b3[0];
+        ym[1] = v[1] + s.b3[1];
     }
     return true;
 }
