@@ -1314,8 +1314,8 @@ static int enqueue_step_t(sfg_context* c, int p) {
     mark(c, SFG_PHASE_BOOKKEEPING);
     launches += 2;
     if (c->M > 0) {
-        launch_interp_move<S, R>(c->d_chans, c->M, c->mb, static_cast<const S*>(c->f[1 - p]),
-                                 c->tb, p, c->d_phi, st);
+        launch_interp_move<S, R>(c->d_chans, c->d_caps, c->NC, c->M, c->mb,
+                                 static_cast<const S*>(c->f[1 - p]), c->tb, p, c->d_phi, st);
         mark(c, SFG_PHASE_INTERP_MOVE);
         launches += 1;
     }

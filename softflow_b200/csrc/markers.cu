@@ -1393,18 +1393,11 @@ __global__ void k_tile_moments(const ChannelDev* __restrict__ chans,
     }
 }
 
-// Interpolate the new velocity and move the markers (simulation.cpp:656-675,
+// Move marker m with its interpolated velocity u (simulation.cpp:656-675,
 // capsule.cpp:267-297).
-template <typename S, typename R>
-__global__ void k_interp_move(const ChannelDev* __restrict__ chans, int M, MarkerBufs mb,
-                              const S* __restrict__ f, const int* __restrict__ tile_slot,
-                              const R* __restrict__ fin, const double* __restrict__ phi_tbl) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= M) return;
-    const ChannelDev& ch = chans[mb.mk_chan[m]];
+__device__ __forceinline__ void move_marker(const ChannelDev& ch, const MarkerBufs& mb, int m,
+                                            double2 u) {
     double2 p = mb.pos[m];
-    double2 u = make_double2(0.0, 0.0);
-    if (mb.valid[m]) u = interp_u_acc<S, R, R>(ch, mb, m, f, tile_slot, fin);
     const double ux = u.x, uy = u.y;
     mb.vel[m] = make_double2(ux, uy);
     // the step's correction before its last sweep (the network's label, or
@@ -1432,6 +1425,157 @@ __global__ void k_interp_move(const ChannelDev* __restrict__ chans, int M, Marke
         if (p.y > ymax) p.y = ymax;
     }
     mb.pos[m] = p;
+}
+
+// Interpolate the new velocity and move the markers (FP64 contexts), one
+// thread per marker.
+template <typename S, typename R>
+__global__ void k_interp_move(const ChannelDev* __restrict__ chans, int M, MarkerBufs mb,
+                              const S* __restrict__ f, const int* __restrict__ tile_slot,
+                              const R* __restrict__ fin, const double* __restrict__ phi_tbl) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    const ChannelDev& ch = chans[mb.mk_chan[m]];
+    double2 u = make_double2(0.0, 0.0);
+    if (mb.valid[m]) u = interp_u_acc<S, R, R>(ch, mb, m, f, tile_slot, fin);
+    move_marker(ch, mb, m, u);
+}
+
+// The marker move of the FP32-arithmetic modes, one warp per capsule: the
+// warp first forms, for every cell of the box that holds its markers'
+// stencils, the new state's moments (rho, jx, jy; zero on SOLID cells) and
+// the cell's final force, into shared memory, the lanes running along the
+// box's rows (each cell's nine populations are read once, coalesced, where
+// the markers' stencils overlap); then each lane interpolates its markers
+// from there with the terms, order and arithmetic of interp_u_acc (the same
+// values, so the same result bit for bit), and moves them.  A capsule whose
+// box exceeds MOVE_BOX_MAX cells interpolates from global memory as
+// k_interp_move does.
+// (out of line: the rare large capsule keeps its registers out of the box path)
+template <typename S>
+__device__ __noinline__ double2 interp_u_acc_global(const ChannelDev& ch, const MarkerBufs& mb,
+                                                    int m, const S* __restrict__ f,
+                                                    const int* __restrict__ tile_slot,
+                                                    const float* __restrict__ fin) {
+    return interp_u_acc<S, float, float>(ch, mb, m, f, tile_slot, fin);
+}
+constexpr int MOVE_WARPS = 4;
+constexpr int MOVE_BOX_MAX = 512;
+struct MoveBox {
+    float rho[MOVE_BOX_MAX], jx[MOVE_BOX_MAX], jy[MOVE_BOX_MAX];
+    float fx[MOVE_BOX_MAX], fy[MOVE_BOX_MAX];
+};
+template <typename S>
+__global__ void __launch_bounds__(MOVE_WARPS * 32)
+k_interp_move_caps(const CapsuleDev* __restrict__ caps, int ncaps,
+                   const ChannelDev* __restrict__ chans, MarkerBufs mb, const S* __restrict__ f,
+                   const int* __restrict__ tile_slot, const float* __restrict__ fin) {
+    extern __shared__ __align__(16) unsigned char move_smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = blockIdx.x * MOVE_WARPS + warp;
+    if (c >= ncaps) return;
+    MoveBox& B = reinterpret_cast<MoveBox*>(move_smem)[warp];
+    const CapsuleDev cp = caps[c];
+    const ChannelDev& ch = chans[cp.chan];
+    const int nx = ch.nx, ny = ch.ny, n = cp.n, off = cp.off;
+    // the stencils' box: x relative to the first marker (minimum image)
+    int ref = 0;
+    for (int k = 0; k < n; ++k)
+        if (mb.valid[off + k]) { ref = mb.ix0[off + k]; break; }
+    int dmin = INT_MAX, dmax = INT_MIN, ymin = INT_MAX, ymax = INT_MIN;
+    for (int k = lane; k < n; k += 32) {
+        if (!mb.valid[off + k]) continue;
+        int d = mb.ix0[off + k] - ref;
+        if (2 * d > nx) d -= nx;
+        if (2 * d < -nx) d += nx;
+        const int y = mb.iy0[off + k];
+        dmin = min(dmin, d);
+        dmax = max(dmax, d);
+        ymin = min(ymin, y);
+        ymax = max(ymax, y);
+    }
+    dmin = __reduce_min_sync(0xffffffffu, dmin);
+    dmax = __reduce_max_sync(0xffffffffu, dmax);
+    ymin = __reduce_min_sync(0xffffffffu, ymin);
+    ymax = __reduce_max_sync(0xffffffffu, ymax);
+    const bool any = dmin <= dmax;
+    const int bw = dmax - dmin + 4, bh = ymax - ymin + 4;
+    const bool boxed = any && (long long)bw * bh <= MOVE_BOX_MAX;
+    if (boxed) {
+        const int bx0 = ref + dmin - 1, by0 = ymin - 1;
+        for (int i = lane; i < bw * bh; i += 32) {
+            const int by = i / bw, bx = i - by * bw;
+            int jx = (bx0 + bx) % nx;
+            if (jx < 0) jx += nx;
+            const int jy = by0 + by;
+            float r = 0.f, a = 0.f, b = 0.f, gx = 0.f, gy = 0.f;
+            if (jy >= 0 && jy < ny && cell_kind(ch, jx, jy) != CK_SOLID) {
+                const long long nn = (long long)jy * ch.pitch + jx;
+                float v[9];
+#pragma unroll
+                for (int q = 0; q < 9; ++q)
+                    v[q] = PopIO<S, float>::ld(f + ch.f_off + q * ch.plane + nn, q);
+                lattice_moments(v, r, a, b);
+                const int t = ch.tile_base + (jy / TILE_H) * ch.tiles_x + jx / TILE_W;
+                const int sl = tile_slot[t];
+                if (sl >= 0) {
+                    const int cell = (jy % TILE_H) * TILE_W + (jx % TILE_W);
+                    gx = fin[(size_t)sl * 2 * TILE_CELLS + cell];
+                    gy = fin[(size_t)sl * 2 * TILE_CELLS + TILE_CELLS + cell];
+                }
+            }
+            B.rho[i] = r;
+            B.jx[i] = a;
+            B.jy[i] = b;
+            B.fx[i] = gx;
+            B.fy[i] = gy;
+        }
+        __syncwarp();
+    }
+    for (int k = lane; k < n; k += 32) {
+        const int m = off + k;
+        double2 u = make_double2(0.0, 0.0);
+        if (mb.valid[m]) {
+            if (!boxed) {
+                u = interp_u_acc_global<S>(ch, mb, m, f, tile_slot, fin);
+            } else {
+                const int ix0 = mb.ix0[m], iy0 = mb.iy0[m];
+                int d = ix0 - ref;
+                if (2 * d > nx) d -= nx;
+                if (2 * d < -nx) d += nx;
+                const double2* wx2 = reinterpret_cast<const double2*>(mb.wx + 4 * (size_t)m);
+                const double2* wy2 = reinterpret_cast<const double2*>(mb.wy + 4 * (size_t)m);
+                const double2 wxa = wx2[0], wxb = wx2[1], wya = wy2[0], wyb = wy2[1];
+                const float wxs[4] = {(float)wxa.x, (float)wxa.y, (float)wxb.x, (float)wxb.y};
+                const float wys[4] = {(float)wya.x, (float)wya.y, (float)wyb.x, (float)wyb.y};
+                float ux = 0.f, uy = 0.f;
+#pragma unroll
+                for (int sy = 0; sy < 4; ++sy) {
+                    const int jy = iy0 - 1 + sy;
+                    if (jy < 0 || jy >= ny) continue;
+                    const int row = (iy0 - ymin + sy) * bw + (d - dmin);
+#pragma unroll
+                    for (int sx = 0; sx < 4; ++sx) {
+                        const float w = wxs[sx] * wys[sy];
+                        if (w > 1e-15f) {
+                            const int i = row + sx;
+                            const float rho = B.rho[i];
+                            float cu = 0.f, cv = 0.f;
+                            if (rho > 1e-15f) {
+                                const float inv = __frcp_rn(rho);
+                                cu = (B.jx[i] + 0.5f * B.fx[i]) * inv;
+                                cv = (B.jy[i] + 0.5f * B.fy[i]) * inv;
+                            }
+                            ux += cu * w;
+                            uy += cv * w;
+                        }
+                    }
+                }
+                u = make_double2((double)ux, (double)uy);
+            }
+        }
+        move_marker(ch, mb, m, u);
+    }
 }
 
 // ============================ launch wrappers ==============================
@@ -1804,11 +1948,21 @@ void launch_tile_moments(const ChannelDev* chans, const S* f, TileBufs& tb, int 
 }
 
 template <typename S, typename R>
-void launch_interp_move(const ChannelDev* chans, int M, const MarkerBufs& mb, const S* f,
-                        TileBufs& tb, int parity, const double* phi_tbl, cudaStream_t st) {
-    const int B = tb.marker_block, G = (M + B - 1) / B;
-    k_interp_move<S, R><<<G, B, 0, st>>>(chans, M, mb, f, tb.tile_slot[parity],
-                                         static_cast<const R*>(tb.fin[parity]), phi_tbl);
+void launch_interp_move(const ChannelDev* chans, const CapsuleDev* caps, int ncaps, int M,
+                        const MarkerBufs& mb, const S* f, TileBufs& tb, int parity,
+                        const double* phi_tbl, cudaStream_t st) {
+    if constexpr (sizeof(R) == 4) {
+        (void)phi_tbl;
+        if (ncaps == 0) return;
+        k_interp_move_caps<S><<<(ncaps + MOVE_WARPS - 1) / MOVE_WARPS, MOVE_WARPS * 32,
+                                MOVE_WARPS * sizeof(MoveBox), st>>>(
+            caps, ncaps, chans, mb, f, tb.tile_slot[parity],
+            static_cast<const float*>(tb.fin[parity]));
+    } else {
+        const int B = tb.marker_block, G = (M + B - 1) / B;
+        k_interp_move<S, R><<<G, B, 0, st>>>(chans, M, mb, f, tb.tile_slot[parity],
+                                             static_cast<const R*>(tb.fin[parity]), phi_tbl);
+    }
 }
 
 #define SFG_INST(S, R)                                                                          \
@@ -1816,8 +1970,9 @@ void launch_interp_move(const ChannelDev* chans, int M, const MarkerBufs& mb, co
                                           TileBufs&, int, int, int, cudaStream_t);              \
     template void launch_tile_moments<S, R>(const ChannelDev*, const S*, TileBufs&, int,       \
                                             cudaStream_t);                                      \
-    template void launch_interp_move<S, R>(const ChannelDev*, int, const MarkerBufs&, const S*, \
-                                           TileBufs&, int, const double*, cudaStream_t);
+    template void launch_interp_move<S, R>(const ChannelDev*, const CapsuleDev*, int, int,     \
+                                           const MarkerBufs&, const S*, TileBufs&, int,        \
+                                           const double*, cudaStream_t);
 SFG_INST(double, double)
 SFG_INST(float, float)
 SFG_INST(__half, float)

@@ -120,8 +120,9 @@ template <typename S, typename R>
 void launch_tile_moments(const ChannelDev* chans, const S* f, TileBufs& tb, int grid,
                          cudaStream_t st);
 template <typename S, typename R>
-void launch_interp_move(const ChannelDev* chans, int M, const MarkerBufs& mb, const S* f,
-                        TileBufs& tb, int parity, const double* phi_tbl, cudaStream_t st);
+void launch_interp_move(const ChannelDev* chans, const CapsuleDev* caps, int ncaps, int M,
+                        const MarkerBufs& mb, const S* f, TileBufs& tb, int parity,
+                        const double* phi_tbl, cudaStream_t st);
 
 // Lattice kernels (lattice_f64.cu / lattice_f32.cu).
 struct LatticeLaunch {
