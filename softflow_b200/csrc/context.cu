@@ -270,6 +270,9 @@ struct sfg_context {
     cudaEvent_t ev_fork = nullptr, ev_contact = nullptr, ev_tiles = nullptr, ev_mom = nullptr;
     cudaEvent_t ev_lat1 = nullptr;      // the lattice pass over untouched force tiles
     cudaEvent_t ev_slots = nullptr;     // the step's slot records exist
+    // the learned gate's fallback flag beside the last spread, the step's
+    // flags beside the marker move
+    cudaEvent_t ev_gate = nullptr, ev_pn = nullptr, ev_lat = nullptr, ev_flags = nullptr;
     bool split_lattice = false;         // that pass beside the forcing (8-cell kernel; off:
                                         // the concurrent pass slowed the forcing more than it
                                         // saved on the ensemble)
@@ -476,7 +479,8 @@ static void free_all(sfg_context* c) {
         }
         c->side[i] = nullptr;
     }
-    for (cudaEvent_t* e : {&c->ev_fork, &c->ev_contact, &c->ev_tiles, &c->ev_mom, &c->ev_lat1, &c->ev_slots}) {
+    for (cudaEvent_t* e : {&c->ev_fork, &c->ev_contact, &c->ev_tiles, &c->ev_mom, &c->ev_lat1, &c->ev_slots,
+                           &c->ev_gate, &c->ev_pn, &c->ev_lat, &c->ev_flags}) {
         if (*e) cudaEventDestroy(*e);
         *e = nullptr;
     }
@@ -1139,7 +1143,8 @@ extern "C" int sfg_initialize(sfg_context* c) {
     CU(cudaStreamSynchronize(c->stream));
     if (c->M > 0 && !c->side[0]) {
         for (int i = 0; i < 3; ++i) CU(cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking));
-        for (cudaEvent_t* e : {&c->ev_fork, &c->ev_contact, &c->ev_tiles, &c->ev_mom, &c->ev_lat1, &c->ev_slots})
+        for (cudaEvent_t* e : {&c->ev_fork, &c->ev_contact, &c->ev_tiles, &c->ev_mom, &c->ev_lat1, &c->ev_slots,
+                           &c->ev_gate, &c->ev_pn, &c->ev_lat, &c->ev_flags})
             CU(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     }
     c->initialized = true;
@@ -1267,9 +1272,19 @@ static int enqueue_step_t(sfg_context* c, int p) {
             mark(c, SFG_PHASE_IBM_SPREAD);
             launch_mdf_interp<S, R>(c->d_chans, c->M, c->mb, fp, c->tb, p, 2, MDF_LEARNED, st);
             mark(c, SFG_PHASE_MDF_INTERP);
-            launch_plain_needed(c->d_chans, nch, c->tb, st);
+            // whether any channel falls back needs the gate residuals only:
+            // it is found beside the last spread, and the plain sweeps wait
+            if (par) {
+                CU(cudaEventRecord(c->ev_gate, st));
+                CU(cudaStreamWaitEvent(c->side[0], c->ev_gate, 0));
+                launch_plain_needed(c->d_chans, nch, c->tb, c->side[0]);
+                CU(cudaEventRecord(c->ev_pn, c->side[0]));
+            } else {
+                launch_plain_needed(c->d_chans, nch, c->tb, st);
+            }
             launch_spread<R>(c->d_chans, c->mb, c->tb, p, 2, MDF_LEARNED, 2, c->spread_grid,
                              c->d_status, st);
+            if (par) CU(cudaStreamWaitEvent(st, c->ev_pn, 0));
             mark(c, SFG_PHASE_IBM_SPREAD);
             launches += 6;
         }
@@ -1307,10 +1322,20 @@ static int enqueue_step_t(sfg_context* c, int p) {
         launches += 2;
     }
     mark(c, SFG_PHASE_LATTICE);
-    k_step_flags<<<(nch + 127) / 128, 128, 0, st>>>(c->d_chans, nch, c->d_stepped,
+    // the step's flags and the marker move are independent: the flags run
+    // beside the move and join before the step ends
+    const bool par_flags = c->M > 0 && !c->profiling && c->side[1] != nullptr;
+    cudaStream_t fs = st;
+    if (par_flags) {
+        CU(cudaEventRecord(c->ev_lat, st));
+        CU(cudaStreamWaitEvent(c->side[1], c->ev_lat, 0));
+        fs = c->side[1];
+    }
+    k_step_flags<<<(nch + 127) / 128, 128, 0, fs>>>(c->d_chans, nch, c->d_stepped,
                                                     c->d_adr_pending, c->d_c_fresh,
                                                     c->d_step_ctr, c->tb.resid_gate,
                                                     c->d_learned_steps, c->d_fallbacks);
+    if (par_flags) CU(cudaEventRecord(c->ev_flags, c->side[1]));
     mark(c, SFG_PHASE_BOOKKEEPING);
     launches += 2;
     if (c->M > 0) {
@@ -1319,6 +1344,7 @@ static int enqueue_step_t(sfg_context* c, int p) {
         mark(c, SFG_PHASE_INTERP_MOVE);
         launches += 1;
     }
+    if (par_flags) CU(cudaStreamWaitEvent(st, c->ev_flags, 0));
     c->launches = launches;
     return SFG_OK;
 }
