@@ -127,7 +127,9 @@ def test_contact_bookkeeping_exact(sfg, oracle_mod):
 
 
 @pytest.mark.parametrize("name,steps,tol", [("c0", 2000, 1e-4), ("c1", 200, 1e-4),
-                                            ("mini_c2", 200, 1e-4), ("seam_single", 200, 1e-4)])
+                                            ("mini_c2", 200, 1e-4), ("seam_single", 200, 1e-4),
+                                            ("narrow_seam", 200, 1e-4),
+                                            ("contact_brute", 200, 1e-4)])
 def test_fp32_velocity(sfg, oracle_mod, name, steps, tol):
     case = CASES[name]
     o = build_oracle(case)
@@ -144,7 +146,7 @@ def test_fp32_velocity(sfg, oracle_mod, name, steps, tol):
 
 
 @pytest.mark.parametrize("name,steps,tol", [("c0", 2000, 1e-3), ("c1", 2000, 1e-3),
-                                            ("mini_c2", 200, 1e-3)])
+                                            ("mini_c2", 200, 1e-3), ("narrow_seam", 200, 1e-3)])
 def test_fp16s_velocity(sfg, oracle_mod, name, steps, tol):
     case = CASES[name]
     o = build_oracle(case)
