@@ -1025,9 +1025,11 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
 // every launch shape and whether a channel runs alone or in an ensemble; the
 // marker lists need no sort.  Each value is v = q 2^-38 with the integer q
 // split into a low part of 20 bits (unsigned, in [0, 2^20)) and a high part
-// (signed): a cell takes at most SPREAD_LIST_MAX + 1 low parts per sweep
-// (below 2^32), and the high parts hold sums up to 2^13 in magnitude, far
-// beyond any lattice force.
+// (signed).  A cell takes at most one term per list entry (channels at
+// least 4 cells wide), so at most SPREAD_LIST_MAX = 4,096 low parts a sweep,
+// whose sum stays below 2^32; the high parts are summed modulo 2^32, exact
+// while the cell's sum stays below 2^13 in magnitude, far beyond any
+// lattice force.
 //
 // A cell that no stencil point of the tile's markers reaches (with weight
 // above 1e-15) receives nothing in any sweep of the step (the lists do not
