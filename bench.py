@@ -445,6 +445,16 @@ def run_product(args, world, rank, local, pg):
         K = max(p.params.ibm_iterations for p in plans)
         spread = spread_roofline(ens, plans, phases["ibm_spread"] / prof_steps,
                                  3 if (learned and K > 2) else K, peak, peak_kind)
+    # the lattice kernel also reads the force tiles' F and G (two floats each
+    # per cell) where markers force the fluid: reported beside the
+    # populations-only figure
+    lattice_force = {}
+    if spread is not None and lat_ms > 0:
+        ftb = spread["force_tiles"] * SLOT_FINAL_BYTES
+        ach_f = (alg_bytes + ftb) / (lat_ms / 1e3) / 1e9
+        lattice_force = {"force_tile_bytes_per_launch": ftb,
+                         "achieved_with_force_tiles": ach_f,
+                         "frac_with_force_tiles": ach_f / peak}
 
     # e2e: host-resident initial state, per-step marker readback
     e2e = run_e2e(args, plans, ens, pg, local)
@@ -527,6 +537,7 @@ def run_product(args, world, rank, local, pg):
                      "peak_source": peak_kind,
                      "share_of_step": phases["lattice"] / total_phase,
                      "algorithmic_bytes_per_launch": alg_bytes,
+                     **lattice_force,
                      # DRAM bytes need a profiler; the bench does not run one
                      "traffic": None},
         "spread_roofline": spread,
