@@ -664,11 +664,10 @@ constexpr size_t spread_smem() { return sizeof(SpreadWarpSmem<A>) * SPREAD_WARPS
 // the reference's order.  On a channel's last sweep the warp also adds the
 // body force on FLUID cells, applies the force cap and counts capped cells
 // (simulation.cpp:540-609), writing the final tile force `fin` (type R).
-// The tile accumulates in R: FP64 contexts in double (bit for bit), the
-// FP32-arithmetic modes in float (each contribution rounded once to float,
-// the sums in float; `acc` / `acc0` then hold float pairs).
-// Resident CTAs per SM asked of the compiler: 4 for the float form (64
-// registers; its shared memory allows 6), 3 for the double form.
+// The tile accumulates in R; the step launches it for FP64 contexts (double,
+// bit for bit), the FP32-arithmetic modes run k_spread_fx.
+// Resident CTAs per SM asked of the compiler: 3 for the double form (4 for a
+// float instantiation).
 template <typename R>
 constexpr int spread_min_ctas() { return sizeof(R) == 4 ? 4 : 3; }
 
@@ -1017,9 +1016,9 @@ k_spread(const ChannelDev* __restrict__ chans, const SlotInfo* __restrict__ slot
 }
 
 // The spread of the FP32-arithmetic modes (FP32 and FP16-shifted storage):
-// the same contributions as k_spread<float> ((float)f (float)w (float)ds for
-// each stencil point with w > 1e-15), summed per cell exactly in fixed point
-// instead of in float.  Integer addition does not depend on the order of the
+// the reference's contributions (f w) ds of each stencil point with
+// w > 1e-15, formed as (float)f (float)w (float)ds and summed per cell
+// exactly in fixed point.  Integer addition does not depend on the order of the
 // terms, so the lanes of a warp add any markers' points in any order, with
 // 32-bit shared-memory atomics, and the result is the same on every run, in
 // every launch shape and whether a channel runs alone or in an ensemble; the
